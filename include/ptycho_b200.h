@@ -1,0 +1,137 @@
+/*
+ * C ABI of the B200 multislice mixed-probe ptychography path.
+ *
+ * Every entry point takes raw device pointers, sizes and a cudaStream_t passed
+ * as void* (NULL = legacy default stream), launches asynchronously on that
+ * stream and returns a status code (PTYCHO_OK = 0).  On failure a message is
+ * kept per host thread and returned by ptycho_get_last_error().  Nothing here
+ * allocates device memory: callers (the Python host layer uses the PyTorch
+ * caching allocator) pass every buffer, including scratch.  Complex arrays are
+ * interleaved float32 pairs (complex64), C-contiguous.
+ *
+ * Reference interfaces replaced (quantem 0.1.8, src/quantem/diffractive_imaging):
+ *   ptycho_forward_loss      probe_models.py:718-720 (ProbePixelated.forward),
+ *                            object_models.py:678-680 (ObjectPixelated.forward),
+ *                            ptychography_base.py:892-906 (forward_operator),
+ *                            detector_models.py:22-30 (DetectorPixelated.forward),
+ *                            ptychography_base.py:908-932 (error_estimate)
+ *   ptycho_forward_adjoint   the above plus loss.backward() of ptychography.py:326-328
+ *   ptycho_obj_constrain     object_models.py:289-300 (apply_hard_constraints, complex)
+ *   ptycho_obj_constrain_vjp autograd of the same constraint
+ *   ptycho_fft2              torch.fft.fft2/ifft2 of the probe stack
+ *                            (ptycho_utils.py:133-135) and of the probe gradient
+ *   ptycho_reduce_partials,
+ *   ptycho_reduce_loss       deterministic reductions of per-CTA partials
+ *   ptycho_adam_step,
+ *   ptycho_sgd_step          torch.optim.Adam/AdamW/SGD step (optimizer_mixin.py:117-123,
+ *                            ptychography_opt.py:336-344)
+ */
+#ifndef PTYCHO_B200_H
+#define PTYCHO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  PTYCHO_OK = 0,
+  PTYCHO_ERR_INVALID = 1,     /* bad pointer, size, alignment or option */
+  PTYCHO_ERR_UNSUPPORTED = 2, /* probe size / configuration not built */
+  PTYCHO_ERR_CUDA = 3,        /* CUDA launch or runtime error */
+  PTYCHO_ERR_NONFINITE = 4    /* reserved: non-finite values detected */
+};
+
+enum {
+  PTYCHO_LOSS_L2_AMPLITUDE = 0,
+  PTYCHO_LOSS_L1_AMPLITUDE = 1,
+  PTYCHO_LOSS_L2_INTENSITY = 2,
+  PTYCHO_LOSS_L1_INTENSITY = 3,
+  PTYCHO_LOSS_POISSON = 4
+};
+
+/* Arguments of one position batch.  Shapes: S slices, P probe modes, N x N probe
+ * window (N = 64 or 128), object Ho x Wo, npos scan positions, B positions in
+ * this batch, grid CTAs. */
+typedef struct ptycho_batch_args {
+  const void* obj;           /* complex64 (S, Ho, Wo): hard-constrained object */
+  const void* probe_hat;     /* complex64 (P, N, N): fft2 of the probe modes */
+  const void* prop;          /* complex64 (S-1, N, N): Fresnel propagators (may be NULL if S == 1) */
+  const float* positions;    /* float32 (npos, 2): scan positions [px] (row, col) */
+  const int64_t* batch_idx;  /* int64 (B,): positions / targets rows of this batch */
+  const float* targets;      /* float32 (npos, N, N): measured amplitudes/intensities, detector layout */
+  const float* mask;         /* float32 (N, N): detector mask, detector layout */
+  void* grad_obj;            /* complex64 (S, Ho, Wo): object gradient, accumulated (adjoint only) */
+  void* probe_grad_part;     /* complex64 (grid, P, N, N): per-CTA partials (adjoint only) */
+  void* scratch;             /* complex64 (grid, P*S + P, N, N) (adjoint only) */
+  double* loss_part;         /* float64 (grid,): per-CTA loss partials */
+  float* out_intensity;      /* optional float32 (B, N, N): predicted intensities, detector layout */
+  void* out_exit;            /* optional complex64 (P, B, N, N): exit waves */
+  void* out_waves;           /* optional complex64 (S, P, B, N, N): wave entering each slice */
+  int* status;               /* optional int32: incremented by the count of non-finite intensities */
+  int n, S, P, B, Ho, Wo, npos, grid;
+  int loss_type;             /* PTYCHO_LOSS_* */
+  float loss_scale;          /* npos_total / (B * mean_intensity) */
+  float inv_mean_intensity;  /* 1 / mean_intensity */
+} ptycho_batch_args;
+
+/* Copy the last error message of this host thread into buf (NUL-terminated). */
+int ptycho_get_last_error(char* buf, size_t len);
+
+/* Library ABI version (increments on incompatible changes). */
+int ptycho_abi_version(void);
+
+/* Number of SMs of the current device. */
+int ptycho_sm_count(int* out);
+
+/* Number of complex64 elements of scratch / partial buffers for a batch launch. */
+int ptycho_workspace_elems(int n, int S, int P, int grid, int64_t* scratch_elems,
+                           int64_t* partial_elems);
+
+/* Forward model + loss of one batch (no gradients). */
+int ptycho_forward_loss(const ptycho_batch_args* a, void* stream);
+
+/* Forward model + loss + adjoint of one batch in a single persistent launch. */
+int ptycho_forward_adjoint(const ptycho_batch_args* a, void* stream);
+
+/* count 2-D FFTs of n x n complex64 arrays, out = scale * (i)fft2(in), unnormalised
+ * transform; in and out may alias. */
+int ptycho_fft2(const void* in, void* out, int count, int n, int inverse, float scale, void* stream);
+
+/* out[i] = sum_g parts[g * count + i] (complex64), fixed summation order. */
+int ptycho_reduce_partials(const void* parts, void* out, int nparts, int64_t count, void* stream);
+
+/* out[0] = (float) sum_g parts[g], fixed summation order. */
+int ptycho_reduce_loss(const double* parts, int nparts, float* out, void* stream);
+
+/* Complex object hard constraint: out = clamp(|o|,0,1) exp(i(angle(o) - mean angle)).
+ * work: float64 scratch of nwork >= 2 * ptycho_reduce_blocks() elements. */
+int ptycho_obj_constrain(const void* obj, void* out, int64_t count, double* work, int nwork, void* stream);
+
+/* Gradient of ptycho_obj_constrain: grad_raw = scale[0] * J^H grad_c (torch convention).
+ * `work` must be the buffer used by the matching ptycho_obj_constrain call;
+ * `scale` is a device float (e.g. autograd's incoming gradient), NULL means 1. */
+int ptycho_obj_constrain_vjp(const void* obj, const void* grad_c, void* grad_raw, int64_t count,
+                             double* work, int nwork, const float* scale, void* stream);
+
+/* Blocks used by the reductions (size of `work` is 2x this). */
+int ptycho_reduce_blocks(void);
+
+/* torch.optim.Adam / AdamW step on float32 data viewed as reals.  bc1 = 1 - beta1^t,
+ * bc2_sqrt = sqrt(1 - beta2^t); decoupled != 0 selects AdamW weight decay.  lr_dev,
+ * if not NULL, is a device float that overrides lr (graph-replay friendly). */
+int ptycho_adam_step(float* param, const float* grad, float* exp_avg, float* exp_avg_sq, int64_t count,
+                     float lr, const float* lr_dev, float beta1, float beta2, float eps,
+                     float weight_decay, int decoupled, float bc1, float bc2_sqrt, void* stream);
+
+/* torch.optim.SGD step without momentum: param -= lr * (grad + wd * param). */
+int ptycho_sgd_step(float* param, const float* grad, int64_t count, float lr, const float* lr_dev,
+                    float weight_decay, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PTYCHO_B200_H */

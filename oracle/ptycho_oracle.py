@@ -1,0 +1,445 @@
+"""CPU oracle for the multislice mixed-probe ptychography iteration.
+
+TEST INFRASTRUCTURE ONLY.  This module restates, in numpy/scipy, the algorithm
+of quantem.diffractive_imaging's gradient-descent iteration so that the CUDA
+path can be checked against it.  Only ``tests/``, ``__graft_entry__.smoke()``
+and ``bench.py``'s CPU-baseline leg may import it; the product package never
+does, and the product fails loudly when its CUDA library is missing.
+
+Precision: every function is dtype-generic.  Parity checks run it in
+complex128/float64 (with the reference's float32 constants restated in float64,
+see ``propagators`` and ``translation_ramp``); the CPU baseline runs it in
+complex64/float32 like the reference's default configuration.
+
+Pinning: the reference ships no golden vectors for this path (its two gradient
+tests compare autograd against analytic gradients by SSIM only).  This oracle is
+pinned against fixtures produced by running the reference itself
+(``tests/golden/make_golden.py``; see ``tests/test_oracle_golden.py``).
+
+Conventions (all from the reference):
+* complex gradients follow torch: grad = dL/dRe + i dL/dIm;
+* FFT norms: propagation uses the unnormalised forward / 1/N inverse pair
+  (ptychography_base.py:988), the detector the orthonormal FFT
+  (detector_models.py:28);
+* object patches are corner-centred windows with modulo wrap
+  (dataset_models.py:514-535); positions are rounded half-to-even
+  (dataset_models.py:1490, torch.round).
+"""
+from __future__ import annotations
+
+import math
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+import scipy.fft as sfft
+
+_WORKERS = int(os.environ.get("QUANTEM_ORACLE_WORKERS", "1"))
+
+
+def set_workers(n: int) -> None:
+    """Number of threads scipy.fft may use (CPU-baseline timing uses all)."""
+    global _WORKERS
+    _WORKERS = max(1, int(n))
+
+
+def fft2(x, norm="backward"):
+    return sfft.fft2(x, axes=(-2, -1), norm=norm, workers=_WORKERS)
+
+
+def ifft2(x, norm="backward"):
+    return sfft.ifft2(x, axes=(-2, -1), norm=norm, workers=_WORKERS)
+
+
+def real_dtype(cdtype):
+    return np.float64 if np.dtype(cdtype) == np.complex128 else np.float32
+
+
+# ----------------------------------------------------------------------------
+# constants and setup restatements
+# ----------------------------------------------------------------------------
+
+def electron_wavelength_angstrom(energy_ev: float) -> float:
+    """Relativistic electron wavelength [A]; core/utils/utils.py:97-104."""
+    m = 9.109383e-31
+    e = 1.602177e-19
+    c = 299792458.0
+    h = 6.62607e-34
+    return (
+        h / math.sqrt(2 * m * e * energy_ev) / math.sqrt(1 + e * energy_ev / 2 / m / c**2) * 1e10
+    )
+
+
+def fftfreq_index(n: int) -> np.ndarray:
+    """Integer fftfreq(n, d=1/n) used for corner-centred patches."""
+    return np.fft.fftfreq(n, d=1.0 / n).astype(np.int64)
+
+
+def propagators(roi_shape, sampling, energy, slice_thicknesses, tilt_mrad=(0.0, 0.0),
+                cdtype=np.complex128):
+    """Fresnel propagators (S-1, H, W); probe_models.py:376-427.
+
+    The reference evaluates k^2 in complex64 (probe_models.py:407,413); this
+    restatement evaluates the same formula in the precision of ``cdtype``.
+    """
+    dz = np.atleast_1d(np.asarray(slice_thicknesses, dtype=np.float64))
+    if dz.size == 0:
+        return np.zeros((0, *roi_shape), dtype=cdtype)
+    kr = np.fft.fftfreq(int(roi_shape[0]), float(sampling[0]))
+    kc = np.fft.fftfreq(int(roi_shape[1]), float(sampling[1]))
+    k2 = kr[:, None] ** 2 + kc[None, :] ** 2
+    lam = electron_wavelength_angstrom(energy)
+    props = np.exp(-1j * np.pi * lam * dz[:, None, None] * k2[None])
+    tr, tc = tilt_mrad
+    if tr != 0:
+        props = props * np.exp(-2j * np.pi * dz[:, None, None] * np.tan(tr / 1e3) * kr[None, :, None])
+    if tc != 0:
+        props = props * np.exp(-2j * np.pi * dz[:, None, None] * np.tan(tc / 1e3) * kc[None, None, :])
+    return props.astype(cdtype)
+
+
+def translation_ramp(frac: np.ndarray, shape, cdtype=np.complex128) -> np.ndarray:
+    """Sub-pixel Fourier translation ramp (B, H, W); ptycho_utils.py:156-176."""
+    nr, nc = shape
+    kr = np.fft.fftfreq(nr, d=1.0)
+    kc = np.fft.fftfreq(nc, d=1.0)
+    r = frac[:, 0][:, None, None]
+    c = frac[:, 1][:, None, None]
+    ramp = np.exp(-2j * np.pi * kr[None, :, None] * r) * np.exp(-2j * np.pi * kc[None, None, :] * c)
+    return ramp.astype(cdtype)
+
+
+def round_half_even(x: np.ndarray) -> np.ndarray:
+    return np.round(x)  # numpy rounds half to even, like torch.round
+
+
+def split_positions(positions_px: np.ndarray):
+    """(r0, c0) integer patch origins and fractional offsets; dataset_models.py:1487-1490."""
+    rounded = round_half_even(positions_px)
+    frac = positions_px - rounded
+    return rounded.astype(np.int64), frac
+
+
+def patch_rows_cols(origins: np.ndarray, roi_shape, obj_shape):
+    """Wrapped row / column index grids of every patch; dataset_models.py:514-535."""
+    fr = fftfreq_index(int(roi_shape[0]))
+    fc = fftfreq_index(int(roi_shape[1]))
+    rows = (origins[:, 0][:, None] + fr[None, :]) % int(obj_shape[0])
+    cols = (origins[:, 1][:, None] + fc[None, :]) % int(obj_shape[1])
+    return rows, cols  # (B, H), (B, W)
+
+
+def gather_patches(obj: np.ndarray, rows: np.ndarray, cols: np.ndarray) -> np.ndarray:
+    """(S, B, H, W) patches; object_models.py:252-265."""
+    return obj[:, rows[:, :, None], cols[:, None, :]]
+
+
+def scatter_patches(grad_patches: np.ndarray, rows, cols, obj_shape_3d) -> np.ndarray:
+    """Adjoint of ``gather_patches`` (index_add); ptycho_utils.py:215-236."""
+    out = np.zeros(obj_shape_3d, dtype=grad_patches.dtype)
+    S = obj_shape_3d[0]
+    for s in range(S):
+        np.add.at(out[s], (rows[:, :, None], cols[:, None, :]), grad_patches[s])
+    return out
+
+
+# ----------------------------------------------------------------------------
+# hard constraints
+# ----------------------------------------------------------------------------
+
+def constrain_object(obj: np.ndarray) -> np.ndarray:
+    """Complex-object hard constraint; object_models.py:289-300.
+
+    o' = clamp(|o|, 0, 1) * exp(i (angle(o) - mean(angle(o)))), mean over the
+    whole (S, Ho, Wo) array.
+    """
+    amp = np.clip(np.abs(obj), 0.0, 1.0)
+    ph = np.angle(obj)
+    ph = ph - ph.mean()
+    return (amp * np.exp(1j * ph)).astype(obj.dtype)
+
+
+def constrain_object_vjp(obj: np.ndarray, grad_out: np.ndarray) -> np.ndarray:
+    """Vector-Jacobian product of ``constrain_object`` (torch gradient convention).
+
+    clamp passes the gradient where 0 <= |o| <= 1 (inclusive), abs contributes
+    sgn(o) * g_a, angle contributes i o / |o|^2 * g_phi (zero at o == 0), and the
+    mean removal subtracts the mean of g_phi over the whole object.
+    """
+    mag = np.abs(obj)
+    amp = np.clip(mag, 0.0, 1.0)
+    ph = np.angle(obj)
+    th = ph - ph.mean()
+    e = np.exp(1j * th)
+    ge = grad_out * np.conj(e)
+    g_amp = ge.real
+    g_th = amp * ge.imag
+    g_ph = g_th - g_th.mean()
+    g_mag = np.where((mag >= 0.0) & (mag <= 1.0), g_amp, 0.0)
+    safe = np.where(mag == 0, 1.0, mag)
+    sgn = np.where(mag == 0, 0.0, obj / safe)
+    dang = np.where(mag == 0, 0.0, 1j * obj / safe**2)
+    return (g_mag * sgn + g_ph * dang).astype(obj.dtype)
+
+
+def gram_schmidt(probe: np.ndarray):
+    """Mixed-state probe orthogonalisation + intensity sort; probe_models.py:484-525.
+
+    Modified Gram-Schmidt with the running vector (as the reference loop), each
+    mode rescaled to its original norm, then sorted by descending intensity.
+    Returns (probes_sorted, order, cache-for-vjp).
+    """
+    P = probe.shape[0]
+    flat = probe.reshape(P, -1)
+    n0 = np.sqrt(np.sum(flat.real**2 + flat.imag**2, axis=1))
+    qs, steps = [], []
+    for i in range(P):
+        u = flat[i].copy()
+        hist = []
+        for j in range(len(qs)):
+            c = np.sum(np.conj(qs[j]) * u)
+            hist.append((u.copy(), c))
+            u = u - c * qs[j]
+        nrm = np.sqrt(np.sum(u.real**2 + u.imag**2))
+        nrm_c = max(nrm, 1e-12)
+        qs.append(u / nrm_c)
+        steps.append((hist, u, nrm, nrm_c))
+    q = np.stack(qs)
+    out = q * n0[:, None]
+    inten = np.sum(np.abs(out) ** 2, axis=1)
+    order = np.argsort(-inten, kind="stable")
+    cache = dict(flat=flat, n0=n0, q=q, steps=steps, order=order)
+    return out[order].reshape(probe.shape), order, cache
+
+
+def gram_schmidt_vjp(cache, grad_sorted: np.ndarray) -> np.ndarray:
+    """Reverse mode of ``gram_schmidt`` (torch gradient convention)."""
+    flat, n0, q, steps, order = (cache[k] for k in ("flat", "n0", "q", "steps", "order"))
+    P, n = flat.shape
+    g_out = np.zeros_like(flat)
+    g_out[order] = grad_sorted.reshape(P, n)
+    g_q = g_out * n0[:, None]
+    g_n0 = np.sum((np.conj(q) * g_out).real, axis=1)
+    g_flat = np.zeros_like(flat)
+    for i in range(P):
+        g_flat[i] += flat[i] / max(n0[i], 1e-300) * g_n0[i]
+    for i in reversed(range(P)):
+        hist, u, nrm, nrm_c = steps[i]
+        gq = g_q[i]
+        g_u = gq / nrm_c
+        if nrm >= 1e-12:
+            g_nrm = -np.sum((np.conj(u) * gq).real) / nrm_c**2
+            g_u = g_u + u / nrm * g_nrm
+        for j in reversed(range(len(hist))):
+            u_prev, c = hist[j]
+            # u = u_prev - c q_j
+            g_c = -np.sum(np.conj(q[j]) * g_u)
+            g_q[j] += -np.conj(c) * g_u
+            # c = sum(conj(q_j) * u_prev)
+            g_uprev = g_u + q[j] * g_c
+            g_q[j] += np.conj(g_c) * u_prev
+            g_u = g_uprev
+        g_flat[i] += g_u
+    return g_flat.reshape(grad_sorted.shape)
+
+
+# ----------------------------------------------------------------------------
+# forward model and loss
+# ----------------------------------------------------------------------------
+
+@dataclass
+class ForwardState:
+    rows: np.ndarray
+    cols: np.ndarray
+    ramp: np.ndarray
+    patches: np.ndarray          # (S, B, H, W)
+    waves: list = field(default_factory=list)  # incoming wave at each slice, (P, B, H, W)
+    far: np.ndarray = None       # orthonormal far field (P, B, H, W)
+    intensity: np.ndarray = None  # corner-centred sum over modes (B, H, W)
+
+
+def forward(obj_c: np.ndarray, probe_o: np.ndarray, positions_px: np.ndarray,
+            props: np.ndarray) -> ForwardState:
+    """Batch forward model.
+
+    probe shift: ptycho_utils.py:128-139 (fft2 -> ramp -> ifft2), probe_models.py:718-720;
+    multislice: ptychography_base.py:934-947, 970-989;
+    detector: detector_models.py:22-30 (orthonormal FFT, |.|^2 summed over modes).
+    The returned intensity is corner-centred (before the detector fftshift).
+    """
+    S = obj_c.shape[0]
+    H, W = probe_o.shape[-2:]
+    origins, frac = split_positions(positions_px)
+    rows, cols = patch_rows_cols(origins, (H, W), obj_c.shape[-2:])
+    ramp = translation_ramp(frac, (H, W), probe_o.dtype)
+    patches = gather_patches(obj_c, rows, cols)
+    psi = ifft2(fft2(probe_o)[:, None] * ramp[None])  # (P, B, H, W)
+    st = ForwardState(rows=rows, cols=cols, ramp=ramp, patches=patches)
+    for s in range(S):
+        st.waves.append(psi)
+        chi = patches[s][None] * psi
+        if s < S - 1:
+            psi = ifft2(fft2(chi) * props[s][None, None])
+        else:
+            psi = chi
+    st.far = fft2(psi, norm="ortho")
+    st.intensity = np.sum(st.far.real**2 + st.far.imag**2, axis=0)
+    return st
+
+
+def detector_intensities(state: ForwardState) -> np.ndarray:
+    """fftshifted predicted intensities (B, H, W) as DetectorPixelated.forward returns."""
+    return np.fft.fftshift(state.intensity, axes=(-2, -1))
+
+
+LOSS_TYPES = ("l2_amplitude", "l1_amplitude", "l2_intensity", "l1_intensity", "poisson")
+
+
+def loss_and_seed(intensity_cc: np.ndarray, targets: np.ndarray, mask: np.ndarray,
+                  num_gpts: int, mean_intensity: float, loss_type: str = "l2_amplitude"):
+    """Consistency loss and dL/dI (corner-centred); ptychography_base.py:908-932.
+
+    ``targets``/``mask`` are in detector (centred) layout, so they are
+    ifftshifted onto the corner-centred intensity grid first.
+    """
+    B = intensity_cc.shape[0]
+    t = np.fft.ifftshift(targets, axes=(-2, -1))
+    m = np.fft.ifftshift(mask, axes=(-2, -1))
+    scale = 1.0 / (B / num_gpts) / mean_intensity
+    if "amplitude" in loss_type:
+        pred = np.sqrt(intensity_cc + 1e-9)
+        dpred_dI = 0.5 / pred
+    else:
+        pred = intensity_cc
+        dpred_dI = np.ones_like(pred)
+    diff = pred * m - t * m
+    if loss_type.startswith("l2"):
+        loss = np.sum(diff**2) * scale
+        dL_dpred = 2 * diff * m * scale
+    elif loss_type.startswith("l1"):
+        loss = np.sum(np.abs(diff)) * scale
+        dL_dpred = np.sign(diff) * m * scale
+    elif loss_type == "poisson":
+        loss = np.sum(pred - t * np.log(pred + 1e-6)) / mean_intensity
+        dL_dpred = (1 - t / (pred + 1e-6)) / mean_intensity
+    else:
+        raise ValueError(loss_type)
+    return float(loss), dL_dpred * dpred_dI
+
+
+def adjoint(obj_c, probe_o, props, st: ForwardState, dL_dI: np.ndarray):
+    """Gradients of the batch loss w.r.t. the constrained object and the
+    orthogonalised probe (torch convention), by reversing ``forward``."""
+    S = obj_c.shape[0]
+    H, W = probe_o.shape[-2:]
+    g_far = 2.0 * st.far * dL_dI[None]
+    g = ifft2(g_far, norm="ortho")  # adjoint of the orthonormal FFT
+    g_patch = np.zeros_like(st.patches)
+    for s in reversed(range(S)):
+        psi = st.waves[s]
+        g_patch[s] = np.sum(np.conj(psi) * g, axis=0)
+        g = np.conj(st.patches[s])[None] * g
+        if s > 0:
+            g = ifft2(fft2(g) * np.conj(props[s - 1])[None, None])
+    # probe shift adjoint: ifft2(sum_b conj(ramp_b) * fft2(g_b))
+    acc = np.sum(fft2(g) * np.conj(st.ramp)[None], axis=1)
+    g_probe = ifft2(acc)
+    g_obj = scatter_patches(g_patch, st.rows, st.cols, obj_c.shape)
+    return g_obj, g_probe
+
+
+def batch_loss_and_grads(obj_c, probe_o, positions_px, props, targets, mask, num_gpts,
+                         mean_intensity, loss_type="l2_amplitude"):
+    st = forward(obj_c, probe_o, positions_px, props)
+    loss, dI = loss_and_seed(st.intensity, targets, mask, num_gpts, mean_intensity, loss_type)
+    g_obj, g_probe = adjoint(obj_c, probe_o, props, st, dI)
+    return loss, g_obj, g_probe, st
+
+
+def full_gradients(obj_raw, probe_raw, positions_px, props, targets, mask, num_gpts,
+                   mean_intensity, upsample_factor, orthogonalize=True,
+                   loss_type="l2_amplitude"):
+    """Loss and gradients w.r.t. the raw parameters, as Ptychography.backward
+    leaves them (autograd branch, ptychography.py:326-332): the object gradient
+    is scaled by upsample_factor**2 / 2."""
+    obj_c = constrain_object(obj_raw)
+    if orthogonalize:
+        probe_o, _, cache = gram_schmidt(probe_raw)
+    else:
+        probe_o, cache = probe_raw, None
+    loss, g_obj_c, g_probe_o, st = batch_loss_and_grads(
+        obj_c, probe_o, positions_px, props, targets, mask, num_gpts, mean_intensity, loss_type)
+    g_obj = constrain_object_vjp(obj_raw, g_obj_c) * (upsample_factor**2 / 2)
+    g_probe = gram_schmidt_vjp(cache, g_probe_o) if orthogonalize else g_probe_o
+    return loss, g_obj, g_probe, st
+
+
+# ----------------------------------------------------------------------------
+# optimiser
+# ----------------------------------------------------------------------------
+
+@dataclass
+class AdamState:
+    step: int = 0
+    exp_avg: np.ndarray = None
+    exp_avg_sq: np.ndarray = None
+
+
+def adam_step(param: np.ndarray, grad: np.ndarray, st: AdamState, lr, betas=(0.9, 0.999),
+              eps=1e-8, weight_decay=0.0, decoupled=False):
+    """torch.optim.Adam / AdamW update on the real view of a complex parameter
+    (optimizer_mixin.py:117-123 selects the torch optimiser)."""
+    rd = real_dtype(param.dtype) if np.iscomplexobj(param) else param.dtype
+    p = param.view(rd) if np.iscomplexobj(param) else param
+    g = grad.astype(param.dtype).view(rd) if np.iscomplexobj(param) else grad
+    if st.exp_avg is None:
+        st.exp_avg = np.zeros_like(p)
+        st.exp_avg_sq = np.zeros_like(p)
+    st.step += 1
+    b1, b2 = betas
+    if weight_decay != 0:
+        if decoupled:
+            p *= 1 - lr * weight_decay
+        else:
+            g = g + weight_decay * p
+    st.exp_avg += (g - st.exp_avg) * (1 - b1)
+    st.exp_avg_sq *= b2
+    st.exp_avg_sq += (1 - b2) * g * g
+    bc1 = 1 - b1**st.step
+    bc2 = 1 - b2**st.step
+    denom = np.sqrt(st.exp_avg_sq) / math.sqrt(bc2) + eps
+    p -= (lr / bc1) * st.exp_avg / denom
+    return param
+
+
+def sgd_step(param, grad, lr):
+    param -= lr * grad.astype(param.dtype)
+    return param
+
+
+# ----------------------------------------------------------------------------
+# batching
+# ----------------------------------------------------------------------------
+
+def batch_order(rng: np.random.Generator, num: int, batch_size: int):
+    """One epoch of SimpleBatcher without validation split; ptycho_utils.py:91-96."""
+    order = rng.permutation(np.arange(num))
+    return [order[i:i + batch_size] for i in range(0, num, batch_size)]
+
+
+# ----------------------------------------------------------------------------
+# synthetic data helpers
+# ----------------------------------------------------------------------------
+
+def gaussian_atom_phase(shape, n_atoms, sigma_px, peak_rad, rng):
+    """Sum of isotropic Gaussian atoms at uniform positions (periodic)."""
+    H, W = shape
+    out = np.zeros((H, W), dtype=np.float64)
+    rr = np.arange(H)[:, None]
+    cc = np.arange(W)[None, :]
+    pos = rng.uniform(0, 1, size=(n_atoms, 2)) * np.array([H, W])
+    for r0, c0 in pos:
+        dr = (rr - r0 + H / 2) % H - H / 2
+        dc = (cc - c0 + W / 2) % W - W / 2
+        out += np.exp(-(dr**2 + dc**2) / (2 * sigma_px**2))
+    return peak_rad * out

@@ -1,0 +1,122 @@
+"""ctypes binding of libptycho_b200.so (the C ABI declared in include/ptycho_b200.h).
+
+The library is loaded from ``quantem_b200/lib`` inside this source tree.  There
+is no fallback: if the library is missing or cannot be loaded, every call raises
+``RuntimeError`` with the reason.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "lib", "libptycho_b200.so")
+
+PTYCHO_OK = 0
+ERR_NAMES = {1: "invalid argument", 2: "unsupported configuration", 3: "CUDA error", 4: "non-finite values"}
+
+LOSS_TYPES = {
+    "l2_amplitude": 0,
+    "l1_amplitude": 1,
+    "l2_intensity": 2,
+    "l1_intensity": 3,
+    "poisson": 4,
+}
+
+# Every symbol include/ptycho_b200.h declares.
+EXPORTED = (
+    "ptycho_get_last_error",
+    "ptycho_abi_version",
+    "ptycho_sm_count",
+    "ptycho_workspace_elems",
+    "ptycho_forward_loss",
+    "ptycho_forward_adjoint",
+    "ptycho_fft2",
+    "ptycho_reduce_partials",
+    "ptycho_reduce_loss",
+    "ptycho_obj_constrain",
+    "ptycho_obj_constrain_vjp",
+    "ptycho_reduce_blocks",
+    "ptycho_adam_step",
+    "ptycho_sgd_step",
+)
+
+_vp = ctypes.c_void_p
+_i64 = ctypes.c_int64
+_int = ctypes.c_int
+_flt = ctypes.c_float
+
+
+class BatchArgs(ctypes.Structure):
+    """Mirror of ``ptycho_batch_args``."""
+
+    _fields_ = [
+        ("obj", _vp), ("probe_hat", _vp), ("prop", _vp), ("positions", _vp), ("batch_idx", _vp),
+        ("targets", _vp), ("mask", _vp), ("grad_obj", _vp), ("probe_grad_part", _vp),
+        ("scratch", _vp), ("loss_part", _vp), ("out_intensity", _vp), ("out_exit", _vp),
+        ("out_waves", _vp), ("status", _vp),
+        ("n", _int), ("S", _int), ("P", _int), ("B", _int), ("Ho", _int), ("Wo", _int),
+        ("npos", _int), ("grid", _int), ("loss_type", _int),
+        ("loss_scale", _flt), ("inv_mean_intensity", _flt),
+    ]
+
+
+_lock = threading.Lock()
+_lib = None
+
+
+def _declare(lib):
+    sig = {
+        "ptycho_get_last_error": (_int, [ctypes.c_char_p, ctypes.c_size_t]),
+        "ptycho_abi_version": (_int, []),
+        "ptycho_sm_count": (_int, [ctypes.POINTER(_int)]),
+        "ptycho_workspace_elems": (_int, [_int, _int, _int, _int, ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
+        "ptycho_forward_loss": (_int, [ctypes.POINTER(BatchArgs), _vp]),
+        "ptycho_forward_adjoint": (_int, [ctypes.POINTER(BatchArgs), _vp]),
+        "ptycho_fft2": (_int, [_vp, _vp, _int, _int, _int, _flt, _vp]),
+        "ptycho_reduce_partials": (_int, [_vp, _vp, _int, _i64, _vp]),
+        "ptycho_reduce_loss": (_int, [_vp, _int, _vp, _vp]),
+        "ptycho_obj_constrain": (_int, [_vp, _vp, _i64, _vp, _int, _vp]),
+        "ptycho_obj_constrain_vjp": (_int, [_vp, _vp, _vp, _i64, _vp, _int, _vp, _vp]),
+        "ptycho_reduce_blocks": (_int, []),
+        "ptycho_adam_step": (_int, [_vp, _vp, _vp, _vp, _i64, _flt, _vp, _flt, _flt, _flt, _flt, _int, _flt, _flt,
+                                    _vp]),
+        "ptycho_sgd_step": (_int, [_vp, _vp, _i64, _flt, _vp, _flt, _vp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+
+
+def lib():
+    """The loaded library; raises RuntimeError (never falls back) if unavailable."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise RuntimeError(
+                    f"libptycho_b200.so not found at {LIB_PATH}; build it with "
+                    "`python -m quantem_b200.build` (the CUDA path has no CPU fallback)")
+            try:
+                handle = ctypes.CDLL(LIB_PATH)
+            except OSError as exc:  # pragma: no cover - depends on the machine
+                raise RuntimeError(f"cannot load {LIB_PATH}: {exc}") from exc
+            _declare(handle)
+            _lib = handle
+    return _lib
+
+
+def last_error() -> str:
+    buf = ctypes.create_string_buffer(512)
+    lib().ptycho_get_last_error(buf, 512)
+    return buf.value.decode(errors="replace")
+
+
+def check(rc: int, what: str = "") -> None:
+    if rc != PTYCHO_OK:
+        kind = ERR_NAMES.get(rc, f"status {rc}")
+        raise RuntimeError(f"ptycho_b200 {what} failed ({kind}): {last_error()}")

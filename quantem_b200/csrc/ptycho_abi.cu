@@ -1,0 +1,356 @@
+// C ABI entry points of libptycho_b200 (declared in include/ptycho_b200.h) and the
+// small element-wise / reduction kernels around the fused batch kernel.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include "ptycho_b200.h"
+#include "ptycho_kernels.cuh"
+
+namespace {
+
+thread_local char g_last_error[512] = "";
+
+int fail(int code, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_last_error, sizeof(g_last_error), fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+int check_launch(const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(PTYCHO_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+  return PTYCHO_OK;
+}
+
+bool aligned(const void* p, size_t a) { return (reinterpret_cast<uintptr_t>(p) % a) == 0; }
+
+constexpr int kReduceBlocks = 592;  // 4 x 148 SMs
+constexpr int kReduceThreads = 256;
+
+// ---------------------------------------------------------------------------
+// object hard constraint (object_models.py:289-300) and its vector-Jacobian product
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double block_sum(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i];
+  }
+  return t;  // valid in thread 0
+}
+
+// Sum of a fixed-order list of partials, computed by every block (deterministic).
+__device__ __forceinline__ double sum_partials(const double* part, int n, double* red, double* bcast) {
+  double v = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) v += part[i];
+  double t = block_sum(v, red);
+  if (threadIdx.x == 0) *bcast = t;
+  __syncthreads();
+  return *bcast;
+}
+
+__global__ void angle_sum_kernel(const float2* __restrict__ obj, int64_t n, double* part) {
+  __shared__ double red[32];
+  double v = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const float2 o = obj[i];
+    v += (double)atan2f(o.y, o.x);
+  }
+  double t = block_sum(v, red);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
+__global__ void constrain_apply_kernel(const float2* __restrict__ obj, float2* __restrict__ out, int64_t n,
+                                       const double* part, int nparts) {
+  __shared__ double red[32];
+  __shared__ double bc;
+  const float mean = (float)(sum_partials(part, nparts, red, &bc) / (double)n);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const float2 o = obj[i];
+    const float amp = fminf(fmaxf(hypotf(o.x, o.y), 0.0f), 1.0f);
+    const float ph = atan2f(o.y, o.x) - mean;
+    float s, c;
+    sincosf(ph, &s, &c);
+    out[i] = make_float2(amp * c, amp * s);
+  }
+}
+
+// g_theta = clamp(|o|) * Im(G conj(e^{i theta})) summed over the object
+__global__ void vjp_sum_kernel(const float2* __restrict__ obj, const float2* __restrict__ gc, int64_t n,
+                               const double* part_fwd, int nparts, double* part) {
+  __shared__ double red[32];
+  __shared__ double bc;
+  const float mean = (float)(sum_partials(part_fwd, nparts, red, &bc) / (double)n);
+  double v = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const float2 o = obj[i], g = gc[i];
+    const float amp = fminf(fmaxf(hypotf(o.x, o.y), 0.0f), 1.0f);
+    float s, c;
+    sincosf(atan2f(o.y, o.x) - mean, &s, &c);
+    v += (double)(amp * (g.y * c - g.x * s));
+  }
+  double t = block_sum(v, red);
+  if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
+__global__ void vjp_apply_kernel(const float2* __restrict__ obj, const float2* __restrict__ gc,
+                                 float2* __restrict__ gout, int64_t n, const double* part_fwd,
+                                 const double* part_g, int nparts, const float* scale) {
+  __shared__ double red[32];
+  __shared__ double bc;
+  const float mean = (float)(sum_partials(part_fwd, nparts, red, &bc) / (double)n);
+  __syncthreads();
+  const float gmean = (float)(sum_partials(part_g, nparts, red, &bc) / (double)n);
+  const float sc = scale ? *scale : 1.0f;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const float2 o = obj[i], g = gc[i];
+    const float mag = hypotf(o.x, o.y);
+    const float amp = fminf(fmaxf(mag, 0.0f), 1.0f);
+    float s, c;
+    sincosf(atan2f(o.y, o.x) - mean, &s, &c);
+    const float g_amp = g.x * c + g.y * s;            // Re(G conj(e))
+    const float g_th = amp * (g.y * c - g.x * s);      // amp * Im(G conj(e))
+    const float g_ph = g_th - gmean;
+    const float g_mag = (mag >= 0.0f && mag <= 1.0f) ? g_amp : 0.0f;
+    float2 r = make_float2(0.f, 0.f);
+    if (mag != 0.0f) {
+      const float inv = 1.0f / mag;
+      // g_mag * o/|o| + g_ph * i o/|o|^2
+      r.x = g_mag * o.x * inv - g_ph * o.y * inv * inv;
+      r.y = g_mag * o.y * inv + g_ph * o.x * inv * inv;
+    }
+    gout[i] = make_float2(r.x * sc, r.y * sc);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// reductions
+// ---------------------------------------------------------------------------
+__global__ void reduce_partials_kernel(const float2* __restrict__ parts, float2* __restrict__ out, int nparts,
+                                       int64_t count) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x) {
+    float2 a = make_float2(0.f, 0.f);
+    for (int g = 0; g < nparts; ++g) {
+      const float2 v = parts[(int64_t)g * count + i];
+      a.x += v.x;
+      a.y += v.y;
+    }
+    out[i] = a;
+  }
+}
+
+__global__ void reduce_loss_kernel(const double* parts, int nparts, float* out) {
+  __shared__ double red[32];
+  double v = 0.0;
+  for (int i = threadIdx.x; i < nparts; i += blockDim.x) v += parts[i];
+  double t = block_sum(v, red);
+  if (threadIdx.x == 0) out[0] = (float)t;
+}
+
+// ---------------------------------------------------------------------------
+// optimisers (torch.optim semantics, real view of complex parameters)
+// ---------------------------------------------------------------------------
+__global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                            float* __restrict__ v, int64_t n, float lr, const float* lr_dev, float b1, float b2,
+                            float eps, float wd, int decoupled, float bc1, float bc2_sqrt) {
+  const float lr_ = lr_dev ? *lr_dev : lr;
+  const float step = lr_ / bc1;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    float pi = p[i];
+    float gi = g[i];
+    if (wd != 0.0f) {
+      if (decoupled) pi *= 1.0f - lr_ * wd;
+      else gi = fmaf(wd, pi, gi);
+    }
+    float mi = m[i];
+    mi = mi + (1.0f - b1) * (gi - mi);
+    float vi = v[i] * b2 + (1.0f - b2) * gi * gi;
+    const float denom = sqrtf(vi) / bc2_sqrt + eps;
+    pi = pi - step * (mi / denom);
+    p[i] = pi;
+    m[i] = mi;
+    v[i] = vi;
+  }
+}
+
+__global__ void sgd_kernel(float* __restrict__ p, const float* __restrict__ g, int64_t n, float lr,
+                           const float* lr_dev, float wd) {
+  const float lr_ = lr_dev ? *lr_dev : lr;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    float gi = g[i];
+    if (wd != 0.0f) gi = fmaf(wd, p[i], gi);
+    p[i] = p[i] - lr_ * gi;
+  }
+}
+
+int grid_for(int64_t n, int threads) {
+  int64_t b = (n + threads - 1) / threads;
+  if (b > 4 * 148) b = 4 * 148;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+}  // namespace
+
+// defined in fused_n64.cu / fused_n128.cu
+int qb_launch_batch_64(const ptycho_batch_args* a, bool adj, cudaStream_t st);
+int qb_launch_batch_128(const ptycho_batch_args* a, bool adj, cudaStream_t st);
+
+namespace {
+
+int validate_batch(const ptycho_batch_args* a, bool adj) {
+  if (!a) return fail(PTYCHO_ERR_INVALID, "args is NULL");
+  if (a->n != 64 && a->n != 128) return fail(PTYCHO_ERR_UNSUPPORTED, "probe window n=%d not built (64, 128)", a->n);
+  if (a->S < 1 || a->P < 1 || a->B < 0 || a->Ho < 1 || a->Wo < 1 || a->npos < 1)
+    return fail(PTYCHO_ERR_INVALID, "bad sizes S=%d P=%d B=%d Ho=%d Wo=%d npos=%d", a->S, a->P, a->B, a->Ho, a->Wo,
+                a->npos);
+  if (a->B > 0 && (a->grid < 1 || a->grid > 65535)) return fail(PTYCHO_ERR_INVALID, "bad grid %d", a->grid);
+  if (!a->obj || !a->probe_hat || !a->positions || !a->batch_idx || !a->targets || !a->mask || !a->loss_part)
+    return fail(PTYCHO_ERR_INVALID, "required pointer is NULL");
+  if (a->S > 1 && !a->prop) return fail(PTYCHO_ERR_INVALID, "prop is NULL with S > 1");
+  if (adj && (!a->grad_obj || !a->probe_grad_part || !a->scratch))
+    return fail(PTYCHO_ERR_INVALID, "adjoint buffers are NULL");
+  const void* ptrs[] = {a->obj, a->probe_hat, a->prop, a->grad_obj, a->probe_grad_part, a->scratch, a->out_exit,
+                        a->out_waves};
+  for (const void* q : ptrs)
+    if (q && !aligned(q, 8)) return fail(PTYCHO_ERR_INVALID, "complex buffer not 8-byte aligned");
+  if (a->loss_type < 0 || a->loss_type > 4) return fail(PTYCHO_ERR_INVALID, "bad loss type %d", a->loss_type);
+  return PTYCHO_OK;
+}
+
+int run_batch(const ptycho_batch_args* a, void* stream, bool adj) {
+  int rc = validate_batch(a, adj);
+  if (rc) return rc;
+  if (a->B == 0) return PTYCHO_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int lrc = a->n == 64 ? qb_launch_batch_64(a, adj, st) : qb_launch_batch_128(a, adj, st);
+  if (lrc) return fail(lrc, "fused_batch_kernel launch: %s", cudaGetErrorString(cudaGetLastError()));
+  return PTYCHO_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ptycho_get_last_error(char* buf, size_t len) {
+  if (!buf || len == 0) return PTYCHO_ERR_INVALID;
+  strncpy(buf, g_last_error, len - 1);
+  buf[len - 1] = '\0';
+  return PTYCHO_OK;
+}
+
+int ptycho_abi_version(void) { return 1; }
+
+int ptycho_sm_count(int* out) {
+  if (!out) return fail(PTYCHO_ERR_INVALID, "out is NULL");
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(out, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return fail(PTYCHO_ERR_CUDA, "sm count: %s", cudaGetErrorString(e));
+  return PTYCHO_OK;
+}
+
+int ptycho_workspace_elems(int n, int S, int P, int grid, int64_t* scratch_elems, int64_t* partial_elems) {
+  if (n < 1 || S < 1 || P < 1 || grid < 1) return fail(PTYCHO_ERR_INVALID, "bad workspace sizes");
+  const int64_t nn = (int64_t)n * n;
+  if (scratch_elems) *scratch_elems = (int64_t)grid * (P * S + P) * nn;
+  if (partial_elems) *partial_elems = (int64_t)grid * P * nn;
+  return PTYCHO_OK;
+}
+
+int ptycho_forward_loss(const ptycho_batch_args* a, void* stream) { return run_batch(a, stream, false); }
+
+int ptycho_forward_adjoint(const ptycho_batch_args* a, void* stream) { return run_batch(a, stream, true); }
+
+int ptycho_fft2(const void* in, void* out, int count, int n, int inverse, float scale, void* stream) {
+  if (!in || !out || count < 0) return fail(PTYCHO_ERR_INVALID, "fft2: bad arguments");
+  if (n != 64 && n != 128) return fail(PTYCHO_ERR_UNSUPPORTED, "fft2: n=%d not built", n);
+  if (count == 0) return PTYCHO_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const float2* i2 = static_cast<const float2*>(in);
+  float2* o2 = static_cast<float2*>(out);
+  const int grid = count < 148 ? count : 148;
+  if (n == 64) {
+    const size_t smem = qb::fft2_smem_bytes<64>();
+    if (inverse) qb::fft2_batch_kernel<64, true><<<grid, 256, smem, st>>>(i2, o2, count, scale);
+    else qb::fft2_batch_kernel<64, false><<<grid, 256, smem, st>>>(i2, o2, count, scale);
+  } else {
+    const size_t smem = qb::fft2_smem_bytes<128>();
+    cudaFuncSetAttribute(qb::fft2_batch_kernel<128, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(qb::fft2_batch_kernel<128, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (inverse) qb::fft2_batch_kernel<128, true><<<grid, 512, smem, st>>>(i2, o2, count, scale);
+    else qb::fft2_batch_kernel<128, false><<<grid, 512, smem, st>>>(i2, o2, count, scale);
+  }
+  return check_launch("fft2_batch_kernel");
+}
+
+int ptycho_reduce_partials(const void* parts, void* out, int nparts, int64_t count, void* stream) {
+  if (!parts || !out || nparts < 1 || count < 0) return fail(PTYCHO_ERR_INVALID, "reduce_partials: bad arguments");
+  if (count == 0) return PTYCHO_OK;
+  reduce_partials_kernel<<<grid_for(count, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      static_cast<const float2*>(parts), static_cast<float2*>(out), nparts, count);
+  return check_launch("reduce_partials_kernel");
+}
+
+int ptycho_reduce_loss(const double* parts, int nparts, float* out, void* stream) {
+  if (!parts || !out || nparts < 1) return fail(PTYCHO_ERR_INVALID, "reduce_loss: bad arguments");
+  reduce_loss_kernel<<<1, 256, 0, static_cast<cudaStream_t>(stream)>>>(parts, nparts, out);
+  return check_launch("reduce_loss_kernel");
+}
+
+int ptycho_reduce_blocks(void) { return kReduceBlocks; }
+
+int ptycho_obj_constrain(const void* obj, void* out, int64_t count, double* work, int nwork, void* stream) {
+  if (!obj || !out || !work || count < 1) return fail(PTYCHO_ERR_INVALID, "obj_constrain: bad arguments");
+  if (nwork < 2 * kReduceBlocks) return fail(PTYCHO_ERR_INVALID, "obj_constrain: work too small (%d)", nwork);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const float2* o = static_cast<const float2*>(obj);
+  angle_sum_kernel<<<kReduceBlocks, kReduceThreads, 0, st>>>(o, count, work);
+  constrain_apply_kernel<<<kReduceBlocks, kReduceThreads, 0, st>>>(o, static_cast<float2*>(out), count, work,
+                                                                   kReduceBlocks);
+  return check_launch("obj_constrain");
+}
+
+int ptycho_obj_constrain_vjp(const void* obj, const void* grad_c, void* grad_raw, int64_t count, double* work,
+                             int nwork, const float* scale, void* stream) {
+  if (!obj || !grad_c || !grad_raw || !work || count < 1)
+    return fail(PTYCHO_ERR_INVALID, "obj_constrain_vjp: bad arguments");
+  if (nwork < 2 * kReduceBlocks) return fail(PTYCHO_ERR_INVALID, "obj_constrain_vjp: work too small");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const float2* o = static_cast<const float2*>(obj);
+  const float2* g = static_cast<const float2*>(grad_c);
+  vjp_sum_kernel<<<kReduceBlocks, kReduceThreads, 0, st>>>(o, g, count, work, kReduceBlocks, work + kReduceBlocks);
+  vjp_apply_kernel<<<kReduceBlocks, kReduceThreads, 0, st>>>(o, g, static_cast<float2*>(grad_raw), count, work,
+                                                             work + kReduceBlocks, kReduceBlocks, scale);
+  return check_launch("obj_constrain_vjp");
+}
+
+int ptycho_adam_step(float* param, const float* grad, float* exp_avg, float* exp_avg_sq, int64_t count, float lr,
+                     const float* lr_dev, float beta1, float beta2, float eps, float weight_decay, int decoupled,
+                     float bc1, float bc2_sqrt, void* stream) {
+  if (!param || !grad || !exp_avg || !exp_avg_sq || count < 0) return fail(PTYCHO_ERR_INVALID, "adam: bad arguments");
+  if (count == 0) return PTYCHO_OK;
+  adam_kernel<<<grid_for(count, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      param, grad, exp_avg, exp_avg_sq, count, lr, lr_dev, beta1, beta2, eps, weight_decay, decoupled, bc1, bc2_sqrt);
+  return check_launch("adam_kernel");
+}
+
+int ptycho_sgd_step(float* param, const float* grad, int64_t count, float lr, const float* lr_dev,
+                    float weight_decay, void* stream) {
+  if (!param || !grad || count < 0) return fail(PTYCHO_ERR_INVALID, "sgd: bad arguments");
+  if (count == 0) return PTYCHO_OK;
+  sgd_kernel<<<grid_for(count, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(param, grad, count, lr, lr_dev,
+                                                                                   weight_decay);
+  return check_launch("sgd_kernel");
+}
+
+}  // extern "C"

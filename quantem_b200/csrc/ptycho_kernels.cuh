@@ -1,0 +1,374 @@
+// Multislice mixed-probe ptychography kernels for sm_100a.
+//
+// fused_batch_kernel<N, ADJ>: one CTA per scan position at a time (persistent
+// grid-stride loop).  For every probe mode the CTA builds the sub-pixel shifted
+// probe from the Fourier-space probe and a separable phase ramp, runs the
+// multislice recursion (transmission by the gathered object patch, Fresnel
+// propagation by FFT * propagator * IFFT), forms the far field with an
+// orthonormal FFT and accumulates |Psi|^2 over modes in shared memory.  The loss
+// and dL/dI follow in the same pass.  With ADJ the CTA then runs the adjoint for
+// every mode: back-projection through the detector FFT, reverse slices with
+// conjugate transmission / propagator, scatter-add of the object gradient
+// (float2 atomics) and accumulation of the Fourier-space probe gradient into a
+// per-CTA partial.  Incoming waves of every slice are kept in a per-CTA scratch
+// slot between forward and adjoint.
+//
+// Reference behaviour (quantem.diffractive_imaging):
+//   probe shift      ptycho_utils.py:128-176, probe_models.py:718-720
+//   patch gather     object_models.py:252-265, dataset_models.py:514-535,1487-1490
+//   multislice       ptychography_base.py:934-947, 970-989
+//   detector         detector_models.py:22-30
+//   loss             ptychography_base.py:908-932
+//   autograd         ptychography.py:326-332 (torch complex-gradient convention)
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fft_engine.cuh"
+
+namespace qb {
+
+enum LossType : int {
+  LOSS_L2_AMPLITUDE = 0,
+  LOSS_L1_AMPLITUDE = 1,
+  LOSS_L2_INTENSITY = 2,
+  LOSS_L1_INTENSITY = 3,
+  LOSS_POISSON = 4,
+};
+
+struct BatchParams {
+  const float2* obj;          // constrained object (S, Ho, Wo)
+  const float2* probe_hat;    // fft2 of the orthogonalised probes (P, N, N)
+  const float2* prop;         // propagators (S-1, N, N)
+  const float* positions;     // (npos, 2) scan positions [px]
+  const int64_t* batch_idx;   // (B,) indices into positions / targets
+  const float* targets;       // (npos, N, N) detector (centred) layout
+  const float* mask;          // (N, N) detector layout
+  float2* grad_obj;           // (S, Ho, Wo) accumulated, ADJ only
+  float2* probe_grad_part;    // (grid, P, N, N) per-CTA Fourier partials, ADJ only
+  float2* scratch;            // (grid, P*S + P, N*N), ADJ only
+  double* loss_part;          // (grid,) per-CTA loss partial sums
+  float* out_intensity;       // optional (B, N, N) detector layout
+  float2* out_exit;           // optional (P, B, N, N) exit waves
+  float2* out_waves;          // optional (S, P, B, N, N) incoming wave of each slice
+  int* status;                // optional non-finite counter
+  int S, P, B, Ho, Wo, npos;
+  float loss_scale;           // num_gpts / (B * mean_intensity)
+  float inv_mean_intensity;   // 1 / mean_intensity (poisson)
+  int loss_type;
+};
+
+__device__ __forceinline__ int fsigned(int k, int n) { return k < n / 2 ? k : k - n; }
+__device__ __forceinline__ int wrap_index(int x, int n) {
+  x %= n;
+  return x < 0 ? x + n : x;
+}
+
+// shared-memory bytes used by fused_batch_kernel<N, *>
+template <int N>
+constexpr size_t fused_smem_bytes() {
+  return sizeof(float2) * (size_t)(Fft2<N>::SM_FLOAT2 + 3 * N) + sizeof(float) * (size_t)N * N +
+         sizeof(int) * (size_t)(2 * N);
+}
+
+template <int N>
+__device__ __forceinline__ void loss_elem(const BatchParams& p, float I, float t, float m,
+                                          double& acc, float& dldi) {
+  switch (p.loss_type) {
+    case LOSS_L2_AMPLITUDE: {
+      const float a = sqrtf(I + 1e-9f);
+      const float d = a * m - t * m;
+      acc += (double)d * d;
+      dldi = p.loss_scale * d * m / a;
+      break;
+    }
+    case LOSS_L1_AMPLITUDE: {
+      const float a = sqrtf(I + 1e-9f);
+      const float d = a * m - t * m;
+      acc += fabs((double)d);
+      const float sg = d > 0.f ? 1.f : (d < 0.f ? -1.f : 0.f);
+      dldi = p.loss_scale * sg * m * 0.5f / a;
+      break;
+    }
+    case LOSS_L2_INTENSITY: {
+      const float d = I * m - t * m;
+      acc += (double)d * d;
+      dldi = p.loss_scale * 2.f * d * m;
+      break;
+    }
+    case LOSS_L1_INTENSITY: {
+      const float d = I * m - t * m;
+      acc += fabs((double)d);
+      const float sg = d > 0.f ? 1.f : (d < 0.f ? -1.f : 0.f);
+      dldi = p.loss_scale * sg * m;
+      break;
+    }
+    default: {  // poisson: sum(I - t log(I + 1e-6)) / mean_I
+      acc += (double)I - (double)t * log((double)I + 1e-6);
+      dldi = p.inv_mean_intensity * (1.f - t / (I + 1e-6f));
+      break;
+    }
+  }
+}
+
+template <int N, bool ADJ>
+__global__ void __launch_bounds__(4 * N, 1) fused_batch_kernel(const BatchParams p) {
+  using F = Fft2<N>;
+  constexpr int E = F::E, D = F::D, G3 = F::G3, T = F::T;
+  extern __shared__ float4 smem_raw[];
+  float2* sm = reinterpret_cast<float2*>(smem_raw);
+  float2* tw = sm + F::SM_FLOAT2;
+  float2* rowf = tw + N;
+  float2* colf = rowf + N;
+  float* inten = reinterpret_cast<float*>(colf + N);
+  int* rowmap = reinterpret_cast<int*>(inten + N * N);
+  int* colmap = rowmap + N;
+  __shared__ double red[32];
+
+  const int tid = threadIdx.x;
+  F f;
+  f.init(tid);
+  for (int k = tid; k < N; k += T) {
+    double s, c;
+    sincospi(-2.0 * (double)k / (double)N, &s, &c);
+    tw[k] = make_float2((float)c, (float)s);
+  }
+  const float inv_n = 1.0f / (float)N;
+  const float inv_n2 = inv_n * inv_n;
+  const size_t NN = (size_t)N * N;
+  const int S = p.S, P = p.P;
+  const size_t HoWo = (size_t)p.Ho * p.Wo;
+  float2* slot = ADJ ? p.scratch + (size_t)blockIdx.x * (size_t)(P * S + P) * NN : nullptr;
+  float2* pgrad = ADJ ? p.probe_grad_part + (size_t)blockIdx.x * (size_t)P * NN : nullptr;
+  if (ADJ) {
+    for (int m = 0; m < P; ++m)
+#pragma unroll
+      for (int g = 0; g < G3; ++g)
+#pragma unroll
+        for (int e = 0; e < D; ++e)
+          pgrad[(size_t)m * NN + (size_t)f.s3_row(g, e) * N + f.s3_c] = make_float2(0.f, 0.f);
+  }
+  double loss_acc = 0.0;
+  int nonfinite = 0;
+
+  for (int b = blockIdx.x; b < p.B; b += gridDim.x) {
+    const int64_t gi = p.batch_idx[b];
+    if (gi < 0 || gi >= p.npos) {  // invalid index: skip the position and report it
+      if (tid == 0 && p.status) atomicAdd(p.status, 1 << 20);
+      continue;
+    }
+    const float py = p.positions[2 * gi], px = p.positions[2 * gi + 1];
+    const float ry = rintf(py), rx = rintf(px);  // round half to even
+    const float fy = py - ry, fx = px - rx;
+    const int r0 = wrap_index((int)ry, p.Ho), c0 = wrap_index((int)rx, p.Wo);
+    __syncthreads();  // previous position finished with rowf/colf/maps
+    for (int k = tid; k < 2 * N; k += T) {
+      const int kk = k < N ? k : k - N;
+      const float fq = (float)fsigned(kk, N) * inv_n;         // fftfreq(N) in float32
+      const float a = -6.283185307179586f * fq;                // -2 pi k
+      float s, c;
+      sincosf(a * (k < N ? fy : fx), &s, &c);
+      if (k < N) {
+        rowf[kk] = make_float2(c, s);
+        rowmap[kk] = wrap_index(r0 + fsigned(kk, N), p.Ho);
+      } else {
+        colf[kk] = make_float2(c, s);
+        colmap[kk] = wrap_index(c0 + fsigned(kk, N), p.Wo);
+      }
+    }
+#pragma unroll
+    for (int g = 0; g < G3; ++g)
+#pragma unroll
+      for (int e = 0; e < D; ++e) inten[(g * D + e) * T + tid] = 0.f;
+    __syncthreads();
+    const int orow = rowmap[f.s1_r];
+
+    // ------------------------------ forward ------------------------------
+    for (int m = 0; m < P; ++m) {
+      float2 x[E];
+      const float2* ph = p.probe_hat + (size_t)m * NN;
+#pragma unroll
+      for (int g = 0; g < G3; ++g)
+#pragma unroll
+        for (int e = 0; e < D; ++e) {
+          const int kr = f.s3_row(g, e), kc = f.s3_c;
+          x[g * D + e] = cmul(cmul(__ldg(ph + (size_t)kr * N + kc), rowf[kr]), colf[kc]);
+        }
+      f.inverse(x, sm, tw);
+#pragma unroll
+      for (int e = 0; e < E; ++e) x[e] = cscale(x[e], inv_n2);
+
+      for (int s = 0; s < S; ++s) {
+        if (ADJ) {
+          float2* wv = slot + (size_t)(m * S + s) * NN;
+#pragma unroll
+          for (int e = 0; e < E; ++e) wv[e * T + tid] = x[e];
+        }
+        if (p.out_waves) {
+          float2* ow = p.out_waves + (((size_t)s * P + m) * p.B + b) * NN + (size_t)f.s1_r * N;
+#pragma unroll
+          for (int e = 0; e < E; ++e) ow[f.s1_col(e)] = x[e];
+        }
+        const float2* orow_ptr = p.obj + (size_t)s * HoWo + (size_t)orow * p.Wo;
+#pragma unroll
+        for (int e = 0; e < E; ++e) x[e] = cmul(x[e], __ldg(orow_ptr + colmap[f.s1_col(e)]));
+        if (s < S - 1) {
+          f.forward(x, sm, tw);
+          const float2* pr = p.prop + (size_t)s * NN;
+#pragma unroll
+          for (int g = 0; g < G3; ++g)
+#pragma unroll
+            for (int e = 0; e < D; ++e)
+              x[g * D + e] = cmul(x[g * D + e], __ldg(pr + (size_t)f.s3_row(g, e) * N + f.s3_c));
+          f.inverse(x, sm, tw);
+#pragma unroll
+          for (int e = 0; e < E; ++e) x[e] = cscale(x[e], inv_n2);
+        }
+      }
+      if (p.out_exit) {
+        float2* oe = p.out_exit + ((size_t)m * p.B + b) * NN + (size_t)f.s1_r * N;
+#pragma unroll
+        for (int e = 0; e < E; ++e) oe[f.s1_col(e)] = x[e];
+      }
+      f.forward(x, sm, tw);
+#pragma unroll
+      for (int e = 0; e < E; ++e) x[e] = cscale(x[e], inv_n);  // orthonormal detector FFT
+      if (ADJ) {
+        float2* fw = slot + (size_t)(P * S + m) * NN;
+#pragma unroll
+        for (int e = 0; e < E; ++e) fw[e * T + tid] = x[e];
+      }
+#pragma unroll
+      for (int e = 0; e < E; ++e) inten[e * T + tid] += cabs2(x[e]);
+    }
+
+    // ------------------------------ loss ------------------------------
+    {
+      const float* tg = p.targets + (size_t)gi * NN;
+#pragma unroll
+      for (int g = 0; g < G3; ++g)
+#pragma unroll
+        for (int e = 0; e < D; ++e) {
+          const int kr = f.s3_row(g, e), kc = f.s3_c;
+          const int di = ((kr + N / 2) & (N - 1)) * N + ((kc + N / 2) & (N - 1));
+          const float I = inten[(g * D + e) * T + tid];
+          if (!isfinite(I)) ++nonfinite;
+          float dldi;
+          loss_elem<N>(p, I, __ldg(tg + di), __ldg(p.mask + di), loss_acc, dldi);
+          inten[(g * D + e) * T + tid] = dldi;
+          if (p.out_intensity) p.out_intensity[(size_t)b * NN + di] = I;
+        }
+    }
+
+    // ------------------------------ adjoint ------------------------------
+    if (ADJ) {
+      for (int m = 0; m < P; ++m) {
+        float2 x[E];
+        const float2* fw = slot + (size_t)(P * S + m) * NN;
+#pragma unroll
+        for (int e = 0; e < E; ++e) x[e] = cscale(fw[e * T + tid], 2.0f * inten[e * T + tid]);
+        f.inverse(x, sm, tw);
+#pragma unroll
+        for (int e = 0; e < E; ++e) x[e] = cscale(x[e], inv_n);  // adjoint of the orthonormal FFT
+        for (int s = S - 1; s >= 0; --s) {
+          const float2* wv = slot + (size_t)(m * S + s) * NN;
+          const float2* orow_ptr = p.obj + (size_t)s * HoWo + (size_t)orow * p.Wo;
+          float2* grow = p.grad_obj + (size_t)s * HoWo + (size_t)orow * p.Wo;
+#pragma unroll
+          for (int e = 0; e < E; ++e) {
+            const int col = colmap[f.s1_col(e)];
+            atomicAdd(grow + col, cmulc(x[e], wv[e * T + tid]));  // conj(psi) * g
+            x[e] = cmulc(x[e], __ldg(orow_ptr + col));            // conj(o) * g
+          }
+          if (s > 0) {
+            f.forward(x, sm, tw);
+            const float2* pr = p.prop + (size_t)(s - 1) * NN;
+#pragma unroll
+            for (int g = 0; g < G3; ++g)
+#pragma unroll
+              for (int e = 0; e < D; ++e)
+                x[g * D + e] = cmulc(x[g * D + e], __ldg(pr + (size_t)f.s3_row(g, e) * N + f.s3_c));
+            f.inverse(x, sm, tw);
+#pragma unroll
+            for (int e = 0; e < E; ++e) x[e] = cscale(x[e], inv_n2);
+          }
+        }
+        // probe-shift adjoint: accumulate conj(ramp) * fft2(g0)
+        f.forward(x, sm, tw);
+        float2* pg = pgrad + (size_t)m * NN;
+#pragma unroll
+        for (int g = 0; g < G3; ++g)
+#pragma unroll
+          for (int e = 0; e < D; ++e) {
+            const int kr = f.s3_row(g, e), kc = f.s3_c;
+            const size_t idx = (size_t)kr * N + kc;
+            pg[idx] = cadd(pg[idx], cmulc(x[g * D + e], cmul(rowf[kr], colf[kc])));
+          }
+      }
+    }
+  }
+
+  // ------------------------------ loss reduction ------------------------------
+  for (int o = 16; o > 0; o >>= 1) loss_acc += __shfl_xor_sync(0xffffffffu, loss_acc, o);
+  if ((tid & 31) == 0) red[tid >> 5] = loss_acc;
+  __syncthreads();
+  if (tid == 0) {
+    double t = 0.0;
+    for (int w = 0; w < T / 32; ++w) t += red[w];
+    // l1/l2: sum / (B / num_gpts) / mean_I ; poisson: sum / mean_I
+    p.loss_part[blockIdx.x] = t * (double)(p.loss_type == LOSS_POISSON ? p.inv_mean_intensity : p.loss_scale);
+  }
+  if (p.status && nonfinite) atomicAdd(p.status, nonfinite);
+}
+
+// Batched 2-D FFT of (count, N, N) arrays, one CTA per transform, natural layout
+// in and out, result multiplied by `scale`.
+template <int N, bool INV>
+__global__ void __launch_bounds__(4 * N, 1) fft2_batch_kernel(const float2* in, float2* out, int count,
+                                                             float scale) {
+  using F = Fft2<N>;
+  constexpr int E = F::E, D = F::D, G3 = F::G3, T = F::T;
+  extern __shared__ float4 smem_raw[];
+  float2* sm = reinterpret_cast<float2*>(smem_raw);
+  float2* tw = sm + F::SM_FLOAT2;
+  const int tid = threadIdx.x;
+  F f;
+  f.init(tid);
+  for (int k = tid; k < N; k += T) {
+    double s, c;
+    sincospi(-2.0 * (double)k / (double)N, &s, &c);
+    tw[k] = make_float2((float)c, (float)s);
+  }
+  __syncthreads();
+  const size_t NN = (size_t)N * N;
+  for (int t = blockIdx.x; t < count; t += gridDim.x) {
+    const float2* src = in + (size_t)t * NN;
+    float2* dst = out + (size_t)t * NN;
+    float2 x[E];
+    if (!INV) {
+#pragma unroll
+      for (int e = 0; e < E; ++e) x[e] = src[(size_t)f.s1_r * N + f.s1_col(e)];
+      f.forward(x, sm, tw);
+#pragma unroll
+      for (int g = 0; g < G3; ++g)
+#pragma unroll
+        for (int e = 0; e < D; ++e) dst[(size_t)f.s3_row(g, e) * N + f.s3_c] = cscale(x[g * D + e], scale);
+    } else {
+#pragma unroll
+      for (int g = 0; g < G3; ++g)
+#pragma unroll
+        for (int e = 0; e < D; ++e) x[g * D + e] = src[(size_t)f.s3_row(g, e) * N + f.s3_c];
+      f.inverse(x, sm, tw);
+#pragma unroll
+      for (int e = 0; e < E; ++e) dst[(size_t)f.s1_r * N + f.s1_col(e)] = cscale(x[e], scale);
+    }
+    __syncthreads();
+  }
+}
+
+template <int N>
+constexpr size_t fft2_smem_bytes() {
+  return sizeof(float2) * (size_t)(Fft2<N>::SM_FLOAT2 + N);
+}
+
+}  // namespace qb

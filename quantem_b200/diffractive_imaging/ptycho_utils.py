@@ -1,0 +1,125 @@
+"""Host-side helpers of the ptychography path (batching, probe orthogonalisation).
+
+Behaviour follows quantem.diffractive_imaging.ptycho_utils / probe_models of the
+reference (file:line cited per function).
+"""
+from __future__ import annotations
+
+from math import ceil
+from typing import Literal
+
+import numpy as np
+import torch
+
+
+class SimpleBatcher:
+    """Per-epoch shuffled position batches with an optional validation split.
+
+    Same index arithmetic and numpy-generator call sequence as the reference's
+    SimpleBatcher (ptycho_utils.py:16-117), so a seeded run visits positions in
+    the same order.
+    """
+
+    def __init__(self, num: int, batch_size: int | None, shuffle: bool = True,
+                 rng: np.random.Generator | int | None = None, val_ratio: float = 0.0,
+                 val_mode: Literal["grid", "random"] = "grid",
+                 train_indices: np.ndarray | None = None, val_indices: np.ndarray | None = None):
+        self.indices = np.arange(num)
+        self.batch_size = batch_size if batch_size is not None else num
+        self.shuffle = shuffle
+        self.rng = rng
+        if train_indices is not None or val_indices is not None:
+            if train_indices is None or val_indices is None:
+                raise ValueError("Both train_indices and val_indices must be provided together.")
+            self.train_indices = np.asarray(train_indices, dtype=int)
+            self.val_indices = np.asarray(val_indices, dtype=int)
+            return
+        if val_ratio < 0 or val_ratio >= 1:
+            val_ratio = 0.0
+        n_val = int(round(len(self.indices) * val_ratio))
+        if n_val > 0:
+            if val_mode == "random":
+                perm = self.rng.permutation(self.indices)
+                self.val_indices = perm[:n_val]
+                self.train_indices = np.setdiff1d(self.indices, self.val_indices, assume_unique=False)
+            else:
+                if val_ratio <= 0.5:
+                    k = max(1, int(round(1.0 / val_ratio)))
+                    invert = False
+                else:
+                    k = max(1, int(round(1.0 / (1.0 - val_ratio))))
+                    invert = True
+                grid_sel = self.indices[::k]
+                if len(grid_sel) > n_val:
+                    grid_sel = grid_sel[:n_val]
+                if invert:
+                    self.train_indices = grid_sel
+                    self.val_indices = np.setdiff1d(self.indices, grid_sel, assume_unique=False)
+                else:
+                    self.val_indices = grid_sel
+                    self.train_indices = np.setdiff1d(self.indices, self.val_indices, assume_unique=False)
+        else:
+            self.val_indices = np.asarray([], dtype=int)
+            self.train_indices = self.indices
+
+    @property
+    def rng(self) -> np.random.Generator:
+        return self._rng
+
+    @rng.setter
+    def rng(self, rng):
+        if rng is None:
+            rng = np.random.default_rng()
+        elif isinstance(rng, (int, float)):
+            rng = np.random.default_rng(rng)
+        elif not isinstance(rng, np.random.Generator):
+            raise TypeError(f"rng should be a np.random.Generator or a seed, got {type(rng)}")
+        self._rng = rng
+
+    def __iter__(self):
+        order = self.rng.permutation(self.train_indices) if self.shuffle else self.train_indices
+        for i in range(0, len(order), self.batch_size):
+            yield order[i:i + self.batch_size]
+
+    def __len__(self):
+        return int(ceil(len(self.train_indices) / self.batch_size))
+
+    def iter_val(self):
+        if len(self.val_indices) == 0:
+            return iter(())
+
+        def _gen():
+            for i in range(0, len(self.val_indices), self.batch_size):
+                yield self.val_indices[i:i + self.batch_size]
+
+        return _gen()
+
+    @property
+    def has_validation(self) -> bool:
+        return len(self.val_indices) > 0
+
+    def val_len(self) -> int:
+        return int(ceil(len(self.val_indices) / self.batch_size)) if self.has_validation else 0
+
+
+def orthogonalize_probes(start_probe: torch.Tensor) -> torch.Tensor:
+    """Mixed-state Gram-Schmidt with norm restore and intensity sort.
+
+    probe_models.py:484-525: modified Gram-Schmidt on the running vector,
+    each mode rescaled to its original norm, modes sorted by descending
+    real-space intensity.  Differentiable (runs as tensor ops of (P, n, n)).
+    """
+    n_probes = start_probe.shape[0]
+    original_norms = torch.sqrt(
+        torch.sum(start_probe.real.square() + start_probe.imag.square(), dim=(-2, -1), keepdim=True))
+    ortho = []
+    for i in range(n_probes):
+        probe_i = start_probe[i]
+        for j in range(len(ortho)):
+            probe_i = probe_i - torch.sum(ortho[j].conj() * probe_i) * ortho[j]
+        norm = torch.sqrt(torch.sum(probe_i.real.square() + probe_i.imag.square())).clamp_min(1e-12)
+        ortho.append(probe_i / norm)
+    probes = torch.stack(ortho) * original_norms.view(-1, 1, 1)
+    intensities = torch.sum(torch.abs(probes).square(), dim=(-2, -1))
+    order = torch.argsort(intensities, descending=True)
+    return torch.complex(probes.real[order], probes.imag[order])

@@ -1,0 +1,367 @@
+"""Torch-facing wrappers around the C ABI of libptycho_b200.
+
+PyTorch supplies device memory (caching allocator), the current CUDA stream and
+autograd plumbing; every computation on the ptychography path runs in the
+hand-written sm_100a kernels of ``csrc/``.  All functions require CUDA tensors
+and raise ``RuntimeError`` if the library is unavailable (no CPU fallback).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import torch
+
+from . import _lib
+
+SUPPORTED_N = (64, 128)
+
+
+def _stream() -> ctypes.c_void_p:
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _p(t):
+    return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+def _req(t: torch.Tensor, name: str, dtype: torch.dtype, device=None):
+    if not isinstance(t, torch.Tensor):
+        raise TypeError(f"{name} must be a torch.Tensor")
+    if not t.is_cuda:
+        raise RuntimeError(f"{name} must be a CUDA tensor (the B200 path has no CPU fallback)")
+    if t.dtype != dtype:
+        raise TypeError(f"{name} must be {dtype}, got {t.dtype}")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+    if device is not None and t.device != device:
+        raise ValueError(f"{name} is on {t.device}, expected {device}")
+    return t
+
+
+_SM_COUNT: dict[int, int] = {}
+
+
+def sm_count(device: torch.device | None = None) -> int:
+    dev = torch.cuda.current_device() if device is None else (device.index or 0)
+    if dev not in _SM_COUNT:
+        with torch.cuda.device(dev):
+            v = ctypes.c_int(0)
+            _lib.check(_lib.lib().ptycho_sm_count(ctypes.byref(v)), "sm_count")
+            _SM_COUNT[dev] = v.value
+    return _SM_COUNT[dev]
+
+
+def reduce_blocks() -> int:
+    return int(_lib.lib().ptycho_reduce_blocks())
+
+
+# ----------------------------------------------------------------------------
+# small building blocks
+# ----------------------------------------------------------------------------
+
+def fft2(x: torch.Tensor, inverse: bool = False, scale: float = 1.0, out: torch.Tensor | None = None):
+    """scale * (i)fft2 of a (..., n, n) complex64 stack, unnormalised transform."""
+    _req(x, "x", torch.complex64)
+    n = x.shape[-1]
+    if x.shape[-2] != n or n not in SUPPORTED_N:
+        raise ValueError(f"fft2 supports square {SUPPORTED_N} windows, got {tuple(x.shape[-2:])}")
+    out = torch.empty_like(x) if out is None else _req(out, "out", torch.complex64)
+    count = x.numel() // (n * n)
+    _lib.check(_lib.lib().ptycho_fft2(_p(x), _p(out), count, n, int(inverse), float(scale), _stream()), "fft2")
+    return out
+
+
+def new_constraint_work(device) -> torch.Tensor:
+    return torch.empty(2 * reduce_blocks(), dtype=torch.float64, device=device)
+
+
+def obj_constrain(obj: torch.Tensor, work: torch.Tensor | None = None, out: torch.Tensor | None = None):
+    """Complex-object hard constraint (object_models.py:289-300)."""
+    _req(obj, "obj", torch.complex64)
+    work = new_constraint_work(obj.device) if work is None else work
+    out = torch.empty_like(obj) if out is None else out
+    _lib.check(_lib.lib().ptycho_obj_constrain(_p(obj), _p(out), obj.numel(), _p(work), work.numel(), _stream()),
+               "obj_constrain")
+    return out, work
+
+
+def obj_constrain_vjp(obj: torch.Tensor, grad_c: torch.Tensor, work: torch.Tensor,
+                      scale: torch.Tensor | None = None, out: torch.Tensor | None = None):
+    _req(obj, "obj", torch.complex64)
+    _req(grad_c, "grad_c", torch.complex64)
+    out = torch.empty_like(obj) if out is None else out
+    if scale is not None:
+        scale = scale.detach().to(torch.float32).contiguous()
+    _lib.check(_lib.lib().ptycho_obj_constrain_vjp(_p(obj), _p(grad_c), _p(out), obj.numel(), _p(work),
+                                                   work.numel(), _p(scale), _stream()), "obj_constrain_vjp")
+    return out
+
+
+class _ObjConstrainFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, obj):
+        out, work = obj_constrain(obj.detach().contiguous())
+        ctx.save_for_backward(obj, work)
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        obj, work = ctx.saved_tensors
+        return obj_constrain_vjp(obj.detach().contiguous(), g.contiguous().to(torch.complex64), work)
+
+
+def constrained_object(obj: torch.Tensor) -> torch.Tensor:
+    """Differentiable hard-constrained object computed by the CUDA kernels."""
+    return _ObjConstrainFn.apply(obj)
+
+
+# ----------------------------------------------------------------------------
+# batch kernels
+# ----------------------------------------------------------------------------
+
+@dataclass
+class BatchGeometry:
+    n: int
+    S: int
+    P: int
+    Ho: int
+    Wo: int
+    npos: int
+
+    @classmethod
+    def of(cls, obj: torch.Tensor, probe: torch.Tensor, npos: int):
+        S, Ho, Wo = obj.shape
+        P, n, n2 = probe.shape
+        if n != n2:
+            raise ValueError("probe window must be square")
+        if n not in SUPPORTED_N:
+            raise ValueError(f"probe window {n} not supported (built: {SUPPORTED_N})")
+        return cls(n=n, S=S, P=P, Ho=Ho, Wo=Wo, npos=npos)
+
+
+class Workspace:
+    """Per-device scratch for batch launches, grown on demand and reused."""
+
+    def __init__(self, device):
+        self.device = torch.device(device)
+        self.scratch = None
+        self.partials = None
+        self.loss_part = None
+        self.status = torch.zeros(1, dtype=torch.int32, device=self.device)
+
+    def get(self, geom: BatchGeometry, grid: int, adjoint: bool):
+        nn = geom.n * geom.n
+        if adjoint:
+            need_s = grid * (geom.P * geom.S + geom.P) * nn
+            need_p = grid * geom.P * nn
+            if self.scratch is None or self.scratch.numel() < need_s:
+                self.scratch = torch.empty(need_s, dtype=torch.complex64, device=self.device)
+            if self.partials is None or self.partials.numel() < need_p:
+                self.partials = torch.empty(need_p, dtype=torch.complex64, device=self.device)
+        if self.loss_part is None or self.loss_part.numel() < grid:
+            self.loss_part = torch.empty(max(grid, 256), dtype=torch.float64, device=self.device)
+        return self
+
+
+_WORKSPACES: dict = {}
+
+
+def workspace(device) -> Workspace:
+    key = str(torch.device(device))
+    if key not in _WORKSPACES:
+        _WORKSPACES[key] = Workspace(device)
+    return _WORKSPACES[key]
+
+
+def default_grid(B: int, device=None) -> int:
+    return max(1, min(B, sm_count(device)))
+
+
+def _batch_args(geom, obj_c, probe_hat, prop, positions, batch_idx, targets, mask, B, grid, loss_type,
+                loss_scale, inv_mean, ws, grad_obj=None, out_intensity=None, out_exit=None, out_waves=None,
+                adjoint=False):
+    a = _lib.BatchArgs()
+    a.obj = obj_c.data_ptr()
+    a.probe_hat = probe_hat.data_ptr()
+    a.prop = prop.data_ptr() if (prop is not None and prop.numel() > 0) else None
+    a.positions = positions.data_ptr()
+    a.batch_idx = batch_idx.data_ptr()
+    a.targets = targets.data_ptr()
+    a.mask = mask.data_ptr()
+    a.grad_obj = grad_obj.data_ptr() if grad_obj is not None else None
+    a.probe_grad_part = ws.partials.data_ptr() if adjoint else None
+    a.scratch = ws.scratch.data_ptr() if adjoint else None
+    a.loss_part = ws.loss_part.data_ptr()
+    a.out_intensity = out_intensity.data_ptr() if out_intensity is not None else None
+    a.out_exit = out_exit.data_ptr() if out_exit is not None else None
+    a.out_waves = out_waves.data_ptr() if out_waves is not None else None
+    a.status = ws.status.data_ptr()
+    a.n, a.S, a.P, a.B = geom.n, geom.S, geom.P, int(B)
+    a.Ho, a.Wo, a.npos, a.grid = geom.Ho, geom.Wo, geom.npos, int(grid)
+    a.loss_type = _lib.LOSS_TYPES[loss_type]
+    a.loss_scale = float(loss_scale)
+    a.inv_mean_intensity = float(inv_mean)
+    return a
+
+
+def _check_batch_inputs(obj_c, probe_o, prop, positions, batch_idx, targets, mask):
+    dev = obj_c.device
+    _req(obj_c, "obj", torch.complex64, dev)
+    _req(probe_o, "probe", torch.complex64, dev)
+    if prop is not None and prop.numel() > 0:
+        _req(prop, "propagators", torch.complex64, dev)
+    _req(positions, "positions", torch.float32, dev)
+    _req(batch_idx, "batch_indices", torch.int64, dev)
+    _req(targets, "targets", torch.float32, dev)
+    _req(mask, "detector_mask", torch.float32, dev)
+    geom = BatchGeometry.of(obj_c, probe_o, positions.shape[0])
+    if targets.shape[1:] != (geom.n, geom.n) or mask.shape != (geom.n, geom.n):
+        raise ValueError("targets / mask must be (npos, n, n) / (n, n)")
+    if geom.S > 1 and (prop is None or tuple(prop.shape) != (geom.S - 1, geom.n, geom.n)):
+        raise ValueError(f"propagators must be ({geom.S - 1}, {geom.n}, {geom.n})")
+    return geom
+
+
+def loss_scale_of(loss_type: str, B: int, num_gpts: int, mean_intensity: float) -> float:
+    # error / (B / N) / mean_I for l1/l2 (ptychography_base.py:924-931)
+    return float(num_gpts) / float(B) / float(mean_intensity)
+
+
+def batch_forward(obj_c, probe_o, prop, positions, batch_idx, targets, mask, num_gpts, mean_intensity,
+                  loss_type="l2_amplitude", want_intensity=True, want_exit=False, want_waves=False,
+                  probe_hat=None, grid=None):
+    """Forward model + loss of one batch with no gradients.
+
+    Returns dict(loss=0-d tensor, intensity=(B,n,n) detector layout or None,
+    exit=(P,B,n,n) or None, waves=(S,P,B,n,n) or None).
+    """
+    geom = _check_batch_inputs(obj_c, probe_o, prop, positions, batch_idx, targets, mask)
+    B = int(batch_idx.numel())
+    dev = obj_c.device
+    grid = default_grid(B, dev) if grid is None else int(grid)
+    ws = workspace(dev).get(geom, grid, adjoint=False)
+    if probe_hat is None:
+        probe_hat = fft2(probe_o)
+    out_i = torch.empty((B, geom.n, geom.n), dtype=torch.float32, device=dev) if want_intensity else None
+    out_e = torch.empty((geom.P, B, geom.n, geom.n), dtype=torch.complex64, device=dev) if want_exit else None
+    out_w = (torch.empty((geom.S, geom.P, B, geom.n, geom.n), dtype=torch.complex64, device=dev)
+             if want_waves else None)
+    a = _batch_args(geom, obj_c, probe_hat, prop, positions, batch_idx, targets, mask, B, grid, loss_type,
+                    loss_scale_of(loss_type, max(B, 1), num_gpts, mean_intensity), 1.0 / mean_intensity, ws,
+                    out_intensity=out_i, out_exit=out_e, out_waves=out_w)
+    _lib.check(_lib.lib().ptycho_forward_loss(ctypes.byref(a), _stream()), "forward_loss")
+    loss = torch.empty((), dtype=torch.float32, device=dev)
+    if B > 0:
+        _lib.check(_lib.lib().ptycho_reduce_loss(_p(ws.loss_part), grid, _p(loss), _stream()), "reduce_loss")
+    else:
+        loss.zero_()
+    return dict(loss=loss, intensity=out_i, exit=out_e, waves=out_w)
+
+
+def batch_forward_adjoint(obj_c, probe_o, prop, positions, batch_idx, targets, mask, num_gpts, mean_intensity,
+                          loss_type="l2_amplitude", probe_hat=None, grid=None, grad_obj=None,
+                          grad_probe=None):
+    """Fused forward + loss + adjoint of one batch.
+
+    Returns (loss 0-d tensor, grad w.r.t. the constrained object (S,Ho,Wo),
+    grad w.r.t. the orthogonalised probe (P,n,n)), torch gradient convention.
+    ``grad_obj`` (if given) is accumulated into, not cleared.
+    """
+    geom = _check_batch_inputs(obj_c, probe_o, prop, positions, batch_idx, targets, mask)
+    B = int(batch_idx.numel())
+    dev = obj_c.device
+    grid = default_grid(B, dev) if grid is None else int(grid)
+    ws = workspace(dev).get(geom, grid, adjoint=True)
+    if probe_hat is None:
+        probe_hat = fft2(probe_o)
+    if grad_obj is None:
+        grad_obj = torch.zeros_like(obj_c)
+    loss = torch.empty((), dtype=torch.float32, device=dev)
+    if grad_probe is None:
+        grad_probe = torch.empty_like(probe_o)
+    if B == 0:
+        loss.zero_()
+        grad_probe.zero_()
+        return loss, grad_obj, grad_probe
+    a = _batch_args(geom, obj_c, probe_hat, prop, positions, batch_idx, targets, mask, B, grid, loss_type,
+                    loss_scale_of(loss_type, B, num_gpts, mean_intensity), 1.0 / mean_intensity, ws,
+                    grad_obj=grad_obj, adjoint=True)
+    lib = _lib.lib()
+    st = _stream()
+    _lib.check(lib.ptycho_forward_adjoint(ctypes.byref(a), st), "forward_adjoint")
+    _lib.check(lib.ptycho_reduce_loss(_p(ws.loss_part), grid, _p(loss), st), "reduce_loss")
+    nn = geom.P * geom.n * geom.n
+    _lib.check(lib.ptycho_reduce_partials(_p(ws.partials), _p(grad_probe), grid, nn, st), "reduce_partials")
+    inv = 1.0 / float(geom.n * geom.n)
+    _lib.check(lib.ptycho_fft2(_p(grad_probe), _p(grad_probe), geom.P, geom.n, 1, inv, st), "fft2")
+    return loss, grad_obj, grad_probe
+
+
+class _BatchLossFn(torch.autograd.Function):
+    """loss(obj_raw, probe_o) of one batch; gradients from the fused adjoint kernel."""
+
+    @staticmethod
+    def forward(ctx, obj_raw, probe_o, prop, positions, batch_idx, targets, mask, cfg):
+        obj_raw_c = obj_raw.detach().contiguous()
+        probe_c = probe_o.detach().contiguous()
+        obj_c, work = obj_constrain(obj_raw_c)
+        need = ctx.needs_input_grad[0] or ctx.needs_input_grad[1]
+        if need:
+            loss, g_obj_c, g_probe = batch_forward_adjoint(
+                obj_c, probe_c, prop, positions, batch_idx, targets, mask, cfg["num_gpts"],
+                cfg["mean_intensity"], cfg["loss_type"], grid=cfg.get("grid"))
+            ctx.save_for_backward(obj_raw_c, work, g_obj_c, g_probe)
+        else:
+            loss = batch_forward(obj_c, probe_c, prop, positions, batch_idx, targets, mask, cfg["num_gpts"],
+                                 cfg["mean_intensity"], cfg["loss_type"], want_intensity=False,
+                                 grid=cfg.get("grid"))["loss"]
+        return loss
+
+    @staticmethod
+    def backward(ctx, gout):
+        obj_raw, work, g_obj_c, g_probe = ctx.saved_tensors
+        gout = gout.detach().to(torch.float32).reshape(1).contiguous()
+        g_obj = None
+        if ctx.needs_input_grad[0]:
+            g_obj = obj_constrain_vjp(obj_raw, g_obj_c, work, scale=gout)
+        g_pr = g_probe * gout if ctx.needs_input_grad[1] else None
+        return g_obj, g_pr, None, None, None, None, None, None
+
+
+def batch_loss(obj_raw, probe_o, prop, positions, batch_idx, targets, mask, num_gpts, mean_intensity,
+               loss_type="l2_amplitude", grid=None):
+    """Differentiable consistency loss of one batch w.r.t. the raw object
+    parameter (hard constraint included) and the orthogonalised probe."""
+    cfg = dict(num_gpts=int(num_gpts), mean_intensity=float(mean_intensity), loss_type=loss_type, grid=grid)
+    return _BatchLossFn.apply(obj_raw, probe_o, prop, positions, batch_idx, targets, mask, cfg)
+
+
+# ----------------------------------------------------------------------------
+# optimiser steps
+# ----------------------------------------------------------------------------
+
+def _real_view(t: torch.Tensor) -> torch.Tensor:
+    return torch.view_as_real(t) if t.is_complex() else t
+
+
+def adam_step(param, grad, exp_avg, exp_avg_sq, step: int, lr: float, betas=(0.9, 0.999), eps=1e-8,
+              weight_decay=0.0, decoupled=False, lr_tensor=None):
+    p, g = _real_view(param), _real_view(grad)
+    m, v = _real_view(exp_avg), _real_view(exp_avg_sq)
+    for name, t in (("param", p), ("grad", g), ("exp_avg", m), ("exp_avg_sq", v)):
+        _req(t.reshape(-1) if t.is_contiguous() else t, name, torch.float32)
+    b1, b2 = betas
+    bc1 = 1.0 - b1 ** step
+    bc2s = (1.0 - b2 ** step) ** 0.5
+    _lib.check(_lib.lib().ptycho_adam_step(_p(p), _p(g), _p(m), _p(v), p.numel(), float(lr), _p(lr_tensor),
+                                           float(b1), float(b2), float(eps), float(weight_decay),
+                                           int(bool(decoupled)), float(bc1), float(bc2s), _stream()), "adam_step")
+
+
+def sgd_step(param, grad, lr: float, weight_decay=0.0, lr_tensor=None):
+    p, g = _real_view(param), _real_view(grad)
+    _req(p, "param", torch.float32)
+    _req(g, "grad", torch.float32)
+    _lib.check(_lib.lib().ptycho_sgd_step(_p(p), _p(g), p.numel(), float(lr), _p(lr_tensor),
+                                          float(weight_decay), _stream()), "sgd_step")

@@ -1,0 +1,233 @@
+"""Generate golden fixtures by running the reference quantem package itself.
+
+Run in a container where the reference source tree is mounted:
+
+    python tests/golden/make_golden.py /root/reference/src
+
+For each seeded case this records the reference's own set-up products
+(targets, mean intensity, scan positions, object shape, initial probe,
+propagators), the predicted intensities / loss / autograd gradients of one
+batch, and the object, probe and losses after a few ``reconstruct`` iterations.
+The fixtures pin the CPU oracle (``oracle/ptycho_oracle.py``), the host-side
+set-up of ``quantem_b200.diffractive_imaging`` and the CUDA path.
+
+Inputs are synthetic: Gaussian-atom phase objects, probes from the reference's
+``real_space_probe`` and Poisson-noised intensities simulated with the oracle's
+forward model.  The reference's own gradient test (tests/diffractive_imaging/
+test_ptychography.py:31-146) is restated as case ``whitenoise64`` with the same
+recipe (white-noise phase, analytic soft-aperture probe, 1 px raster).
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle import ptycho_oracle as O  # noqa: E402
+from oracle.quantem_shim import import_reference  # noqa: E402
+
+
+def _c64(x):
+    return np.asarray(x).astype(np.complex64)
+
+
+def _f32(x):
+    return np.asarray(x).astype(np.float32)
+
+
+def simulate_data(true_obj, probes, positions_px, props, counts, rng):
+    """Poisson diffraction data in detector (centred) layout, shape (N, H, W)."""
+    st = O.forward(true_obj, probes, positions_px, props)
+    inten = O.detector_intensities(st)
+    inten = inten / inten.sum(axis=(-2, -1), keepdims=True).mean() * counts
+    return rng.poisson(inten).astype(np.float32)
+
+
+def run_case(name, *, H, S, P, nscan, step_px, pad, dz, counts, jitter, batch, iters,
+             weights=None, seed=0, opt=None, orthogonalize=True, keep_data=True):
+    import torch
+    from quantem.core.datastructures.dataset4dstem import Dataset4dstem
+    from quantem.diffractive_imaging.complex_probe import real_space_probe
+    from quantem.diffractive_imaging.dataset_models import PtychographyDatasetRaster
+    from quantem.diffractive_imaging.detector_models import DetectorPixelated
+    from quantem.diffractive_imaging.object_models import ObjectPixelated
+    from quantem.diffractive_imaging.probe_models import ProbePixelated
+    from quantem.diffractive_imaging.ptychography import Ptychography
+
+    rng = np.random.default_rng(seed)
+    px = 0.2  # real-space pixel [A]
+    rs = 1.0 / (H * px)
+    energy = 300e3
+    # --- synthetic truth (oracle forward model, FP64) ---
+    probe1 = real_space_probe(gpts=(H, H), sampling=(px, px), energy=energy, semiangle_cutoff=20.0,
+                              aberration_coefs={"C10": -200.0}).numpy().astype(np.complex128)
+    probes = np.stack([probe1] + [np.roll(probe1, k + 1, axis=1) * 0.3 for k in range(P - 1)])
+    ext = (nscan - 1) * step_px
+    obj_hw = int(ext + 2 * pad)
+    obj_hw += (-obj_hw) % 8
+    phase = np.stack([O.gaussian_atom_phase((obj_hw, obj_hw), max(4, obj_hw * obj_hw // 400), 1.5,
+                                            0.3 if S == 1 else 0.1, rng) for _ in range(S)])
+    true_obj = np.exp(1j * phase)
+    grid = np.stack(np.meshgrid(np.arange(nscan), np.arange(nscan), indexing="ij"), -1).reshape(-1, 2)
+    pos_true = grid * step_px + pad
+    if jitter:
+        pos_true = pos_true + rng.uniform(-0.5, 0.5, size=pos_true.shape)
+    props_true = O.propagators((H, H), (px, px), energy, [dz] * (S - 1))
+    data = simulate_data(true_obj, probes, pos_true, props_true, counts, rng)
+
+    d4 = Dataset4dstem.from_array(data.reshape(nscan, nscan, H, H),
+                                  sampling=(step_px * px, step_px * px, rs, rs),
+                                  units=("A", "A", "A^-1", "A^-1"))
+    pd = PtychographyDatasetRaster.from_dataset4dstem(d4, verbose=0)
+    pd.preprocess(com_fit_function="constant", force_com_rotation=0, force_com_transpose=False,
+                  plot_rotation=False, plot_com=False, probe_energy=energy)
+    obj_model = ObjectPixelated.from_uniform(num_slices=S, slice_thicknesses=dz, obj_type="complex")
+    probe_model = ProbePixelated.from_params(
+        probe_params={"energy": energy, "defocus": 200.0, "semiangle_cutoff": 20.0},
+        num_probes=P, rng=seed + 1, initial_probe_weights=weights)
+    pt = Ptychography.from_models(dset=pd, obj_model=obj_model, probe_model=probe_model,
+                                  detector_model=DetectorPixelated(), device="cpu", verbose=0,
+                                  rng=seed + 2)
+    pt.preprocess(obj_padding_px=(pad, pad))
+    if jitter:
+        jit = rng.uniform(-0.5, 0.5, size=(pd.num_gpts, 2)).astype(np.float32)
+        pd.scan_positions_px = pd.scan_positions_px.detach() + torch.tensor(jit)
+
+    out = dict(
+        H=H, S=S, P=P, nscan=nscan, step_px=step_px, pad=pad, dz=dz, px=px, energy=energy,
+        jitter=int(jitter), batch=batch, iters=iters, seed=seed, counts=counts,
+        weights=np.asarray(weights if weights is not None else [], dtype=np.float64),
+        orthogonalize=int(orthogonalize),
+        data=data if keep_data else np.zeros(0, np.float32),
+        targets=_f32(pd.targets.numpy()),
+        mean_intensity=np.float64(pd.mean_diffraction_intensity),
+        positions=_f32(pd.scan_positions_px.detach().numpy()),
+        initial_positions=_f32(pd.initial_scan_positions_px.numpy()),
+        obj_shape=np.asarray(pt.obj_shape_full),
+        obj_padding_px=np.asarray(pt.obj_padding_px),
+        upsample_factor=np.float64(pd.upsample_factor),
+        probe_init=_c64(probe_model._probe.detach().numpy()),
+        propagators=_c64(pt._propagators.numpy()) if S > 1 else np.zeros((0, H, H), np.complex64),
+        sampling=np.asarray(pt.sampling, dtype=np.float64),
+    )
+
+    # --- one batch at a perturbed object: intensities, loss, gradients ---
+    constraints = {"probe": {"orthogonalize_probe": bool(orthogonalize)}}
+    pt.constraints = constraints
+    with torch.no_grad():
+        shp = tuple(obj_model._obj.shape)
+        amp = 1.0 - 0.3 * rng.random(shp)
+        ph = 0.4 * rng.standard_normal(shp)
+        obj_model._obj.data = torch.tensor(amp * np.exp(1j * ph), dtype=torch.complex64)
+    out["obj_perturbed"] = _c64(obj_model._obj.detach().numpy())
+    bi = np.arange(min(batch, pd.num_gpts))
+    obj_model._obj.grad = None
+    probe_model._probe.grad = None
+    pt.dset._set_targets("l2_amplitude")
+    pt.compute_propagator_arrays()
+    patch_indices, _pos, frac, descan = pt.dset.forward(bi, pt.obj_padding_px)
+    sp = probe_model.forward(frac)
+    op = obj_model.forward(patch_indices)
+    prop, ov = pt.forward_operator(op, sp, descan)
+    inten = pt.detector_model.forward(ov)
+    loss, tg = pt.error_estimate(inten, bi)
+    pt.backward(loss, True, op, prop, ov, patch_indices, tg)
+    out.update(
+        batch_indices=bi,
+        batch_intensities=_f32(inten.detach().numpy()),
+        batch_loss=np.float64(loss.item()),
+        grad_obj=_c64(obj_model._obj.grad.numpy()),
+        grad_probe=_c64(probe_model._probe.grad.numpy()),
+        probe_ortho=_c64(probe_model.probe.detach().numpy()),
+    )
+
+    # --- a few reconstruct iterations from the same state ---
+    with torch.no_grad():
+        obj_model._obj.grad = None
+        probe_model._probe.grad = None
+    opt = opt or {"object": {"type": "adam"}, "probe": {"type": "adam"}}
+    pt.rng = seed + 3
+    pt.reconstruct(num_iters=iters, batch_size=batch, optimizer_params=opt,
+                   constraints=constraints, device="cpu")
+    out.update(
+        recon_obj=_c64(obj_model._obj.detach().numpy()),
+        recon_probe=_c64(probe_model._probe.detach().numpy()),
+        recon_losses=np.asarray(pt._iter_losses, dtype=np.float64),
+        recon_rng_seed=np.int64(seed + 3),
+    )
+    path = os.path.join(HERE, f"{name}.npz")
+    np.savez_compressed(path, **out)
+    print(f"wrote {path}: obj {tuple(pt.obj_shape_full)} N={pd.num_gpts} losses={out['recon_losses']}")
+
+
+def whitenoise_case():
+    """The reference gradient test's fixture (test_ptychography.py:19-212), restated."""
+    import torch
+    from quantem.core.datastructures.dataset4dstem import Dataset4dstem
+    from quantem.diffractive_imaging.dataset_models import PtychographyDatasetRaster
+    from quantem.diffractive_imaging.detector_models import DetectorPixelated
+    from quantem.diffractive_imaging.object_models import ObjectPixelated
+    from quantem.diffractive_imaging.probe_models import ProbePixelated
+    from quantem.diffractive_imaging.ptychography import Ptychography
+
+    from tests.golden.whitenoise import whitenoise_inputs
+
+    inp = whitenoise_inputs()
+    N = inp["N"]
+    d4 = Dataset4dstem.from_array(inp["data4d"], sampling=inp["sampling4d"],
+                                  units=("A", "A", "A^-1", "A^-1"))
+    pd = PtychographyDatasetRaster.from_dataset4dstem(d4, verbose=0)
+    pd.preprocess(com_fit_function="constant", plot_rotation=False, plot_com=False,
+                  probe_energy=inp["energy"], force_com_rotation=0, force_com_transpose=False)
+    out = {}
+    for nprobe in (1, 2):
+        for autograd in (True, False):
+            obj_model = ObjectPixelated.from_uniform(num_slices=1, obj_type="complex",
+                                                     slice_thicknesses=1)
+            # a (P, N, N) stack: the reference's from_array concatenates a 2-D
+            # array along rows when num_probes > 1 (probe_models.py:603-606)
+            probe_model = ProbePixelated.from_array(
+                num_probes=nprobe, probe_params=inp["probe_params"],
+                probe_array=np.stack([inp["probe"]] * nprobe).astype(np.complex64))
+            pt = Ptychography.from_models(dset=pd, obj_model=obj_model, probe_model=probe_model,
+                                          detector_model=DetectorPixelated(), rng=42, verbose=0)
+            pt.preprocess(obj_padding_px=(0, 0))
+            pt.reconstruct(num_iters=1, reset=True, autograd=autograd,
+                           constraints={"probe": {"orthogonalize_probe": False}},
+                           optimizer_params={"object": {"type": "sgd", "lr": 0.5},
+                                             "probe": {"type": "sgd", "lr": 0.5}},
+                           batch_size=N * N, device="cpu")
+            tag = f"p{nprobe}_{'ad' if autograd else 'an'}"
+            out[f"grad_obj_{tag}"] = _c64(obj_model._obj.grad.numpy())
+            out[f"grad_probe_{tag}"] = _c64(probe_model._probe.grad.numpy())
+            out[f"loss_{tag}"] = np.asarray(pt._iter_losses, dtype=np.float64)
+    out["targets_sum"] = np.float64(pd.targets.numpy().astype(np.float64).sum())
+    out["mean_intensity"] = np.float64(pd.mean_diffraction_intensity)
+    path = os.path.join(HERE, "whitenoise64.npz")
+    np.savez_compressed(path, **out)
+    print(f"wrote {path}")
+    del torch
+
+
+def main(src):
+    import torch
+
+    torch.manual_seed(0)
+    import_reference(src)
+    run_case("single64", H=64, S=1, P=1, nscan=6, step_px=4, pad=32, dz=20.0, counts=1e5,
+             jitter=False, batch=12, iters=3, seed=11)
+    run_case("mixed64", H=64, S=3, P=3, nscan=5, step_px=6, pad=32, dz=20.0, counts=1e5,
+             jitter=True, batch=10, iters=2, weights=[0.7, 0.2, 0.1], seed=21)
+    run_case("mixed128", H=128, S=4, P=4, nscan=3, step_px=6, pad=64, dz=20.0, counts=1e5,
+             jitter=True, batch=9, iters=2, weights=[0.7, 0.15, 0.1, 0.05], seed=31,
+             keep_data=False)
+    whitenoise_case()
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src")
