@@ -1,0 +1,360 @@
+"""Benchmark of the multislice mixed-probe ptychography iteration on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one "step" = one full gradient iteration over every scan position):
+object 512 x 512 x 8 slices (20 A), 4 probe modes at 128 x 128 (weights
+0.7/0.15/0.1/0.05), 64 x 64 raster with 6 px step and +-0.5 px jitter, 1e5
+counts/pattern Poisson data, l2_amplitude loss, Adam on object and probe, batch
+= all 4096 positions (the reference's default batch size).  Data are seeded
+synthetic inputs simulated with this package's forward kernels.
+
+``--impl ours`` times the CUDA path (device-resident ``value``; ``e2e`` through
+the public reconstruct call with the measured data copied from pinned host
+memory every step).  ``--impl reference`` times the CPU oracle port of the
+reference algorithm on the host cores on a bounded sample of the same workload.
+With ``--gpus N`` (torchrun), every rank reconstructs its own dataset: N
+independent replicas, no collective.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "scan positions/s per iteration"
+WORKLOAD = "multislice mixed-probe: 512x512x8 object, 4 modes at 128x128, 64x64 scan, batch 4096"
+FLOPS_PER_POS = 167.8e6     # 4*P*S FFTs * 5*HW*log2(HW) + 40*P*S*HW (c2)
+BYTES_PER_POS = 3.06 * 2**20  # streaming lower bound per position (c2)
+
+
+def _peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        try:
+            with open(self.path) as fh:
+                for line in fh:
+                    f = [x.strip() for x in line.split(",")]
+                    if len(f) < 9:
+                        continue
+                    try:
+                        sm.append(float(f[1]))
+                        smax = float(f[2])
+                    except ValueError:
+                        continue
+                    for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                                        "sw_power_cap"), f[5:9]):
+                        if v.lower().startswith("active"):
+                            reasons.add(name)
+        except Exception:
+            pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def _init_dist(world, backend):
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=120))
+        return dist
+    return None
+
+
+def build_problem(seed, device, batch_size):
+    import torch
+
+    from quantem_b200 import engine, synthetic
+    from quantem_b200.diffractive_imaging.ptycho_utils import SimpleBatcher
+
+    cfg = synthetic.SyntheticConfig(seed=seed)
+    ds = synthetic.make_dataset(cfg, device)
+    S, Ho, Wo = ds["obj_shape"]
+    obj = torch.ones((S, Ho, Wo), dtype=torch.complex64, device=device).requires_grad_(True)
+    probe = (ds["probes"][:1].repeat(cfg.modes, 1, 1) * torch.linspace(1.0, 0.3, cfg.modes, device=device)[:, None, None]
+             ).to(torch.complex64)
+    k = torch.fft.fftfreq(cfg.n, device=device)
+    for m in range(1, cfg.modes):  # decorrelate the initial modes
+        probe[m] *= torch.exp(-2j * torch.pi * (0.3 * m) * k[:, None]).to(torch.complex64)
+    # Parseval: sum over modes of |probe|^2 equals the mean pattern intensity
+    # (the reference's _apply_weights normalisation, probe_models.py:860-873)
+    probe = probe * torch.sqrt(ds["mean_intensity"] / probe.abs().square().sum())
+    probe = probe.contiguous().requires_grad_(True)
+    pt = engine.ProblemTensors(
+        obj=obj, probe=probe, prop=ds["propagators"], positions=ds["positions"],
+        targets=ds["amplitudes"].contiguous(), mask=torch.ones((cfg.n, cfg.n), device=device),
+        mean_intensity=ds["mean_intensity"], upsample_factor=cfg.step_px)
+    opts = [engine.make_optimizer([obj], {"type": "adam", "lr": 5e-3}),
+            engine.make_optimizer([probe], {"type": "adam", "lr": 1e-3})]
+    batcher = SimpleBatcher(pt.num_gpts, batch_size, rng=seed)
+    return cfg, ds, pt, opts, batcher
+
+
+def fp32_peak_tflops(device):
+    """FP32 FMA throughput of this GPU (own microbenchmark kernel), TFLOP/s."""
+    import ctypes
+
+    import torch
+
+    from quantem_b200 import _lib
+
+    lib = _lib.lib()
+    if not hasattr(lib, "ptycho_fp32_fma_probe"):
+        return None
+    fn = lib.ptycho_fp32_fma_probe
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+    out = torch.empty(148 * 4 * 1024, dtype=torch.float32, device=device)
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    iters = 4096
+    blocks = 148 * 4
+    for _ in range(3):
+        _lib.check(fn(ctypes.c_void_p(out.data_ptr()), iters, blocks, st), "fma probe")
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(5):
+        fn(ctypes.c_void_p(out.data_ptr()), iters, blocks, st)
+    e.record()
+    torch.cuda.synchronize()
+    ms = s.elapsed_time(e) / 5
+    flops = blocks * 512 * iters * 16 * 2  # 16 independent FMA chains per thread
+    return flops / (ms * 1e-3) / 1e12
+
+
+def run_ours(args):
+    import torch
+
+    from quantem_b200 import engine, ops
+
+    rank, world, local = _dist_env()
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    dist = _init_dist(world, "nccl")
+    cfg, ds, pt, opts, batcher = build_problem(1234 + rank, device, args.batch_size)
+    npos = pt.num_gpts
+
+    # warm-up
+    for _ in range(args.warmup):
+        engine.run_iteration(pt, batcher, opts)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+
+    # ---- device-resident timed region ----
+    fused_events = []
+    ops.PROFILE_EVENTS = fused_events
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record()
+        losses = []
+        for _ in range(args.steps):
+            losses.append(engine.run_iteration(pt, batcher, opts))
+        t1.record()
+        torch.cuda.synchronize()
+    ops.PROFILE_EVENTS = None
+    ms = t0.elapsed_time(t1) / args.steps
+    fused_ms = [a.elapsed_time(b) for a, b in fused_events]
+    launches_per_batch = 11
+    nbatches = len(batcher) * args.steps
+
+    # ---- end to end through the public call with host buffers ----
+    host_t = ds["amplitudes"].cpu().pin_memory()
+    host_p = pt.positions.cpu().pin_memory()
+    loss_host = torch.empty(1, dtype=torch.float32).pin_memory()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(args.steps):
+        pt.targets.copy_(host_t, non_blocking=True)
+        pt.positions.copy_(host_p, non_blocking=True)
+        l = engine.run_iteration(pt, batcher, opts)
+        loss_host.copy_(l.reshape(1), non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / args.steps
+
+    ms_t = torch.tensor([ms, e2e_ms], device=device)
+    if dist:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms, e2e_ms = ms_t.tolist()
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    value = npos * world / (ms * 1e-3)
+    e2e = npos * world / (e2e_ms * 1e-3)
+    hbm_peak, peak_kind = _peaks()
+    fused_avg_ms = statistics.mean(fused_ms) if fused_ms else None
+    pos_per_launch = args.batch_size if args.batch_size else npos
+    roofline = None
+    if fused_avg_ms:
+        achieved = BYTES_PER_POS * pos_per_launch / (fused_avg_ms * 1e-3) / 1e9
+        roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
+                    "frac": round(achieved / hbm_peak, 4), "traffic": _ncu_traffic(), "peak_source": peak_kind,
+                    "kernel": "fused_batch_kernel<128,adjoint>", "kernel_ms": round(fused_avg_ms, 4)}
+    fp32 = fp32_peak_tflops(device)
+    fp32_roof = None
+    if fused_avg_ms and fp32:
+        ach = FLOPS_PER_POS * pos_per_launch / (fused_avg_ms * 1e-3) / 1e12
+        fp32_roof = {"bound": "fp32", "achieved": round(ach, 2), "peak": round(fp32, 2), "unit": "TFLOP/s",
+                     "frac": round(ach / fp32, 4), "peak_source": "measured (own FMA probe)"}
+    cpu = cpu_baseline_sample(args)
+    line = {
+        "metric": METRIC, "value": round(value, 1), "unit": "positions/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c64/f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "global_batch": pos_per_launch * world, "positions": npos,
+                   "object": [cfg.slices, 512, 512], "probe": [cfg.modes, cfg.n, cfg.n],
+                   "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (targets 256 MiB/step)"},
+        "e2e": {"value": round(e2e, 1), "unit": "positions/s", "h2d_bytes_per_step": int(host_t.numel() * 4
+                                                                                          + host_p.numel() * 4),
+                "d2h_bytes_per_step": 4},
+        "gpu_launches": launches_per_batch * nbatches,
+        "roofline": roofline, "roofline_fp32": fp32_roof,
+        "cpu_baseline": cpu,
+        "clocks": clk.summary(),
+        "final_loss": float(losses[-1].item()),
+    }
+    print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+
+
+def _ncu_traffic():
+    """DRAM bytes per launch of the fused kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "fused_batch_kernel_traffic.json")
+    try:
+        with open(path) as fh:
+            return json.load(fh)["dram_bytes_per_launch_full_batch"]
+    except Exception:
+        return None
+
+
+def cpu_baseline_sample(args, positions=8):
+    """Time the oracle port (the reference algorithm restated in numpy/scipy,
+    complex64, scipy.fft with every host core) on a bounded sample of the
+    workload: one batch of `positions` positions, forward + loss + adjoint."""
+    from oracle import ptycho_oracle as O
+
+    ncores = os.cpu_count() or 1
+    O.set_workers(ncores)
+    rng = np.random.default_rng(0)
+    S, P, n, Ho = 8, 4, 128, 512
+    obj = np.exp(1j * 0.1 * rng.standard_normal((S, Ho, Ho))).astype(np.complex64)
+    probe = (rng.standard_normal((P, n, n)) + 1j * rng.standard_normal((P, n, n))).astype(np.complex64)
+    props = O.propagators((n, n), (0.2, 0.2), 300e3, [20.0] * (S - 1), cdtype=np.complex64)
+    pos = rng.uniform(70, 440, size=(positions, 2)).astype(np.float32)
+    tg = np.abs(rng.standard_normal((positions, n, n))).astype(np.float32)
+    mask = np.ones((n, n), np.float32)
+    reps = 0
+    t0 = time.perf_counter()
+    while True:
+        O.full_gradients(obj, probe, pos, props, tg, mask, 4096, 1e5, 6.0)
+        reps += 1
+        el = time.perf_counter() - t0
+        if el > args.cpu_seconds or reps >= 50:
+            break
+    rate = reps * positions / el
+    return {"value": round(rate, 2), "unit": "positions/s", "cores": ncores, "kind": "port",
+            "sample": f"{reps} x {positions}-position batches of the same geometry, forward+loss+adjoint "
+                      f"(optimizer step excluded), complex64, scipy.fft workers={ncores}"}
+
+
+def run_reference(args):
+    rank, world, _ = _dist_env()
+    if rank != 0:
+        return
+    cpu = cpu_baseline_sample(args)
+    line = {"metric": METRIC, "value": cpu["value"], "unit": "positions/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c64/f32", "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD, "parallelism": "host cores"},
+            "cpu_baseline": cpu, "e2e": {"value": cpu["value"], "unit": "positions/s",
+                                          "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--batch-size", type=int, default=4096)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -130,6 +130,11 @@ int ptycho_adam_step(float* param, const float* grad, float* exp_avg, float* exp
 int ptycho_sgd_step(float* param, const float* grad, int64_t count, float lr, const float* lr_dev,
                     float weight_decay, void* stream);
 
+/* Measurement utility (no reference counterpart): FP32 FMA throughput probe used to
+ * state the FP32-pipe roofline.  `out` holds blocks * 512 floats; each thread runs
+ * 16 independent FMA chains of `iters` steps (32 * iters flops per thread). */
+int ptycho_fp32_fma_probe(float* out, int iters, int blocks, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

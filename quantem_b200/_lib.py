@@ -40,6 +40,7 @@ EXPORTED = (
     "ptycho_reduce_blocks",
     "ptycho_adam_step",
     "ptycho_sgd_step",
+    "ptycho_fp32_fma_probe",
 )
 
 _vp = ctypes.c_void_p
@@ -83,6 +84,7 @@ def _declare(lib):
         "ptycho_adam_step": (_int, [_vp, _vp, _vp, _vp, _i64, _flt, _vp, _flt, _flt, _flt, _flt, _int, _flt, _flt,
                                     _vp]),
         "ptycho_sgd_step": (_int, [_vp, _vp, _i64, _flt, _vp, _flt, _vp]),
+        "ptycho_fp32_fma_probe": (_int, [_vp, _int, _int, _vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

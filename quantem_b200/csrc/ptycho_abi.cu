@@ -192,6 +192,22 @@ __global__ void sgd_kernel(float* __restrict__ p, const float* __restrict__ g, i
   }
 }
 
+// FP32 FMA throughput probe: 16 independent dependent-FMA chains per thread.
+__global__ void __launch_bounds__(512) fma_probe_kernel(float* out, int iters) {
+  float a[16];
+  const float b = 1.0000001f + threadIdx.x * 1e-9f, c = 1e-7f;
+#pragma unroll
+  for (int k = 0; k < 16; ++k) a[k] = (float)(threadIdx.x + k) * 1e-3f;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < 16; ++k) a[k] = fmaf(a[k], b, c);
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int k = 0; k < 16; ++k) s += a[k];
+  out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
 int grid_for(int64_t n, int threads) {
   int64_t b = (n + threads - 1) / threads;
   if (b > 4 * 148) b = 4 * 148;
@@ -342,6 +358,12 @@ int ptycho_adam_step(float* param, const float* grad, float* exp_avg, float* exp
   adam_kernel<<<grid_for(count, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
       param, grad, exp_avg, exp_avg_sq, count, lr, lr_dev, beta1, beta2, eps, weight_decay, decoupled, bc1, bc2_sqrt);
   return check_launch("adam_kernel");
+}
+
+int ptycho_fp32_fma_probe(float* out, int iters, int blocks, void* stream) {
+  if (!out || iters < 1 || blocks < 1) return fail(PTYCHO_ERR_INVALID, "fma probe: bad arguments");
+  fma_probe_kernel<<<blocks, 512, 0, static_cast<cudaStream_t>(stream)>>>(out, iters);
+  return check_launch("fma_probe_kernel");
 }
 
 int ptycho_sgd_step(float* param, const float* grad, int64_t count, float lr, const float* lr_dev,

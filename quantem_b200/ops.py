@@ -16,6 +16,11 @@ from . import _lib
 
 SUPPORTED_N = (64, 128)
 
+# When set to a list, every fused forward+adjoint launch appends a pair of CUDA
+# events recorded on the launching stream around it (used by bench.py to time
+# the dominant kernel inside the timed region).
+PROFILE_EVENTS = None
+
 
 def _stream() -> ctypes.c_void_p:
     return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
@@ -289,7 +294,13 @@ def batch_forward_adjoint(obj_c, probe_o, prop, positions, batch_idx, targets, m
                     grad_obj=grad_obj, adjoint=True)
     lib = _lib.lib()
     st = _stream()
+    if PROFILE_EVENTS is not None:
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
     _lib.check(lib.ptycho_forward_adjoint(ctypes.byref(a), st), "forward_adjoint")
+    if PROFILE_EVENTS is not None:
+        ev1.record()
+        PROFILE_EVENTS.append((ev0, ev1))
     _lib.check(lib.ptycho_reduce_loss(_p(ws.loss_part), grid, _p(loss), st), "reduce_loss")
     nn = geom.P * geom.n * geom.n
     _lib.check(lib.ptycho_reduce_partials(_p(ws.partials), _p(grad_probe), grid, nn, st), "reduce_partials")
