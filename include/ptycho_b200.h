@@ -135,6 +135,23 @@ int ptycho_sgd_step(float* param, const float* grad, int64_t count, float lr, co
  * 16 independent FMA chains of `iters` steps (32 * iters flops per thread). */
 int ptycho_fp32_fma_probe(float* out, int iters, int blocks, void* stream);
 
+/* Largest launch grid accepted by ptycho_forward_loss_noalloc. */
+#define PTYCHO_NOALLOC_MAX_GRID 1024
+
+/* No counterpart in the reference.  Same as ptycho_forward_loss followed by
+ * ptycho_reduce_loss, for callers that cannot allocate device memory (their
+ * memory belongs to another framework's allocator, or allocation and the device
+ * synchronisation it can cause are not allowed where they run).  The per-CTA
+ * loss partials live in a static device array owned by the library
+ * (PTYCHO_NOALLOC_MAX_GRID doubles, held on every GPU that loads the library
+ * until exit); a->loss_part is ignored and the summed loss is written to the
+ * device float *out_loss.  Nothing is allocated or freed.  a->grid above
+ * PTYCHO_NOALLOC_MAX_GRID is rejected with PTYCHO_ERR_INVALID.  The first call
+ * on a device looks up the array's device address (cudaGetSymbolAddress), so
+ * make that first call before any stream capture.  All calls on a device share
+ * the array: calls that overlap on the GPU race. */
+int ptycho_forward_loss_noalloc(const ptycho_batch_args* a, float* out_loss, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -41,6 +41,7 @@ EXPORTED = (
     "ptycho_adam_step",
     "ptycho_sgd_step",
     "ptycho_fp32_fma_probe",
+    "ptycho_forward_loss_noalloc",
 )
 
 _vp = ctypes.c_void_p
@@ -85,6 +86,7 @@ def _declare(lib):
                                     _vp]),
         "ptycho_sgd_step": (_int, [_vp, _vp, _i64, _flt, _vp, _flt, _vp]),
         "ptycho_fp32_fma_probe": (_int, [_vp, _int, _int, _vp]),
+        "ptycho_forward_loss_noalloc": (_int, [ctypes.POINTER(BatchArgs), _vp, _vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -217,6 +217,9 @@ int grid_for(int64_t n, int threads) {
 
 }  // namespace
 
+// Records `msg` as this host thread's last error (used by noalloc.cu).
+int qb_record_error(int code, const char* msg) { return fail(code, "%s", msg); }
+
 // defined in fused_n64.cu / fused_n128.cu
 int qb_launch_batch_64(const ptycho_batch_args* a, bool adj, cudaStream_t st);
 int qb_launch_batch_128(const ptycho_batch_args* a, bool adj, cudaStream_t st);
