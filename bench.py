@@ -325,6 +325,35 @@ def cpu_baseline_sample(args, positions=8):
                       f"(optimizer step excluded), complex64, scipy.fft workers={ncores}"}
 
 
+def run_kernel_only(args):
+    """Launch only the fused forward+adjoint batch kernel on `--positions`
+    positions of the same geometry (small cases for ncu captures)."""
+    import torch
+
+    from quantem_b200 import ops, synthetic
+
+    device = torch.device("cuda", 0)
+    cfg = synthetic.SyntheticConfig(seed=7, scan=(32, 32))  # 1024 positions: small device footprint
+    ds = synthetic.make_dataset(cfg, device)
+    S, Ho, Wo = ds["obj_shape"]
+    obj_c, _ = ops.obj_constrain(ds["obj"])
+    probes = ds["probes"] * (ds["mean_intensity"] ** 0.5)
+    idx = torch.arange(args.positions, device=device, dtype=torch.int64)
+    mask = torch.ones((cfg.n, cfg.n), device=device)
+    times = []
+    for i in range(args.warmup + args.steps):
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record()
+        ops.batch_forward_adjoint(obj_c, probes, ds["propagators"], ds["positions"], idx, ds["amplitudes"], mask,
+                                  ds["positions"].shape[0], ds["mean_intensity"])
+        s1.record()
+        torch.cuda.synchronize()
+        if i >= args.warmup:
+            times.append(s0.elapsed_time(s1))
+    print(json.dumps({"mode": "kernel-only", "positions": args.positions, "ms_per_batch": statistics.mean(times),
+                      "positions_per_s": args.positions / (statistics.mean(times) * 1e-3)}))
+
+
 def run_reference(args):
     rank, world, _ = _dist_env()
     if rank != 0:
@@ -347,10 +376,14 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--batch-size", type=int, default=4096)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--kernel-only", action="store_true", help="time only the fused batch kernel")
+    ap.add_argument("--positions", type=int, default=296, help="positions per launch with --kernel-only")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == "reference":
+    if args.kernel_only:
+        run_kernel_only(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)
