@@ -58,7 +58,8 @@ enum {
 typedef struct ptycho_batch_args {
   const void* obj;           /* complex64 (S, Ho, Wo): hard-constrained object */
   const void* probe_hat;     /* complex64 (P, N, N): fft2 of the probe modes */
-  const void* prop;          /* complex64 (S-1, N, N): Fresnel propagators (may be NULL if S == 1) */
+  const void* prop;          /* complex64 (S-1, N, N): Fresnel propagators (may be NULL if S == 1
+                                or if prop_r/prop_c are given) */
   const float* positions;    /* float32 (npos, 2): scan positions [px] (row, col) */
   const int64_t* batch_idx;  /* int64 (B,): positions / targets rows of this batch */
   const float* targets;      /* float32 (npos, N, N): measured amplitudes/intensities, detector layout */
@@ -71,6 +72,8 @@ typedef struct ptycho_batch_args {
   void* out_exit;            /* optional complex64 (P, B, N, N): exit waves */
   void* out_waves;           /* optional complex64 (S, P, B, N, N): wave entering each slice */
   int* status;               /* optional int32: incremented by the count of non-finite intensities */
+  const void* prop_r;        /* optional complex64 (S-1, N): separable propagator factors, */
+  const void* prop_c;        /*   K_s[kr][kc] = prop_r[s][kr] * prop_c[s][kc] (kept in shared memory) */
   int n, S, P, B, Ho, Wo, npos, grid;
   int loss_type;             /* PTYCHO_LOSS_* */
   float loss_scale;          /* npos_total / (B * mean_intensity) */

@@ -443,3 +443,31 @@ def gaussian_atom_phase(shape, n_atoms, sigma_px, peak_rad, rng):
         dc = (cc - c0 + W / 2) % W - W / 2
         out += np.exp(-(dr**2 + dc**2) / (2 * sigma_px**2))
     return peak_rad * out
+
+
+# ----------------------------------------------------------------------------
+# iteration driver
+# ----------------------------------------------------------------------------
+
+def reconstruct(obj_raw, probe_raw, positions_px, props, targets, mask, mean_intensity, upsample_factor,
+                num_iters, batch_size, rng, lr_obj=5e-3, lr_probe=1e-3, orthogonalize=True,
+                loss_type="l2_amplitude"):
+    """Adam iterations of Ptychography.reconstruct (ptychography.py:208-245) on
+    the given state; batches from a numpy generator like SimpleBatcher.
+    Returns (obj, probe, per-iteration mean batch losses)."""
+    obj = obj_raw.copy()
+    probe = probe_raw.copy()
+    so, sp = AdamState(), AdamState()
+    npos = positions_px.shape[0]
+    losses = []
+    for _ in range(num_iters):
+        tot, nb = 0.0, 0
+        for bi in batch_order(rng, npos, batch_size):
+            loss, g_obj, g_probe, _ = full_gradients(obj, probe, positions_px[bi], props, targets[bi], mask, npos,
+                                                     mean_intensity, upsample_factor, orthogonalize, loss_type)
+            adam_step(obj, g_obj, so, lr_obj)
+            adam_step(probe, g_probe, sp, lr_probe)
+            tot += loss
+            nb += 1
+        losses.append(tot / nb)
+    return obj, probe, np.array(losses)

@@ -57,7 +57,7 @@ class BatchArgs(ctypes.Structure):
         ("obj", _vp), ("probe_hat", _vp), ("prop", _vp), ("positions", _vp), ("batch_idx", _vp),
         ("targets", _vp), ("mask", _vp), ("grad_obj", _vp), ("probe_grad_part", _vp),
         ("scratch", _vp), ("loss_part", _vp), ("out_intensity", _vp), ("out_exit", _vp),
-        ("out_waves", _vp), ("status", _vp),
+        ("out_waves", _vp), ("status", _vp), ("prop_r", _vp), ("prop_c", _vp),
         ("n", _int), ("S", _int), ("P", _int), ("B", _int), ("Ho", _int), ("Wo", _int),
         ("npos", _int), ("grid", _int), ("loss_type", _int),
         ("loss_scale", _flt), ("inv_mean_intensity", _flt),

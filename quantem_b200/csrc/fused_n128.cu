@@ -11,6 +11,8 @@ int launch_batch(const ptycho_batch_args* a, bool adj, cudaStream_t st) {
   p.obj = static_cast<const float2*>(a->obj);
   p.probe_hat = static_cast<const float2*>(a->probe_hat);
   p.prop = static_cast<const float2*>(a->prop);
+  p.prop_r = static_cast<const float2*>(a->prop_r);
+  p.prop_c = static_cast<const float2*>(a->prop_c);
   p.positions = a->positions;
   p.batch_idx = a->batch_idx;
   p.targets = a->targets;
@@ -32,7 +34,7 @@ int launch_batch(const ptycho_batch_args* a, bool adj, cudaStream_t st) {
   p.loss_scale = a->loss_scale;
   p.inv_mean_intensity = a->inv_mean_intensity;
   p.loss_type = a->loss_type;
-  const size_t smem = qb::fused_smem_bytes<N>();
+  const size_t smem = a->prop_r ? qb::fused_smem_bytes_sep<N>(a->S) : qb::fused_smem_bytes<N>();
   // the attribute is per device; setting it on every launch keeps multi-device
   // processes correct and costs far less than one launch
   if (adj) {

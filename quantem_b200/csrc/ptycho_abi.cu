@@ -235,11 +235,20 @@ int validate_batch(const ptycho_batch_args* a, bool adj) {
   if (a->B > 0 && (a->grid < 1 || a->grid > 65535)) return fail(PTYCHO_ERR_INVALID, "bad grid %d", a->grid);
   if (!a->obj || !a->probe_hat || !a->positions || !a->batch_idx || !a->targets || !a->mask || !a->loss_part)
     return fail(PTYCHO_ERR_INVALID, "required pointer is NULL");
-  if (a->S > 1 && !a->prop) return fail(PTYCHO_ERR_INVALID, "prop is NULL with S > 1");
+  if (a->S > 1 && !a->prop && !(a->prop_r && a->prop_c))
+    return fail(PTYCHO_ERR_INVALID, "propagators are NULL with S > 1");
+  if ((a->prop_r == nullptr) != (a->prop_c == nullptr))
+    return fail(PTYCHO_ERR_INVALID, "prop_r and prop_c must be given together");
+  if (a->prop_r) {
+    const size_t need = (size_t)(a->n == 64 ? qb::fused_smem_bytes_sep<64>(a->S) : qb::fused_smem_bytes_sep<128>(a->S));
+    if (need + 1024 > 232448)
+      return fail(PTYCHO_ERR_UNSUPPORTED, "separable propagators of %d slices do not fit in shared memory; pass prop",
+                  a->S);
+  }
   if (adj && (!a->grad_obj || !a->probe_grad_part || !a->scratch))
     return fail(PTYCHO_ERR_INVALID, "adjoint buffers are NULL");
   const void* ptrs[] = {a->obj, a->probe_hat, a->prop, a->grad_obj, a->probe_grad_part, a->scratch, a->out_exit,
-                        a->out_waves};
+                        a->out_waves, a->prop_r, a->prop_c};
   for (const void* q : ptrs)
     if (q && !aligned(q, 8)) return fail(PTYCHO_ERR_INVALID, "complex buffer not 8-byte aligned");
   if (a->loss_type < 0 || a->loss_type > 4) return fail(PTYCHO_ERR_INVALID, "bad loss type %d", a->loss_type);

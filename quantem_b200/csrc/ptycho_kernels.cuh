@@ -39,7 +39,9 @@ enum LossType : int {
 struct BatchParams {
   const float2* obj;          // constrained object (S, Ho, Wo)
   const float2* probe_hat;    // fft2 of the orthogonalised probes (P, N, N)
-  const float2* prop;         // propagators (S-1, N, N)
+  const float2* prop;         // propagators (S-1, N, N), used when prop_r is null
+  const float2* prop_r;       // separable propagator row factors (S-1, N) or null
+  const float2* prop_c;       // separable propagator column factors (S-1, N)
   const float* positions;     // (npos, 2) scan positions [px]
   const int64_t* batch_idx;   // (B,) indices into positions / targets
   const float* targets;       // (npos, N, N) detector (centred) layout
@@ -64,11 +66,16 @@ __device__ __forceinline__ int wrap_index(int x, int n) {
   return x < 0 ? x + n : x;
 }
 
-// shared-memory bytes used by fused_batch_kernel<N, *>
+// shared-memory bytes used by fused_batch_kernel<N, *> (without the separable
+// propagator factors, which add 2 * N * (S-1) float2 when used)
 template <int N>
 constexpr size_t fused_smem_bytes() {
   return sizeof(float2) * (size_t)(Fft2<N>::SM_FLOAT2 + 3 * N) + sizeof(float) * (size_t)N * N +
          sizeof(int) * (size_t)(2 * N);
+}
+template <int N>
+constexpr size_t fused_smem_bytes_sep(int S) {
+  return fused_smem_bytes<N>() + sizeof(float2) * (size_t)2 * N * (size_t)(S > 1 ? S - 1 : 0);
 }
 
 template <int N>
@@ -111,6 +118,34 @@ __device__ __forceinline__ void loss_elem(const BatchParams& p, float I, float t
   }
 }
 
+// x (S3 layout, Fourier space) *= K_s (CONJ: conj(K_s)), separable factors from
+// shared memory or the full (S-1, N, N) array from global memory.
+template <int N, bool CONJ>
+__device__ __forceinline__ void apply_prop(const Fft2<N>& f, float2 (&x)[Fft2<N>::E], const BatchParams& p, int s,
+                                           bool sep, const float2* sKr, const float2* sKc) {
+  constexpr int D = Fft2<N>::D, G3 = Fft2<N>::G3;
+  if (sep) {
+#pragma unroll
+    for (int g = 0; g < G3; ++g) {
+      const float2 kc = sKc[s * N + f.s3_c];
+#pragma unroll
+      for (int e = 0; e < D; ++e) {
+        const float2 k = cmul(sKr[s * N + f.s3_row(g, e)], kc);
+        x[g * D + e] = CONJ ? cmulc(x[g * D + e], k) : cmul(x[g * D + e], k);
+      }
+    }
+  } else {
+    const float2* pr = p.prop + (size_t)s * N * N;
+#pragma unroll
+    for (int g = 0; g < G3; ++g)
+#pragma unroll
+      for (int e = 0; e < D; ++e) {
+        const float2 k = __ldg(pr + (size_t)f.s3_row(g, e) * N + f.s3_c);
+        x[g * D + e] = CONJ ? cmulc(x[g * D + e], k) : cmul(x[g * D + e], k);
+      }
+  }
+}
+
 template <int N, bool ADJ>
 __global__ void __launch_bounds__(4 * N, 1) fused_batch_kernel(const BatchParams p) {
   using F = Fft2<N>;
@@ -123,6 +158,11 @@ __global__ void __launch_bounds__(4 * N, 1) fused_batch_kernel(const BatchParams
   float* inten = reinterpret_cast<float*>(colf + N);
   int* rowmap = reinterpret_cast<int*>(inten + N * N);
   int* colmap = rowmap + N;
+  // separable propagators K_s[kr][kc] = Kr_s[kr] * Kc_s[kc] (probe_models.py:376-427
+  // builds exp(-i pi lambda dz (kr^2 + kc^2)) times per-axis tilt ramps)
+  float2* sKr = reinterpret_cast<float2*>(colmap + N);
+  float2* sKc = sKr + (size_t)N * (p.S > 1 ? p.S - 1 : 0);
+  const bool sep = p.prop_r != nullptr;
   __shared__ double red[32];
 
   const int tid = threadIdx.x;
@@ -132,6 +172,12 @@ __global__ void __launch_bounds__(4 * N, 1) fused_batch_kernel(const BatchParams
     double s, c;
     sincospi(-2.0 * (double)k / (double)N, &s, &c);
     tw[k] = make_float2((float)c, (float)s);
+  }
+  if (sep) {
+    for (int k = tid; k < (p.S - 1) * N; k += T) {
+      sKr[k] = p.prop_r[k];
+      sKc[k] = p.prop_c[k];
+    }
   }
   const float inv_n = 1.0f / (float)N;
   const float inv_n2 = inv_n * inv_n;
@@ -214,12 +260,7 @@ __global__ void __launch_bounds__(4 * N, 1) fused_batch_kernel(const BatchParams
         for (int e = 0; e < E; ++e) x[e] = cmul(x[e], __ldg(orow_ptr + colmap[f.s1_col(e)]));
         if (s < S - 1) {
           f.forward(x, sm, tw);
-          const float2* pr = p.prop + (size_t)s * NN;
-#pragma unroll
-          for (int g = 0; g < G3; ++g)
-#pragma unroll
-            for (int e = 0; e < D; ++e)
-              x[g * D + e] = cmul(x[g * D + e], __ldg(pr + (size_t)f.s3_row(g, e) * N + f.s3_c));
+          apply_prop<N, false>(f, x, p, s, sep, sKr, sKc);
           f.inverse(x, sm, tw);
 #pragma unroll
           for (int e = 0; e < E; ++e) x[e] = cscale(x[e], inv_n2);
@@ -282,12 +323,7 @@ __global__ void __launch_bounds__(4 * N, 1) fused_batch_kernel(const BatchParams
           }
           if (s > 0) {
             f.forward(x, sm, tw);
-            const float2* pr = p.prop + (size_t)(s - 1) * NN;
-#pragma unroll
-            for (int g = 0; g < G3; ++g)
-#pragma unroll
-              for (int e = 0; e < D; ++e)
-                x[g * D + e] = cmulc(x[g * D + e], __ldg(pr + (size_t)f.s3_row(g, e) * N + f.s3_c));
+            apply_prop<N, true>(f, x, p, s - 1, sep, sKr, sKc);
             f.inverse(x, sm, tw);
 #pragma unroll
             for (int e = 0; e < E; ++e) x[e] = cscale(x[e], inv_n2);

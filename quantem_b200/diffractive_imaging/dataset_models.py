@@ -1,0 +1,471 @@
+"""Raster-scan ptychography dataset model (host-side set-up + per-batch positions).
+
+Mirrors quantem.diffractive_imaging.dataset_models.PtychographyDatasetRaster of
+the reference: CoM fitting (dataset_models.py:1027-1112, ptycho_utils.py:352-415),
+relative rotation (1114-1370), diffraction normalisation to corner-centred target
+amplitudes (1372-1480), raster scan positions (883-944), hard constraints on the
+positions (597-613) and the per-batch ``forward`` (1482-1499).  Set-up runs on
+the host (numpy / torch on the CPU); the batch kernels compute patch indices from
+the positions on the GPU, and ``patch_indices`` is built only on request.
+"""
+from __future__ import annotations
+
+from typing import Literal
+
+import numpy as np
+import torch
+from scipy.optimize import curve_fit
+
+from ..core import config
+from ..core.datasets import Dataset4dstem
+from ..core.optim import OptimizerMixin
+from .complex_probe import electron_wavelength_angstrom
+
+
+def _plane(xy, mx, my, b):
+    return mx * xy[0] + my * xy[1] + b
+
+
+def _parabola(xy, c0, cx1, cx2, cy1, cy2, cxy):
+    return c0 + cx1 * xy[0] + cy1 * xy[1] + cx2 * xy[0] ** 2 + cy2 * xy[1] ** 2 + cxy * xy[0] * xy[1]
+
+
+def fit_origin(data, mask=None, fit_function="plane"):
+    """Fit of the diffraction origin over the scan (ptycho_utils.py:352-415)."""
+    qr0, qc0 = data
+    if fit_function == "constant":
+        fr = np.mean(qr0) * np.ones_like(qr0)
+        fc = np.mean(qc0) * np.ones_like(qc0)
+        return fr, fc, qr0 - fr, qc0 - fc
+    f = {"plane": _plane, "parabola": _parabola}.get(fit_function)
+    if f is None:
+        raise ValueError("fit_function must be one of 'plane', 'parabola', 'constant'")
+    shape = qr0.shape
+    r, c = np.indices(shape)
+    rc = np.vstack((r.reshape(1, -1), c.reshape(1, -1)))
+    if mask is not None:
+        m1 = mask.reshape(1, -1)
+        rcm = np.vstack((r.reshape(1, -1) * m1, c.reshape(1, -1) * m1))
+        pr, _ = curve_fit(f, rcm, qr0[mask])
+        pc, _ = curve_fit(f, rcm, qc0[mask])
+    else:
+        pr, _ = curve_fit(f, rc, qr0.ravel())
+        pc, _ = curve_fit(f, rc, qc0.ravel())
+    fr = f(rc, *pr).reshape(shape)
+    fc = f(rc, *pc).reshape(shape)
+    return fr, fc, qr0 - fr, qc0 - fc
+
+
+def fourier_shift_real(ar: np.ndarray, rshift, cshift) -> np.ndarray:
+    """Periodic sub-pixel Fourier shift of real images (ptycho_utils.py:239-300, non-bilinear).
+
+    Works on (..., nr, nc) stacks with per-image shifts of shape (...)."""
+    nr, nc = ar.shape[-2:]
+    qr = np.fft.fftfreq(nr, 1)[:, None]
+    qc = np.fft.fftfreq(nc, 1)[None, :]
+    rs = np.asarray(rshift)[..., None, None]
+    cs = np.asarray(cshift)[..., None, None]
+    p = np.exp(-(2j * np.pi) * ((cs * qc) + (rs * qr)))
+    return np.real(np.fft.ifft2(np.fft.fft2(ar) * p))
+
+
+class PtychographyDatasetRaster(OptimizerMixin):
+    """4D-STEM raster dataset: targets, scan positions and their constraints."""
+
+    _token = object()
+    DEFAULT_CONSTRAINTS = {
+        "descan_tv_weight": 0.0,
+        "descan_shifts_constant": False,
+        "center_scan_positions": False,
+        "clip_scan_positions": True,
+    }
+
+    def __init__(self, dset: Dataset4dstem, detector_mask=None, verbose=1, learn_descan=True,
+                 learn_scan_positions=True, _token=None):
+        if _token is not self._token:
+            raise RuntimeError("Use PtychographyDatasetRaster.from_* to instantiate this class.")
+        OptimizerMixin.__init__(self)
+        if dset.units[-1] not in ("A^-1", "mrad"):
+            raise ValueError(f"Expected diffraction units to be 'A^-1', got {dset.units[-1]}")
+        self.scan_sampling = np.asarray(dset.sampling[:2], dtype=float)
+        self.scan_units = list(dset.units[:2])
+        self.gpts = np.asarray(dset.shape[:2], dtype=int)
+        self.intensities_4d = np.asarray(dset.array).copy()
+        shp = self.intensities_4d.shape
+        self._array3d = self.intensities_4d.reshape(shp[0] * shp[1], shp[2], shp[3])
+        self.detector_sampling = np.asarray(dset.sampling[-2:], dtype=float)
+        self.detector_units = list(dset.units[-2:])
+        self.verbose = verbose
+        self.learn_descan = bool(learn_descan)
+        self.learn_scan_positions = bool(learn_scan_positions)
+        self._preprocessed = False
+        self._preprocessing_params = {}
+        self.com_rotation_rad = 0.0
+        self.com_transpose = False
+        self._probe_energy = None
+        self._device = "cpu"
+        dt = getattr(torch, config.get("dtype_real"))
+        self._scan_positions_px = torch.zeros((self.num_gpts, 2), dtype=dt)
+        self._initial_scan_positions_px = torch.zeros((self.num_gpts, 2), dtype=dt)
+        self._descan_shifts = torch.zeros((self.num_gpts, 2), dtype=dt)
+        self._initial_descan_shifts = torch.zeros((self.num_gpts, 2), dtype=dt)
+        self.detector_mask = detector_mask
+        self._constraints = dict(self.DEFAULT_CONSTRAINTS)
+        self._targets = None
+        self._patch_indices = None
+        self._last_patch_positions_px = None
+
+    @classmethod
+    def from_dataset4dstem(cls, dset: Dataset4dstem, detector_mask=None, verbose=1, learn_descan=True,
+                           learn_scan_positions=True):
+        return cls(dset, detector_mask, verbose, learn_descan, learn_scan_positions, _token=cls._token)
+
+    # ------------------------------------------------------------------ props
+    @property
+    def num_gpts(self) -> int:
+        return int(self._array3d.shape[0])
+
+    @property
+    def roi_shape(self) -> np.ndarray:
+        return np.array(self._array3d.shape[-2:])
+
+    @property
+    def device(self):
+        return self._device
+
+    @property
+    def preprocessed(self) -> bool:
+        return self._preprocessed
+
+    @property
+    def probe_energy(self):
+        return self._probe_energy
+
+    @probe_energy.setter
+    def probe_energy(self, e):
+        self._probe_energy = None if e is None else float(e)
+
+    @property
+    def reciprocal_sampling(self) -> np.ndarray:
+        units = self.detector_units
+        s = self.detector_sampling
+        if units[0] == "A^-1":
+            return s
+        if units[0] == "mrad":
+            if self.probe_energy is None:
+                raise ValueError("dset Q units given in mrad but no probe energy defined")
+            return s / electron_wavelength_angstrom(self.probe_energy) / 1e3
+        raise ValueError(f"Unknown dset Q units: {units}")
+
+    @property
+    def obj_sampling(self) -> np.ndarray:
+        return 1 / (self.roi_shape * self.reciprocal_sampling)
+
+    @property
+    def fov(self) -> np.ndarray:
+        return self.scan_sampling * (self.gpts - 1)
+
+    @property
+    def _obj_shape_crop_2d(self) -> np.ndarray:
+        shp = np.floor(self.fov / self.obj_sampling)
+        shp += shp % 2
+        return shp.astype("int")
+
+    @property
+    def upsample_factor(self) -> float:
+        return float((self._obj_shape_crop_2d / self.gpts).mean())
+
+    @property
+    def _obj_shape_rot_2d(self) -> np.ndarray:
+        c = self._obj_shape_crop_2d.copy()
+        a = self.com_rotation_rad
+        rot = np.floor([abs(c[-1] * np.sin(a)) + abs(c[-2] * np.cos(a)),
+                        abs(c[-2] * np.sin(a)) + abs(c[-1] * np.cos(a))])
+        rot += rot % 2
+        return rot.astype("int")
+
+    def _obj_shape_full_2d(self, obj_padding_px) -> np.ndarray:
+        return (self._obj_shape_rot_2d + 2 * np.array(obj_padding_px)).astype("int")
+
+    @property
+    def detector_mask(self) -> torch.Tensor:
+        return self._detector_mask
+
+    @detector_mask.setter
+    def detector_mask(self, mask):
+        dt = getattr(torch, config.get("dtype_real"))
+        if mask is None:
+            mask = torch.ones(*[int(x) for x in self.roi_shape], dtype=dt)
+        else:
+            mask = torch.as_tensor(np.asarray(mask) if not isinstance(mask, torch.Tensor) else mask, dtype=dt)
+            if tuple(mask.shape) != tuple(self.roi_shape):
+                raise ValueError(f"detector_mask must have shape {tuple(self.roi_shape)}")
+        self._detector_mask = mask.to(self._device)
+
+    @property
+    def scan_positions_px(self) -> torch.Tensor:
+        return self._scan_positions_px
+
+    @scan_positions_px.setter
+    def scan_positions_px(self, positions):
+        t = torch.as_tensor(positions.detach().cpu().numpy() if isinstance(positions, torch.Tensor)
+                            else np.asarray(positions), dtype=getattr(torch, config.get("dtype_real")))
+        if tuple(t.shape) != (self.num_gpts, 2):
+            raise ValueError(f"scan_positions_px must have shape {(self.num_gpts, 2)}")
+        self._scan_positions_px = t.to(self._device).contiguous()
+
+    @property
+    def initial_scan_positions_px(self) -> torch.Tensor:
+        return self._initial_scan_positions_px
+
+    @property
+    def descan_shifts(self) -> torch.Tensor:
+        return self._descan_shifts
+
+    @property
+    def positions_px_fractional(self) -> torch.Tensor:
+        return self.scan_positions_px - torch.round(self.scan_positions_px)
+
+    @property
+    def targets(self) -> torch.Tensor:
+        if not self._preprocessed:
+            raise ValueError("dset must be preprocessed before targets can be accessed")
+        return self._targets
+
+    @property
+    def constraints(self) -> dict:
+        return self._constraints
+
+    def add_constraint(self, key, value):
+        if key not in self.DEFAULT_CONSTRAINTS:
+            raise KeyError(f"Unknown dataset constraint {key!r}")
+        self._constraints[key] = value
+
+    def get_optimization_parameters(self):
+        raise NotImplementedError("learning scan positions / descan is not part of the B200 path")
+
+    def reset_iter_constraint_losses(self):
+        pass
+
+    def reset(self):
+        self._scan_positions_px = self._initial_scan_positions_px.clone().to(self._device)
+
+    def to(self, device):
+        dev, _ = config.validate_device(device)
+        self._device = dev
+        for name in ("_scan_positions_px", "_initial_scan_positions_px", "_descan_shifts", "_detector_mask",
+                     "_targets", "_centered_amplitudes", "_amplitudes", "_centered_intensities", "_intensities"):
+            v = getattr(self, name, None)
+            if isinstance(v, torch.Tensor):
+                setattr(self, name, v.to(dev))
+        return self
+
+    # ---------------------------------------------------------- preprocessing
+    def preprocess(self, com_fit_function: Literal["none", "plane", "parabola", "constant", "no_shift"] = "plane",
+                   force_com_rotation: float | None = None, force_com_transpose: bool | None = None,
+                   bilinear: bool = False, padded_diffraction_intensities_shape=None, obj_padding_px=(0, 0),
+                   plot_rotation: bool = True, plot_com: str | bool = True, vectorized: bool = True,
+                   probe_energy: float | None = None):
+        """dataset_models.py:946-1025 (plots are not produced)."""
+        if padded_diffraction_intensities_shape is not None:
+            raise NotImplementedError("padded diffraction intensities are not part of the B200 path")
+        if bilinear:
+            raise NotImplementedError("bilinear centring is not part of the B200 path")
+        self._preprocessing_params = dict(com_fit_function=com_fit_function, force_com_rotation=force_com_rotation,
+                                          force_com_transpose=force_com_transpose, obj_padding_px=obj_padding_px)
+        if probe_energy is not None:
+            self.probe_energy = probe_energy
+        self._set_intensities_com(self.intensities_4d, com_fit_function)
+        self._set_com_relative_rotation(force_com_rotation, force_com_transpose)
+        self._normalize_diffraction_intensities()
+        self._set_initial_scan_positions_px(obj_padding_px)
+        self._set_patch_indices(obj_padding_px)
+        self._set_targets("l2_amplitude")
+        self._preprocessed = True
+
+    def _set_intensities_com(self, intensities, fit_function):
+        """Vectorised centre of mass (dataset_models.py:1027-1112)."""
+        dt = config.get("dtype_real")
+        kr = np.arange(intensities.shape[-2])
+        kc = np.arange(intensities.shape[-1])
+        krm, kcm = np.meshgrid(kr, kc, indexing="ij")
+        im = intensities.astype(dt)
+        com_r = np.sum(im * krm[None, None], axis=(-2, -1))
+        com_c = np.sum(im * kcm[None, None], axis=(-2, -1))
+        tot = np.sum(im, axis=(-2, -1))
+        com_r /= tot
+        com_c /= tot
+        if fit_function == "none":
+            fr, fc = com_r, com_c
+        elif fit_function == "no_shift":
+            fr = np.ones_like(com_r) * self.roi_shape[0] / 2
+            fc = np.ones_like(com_c) * self.roi_shape[1] / 2
+        else:
+            fr, fc, _, _ = fit_origin((com_r, com_c), mask=np.isfinite(com_r), fit_function=fit_function)
+        self.com_measured = np.array((com_r, com_c))
+        self.com_fit = np.array((fr, fc))
+
+    @property
+    def com_normalized(self) -> np.ndarray:
+        return np.nan_to_num(self.com_measured - self.com_fit) * self.reciprocal_sampling[:, None, None]
+
+    def _set_com_relative_rotation(self, force_com_rotation=None, force_com_transpose=None,
+                                   rotation_angles_deg=None):
+        """Curl-minimising rotation search (dataset_models.py:1114-1370)."""
+
+        def curl_for(angles, com, transpose):
+            a = angles[:, None, None]
+            cr, cc = com[0][None], com[1][None]
+            if transpose:
+                rr = np.cos(a) * cc - np.sin(a) * cr
+                rc = np.sin(a) * cc + np.cos(a) * cr
+            else:
+                rr = np.cos(a) * cr - np.sin(a) * cc
+                rc = np.sin(a) * cr + np.cos(a) * cc
+            g1 = rr[:, 1:-1, 2:] - rr[:, 1:-1, :-2]
+            g2 = rc[:, 2:, 1:-1] - rc[:, :-2, 1:-1]
+            return np.mean(np.abs(g2 - g1), axis=(-2, -1))
+
+        if rotation_angles_deg is None:
+            rotation_angles_deg = np.arange(-89.0, 90.0, 1.0)
+        ang = np.deg2rad(np.asarray(rotation_angles_deg))
+        if force_com_rotation is not None:
+            best = np.deg2rad(force_com_rotation)
+            if force_com_transpose is not None:
+                transpose = bool(force_com_transpose)
+            else:
+                c0 = curl_for(np.array([best]), self.com_normalized, False)[0]
+                c1 = curl_for(np.array([best]), self.com_normalized, True)[0]
+                transpose = bool(c1 < c0)
+        elif force_com_transpose is not None:
+            transpose = bool(force_com_transpose)
+            best = ang[int(np.argmin(curl_for(ang, self.com_normalized, transpose)))]
+        else:
+            c0 = curl_for(ang, self.com_normalized, False)
+            c1 = curl_for(ang, self.com_normalized, True)
+            i0, i1 = int(np.argmin(c0)), int(np.argmin(c1))
+            if c0[i0] <= c1[i1]:
+                best, transpose = ang[i0], False
+            else:
+                best, transpose = ang[i1], True
+        self.com_rotation_rad = float(best)
+        self.com_transpose = bool(transpose)
+
+    def _normalize_diffraction_intensities(self):
+        """Centred target amplitudes (dataset_models.py:1372-1480), vectorised over
+        positions: amplitude = sqrt(max(I,0)) Fourier-shifted by -CoM_fit,
+        clipped at 0 and fftshifted."""
+        dt = config.get("dtype_real")
+        di = self.intensities_4d.astype(dt)
+        inten = np.maximum(di, 0)
+        amp = np.maximum(np.sqrt(inten), 0)
+        mean_intensity = float(np.sum(np.sum(inten, axis=(-2, -1), dtype=np.float64)))
+        cr = -(self.com_fit[0] + 0.0)
+        cc = -(self.com_fit[1] + 0.0)
+        nr, nc = amp.shape[:2]
+        centered = np.empty_like(amp)
+        centered_i = np.empty_like(amp)
+        chunk = max(1, 2048 // max(1, nc))
+        for r0 in range(0, nr, chunk):
+            sh = fourier_shift_real(amp[r0:r0 + chunk].astype(np.float64), cr[r0:r0 + chunk], cc[r0:r0 + chunk])
+            sh = np.fft.fftshift(np.maximum(sh, 0), axes=(-2, -1))
+            centered[r0:r0 + chunk] = sh.astype(dt)
+            centered_i[r0:r0 + chunk] = (sh**2).astype(dt)
+        npos = nr * nc
+        roi = tuple(int(x) for x in self.roi_shape)
+        self._amplitudes = torch.as_tensor(amp.reshape(-1, *roi))
+        self._centered_amplitudes = torch.as_tensor(centered.reshape(-1, *roi))
+        self._intensities = torch.as_tensor(inten.reshape(-1, *roi))
+        self._centered_intensities = torch.as_tensor(centered_i.reshape(-1, *roi))
+        self.mean_diffraction_intensity = mean_intensity / npos
+        descan = -1 * self.com_fit.reshape((2, -1)) + self.roi_shape[:, None] / 2
+        self._descan_shifts = torch.as_tensor(descan.T.astype(dt))
+        self._initial_descan_shifts = self._descan_shifts.clone()
+
+    @property
+    def centered_amplitudes(self) -> torch.Tensor:
+        return self._centered_amplitudes
+
+    @property
+    def amplitudes(self) -> torch.Tensor:
+        return self._amplitudes
+
+    def _set_initial_scan_positions_px(self, obj_padding_px):
+        """Raster positions in object pixels (dataset_models.py:883-944)."""
+        if obj_padding_px is None:
+            obj_padding_px = np.array([0, 0])
+        nr, nc = self.gpts
+        sr, sc = self.scan_sampling
+        r, c = np.meshgrid(np.arange(nr) * sr, np.arange(nc) * sc, indexing="ij")
+        pos = np.stack((r.ravel(), c.ravel()), axis=-1).astype(config.get("dtype_real"))
+        if self.com_rotation_rad != 0:
+            # AffineTransform(angle)(x, origin) = (x - origin) @ R + origin (ptycho_utils.py:510-567)
+            a = self.com_rotation_rad
+            origin = np.asarray(pos.mean(0), dtype=np.float32)
+            rot = np.array([[np.cos(a), -np.sin(a)], [np.sin(a), np.cos(a)]], dtype=np.float32)
+            pos = ((pos - origin) @ rot + origin).astype(pos.dtype)
+        sampling = self.obj_sampling
+        if self.com_transpose:
+            pos = np.flip(pos, axis=1)
+            sampling = sampling[::-1]
+        m = np.min(pos, axis=0).clip(-np.inf, 0)
+        pos -= m
+        pos[:, 0] /= sampling[0]
+        pos[:, 1] /= sampling[1]
+        pos[:, 0] += obj_padding_px[0]
+        pos[:, 1] += obj_padding_px[1]
+        self.scan_positions_px = pos
+        self._initial_scan_positions_px = self._scan_positions_px.clone()
+
+    def _set_patch_indices(self, obj_padding_px):
+        """Remember the rounded positions the patch windows correspond to
+        (dataset_models.py:514-539); the windows themselves are formed inside the
+        batch kernels, and ``patch_indices`` builds them only when read."""
+        self._patch_obj_shape = self._obj_shape_full_2d(obj_padding_px)
+        self._last_patch_positions_px = self.scan_positions_px.clone()
+        self._patch_indices = None
+
+    @property
+    def patch_indices(self) -> torch.Tensor:
+        if self._patch_indices is None:
+            shp = self._patch_obj_shape
+            r0 = torch.round(self._last_patch_positions_px[:, 0]).to(torch.int32)
+            c0 = torch.round(self._last_patch_positions_px[:, 1]).to(torch.int32)
+            x = torch.fft.fftfreq(int(self.roi_shape[0]), d=1 / int(self.roi_shape[0])).to(r0.device)
+            y = torch.fft.fftfreq(int(self.roi_shape[1]), d=1 / int(self.roi_shape[1])).to(r0.device)
+            row = (r0[:, None, None] + x[None, :, None]) % int(shp[-2])
+            col = (c0[:, None, None] + y[None, None, :]) % int(shp[-1])
+            self._patch_indices = (row * int(shp[-1]) + col).to(torch.int32)
+        return self._patch_indices
+
+    def _set_targets(self, loss_type):
+        """dataset_models.py:225-242 (descan is not learned on this path)."""
+        if "amplitude" in loss_type:
+            t = self._centered_amplitudes
+        elif "intensity" in loss_type or loss_type == "poisson":
+            t = self._centered_intensities
+        else:
+            raise ValueError(f"Unknown loss type {loss_type}")
+        self._targets = t.clone().to(self._device).contiguous()
+
+    # --------------------------------------------------------- per batch
+    def apply_hard_constraints(self, obj_padding_px):
+        """Position clipping / centring (dataset_models.py:597-613)."""
+        pos = self.scan_positions_px
+        shp = torch.tensor(self._obj_shape_full_2d(obj_padding_px), device=pos.device, dtype=pos.dtype)
+        if self._constraints.get("clip_scan_positions", True):
+            pos = torch.minimum(torch.maximum(pos, torch.zeros_like(shp)), shp - 1)
+        if self._constraints.get("center_scan_positions", False):
+            pos = pos - pos.mean(dim=0, keepdim=True) + shp / 2
+        self._scan_positions_px = pos.contiguous()
+
+    def forward(self, batch_indices, obj_padding_px):
+        """(patch_indices, positions_px, positions_px_fractional, None) of a batch."""
+        self.apply_hard_constraints(obj_padding_px)
+        bi = torch.as_tensor(np.asarray(batch_indices), device=self.scan_positions_px.device)
+        positions = self.scan_positions_px[bi]
+        frac = positions - torch.round(positions)
+        if not torch.equal(torch.round(self._last_patch_positions_px.to(positions.device)),
+                           torch.round(self.scan_positions_px)):
+            self._set_patch_indices(obj_padding_px)
+        return self.patch_indices.to(positions.device)[bi], positions, frac, None

@@ -1,0 +1,578 @@
+"""Ptychography engine: drop-in for quantem.diffractive_imaging.Ptychography.
+
+Same construction and call sequence as the reference (ptychography.py:36-58,
+ptychography_base.py:135-189, ptychography.py:146-308): ``from_models`` ->
+``preprocess`` -> ``reconstruct``.  Each batch runs one fused forward + loss +
+adjoint CUDA launch (quantem_b200.ops) followed by the fused optimiser kernels;
+the batch loss stays on the device and every iteration reads the loss back once
+(the reference reads it twice per batch).
+"""
+from __future__ import annotations
+
+from typing import Literal
+
+import numpy as np
+import scipy.ndimage as ndi
+import torch
+
+from ..core import config
+from .. import ops
+from .dataset_models import PtychographyDatasetRaster
+from .detector_models import DetectorPixelated
+from .object_models import ObjectPixelated
+from .probe_models import ProbePixelated
+from .ptycho_utils import SimpleBatcher
+
+
+def adjust_padding_power2(pad, shape, power2_level):
+    """Pad so that (shape + 2 pad) is divisible by 2**power2_level (ptychography_base.py:1002-1016)."""
+    div = 2**power2_level
+    pad = np.array(pad, dtype=np.int64)
+    r0 = (shape[-2] + 2 * pad[-2]) % div
+    r1 = (shape[-1] + 2 * pad[-1]) % div
+    if r0:
+        pad[-2] += (div - r0) // 2
+    if r1:
+        pad[-1] += (div - r1) // 2
+    if (shape[-2] + 2 * pad[-2]) % div or (shape[-1] + 2 * pad[-1]) % div:
+        raise ValueError(f"Adjustment failed to achieve divisibility by {div}")
+    return pad
+
+
+class Ptychography:
+    """Multislice mixed-probe gradient-descent ptychography on B200."""
+
+    _token = object()
+    OPTIMIZABLE_VALS = ["object", "probe", "dataset"]
+    DEFAULT_OPTIMIZER_TYPE = "adam"
+
+    def __init__(self, dset, obj_model, probe_model, detector_model, logger=None, device="cpu", verbose=True,
+                 rng=None, _token=None):
+        if _token is not self._token:
+            raise RuntimeError("Use Ptychography.from_models() to instantiate this class.")
+        if not isinstance(dset, PtychographyDatasetRaster):
+            raise TypeError(f"dset should be a PtychographyDatasetRaster, got {type(dset)}")
+        if not isinstance(obj_model, ObjectPixelated):
+            raise TypeError(f"obj_model must be ObjectPixelated, got {type(obj_model)}")
+        if not isinstance(probe_model, ProbePixelated):
+            raise TypeError(f"probe_model must be ProbePixelated, got {type(probe_model)}")
+        if not isinstance(detector_model, DetectorPixelated):
+            raise TypeError(f"detector_model must be DetectorPixelated, got {type(detector_model)}")
+        self.verbose = verbose
+        self.dset = dset
+        self._device = config.validate_device(device)[0]
+        self.rng = rng
+        self._preprocessed = False
+        self._obj_padding_force_power2_level = 3
+        self._store_snapshots = False
+        self._store_snapshot_every = 1
+        self._iter_losses: list[float] = []
+        self._iter_val_losses: list[float] = []
+        self._iter_lrs: dict[str, list] = {}
+        self._snapshots: list[dict] = []
+        self._obj_padding_px = np.array([0, 0])
+        self.batch_size = dset.num_gpts
+        self._val_ratio = 0.0
+        self._val_mode = "grid"
+        self._probe_model = probe_model
+        if dset.preprocessed:
+            probe_model.set_initial_probe(self.roi_shape, self.reciprocal_sampling, dset.mean_diffraction_intensity,
+                                          device=self._device)
+        self._obj_model = obj_model
+        self.detector_model = detector_model
+        self.logger = logger
+        self._propagators = torch.tensor([])
+        self._prop_factors = None
+        self.to(self._device)
+
+    @classmethod
+    def from_models(cls, dset, obj_model, probe_model, detector_model, logger=None, device="cpu", verbose=True,
+                    rng=None):
+        return cls(dset, obj_model, probe_model, detector_model, logger, device, verbose, rng, _token=cls._token)
+
+    # ------------------------------------------------------------ basic state
+    @property
+    def rng(self) -> np.random.Generator:
+        return self._rng
+
+    @rng.setter
+    def rng(self, rng):
+        if rng is None:
+            self._rng_seed = None
+            rng = np.random.default_rng()
+        elif isinstance(rng, (int, float)):
+            self._rng_seed = int(rng)
+            rng = np.random.default_rng(rng)
+        elif isinstance(rng, np.random.Generator):
+            self._rng_seed = None
+        else:
+            raise TypeError(f"rng should be a np.random.Generator or a seed, got {type(rng)}")
+        self._rng = rng
+
+    def _reset_rng(self):
+        if self._rng_seed is not None:
+            self.rng = self._rng_seed
+
+    @property
+    def device(self) -> str:
+        return self._device
+
+    @property
+    def obj_model(self) -> ObjectPixelated:
+        return self._obj_model
+
+    @property
+    def probe_model(self) -> ProbePixelated:
+        return self._probe_model
+
+    @property
+    def roi_shape(self) -> np.ndarray:
+        return self.dset.roi_shape
+
+    @property
+    def gpts(self) -> np.ndarray:
+        return self.dset.gpts
+
+    @property
+    def reciprocal_sampling(self) -> np.ndarray:
+        return self.dset.reciprocal_sampling
+
+    @property
+    def sampling(self) -> np.ndarray:
+        return self.dset.obj_sampling
+
+    @property
+    def num_slices(self) -> int:
+        return self.obj_model.num_slices
+
+    @property
+    def num_probes(self) -> int:
+        return self.probe_model.num_probes
+
+    @property
+    def slice_thicknesses(self) -> np.ndarray:
+        t = self.obj_model.slice_thicknesses
+        return np.array([]) if t is None else t.cpu().numpy()
+
+    @property
+    def obj_padding_px(self) -> np.ndarray:
+        return self._obj_padding_px
+
+    @obj_padding_px.setter
+    def obj_padding_px(self, pad):
+        p2 = np.asarray(pad, dtype=np.int64).reshape(2)
+        if self._obj_padding_force_power2_level > 0:
+            p2 = adjust_padding_power2(p2, self.dset._obj_shape_full_2d((0, 0)), self._obj_padding_force_power2_level)
+        self._obj_padding_px = p2
+        self.obj_model._initialize_obj(shape=self.obj_shape_full, sampling=self.sampling)
+        self.obj_model.to(self._device)
+        self.dset._set_initial_scan_positions_px(self._obj_padding_px)
+        self.dset._set_patch_indices(self._obj_padding_px)
+
+    @property
+    def obj_shape_full(self) -> np.ndarray:
+        return np.concatenate([[self.num_slices], self.dset._obj_shape_full_2d(self.obj_padding_px)])
+
+    @property
+    def obj_shape_crop(self) -> np.ndarray:
+        shp = np.floor(self.dset.fov / self.sampling)
+        shp += shp % 2
+        return np.concatenate([[self.num_slices], shp]).astype("int")
+
+    @property
+    def batch_size(self) -> int:
+        return self._batch_size
+
+    @batch_size.setter
+    def batch_size(self, val):
+        if val is not None:
+            if int(val) <= 0:
+                raise ValueError("batch_size must be > 0")
+            self._batch_size = int(val)
+
+    @property
+    def val_ratio(self) -> float:
+        return float(self._val_ratio)
+
+    @val_ratio.setter
+    def val_ratio(self, r):
+        r = float(r)
+        if r < 0.0 or r > 1.0:
+            raise ValueError("val_ratio must satisfy 0 <= val_ratio <= 1")
+        self._val_ratio = r
+
+    @property
+    def val_mode(self):
+        return self._val_mode
+
+    @val_mode.setter
+    def val_mode(self, mode):
+        if mode not in ("grid", "random"):
+            raise ValueError(f"val_mode must be either 'grid' or 'random', got {mode}")
+        self._val_mode = mode
+
+    @property
+    def iter_losses(self) -> np.ndarray:
+        return np.array(self._iter_losses)
+
+    @property
+    def val_iter_losses(self) -> np.ndarray:
+        return np.array(self._iter_val_losses)
+
+    @property
+    def num_iters(self) -> int:
+        return len(self._iter_losses)
+
+    @property
+    def iter_lrs(self) -> dict:
+        return {k: np.array(v) for k, v in self._iter_lrs.items()}
+
+    @property
+    def snapshots(self):
+        return self._snapshots
+
+    @property
+    def propagators(self) -> torch.Tensor:
+        return torch.tensor([]) if self.num_slices == 1 else self._propagators
+
+    def to(self, device):
+        dev, _ = config.validate_device(device)
+        self._device = dev
+        self.obj_model.to(dev)
+        self.probe_model.to(dev)
+        self.dset.to(dev)
+        if isinstance(self._propagators, torch.Tensor):
+            self._propagators = self._propagators.to(dev)
+        if self._prop_factors is not None:
+            self._prop_factors = tuple(t.to(dev) for t in self._prop_factors)
+        return self
+
+    def vprint(self, m, level=1):
+        if self.verbose >= level:
+            print(m)
+
+    def _check_preprocessed(self):
+        if not self._preprocessed:
+            raise AttributeError("Preprocessing has not been completed. Please run Ptycho.preprocess()")
+
+    # ------------------------------------------------------------ set-up
+    def preprocess(self, obj_padding_px=(0, 0), val_ratio=0.0, val_mode="grid", vectorized=True, batch_size=None,
+                   com_fit_function="constant", force_com_rotation=None, force_com_transpose=None,
+                   padded_diffraction_intensities_shape=None, plot_rotation=True, plot_com=True,
+                   plot_probe_overlap=False):
+        """ptychography_base.py:135-189 (no plots)."""
+        if not self.dset.preprocessed:
+            self.vprint("Dataset was not preprocessed, proceeding with defaults.")
+            self.dset.preprocess(com_fit_function=com_fit_function, force_com_rotation=force_com_rotation,
+                                 force_com_transpose=force_com_transpose,
+                                 padded_diffraction_intensities_shape=padded_diffraction_intensities_shape,
+                                 obj_padding_px=obj_padding_px)
+            self.probe_model.set_initial_probe(self.roi_shape, self.reciprocal_sampling,
+                                               self.dset.mean_diffraction_intensity, device=self.device)
+        self.obj_padding_px = obj_padding_px
+        self.dset._set_initial_scan_positions_px(self.obj_padding_px)
+        self.dset._set_patch_indices(self.obj_padding_px)
+        self.compute_propagator_arrays()
+        self._preprocessed = True
+        self.val_ratio = float(val_ratio)
+        self.val_mode = val_mode
+        return self
+
+    def compute_propagator_arrays(self):
+        """Propagators like the reference (complex64, probe_models.py:376-427) plus
+        their per-axis factors for the batch kernels."""
+        if self.num_slices == 1:
+            self._propagators = torch.tensor([])
+            self._prop_factors = None
+            return
+        self._propagators = self.probe_model._compute_propagator_arrays(
+            self.sampling, self.num_slices, self.slice_thicknesses).to(self._device)
+        if torch.device(self._device).type == "cuda":
+            self._prop_factors = self.probe_model.separable_propagators(self.sampling, self.slice_thicknesses,
+                                                                        self._device)
+        else:
+            self._prop_factors = None
+
+    # ------------------------------------------------------------ optimisers
+    def _get_default_lr(self, key):
+        if key == "object":
+            return self.obj_model.DEFAULT_LRS.get("object", 5e-3)
+        if key == "probe":
+            return self.probe_model.DEFAULT_LRS.get("probe", 1e-3)
+        if key == "dataset":
+            return 1e-3
+        raise ValueError(f"Unknown optimization key: {key}")
+
+    @property
+    def optimizer_params(self) -> dict:
+        return {k: p for k, p in (("object", self.obj_model.optimizer_params),
+                                  ("probe", self.probe_model.optimizer_params),
+                                  ("dataset", self.dset.optimizer_params)) if p}
+
+    @optimizer_params.setter
+    def optimizer_params(self, d):
+        """ptychography_opt.py:183-228."""
+        if isinstance(d, (tuple, list)):
+            d = {k: {} for k in d}
+        for k, v in d.items():
+            v = dict(v)
+            v.setdefault("type", self.DEFAULT_OPTIMIZER_TYPE)
+            v.setdefault("lr", self._get_default_lr(k))
+            if k == "object":
+                self.obj_model.optimizer_params = v
+            elif k == "probe":
+                self.probe_model.optimizer_params = v
+            elif k == "dataset":
+                if v.get("type", "adam") != "none":
+                    raise NotImplementedError("learning scan positions / descan is not part of the B200 path")
+            else:
+                raise ValueError(f"key to be optimized, {k}, not in allowed keys: {self.OPTIMIZABLE_VALS}")
+
+    @property
+    def optimizers(self) -> dict:
+        out = {}
+        if self.obj_model.has_optimizer():
+            out["object"] = self.obj_model.optimizer
+        if self.probe_model.has_optimizer():
+            out["probe"] = self.probe_model.optimizer
+        return out
+
+    def set_optimizers(self):
+        for key, params in self.optimizer_params.items():
+            (self.obj_model if key == "object" else self.probe_model).set_optimizer(params)
+
+    @property
+    def scheduler_params(self) -> dict:
+        return {"object": self.obj_model.scheduler_params, "probe": self.probe_model.scheduler_params,
+                "dataset": self.dset.scheduler_params}
+
+    @scheduler_params.setter
+    def scheduler_params(self, d):
+        for k in self.OPTIMIZABLE_VALS:
+            d.setdefault(k, {})
+        for k, v in d.items():
+            if k == "object":
+                self.obj_model.scheduler_params = v
+            elif k == "probe":
+                self.probe_model.scheduler_params = v
+            elif k == "dataset":
+                self.dset.scheduler_params = v
+            else:
+                raise ValueError(f"key to be optimized, {k}, not in allowed keys: {self.OPTIMIZABLE_VALS}")
+
+    def set_schedulers(self, params, num_iter=None):
+        for key, sp in params.items():
+            if key == "object":
+                self.obj_model.set_scheduler(sp, num_iter)
+            elif key == "probe":
+                self.probe_model.set_scheduler(sp, num_iter)
+
+    def step_schedulers(self, loss=None):
+        self.obj_model.step_scheduler(loss)
+        self.probe_model.step_scheduler(loss)
+
+    @property
+    def constraints(self) -> dict:
+        return {"object": self.obj_model.constraints, "probe": self.probe_model.constraints,
+                "dataset": self.dset.constraints, "detector": {"detector_mask": None}}
+
+    @constraints.setter
+    def constraints(self, c: dict):
+        handlers = {"object": self.obj_model, "probe": self.probe_model, "dataset": self.dset}
+        for key, value in c.items():
+            if key in handlers and isinstance(value, dict):
+                for sk, sv in value.items():
+                    handlers[key].add_constraint(sk, sv)
+            elif key == "detector" and isinstance(value, dict):
+                pass
+            else:
+                raise KeyError(f"Invalid constraint category '{key}'. Valid categories are: "
+                               f"{list(handlers) + ['detector']}")
+
+    def reset_recon(self):
+        """ptychography_base.py:834-848 and ptychography.py:96-100."""
+        self._reset_rng()
+        self.obj_model.reset()
+        self.probe_model.reset()
+        self.dset.reset()
+        self.compute_propagator_arrays()
+        self.obj_model.constraints = self.obj_model.DEFAULT_CONSTRAINTS
+        self._iter_losses, self._iter_val_losses, self._iter_lrs, self._snapshots = [], [], {}, []
+        self.obj_model.reset_optimizer()
+        self.probe_model.reset_optimizer()
+
+    # ------------------------------------------------------------ forward model API
+    def _batch_tensors(self):
+        dev = torch.device(self._device)
+        if dev.type != "cuda":
+            raise RuntimeError("the B200 ptychography path runs on CUDA devices only (use device='gpu')")
+        prop = self._prop_factors if self._prop_factors is not None else self._propagators
+        if self.num_slices == 1:
+            n = int(self.roi_shape[0])
+            prop = torch.zeros((0, n, n), dtype=torch.complex64, device=dev)
+        return prop, self.dset.scan_positions_px.contiguous(), self.dset.targets, \
+            self.dset.detector_mask.to(dev).contiguous()
+
+    def forward_intensities(self, batch_indices, loss_type="l2_amplitude"):
+        """Predicted detector intensities (B, H, W) and batch loss, no gradients."""
+        prop, pos, tg, mask = self._batch_tensors()
+        bi = torch.as_tensor(np.asarray(batch_indices, dtype=np.int64), device=self._device)
+        with torch.no_grad():
+            obj_c = self.obj_model.obj.detach().contiguous()
+            probe_o = self.probe_model.probe.detach().contiguous()
+        out = ops.batch_forward(obj_c, probe_o, prop, pos, bi, tg, mask, self.dset.num_gpts,
+                                self.dset.mean_diffraction_intensity, loss_type)
+        return out["intensity"], out["loss"]
+
+    def forward_operator(self, obj_patches=None, shifted_input_probes=None, descan=None, batch_indices=None):
+        """(propagated probes (S,P,B,H,W), exit waves (P,B,H,W)) of a batch
+        (ptychography_base.py:892-906), computed by the batch kernel."""
+        if batch_indices is None:
+            raise ValueError("forward_operator on the B200 path takes batch_indices (positions are gathered in-kernel)")
+        prop, pos, tg, mask = self._batch_tensors()
+        bi = torch.as_tensor(np.asarray(batch_indices, dtype=np.int64), device=self._device)
+        with torch.no_grad():
+            out = ops.batch_forward(self.obj_model.obj.detach().contiguous(),
+                                    self.probe_model.probe.detach().contiguous(), prop, pos, bi, tg, mask,
+                                    self.dset.num_gpts, self.dset.mean_diffraction_intensity,
+                                    want_intensity=False, want_exit=True, want_waves=True)
+        return out["waves"], out["exit"]
+
+    # ------------------------------------------------------------ reconstruction
+    def reconstruct(self, num_iters: int = 0, reset: bool = False, optimizer_params: dict | None = None,
+                    scheduler_params: dict | None = None, constraints: dict = {}, batch_size: int | None = None,
+                    store_snapshots: bool | None = None, store_snapshots_every: int | None = None,
+                    device: Literal["cpu", "gpu"] | None = None, autograd: bool = True,
+                    loss_type: Literal["l2_amplitude", "l1_amplitude", "l2_intensity", "l1_intensity",
+                                       "poisson"] = "l2_amplitude"):
+        """Gradient-descent iterations (ptychography.py:146-308)."""
+        self._check_preprocessed()
+        if not autograd:
+            raise NotImplementedError("the analytic (autograd=False) update is not part of the B200 path yet")
+        if device is not None:
+            self.to(device)
+        self.batch_size = batch_size
+        if store_snapshots_every is not None:
+            self._store_snapshot_every = int(store_snapshots_every)
+            if store_snapshots is None:
+                store_snapshots = True
+        if store_snapshots is not None:
+            self._store_snapshots = bool(store_snapshots)
+        if reset:
+            self.reset_recon()
+        self.constraints = constraints
+        new_sched = reset
+        if optimizer_params is not None:
+            self.optimizer_params = optimizer_params
+            self.set_optimizers()
+            new_sched = True
+        if scheduler_params is not None:
+            self.scheduler_params = scheduler_params
+            new_sched = True
+        if new_sched:
+            self.set_schedulers(self.scheduler_params, num_iter=num_iters)
+        self.dset._set_targets(loss_type)
+        self.compute_propagator_arrays()
+        batcher = SimpleBatcher(self.dset.num_gpts, self.batch_size, rng=self.rng, val_ratio=self.val_ratio,
+                                val_mode=self.val_mode)
+        prop, _, tg, mask = self._batch_tensors()
+        opts = [o for o in (self.obj_model.optimizer, self.probe_model.optimizer) if o is not None]
+        dev = torch.device(self._device)
+        for a0 in range(num_iters):
+            total = torch.zeros((), dtype=torch.float32, device=dev)
+            nb = 0
+            for bi in batcher:
+                for o in opts:
+                    o.zero_grad(set_to_none=True)
+                self.dset.apply_hard_constraints(self.obj_padding_px)
+                pos = self.dset.scan_positions_px.contiguous()
+                idx = torch.as_tensor(np.asarray(bi, dtype=np.int64)).to(dev, non_blocking=True)
+                probe_o = self.probe_model.probe
+                loss = ops.batch_loss(self.obj_model._obj, probe_o, prop, pos, idx, tg, mask, self.dset.num_gpts,
+                                      self.dset.mean_diffraction_intensity, loss_type)
+                if self.obj_model._obj.requires_grad or self.probe_model._probe.requires_grad:
+                    loss.backward()
+                    if self.obj_model._obj.grad is not None:
+                        # ptychography.py:330-332
+                        self.obj_model._obj.grad.mul_(self.dset.upsample_factor ** 2 / 2)
+                for o in opts:
+                    o.step()
+                total += loss.detach()
+                nb += 1
+            total_loss = float((total / max(nb, 1)).item())
+            val_loss = None
+            if batcher.has_validation:
+                vl, vb = 0.0, 0
+                for bi in batcher.iter_val():
+                    _, l = self.forward_intensities(bi, loss_type)
+                    vl += float(l.item())
+                    vb += 1
+                if vb:
+                    val_loss = vl / vb
+                    self._iter_val_losses.append(val_loss)
+            self._record_iter(total_loss)
+            self.step_schedulers(total_loss)
+            if self._store_snapshots and (a0 % self._store_snapshot_every) == 0:
+                self._snapshots.append(dict(iteration=self.num_iters, obj=self.obj, probe=self.probe))
+            if self.logger is not None:
+                self.logger.log_iter(self.obj_model, self.probe_model, self.dset, self.num_iters - 1, total_loss,
+                                     nb, self._get_current_lrs())
+        return self
+
+    def _get_current_lrs(self):
+        return {k: o.param_groups[0]["lr"] for k, o in self.optimizers.items()}
+
+    def _record_iter(self, loss):
+        self._iter_losses.append(loss)
+        opts = self.optimizers
+        for key in set(self._iter_lrs) | set(opts):
+            if key in self._iter_lrs:
+                self._iter_lrs[key].append(opts[key].param_groups[0]["lr"] if key in opts else 0.0)
+            else:
+                self._iter_lrs[key] = [0.0] * (self.num_iters - 1) + [opts[key].param_groups[0]["lr"]]
+
+    # ------------------------------------------------------------ results
+    @property
+    def obj(self) -> np.ndarray:
+        """Constrained object with the mean phase removed (ptychography_base.py:312-318)."""
+        with torch.no_grad():
+            o = self.obj_model.obj.detach().cpu().numpy()
+        ph = np.angle(o)
+        return np.abs(o) * np.exp(1j * (ph - ph.mean()))
+
+    @property
+    def probe(self) -> np.ndarray:
+        with torch.no_grad():
+            return self.probe_model.probe.detach().cpu().numpy()
+
+    @property
+    def obj_cropped(self) -> np.ndarray:
+        c = self._crop_rotate_obj_fov(self.obj)
+        ph = np.angle(c)
+        return np.abs(c) * np.exp(1j * (ph - ph.mean()))
+
+    def _crop_rotate_obj_fov(self, array, positions_px=None, com_rotation_rad=None, transpose=None, padding=None):
+        """ptychography_base.py:782-831."""
+        array = np.asarray(array).copy()
+        rot = self.dset.com_rotation_rad if com_rotation_rad is None else com_rotation_rad
+        transpose = self.dset.com_transpose if transpose is None else transpose
+        angle = rot if transpose else -1 * rot
+        pos = self.dset.initial_scan_positions_px.cpu().numpy() if positions_px is None else positions_px
+        origin = pos.mean(0).astype(np.float32)
+        R = np.array([[np.cos(angle), -np.sin(angle)], [np.sin(angle), np.cos(angle)]], dtype=np.float32)
+        pts = (pos - origin) @ R + origin + 1e-9
+        min_r, min_c = np.floor(np.min(pts, axis=0)).astype("int")
+        max_r, max_c = np.ceil(np.max(pts, axis=0)).astype("int")
+        min_r, min_c = max(min_r, 0), max(min_c, 0)
+        max_r, max_c = min(max_r, array.shape[-2]), min(max_c, array.shape[-1])
+        out = ndi.rotate(array, np.rad2deg(-angle), order=1, reshape=False, axes=(-2, -1))[..., min_r:max_r,
+                                                                                                min_c:max_c]
+        if transpose:
+            out = out.swapaxes(-2, -1)
+        tgt = tuple(self.obj_shape_crop)
+        sl = []
+        for ax, t in zip(range(-3, 0), tgt):
+            n = out.shape[ax]
+            s0 = max((n - t) // 2, 0)
+            sl.append(slice(s0, s0 + min(t, n)))
+        return out[tuple(sl)]

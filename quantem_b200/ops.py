@@ -189,7 +189,12 @@ def _batch_args(geom, obj_c, probe_hat, prop, positions, batch_idx, targets, mas
     a = _lib.BatchArgs()
     a.obj = obj_c.data_ptr()
     a.probe_hat = probe_hat.data_ptr()
-    a.prop = prop.data_ptr() if (prop is not None and prop.numel() > 0) else None
+    if isinstance(prop, (tuple, list)):
+        a.prop = None
+        a.prop_r = prop[0].data_ptr() if prop[0].numel() > 0 else None
+        a.prop_c = prop[1].data_ptr() if prop[1].numel() > 0 else None
+    else:
+        a.prop = prop.data_ptr() if (prop is not None and prop.numel() > 0) else None
     a.positions = positions.data_ptr()
     a.batch_idx = batch_idx.data_ptr()
     a.targets = targets.data_ptr()
@@ -214,7 +219,11 @@ def _check_batch_inputs(obj_c, probe_o, prop, positions, batch_idx, targets, mas
     dev = obj_c.device
     _req(obj_c, "obj", torch.complex64, dev)
     _req(probe_o, "probe", torch.complex64, dev)
-    if prop is not None and prop.numel() > 0:
+    sep = isinstance(prop, (tuple, list))
+    if sep:
+        for t in prop:
+            _req(t, "separable propagator factors", torch.complex64, dev)
+    elif prop is not None and prop.numel() > 0:
         _req(prop, "propagators", torch.complex64, dev)
     _req(positions, "positions", torch.float32, dev)
     _req(batch_idx, "batch_indices", torch.int64, dev)
@@ -223,8 +232,12 @@ def _check_batch_inputs(obj_c, probe_o, prop, positions, batch_idx, targets, mas
     geom = BatchGeometry.of(obj_c, probe_o, positions.shape[0])
     if targets.shape[1:] != (geom.n, geom.n) or mask.shape != (geom.n, geom.n):
         raise ValueError("targets / mask must be (npos, n, n) / (n, n)")
-    if geom.S > 1 and (prop is None or tuple(prop.shape) != (geom.S - 1, geom.n, geom.n)):
-        raise ValueError(f"propagators must be ({geom.S - 1}, {geom.n}, {geom.n})")
+    if geom.S > 1:
+        if sep:
+            if any(tuple(t.shape) != (geom.S - 1, geom.n) for t in prop):
+                raise ValueError(f"separable propagator factors must be ({geom.S - 1}, {geom.n}) each")
+        elif prop is None or tuple(prop.shape) != (geom.S - 1, geom.n, geom.n):
+            raise ValueError(f"propagators must be ({geom.S - 1}, {geom.n}, {geom.n})")
     return geom
 
 
@@ -346,6 +359,28 @@ def batch_loss(obj_raw, probe_o, prop, positions, batch_idx, targets, mask, num_
     parameter (hard constraint included) and the orthogonalised probe."""
     cfg = dict(num_gpts=int(num_gpts), mean_intensity=float(mean_intensity), loss_type=loss_type, grid=grid)
     return _BatchLossFn.apply(obj_raw, probe_o, prop, positions, batch_idx, targets, mask, cfg)
+
+
+def separable_propagators(n, sampling, energy, slice_thicknesses, tilt_mrad=(0.0, 0.0), device="cuda"):
+    """Per-axis factors of the Fresnel propagators (probe_models.py:376-427).
+
+    K_s[kr, kc] = exp(-i pi lambda dz_s (kr^2 + kc^2)) exp(-2 pi i dz_s tan(tr) kr)
+    exp(-2 pi i dz_s tan(tc) kc) = Kr_s[kr] * Kc_s[kc].  Evaluated in float64 and
+    rounded to complex64.  Returns (Kr, Kc), each (S-1, n)."""
+    import math
+
+    from .diffractive_imaging.complex_probe import electron_wavelength_angstrom
+
+    dz = torch.as_tensor(slice_thicknesses, dtype=torch.float64).reshape(-1)
+    lam = electron_wavelength_angstrom(energy)
+    out = []
+    for ax, tilt in ((0, tilt_mrad[0]), (1, tilt_mrad[1])):
+        k = torch.fft.fftfreq(int(n), float(sampling[ax]), dtype=torch.float64)
+        ph = -math.pi * lam * dz[:, None] * k[None] ** 2
+        if tilt:
+            ph = ph - 2 * math.pi * dz[:, None] * math.tan(float(tilt) / 1e3) * k[None]
+        out.append(torch.polar(torch.ones_like(ph), ph).to(torch.complex64).to(device).contiguous())
+    return tuple(out)
 
 
 # ----------------------------------------------------------------------------

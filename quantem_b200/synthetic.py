@@ -105,7 +105,8 @@ def make_dataset(cfg: SyntheticConfig, device="cuda"):
         pos = pos + (torch.rand(pos.shape, generator=gen, device=dev, dtype=torch.float64) * 2 - 1) * cfg.jitter_px
     pos = pos.float().contiguous()
     probes = make_probe_modes(cfg, dev)
-    props = fresnel_propagators(cfg.n, cfg.pixel, cfg.energy, cfg.slice_thickness, cfg.slices, dev)
+    props = ops.separable_propagators(cfg.n, (cfg.pixel, cfg.pixel), cfg.energy,
+                                      [cfg.slice_thickness] * (cfg.slices - 1), device=dev)
     npos = pos.shape[0]
     dummy_t = torch.zeros((npos, cfg.n, cfg.n), device=dev, dtype=torch.float32)
     mask = torch.ones((cfg.n, cfg.n), device=dev, dtype=torch.float32)

@@ -203,6 +203,7 @@ def whitenoise_case():
                                              "probe": {"type": "sgd", "lr": 0.5}},
                            batch_size=N * N, device="cpu")
             tag = f"p{nprobe}_{'ad' if autograd else 'an'}"
+            out[f"probe_used_{tag}"] = _c64(probe_model._initial_probe.detach().numpy())
             out[f"grad_obj_{tag}"] = _c64(obj_model._obj.grad.numpy())
             out[f"grad_probe_{tag}"] = _c64(probe_model._probe.grad.numpy())
             out[f"loss_{tag}"] = np.asarray(pt._iter_losses, dtype=np.float64)
@@ -219,6 +220,9 @@ def main(src):
 
     torch.manual_seed(0)
     import_reference(src)
+    if os.environ.get("GOLDEN_ONLY") == "whitenoise":
+        whitenoise_case()
+        return
     run_case("single64", H=64, S=1, P=1, nscan=6, step_px=4, pad=32, dz=20.0, counts=1e5,
              jitter=False, batch=12, iters=3, seed=11)
     run_case("mixed64", H=64, S=3, P=3, nscan=5, step_px=6, pad=32, dz=20.0, counts=1e5,

@@ -1,0 +1,70 @@
+"""The drop-in API end to end on the GPU: ``Ptychography.reconstruct`` from the
+same state as the reference run recorded in the golden fixtures."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import ptycho_oracle as O
+from tests.conftest import load_golden, rel
+from tests.test_host_setup import build_from_golden
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("case", ["single64", "mixed64"])
+def test_reconstruct_matches_reference(cuda_device, case):
+    z = load_golden(case)
+    pt = build_from_golden(z, device="gpu")
+    dev = cuda_device
+    pt.dset.scan_positions_px = torch.as_tensor(z["positions"])
+    pt.obj_model._obj = torch.as_tensor(z["obj_perturbed"]).to(dev).requires_grad_(True)
+    pt.probe_model._probe = torch.as_tensor(z["probe_init"]).to(dev).requires_grad_(True)
+    pt.rng = int(z["recon_rng_seed"])
+    pt.reconstruct(num_iters=int(z["iters"]), batch_size=int(z["batch"]),
+                   optimizer_params={"object": {"type": "adam"}, "probe": {"type": "adam"}},
+                   constraints={"probe": {"orthogonalize_probe": bool(z["orthogonalize"])}}, device="gpu")
+    np.testing.assert_allclose(pt.iter_losses, z["recon_losses"], rtol=1e-4)
+    # Adam's first steps are ~lr * sign(g): float32 rounding of near-zero gradient
+    # components flips some of them, so any float32 run drifts from the float64
+    # trajectory.  Bound: 3x the reference's own measured drift from the FP64
+    # oracle on the same case (floor 1e-5).
+    H = int(z["H"])
+    props = z["propagators"].astype(np.complex128) if int(z["S"]) > 1 else np.zeros((0, H, H))
+    obj64, probe64, _ = O.reconstruct(z["obj_perturbed"].astype(np.complex128), z["probe_init"].astype(np.complex128),
+                                      z["positions"].astype(np.float64), props, z["targets"].astype(np.float64),
+                                      np.ones((H, H)), float(z["mean_intensity"]), float(z["upsample_factor"]),
+                                      int(z["iters"]), int(z["batch"]), np.random.default_rng(int(z["recon_rng_seed"])))
+    for mine, ref, truth in ((pt.obj_model._obj, z["recon_obj"], obj64), (pt.probe_model._probe, z["recon_probe"], probe64)):
+        bound = max(3 * rel(ref, truth), 1e-5)
+        assert rel(mine.detach().cpu().numpy(), truth) < bound
+
+
+def test_reference_gradient_test_case_on_gpu(cuda_device):
+    """The reference's own gradient-test inputs through the CUDA path (see
+    tests/test_oracle_golden.py for why the gradient bar is set by float32
+    conditioning here)."""
+    from quantem_b200 import ops
+    from quantem_b200.diffractive_imaging import Dataset4dstem, PtychographyDatasetRaster
+    from tests.golden.whitenoise import whitenoise_inputs
+
+    inp = whitenoise_inputs()
+    z = load_golden("whitenoise64")
+    N = inp["N"]
+    d4 = Dataset4dstem.from_array(inp["data4d"], sampling=inp["sampling4d"], units=("A", "A", "A^-1", "A^-1"))
+    pd = PtychographyDatasetRaster.from_dataset4dstem(d4, verbose=0)
+    pd.preprocess(com_fit_function="constant", force_com_rotation=0, force_com_transpose=False,
+                  probe_energy=inp["energy"])
+    dev = cuda_device
+    probe = torch.as_tensor(z["probe_used_p1_ad"]).to(dev)
+    obj = torch.ones((1, N, N), dtype=torch.complex64, device=dev)
+    loss, g_obj, _ = ops.batch_forward_adjoint(
+        ops.obj_constrain(obj)[0], probe, torch.zeros((0, N, N), dtype=torch.complex64, device=dev),
+        pd.scan_positions_px.to(dev), torch.arange(pd.num_gpts, device=dev), pd.targets.to(dev),
+        torch.ones((N, N), device=dev), pd.num_gpts, pd.mean_diffraction_intensity)
+    assert abs(loss.item() - z["loss_p1_ad"][0]) / z["loss_p1_ad"][0] < 1e-5
+    _, g_ref, _, _ = O.batch_loss_and_grads(np.ones((1, N, N), np.complex128),
+                                            z["probe_used_p1_ad"].astype(np.complex128),
+                                            pd.scan_positions_px.numpy().astype(np.float64), np.zeros((0, N, N)),
+                                            pd.targets.numpy().astype(np.float64), np.ones((N, N)), pd.num_gpts,
+                                            pd.mean_diffraction_intensity)
+    assert rel(g_obj.cpu().numpy(), g_ref) < 2e-2

@@ -1,0 +1,83 @@
+"""Host-side set-up of the drop-in API against the reference's own set-up
+products recorded in the golden fixtures (CPU only, no CUDA needed)."""
+import numpy as np
+import pytest
+import torch
+
+from tests.conftest import load_golden, rel
+
+
+def build_from_golden(z, device="cpu"):
+    from quantem_b200.diffractive_imaging import (Dataset4dstem, DetectorPixelated, ObjectPixelated,
+                                                  ProbePixelated, Ptychography, PtychographyDatasetRaster)
+
+    H, nscan = int(z["H"]), int(z["nscan"])
+    px, step = float(z["px"]), float(z["step_px"])
+    rs = 1.0 / (H * px)
+    d4 = Dataset4dstem.from_array(z["data"].reshape(nscan, nscan, H, H), sampling=(step * px, step * px, rs, rs),
+                                  units=("A", "A", "A^-1", "A^-1"))
+    pd = PtychographyDatasetRaster.from_dataset4dstem(d4, verbose=0)
+    pd.preprocess(com_fit_function="constant", force_com_rotation=0, force_com_transpose=False,
+                  plot_rotation=False, plot_com=False, probe_energy=float(z["energy"]))
+    S, P, seed = int(z["S"]), int(z["P"]), int(z["seed"])
+    w = z["weights"] if z["weights"].size else None
+    obj = ObjectPixelated.from_uniform(num_slices=S, slice_thicknesses=float(z["dz"]), obj_type="complex")
+    probe = ProbePixelated.from_params(probe_params={"energy": float(z["energy"]), "defocus": 200.0,
+                                                     "semiangle_cutoff": 20.0},
+                                       num_probes=P, rng=seed + 1, initial_probe_weights=w)
+    pt = Ptychography.from_models(dset=pd, obj_model=obj, probe_model=probe, detector_model=DetectorPixelated(),
+                                  device=device, verbose=0, rng=seed + 2)
+    pad = int(z["pad"])
+    pt.preprocess(obj_padding_px=(pad, pad))
+    return pt
+
+
+@pytest.mark.parametrize("case", ["single64", "mixed64"])
+def test_setup_matches_reference(case):
+    z = load_golden(case)
+    pt = build_from_golden(z)
+    d = pt.dset
+    assert abs(d.mean_diffraction_intensity - float(z["mean_intensity"])) / float(z["mean_intensity"]) < 1e-6
+    assert rel(d.targets.numpy(), z["targets"]) < 1e-6
+    np.testing.assert_allclose(d.initial_scan_positions_px.numpy(), z["initial_positions"], rtol=0, atol=1e-4)
+    assert tuple(pt.obj_shape_full) == tuple(z["obj_shape"])
+    np.testing.assert_array_equal(pt.obj_padding_px, z["obj_padding_px"])
+    assert abs(d.upsample_factor - float(z["upsample_factor"])) < 1e-12
+    assert rel(pt.probe_model._probe.detach().numpy(), z["probe_init"]) < 1e-5
+    if int(z["S"]) > 1:
+        assert rel(pt.propagators.numpy(), z["propagators"]) < 1e-6
+
+
+def test_batcher_matches_reference_order():
+    """Same numpy generator call sequence as the reference SimpleBatcher."""
+    from quantem_b200.diffractive_imaging.ptycho_utils import SimpleBatcher
+
+    b = SimpleBatcher(37, 10, rng=5)
+    got = [x.tolist() for x in b]
+    rng = np.random.default_rng(5)
+    order = rng.permutation(np.arange(37))
+    assert got == [order[i:i + 10].tolist() for i in range(0, 37, 10)]
+    v = SimpleBatcher(20, 4, rng=1, val_ratio=0.25)
+    assert len(v.val_indices) == 5 and len(v.train_indices) == 15
+
+
+def test_gram_schmidt_matches_oracle():
+    from oracle import ptycho_oracle as O
+    from quantem_b200.diffractive_imaging.ptycho_utils import orthogonalize_probes
+
+    rng = np.random.default_rng(0)
+    p = rng.standard_normal((3, 16, 16)) + 1j * rng.standard_normal((3, 16, 16))
+    p[1] *= 2.0
+    ref, _, _ = O.gram_schmidt(p)
+    got = orthogonalize_probes(torch.as_tensor(p)).numpy()
+    assert rel(got, ref) < 1e-12
+
+
+def test_unsupported_options_raise():
+    from quantem_b200.diffractive_imaging import ObjectPixelated
+
+    with pytest.raises(NotImplementedError):
+        ObjectPixelated.from_uniform(num_slices=1, obj_type="potential")
+    o = ObjectPixelated.from_uniform(num_slices=1)
+    with pytest.raises(NotImplementedError):
+        o.add_constraint("tv_weight_xy", 0.1)
