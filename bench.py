@@ -345,12 +345,12 @@ def run_kernel_only(args):
         s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s0.record()
         ops.batch_forward_adjoint(obj_c, probes, ds["propagators"], ds["positions"], idx, ds["amplitudes"], mask,
-                                  ds["positions"].shape[0], ds["mean_intensity"])
+                                  ds["positions"].shape[0], ds["mean_intensity"], variant=args.variant)
         s1.record()
         torch.cuda.synchronize()
         if i >= args.warmup:
             times.append(s0.elapsed_time(s1))
-    print(json.dumps({"mode": "kernel-only", "positions": args.positions, "ms_per_batch": statistics.mean(times),
+    print(json.dumps({"mode": "kernel-only", "variant": args.variant, "positions": args.positions, "ms_per_batch": statistics.mean(times),
                       "positions_per_s": args.positions / (statistics.mean(times) * 1e-3)}))
 
 
@@ -378,6 +378,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--kernel-only", action="store_true", help="time only the fused batch kernel")
     ap.add_argument("--positions", type=int, default=296, help="positions per launch with --kernel-only")
+    ap.add_argument("--variant", default="auto", choices=["auto", "serial", "cluster"],
+                    help="mapping of probe modes onto CTAs (--kernel-only)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -78,7 +78,14 @@ typedef struct ptycho_batch_args {
   int loss_type;             /* PTYCHO_LOSS_* */
   float loss_scale;          /* npos_total / (B * mean_intensity) */
   float inv_mean_intensity;  /* 1 / mean_intensity */
+  int variant;               /* PTYCHO_VARIANT_*: how probe modes map onto CTAs */
 } ptycho_batch_args;
+
+enum {
+  PTYCHO_VARIANT_AUTO = 0,    /* the faster of the two on B200 (currently serial) */
+  PTYCHO_VARIANT_SERIAL = 1,  /* one CTA per position, modes in sequence */
+  PTYCHO_VARIANT_CLUSTER = 2  /* one thread-block cluster of P CTAs per position */
+};
 
 /* Copy the last error message of this host thread into buf (NUL-terminated). */
 int ptycho_get_last_error(char* buf, size_t len);
@@ -92,6 +99,12 @@ int ptycho_sm_count(int* out);
 /* Number of complex64 elements of scratch / partial buffers for a batch launch. */
 int ptycho_workspace_elems(int n, int S, int P, int grid, int64_t* scratch_elems,
                            int64_t* partial_elems);
+
+/* Launch plan of a batch: resolved variant, grid (CTAs) and the complex64
+ * element counts of the scratch and probe-gradient partial buffers the adjoint
+ * launch needs.  Reads n, S, P, B and variant from *a. */
+int ptycho_batch_plan(const ptycho_batch_args* a, int adjoint, int* variant, int* grid, int64_t* scratch_elems,
+                      int64_t* partial_elems, int* partial_parts);
 
 /* Forward model + loss of one batch (no gradients). */
 int ptycho_forward_loss(const ptycho_batch_args* a, void* stream);

@@ -14,6 +14,7 @@ _PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_PKG, "lib", "libptycho_b200.so")
 
 PTYCHO_OK = 0
+VARIANTS = {"auto": 0, "serial": 1, "cluster": 2}
 ERR_NAMES = {1: "invalid argument", 2: "unsupported configuration", 3: "CUDA error", 4: "non-finite values"}
 
 LOSS_TYPES = {
@@ -30,6 +31,7 @@ EXPORTED = (
     "ptycho_abi_version",
     "ptycho_sm_count",
     "ptycho_workspace_elems",
+    "ptycho_batch_plan",
     "ptycho_forward_loss",
     "ptycho_forward_adjoint",
     "ptycho_fft2",
@@ -60,7 +62,7 @@ class BatchArgs(ctypes.Structure):
         ("out_waves", _vp), ("status", _vp), ("prop_r", _vp), ("prop_c", _vp),
         ("n", _int), ("S", _int), ("P", _int), ("B", _int), ("Ho", _int), ("Wo", _int),
         ("npos", _int), ("grid", _int), ("loss_type", _int),
-        ("loss_scale", _flt), ("inv_mean_intensity", _flt),
+        ("loss_scale", _flt), ("inv_mean_intensity", _flt), ("variant", _int),
     ]
 
 
@@ -74,6 +76,8 @@ def _declare(lib):
         "ptycho_abi_version": (_int, []),
         "ptycho_sm_count": (_int, [ctypes.POINTER(_int)]),
         "ptycho_workspace_elems": (_int, [_int, _int, _int, _int, ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
+        "ptycho_batch_plan": (_int, [ctypes.POINTER(BatchArgs), _int, ctypes.POINTER(_int), ctypes.POINTER(_int),
+                                     ctypes.POINTER(_i64), ctypes.POINTER(_i64), ctypes.POINTER(_int)]),
         "ptycho_forward_loss": (_int, [ctypes.POINTER(BatchArgs), _vp]),
         "ptycho_forward_adjoint": (_int, [ctypes.POINTER(BatchArgs), _vp]),
         "ptycho_fft2": (_int, [_vp, _vp, _int, _int, _int, _flt, _vp]),

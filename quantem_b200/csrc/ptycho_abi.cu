@@ -220,9 +220,13 @@ int grid_for(int64_t n, int threads) {
 // Records `msg` as this host thread's last error (used by noalloc.cu).
 int qb_record_error(int code, const char* msg) { return fail(code, "%s", msg); }
 
-// defined in fused_n64.cu / fused_n128.cu
-int qb_launch_batch_64(const ptycho_batch_args* a, bool adj, cudaStream_t st);
-int qb_launch_batch_128(const ptycho_batch_args* a, bool adj, cudaStream_t st);
+// defined in fused_n{64,128}.cu and cluster_n{64,128}.cu
+int qb_launch_serial_64(const ptycho_batch_args* a, bool adj, cudaStream_t st);
+int qb_launch_serial_128(const ptycho_batch_args* a, bool adj, cudaStream_t st);
+int qb_launch_cluster_64(const ptycho_batch_args* a, bool adj, cudaStream_t st);
+int qb_launch_cluster_128(const ptycho_batch_args* a, bool adj, cudaStream_t st);
+int qb_max_clusters_64(const ptycho_batch_args* a, bool adj);
+int qb_max_clusters_128(const ptycho_batch_args* a, bool adj);
 
 namespace {
 
@@ -255,12 +259,27 @@ int validate_batch(const ptycho_batch_args* a, bool adj) {
   return PTYCHO_OK;
 }
 
+// PTYCHO_VARIANT_CLUSTER or PTYCHO_VARIANT_SERIAL for this configuration, or -1.
+int resolve_variant(const ptycho_batch_args* a) {
+  if (a->variant == PTYCHO_VARIANT_SERIAL) return PTYCHO_VARIANT_SERIAL;
+  if (a->variant == PTYCHO_VARIANT_CLUSTER) return (a->P >= 1 && a->P <= 8) ? PTYCHO_VARIANT_CLUSTER : -1;
+  // measured on B200 (8 slices, 4 modes, 128^2): serial 5.9 ms vs cluster 6.9 ms per 592 positions
+  if (a->variant == PTYCHO_VARIANT_AUTO) return PTYCHO_VARIANT_SERIAL;
+  return -1;
+}
+
 int run_batch(const ptycho_batch_args* a, void* stream, bool adj) {
   int rc = validate_batch(a, adj);
   if (rc) return rc;
   if (a->B == 0) return PTYCHO_OK;
+  const int variant = resolve_variant(a);
+  if (variant < 0) return fail(PTYCHO_ERR_UNSUPPORTED, "variant %d not available for P=%d", a->variant, a->P);
+  if (variant == PTYCHO_VARIANT_CLUSTER && a->grid % a->P != 0)
+    return fail(PTYCHO_ERR_INVALID, "cluster launch: grid %d is not a multiple of P=%d", a->grid, a->P);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  const int lrc = a->n == 64 ? qb_launch_batch_64(a, adj, st) : qb_launch_batch_128(a, adj, st);
+  const bool cl = variant == PTYCHO_VARIANT_CLUSTER;
+  const int lrc = cl ? (a->n == 64 ? qb_launch_cluster_64(a, adj, st) : qb_launch_cluster_128(a, adj, st))
+                     : (a->n == 64 ? qb_launch_serial_64(a, adj, st) : qb_launch_serial_128(a, adj, st));
   if (lrc) return fail(lrc, "fused_batch_kernel launch: %s", cudaGetErrorString(cudaGetLastError()));
   return PTYCHO_OK;
 }
@@ -292,6 +311,43 @@ int ptycho_workspace_elems(int n, int S, int P, int grid, int64_t* scratch_elems
   const int64_t nn = (int64_t)n * n;
   if (scratch_elems) *scratch_elems = (int64_t)grid * (P * S + P) * nn;
   if (partial_elems) *partial_elems = (int64_t)grid * P * nn;
+  return PTYCHO_OK;
+}
+
+int ptycho_batch_plan(const ptycho_batch_args* a, int adjoint, int* variant, int* grid, int64_t* scratch_elems,
+                      int64_t* partial_elems, int* partial_parts) {
+  if (!a) return fail(PTYCHO_ERR_INVALID, "plan: args is NULL");
+  if (a->n != 64 && a->n != 128) return fail(PTYCHO_ERR_UNSUPPORTED, "probe window n=%d not built (64, 128)", a->n);
+  if (a->S < 1 || a->P < 1 || a->B < 0) return fail(PTYCHO_ERR_INVALID, "plan: bad sizes");
+  const int v = resolve_variant(a);
+  if (v < 0) return fail(PTYCHO_ERR_UNSUPPORTED, "variant %d not available for P=%d", a->variant, a->P);
+  int sms = 0, dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return fail(PTYCHO_ERR_CUDA, "plan: %s", cudaGetErrorString(e));
+  const int64_t nn = (int64_t)a->n * a->n;
+  const int B = a->B > 0 ? a->B : 1;
+  int g, parts;
+  int64_t scr, part;
+  if (v == PTYCHO_VARIANT_CLUSTER) {
+    int mc = a->n == 64 ? qb_max_clusters_64(a, adjoint != 0) : qb_max_clusters_128(a, adjoint != 0);
+    if (mc < 1) return fail(PTYCHO_ERR_UNSUPPORTED, "no cluster of %d CTAs fits on this device", a->P);
+    const int ncl = B < mc ? B : mc;
+    g = ncl * a->P;
+    parts = ncl;
+    scr = (int64_t)g * a->S * nn;
+    part = (int64_t)g * nn;
+  } else {
+    g = B < sms ? B : sms;
+    parts = g;
+    scr = (int64_t)g * (a->P * a->S + a->P) * nn;
+    part = (int64_t)g * a->P * nn;
+  }
+  if (variant) *variant = v;
+  if (grid) *grid = g;
+  if (scratch_elems) *scratch_elems = scr;
+  if (partial_elems) *partial_elems = part;
+  if (partial_parts) *partial_parts = parts;
   return PTYCHO_OK;
 }
 

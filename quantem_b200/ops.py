@@ -155,15 +155,12 @@ class Workspace:
         self.loss_part = None
         self.status = torch.zeros(1, dtype=torch.int32, device=self.device)
 
-    def get(self, geom: BatchGeometry, grid: int, adjoint: bool):
-        nn = geom.n * geom.n
-        if adjoint:
-            need_s = grid * (geom.P * geom.S + geom.P) * nn
-            need_p = grid * geom.P * nn
-            if self.scratch is None or self.scratch.numel() < need_s:
-                self.scratch = torch.empty(need_s, dtype=torch.complex64, device=self.device)
-            if self.partials is None or self.partials.numel() < need_p:
-                self.partials = torch.empty(need_p, dtype=torch.complex64, device=self.device)
+    def ensure(self, scratch_elems: int, partial_elems: int, grid: int):
+        if scratch_elems and (self.scratch is None or self.scratch.numel() < scratch_elems):
+            self.scratch = None
+            self.scratch = torch.empty(int(scratch_elems), dtype=torch.complex64, device=self.device)
+        if partial_elems and (self.partials is None or self.partials.numel() < partial_elems):
+            self.partials = torch.empty(int(partial_elems), dtype=torch.complex64, device=self.device)
         if self.loss_part is None or self.loss_part.numel() < grid:
             self.loss_part = torch.empty(max(grid, 256), dtype=torch.float64, device=self.device)
         return self
@@ -183,9 +180,8 @@ def default_grid(B: int, device=None) -> int:
     return max(1, min(B, sm_count(device)))
 
 
-def _batch_args(geom, obj_c, probe_hat, prop, positions, batch_idx, targets, mask, B, grid, loss_type,
-                loss_scale, inv_mean, ws, grad_obj=None, out_intensity=None, out_exit=None, out_waves=None,
-                adjoint=False):
+def _batch_args(geom, obj_c, probe_hat, prop, positions, batch_idx, targets, mask, B, loss_type, loss_scale,
+                inv_mean, grad_obj=None, out_intensity=None, out_exit=None, out_waves=None, variant="auto"):
     a = _lib.BatchArgs()
     a.obj = obj_c.data_ptr()
     a.probe_hat = probe_hat.data_ptr()
@@ -200,19 +196,39 @@ def _batch_args(geom, obj_c, probe_hat, prop, positions, batch_idx, targets, mas
     a.targets = targets.data_ptr()
     a.mask = mask.data_ptr()
     a.grad_obj = grad_obj.data_ptr() if grad_obj is not None else None
-    a.probe_grad_part = ws.partials.data_ptr() if adjoint else None
-    a.scratch = ws.scratch.data_ptr() if adjoint else None
-    a.loss_part = ws.loss_part.data_ptr()
     a.out_intensity = out_intensity.data_ptr() if out_intensity is not None else None
     a.out_exit = out_exit.data_ptr() if out_exit is not None else None
     a.out_waves = out_waves.data_ptr() if out_waves is not None else None
-    a.status = ws.status.data_ptr()
     a.n, a.S, a.P, a.B = geom.n, geom.S, geom.P, int(B)
-    a.Ho, a.Wo, a.npos, a.grid = geom.Ho, geom.Wo, geom.npos, int(grid)
+    a.Ho, a.Wo, a.npos = geom.Ho, geom.Wo, geom.npos
     a.loss_type = _lib.LOSS_TYPES[loss_type]
     a.loss_scale = float(loss_scale)
     a.inv_mean_intensity = float(inv_mean)
+    a.variant = _lib.VARIANTS[variant]
     return a
+
+
+def plan_and_bind(a, device, adjoint: bool, grid=None):
+    """Resolve the launch plan of ``a`` (variant, grid, workspace sizes), bind the
+    device workspace and return (grid, number of probe-gradient partials)."""
+    v, g, parts = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0)
+    se, pe = ctypes.c_int64(0), ctypes.c_int64(0)
+    _lib.check(_lib.lib().ptycho_batch_plan(ctypes.byref(a), int(adjoint), ctypes.byref(v), ctypes.byref(g),
+                                            ctypes.byref(se), ctypes.byref(pe), ctypes.byref(parts)), "batch_plan")
+    grid_v, parts_v = g.value, parts.value
+    if grid is not None:  # caller-chosen grid (serial variant only)
+        if v.value != _lib.VARIANTS["serial"]:
+            raise ValueError("an explicit grid is only accepted with variant='serial'")
+        grid_v = parts_v = int(grid)
+        nn = a.n * a.n
+        se.value, pe.value = grid_v * (a.P * a.S + a.P) * nn, grid_v * a.P * nn
+    ws = workspace(device).ensure(se.value if adjoint else 0, pe.value if adjoint else 0, grid_v)
+    a.grid = grid_v
+    a.scratch = ws.scratch.data_ptr() if adjoint else None
+    a.probe_grad_part = ws.partials.data_ptr() if adjoint else None
+    a.loss_part = ws.loss_part.data_ptr()
+    a.status = ws.status.data_ptr()
+    return grid_v, parts_v, ws
 
 
 def _check_batch_inputs(obj_c, probe_o, prop, positions, batch_idx, targets, mask):
@@ -248,7 +264,7 @@ def loss_scale_of(loss_type: str, B: int, num_gpts: int, mean_intensity: float) 
 
 def batch_forward(obj_c, probe_o, prop, positions, batch_idx, targets, mask, num_gpts, mean_intensity,
                   loss_type="l2_amplitude", want_intensity=True, want_exit=False, want_waves=False,
-                  probe_hat=None, grid=None):
+                  probe_hat=None, grid=None, variant="auto"):
     """Forward model + loss of one batch with no gradients.
 
     Returns dict(loss=0-d tensor, intensity=(B,n,n) detector layout or None,
@@ -257,29 +273,28 @@ def batch_forward(obj_c, probe_o, prop, positions, batch_idx, targets, mask, num
     geom = _check_batch_inputs(obj_c, probe_o, prop, positions, batch_idx, targets, mask)
     B = int(batch_idx.numel())
     dev = obj_c.device
-    grid = default_grid(B, dev) if grid is None else int(grid)
-    ws = workspace(dev).get(geom, grid, adjoint=False)
     if probe_hat is None:
         probe_hat = fft2(probe_o)
     out_i = torch.empty((B, geom.n, geom.n), dtype=torch.float32, device=dev) if want_intensity else None
     out_e = torch.empty((geom.P, B, geom.n, geom.n), dtype=torch.complex64, device=dev) if want_exit else None
     out_w = (torch.empty((geom.S, geom.P, B, geom.n, geom.n), dtype=torch.complex64, device=dev)
              if want_waves else None)
-    a = _batch_args(geom, obj_c, probe_hat, prop, positions, batch_idx, targets, mask, B, grid, loss_type,
-                    loss_scale_of(loss_type, max(B, 1), num_gpts, mean_intensity), 1.0 / mean_intensity, ws,
-                    out_intensity=out_i, out_exit=out_e, out_waves=out_w)
-    _lib.check(_lib.lib().ptycho_forward_loss(ctypes.byref(a), _stream()), "forward_loss")
+    a = _batch_args(geom, obj_c, probe_hat, prop, positions, batch_idx, targets, mask, B, loss_type,
+                    loss_scale_of(loss_type, max(B, 1), num_gpts, mean_intensity), 1.0 / mean_intensity,
+                    out_intensity=out_i, out_exit=out_e, out_waves=out_w, variant=variant)
+    grid_v, _, ws = plan_and_bind(a, dev, adjoint=False, grid=grid)
     loss = torch.empty((), dtype=torch.float32, device=dev)
-    if B > 0:
-        _lib.check(_lib.lib().ptycho_reduce_loss(_p(ws.loss_part), grid, _p(loss), _stream()), "reduce_loss")
-    else:
+    if B == 0:
         loss.zero_()
+        return dict(loss=loss, intensity=out_i, exit=out_e, waves=out_w)
+    _lib.check(_lib.lib().ptycho_forward_loss(ctypes.byref(a), _stream()), "forward_loss")
+    _lib.check(_lib.lib().ptycho_reduce_loss(_p(ws.loss_part), grid_v, _p(loss), _stream()), "reduce_loss")
     return dict(loss=loss, intensity=out_i, exit=out_e, waves=out_w)
 
 
 def batch_forward_adjoint(obj_c, probe_o, prop, positions, batch_idx, targets, mask, num_gpts, mean_intensity,
                           loss_type="l2_amplitude", probe_hat=None, grid=None, grad_obj=None,
-                          grad_probe=None):
+                          grad_probe=None, variant="auto"):
     """Fused forward + loss + adjoint of one batch.
 
     Returns (loss 0-d tensor, grad w.r.t. the constrained object (S,Ho,Wo),
@@ -289,8 +304,6 @@ def batch_forward_adjoint(obj_c, probe_o, prop, positions, batch_idx, targets, m
     geom = _check_batch_inputs(obj_c, probe_o, prop, positions, batch_idx, targets, mask)
     B = int(batch_idx.numel())
     dev = obj_c.device
-    grid = default_grid(B, dev) if grid is None else int(grid)
-    ws = workspace(dev).get(geom, grid, adjoint=True)
     if probe_hat is None:
         probe_hat = fft2(probe_o)
     if grad_obj is None:
@@ -302,9 +315,10 @@ def batch_forward_adjoint(obj_c, probe_o, prop, positions, batch_idx, targets, m
         loss.zero_()
         grad_probe.zero_()
         return loss, grad_obj, grad_probe
-    a = _batch_args(geom, obj_c, probe_hat, prop, positions, batch_idx, targets, mask, B, grid, loss_type,
-                    loss_scale_of(loss_type, B, num_gpts, mean_intensity), 1.0 / mean_intensity, ws,
-                    grad_obj=grad_obj, adjoint=True)
+    a = _batch_args(geom, obj_c, probe_hat, prop, positions, batch_idx, targets, mask, B, loss_type,
+                    loss_scale_of(loss_type, B, num_gpts, mean_intensity), 1.0 / mean_intensity,
+                    grad_obj=grad_obj, variant=variant)
+    grid_v, parts, ws = plan_and_bind(a, dev, adjoint=True, grid=grid)
     lib = _lib.lib()
     st = _stream()
     if PROFILE_EVENTS is not None:
@@ -314,9 +328,9 @@ def batch_forward_adjoint(obj_c, probe_o, prop, positions, batch_idx, targets, m
     if PROFILE_EVENTS is not None:
         ev1.record()
         PROFILE_EVENTS.append((ev0, ev1))
-    _lib.check(lib.ptycho_reduce_loss(_p(ws.loss_part), grid, _p(loss), st), "reduce_loss")
+    _lib.check(lib.ptycho_reduce_loss(_p(ws.loss_part), grid_v, _p(loss), st), "reduce_loss")
     nn = geom.P * geom.n * geom.n
-    _lib.check(lib.ptycho_reduce_partials(_p(ws.partials), _p(grad_probe), grid, nn, st), "reduce_partials")
+    _lib.check(lib.ptycho_reduce_partials(_p(ws.partials), _p(grad_probe), parts, nn, st), "reduce_partials")
     inv = 1.0 / float(geom.n * geom.n)
     _lib.check(lib.ptycho_fft2(_p(grad_probe), _p(grad_probe), geom.P, geom.n, 1, inv, st), "fft2")
     return loss, grad_obj, grad_probe
@@ -334,12 +348,12 @@ class _BatchLossFn(torch.autograd.Function):
         if need:
             loss, g_obj_c, g_probe = batch_forward_adjoint(
                 obj_c, probe_c, prop, positions, batch_idx, targets, mask, cfg["num_gpts"],
-                cfg["mean_intensity"], cfg["loss_type"], grid=cfg.get("grid"))
+                cfg["mean_intensity"], cfg["loss_type"], grid=cfg.get("grid"), variant=cfg.get("variant", "auto"))
             ctx.save_for_backward(obj_raw_c, work, g_obj_c, g_probe)
         else:
             loss = batch_forward(obj_c, probe_c, prop, positions, batch_idx, targets, mask, cfg["num_gpts"],
                                  cfg["mean_intensity"], cfg["loss_type"], want_intensity=False,
-                                 grid=cfg.get("grid"))["loss"]
+                                 grid=cfg.get("grid"), variant=cfg.get("variant", "auto"))["loss"]
         return loss
 
     @staticmethod
@@ -354,10 +368,11 @@ class _BatchLossFn(torch.autograd.Function):
 
 
 def batch_loss(obj_raw, probe_o, prop, positions, batch_idx, targets, mask, num_gpts, mean_intensity,
-               loss_type="l2_amplitude", grid=None):
+               loss_type="l2_amplitude", grid=None, variant="auto"):
     """Differentiable consistency loss of one batch w.r.t. the raw object
     parameter (hard constraint included) and the orthogonalised probe."""
-    cfg = dict(num_gpts=int(num_gpts), mean_intensity=float(mean_intensity), loss_type=loss_type, grid=grid)
+    cfg = dict(num_gpts=int(num_gpts), mean_intensity=float(mean_intensity), loss_type=loss_type, grid=grid,
+               variant=variant)
     return _BatchLossFn.apply(obj_raw, probe_o, prop, positions, batch_idx, targets, mask, cfg)
 
 

@@ -59,8 +59,9 @@ def _golden_inputs(z, dev):
     )
 
 
+@pytest.mark.parametrize("variant", ["serial", "cluster"])
 @pytest.mark.parametrize("case", ["single64", "mixed64", "mixed128"])
-def test_batch_forward_matches_reference(cuda_device, case):
+def test_batch_forward_matches_reference(cuda_device, case, variant):
     from quantem_b200 import ops
 
     z = load_golden(case)
@@ -69,13 +70,14 @@ def test_batch_forward_matches_reference(cuda_device, case):
     obj_c, _ = ops.obj_constrain(_t(z["obj_perturbed"], dev))
     probe_o = _t(z["probe_ortho"], dev)
     out = ops.batch_forward(obj_c, probe_o, inp["prop"], inp["positions"], inp["batch_idx"], inp["targets"],
-                            inp["mask"], int(z["positions"].shape[0]), float(z["mean_intensity"]))
+                            inp["mask"], int(z["positions"].shape[0]), float(z["mean_intensity"]), variant=variant)
     assert rel(out["intensity"].cpu().numpy(), z["batch_intensities"]) < TOL_I
     assert abs(out["loss"].item() - float(z["batch_loss"])) / float(z["batch_loss"]) < TOL_I
 
 
+@pytest.mark.parametrize("variant", ["serial", "cluster"])
 @pytest.mark.parametrize("case", ["single64", "mixed64", "mixed128"])
-def test_batch_gradients_match_reference(cuda_device, case):
+def test_batch_gradients_match_reference(cuda_device, case, variant):
     from quantem_b200 import ops
     from quantem_b200.diffractive_imaging.ptycho_utils import orthogonalize_probes
 
@@ -86,7 +88,7 @@ def test_batch_gradients_match_reference(cuda_device, case):
     probe = _t(z["probe_init"], dev).requires_grad_(True)
     probe_o = orthogonalize_probes(probe) if int(z["orthogonalize"]) else probe
     loss = ops.batch_loss(obj, probe_o, inp["prop"], inp["positions"], inp["batch_idx"], inp["targets"],
-                          inp["mask"], int(z["positions"].shape[0]), float(z["mean_intensity"]))
+                          inp["mask"], int(z["positions"].shape[0]), float(z["mean_intensity"]), variant=variant)
     loss.backward()
     g_obj = obj.grad.cpu().numpy() * float(z["upsample_factor"]) ** 2 / 2
     assert abs(loss.item() - float(z["batch_loss"])) / float(z["batch_loss"]) < TOL_I
@@ -104,7 +106,8 @@ def _c2_like(rng, S=8, P=4, n=128, Ho=512, B=6):
     return obj, probe, props, positions, targets
 
 
-def test_c2_geometry_matches_fp64_oracle(cuda_device):
+@pytest.mark.parametrize("variant", ["serial", "cluster"])
+def test_c2_geometry_matches_fp64_oracle(cuda_device, variant):
     """512^2 x 8 slices, 4 modes at 128^2 (the multislice mixed-probe configuration)."""
     from quantem_b200 import ops
 
@@ -124,15 +127,16 @@ def test_c2_geometry_matches_fp64_oracle(cuda_device):
             _t(props.astype(np.complex64), dev), _t(pos_full, dev, torch.float32),
             torch.arange(B, device=dev, dtype=torch.int64), _t(tg_full, dev, torch.float32),
             torch.ones((128, 128), device=dev), npos, mean_i)
-    out = ops.batch_forward(*args)
+    out = ops.batch_forward(*args, variant=variant)
     assert rel(out["intensity"].cpu().numpy(), I_o) < TOL_I
-    loss, g_obj, g_probe = ops.batch_forward_adjoint(*args)
+    loss, g_obj, g_probe = ops.batch_forward_adjoint(*args, variant=variant)
     assert abs(loss.item() - loss_o) / loss_o < TOL_I
     assert rel(g_obj.cpu().numpy(), g_obj_o) < TOL_G
     assert rel(g_probe.cpu().numpy(), g_probe_o) < TOL_G
 
 
-def test_c2_geometry_separable_propagators(cuda_device):
+@pytest.mark.parametrize("variant", ["serial", "cluster"])
+def test_c2_geometry_separable_propagators(cuda_device, variant):
     """Same geometry with the propagators passed as per-axis factors (shared-memory path)."""
     from quantem_b200 import ops
 
@@ -151,9 +155,9 @@ def test_c2_geometry_separable_propagators(cuda_device):
     args = (_t(obj_c.astype(np.complex64), dev), _t(probe.astype(np.complex64), dev), (kr, kc),
             _t(pos_full, dev, torch.float32), torch.arange(B, device=dev, dtype=torch.int64),
             _t(tg_full, dev, torch.float32), torch.ones((128, 128), device=dev), npos, mean_i)
-    out = ops.batch_forward(*args)
+    out = ops.batch_forward(*args, variant=variant)
     assert rel(out["intensity"].cpu().numpy(), O.detector_intensities(st)) < TOL_I
-    loss, g_obj, g_probe = ops.batch_forward_adjoint(*args)
+    loss, g_obj, g_probe = ops.batch_forward_adjoint(*args, variant=variant)
     assert abs(loss.item() - loss_o) / loss_o < TOL_I
     assert rel(g_obj.cpu().numpy(), g_obj_o) < TOL_G
     assert rel(g_probe.cpu().numpy(), g_probe_o) < TOL_G

@@ -45,7 +45,6 @@ def test_forward_loss_noalloc_matches_allocating_entry_point(cuda_device):
     probe_hat = ops.fft2(probe_o)
     geom = ops.BatchGeometry.of(obj_c, probe_o, npos)
     B = int(bidx.numel())
-    grid = ops.default_grid(B, dev)
     lib = _lib.lib()
     stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
     for call in range(2):
@@ -58,7 +57,10 @@ def test_forward_loss_noalloc_matches_allocating_entry_point(cuda_device):
         a.loss_part = None  # ignored: the partials live in the library's static array
         a.out_intensity = out_i.data_ptr()
         a.n, a.S, a.P, a.B = geom.n, geom.S, geom.P, B
-        a.Ho, a.Wo, a.npos, a.grid = geom.Ho, geom.Wo, npos, grid
+        a.Ho, a.Wo, a.npos = geom.Ho, geom.Wo, npos
+        grid = ctypes.c_int(0)
+        _lib.check(lib.ptycho_batch_plan(ctypes.byref(a), 0, None, ctypes.byref(grid), None, None, None), "plan")
+        a.grid = grid.value
         a.loss_type = _lib.LOSS_TYPES["l2_amplitude"]
         a.loss_scale = ops.loss_scale_of("l2_amplitude", B, npos, mean_i)
         a.inv_mean_intensity = 1.0 / mean_i
