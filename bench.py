@@ -103,6 +103,16 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(values, dist, device="cpu"):
+    """Element-wise maximum of per-rank timings (identity on one rank)."""
+    import torch
+
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
 def _dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -238,10 +248,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1) / args.steps
 
-    ms_t = torch.tensor([ms, e2e_ms], device=device)
-    if dist:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms, e2e_ms = ms_t.tolist()
+    ms, e2e_ms = max_over_ranks([ms, e2e_ms], dist, device)
     if rank != 0:
         if dist:
             dist.destroy_process_group()

@@ -14,6 +14,11 @@ GOLDEN = os.path.join(ROOT, "tests", "golden")
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and the built library")
     config.addinivalue_line("markers", "slow: long-running test")
+    # the CUDA library is built in-tree (nvcc cross-compiles without a GPU)
+    from quantem_b200 import build as _build
+
+    if not os.path.exists(_build.LIB):
+        _build.build()
 
 
 def load_golden(name):

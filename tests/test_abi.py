@@ -1,0 +1,57 @@
+"""The C ABI library loads and exports every symbol include/ptycho_b200.h declares
+(no GPU needed: nothing here launches work)."""
+import ctypes
+import os
+import re
+
+from tests.conftest import ROOT
+
+
+def _declared():
+    txt = open(os.path.join(ROOT, "include", "ptycho_b200.h")).read()
+    return sorted(set(re.findall(r"^int\s+(ptycho_\w+)\s*\(", txt, flags=re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    from quantem_b200 import _lib
+
+    lib = _lib.lib()
+    names = _declared()
+    assert len(names) >= 15
+    for n in names:
+        assert hasattr(lib, n), n
+    assert sorted(_lib.EXPORTED) == names
+
+
+def test_host_side_validation_without_gpu():
+    from quantem_b200 import _lib
+
+    lib = _lib.lib()
+    assert lib.ptycho_abi_version() >= 1
+    # NULL arguments are rejected before any CUDA call, with a message
+    assert lib.ptycho_forward_loss(None, None) == 1
+    assert "NULL" in _lib.last_error()
+    a = _lib.BatchArgs()
+    a.n = 96
+    assert lib.ptycho_forward_adjoint(ctypes.byref(a), None) == 2  # 96 x 96 window not built
+    assert "96" in _lib.last_error()
+    a.n, a.S, a.P, a.B, a.Ho, a.Wo, a.npos = 128, 2, 1, 4, 64, 64, 4
+    assert lib.ptycho_forward_loss(ctypes.byref(a), None) == 1      # missing pointers
+    assert lib.ptycho_reduce_loss(None, 1, None, None) == 1
+    assert lib.ptycho_fft2(None, None, 1, 128, 0, 1.0, None) == 1
+    buf = ctypes.create_string_buffer(8)
+    assert lib.ptycho_get_last_error(buf, 8) == 0 and len(buf.value) <= 7
+
+
+def test_product_has_no_cpu_fallback():
+    """Compute entry points refuse CPU tensors instead of computing elsewhere."""
+    import pytest
+    import torch
+
+    from quantem_b200 import ops
+
+    x = torch.zeros((1, 64, 64), dtype=torch.complex64)
+    with pytest.raises(RuntimeError, match="CUDA"):
+        ops.fft2(x)
+    with pytest.raises(RuntimeError, match="CUDA"):
+        ops.obj_constrain(x)
