@@ -271,6 +271,7 @@ def run_ours(args):
         fp32_roof = {"bound": "fp32", "achieved": round(ach, 2), "peak": round(fp32, 2), "unit": "TFLOP/s",
                      "frac": round(ach / fp32, 4), "peak_source": "measured (own FMA probe)"}
     cpu = cpu_baseline_sample(args)
+    torch_ref = torch_eager_reference(pt, args.batch_size) if not args.skip_torch_reference else None
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": "positions/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
@@ -284,6 +285,7 @@ def run_ours(args):
         "gpu_launches": launches_per_batch * nbatches,
         "roofline": roofline, "roofline_fp32": fp32_roof,
         "cpu_baseline": cpu,
+        "torch_eager_reference_gpu": torch_ref,
         "clocks": clk.summary(),
         "final_loss": float(losses[-1].item()),
     }
@@ -300,6 +302,103 @@ def _ncu_traffic():
             return json.load(fh)["dram_bytes_per_launch_full_batch"]
     except Exception:
         return None
+
+
+def torch_eager_reference(pt, batch_size, steps=3, warmup=2):
+    """Positions/s of the reference's PyTorch op sequence run eagerly on this GPU.
+
+    A restatement (not the reference's code) of what quantem's
+    Ptychography.reconstruct does per batch on device="gpu": probe
+    Gram-Schmidt, fourier_shift_expand (fft2 * ramp -> ifft2, ptycho_utils.py:128-176),
+    hard-constrained object and real/imag patch gather with int32 flat patch
+    indices (object_models.py:252-339, dataset_models.py:514-535), multislice with
+    torch.fft (ptychography_base.py:934-989), detector fft2(ortho)/|.|^2/mode
+    sum/fftshift (detector_models.py:22-30), l2_amplitude loss (908-932), autograd
+    backward, obj-grad rescale and torch.optim.Adam (optimizer_mixin.py:117-123).
+    Batches that do not fit in memory are split; the number of positions per
+    batch used is reported."""
+    import torch
+
+    from quantem_b200.diffractive_imaging.ptycho_utils import orthogonalize_probes
+
+    dev = pt.obj.device
+    obj = pt.obj.detach().clone().requires_grad_(True)
+    probe = pt.probe.detach().clone().requires_grad_(True)
+    P, n, _ = probe.shape
+    S, Ho, Wo = obj.shape
+    kr, kc = pt.prop
+    prop = (kr[:, :, None] * kc[:, None, :]).contiguous()
+    opt_o = torch.optim.Adam([obj], lr=5e-3)
+    opt_p = torch.optim.Adam([probe], lr=1e-3)
+    pos_all = pt.positions
+    f = torch.fft.fftfreq(n, d=1 / n, device=dev)
+    kf = torch.fft.fftfreq(n, d=1.0, device=dev).to(torch.float32)
+    npos = pos_all.shape[0]
+
+    def one_batch(bi):
+        pos = pos_all[bi]
+        frac = pos - torch.round(pos)
+        r0 = torch.round(pos[:, 0]).to(torch.int32)
+        c0 = torch.round(pos[:, 1]).to(torch.int32)
+        rows = (r0[:, None, None] + f[None, :, None]) % Ho
+        cols = (c0[:, None, None] + f[None, None, :]) % Wo
+        pidx = (rows * Wo + cols).to(torch.int32).long()
+        pr = orthogonalize_probes(probe)
+        ramp = (torch.exp(-2j * torch.pi * kf[None, :, None] * frac[:, 0][:, None, None])
+                * torch.exp(-2j * torch.pi * kf[None, None, :] * frac[:, 1][:, None, None]))
+        shifted = torch.fft.ifft2(torch.fft.fft2(pr) * ramp[:, None]).swapaxes(0, 1)
+        amp = torch.clamp(torch.abs(obj), 0.0, 1.0)
+        phase = obj.angle() - obj.angle().mean()
+        oc = (amp * torch.exp(1.0j * phase)).reshape(S, -1)
+        patches = torch.complex(oc.real[:, pidx], oc.imag[:, pidx])
+        ov = patches[0] * shifted
+        for s in range(1, S):
+            ov = patches[s] * torch.fft.ifft2(torch.fft.fft2(ov) * prop[s - 1])
+        inten = torch.fft.fftshift(torch.sum(torch.abs(torch.fft.fft2(ov, norm="ortho")) ** 2, dim=0), dim=(-2, -1))
+        tg = pt.targets[bi]
+        diff = torch.sqrt(inten + 1e-9) * pt.mask - tg * pt.mask
+        loss = torch.sum(torch.abs(diff) ** 2) / (diff.shape[0] / npos) / pt.mean_intensity
+        return loss
+
+    def iteration(bs):
+        order = torch.randperm(npos, device=dev)
+        for i in range(0, npos, bs):
+            bi = order[i:i + bs]
+            opt_o.zero_grad()
+            opt_p.zero_grad()
+            loss = one_batch(bi)
+            loss.backward()
+            obj.grad.mul_(pt.upsample_factor ** 2 / 2)
+            opt_o.step()
+            opt_p.step()
+
+    bs = batch_size
+    while True:
+        try:
+            iteration(bs)
+            torch.cuda.synchronize()
+            break
+        except torch.OutOfMemoryError:
+            torch.cuda.empty_cache()
+            bs //= 2
+            if bs < 1:
+                return None
+    for _ in range(warmup - 1):
+        iteration(bs)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        iteration(bs)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    del opt_o, opt_p, obj, probe
+    torch.cuda.empty_cache()
+    return {"value": round(npos / (ms * 1e-3), 1), "unit": "positions/s", "batch_size": bs,
+            "ms_per_step": round(ms, 2),
+            "what": "PyTorch-eager restatement of the reference's per-batch op sequence (torch.fft/cuFFT, "
+                    "autograd, torch.optim.Adam) on this GPU"}
 
 
 def cpu_baseline_sample(args, positions=8):
@@ -384,6 +483,8 @@ def main():
     ap.add_argument("--batch-size", type=int, default=4096)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--kernel-only", action="store_true", help="time only the fused batch kernel")
+    ap.add_argument("--skip-torch-reference", action="store_true",
+                    help="do not time the PyTorch-eager restatement of the reference path")
     ap.add_argument("--positions", type=int, default=296, help="positions per launch with --kernel-only")
     ap.add_argument("--variant", default="auto", choices=["auto", "serial", "cluster"],
                     help="mapping of probe modes onto CTAs (--kernel-only)")

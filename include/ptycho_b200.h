@@ -66,7 +66,8 @@ typedef struct ptycho_batch_args {
   const float* mask;         /* float32 (N, N): detector mask, detector layout */
   void* grad_obj;            /* complex64 (S, Ho, Wo): object gradient, accumulated (adjoint only) */
   void* probe_grad_part;     /* complex64 (grid, P, N, N): per-CTA partials (adjoint only) */
-  void* scratch;             /* complex64 (grid, P*S + P, N, N) (adjoint only) */
+  void* scratch;             /* complex64 (grid, P*S + P + 1, N, N) serial / (grid, S, N, N) cluster
+                                (adjoint only); size it with ptycho_batch_plan */
   double* loss_part;         /* float64 (grid,): per-CTA loss partials */
   float* out_intensity;      /* optional float32 (B, N, N): predicted intensities, detector layout */
   void* out_exit;            /* optional complex64 (P, B, N, N): exit waves */

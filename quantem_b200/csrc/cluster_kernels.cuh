@@ -137,8 +137,7 @@ __global__ void __launch_bounds__(4 * N, 1) cluster_batch_kernel(const BatchPara
 #pragma unroll
           for (int e = 0; e < E; ++e) ow[f.s1_col(e)] = x[e];
         }
-#pragma unroll
-        for (int e = 0; e < E; ++e) x[e] = cmul(x[e], __ldg(orow_ptr + colmap[f.s1_col(e)]));
+        gather_mul<N, false>(f, x, orow_ptr, colmap);
         if (s == S - 1 && p.out_exit) {
           float2* oe = p.out_exit + ((size_t)m * p.B + b) * NN + (size_t)f.s1_r * N;
 #pragma unroll
@@ -151,7 +150,13 @@ __global__ void __launch_bounds__(4 * N, 1) cluster_batch_kernel(const BatchPara
         const float2* wv = slot + (size_t)s * NN;
         __syncthreads();  // exchange buffer free (the inverse finished reading it)
 #pragma unroll
-        for (int e = 0; e < E; ++e) sm[f.s1_r * PITCH + f.s1_col(e)] = cmulc(x[e], wv[e * T + tid]);
+        for (int e0 = 0; e0 < E; e0 += 8) {
+          float2 ps[8];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) ps[j] = wv[(e0 + j) * T + tid];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) sm[f.s1_r * PITCH + f.s1_col(e0 + j)] = cmulc(x[e0 + j], ps[j]);
+        }
         cluster.sync();  // every mode's contribution tile is in place
         float2* grow_s = p.grad_obj + (size_t)s * HoWo;
         const int nel = (row_hi - row_lo) * N;
@@ -162,8 +167,7 @@ __global__ void __launch_bounds__(4 * N, 1) cluster_batch_kernel(const BatchPara
           atomicAdd(grow_s + (size_t)rowmap[r] * p.Wo + colmap[c], a);
         }
         cluster.sync();  // all tiles read before any exchange buffer is reused
-#pragma unroll
-        for (int e = 0; e < E; ++e) x[e] = cmulc(x[e], __ldg(orow_ptr + colmap[f.s1_col(e)]));
+        gather_mul<N, true>(f, x, orow_ptr, colmap);
       }
       f.forward(x, sm, tw);
       // ---------------- Fourier space (S3 layout) ----------------
@@ -215,14 +219,7 @@ __global__ void __launch_bounds__(4 * N, 1) cluster_batch_kernel(const BatchPara
         continue;
       }
       // probe-shift adjoint: conj(ramp) * fft2(g0) into this CTA's partial
-#pragma unroll
-      for (int g = 0; g < G3; ++g)
-#pragma unroll
-        for (int e = 0; e < D; ++e) {
-          const int kr = f.s3_row(g, e), kc = f.s3_c;
-          const size_t idx = (size_t)kr * N + kc;
-          pgrad[idx] = cadd(pgrad[idx], cmulc(x[g * D + e], cmul(rowf[kr], colf[kc])));
-        }
+      accumulate_probe_grad<N>(f, x, pgrad, rowf, colf);
       break;
     }
   }

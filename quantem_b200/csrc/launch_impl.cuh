@@ -48,11 +48,15 @@ size_t batch_smem(const ptycho_batch_args* a) {
 template <int N>
 int launch_serial(const ptycho_batch_args* a, bool adj, cudaStream_t st) {
   const BatchParams p = to_params(a);
-  const size_t smem = batch_smem<N>(a);
+  const size_t smem = adj ? batch_smem_bytes<N, true>(a->prop_r != nullptr, a->S)
+                          : batch_smem_bytes<N, false>(a->prop_r != nullptr, a->S);
   // the attribute is per device; setting it on every launch keeps multi-device
   // processes correct and costs far less than one launch
   if (adj) {
     cudaFuncSetAttribute(fused_batch_kernel<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // smallest shared-memory carve-out that fits: the rest of the 256 KB is L1 for spills
+    cudaFuncSetAttribute(fused_batch_kernel<N, true>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         (int)((smem + 1024) * 100 / (228 * 1024) + 1));
     fused_batch_kernel<N, true><<<a->grid, 4 * N, smem, st>>>(p);
   } else {
     cudaFuncSetAttribute(fused_batch_kernel<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -109,6 +113,8 @@ int launch_cluster(const ptycho_batch_args* a, bool adj, cudaStream_t st) {
   if (adj) {
     cudaFuncSetAttribute(cluster_batch_kernel<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)batch_smem<N>(a));
+    cudaFuncSetAttribute(cluster_batch_kernel<N, true>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         (int)((batch_smem<N>(a) + 1024) * 100 / (228 * 1024) + 1));
     cudaLaunchConfig_t cfg = cluster_config<N, true>(a, a->grid, st, attr);
     e = cudaLaunchKernelEx(&cfg, cluster_batch_kernel<N, true>, p);
   } else {

@@ -309,7 +309,7 @@ int ptycho_sm_count(int* out) {
 int ptycho_workspace_elems(int n, int S, int P, int grid, int64_t* scratch_elems, int64_t* partial_elems) {
   if (n < 1 || S < 1 || P < 1 || grid < 1) return fail(PTYCHO_ERR_INVALID, "bad workspace sizes");
   const int64_t nn = (int64_t)n * n;
-  if (scratch_elems) *scratch_elems = (int64_t)grid * (P * S + P) * nn;
+  if (scratch_elems) *scratch_elems = (int64_t)grid * (P * S + P + 1) * nn;
   if (partial_elems) *partial_elems = (int64_t)grid * P * nn;
   return PTYCHO_OK;
 }
@@ -340,7 +340,7 @@ int ptycho_batch_plan(const ptycho_batch_args* a, int adjoint, int* variant, int
   } else {
     g = B < sms ? B : sms;
     parts = g;
-    scr = (int64_t)g * (a->P * a->S + a->P) * nn;
+    scr = (int64_t)g * (a->P * a->S + a->P + 1) * nn;  // waves, far fields, intensity tile
     part = (int64_t)g * a->P * nn;
   }
   if (variant) *variant = v;

@@ -77,6 +77,13 @@ template <int N>
 constexpr size_t fused_smem_bytes_sep(int S) {
   return fused_smem_bytes<N>() + sizeof(float2) * (size_t)2 * N * (size_t)(S > 1 ? S - 1 : 0);
 }
+// The adjoint kernel keeps its intensity / dL/dI tile in its global scratch slot
+// (L2-resident, 64 KB per CTA at 128^2) instead of shared memory; the 64 KB left
+// to the L1 cache hold the register spills of the 512-thread CTA.
+template <int N, bool ADJ>
+constexpr size_t batch_smem_bytes(bool sep, int S) {
+  return (sep ? fused_smem_bytes_sep<N>(S) : fused_smem_bytes<N>()) - (ADJ ? sizeof(float) * (size_t)N * N : 0);
+}
 
 template <int N>
 __device__ __forceinline__ void loss_elem(const BatchParams& p, float I, float t, float m,
@@ -146,6 +153,43 @@ __device__ __forceinline__ void apply_prop(const Fft2<N>& f, float2 (&x)[Fft2<N>
   }
 }
 
+// x (S1 layout) *= o (CONJ: conj(o)) for the object row orow_ptr, columns through
+// colmap.  Loads go in batches of 8 so that a batch is in flight at once while
+// the wave occupies half of the register file.
+template <int N, bool CONJ>
+__device__ __forceinline__ void gather_mul(const Fft2<N>& f, float2 (&x)[Fft2<N>::E], const float2* orow_ptr,
+                                           const int* colmap) {
+  constexpr int E = Fft2<N>::E;
+#pragma unroll
+  for (int e0 = 0; e0 < E; e0 += 8) {
+    float2 ob[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) ob[j] = __ldg(orow_ptr + colmap[f.s1_col(e0 + j)]);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) x[e0 + j] = CONJ ? cmulc(x[e0 + j], ob[j]) : cmul(x[e0 + j], ob[j]);
+  }
+}
+
+// Fourier-space probe-gradient partial (S3 layout): pg += conj(ramp) * x, batched RMW.
+template <int N>
+__device__ __forceinline__ void accumulate_probe_grad(const Fft2<N>& f, const float2 (&x)[Fft2<N>::E], float2* pg,
+                                                      const float2* rowf, const float2* colf) {
+  constexpr int D = Fft2<N>::D, G3 = Fft2<N>::G3;
+#pragma unroll
+  for (int g = 0; g < G3; ++g)
+#pragma unroll
+    for (int e0 = 0; e0 < D; e0 += 8) {
+      float2 old[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) old[j] = pg[(size_t)f.s3_row(g, e0 + j) * N + f.s3_c];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int kr = f.s3_row(g, e0 + j), kc = f.s3_c;
+        pg[(size_t)kr * N + kc] = cadd(old[j], cmulc(x[g * D + e0 + j], cmul(rowf[kr], colf[kc])));
+      }
+    }
+}
+
 template <int N, bool ADJ>
 __global__ void __launch_bounds__(4 * N, 1) fused_batch_kernel(const BatchParams p) {
   using F = Fft2<N>;
@@ -155,8 +199,9 @@ __global__ void __launch_bounds__(4 * N, 1) fused_batch_kernel(const BatchParams
   float2* tw = sm + F::SM_FLOAT2;
   float2* rowf = tw + N;
   float2* colf = rowf + N;
-  float* inten = reinterpret_cast<float*>(colf + N);
-  int* rowmap = reinterpret_cast<int*>(inten + N * N);
+  // intensity / dL/dI tile: shared memory (forward-only) or the CTA's scratch slot (ADJ)
+  float* inten_sm = reinterpret_cast<float*>(colf + N);
+  int* rowmap = reinterpret_cast<int*>(ADJ ? reinterpret_cast<float*>(colf + N) : inten_sm + N * N);
   int* colmap = rowmap + N;
   // separable propagators K_s[kr][kc] = Kr_s[kr] * Kc_s[kc] (probe_models.py:376-427
   // builds exp(-i pi lambda dz (kr^2 + kc^2)) times per-axis tilt ramps)
@@ -184,7 +229,8 @@ __global__ void __launch_bounds__(4 * N, 1) fused_batch_kernel(const BatchParams
   const size_t NN = (size_t)N * N;
   const int S = p.S, P = p.P;
   const size_t HoWo = (size_t)p.Ho * p.Wo;
-  float2* slot = ADJ ? p.scratch + (size_t)blockIdx.x * (size_t)(P * S + P) * NN : nullptr;
+  float2* slot = ADJ ? p.scratch + (size_t)blockIdx.x * (size_t)(P * S + P + 1) * NN : nullptr;
+  float* inten = ADJ ? reinterpret_cast<float*>(slot + (size_t)(P * S + P) * NN) : inten_sm;
   float2* pgrad = ADJ ? p.probe_grad_part + (size_t)blockIdx.x * (size_t)P * NN : nullptr;
   if (ADJ) {
     for (int m = 0; m < P; ++m)
@@ -255,9 +301,7 @@ __global__ void __launch_bounds__(4 * N, 1) fused_batch_kernel(const BatchParams
 #pragma unroll
           for (int e = 0; e < E; ++e) ow[f.s1_col(e)] = x[e];
         }
-        const float2* orow_ptr = p.obj + (size_t)s * HoWo + (size_t)orow * p.Wo;
-#pragma unroll
-        for (int e = 0; e < E; ++e) x[e] = cmul(x[e], __ldg(orow_ptr + colmap[f.s1_col(e)]));
+        gather_mul<N, false>(f, x, p.obj + (size_t)s * HoWo + (size_t)orow * p.Wo, colmap);
         if (s < S - 1) {
           f.forward(x, sm, tw);
           apply_prop<N, false>(f, x, p, s, sep, sKr, sKc);
@@ -316,10 +360,20 @@ __global__ void __launch_bounds__(4 * N, 1) fused_batch_kernel(const BatchParams
           const float2* orow_ptr = p.obj + (size_t)s * HoWo + (size_t)orow * p.Wo;
           float2* grow = p.grad_obj + (size_t)s * HoWo + (size_t)orow * p.Wo;
 #pragma unroll
-          for (int e = 0; e < E; ++e) {
-            const int col = colmap[f.s1_col(e)];
-            atomicAdd(grow + col, cmulc(x[e], wv[e * T + tid]));  // conj(psi) * g
-            x[e] = cmulc(x[e], __ldg(orow_ptr + col));            // conj(o) * g
+          for (int e0 = 0; e0 < E; e0 += 8) {
+            float2 ps[8], ob[8];
+            int col[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+              col[j] = colmap[f.s1_col(e0 + j)];
+              ps[j] = wv[(e0 + j) * T + tid];
+              ob[j] = __ldg(orow_ptr + col[j]);
+            }
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+              atomicAdd(grow + col[j], cmulc(x[e0 + j], ps[j]));  // conj(psi) * g
+              x[e0 + j] = cmulc(x[e0 + j], ob[j]);                // conj(o) * g
+            }
           }
           if (s > 0) {
             f.forward(x, sm, tw);
@@ -331,15 +385,7 @@ __global__ void __launch_bounds__(4 * N, 1) fused_batch_kernel(const BatchParams
         }
         // probe-shift adjoint: accumulate conj(ramp) * fft2(g0)
         f.forward(x, sm, tw);
-        float2* pg = pgrad + (size_t)m * NN;
-#pragma unroll
-        for (int g = 0; g < G3; ++g)
-#pragma unroll
-          for (int e = 0; e < D; ++e) {
-            const int kr = f.s3_row(g, e), kc = f.s3_c;
-            const size_t idx = (size_t)kr * N + kc;
-            pg[idx] = cadd(pg[idx], cmulc(x[g * D + e], cmul(rowf[kr], colf[kc])));
-          }
+        accumulate_probe_grad<N>(f, x, pgrad + (size_t)m * NN, rowf, colf);
       }
     }
   }

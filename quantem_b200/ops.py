@@ -221,7 +221,7 @@ def plan_and_bind(a, device, adjoint: bool, grid=None):
             raise ValueError("an explicit grid is only accepted with variant='serial'")
         grid_v = parts_v = int(grid)
         nn = a.n * a.n
-        se.value, pe.value = grid_v * (a.P * a.S + a.P) * nn, grid_v * a.P * nn
+        se.value, pe.value = grid_v * (a.P * a.S + a.P + 1) * nn, grid_v * a.P * nn
     ws = workspace(device).ensure(se.value if adjoint else 0, pe.value if adjoint else 0, grid_v)
     a.grid = grid_v
     a.scratch = ws.scratch.data_ptr() if adjoint else None
