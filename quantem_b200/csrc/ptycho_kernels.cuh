@@ -268,17 +268,15 @@ __global__ void __launch_bounds__(4 * N, 1) fused_batch_kernel(const BatchParams
         colmap[kk] = wrap_index(c0 + fsigned(kk, N), p.Wo);
       }
     }
-#pragma unroll
-    for (int g = 0; g < G3; ++g)
-#pragma unroll
-      for (int e = 0; e < D; ++e) inten[(g * D + e) * T + tid] = 0.f;
     __syncthreads();
     const int orow = rowmap[f.s1_r];
 
-    // ------------------------------ forward ------------------------------
-    for (int m = 0; m < P; ++m) {
-      float2 x[E];
-      const float2* ph = p.probe_hat + (size_t)m * NN;
+    // One loop with a single inverse and a single forward transform site walks
+    // the forward chains of all modes, the loss, and (ADJ) the reverse chains.
+    // x always enters the loop top in S3 (Fourier) layout.
+    float2 x[E];
+    auto load_probe = [&](int mm) {
+      const float2* ph = p.probe_hat + (size_t)mm * NN;
 #pragma unroll
       for (int g = 0; g < G3; ++g)
 #pragma unroll
@@ -286,11 +284,23 @@ __global__ void __launch_bounds__(4 * N, 1) fused_batch_kernel(const BatchParams
           const int kr = f.s3_row(g, e), kc = f.s3_c;
           x[g * D + e] = cmul(cmul(__ldg(ph + (size_t)kr * N + kc), rowf[kr]), colf[kc]);
         }
-      f.inverse(x, sm, tw);
+    };
+    // far field of mode mm times 2 dL/dI (start of the adjoint chain)
+    auto load_far_seed = [&](int mm) {
+      const float2* fw = slot + (size_t)(P * S + mm) * NN;
 #pragma unroll
-      for (int e = 0; e < E; ++e) x[e] = cscale(x[e], inv_n2);
-
-      for (int s = 0; s < S; ++s) {
+      for (int e = 0; e < E; ++e) x[e] = cscale(fw[e * T + tid], 2.0f * inten[e * T + tid]);
+    };
+    int m = 0, s = 0;
+    bool bwd = false, first_bwd = false;
+    load_probe(0);
+    while (true) {
+      f.inverse(x, sm, tw);
+      // ---------------- real space (S1 layout) ----------------
+      const float2* orow_ptr = p.obj + (size_t)s * HoWo + (size_t)orow * p.Wo;
+      if (!bwd) {
+#pragma unroll
+        for (int e = 0; e < E; ++e) x[e] = cscale(x[e], inv_n2);
         if (ADJ) {
           float2* wv = slot + (size_t)(m * S + s) * NN;
 #pragma unroll
@@ -301,92 +311,97 @@ __global__ void __launch_bounds__(4 * N, 1) fused_batch_kernel(const BatchParams
 #pragma unroll
           for (int e = 0; e < E; ++e) ow[f.s1_col(e)] = x[e];
         }
-        gather_mul<N, false>(f, x, p.obj + (size_t)s * HoWo + (size_t)orow * p.Wo, colmap);
-        if (s < S - 1) {
-          f.forward(x, sm, tw);
-          apply_prop<N, false>(f, x, p, s, sep, sKr, sKc);
-          f.inverse(x, sm, tw);
+        gather_mul<N, false>(f, x, orow_ptr, colmap);
+        if (s == S - 1 && p.out_exit) {
+          float2* oe = p.out_exit + ((size_t)m * p.B + b) * NN + (size_t)f.s1_r * N;
 #pragma unroll
-          for (int e = 0; e < E; ++e) x[e] = cscale(x[e], inv_n2);
+          for (int e = 0; e < E; ++e) oe[f.s1_col(e)] = x[e];
         }
-      }
-      if (p.out_exit) {
-        float2* oe = p.out_exit + ((size_t)m * p.B + b) * NN + (size_t)f.s1_r * N;
+      } else {
+        const float sc = first_bwd ? inv_n : inv_n2;  // adjoint of the orthonormal FFT, or of a propagation
+        const float2* wv = slot + (size_t)(m * S + s) * NN;
+        float2* grow = p.grad_obj + (size_t)s * HoWo + (size_t)orow * p.Wo;
 #pragma unroll
-        for (int e = 0; e < E; ++e) oe[f.s1_col(e)] = x[e];
+        for (int e0 = 0; e0 < E; e0 += 8) {
+          float2 ps[8], ob[8];
+          int col[8];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            col[j] = colmap[f.s1_col(e0 + j)];
+            ps[j] = wv[(e0 + j) * T + tid];
+            ob[j] = __ldg(orow_ptr + col[j]);
+          }
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const float2 g = cscale(x[e0 + j], sc);
+            atomicAdd(grow + col[j], cmulc(g, ps[j]));  // conj(psi) * g
+            x[e0 + j] = cmulc(g, ob[j]);                 // conj(o) * g
+          }
+        }
       }
       f.forward(x, sm, tw);
-#pragma unroll
-      for (int e = 0; e < E; ++e) x[e] = cscale(x[e], inv_n);  // orthonormal detector FFT
-      if (ADJ) {
-        float2* fw = slot + (size_t)(P * S + m) * NN;
-#pragma unroll
-        for (int e = 0; e < E; ++e) fw[e * T + tid] = x[e];
-      }
-#pragma unroll
-      for (int e = 0; e < E; ++e) inten[e * T + tid] += cabs2(x[e]);
-    }
-
-    // ------------------------------ loss ------------------------------
-    {
-      const float* tg = p.targets + (size_t)gi * NN;
-#pragma unroll
-      for (int g = 0; g < G3; ++g)
-#pragma unroll
-        for (int e = 0; e < D; ++e) {
-          const int kr = f.s3_row(g, e), kc = f.s3_c;
-          const int di = ((kr + N / 2) & (N - 1)) * N + ((kc + N / 2) & (N - 1));
-          const float I = inten[(g * D + e) * T + tid];
-          if (!isfinite(I)) ++nonfinite;
-          float dldi;
-          loss_elem<N>(p, I, __ldg(tg + di), __ldg(p.mask + di), loss_acc, dldi);
-          inten[(g * D + e) * T + tid] = dldi;
-          if (p.out_intensity) p.out_intensity[(size_t)b * NN + di] = I;
+      // ---------------- Fourier space (S3 layout) ----------------
+      if (!bwd) {
+        if (s < S - 1) {
+          apply_prop<N, false>(f, x, p, s, sep, sKr, sKc);
+          ++s;
+          continue;
         }
-    }
-
-    // ------------------------------ adjoint ------------------------------
-    if (ADJ) {
-      for (int m = 0; m < P; ++m) {
-        float2 x[E];
-        const float2* fw = slot + (size_t)(P * S + m) * NN;
 #pragma unroll
-        for (int e = 0; e < E; ++e) x[e] = cscale(fw[e * T + tid], 2.0f * inten[e * T + tid]);
-        f.inverse(x, sm, tw);
+        for (int e = 0; e < E; ++e) x[e] = cscale(x[e], inv_n);  // orthonormal detector FFT
+        if (ADJ) {
+          float2* fw = slot + (size_t)(P * S + m) * NN;
 #pragma unroll
-        for (int e = 0; e < E; ++e) x[e] = cscale(x[e], inv_n);  // adjoint of the orthonormal FFT
-        for (int s = S - 1; s >= 0; --s) {
-          const float2* wv = slot + (size_t)(m * S + s) * NN;
-          const float2* orow_ptr = p.obj + (size_t)s * HoWo + (size_t)orow * p.Wo;
-          float2* grow = p.grad_obj + (size_t)s * HoWo + (size_t)orow * p.Wo;
-#pragma unroll
-          for (int e0 = 0; e0 < E; e0 += 8) {
-            float2 ps[8], ob[8];
-            int col[8];
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-              col[j] = colmap[f.s1_col(e0 + j)];
-              ps[j] = wv[(e0 + j) * T + tid];
-              ob[j] = __ldg(orow_ptr + col[j]);
-            }
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-              atomicAdd(grow + col[j], cmulc(x[e0 + j], ps[j]));  // conj(psi) * g
-              x[e0 + j] = cmulc(x[e0 + j], ob[j]);                // conj(o) * g
-            }
-          }
-          if (s > 0) {
-            f.forward(x, sm, tw);
-            apply_prop<N, true>(f, x, p, s - 1, sep, sKr, sKc);
-            f.inverse(x, sm, tw);
-#pragma unroll
-            for (int e = 0; e < E; ++e) x[e] = cscale(x[e], inv_n2);
-          }
+          for (int e = 0; e < E; ++e) fw[e * T + tid] = x[e];
         }
-        // probe-shift adjoint: accumulate conj(ramp) * fft2(g0)
-        f.forward(x, sm, tw);
-        accumulate_probe_grad<N>(f, x, pgrad + (size_t)m * NN, rowf, colf);
+#pragma unroll
+        for (int e = 0; e < E; ++e) inten[e * T + tid] = (m == 0 ? 0.f : inten[e * T + tid]) + cabs2(x[e]);
+        if (m < P - 1) {
+          ++m;
+          s = 0;
+          load_probe(m);
+          continue;
+        }
+        // loss over the mode-summed intensity (each thread owns its S3 slots)
+        {
+          const float* tg = p.targets + (size_t)gi * NN;
+#pragma unroll
+          for (int g = 0; g < G3; ++g)
+#pragma unroll
+            for (int e = 0; e < D; ++e) {
+              const int kr = f.s3_row(g, e), kc = f.s3_c;
+              const int di = ((kr + N / 2) & (N - 1)) * N + ((kc + N / 2) & (N - 1));
+              const float I = inten[(g * D + e) * T + tid];
+              if (!isfinite(I)) ++nonfinite;
+              float dldi;
+              loss_elem<N>(p, I, __ldg(tg + di), __ldg(p.mask + di), loss_acc, dldi);
+              inten[(g * D + e) * T + tid] = dldi;
+              if (p.out_intensity) p.out_intensity[(size_t)b * NN + di] = I;
+            }
+        }
+        if (!ADJ) break;
+        bwd = true;
+        first_bwd = true;
+        m = 0;
+        s = S - 1;
+        load_far_seed(0);
+        continue;
       }
+      first_bwd = false;
+      if (s > 0) {
+        apply_prop<N, true>(f, x, p, s - 1, sep, sKr, sKc);
+        --s;
+        continue;
+      }
+      accumulate_probe_grad<N>(f, x, pgrad + (size_t)m * NN, rowf, colf);
+      if (m < P - 1) {
+        ++m;
+        s = S - 1;
+        first_bwd = true;
+        load_far_seed(m);
+        continue;
+      }
+      break;
     }
   }
 
