@@ -80,6 +80,10 @@ typedef struct ptycho_batch_args {
   float loss_scale;          /* npos_total / (B * mean_intensity) */
   float inv_mean_intensity;  /* 1 / mean_intensity */
   int variant;               /* PTYCHO_VARIANT_*: how probe modes map onto CTAs */
+  int analytic;              /* adjoint launch: 0 = autograd gradients, 1 = analytic update directions
+                                (serial variant; needs an_norm and the partials in real space) */
+  float* an_norm;            /* analytic: float32 (S, P, Ho, Wo) zero-initialised accumulator of
+                                sum_patches(|psi|^2) */
 } ptycho_batch_args;
 
 enum {
@@ -146,6 +150,19 @@ int ptycho_adam_step(float* param, const float* grad, float* exp_avg, float* exp
 /* torch.optim.SGD step without momentum: param -= lr * (grad + wd * param). */
 int ptycho_sgd_step(float* param, const float* grad, int64_t count, float lr, const float* lr_dev,
                     float weight_decay, void* stream);
+
+/* Analytic (autograd=False) update, finalisation steps after an analytic adjoint launch
+ * (a->analytic = 1; object_models.py:686-725, probe_models.py:774-783):
+ *   ptycho_patch_energy_max        out[0] = max over slices and batch positions of sum |o_patch|^2
+ *                                  (the probe update's obj_normalization);
+ *   ptycho_analytic_obj_finalize   out[s] = -upd[s] / sum_p max(norm[s, p]) with maxes (S*P floats) as work;
+ *   ptycho_analytic_probe_finalize probe_grad *= -1 / (obj_norm[0] * ortho_norm). */
+int ptycho_patch_energy_max(const void* obj, const float* positions, const int64_t* batch_idx, int S, int Ho,
+                            int Wo, int n, int B, int npos, float* out, void* stream);
+int ptycho_analytic_obj_finalize(const void* upd, const float* norm, float* maxes, int S, int P, int64_t plane,
+                                 void* out, void* stream);
+int ptycho_analytic_probe_finalize(void* probe_grad, int64_t count, const float* obj_norm, float ortho_norm,
+                                   void* stream);
 
 /* Measurement utility (no reference counterpart): FP32 FMA throughput probe used to
  * state the FP32-pipe roofline.  `out` holds blocks * 512 floats; each thread runs

@@ -471,3 +471,57 @@ def reconstruct(obj_raw, probe_raw, positions_px, props, targets, mask, mean_int
             nb += 1
         losses.append(tot / nb)
     return obj, probe, np.array(losses)
+
+
+# ----------------------------------------------------------------------------
+# analytic (autograd=False) update directions
+# ----------------------------------------------------------------------------
+
+def fourier_projection_seed(far: np.ndarray, targets: np.ndarray) -> np.ndarray:
+    """Fourier-space seed m(Psi) - Psi of the analytic update (ptychography.py:350-372).
+
+    ``far`` is the orthonormal far field (P, B, H, W), ``targets`` the measured
+    amplitudes in detector (centred) layout.  One mode: measured amplitude with
+    the estimated phase; several modes: Psi * measured / estimated amplitude with
+    the estimate sqrt(sum_p |Psi_p + 1e-9|^2) (ptychography_base.py:949-961) and
+    zero estimates mapped to infinity.  Returns (mod - Psi) in Fourier space.
+    """
+    meas = np.fft.fftshift(targets, axes=(-2, -1))[None]
+    P = far.shape[0]
+    if P == 1:
+        mod = meas * np.exp(1j * np.angle(far))
+    else:
+        amps = np.sqrt(np.sum(np.abs(far + 1e-9) ** 2, axis=0))
+        amps = np.where(amps == 0, np.inf, amps)
+        mod = (meas / amps) * far
+    return mod - far
+
+
+def analytic_gradients(obj_raw, probe_raw, positions_px, props, targets, orthogonalize=False):
+    """Object and probe update directions of the analytic path, as
+    ``Ptychography.backward(autograd=False)`` leaves them in ``.grad``
+    (ptychography.py:339-348, object_models.py:686-725, probe_models.py:774-783).
+    """
+    obj_c = constrain_object(obj_raw)
+    probe_o = gram_schmidt(probe_raw)[0] if orthogonalize else probe_raw
+    S = obj_c.shape[0]
+    P, H, W = probe_o.shape
+    st = forward(obj_c, probe_o, positions_px, props)
+    grad = ifft2(fourier_projection_seed(st.far, targets), norm="ortho")
+    g_obj = np.zeros(obj_c.shape, dtype=obj_c.dtype)
+    for s in reversed(range(S)):
+        psi = st.waves[s]
+        norm = 0.0
+        upd = np.zeros(obj_c.shape[1:], dtype=obj_c.dtype)
+        for a in range(P):
+            inten = scatter_patches((np.abs(psi[a]) ** 2)[None], st.rows, st.cols, (1,) + obj_c.shape[1:])[0]
+            norm += inten.max()
+            upd += scatter_patches((np.conj(psi[a]) * grad[a])[None], st.rows, st.cols, (1,) + obj_c.shape[1:])[0]
+        g_obj[s] = upd / norm
+        grad = np.conj(st.patches[s])[None] * grad
+        if s > 0:
+            grad = ifft2(fft2(grad) * np.conj(props[s - 1])[None, None])
+    obj_norm = np.max(np.sum(np.abs(st.patches) ** 2, axis=(-2, -1)))
+    ortho_norm = 2 * np.sqrt(H * W) if P == 1 else 1 / (2 * np.sqrt(H * W))
+    g_probe = np.sum(grad, axis=1) / obj_norm / ortho_norm
+    return -g_obj, -g_probe, st

@@ -42,6 +42,9 @@ EXPORTED = (
     "ptycho_reduce_blocks",
     "ptycho_adam_step",
     "ptycho_sgd_step",
+    "ptycho_patch_energy_max",
+    "ptycho_analytic_obj_finalize",
+    "ptycho_analytic_probe_finalize",
     "ptycho_fp32_fma_probe",
     "ptycho_forward_loss_noalloc",
 )
@@ -63,6 +66,7 @@ class BatchArgs(ctypes.Structure):
         ("n", _int), ("S", _int), ("P", _int), ("B", _int), ("Ho", _int), ("Wo", _int),
         ("npos", _int), ("grid", _int), ("loss_type", _int),
         ("loss_scale", _flt), ("inv_mean_intensity", _flt), ("variant", _int),
+        ("analytic", _int), ("an_norm", _vp),
     ]
 
 
@@ -90,6 +94,9 @@ def _declare(lib):
                                     _vp]),
         "ptycho_sgd_step": (_int, [_vp, _vp, _i64, _flt, _vp, _flt, _vp]),
         "ptycho_fp32_fma_probe": (_int, [_vp, _int, _int, _vp]),
+        "ptycho_patch_energy_max": (_int, [_vp, _vp, _vp, _int, _int, _int, _int, _int, _int, _vp, _vp]),
+        "ptycho_analytic_obj_finalize": (_int, [_vp, _vp, _vp, _int, _int, _i64, _vp, _vp]),
+        "ptycho_analytic_probe_finalize": (_int, [_vp, _i64, _vp, _flt, _vp]),
         "ptycho_forward_loss_noalloc": (_int, [ctypes.POINTER(BatchArgs), _vp, _vp]),
     }
     for name, (res, args) in sig.items():

@@ -36,6 +36,8 @@ inline BatchParams to_params(const ptycho_batch_args* a) {
   p.loss_scale = a->loss_scale;
   p.inv_mean_intensity = a->inv_mean_intensity;
   p.loss_type = a->loss_type;
+  p.analytic = a->analytic;
+  p.an_norm = a->an_norm;
   return p;
 }
 

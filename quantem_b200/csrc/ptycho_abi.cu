@@ -192,6 +192,65 @@ __global__ void sgd_kernel(float* __restrict__ p, const float* __restrict__ g, i
   }
 }
 
+// ---------------------------------------------------------------------------
+// analytic update finalisation (object_models.py:686-725, probe_models.py:774-783)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void atomic_max_nonneg(float* addr, float v) {
+  atomicMax(reinterpret_cast<int*>(addr), __float_as_int(v));  // ordered like floats for v >= 0
+}
+
+// max over (slice, position) of the summed |o|^2 of each object patch
+__global__ void patch_energy_max_kernel(const float2* __restrict__ obj, const float* __restrict__ positions,
+                                        const int64_t* __restrict__ batch_idx, int S, int Ho, int Wo, int n, int B,
+                                        int npos, float* out) {
+  __shared__ double red[32];
+  for (int b = blockIdx.x; b < B; b += gridDim.x) {
+    const int64_t gi = batch_idx[b];
+    if (gi < 0 || gi >= npos) continue;
+    const int r0 = qb::wrap_index((int)rintf(positions[2 * gi]), Ho);
+    const int c0 = qb::wrap_index((int)rintf(positions[2 * gi + 1]), Wo);
+    for (int s = 0; s < S; ++s) {
+      double v = 0.0;
+      for (int i = threadIdx.x; i < n * n; i += blockDim.x) {
+        const int r = i / n, c = i % n;
+        const int row = qb::wrap_index(r0 + qb::fsigned(r, n), Ho);
+        const int col = qb::wrap_index(c0 + qb::fsigned(c, n), Wo);
+        v += (double)qb::cabs2(obj[((size_t)s * Ho + row) * Wo + col]);
+      }
+      const double t = block_sum(v, red);
+      if (threadIdx.x == 0) atomic_max_nonneg(out, (float)t);
+    }
+  }
+}
+
+__global__ void plane_max_kernel(const float* __restrict__ a, int64_t plane, int planes, float* maxes) {
+  const int pl = blockIdx.y;
+  float v = 0.f;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < plane; i += (int64_t)gridDim.x * blockDim.x)
+    v = fmaxf(v, a[(int64_t)pl * plane + i]);
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  if ((threadIdx.x & 31) == 0) atomic_max_nonneg(maxes + pl, v);
+}
+
+__global__ void analytic_obj_kernel(const float2* __restrict__ upd, const float* __restrict__ maxes, int P,
+                                    int64_t plane, int S, float2* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (int64_t)S * plane;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int s = (int)(i / plane);
+    float nrm = 0.f;
+    for (int q = 0; q < P; ++q) nrm += maxes[s * P + q];
+    const float2 u = upd[i];
+    out[i] = make_float2(-u.x / nrm, -u.y / nrm);
+  }
+}
+
+__global__ void analytic_probe_kernel(float2* __restrict__ x, int64_t count, const float* __restrict__ obj_norm,
+                                      float ortho_norm) {
+  const float sc = -1.0f / (obj_norm[0] * ortho_norm);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x)
+    x[i] = make_float2(x[i].x * sc, x[i].y * sc);
+}
+
 // FP32 FMA throughput probe: 16 independent dependent-FMA chains per thread.
 __global__ void __launch_bounds__(512) fma_probe_kernel(float* out, int iters) {
   float a[16];
@@ -256,6 +315,12 @@ int validate_batch(const ptycho_batch_args* a, bool adj) {
   for (const void* q : ptrs)
     if (q && !aligned(q, 8)) return fail(PTYCHO_ERR_INVALID, "complex buffer not 8-byte aligned");
   if (a->loss_type < 0 || a->loss_type > 4) return fail(PTYCHO_ERR_INVALID, "bad loss type %d", a->loss_type);
+  if (a->analytic) {
+    if (!adj) return fail(PTYCHO_ERR_INVALID, "analytic is an adjoint-launch option");
+    if (!a->an_norm) return fail(PTYCHO_ERR_INVALID, "analytic update needs an_norm");
+    if (a->variant == PTYCHO_VARIANT_CLUSTER)
+      return fail(PTYCHO_ERR_UNSUPPORTED, "the analytic update runs on the serial variant");
+  }
   return PTYCHO_OK;
 }
 
@@ -272,7 +337,7 @@ int run_batch(const ptycho_batch_args* a, void* stream, bool adj) {
   int rc = validate_batch(a, adj);
   if (rc) return rc;
   if (a->B == 0) return PTYCHO_OK;
-  const int variant = resolve_variant(a);
+  const int variant = a->analytic ? PTYCHO_VARIANT_SERIAL : resolve_variant(a);
   if (variant < 0) return fail(PTYCHO_ERR_UNSUPPORTED, "variant %d not available for P=%d", a->variant, a->P);
   if (variant == PTYCHO_VARIANT_CLUSTER && a->grid % a->P != 0)
     return fail(PTYCHO_ERR_INVALID, "cluster launch: grid %d is not a multiple of P=%d", a->grid, a->P);
@@ -319,7 +384,7 @@ int ptycho_batch_plan(const ptycho_batch_args* a, int adjoint, int* variant, int
   if (!a) return fail(PTYCHO_ERR_INVALID, "plan: args is NULL");
   if (a->n != 64 && a->n != 128) return fail(PTYCHO_ERR_UNSUPPORTED, "probe window n=%d not built (64, 128)", a->n);
   if (a->S < 1 || a->P < 1 || a->B < 0) return fail(PTYCHO_ERR_INVALID, "plan: bad sizes");
-  const int v = resolve_variant(a);
+  const int v = a->analytic ? PTYCHO_VARIANT_SERIAL : resolve_variant(a);
   if (v < 0) return fail(PTYCHO_ERR_UNSUPPORTED, "variant %d not available for P=%d", a->variant, a->P);
   int sms = 0, dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -426,6 +491,43 @@ int ptycho_adam_step(float* param, const float* grad, float* exp_avg, float* exp
   adam_kernel<<<grid_for(count, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
       param, grad, exp_avg, exp_avg_sq, count, lr, lr_dev, beta1, beta2, eps, weight_decay, decoupled, bc1, bc2_sqrt);
   return check_launch("adam_kernel");
+}
+
+int ptycho_patch_energy_max(const void* obj, const float* positions, const int64_t* batch_idx, int S, int Ho,
+                            int Wo, int n, int B, int npos, float* out, void* stream) {
+  if (!obj || !positions || !batch_idx || !out || S < 1 || Ho < 1 || Wo < 1 || n < 1 || B < 0 || npos < 1)
+    return fail(PTYCHO_ERR_INVALID, "patch_energy_max: bad arguments");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (cudaMemsetAsync(out, 0, sizeof(float), st) != cudaSuccess) return check_launch("patch_energy_max memset");
+  if (B == 0) return PTYCHO_OK;
+  const int grid = B < kReduceBlocks ? B : kReduceBlocks;
+  patch_energy_max_kernel<<<grid, 256, 0, st>>>(static_cast<const float2*>(obj), positions, batch_idx, S, Ho, Wo, n,
+                                                B, npos, out);
+  return check_launch("patch_energy_max_kernel");
+}
+
+int ptycho_analytic_obj_finalize(const void* upd, const float* norm, float* maxes, int S, int P, int64_t plane,
+                                 void* out, void* stream) {
+  if (!upd || !norm || !maxes || !out || S < 1 || P < 1 || plane < 1)
+    return fail(PTYCHO_ERR_INVALID, "analytic_obj_finalize: bad arguments");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (cudaMemsetAsync(maxes, 0, sizeof(float) * (size_t)S * P, st) != cudaSuccess)
+    return check_launch("analytic_obj_finalize memset");
+  int bx = (int)((plane + 255) / 256);
+  if (bx > 64) bx = 64;
+  plane_max_kernel<<<dim3(bx, S * P), 256, 0, st>>>(norm, plane, S * P, maxes);
+  analytic_obj_kernel<<<grid_for((int64_t)S * plane, 256), 256, 0, st>>>(static_cast<const float2*>(upd), maxes, P,
+                                                                          plane, S, static_cast<float2*>(out));
+  return check_launch("analytic_obj_finalize");
+}
+
+int ptycho_analytic_probe_finalize(void* probe_grad, int64_t count, const float* obj_norm, float ortho_norm,
+                                   void* stream) {
+  if (!probe_grad || !obj_norm || count < 0) return fail(PTYCHO_ERR_INVALID, "analytic_probe_finalize: bad arguments");
+  if (count == 0) return PTYCHO_OK;
+  analytic_probe_kernel<<<grid_for(count, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      static_cast<float2*>(probe_grad), count, obj_norm, ortho_norm);
+  return check_launch("analytic_probe_kernel");
 }
 
 int ptycho_fp32_fma_probe(float* out, int iters, int blocks, void* stream) {

@@ -58,6 +58,8 @@ struct BatchParams {
   float loss_scale;           // num_gpts / (B * mean_intensity)
   float inv_mean_intensity;   // 1 / mean_intensity (poisson)
   int loss_type;
+  int analytic;               // 0: autograd adjoint; 1: analytic update (ptychography.py:339-372), serial kernel
+  float* an_norm;             // (S, P, Ho, Wo) scatter of |psi|^2 for the analytic normalisation
 };
 
 __device__ __forceinline__ int fsigned(int k, int n) { return k < n / 2 ? k : k - n; }
@@ -285,11 +287,24 @@ __global__ void __launch_bounds__(4 * N, 1) fused_batch_kernel(const BatchParams
           x[g * D + e] = cmul(cmul(__ldg(ph + (size_t)kr * N + kc), rowf[kr]), colf[kc]);
         }
     };
-    // far field of mode mm times 2 dL/dI (start of the adjoint chain)
+    // start of the reverse chain of mode mm, in S3 layout: autograd seeds the far
+    // field times 2 dL/dI; the analytic update seeds the Fourier projection
+    // m(Psi) - Psi = Psi (f - 1) + fix (ptychography.py:357-372), f and fix
+    // stored by the loss step
+    float* tile2 = ADJ ? inten + NN : nullptr;
     auto load_far_seed = [&](int mm) {
       const float2* fw = slot + (size_t)(P * S + mm) * NN;
+      if (p.analytic) {
 #pragma unroll
-      for (int e = 0; e < E; ++e) x[e] = cscale(fw[e * T + tid], 2.0f * inten[e * T + tid]);
+        for (int e = 0; e < E; ++e) {
+          const float2 v = fw[e * T + tid];
+          const float fm1 = inten[e * T + tid] - 1.0f;
+          x[e] = make_float2(fmaf(v.x, fm1, tile2[e * T + tid]), v.y * fm1);
+        }
+      } else {
+#pragma unroll
+        for (int e = 0; e < E; ++e) x[e] = cscale(fw[e * T + tid], 2.0f * inten[e * T + tid]);
+      }
     };
     int m = 0, s = 0;
     bool bwd = false, first_bwd = false;
@@ -337,6 +352,32 @@ __global__ void __launch_bounds__(4 * N, 1) fused_batch_kernel(const BatchParams
             atomicAdd(grow + col[j], cmulc(g, ps[j]));  // conj(psi) * g
             x[e0 + j] = cmulc(g, ob[j]);                 // conj(o) * g
           }
+          if (p.analytic) {  // sum_patches(|psi|^2) of this slice and mode (object_models.py:701-703)
+            float* nrow = p.an_norm + ((size_t)s * P + m) * HoWo + (size_t)orow * p.Wo;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) atomicAdd(nrow + col[j], cabs2(ps[j]));
+          }
+        }
+        if (p.analytic && s == 0) {
+          // analytic probe update: sum over positions of the back-propagated
+          // gradient at the probe plane, no inverse shift (probe_models.py:774-783)
+          float2* pg = pgrad + (size_t)m * NN + (size_t)f.s1_r * N;
+#pragma unroll
+          for (int e0 = 0; e0 < E; e0 += 8) {
+            float2 old[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) old[j] = pg[f.s1_col(e0 + j)];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) pg[f.s1_col(e0 + j)] = cadd(old[j], x[e0 + j]);
+          }
+          if (m < P - 1) {
+            ++m;
+            s = S - 1;
+            first_bwd = true;
+            load_far_seed(m);
+            continue;
+          }
+          break;
         }
       }
       f.forward(x, sm, tw);
@@ -356,6 +397,11 @@ __global__ void __launch_bounds__(4 * N, 1) fused_batch_kernel(const BatchParams
         }
 #pragma unroll
         for (int e = 0; e < E; ++e) inten[e * T + tid] = (m == 0 ? 0.f : inten[e * T + tid]) + cabs2(x[e]);
+        if (ADJ && p.analytic) {  // sum_p |Psi_p + 1e-9|^2 (ptychography_base.py:958)
+#pragma unroll
+          for (int e = 0; e < E; ++e)
+            tile2[e * T + tid] = (m == 0 ? 0.f : tile2[e * T + tid]) + cabs2(make_float2(x[e].x + 1e-9f, x[e].y));
+        }
         if (m < P - 1) {
           ++m;
           s = 0;
@@ -374,7 +420,20 @@ __global__ void __launch_bounds__(4 * N, 1) fused_batch_kernel(const BatchParams
               const float I = inten[(g * D + e) * T + tid];
               if (!isfinite(I)) ++nonfinite;
               float dldi;
-              loss_elem<N>(p, I, __ldg(tg + di), __ldg(p.mask + di), loss_acc, dldi);
+              const float tv = __ldg(tg + di);
+              loss_elem<N>(p, I, tv, __ldg(p.mask + di), loss_acc, dldi);
+              if (ADJ && p.analytic) {
+                // factor f and additive fix of the Fourier projection seed
+                const int li = (g * D + e) * T + tid;
+                if (P == 1) {
+                  dldi = I > 0.f ? tv / sqrtf(I) : 0.f;   // t exp(i angle(Psi)) = Psi t / |Psi|
+                  tile2[li] = I > 0.f ? 0.f : tv;        // angle(0) = 0
+                } else {
+                  const float A = sqrtf(tile2[li]);
+                  dldi = A > 0.f ? tv / A : 0.f;         // zero estimate -> infinity -> factor 0
+                  tile2[li] = 0.f;
+                }
+              }
               inten[(g * D + e) * T + tid] = dldi;
               if (p.out_intensity) p.out_intensity[(size_t)b * NN + di] = I;
             }

@@ -447,8 +447,6 @@ class Ptychography:
                                        "poisson"] = "l2_amplitude"):
         """Gradient-descent iterations (ptychography.py:146-308)."""
         self._check_preprocessed()
-        if not autograd:
-            raise NotImplementedError("the analytic (autograd=False) update is not part of the B200 path yet")
         if device is not None:
             self.to(device)
         self.batch_size = batch_size
@@ -487,14 +485,25 @@ class Ptychography:
                 self.dset.apply_hard_constraints(self.obj_padding_px)
                 pos = self.dset.scan_positions_px.contiguous()
                 idx = torch.as_tensor(np.asarray(bi, dtype=np.int64)).to(dev, non_blocking=True)
-                probe_o = self.probe_model.probe
-                loss = ops.batch_loss(self.obj_model._obj, probe_o, prop, pos, idx, tg, mask, self.dset.num_gpts,
-                                      self.dset.mean_diffraction_intensity, loss_type)
-                if self.obj_model._obj.requires_grad or self.probe_model._probe.requires_grad:
-                    loss.backward()
-                    if self.obj_model._obj.grad is not None:
-                        # ptychography.py:330-332
-                        self.obj_model._obj.grad.mul_(self.dset.upsample_factor ** 2 / 2)
+                if autograd:
+                    probe_o = self.probe_model.probe
+                    loss = ops.batch_loss(self.obj_model._obj, probe_o, prop, pos, idx, tg, mask,
+                                          self.dset.num_gpts, self.dset.mean_diffraction_intensity, loss_type)
+                    if self.obj_model._obj.requires_grad or self.probe_model._probe.requires_grad:
+                        loss.backward()
+                        if self.obj_model._obj.grad is not None:
+                            # ptychography.py:330-332
+                            self.obj_model._obj.grad.mul_(self.dset.upsample_factor ** 2 / 2)
+                else:
+                    # analytic update directions (ptychography.py:339-348), no autograd graph
+                    with torch.no_grad():
+                        probe_o = self.probe_model.probe.detach().contiguous()
+                        obj_c, _ = ops.obj_constrain(self.obj_model._obj.detach().contiguous())
+                        loss, g_obj, g_probe = ops.batch_analytic(
+                            obj_c, probe_o, prop, pos, idx, tg, mask, self.dset.num_gpts,
+                            self.dset.mean_diffraction_intensity, loss_type)
+                    self.obj_model._obj.grad = g_obj
+                    self.probe_model._probe.grad = g_probe
                 for o in opts:
                     o.step()
                 total += loss.detach()

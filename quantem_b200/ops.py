@@ -336,6 +336,52 @@ def batch_forward_adjoint(obj_c, probe_o, prop, positions, batch_idx, targets, m
     return loss, grad_obj, grad_probe
 
 
+def batch_analytic(obj_c, probe_o, prop, positions, batch_idx, targets, mask, num_gpts, mean_intensity,
+                   loss_type="l2_amplitude", probe_hat=None):
+    """Analytic (autograd=False) update directions of one batch, as the reference's
+    ``Ptychography.backward(autograd=False)`` leaves them in ``_obj.grad`` and
+    ``_probe.grad`` (ptychography.py:339-372, object_models.py:686-725,
+    probe_models.py:774-783): Fourier-projection seed, reverse multislice,
+    object update / sum over modes of max(sum_patches |psi|^2), probe update =
+    minus the batch sum of the probe-plane gradient / max patch energy / the
+    reference's orthonormal-FFT factor.  Returns (loss, grad_obj, grad_probe)."""
+    geom = _check_batch_inputs(obj_c, probe_o, prop, positions, batch_idx, targets, mask)
+    B = int(batch_idx.numel())
+    dev = obj_c.device
+    if probe_hat is None:
+        probe_hat = fft2(probe_o)
+    upd = torch.zeros_like(obj_c)
+    loss = torch.zeros((), dtype=torch.float32, device=dev)
+    g_probe = torch.zeros_like(probe_o)
+    if B == 0:
+        return loss, upd, g_probe
+    an_norm = torch.zeros((geom.S, geom.P, geom.Ho, geom.Wo), dtype=torch.float32, device=dev)
+    a = _batch_args(geom, obj_c, probe_hat, prop, positions, batch_idx, targets, mask, B, loss_type,
+                    loss_scale_of(loss_type, B, num_gpts, mean_intensity), 1.0 / mean_intensity,
+                    grad_obj=upd, variant="serial")
+    a.analytic = 1
+    a.an_norm = an_norm.data_ptr()
+    grid_v, parts, ws = plan_and_bind(a, dev, adjoint=True)
+    lib = _lib.lib()
+    st = _stream()
+    _lib.check(lib.ptycho_forward_adjoint(ctypes.byref(a), st), "forward_adjoint(analytic)")
+    _lib.check(lib.ptycho_reduce_loss(_p(ws.loss_part), grid_v, _p(loss), st), "reduce_loss")
+    nn = geom.P * geom.n * geom.n
+    _lib.check(lib.ptycho_reduce_partials(_p(ws.partials), _p(g_probe), parts, nn, st), "reduce_partials")
+    obj_norm = torch.empty(1, dtype=torch.float32, device=dev)
+    _lib.check(lib.ptycho_patch_energy_max(_p(obj_c), _p(positions), _p(batch_idx), geom.S, geom.Ho, geom.Wo,
+                                           geom.n, B, geom.npos, _p(obj_norm), st), "patch_energy_max")
+    maxes = torch.empty(geom.S * geom.P, dtype=torch.float32, device=dev)
+    g_obj = torch.empty_like(obj_c)
+    _lib.check(lib.ptycho_analytic_obj_finalize(_p(upd), _p(an_norm), _p(maxes), geom.S, geom.P,
+                                                geom.Ho * geom.Wo, _p(g_obj), st), "analytic_obj_finalize")
+    hw = float(geom.n * geom.n)
+    ortho = 2.0 * hw**0.5 if geom.P == 1 else 1.0 / (2.0 * hw**0.5)
+    _lib.check(lib.ptycho_analytic_probe_finalize(_p(g_probe), nn, _p(obj_norm), float(ortho), st),
+               "analytic_probe_finalize")
+    return loss, g_obj, g_probe
+
+
 class _BatchLossFn(torch.autograd.Function):
     """loss(obj_raw, probe_o) of one batch; gradients from the fused adjoint kernel."""
 

@@ -146,6 +146,20 @@ def run_case(name, *, H, S, P, nscan, step_px, pad, dz, counts, jitter, batch, i
         probe_ortho=_c64(probe_model.probe.detach().numpy()),
     )
 
+    # --- analytic (autograd=False) update directions at the same state ---
+    with torch.no_grad():
+        obj_model._obj.grad = None
+        probe_model._probe.grad = None
+        patch_indices, _pos, frac, descan = pt.dset.forward(bi, pt.obj_padding_px)
+        sp = probe_model.forward(frac)
+        op = obj_model.forward(patch_indices)
+        prop, ov = pt.forward_operator(op, sp, descan)
+        inten = pt.detector_model.forward(ov)
+        loss_an, tg = pt.error_estimate(inten, bi)
+        pt.backward(loss_an, False, op, prop, ov, patch_indices, tg)
+    out.update(grad_obj_an=_c64(obj_model._obj.grad.numpy()),
+               grad_probe_an=_c64(probe_model._probe.grad.numpy()))
+
     # --- a few reconstruct iterations from the same state ---
     with torch.no_grad():
         obj_model._obj.grad = None

@@ -68,3 +68,33 @@ def test_reference_gradient_test_case_on_gpu(cuda_device):
                                             pd.targets.numpy().astype(np.float64), np.ones((N, N)), pd.num_gpts,
                                             pd.mean_diffraction_intensity)
     assert rel(g_obj.cpu().numpy(), g_ref) < 2e-2
+
+
+@pytest.mark.parametrize("case", ["single64", "mixed64"])
+def test_reconstruct_analytic_matches_oracle(cuda_device, case):
+    """reconstruct(autograd=False): one SGD iteration over seeded batches against
+    the FP64 oracle applying the reference's analytic update directions."""
+    z = load_golden(case)
+    pt = build_from_golden(z, device="gpu")
+    dev = cuda_device
+    pt.dset.scan_positions_px = torch.as_tensor(z["positions"])
+    pt.obj_model._obj = torch.as_tensor(z["obj_perturbed"]).to(dev).requires_grad_(True)
+    pt.probe_model._probe = torch.as_tensor(z["probe_init"]).to(dev).requires_grad_(True)
+    pt.rng = 7
+    lr = 0.1
+    pt.reconstruct(num_iters=1, batch_size=int(z["batch"]), autograd=False,
+                   optimizer_params={"object": {"type": "sgd", "lr": lr}, "probe": {"type": "sgd", "lr": lr}},
+                   constraints={"probe": {"orthogonalize_probe": bool(z["orthogonalize"])}}, device="gpu")
+    H = int(z["H"])
+    props = z["propagators"].astype(np.complex128) if int(z["S"]) > 1 else np.zeros((0, H, H))
+    obj = z["obj_perturbed"].astype(np.complex128)
+    probe = z["probe_init"].astype(np.complex128)
+    pos = z["positions"].astype(np.float64)
+    tg = z["targets"].astype(np.float64)
+    for bi in O.batch_order(np.random.default_rng(7), pos.shape[0], int(z["batch"])):
+        g_obj, g_probe, _ = O.analytic_gradients(obj, probe, pos[bi], props, tg[bi],
+                                                 orthogonalize=bool(z["orthogonalize"]))
+        obj = obj - lr * g_obj
+        probe = probe - lr * g_probe
+    assert rel(pt.obj_model._obj.detach().cpu().numpy(), obj) < 1e-5
+    assert rel(pt.probe_model._probe.detach().cpu().numpy(), probe) < 1e-5

@@ -73,3 +73,18 @@ def test_oracle_matches_reference_gradient_test_case(nprobe):
     assert rel(g_obj, z[f"grad_obj_{tag}"]) < 2e-2
     assert _cos(g_obj, z[f"grad_obj_{tag}"]) > 0.9999
     assert _cos(g_probe, z[f"grad_probe_{tag}"]) > 0.9
+
+
+@pytest.mark.parametrize("case", ["single64", "mixed64", "mixed128"])
+def test_oracle_analytic_update_matches_reference(case):
+    z = load_golden(case)
+    S, H = int(z["S"]), int(z["H"])
+    props = z["propagators"].astype(np.complex128) if S > 1 else np.zeros((0, H, H))
+    bi = z["batch_indices"]
+    g_obj, g_probe, _ = O.analytic_gradients(z["obj_perturbed"].astype(np.complex128),
+                                             z["probe_init"].astype(np.complex128),
+                                             z["positions"].astype(np.float64)[bi], props,
+                                             z["targets"].astype(np.float64)[bi],
+                                             orthogonalize=bool(z["orthogonalize"]))
+    assert rel(g_obj, z["grad_obj_an"]) < 5e-6
+    assert rel(g_probe, z["grad_probe_an"]) < 5e-6
