@@ -117,6 +117,16 @@ int ptycho_forward_loss(const ptycho_batch_args* a, void* stream);
 /* Forward model + loss + adjoint of one batch in a single persistent launch. */
 int ptycho_forward_adjoint(const ptycho_batch_args* a, void* stream);
 
+/* Largest number of datasets of one ptycho_forward_adjoint_multi launch. */
+#define PTYCHO_MAX_DATASETS 16
+
+/* Forward + loss + adjoint of several independent datasets (same n; any S, P,
+ * object size, scan size, loss, analytic flag) in one persistent launch of the
+ * serial kernel: CTAs are partitioned between datasets by their sets[d].grid
+ * (each dataset's buffers sized for its grid with ptycho_batch_plan semantics).
+ * Replaces a loop of Ptychography.reconstruct calls over datasets. */
+int ptycho_forward_adjoint_multi(const ptycho_batch_args* sets, int nsets, void* stream);
+
 /* count 2-D FFTs of n x n complex64 arrays, out = scale * (i)fft2(in), unnormalised
  * transform; in and out may alias. */
 int ptycho_fft2(const void* in, void* out, int count, int n, int inverse, float scale, void* stream);
@@ -146,6 +156,16 @@ int ptycho_reduce_blocks(void);
 int ptycho_adam_step(float* param, const float* grad, float* exp_avg, float* exp_avg_sq, int64_t count,
                      float lr, const float* lr_dev, float beta1, float beta2, float eps,
                      float weight_decay, int decoupled, float bc1, float bc2_sqrt, void* stream);
+
+/* Adam with the step count held on the device (*step_dev, advanced with
+ * ptycho_add_scalar before the update) so that a captured iteration replays
+ * with the right bias corrections; lr from *lr_dev. */
+int ptycho_adam_step_dev(float* param, const float* grad, float* exp_avg, float* exp_avg_sq, int64_t count,
+                         const float* lr_dev, const float* step_dev, float beta1, float beta2, float eps,
+                         float weight_decay, int decoupled, void* stream);
+
+/* x[0] += v on the device (step counters of captured iterations). */
+int ptycho_add_scalar(float* x, float v, void* stream);
 
 /* torch.optim.SGD step without momentum: param -= lr * (grad + wd * param). */
 int ptycho_sgd_step(float* param, const float* grad, int64_t count, float lr, const float* lr_dev,

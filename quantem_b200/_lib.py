@@ -34,6 +34,7 @@ EXPORTED = (
     "ptycho_batch_plan",
     "ptycho_forward_loss",
     "ptycho_forward_adjoint",
+    "ptycho_forward_adjoint_multi",
     "ptycho_fft2",
     "ptycho_reduce_partials",
     "ptycho_reduce_loss",
@@ -42,6 +43,8 @@ EXPORTED = (
     "ptycho_reduce_blocks",
     "ptycho_adam_step",
     "ptycho_sgd_step",
+    "ptycho_adam_step_dev",
+    "ptycho_add_scalar",
     "ptycho_patch_energy_max",
     "ptycho_analytic_obj_finalize",
     "ptycho_analytic_probe_finalize",
@@ -84,6 +87,9 @@ def _declare(lib):
                                      ctypes.POINTER(_i64), ctypes.POINTER(_i64), ctypes.POINTER(_int)]),
         "ptycho_forward_loss": (_int, [ctypes.POINTER(BatchArgs), _vp]),
         "ptycho_forward_adjoint": (_int, [ctypes.POINTER(BatchArgs), _vp]),
+        "ptycho_forward_adjoint_multi": (_int, [_vp, _int, _vp]),
+        "ptycho_adam_step_dev": (_int, [_vp, _vp, _vp, _vp, _i64, _vp, _vp, _flt, _flt, _flt, _flt, _int, _vp]),
+        "ptycho_add_scalar": (_int, [_vp, _flt, _vp]),
         "ptycho_fft2": (_int, [_vp, _vp, _int, _int, _int, _flt, _vp]),
         "ptycho_reduce_partials": (_int, [_vp, _vp, _int, _i64, _vp]),
         "ptycho_reduce_loss": (_int, [_vp, _int, _vp, _vp]),

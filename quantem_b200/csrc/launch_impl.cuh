@@ -67,6 +67,26 @@ int launch_serial(const ptycho_batch_args* a, bool adj, cudaStream_t st) {
   return cudaPeekAtLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_CUDA;
 }
 
+// several datasets in one persistent launch (serial body, adjoint)
+template <int N>
+int launch_multi(const ptycho_batch_args* sets, int nsets, cudaStream_t st) {
+  MultiParams mp;
+  mp.nd = nsets;
+  mp.begin[0] = 0;
+  size_t smem = 0;
+  for (int d = 0; d < nsets; ++d) {
+    mp.d[d] = to_params(&sets[d]);
+    mp.begin[d + 1] = mp.begin[d] + sets[d].grid;
+    const size_t sd = batch_smem_bytes<N, true>(sets[d].prop_r != nullptr, sets[d].S);
+    if (sd > smem) smem = sd;
+  }
+  cudaFuncSetAttribute(multi_batch_kernel<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaFuncSetAttribute(multi_batch_kernel<N, true>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                       (int)((smem + 1024) * 100 / (228 * 1024) + 1));
+  multi_batch_kernel<N, true><<<mp.begin[nsets], 4 * N, smem, st>>>(mp);
+  return cudaPeekAtLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_CUDA;
+}
+
 template <int N, bool ADJ>
 cudaLaunchConfig_t cluster_config(const ptycho_batch_args* a, int grid, cudaStream_t st, cudaLaunchAttribute* attr) {
   cudaLaunchConfig_t cfg = {};

@@ -182,6 +182,35 @@ __global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ g, 
   }
 }
 
+// Adam with the step count on the device (CUDA-graph replays advance it): the
+// bias corrections 1 - beta^t are evaluated per launch from *step.
+__global__ void adam_dev_kernel(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                                float* __restrict__ v, int64_t n, const float* lr_dev, const float* step, float b1,
+                                float b2, float eps, float wd, int decoupled) {
+  const float t = *step;
+  const float lr_ = *lr_dev;
+  const float bc1 = 1.0f - powf(b1, t);
+  const float bc2s = sqrtf(1.0f - powf(b2, t));
+  const float stp = lr_ / bc1;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    float pi = p[i];
+    float gi = g[i];
+    if (wd != 0.0f) {
+      if (decoupled) pi *= 1.0f - lr_ * wd;
+      else gi = fmaf(wd, pi, gi);
+    }
+    float mi = m[i];
+    mi = mi + (1.0f - b1) * (gi - mi);
+    float vi = v[i] * b2 + (1.0f - b2) * gi * gi;
+    pi = pi - stp * (mi / (sqrtf(vi) / bc2s + eps));
+    p[i] = pi;
+    m[i] = mi;
+    v[i] = vi;
+  }
+}
+
+__global__ void add_scalar_kernel(float* x, float v) { x[0] += v; }
+
 __global__ void sgd_kernel(float* __restrict__ p, const float* __restrict__ g, int64_t n, float lr,
                            const float* lr_dev, float wd) {
   const float lr_ = lr_dev ? *lr_dev : lr;
@@ -284,6 +313,8 @@ int qb_launch_serial_64(const ptycho_batch_args* a, bool adj, cudaStream_t st);
 int qb_launch_serial_128(const ptycho_batch_args* a, bool adj, cudaStream_t st);
 int qb_launch_cluster_64(const ptycho_batch_args* a, bool adj, cudaStream_t st);
 int qb_launch_cluster_128(const ptycho_batch_args* a, bool adj, cudaStream_t st);
+int qb_launch_multi_64(const ptycho_batch_args* sets, int nsets, cudaStream_t st);
+int qb_launch_multi_128(const ptycho_batch_args* sets, int nsets, cudaStream_t st);
 int qb_max_clusters_64(const ptycho_batch_args* a, bool adj);
 int qb_max_clusters_128(const ptycho_batch_args* a, bool adj);
 
@@ -418,6 +449,29 @@ int ptycho_batch_plan(const ptycho_batch_args* a, int adjoint, int* variant, int
 
 int ptycho_forward_loss(const ptycho_batch_args* a, void* stream) { return run_batch(a, stream, false); }
 
+int ptycho_forward_adjoint_multi(const ptycho_batch_args* sets, int nsets, void* stream) {
+  if (!sets || nsets < 1 || nsets > PTYCHO_MAX_DATASETS)
+    return fail(PTYCHO_ERR_INVALID, "multi: nsets must be in [1, %d]", PTYCHO_MAX_DATASETS);
+  long total = 0;
+  for (int d = 0; d < nsets; ++d) {
+    const int rc = validate_batch(&sets[d], true);
+    if (rc) {
+      char why[512];
+      strncpy(why, g_last_error, sizeof(why) - 1);
+      why[sizeof(why) - 1] = '\0';
+      return fail(rc, "multi: dataset %d: %s", d, why);
+    }
+    if (sets[d].n != sets[0].n) return fail(PTYCHO_ERR_INVALID, "multi: every dataset needs the same probe window");
+    if (sets[d].grid < 1) return fail(PTYCHO_ERR_INVALID, "multi: dataset %d has grid %d", d, sets[d].grid);
+    total += sets[d].grid;
+  }
+  if (total > 65535) return fail(PTYCHO_ERR_INVALID, "multi: %ld CTAs in total", total);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int lrc = sets[0].n == 64 ? qb_launch_multi_64(sets, nsets, st) : qb_launch_multi_128(sets, nsets, st);
+  if (lrc) return fail(lrc, "multi_batch_kernel launch: %s", cudaGetErrorString(cudaGetLastError()));
+  return PTYCHO_OK;
+}
+
 int ptycho_forward_adjoint(const ptycho_batch_args* a, void* stream) { return run_batch(a, stream, true); }
 
 int ptycho_fft2(const void* in, void* out, int count, int n, int inverse, float scale, void* stream) {
@@ -534,6 +588,23 @@ int ptycho_fp32_fma_probe(float* out, int iters, int blocks, void* stream) {
   if (!out || iters < 1 || blocks < 1) return fail(PTYCHO_ERR_INVALID, "fma probe: bad arguments");
   fma_probe_kernel<<<blocks, 512, 0, static_cast<cudaStream_t>(stream)>>>(out, iters);
   return check_launch("fma_probe_kernel");
+}
+
+int ptycho_adam_step_dev(float* param, const float* grad, float* exp_avg, float* exp_avg_sq, int64_t count,
+                         const float* lr_dev, const float* step_dev, float beta1, float beta2, float eps,
+                         float weight_decay, int decoupled, void* stream) {
+  if (!param || !grad || !exp_avg || !exp_avg_sq || !lr_dev || !step_dev || count < 0)
+    return fail(PTYCHO_ERR_INVALID, "adam_dev: bad arguments");
+  if (count == 0) return PTYCHO_OK;
+  adam_dev_kernel<<<grid_for(count, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      param, grad, exp_avg, exp_avg_sq, count, lr_dev, step_dev, beta1, beta2, eps, weight_decay, decoupled);
+  return check_launch("adam_dev_kernel");
+}
+
+int ptycho_add_scalar(float* x, float v, void* stream) {
+  if (!x) return fail(PTYCHO_ERR_INVALID, "add_scalar: NULL");
+  add_scalar_kernel<<<1, 1, 0, static_cast<cudaStream_t>(stream)>>>(x, v);
+  return check_launch("add_scalar_kernel");
 }
 
 int ptycho_sgd_step(float* param, const float* grad, int64_t count, float lr, const float* lr_dev,

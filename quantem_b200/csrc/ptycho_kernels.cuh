@@ -192,8 +192,10 @@ __device__ __forceinline__ void accumulate_probe_grad(const Fft2<N>& f, const fl
     }
 }
 
+// Body of the serial batch kernel for one dataset: CTA `cta` of the `ncta` CTAs
+// that work on this dataset's positions.
 template <int N, bool ADJ>
-__global__ void __launch_bounds__(4 * N, 1) fused_batch_kernel(const BatchParams p) {
+__device__ __forceinline__ void serial_body(const BatchParams& p, const int cta, const int ncta) {
   using F = Fft2<N>;
   constexpr int E = F::E, D = F::D, G3 = F::G3, T = F::T;
   extern __shared__ float4 smem_raw[];
@@ -231,9 +233,9 @@ __global__ void __launch_bounds__(4 * N, 1) fused_batch_kernel(const BatchParams
   const size_t NN = (size_t)N * N;
   const int S = p.S, P = p.P;
   const size_t HoWo = (size_t)p.Ho * p.Wo;
-  float2* slot = ADJ ? p.scratch + (size_t)blockIdx.x * (size_t)(P * S + P + 1) * NN : nullptr;
+  float2* slot = ADJ ? p.scratch + (size_t)cta * (size_t)(P * S + P + 1) * NN : nullptr;
   float* inten = ADJ ? reinterpret_cast<float*>(slot + (size_t)(P * S + P) * NN) : inten_sm;
-  float2* pgrad = ADJ ? p.probe_grad_part + (size_t)blockIdx.x * (size_t)P * NN : nullptr;
+  float2* pgrad = ADJ ? p.probe_grad_part + (size_t)cta * (size_t)P * NN : nullptr;
   if (ADJ) {
     for (int m = 0; m < P; ++m)
 #pragma unroll
@@ -245,7 +247,7 @@ __global__ void __launch_bounds__(4 * N, 1) fused_batch_kernel(const BatchParams
   double loss_acc = 0.0;
   int nonfinite = 0;
 
-  for (int b = blockIdx.x; b < p.B; b += gridDim.x) {
+  for (int b = cta; b < p.B; b += ncta) {
     const int64_t gi = p.batch_idx[b];
     if (gi < 0 || gi >= p.npos) {  // invalid index: skip the position and report it
       if (tid == 0 && p.status) atomicAdd(p.status, 1 << 20);
@@ -472,9 +474,32 @@ __global__ void __launch_bounds__(4 * N, 1) fused_batch_kernel(const BatchParams
     double t = 0.0;
     for (int w = 0; w < T / 32; ++w) t += red[w];
     // l1/l2: sum / (B / num_gpts) / mean_I ; poisson: sum / mean_I
-    p.loss_part[blockIdx.x] = t * (double)(p.loss_type == LOSS_POISSON ? p.inv_mean_intensity : p.loss_scale);
+    p.loss_part[cta] = t * (double)(p.loss_type == LOSS_POISSON ? p.inv_mean_intensity : p.loss_scale);
   }
   if (p.status && nonfinite) atomicAdd(p.status, nonfinite);
+}
+
+template <int N, bool ADJ>
+__global__ void __launch_bounds__(4 * N, 1) fused_batch_kernel(const BatchParams p) {
+  serial_body<N, ADJ>(p, blockIdx.x, gridDim.x);
+}
+
+// Several independent datasets (same probe window N; any S, P, object size,
+// scan size) in one persistent launch: CTAs [begin[d], begin[d+1]) work on
+// dataset d.  The descriptors stay in the launch's parameter space
+// (__grid_constant__), indexed by the CTA's uniform dataset id.
+constexpr int kMaxDatasets = 16;
+struct MultiParams {
+  int nd;
+  int begin[kMaxDatasets + 1];
+  BatchParams d[kMaxDatasets];
+};
+
+template <int N, bool ADJ>
+__global__ void __launch_bounds__(4 * N, 1) multi_batch_kernel(const __grid_constant__ MultiParams mp) {
+  int d = 0;
+  while (d + 1 < mp.nd && (int)blockIdx.x >= mp.begin[d + 1]) ++d;
+  serial_body<N, ADJ>(mp.d[d], (int)blockIdx.x - mp.begin[d], mp.begin[d + 1] - mp.begin[d]);
 }
 
 // Batched 2-D FFT of (count, N, N) arrays, one CTA per transform, natural layout
