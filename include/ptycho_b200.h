@@ -206,6 +206,95 @@ int ptycho_fp32_fma_probe(float* out, int iters, int blocks, void* stream);
  * the array: calls that overlap on the GPU race. */
 int ptycho_forward_loss_noalloc(const ptycho_batch_args* a, float* out_loss, void* stream);
 
+
+/* ------------------------------------------------------------------------
+ * Learned initialiser: CNN training and inference kernels.
+ *
+ * They replace the torch.nn layers of the reference's UNet-like CNN2d
+ * (src/quantem/core/ml/cnn.py:17-212): Conv2dBlock = Conv2d 3x3 with circular
+ * padding, activation, BatchNorm2d (core/ml/blocks.py:53-140); the 2x2 MaxPool2d
+ * between levels (cnn.py:86, 184-191); Upsample2dBlock = ConvTranspose2d 3x3
+ * stride 2 + 1x1 Conv2d + BatchNorm2d (blocks.py:143-205); channel
+ * concatenation of the skips (cnn.py:194-198).
+ *
+ * Activations are channels-last matrices: R = B*H*W rows (r = (b*H + y)*W + x)
+ * with a leading dimension ld >= C, so a channel slice of a wider buffer is a
+ * column offset plus the wider ld.  BF16 tensors are passed as void*.
+ * ------------------------------------------------------------------------ */
+
+/* GEMM epilogue flags. */
+#define PTYCHO_GEMM_BF16 1   /* store BF16 instead of FP32 */
+#define PTYCHO_GEMM_RELU 2   /* max(x, 0) after the bias */
+#define PTYCHO_GEMM_ATOMIC 4 /* add into FP32 C atomically, C not cleared (splits > 1 without it clears C) */
+
+/* C[M][ldc] (op)= A[M][lda] * B[N][ldb]^T (+ bias[N]): BF16 operands, K-major
+ * (K contiguous), FP32 accumulation on the tcgen05 tensor cores (TMA-fed
+ * 128 x {32,64,128} tiles, accumulator in tensor memory).  Replaces the matrix
+ * products inside nn.Conv2d / nn.ConvTranspose2d forward and backward.  A and B
+ * 16-byte aligned, lda and ldb multiples of 8.  splits > 1 splits K across CTAs.
+ * `status` (optional device int) gets bit 0 set if a bounded wait expired. */
+int ptycho_gemm_bf16(const void* A, int lda, const void* B, int ldb, void* C, int ldc, int M, int N, int K,
+                     const float* bias, int flags, int splits, int* status, void* stream);
+
+/* col[r][(ky*3+kx)*C + c] = x[b, (y+ky-1) mod H, (x+kx-1) mod W, c] (BF16): the
+ * circular-padded 3x3 patches of nn.Conv2d(padding=1, padding_mode="circular"). */
+int ptycho_cnn_im2col3x3(const void* x, int B, int H, int W, int C, int ldx, void* col, int ldcol, void* stream);
+
+/* Adjoint of ptycho_cnn_im2col3x3 on FP32: dx (+)= fold(dcol). */
+int ptycho_cnn_col2im3x3(const float* dcol, int ldcol, int B, int H, int W, int C, float* dx, int ldx, int accumulate,
+                         void* stream);
+
+/* nn.ConvTranspose2d(k=3, stride=2, padding=1, output_padding=1) output assembly:
+ * out (B, 2H, 2W, Co) BF16 = bias + sum of the per-input-pixel products
+ * colT[(b,iy,ix)][(ky*3+kx)*Co + co] landing on (2iy-1+ky, 2ix-1+kx). */
+int ptycho_cnn_convT_gather(const float* colT, int ldcol, int B, int H, int W, int Co, const float* bias, void* out,
+                            int ldo, void* stream);
+
+/* Adjoint of the assembly: dcol[(b,iy,ix)][(ky*3+kx)*Co + co] = dout[b, 2iy-1+ky, 2ix-1+kx, co] (BF16, 0 outside). */
+int ptycho_cnn_convT_im2col(const float* dout, int ldo, int B, int H, int W, int Co, void* dcol, int ldcol,
+                            void* stream);
+
+/* out[z][c][r] = in[z][r][c]; dtypes 0 = FP32, 1 = BF16 (layout changes between
+ * NCHW and channels-last, and operand transposes for the weight gradients). */
+int ptycho_cnn_transpose(const void* in, int in_dtype, int R, int C, int ldi, int64_t batch_stride_in, void* out,
+                         int out_dtype, int ldo, int64_t batch_stride_out, int batch, void* stream);
+
+/* nn.BatchNorm2d forward (torch.nn.functional.batch_norm): training = batch
+ * statistics (biased variance for normalisation, running statistics updated with
+ * the unbiased one and `momentum`), else running statistics.  gamma == NULL skips
+ * the normalisation (plain BF16 conversion).  Writes the used mean / rstd.
+ * `work` holds >= 2 * C doubles (more gives more parallel partial sums). */
+int ptycho_cnn_bn_forward(const float* x, int ldx, int R, int C, const float* gamma, const float* beta,
+                          float* run_mean, float* run_var, float momentum, float eps, int training, float* mean,
+                          float* rstd, double* work, int64_t work_elems, void* out, int ldo, void* stream);
+
+/* Backward of batch norm (gamma != NULL) followed by the ReLU mask of its input x
+ * (relu != 0): dz = [x > 0] * dBN(dy).  Writes dgamma / dbeta and dz as FP32
+ * and/or BF16 (either may be NULL). */
+int ptycho_cnn_bn_backward(const float* dy, int lddy, const float* x, int ldx, int R, int C, const float* gamma,
+                           const float* mean, const float* rstd, int training, int relu, float* dgamma, float* dbeta,
+                           double* work, int64_t work_elems, float* dz32, void* dz16, int ldz, void* stream);
+
+/* out[c] (+)= sum_r a[r][c] (bias gradients), deterministic order. */
+int ptycho_cnn_colsum(const float* a, int lda, int R, int C, float* out, int accumulate, double* work,
+                      int64_t work_elems, void* stream);
+
+/* nn.MaxPool2d(2, 2) on BF16 with the argmax code (2*dy + dx) per output. */
+int ptycho_cnn_maxpool2(const void* in, int ldi, int B, int H, int W, int C, void* out, int ldo, void* argmax,
+                        void* stream);
+
+/* Its adjoint: din (+)= dout routed to the argmax positions (FP32). */
+int ptycho_cnn_maxpool2_backward(const float* dout, int lddo, const void* argmax, int B, int H, int W, int C,
+                                 float* din, int lddi, int accumulate, void* stream);
+
+/* out (BF16) = in (FP32), n values: BF16 weight copies of the FP32 master weights. */
+int ptycho_cnn_cast_bf16(const float* in, void* out, int64_t n, void* stream);
+
+/* loss = mean((pred - target)^2) (device float); dpred = 2 (pred - target) / n as
+ * FP32 and/or BF16 (either may be NULL).  work >= 296 doubles. */
+int ptycho_cnn_mse(const float* pred, const float* target, int64_t n, float* loss, float* dpred32, void* dpred16,
+                   double* work, int64_t work_elems, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -50,6 +50,19 @@ EXPORTED = (
     "ptycho_analytic_probe_finalize",
     "ptycho_fp32_fma_probe",
     "ptycho_forward_loss_noalloc",
+    "ptycho_gemm_bf16",
+    "ptycho_cnn_im2col3x3",
+    "ptycho_cnn_col2im3x3",
+    "ptycho_cnn_convT_gather",
+    "ptycho_cnn_convT_im2col",
+    "ptycho_cnn_transpose",
+    "ptycho_cnn_bn_forward",
+    "ptycho_cnn_bn_backward",
+    "ptycho_cnn_colsum",
+    "ptycho_cnn_maxpool2",
+    "ptycho_cnn_maxpool2_backward",
+    "ptycho_cnn_cast_bf16",
+    "ptycho_cnn_mse",
 )
 
 _vp = ctypes.c_void_p
@@ -104,6 +117,21 @@ def _declare(lib):
         "ptycho_analytic_obj_finalize": (_int, [_vp, _vp, _vp, _int, _int, _i64, _vp, _vp]),
         "ptycho_analytic_probe_finalize": (_int, [_vp, _i64, _vp, _flt, _vp]),
         "ptycho_forward_loss_noalloc": (_int, [ctypes.POINTER(BatchArgs), _vp, _vp]),
+        "ptycho_gemm_bf16": (_int, [_vp, _int, _vp, _int, _vp, _int, _int, _int, _int, _vp, _int, _int, _vp, _vp]),
+        "ptycho_cnn_im2col3x3": (_int, [_vp, _int, _int, _int, _int, _int, _vp, _int, _vp]),
+        "ptycho_cnn_col2im3x3": (_int, [_vp, _int, _int, _int, _int, _int, _vp, _int, _int, _vp]),
+        "ptycho_cnn_convT_gather": (_int, [_vp, _int, _int, _int, _int, _int, _vp, _vp, _int, _vp]),
+        "ptycho_cnn_convT_im2col": (_int, [_vp, _int, _int, _int, _int, _int, _vp, _int, _vp]),
+        "ptycho_cnn_transpose": (_int, [_vp, _int, _int, _int, _int, _i64, _vp, _int, _int, _i64, _int, _vp]),
+        "ptycho_cnn_bn_forward": (_int, [_vp, _int, _int, _int, _vp, _vp, _vp, _vp, _flt, _flt, _int, _vp, _vp, _vp,
+                                         _i64, _vp, _int, _vp]),
+        "ptycho_cnn_bn_backward": (_int, [_vp, _int, _vp, _int, _int, _int, _vp, _vp, _vp, _int, _int, _vp, _vp,
+                                          _vp, _i64, _vp, _vp, _int, _vp]),
+        "ptycho_cnn_colsum": (_int, [_vp, _int, _int, _int, _vp, _int, _vp, _i64, _vp]),
+        "ptycho_cnn_maxpool2": (_int, [_vp, _int, _int, _int, _int, _int, _vp, _int, _vp, _vp]),
+        "ptycho_cnn_maxpool2_backward": (_int, [_vp, _int, _vp, _int, _int, _int, _int, _vp, _int, _int, _vp]),
+        "ptycho_cnn_cast_bf16": (_int, [_vp, _vp, _i64, _vp]),
+        "ptycho_cnn_mse": (_int, [_vp, _vp, _i64, _vp, _vp, _vp, _vp, _i64, _vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -1,0 +1,76 @@
+"""Golden fixtures for the learned initialiser's CNN, made by the reference itself.
+
+Run in a container where the reference source tree is mounted:
+
+    python tests/golden/make_golden_cnn.py /root/reference/src
+
+Builds the reference's ``quantem.core.ml.cnn.CNN2d`` (UNet topology of
+core/ml/cnn.py:17-212 with the blocks of core/ml/blocks.py) for a few small
+configurations, with torch's default initialisation under a fixed seed, and
+records in FP64: the state dict, an input, the training-mode output (batch-norm
+batch statistics), the gradients of sum(output * dy) with respect to every
+parameter and to the input, the running statistics after that step and the
+eval-mode output.  The fixtures pin the FP64 NumPy oracle (``oracle/cnn_oracle.py``)
+and the CUDA network (``quantem_b200.core.ml.cnn.CNN2d``).
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle.quantem_shim import import_reference  # noqa: E402
+
+CASES = {
+    # name: (in_ch, out_ch, start_filters, num_layers, num_per_layer, skip, batchnorm, B, H, W)
+    "cnn_unet2": (4, 3, 8, 2, 2, True, True, 2, 16, 16),
+    "cnn_unet2_noskip": (8, 2, 8, 2, 2, False, True, 2, 16, 24),
+    "cnn_unet1_nobn": (16, 5, 16, 1, 2, True, False, 3, 8, 8),
+}
+
+
+def run_case(name, cfg):
+    import torch
+    from quantem.core.ml.cnn import CNN2d
+
+    cin, cout, sf, L, npl, skip, bn, B, H, W = cfg
+    torch.manual_seed(1234 + len(name))
+    net = CNN2d(cin, cout, start_filters=sf, num_layers=L, num_per_layer=npl, use_skip_connections=skip,
+                use_batchnorm=bn, dtype=torch.float32).double()
+    net.train()
+    g = torch.Generator().manual_seed(99)
+    x = torch.randn(B, cin, H, W, generator=g, dtype=torch.float64).requires_grad_(True)
+    dy = torch.randn(B, cout, H, W, generator=g, dtype=torch.float64)
+    sd0 = {k: v.detach().clone() for k, v in net.state_dict().items()}
+    y = net(x)
+    (y * dy).sum().backward()
+    out = {"x": x.detach().numpy(), "dy": dy.numpy(), "y_train": y.detach().numpy(),
+           "dx": x.grad.numpy(), "config": np.array(cfg[:5] + (int(skip), int(bn)), dtype=np.int64)}
+    for k, v in sd0.items():
+        out["sd/" + k] = v.numpy()
+    for k, p in net.named_parameters():  # unused parameters (the upsample bn without batch norm) get zeros
+        out["grad/" + k] = p.grad.numpy() if p.grad is not None else np.zeros(tuple(p.shape))
+    for k, v in net.state_dict().items():
+        if "running" in k:
+            out["after/" + k] = v.numpy()
+    net.eval()
+    with torch.no_grad():
+        out["y_eval"] = net(x.detach()).numpy()
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+    print(name, "params", sum(p.numel() for p in net.parameters()))
+
+
+def main():
+    src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src"
+    import_reference(src)
+    for name, cfg in CASES.items():
+        run_case(name, cfg)
+
+
+if __name__ == "__main__":
+    main()

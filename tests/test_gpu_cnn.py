@@ -1,0 +1,245 @@
+"""GPU parity of the CUDA CNN2d (tcgen05 BF16 GEMMs + layer kernels) with the
+reference's CNN2d and with the FP64 NumPy oracle.
+
+* Per layer, teacher-forced (the tight bar): every conv / transposed-conv /
+  batch-norm layer is recomputed by the oracle from the CUDA layer's own inputs
+  (recorded with ``net.trace``), forward and backward, with BF16 rounding at the
+  same points as the CUDA path.  FP32 products agree to 1e-5; values stored as
+  BF16 agree to 2e-3 (an occasional one-ulp rounding flip); a layout or
+  indexing bug shows as O(1).
+* Whole network: BF16 storage errors are amplified from layer to layer by
+  batch norms whose statistics come from few samples (32 per channel at the
+  4 x 4 bottleneck of the fixtures), so even an exact BF16 model of the
+  computation (the oracle with ``emulate_bf16=True``) differs from the FP64
+  reference by 2-5 % in the outputs and up to ~35 % in the input / weight
+  gradients of these small networks.  The end-to-end bar is relative to that
+  model: the CUDA result's distance to the FP64 result must be at most 1.5x the
+  emulating oracle's distance plus 5e-3."""
+import numpy as np
+import pytest
+import torch
+
+from oracle.cnn_oracle import CNN2dOracle
+from tests.conftest import load_golden
+
+pytestmark = pytest.mark.gpu
+
+CASES = ["cnn_unet2", "cnn_unet2_noskip", "cnn_unet1_nobn"]
+
+
+def _rel(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def _cfg(z):
+    c = [int(v) for v in z["config"]]
+    return dict(in_channels=c[0], out_channels=c[1], start_filters=c[2], num_layers=c[3], num_per_layer=c[4],
+                use_skip_connections=bool(c[5]), use_batchnorm=bool(c[6]))
+
+
+def _flatgrads(d, keys):
+    return np.concatenate([np.asarray(d[k], dtype=np.float64).ravel() for k in keys])
+
+
+def _run_cuda(net, x, dy, dev):
+    xt = torch.as_tensor(x, dtype=torch.float32, device=dev).requires_grad_(True)
+    net.train()
+    y = net(xt)
+    (y * torch.as_tensor(dy, dtype=torch.float32, device=dev)).sum().backward()
+    torch.cuda.synchronize()
+    g = {k: v.double().cpu().numpy() for k, v in net.named_gradients().items()}
+    return y.detach().double().cpu().numpy(), xt.grad.double().cpu().numpy(), g
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_cnn_matches_reference_and_oracle(cuda_device, name):
+    from quantem_b200.core.ml.cnn import CNN2d
+
+    z = load_golden(name)
+    cfg = _cfg(z)
+    sd = {k[3:]: torch.as_tensor(z[k]) for k in z if k.startswith("sd/")}
+    net = CNN2d(**cfg, device=cuda_device)
+    net.load_state_dict(sd)
+    y, dx, g = _run_cuda(net, z["x"], z["dy"], cuda_device)
+    keys = sorted(k[5:] for k in z if k.startswith("grad/"))
+    gref = _flatgrads({k: z["grad/" + k] for k in keys}, keys)
+    # the exact BF16 model of the computation, and its own distance to the FP64 reference
+    orc = CNN2dOracle({k: v.numpy() for k, v in sd.items()}, **{k: v for k, v in cfg.items()}, emulate_bf16=True)
+    yo = orc.forward(z["x"], training=True)
+    dxo, go = orc.backward(z["dy"])
+    bar = lambda model_err: 1.5 * model_err + 5e-3  # noqa: E731
+    assert _rel(y, z["y_train"]) < bar(_rel(yo, z["y_train"]))
+    assert _rel(dx, z["dx"]) < bar(_rel(dxo, z["dx"]))
+    assert _rel(_flatgrads(g, keys), gref) < bar(_rel(_flatgrads(go, keys), gref))
+    # running statistics after the step, then eval mode
+    st = net.state_dict()
+    for k in z:
+        if k.startswith("after/"):
+            assert _rel(st[k[6:]].cpu().numpy(), z[k]) < bar(_rel(orc.sd[k[6:]], z[k])), k
+    net.eval()
+    with torch.no_grad():
+        ye = net(torch.as_tensor(z["x"], dtype=torch.float32, device=cuda_device)).double().cpu().numpy()
+    assert _rel(ye, z["y_eval"]) < bar(_rel(orc.forward(z["x"], training=False), z["y_eval"]))
+
+
+def test_cnn_padded_channels_and_odd_outputs(cuda_device):
+    """Input channels not a multiple of 8 (zero-padded inside), 36 output channels
+    (final GEMM N and gradient leading dimensions not multiples of 8), 3 levels."""
+    from quantem_b200.core.ml.cnn import CNN2d
+
+    net = CNN2d(20, 36, start_filters=16, num_layers=3, num_per_layer=2, device=cuda_device, seed=3)
+    sd = {k: v.cpu() for k, v in net.state_dict().items()}
+    rng = np.random.default_rng(4)
+    x = rng.standard_normal((2, 20, 32, 32))
+    dy = rng.standard_normal((2, 36, 32, 32))
+    y, dx, g = _run_cuda(net, x, dy, cuda_device)
+    sdn = {k: v.numpy() for k, v in sd.items()}
+    exact = CNN2dOracle(sdn, 20, 36, 16, 3, 2)
+    ye = exact.forward(x, training=True)
+    dxe, ge = exact.backward(dy)
+    model = CNN2dOracle(sdn, 20, 36, 16, 3, 2, emulate_bf16=True)
+    ym = model.forward(x, training=True)
+    dxm, gm = model.backward(dy)
+    keys = sorted(ge)
+    bar = lambda model_err: 1.5 * model_err + 5e-3  # noqa: E731
+    assert _rel(y, ye) < bar(_rel(ym, ye))
+    assert _rel(dx, dxe) < bar(_rel(dxm, dxe))
+    assert _rel(_flatgrads(g, keys), _flatgrads(ge, keys)) < bar(_rel(_flatgrads(gm, keys), _flatgrads(ge, keys)))
+
+
+def _nchw(m, B, H, W):
+    return np.asarray(m, dtype=np.float64).reshape(B, H, W, -1).transpose(0, 3, 1, 2)
+
+
+def _np(t):
+    return t.double().cpu().numpy()
+
+
+def _conv_name(prefix, j, bn):
+    return f"{prefix}.block.{(3 if bn else 2) * j}", (f"{prefix}.block.{3 * j + 2}" if bn else None)
+
+
+def _prefix(key):
+    if key[0] == "final":
+        return "final_conv"
+    kind = key[0][0]
+    if kind == "down":
+        return f"down_conv_blocks.{key[0][1]}"
+    if kind == "bott":
+        return "bottleneck"
+    return f"up_conv_blocks.{key[0][1]}"
+
+
+@pytest.mark.parametrize("cfg", [(20, 36, 16, 3, True, True, 2, 32, 32), (4, 3, 8, 2, False, True, 3, 16, 24),
+                                 (16, 5, 16, 1, True, False, 2, 16, 16)])
+def test_cnn_layers_teacher_forced(cuda_device, cfg):
+    """Every layer of a CUDA pass against the oracle fed with that layer's CUDA inputs."""
+    from oracle import cnn_oracle as O
+    from quantem_b200.core.ml.cnn import CNN2d
+
+    cin, cout, sf, L, skip, bn, B, H, W = cfg
+    net = CNN2d(cin, cout, start_filters=sf, num_layers=L, use_skip_connections=skip, use_batchnorm=bn,
+                device=cuda_device, seed=7)
+    sd = {k: v.double().cpu().numpy() for k, v in net.state_dict().items()}
+    rng = np.random.default_rng(8)
+    x = torch.as_tensor(rng.standard_normal((B, cin, H, W)), dtype=torch.float32, device=cuda_device)
+    dy = torch.as_tensor(rng.standard_normal((B, cout, H, W)), dtype=torch.float32, device=cuda_device)
+    net.trace = {}
+    net.train()
+    (net(x) * dy).sum().backward()
+    torch.cuda.synchronize()
+    tr, net.trace = net.trace, None
+    grads = {k: _np(v) for k, v in net.named_gradients().items()}
+    w16 = {k: O.bf16(v) for k, v in sd.items() if k.endswith("weight") and v.ndim == 4}
+    nconv = 0
+    for key, f in tr.items():
+        if key[0] != "fwd":
+            continue
+        lk = key[1:]
+        # spatial size of the layer from its row count
+        R = f["x"].shape[0]
+        scale = int(round((B * H * W / R) ** 0.5))
+        h, w = H // scale, W // scale
+        prefix = _prefix(lk)
+        final = lk[0] == "final"
+        cname, bname = ("final_conv.block.0", None) if final else _conv_name(prefix, lk[1], bn)
+        wt = w16[cname + ".weight"]
+        ci = wt.shape[1]
+        xin = _nchw(_np(f["x"])[:, :ci], B, h, w)
+        z = O.conv3x3_circ(xin, wt, sd[cname + ".bias"])
+        a = z if (final and not net._final_relu) else np.maximum(z, 0.0)
+        r_cuda = _nchw(_np(f["r"]), B, h, w)
+        assert _rel(r_cuda, a) < 1e-5, (key, "conv")
+        if not final:
+            if bname is not None:
+                yb, cache = O.batchnorm_train(r_cuda, sd[bname + ".weight"], sd[bname + ".bias"])
+            else:
+                yb, cache = r_cuda, None
+            assert _rel(_nchw(_np(f["y"]), B, h, w), O.bf16(yb)) < 2e-3, (key, "bn")
+        b_ = tr[("bwd",) + lk]
+        g = _nchw(_np(b_["dy"]), B, h, w)
+        dbn = None
+        if bname is not None:
+            g, dg, dbb = O.batchnorm_train_bwd(g, sd[bname + ".weight"], cache)
+            dbn = (dg, dbb)
+        if not final or net._final_relu:
+            g = g * (r_cuda > 0)
+        dx, dw, _ = O.conv3x3_circ_bwd(xin, wt, O.bf16(g))
+        assert _rel(grads[cname + ".weight"], dw) < 2e-3, (key, "dW")
+        assert _rel(grads[cname + ".bias"], g.sum(axis=(0, 2, 3))) < 1e-4, (key, "db")
+        if dbn is not None:
+            assert _rel(grads[bname + ".weight"], dbn[0]) < 1e-4, (key, "dgamma")
+            assert _rel(grads[bname + ".bias"], dbn[1]) < 1e-4, (key, "dbeta")
+        if "dx" in b_:
+            assert _rel(_nchw(_np(b_["dx"]), B, h, w)[:, :ci], dx) < 2e-3, (key, "dx")
+        nconv += 1
+    assert nconv == 2 * (2 * L + 1) + 1
+    for u in range(L):
+        f, b_ = tr[("upfwd", u)], tr[("upbwd", u)]
+        p = f"upsample_blocks.{u}"
+        R = f["x"].shape[0]
+        scale = int(round((B * H * W / R) ** 0.5))
+        hin, win = H // scale, W // scale
+        xin = _nchw(_np(f["x"]), B, hin, win)
+        t = O.conv_transpose3x3_s2(xin, w16[p + ".upsample2x.weight"], sd[p + ".upsample2x.bias"])
+        t_cuda = _nchw(_np(f["t"]), B, 2 * hin, 2 * win)
+        assert _rel(t_cuda, O.bf16(t)) < 2e-3, (u, "convT")
+        a = O.conv1x1(t_cuda, w16[p + ".conv.weight"], sd[p + ".conv.bias"])
+        r_cuda = _nchw(_np(f["r"]), B, 2 * hin, 2 * win)
+        assert _rel(r_cuda, a) < 1e-5, (u, "1x1")
+        g = _nchw(_np(b_["dup"]), B, 2 * hin, 2 * win)
+        if bn:
+            yb, cache = O.batchnorm_train(r_cuda, sd[p + ".bn.weight"], sd[p + ".bn.bias"])
+            assert _rel(_nchw(_np(f["y"]), B, 2 * hin, 2 * win), O.bf16(yb)) < 2e-3, (u, "bn")
+            g, dg, dbb = O.batchnorm_train_bwd(g, sd[p + ".bn.weight"], cache)
+            assert _rel(grads[p + ".bn.weight"], dg) < 1e-4 and _rel(grads[p + ".bn.bias"], dbb) < 1e-4
+        dt, dw1, _ = O.conv1x1_bwd(t_cuda, w16[p + ".conv.weight"], O.bf16(g))
+        dt_cuda = _nchw(_np(b_["dt"]), B, 2 * hin, 2 * win)
+        assert _rel(dt_cuda, dt) < 2e-3, (u, "dt")
+        assert _rel(grads[p + ".conv.weight"], dw1) < 2e-3, (u, "dW1")
+        dx, dwt, _ = O.conv_transpose3x3_s2_bwd(xin, w16[p + ".upsample2x.weight"], dt_cuda, dcol_round=O.bf16)
+        assert _rel(_nchw(_np(b_["dx"]), B, hin, win), dx) < 2e-3, (u, "dx")
+        assert _rel(grads[p + ".upsample2x.weight"], dwt) < 2e-3, (u, "dWt")
+        assert _rel(grads[p + ".upsample2x.bias"], dt_cuda.sum(axis=(0, 2, 3))) < 1e-4, (u, "dbt")
+
+
+def test_cnn_training_reduces_loss(cuda_device):
+    """A few fused-Adam steps on the CUDA network lower an MSE regression loss."""
+    from quantem_b200.core.ml.cnn import CNN2d, mse_loss
+    from quantem_b200.engine import FusedAdam
+
+    torch.manual_seed(0)
+    net = CNN2d(8, 1, start_filters=8, num_layers=2, device=cuda_device, seed=1)
+    x = torch.randn(4, 8, 16, 16, device=cuda_device)
+    target = x[:, :1] * 0.5 + x[:, 1:2].roll(1, dims=-1) * 0.25
+    opt = FusedAdam([net.flat], lr=3e-3)
+    losses = []
+    for _ in range(40):
+        opt.zero_grad()
+        loss = mse_loss(net(x), target)
+        loss.backward()
+        opt.step()
+        losses.append(float(loss.item()))
+    assert losses[-1] < 0.5 * losses[0]
