@@ -532,6 +532,155 @@ def run_c3(args):
                                            "per_dataset": round(ms_loop, 3)}}))
 
 
+def _bf16_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d["bf16_tflops"]), "measured"
+    except Exception:
+        return 1590.0, "fallback"
+
+
+def run_c4(args):
+    """Learned initialiser: train the CNN2d (5 levels, 32 base filters, BF16 tcgen05
+    kernels) on objects simulated by the forward kernel, then compare the time to a
+    phase NRMSE target of the plain reconstruction from a flat start and from the
+    learned start, on the 512x512x8 / 4-mode / 128^2 / 64x64-scan problem at the
+    configured dose (1e5 counts) and noiseless.  Probe known and fixed in both arms,
+    Adam lr 5e-3 decaying 0.97 per iteration, batch 256."""
+    import torch
+
+    from quantem_b200 import engine, ops, synthetic
+    from quantem_b200.core.ml import kernels as kk
+    from quantem_b200.diffractive_imaging.learned_init import LearnedInitConfig, LearnedInitializer
+    from quantem_b200.diffractive_imaging.ptycho_utils import SimpleBatcher, orthogonalize_probes
+
+    dev = torch.device("cuda", 0)
+    scfg = synthetic.SyntheticConfig(seed=0)
+    probes = orthogonalize_probes(synthetic.make_probe_modes(scfg, dev))
+    props = ops.separable_propagators(scfg.n, (scfg.pixel, scfg.pixel), scfg.energy,
+                                      [scfg.slice_thickness] * (scfg.slices - 1), device=dev)
+    cfg = LearnedInitConfig(lr=2e-3)
+    li = LearnedInitializer(probes, props, cfg, dev, seed=0)
+    nobj = args.c4_objects
+    torch.cuda.synchronize()
+    t0 = time.time()
+    li.train(nobj, total_objects=nobj)
+    torch.cuda.synchronize()
+    train_s = time.time() - t0
+    held_out = li.evaluate(32)
+
+    # dominant CNN kernel: the first-layer convolution GEMM (im2col rows x 9*1024) of a training step
+    M, K, N = cfg.batch_objects * cfg.scan_crop ** 2, 9 * li.C, cfg.start_filters
+    A = torch.randn(M, K, device=dev).to(torch.bfloat16)
+    B = torch.randn(N, K, device=dev).to(torch.bfloat16)
+    C = torch.empty(M, N, device=dev)
+    for _ in range(3):
+        kk.gemm(A, B, C)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    reps = 20
+    for _ in range(reps):
+        kk.gemm(A, B, C)
+    e1.record()
+    torch.cuda.synchronize()
+    gemm_s = e0.elapsed_time(e1) / 1e3 / reps
+    gemm_bytes = 2 * M * K + 2 * N * K + 4 * M * N
+    hbm, hbm_src = _peaks()
+    bf16, bf16_src = _bf16_peak()
+    del A, B, C
+
+    def proj_phase(o):
+        p = o[0]
+        for k in range(1, o.shape[0]):
+            p = p * o[k]
+        return torch.angle(p)
+
+    def nrmse(a, t):
+        a, t = a.double(), t.double()
+        d = (a - a.mean()) - (t - t.mean())
+        return float(d.norm() / (t - t.mean()).norm())
+
+    thresholds = (0.5, 0.3, 0.1, 0.05, 0.02, 0.01)
+    results = {}
+    for dose in ("1e5", "noiseless"):
+        dcfg = synthetic.SyntheticConfig(seed=0, counts=1e5 if dose == "1e5" else 1e12)
+        ds = synthetic.make_dataset(dcfg, dev)
+        truth = proj_phase(ds["obj"])
+        lo, hi = dcfg.pad_px, dcfg.pad_px + int((dcfg.scan[0] - 1) * dcfg.step_px)
+        crop = (slice(lo, hi), slice(lo, hi))
+        S, Ho, Wo = ds["obj_shape"]
+        probe = (ds["probes"] * (ds["mean_intensity"] / ds["probes"].abs().square().sum()) ** 0.5).contiguous()
+        arms = {}
+        for arm in ("plain", "learned"):
+            torch.cuda.synchronize()
+            t0 = time.time()
+            if arm == "learned":
+                judge = dict(probe=probe, prop=ds["propagators"], positions=ds["positions"],
+                             targets=ds["amplitudes"].contiguous(), mask=torch.ones((dcfg.n, dcfg.n), device=dev),
+                             mean_intensity=ds["mean_intensity"],
+                             batch=torch.arange(0, ds["positions"].shape[0], 4, device=dev))
+                o0 = li.initial_object(ds["amplitudes"], dcfg.scan, (S, Ho, Wo), (dcfg.pad_px, dcfg.pad_px),
+                                       judge=judge)
+            else:
+                o0 = torch.ones((S, Ho, Wo), dtype=torch.complex64, device=dev)
+            torch.cuda.synchronize()
+            elapsed = time.time() - t0
+            obj = o0.clone().requires_grad_(True)
+            pt = engine.ProblemTensors(obj=obj, probe=probe.clone().requires_grad_(True), prop=ds["propagators"],
+                                       positions=ds["positions"], targets=ds["amplitudes"].contiguous(),
+                                       mask=torch.ones((dcfg.n, dcfg.n), device=dev),
+                                       mean_intensity=ds["mean_intensity"], upsample_factor=dcfg.step_px)
+            opt = engine.make_optimizer([obj], {"type": "adam", "lr": 5e-3})
+            sched = torch.optim.lr_scheduler.ExponentialLR(opt, 0.97)
+            bt = SimpleBatcher(pt.num_gpts, 256, rng=0)
+            with torch.no_grad():
+                curve = [(0, round(elapsed, 4), round(nrmse(proj_phase(ops.constrained_object(obj.detach()))[crop],
+                                                           truth[crop]), 5))]
+            for it in range(1, args.c4_iters + 1):
+                s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                s0.record()
+                engine.run_iteration(pt, bt, [opt])
+                s1.record()
+                sched.step()
+                torch.cuda.synchronize()
+                elapsed += s0.elapsed_time(s1) / 1e3
+                with torch.no_grad():
+                    curve.append((it, round(elapsed, 4),
+                                  round(nrmse(proj_phase(ops.constrained_object(obj.detach()))[crop], truth[crop]), 5)))
+            reach = {}
+            for th in thresholds:
+                hit = next((c for c in curve if c[2] <= th), None)
+                reach[str(th)] = None if hit is None else hit[1]
+            arms[arm] = dict(time_to_nrmse_s=reach, start_nrmse=curve[0][2], best_nrmse=min(c[2] for c in curve),
+                             final_nrmse=curve[-1][2], curve=curve[:: max(1, len(curve) // 12)],
+                             used_learned_start=(getattr(li, "used_learned", None) if arm == "learned" else None))
+        results[dose] = arms
+    tp = results["noiseless"]["plain"]["time_to_nrmse_s"]["0.01"]
+    tl = results["noiseless"]["learned"]["time_to_nrmse_s"]["0.01"]
+    print(json.dumps({
+        "metric": "time to phase NRMSE<=1e-2, learned vs plain",
+        "value": (round(tl / tp, 4) if (tp and tl) else None), "unit": "ratio (learned time / plain time)",
+        "higher_is_better": False, "data": "synthetic",
+        "config": {"workload": "c4: CNN2d 5 levels x 32 filters on 32x32-binned patterns of a 64x64 scan -> "
+                               "projected phase; refinement 512x512x8, 4 modes at 128x128",
+                   "training_objects": nobj, "refine_iterations": args.c4_iters, "probe": "known, fixed"},
+        "cnn": {"train_s": round(train_s, 2), "objects_per_s": round(nobj / train_s, 1),
+                "held_out_phase_nrmse": round(held_out, 4),
+                "first_layer_gemm": {"M": M, "N": N, "K": K, "ms": round(gemm_s * 1e3, 4),
+                                     "tflops": round(2 * M * N * K / gemm_s / 1e12, 2),
+                                     "gbs": round(gemm_bytes / gemm_s / 1e9, 1),
+                                     "roofline": {"bound": "hbm", "achieved": round(gemm_bytes / gemm_s / 1e9, 1),
+                                                  "peak": hbm, "unit": "GB/s",
+                                                  "frac": round(gemm_bytes / gemm_s / 1e9 / hbm, 4),
+                                                  "peak_source": hbm_src},
+                                     "tensor_frac_of_bf16_peak": round(2 * M * N * K / gemm_s / 1e12 / bf16, 4),
+                                     "bf16_peak_source": bf16_src}},
+        "results": results,
+    }))
+
+
 def run_reference(args):
     rank, world, _ = _dist_env()
     if rank != 0:
@@ -555,8 +704,11 @@ def main():
     ap.add_argument("--batch-size", type=int, default=4096)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--kernel-only", action="store_true", help="time only the fused batch kernel")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3"],
-                    help="c2: the headline multislice mixed-probe iteration; c3: uneven multi-dataset launch")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4"],
+                    help="c2: the headline multislice mixed-probe iteration; c3: uneven multi-dataset launch; "
+                         "c4: learned initialiser vs flat start")
+    ap.add_argument("--c4-objects", type=int, default=20000, help="training objects for --workload c4")
+    ap.add_argument("--c4-iters", type=int, default=120, help="refinement iterations per arm for --workload c4")
     ap.add_argument("--skip-torch-reference", action="store_true",
                     help="do not time the PyTorch-eager restatement of the reference path")
     ap.add_argument("--positions", type=int, default=296, help="positions per launch with --kernel-only")
@@ -567,6 +719,8 @@ def main():
         args.warmup = 3
     if args.workload == "c3":
         run_c3(args)
+    elif args.workload == "c4":
+        run_c4(args)
     elif args.kernel_only:
         run_kernel_only(args)
     elif args.impl == "reference":

@@ -290,6 +290,15 @@ int ptycho_cnn_maxpool2_backward(const float* dout, int lddo, const void* argmax
 /* out (BF16) = in (FP32), n values: BF16 weight copies of the FP32 master weights. */
 int ptycho_cnn_cast_bf16(const float* in, void* out, int64_t n, void* stream);
 
+/* Learned-initialiser input features: for each of npos patterns (n x n, FP32,
+ * intensities or amplitudes when `amplitudes` != 0) and each bin x bin block
+ * (u, v): out[p][u*(n/bin) + v] = (sqrt(norm * block intensity sum) - mean[u*(n/bin)+v]) * scale
+ * as BF16 (mean may be NULL; norm = 1 / mean pattern total makes the features
+ * dose-independent).  One row per scan position = the channels-last input
+ * matrix of the CNN on the scan grid. */
+int ptycho_cnn_bin_features(const float* patterns, int npos, int n, int bin, int amplitudes, float norm,
+                            const float* mean, float scale, void* out, int ldo, void* stream);
+
 /* loss = mean((pred - target)^2) (device float); dpred = 2 (pred - target) / n as
  * FP32 and/or BF16 (either may be NULL).  work >= 296 doubles. */
 int ptycho_cnn_mse(const float* pred, const float* target, int64_t n, float* loss, float* dpred32, void* dpred16,

@@ -63,6 +63,7 @@ EXPORTED = (
     "ptycho_cnn_maxpool2_backward",
     "ptycho_cnn_cast_bf16",
     "ptycho_cnn_mse",
+    "ptycho_cnn_bin_features",
 )
 
 _vp = ctypes.c_void_p
@@ -132,6 +133,7 @@ def _declare(lib):
         "ptycho_cnn_maxpool2_backward": (_int, [_vp, _int, _vp, _int, _int, _int, _int, _vp, _int, _int, _vp]),
         "ptycho_cnn_cast_bf16": (_int, [_vp, _vp, _i64, _vp]),
         "ptycho_cnn_mse": (_int, [_vp, _vp, _i64, _vp, _vp, _vp, _vp, _i64, _vp]),
+        "ptycho_cnn_bin_features": (_int, [_vp, _int, _int, _int, _int, _flt, _vp, _flt, _vp, _int, _vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

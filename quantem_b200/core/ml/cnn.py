@@ -296,7 +296,17 @@ class CNN2d(torch.nn.Module):
             self.num_batches_tracked = int(torch.as_tensor(sd[pref + ".num_batches_tracked"]).item())
 
     # ------------------------------------------------------------------ compute
-    def forward(self, x: torch.Tensor) -> torch.Tensor:
+    def forward(self, x: torch.Tensor, rows: tuple | None = None) -> torch.Tensor:
+        """x: (B, in_channels, H, W) FP32, or with ``rows=(B, H, W)`` the channels-last
+        BF16 input matrix (B*H*W, in_channels rounded up to 8) itself."""
+        if rows is not None:
+            B, H, W = (int(v) for v in rows)
+            if x.dtype != torch.bfloat16 or x.dim() != 2 or tuple(x.shape) != (B * H * W, self.cin_pad):
+                raise ValueError(f"row input must be bfloat16 ({B * H * W}, {self.cin_pad})")
+            f = 2 ** self.num_layers
+            if H % f or W % f:
+                raise ValueError(f"H and W must be divisible by 2**num_layers = {f}")
+            return _CNNFn.apply(x, self.flat, self, (B, H, W))
         if x.dim() != 4 or x.shape[1] != self.in_channels:
             raise ValueError(f"expected (B, {self.in_channels}, H, W), got {tuple(x.shape)}")
         if not x.is_cuda:
@@ -304,7 +314,7 @@ class CNN2d(torch.nn.Module):
         f = 2 ** self.num_layers
         if x.shape[2] % f or x.shape[3] % f:
             raise ValueError(f"H and W must be divisible by 2**num_layers = {f}")
-        return _CNNFn.apply(x.float().contiguous(), self.flat, self)
+        return _CNNFn.apply(x.float().contiguous(), self.flat, self, None)
 
     __call__ = forward
 
@@ -365,6 +375,15 @@ class _Run:
         net = self.net
         B, H, W = self.B, self.H, self.W
         L = net.num_layers
+        if x.dim() == 2:  # channels-last BF16 rows given directly
+            x16 = x
+        else:
+            x16 = self._to_rows(x)
+        return self._forward_rows(x16)
+
+    def _to_rows(self, x: torch.Tensor) -> torch.Tensor:
+        net = self.net
+        B, H, W = self.B, self.H, self.W
         # NCHW FP32 -> channels-last BF16 (padded channels stay zero)
         x16 = self.empty(B * H * W, net.cin_pad, dtype=torch.bfloat16)
         if net.cin_pad != net.in_channels:
@@ -376,6 +395,12 @@ class _Run:
             tmp = self.empty(B, H * W, net.in_channels, dtype=torch.bfloat16)
             kk.transpose(xc, tmp)
             x16.view(B, H * W, net.cin_pad)[..., : net.in_channels].copy_(tmp)
+        return x16
+
+    def _forward_rows(self, x16: torch.Tensor) -> torch.Tensor:
+        net = self.net
+        B, H, W = self.B, self.H, self.W
+        L = net.num_layers
         self.cat = []
         self.pool_arg = []
         y = x16
@@ -598,15 +623,15 @@ def _gemm_acc(A: torch.Tensor, B: torch.Tensor, out: torch.Tensor, run: _Run):
 
 class _CNNFn(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, x, flat, net):
-        B, _, H, W = x.shape
+    def forward(ctx, x, flat, net, rows):
+        B, H, W = rows if rows is not None else (x.shape[0], x.shape[2], x.shape[3])
         net.sync_weights()
         run = _Run(net, B, H, W, net.training)
         y = run.forward(x)
         if net.training:
             net.num_batches_tracked += 1
         ctx.run = run
-        ctx.needs_x = ctx.needs_input_grad[0]
+        ctx.needs_x = ctx.needs_input_grad[0] and rows is None
         return y
 
     @staticmethod
@@ -615,7 +640,7 @@ class _CNNFn(torch.autograd.Function):
         ctx.run = None
         grad = torch.zeros_like(run.net.flat.data)
         dx = run.backward(dy.float().contiguous(), grad, ctx.needs_x)
-        return dx, grad, None
+        return dx, grad, None, None
 
 
 def mse_loss(pred: torch.Tensor, target: torch.Tensor) -> torch.Tensor:

@@ -158,3 +158,14 @@ def mse(pred, target, loss, work, dpred32=None, dpred16=None):
     _call("ptycho_cnn_mse", _p(pred), _p(target), pred.numel(), _p(loss), _p(dpred32), _p(dpred16), _p(work),
           work.numel(), _s())
     return loss
+
+
+def bin_features(patterns: torch.Tensor, bin: int, out: torch.Tensor, mean: torch.Tensor | None = None,
+                 scale: float = 1.0, amplitudes: bool = False, norm: float = 1.0) -> torch.Tensor:
+    """Rows (npos, (n/bin)^2) BF16 of sqrt-binned pattern features (see ptycho_cnn_bin_features)."""
+    if patterns.dtype != torch.float32 or not patterns.is_contiguous() or patterns.dim() != 3:
+        raise ValueError("patterns must be contiguous float32 (npos, n, n)")
+    npos, n, _ = patterns.shape
+    _call("ptycho_cnn_bin_features", _p(patterns), npos, n, int(bin), int(amplitudes), ctypes.c_float(norm),
+          _p(mean), ctypes.c_float(scale), _p(out), _ld(out, "out"), _s())
+    return out

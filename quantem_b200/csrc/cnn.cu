@@ -454,6 +454,31 @@ __global__ void mse_final_kernel(const double* part, int nparts, int64_t n, floa
   }
 }
 
+// Network input features from diffraction data: per scan position p and bin (u, v)
+// of a bin x bin block, f = sqrt(norm * sum of the block's intensities) (amplitudes
+// are squared first), then (f - mean[u*nb + v]) * scale, written as BF16 row p.
+__global__ void bin_features_kernel(const float* __restrict__ pat, int npos, int n, int bin, int amplitudes,
+                                    float norm, const float* __restrict__ mean, float scale, bf16* __restrict__ out,
+                                    int ldo) {
+  const int nb = n / bin;
+  const int64_t total = (int64_t)npos * nb * nb;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int c = (int)(i % (nb * nb));
+    const int64_t p = i / (nb * nb);
+    const int u = c / nb, v = c % nb;
+    const float* src = pat + p * n * n + (int64_t)(u * bin) * n + v * bin;
+    float s = 0.0f;
+    for (int a = 0; a < bin; ++a)
+      for (int b = 0; b < bin; ++b) {
+        const float x = src[a * n + b];
+        s += amplitudes ? x * x : x;
+      }
+    float f = sqrtf(fmaxf(s * norm, 0.0f));
+    if (mean) f -= mean[c];
+    out[p * ldo + c] = __float2bfloat16_rn(f * scale);
+  }
+}
+
 constexpr int kMseBlocks = 296;
 
 int colsum(int mode, const float* a, int lda, const float* b, int ldb, const float* mean, const float* rstd, int R,
@@ -674,6 +699,16 @@ int ptycho_cnn_mse(const float* pred, const float* target, int64_t n, float* los
   if (int rc = check_launch("mse_kernel")) return rc;
   mse_final_kernel<<<1, 32, 0, st>>>(work, kMseBlocks, n, loss);
   return check_launch("mse_final_kernel");
+}
+
+int ptycho_cnn_bin_features(const float* patterns, int npos, int n, int bin, int amplitudes, float norm,
+                            const float* mean, float scale, void* out, int ldo, void* stream) {
+  if (!patterns || !out || npos < 1 || n < 1 || bin < 1 || n % bin || ldo < (n / bin) * (n / bin))
+    return fail(PTYCHO_ERR_INVALID, "bin_features: bad arguments (n divisible by bin, ldo >= (n/bin)^2)");
+  const int64_t total = (int64_t)npos * (n / bin) * (n / bin);
+  bin_features_kernel<<<blocks_for(total, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      patterns, npos, n, bin, amplitudes, norm, mean, scale, static_cast<bf16*>(out), ldo);
+  return check_launch("bin_features_kernel");
 }
 
 }  // extern "C"

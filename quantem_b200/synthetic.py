@@ -14,6 +14,7 @@ import torch
 
 from . import ops
 from .diffractive_imaging.complex_probe import electron_wavelength_angstrom, real_space_probe
+from .diffractive_imaging.ptycho_utils import orthogonalize_probes
 
 
 @dataclass
@@ -104,7 +105,10 @@ def make_dataset(cfg: SyntheticConfig, device="cuda"):
     if cfg.jitter_px:
         pos = pos + (torch.rand(pos.shape, generator=gen, device=dev, dtype=torch.float64) * 2 - 1) * cfg.jitter_px
     pos = pos.float().contiguous()
-    probes = make_probe_modes(cfg, dev)
+    # simulate with the orthogonalised, intensity-sorted modes: the reconstruction
+    # applies the same Gram-Schmidt (probe_models.py:484-525) to its probe, which
+    # leaves these modes unchanged, so data and model describe one mixed state
+    probes = orthogonalize_probes(make_probe_modes(cfg, dev))
     props = ops.separable_propagators(cfg.n, (cfg.pixel, cfg.pixel), cfg.energy,
                                       [cfg.slice_thickness] * (cfg.slices - 1), device=dev)
     npos = pos.shape[0]
