@@ -84,6 +84,9 @@ typedef struct ptycho_batch_args {
                                 (serial variant; needs an_norm and the partials in real space) */
   float* an_norm;            /* analytic: float32 (S, P, Ho, Wo) zero-initialised accumulator of
                                 sum_patches(|psi|^2) */
+  int recompute_every;       /* n = 256 adjoint: 0 keeps every slice's incident wave; k > 0 keeps the
+                                wave entering every k-th slice and recomputes the others in the
+                                reverse sweep (smaller scratch, S - S/k extra propagations per mode) */
 } ptycho_batch_args;
 
 enum {

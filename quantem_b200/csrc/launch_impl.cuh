@@ -38,6 +38,7 @@ inline BatchParams to_params(const ptycho_batch_args* a) {
   p.loss_type = a->loss_type;
   p.analytic = a->analytic;
   p.an_norm = a->an_norm;
+  p.ckpt = a->recompute_every;
   return p;
 }
 

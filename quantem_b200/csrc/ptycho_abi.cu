@@ -7,6 +7,7 @@
 #include <string.h>
 
 #include "ptycho_b200.h"
+#include "cluster256_kernels.cuh"
 #include "ptycho_kernels.cuh"
 
 namespace {
@@ -317,12 +318,25 @@ int qb_launch_multi_64(const ptycho_batch_args* sets, int nsets, cudaStream_t st
 int qb_launch_multi_128(const ptycho_batch_args* sets, int nsets, cudaStream_t st);
 int qb_max_clusters_64(const ptycho_batch_args* a, bool adj);
 int qb_max_clusters_128(const ptycho_batch_args* a, bool adj);
+// defined in c256.cu: 256 x 256 windows on clusters of 4 CTAs
+int qb_max_clusters_256(bool adj);
+int qb_launch_c256(const ptycho_batch_args* a, bool adj, cudaStream_t st);
+int qb_fft256(const void* in, void* out, int count, bool inverse, float scale, cudaStream_t st);
 
 namespace {
 
 int validate_batch(const ptycho_batch_args* a, bool adj) {
   if (!a) return fail(PTYCHO_ERR_INVALID, "args is NULL");
-  if (a->n != 64 && a->n != 128) return fail(PTYCHO_ERR_UNSUPPORTED, "probe window n=%d not built (64, 128)", a->n);
+  if (a->n != 64 && a->n != 128 && a->n != 256)
+    return fail(PTYCHO_ERR_UNSUPPORTED, "probe window n=%d not built (64, 128, 256)", a->n);
+  if (a->n == 256) {
+    if (a->analytic) return fail(PTYCHO_ERR_UNSUPPORTED, "the analytic update is built for n = 64, 128");
+    if (a->out_exit || a->out_waves)
+      return fail(PTYCHO_ERR_UNSUPPORTED, "exit-wave / wave outputs are built for n = 64, 128");
+    if (a->recompute_every < 0 || a->recompute_every > a->S)
+      return fail(PTYCHO_ERR_INVALID, "recompute_every=%d outside [0, S=%d]", a->recompute_every, a->S);
+    if (a->B > 0 && a->grid % 4 != 0) return fail(PTYCHO_ERR_INVALID, "n=256: grid %d is not a multiple of 4", a->grid);
+  }
   if (a->S < 1 || a->P < 1 || a->B < 0 || a->Ho < 1 || a->Wo < 1 || a->npos < 1)
     return fail(PTYCHO_ERR_INVALID, "bad sizes S=%d P=%d B=%d Ho=%d Wo=%d npos=%d", a->S, a->P, a->B, a->Ho, a->Wo,
                 a->npos);
@@ -333,7 +347,7 @@ int validate_batch(const ptycho_batch_args* a, bool adj) {
     return fail(PTYCHO_ERR_INVALID, "propagators are NULL with S > 1");
   if ((a->prop_r == nullptr) != (a->prop_c == nullptr))
     return fail(PTYCHO_ERR_INVALID, "prop_r and prop_c must be given together");
-  if (a->prop_r) {
+  if (a->prop_r && a->n != 256) {  // n = 256 reads the factors through the L1 cache
     const size_t need = (size_t)(a->n == 64 ? qb::fused_smem_bytes_sep<64>(a->S) : qb::fused_smem_bytes_sep<128>(a->S));
     if (need + 1024 > 232448)
       return fail(PTYCHO_ERR_UNSUPPORTED, "separable propagators of %d slices do not fit in shared memory; pass prop",
@@ -368,6 +382,11 @@ int run_batch(const ptycho_batch_args* a, void* stream, bool adj) {
   int rc = validate_batch(a, adj);
   if (rc) return rc;
   if (a->B == 0) return PTYCHO_OK;
+  if (a->n == 256) {
+    const int lrc = qb_launch_c256(a, adj, static_cast<cudaStream_t>(stream));
+    if (lrc) return fail(lrc, "cluster256_kernel launch: %s", cudaGetErrorString(cudaGetLastError()));
+    return PTYCHO_OK;
+  }
   const int variant = a->analytic ? PTYCHO_VARIANT_SERIAL : resolve_variant(a);
   if (variant < 0) return fail(PTYCHO_ERR_UNSUPPORTED, "variant %d not available for P=%d", a->variant, a->P);
   if (variant == PTYCHO_VARIANT_CLUSTER && a->grid % a->P != 0)
@@ -413,8 +432,23 @@ int ptycho_workspace_elems(int n, int S, int P, int grid, int64_t* scratch_elems
 int ptycho_batch_plan(const ptycho_batch_args* a, int adjoint, int* variant, int* grid, int64_t* scratch_elems,
                       int64_t* partial_elems, int* partial_parts) {
   if (!a) return fail(PTYCHO_ERR_INVALID, "plan: args is NULL");
-  if (a->n != 64 && a->n != 128) return fail(PTYCHO_ERR_UNSUPPORTED, "probe window n=%d not built (64, 128)", a->n);
+  if (a->n != 64 && a->n != 128 && a->n != 256)
+    return fail(PTYCHO_ERR_UNSUPPORTED, "probe window n=%d not built (64, 128, 256)", a->n);
   if (a->S < 1 || a->P < 1 || a->B < 0) return fail(PTYCHO_ERR_INVALID, "plan: bad sizes");
+  if (a->n == 256) {  // one cluster of 4 CTAs per position; each CTA holds a quarter of every wave
+    const int mc = qb_max_clusters_256(adjoint != 0);
+    if (mc < 1) return fail(PTYCHO_ERR_UNSUPPORTED, "no cluster of 4 CTAs with %zu B shared memory fits",
+                            qb::c256_smem_bytes());
+    const int B1 = a->B > 0 ? a->B : 1;
+    const int ncl = B1 < mc ? B1 : mc;
+    const int64_t q = (int64_t)256 * 256 / 4;
+    if (variant) *variant = PTYCHO_VARIANT_CLUSTER;
+    if (grid) *grid = 4 * ncl;
+    if (scratch_elems) *scratch_elems = adjoint ? (int64_t)4 * ncl * qb::c256_slots(a->S, a->P, a->recompute_every) * q : 0;
+    if (partial_elems) *partial_elems = (int64_t)ncl * a->P * 256 * 256;
+    if (partial_parts) *partial_parts = ncl;
+    return PTYCHO_OK;
+  }
   const int v = a->analytic ? PTYCHO_VARIANT_SERIAL : resolve_variant(a);
   if (v < 0) return fail(PTYCHO_ERR_UNSUPPORTED, "variant %d not available for P=%d", a->variant, a->P);
   int sms = 0, dev = 0;
@@ -476,9 +510,13 @@ int ptycho_forward_adjoint(const ptycho_batch_args* a, void* stream) { return ru
 
 int ptycho_fft2(const void* in, void* out, int count, int n, int inverse, float scale, void* stream) {
   if (!in || !out || count < 0) return fail(PTYCHO_ERR_INVALID, "fft2: bad arguments");
-  if (n != 64 && n != 128) return fail(PTYCHO_ERR_UNSUPPORTED, "fft2: n=%d not built", n);
+  if (n != 64 && n != 128 && n != 256) return fail(PTYCHO_ERR_UNSUPPORTED, "fft2: n=%d not built", n);
   if (count == 0) return PTYCHO_OK;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (n == 256) {  // in place is safe: a cluster loads its transform before its first cluster barrier
+    if (qb_fft256(in, out, count, inverse != 0, scale, st)) return check_launch("fft256_batch_kernel");
+    return check_launch("fft256_batch_kernel");
+  }
   const float2* i2 = static_cast<const float2*>(in);
   float2* o2 = static_cast<float2*>(out);
   const int grid = count < 148 ? count : 148;

@@ -60,6 +60,7 @@ struct BatchParams {
   int loss_type;
   int analytic;               // 0: autograd adjoint; 1: analytic update (ptychography.py:339-372), serial kernel
   float* an_norm;             // (S, P, Ho, Wo) scatter of |psi|^2 for the analytic normalisation
+  int ckpt;                   // 256^2 cluster kernel: checkpoint interval of the adjoint (0 = keep all waves)
 };
 
 __device__ __forceinline__ int fsigned(int k, int n) { return k < n / 2 ? k : k - n; }

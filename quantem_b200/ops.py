@@ -14,7 +14,11 @@ import torch
 
 from . import _lib
 
-SUPPORTED_N = (64, 128)
+SUPPORTED_N = (64, 128, 256)
+
+# Adjoint checkpoint interval for 256 x 256 windows (0: keep every slice's wave;
+# k > 0: keep every k-th and recompute the rest in the reverse sweep).
+RECOMPUTE_EVERY = 0
 
 # When set to a list, every fused forward+adjoint launch appends a pair of CUDA
 # events recorded on the launching stream around it (used by bench.py to time
@@ -181,8 +185,10 @@ def default_grid(B: int, device=None) -> int:
 
 
 def _batch_args(geom, obj_c, probe_hat, prop, positions, batch_idx, targets, mask, B, loss_type, loss_scale,
-                inv_mean, grad_obj=None, out_intensity=None, out_exit=None, out_waves=None, variant="auto"):
+                inv_mean, grad_obj=None, out_intensity=None, out_exit=None, out_waves=None, variant="auto",
+                recompute_every=None):
     a = _lib.BatchArgs()
+    a.recompute_every = int(RECOMPUTE_EVERY if recompute_every is None else recompute_every)
     a.obj = obj_c.data_ptr()
     a.probe_hat = probe_hat.data_ptr()
     if isinstance(prop, (tuple, list)):
@@ -294,7 +300,7 @@ def batch_forward(obj_c, probe_o, prop, positions, batch_idx, targets, mask, num
 
 def batch_forward_adjoint(obj_c, probe_o, prop, positions, batch_idx, targets, mask, num_gpts, mean_intensity,
                           loss_type="l2_amplitude", probe_hat=None, grid=None, grad_obj=None,
-                          grad_probe=None, variant="auto"):
+                          grad_probe=None, variant="auto", recompute_every=None):
     """Fused forward + loss + adjoint of one batch.
 
     Returns (loss 0-d tensor, grad w.r.t. the constrained object (S,Ho,Wo),
@@ -317,7 +323,7 @@ def batch_forward_adjoint(obj_c, probe_o, prop, positions, batch_idx, targets, m
         return loss, grad_obj, grad_probe
     a = _batch_args(geom, obj_c, probe_hat, prop, positions, batch_idx, targets, mask, B, loss_type,
                     loss_scale_of(loss_type, B, num_gpts, mean_intensity), 1.0 / mean_intensity,
-                    grad_obj=grad_obj, variant=variant)
+                    grad_obj=grad_obj, variant=variant, recompute_every=recompute_every)
     grid_v, parts, ws = plan_and_bind(a, dev, adjoint=True, grid=grid)
     lib = _lib.lib()
     st = _stream()
