@@ -27,7 +27,7 @@ constexpr int C256_CLUSTER = 4;
 // dynamic shared memory of cluster256_kernel: exchange buffer, twiddles, shift
 // ramps, wrap maps and the CTA's quarter of the intensity / dL/dI tile
 constexpr size_t c256_smem_bytes() {
-  return sizeof(float2) * (size_t)(Fft256C::SM_FLOAT2 + 3 * 256) + sizeof(int) * 512 +
+  return sizeof(float2) * (size_t)(Fft256C::SM_FLOAT2 + Fft256C::TW_FLOAT2 + 2 * 256) + sizeof(int) * 512 +
          sizeof(float) * (size_t)Fft256C::T * Fft256C::E;
 }
 // scratch slots (each T*E float2) per CTA
@@ -43,7 +43,7 @@ __global__ void __launch_bounds__(512, 1) cluster256_kernel(const BatchParams p)
   extern __shared__ float4 smem_raw[];
   float2* sm = reinterpret_cast<float2*>(smem_raw);
   float2* tw = sm + F::SM_FLOAT2;
-  float2* rowf = tw + N;
+  float2* rowf = tw + F::TW_FLOAT2;
   float2* colf = rowf + N;
   int* rowmap = reinterpret_cast<int*>(colf + N);
   int* colmap = rowmap + N;
@@ -55,11 +55,7 @@ __global__ void __launch_bounds__(512, 1) cluster256_kernel(const BatchParams p)
   const int cid = blockIdx.x / C256_CLUSTER, ncl = gridDim.x / C256_CLUSTER;
   F f;
   f.init(tid, q);
-  for (int k = tid; k < N; k += T) {
-    double s, c;
-    sincospi(-2.0 * (double)k / (double)N, &s, &c);
-    tw[k] = make_float2((float)c, (float)s);
-  }
+  F::fill_twiddles(tw, tid, T);
   const float inv_n = 1.0f / (float)N;
   const float inv_n2 = inv_n * inv_n;
   const size_t NN = (size_t)N * N;
@@ -206,17 +202,17 @@ __global__ void __launch_bounds__(512, 1) cluster256_kernel(const BatchParams p)
         const float2* orow_ptr = p.obj + (size_t)s * HoWo + (size_t)orow * p.Wo;
         float2* grow = p.grad_obj + (size_t)s * HoWo + (size_t)orow * p.Wo;
 #pragma unroll
-        for (int e0 = 0; e0 < E; e0 += 8) {
-          float2 ps[8], ob[8];
-          int col[8];
+        for (int e0 = 0; e0 < E; e0 += 4) {
+          float2 ps[4], ob[4];
+          int col[4];
 #pragma unroll
-          for (int j = 0; j < 8; ++j) {
+          for (int j = 0; j < 4; ++j) {
             col[j] = colmap[f.a_col(e0 + j)];
             ps[j] = wv[(e0 + j) * T + tid];
             ob[j] = __ldg(orow_ptr + col[j]);
           }
 #pragma unroll
-          for (int j = 0; j < 8; ++j) {
+          for (int j = 0; j < 4; ++j) {
             const float2 g = cscale(x[e0 + j], sc);
             atomicAdd(grow + col[j], cmulc(g, ps[j]));
             x[e0 + j] = cmulc(g, ob[j]);
@@ -252,18 +248,20 @@ __global__ void __launch_bounds__(512, 1) cluster256_kernel(const BatchParams p)
           continue;
         }
         {
-          const float* tg = p.targets + (size_t)gi * NN;
-          const int dc = (kc + N / 2) & (N - 1);
+          // detector (centred) index of (kr, kc): kr = 4tl + a + 32kB shifts to 4tl + a + 32((kB + 4) % 8)
+          const int dbase = 4 * f.tl * N + ((kc + N / 2) & (N - 1));
+          const float* tg = p.targets + (size_t)gi * NN + dbase;
+          const float* mk = p.mask + dbase;
+          float* oi = p.out_intensity ? p.out_intensity + (size_t)b * NN + dbase : nullptr;
 #pragma unroll
           for (int i = 0; i < E; ++i) {
-            const int kr = f.b_kr(i);
-            const int di = ((kr + N / 2) & (N - 1)) * N + dc;
+            const int doff = ((i >> 3) + 32 * (((i & 7) + 4) & 7)) * N;
             const float I = inten[i * T + tid];
             if (!isfinite(I)) ++nonfinite;
             float dldi;
-            loss_elem<N>(p, I, __ldg(tg + di), __ldg(p.mask + di), loss_acc, dldi);
+            loss_elem<N>(p, I, __ldg(tg + doff), __ldg(mk + doff), loss_acc, dldi);
             inten[i * T + tid] = dldi;
-            if (p.out_intensity) p.out_intensity[(size_t)b * NN + di] = I;
+            if (oi) oi[doff] = I;
           }
         }
         if (!ADJ) break;
@@ -336,11 +334,7 @@ __global__ void __launch_bounds__(512, 1) fft256_batch_kernel(const float2* __re
   const int tid = threadIdx.x;
   F f;
   f.init(tid, (int)cl.block_rank());
-  for (int k = tid; k < N; k += T) {
-    double s, c;
-    sincospi(-2.0 * (double)k / (double)N, &s, &c);
-    tw[k] = make_float2((float)c, (float)s);
-  }
+  F::fill_twiddles(tw, tid, T);
   cl.sync();
   const int cid = blockIdx.x / C256_CLUSTER, ncl = gridDim.x / C256_CLUSTER;
   const size_t NN = (size_t)N * N;
@@ -369,6 +363,6 @@ __global__ void __launch_bounds__(512, 1) fft256_batch_kernel(const float2* __re
   cl.sync();
 }
 
-constexpr size_t fft256_smem_bytes() { return sizeof(float2) * (size_t)(Fft256C::SM_FLOAT2 + 256); }
+constexpr size_t fft256_smem_bytes() { return sizeof(float2) * (size_t)(Fft256C::SM_FLOAT2 + Fft256C::TW_FLOAT2); }
 
 }  // namespace qb

@@ -33,8 +33,18 @@ struct Fft256C {
   static constexpr int T = 512;
   static constexpr int E = 32;
   static constexpr int LINES = 64;
-  static constexpr int PITCH = 264;  // == 8 (mod 16) float2: line pairs fall on opposite bank halves
-  static constexpr int SM_FLOAT2 = LINES * PITCH;
+  static constexpr int SM_FLOAT2 = 17536;  // >= the largest of the three layouts below (63*274 + 271)
+  // twiddle table: tw[t*33 + k1] = w256^(t*k1), t < 8, k1 < 32 (row padding 33 keeps the
+  // eight t rows on distinct banks)
+  static constexpr int TW_FLOAT2 = 8 * 33;
+  static __device__ __forceinline__ void fill_twiddles(float2* tw, int tid, int nthreads) {
+    for (int k = tid; k < 8 * 32; k += nthreads) {
+      const int t = k >> 5, k1 = k & 31;
+      double s, c;
+      sincospi(-2.0 * (double)(t * k1) / 256.0, &s, &c);
+      tw[t * 33 + k1] = make_float2((float)c, (float)s);
+    }
+  }
 
   int q;     // cluster rank (0..3)
   int line;  // tid / 8
@@ -45,15 +55,18 @@ struct Fft256C {
     line = tid >> 3;
     tl = tid & 7;
   }
-  // line-local exchange between the 32-point and the 8-point stage: element
-  // (k1, t) of a line
-  __device__ __forceinline__ int lx(int ln, int k1, int t) const { return ln * PITCH + 8 * k1 + (t ^ (k1 >> 2)); }
-  // column-slab buffer: element (kc_local, r)
-  __device__ __forceinline__ int bx(int kcl, int r) const { return kcl * PITCH + (r ^ (((kcl >> 2) & 3) << 2)); }
-  // row-slab spectrum buffer: element (r_local, kc)
-  __device__ __forceinline__ int ax(int rl, int kc) const {
-    return rl * PITCH + (kc ^ ((kc >> 4) & 3) ^ (((rl >> 1) & 3) << 2));
-  }
+  // Buffer layouts (float2 index).  Padding is additive, so every access is a
+  // per-thread base plus a compile-time offset (one address register per loop);
+  // the paddings were chosen by exhaustive search so that each warp access of
+  // every exchange touches each of the 16 float2 bank pairs at most twice.
+  //   line-local exchange, element (k1, t) of line ln:  ln*264 + 33*(k1/4) + 8*(k1%4) + t
+  //   column slab, element (kc_local, r):               kcl*260 + 2*(kcl/4) + r
+  //   row slab spectrum, element (r_local, kc):         rl*274 + kc + kc/16
+  // (row lengths cover each padded row: 262 < 264, 256 < 260, 271 < 274)
+  static constexpr int LP = 264, BP = 260, AP = 274;
+  __device__ __forceinline__ int lx(int ln, int k1, int t) const { return ln * LP + 33 * (k1 >> 2) + 8 * (k1 & 3) + t; }
+  __device__ __forceinline__ int bx(int kcl, int r) const { return kcl * BP + 2 * (kcl >> 2) + r; }
+  __device__ __forceinline__ int ax(int rl, int kc) const { return rl * AP + kc + (kc >> 4); }
 
   // coordinates
   __device__ __forceinline__ int a_row() const { return 64 * q + line; }     // layout A row
@@ -75,19 +88,25 @@ struct Fft256C {
   template <bool INV>
   __device__ __forceinline__ void line_fwd(float2 (&x)[E], float2* sm, const float2* tw) const {
     dft_reg<32, INV>(x);
+    {
+      const float2* twr = tw + 33 * tl;
 #pragma unroll
-    for (int k1 = 1; k1 < 32; ++k1) {
-      const float2 w = tw[(tl * k1) & 255];
-      x[k1] = INV ? cmulc(x[k1], w) : cmul(x[k1], w);
+      for (int k1 = 1; k1 < 32; ++k1) x[k1] = INV ? cmulc(x[k1], twr[k1]) : cmul(x[k1], twr[k1]);
     }
     __syncthreads();
+    {
+      float2* w = sm + line * LP + tl;  // + lx offset of (k1, 0)
 #pragma unroll
-    for (int k1 = 0; k1 < 32; ++k1) sm[lx(line, k1, tl)] = x[k1];
+      for (int k1 = 0; k1 < 32; ++k1) w[33 * (k1 >> 2) + 8 * (k1 & 3)] = x[k1];
+    }
     __syncthreads();
+    {
+      const float2* r = sm + line * LP + 33 * tl;  // group g = tl: k1 = 4g + a
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+      for (int a = 0; a < 4; ++a)
 #pragma unroll
-      for (int t = 0; t < 8; ++t) x[a * 8 + t] = sm[lx(line, 4 * tl + a, t)];
+        for (int t = 0; t < 8; ++t) x[a * 8 + t] = r[8 * a + t];
+    }
     dft8_groups<INV, 0>(x);
   }
   // inverse direction of line_fwd's data flow: frequency distribution in,
@@ -96,59 +115,77 @@ struct Fft256C {
   __device__ __forceinline__ void line_bwd(float2 (&x)[E], float2* sm, const float2* tw) const {
     dft8_groups<INV, 0>(x);
     __syncthreads();
+    {
+      float2* w = sm + line * LP + 33 * tl;
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+      for (int a = 0; a < 4; ++a)
 #pragma unroll
-      for (int t = 0; t < 8; ++t) sm[lx(line, 4 * tl + a, t)] = x[a * 8 + t];
+        for (int t = 0; t < 8; ++t) w[8 * a + t] = x[a * 8 + t];
+    }
     __syncthreads();
+    {
+      const float2* r = sm + line * LP + tl;
 #pragma unroll
-    for (int k1 = 0; k1 < 32; ++k1) x[k1] = sm[lx(line, k1, tl)];
+      for (int k1 = 0; k1 < 32; ++k1) x[k1] = r[33 * (k1 >> 2) + 8 * (k1 & 3)];
+    }
+    {
+      const float2* twr = tw + 33 * tl;
 #pragma unroll
-    for (int k1 = 1; k1 < 32; ++k1) {
-      const float2 w = tw[(tl * k1) & 255];
-      x[k1] = INV ? cmulc(x[k1], w) : cmul(x[k1], w);
+      for (int k1 = 1; k1 < 32; ++k1) x[k1] = INV ? cmulc(x[k1], twr[k1]) : cmul(x[k1], twr[k1]);
     }
     dft_reg<32, INV>(x);
   }
 
   // ---- cluster exchanges ----
+  // 32-bit shared::cluster address of `local` in the CTA of cluster rank `rank`
+  static __device__ __forceinline__ uint32_t peer_addr(const void* local, uint32_t rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;"
+                 : "=r"(r)
+                 : "r"((uint32_t)__cvta_generic_to_shared(local)), "r"(rank));
+    return r;
+  }
+  static __device__ __forceinline__ void st_peer(uint32_t addr, float2 v) {
+    asm volatile("st.shared::cluster.v2.f32 [%0], {%1, %2};" ::"r"(addr), "f"(v.x), "f"(v.y) : "memory");
+  }
   // A (row spectrum, register a*8+kB holds kc = 4tl + a + 32kB of row a_row())
   //   -> B (column slab, register e holds r = tl + 8e of spectral column b_kc())
   __device__ __forceinline__ void a_to_b(float2 (&x)[E], float2* sm, cg::cluster_group& cl) const {
     cl.sync();  // every CTA of the cluster is done reading its buffer
-    const int r = a_row();
+    // bx(4tl + a + 32x, 64q + line) = [1042 tl + 64q + line] + 260a + 8336x
+    const float2* mine = sm + 1042 * tl + 64 * q + line;
 #pragma unroll
-    for (int kB = 0; kB < 8; ++kB) {
-      float2* dst = cl.map_shared_rank(sm, (unsigned)(kB >> 1));
+    for (int d = 0; d < 4; ++d) {
+      const uint32_t dst = peer_addr(mine, (uint32_t)d);
 #pragma unroll
-      for (int a = 0; a < 4; ++a) {
-        const int kcl = 4 * tl + a + 32 * (kB & 1);
-        dst[bx(kcl, r)] = x[a * 8 + kB];
-      }
+      for (int xb = 0; xb < 2; ++xb)
+#pragma unroll
+        for (int a = 0; a < 4; ++a) st_peer(dst + 8u * (uint32_t)(260 * a + 8336 * xb), x[a * 8 + 2 * d + xb]);
     }
     cl.sync();
+    const float2* r = sm + BP * line + 2 * (line >> 2) + tl;
 #pragma unroll
-    for (int e = 0; e < E; ++e) x[e] = sm[bx(line, tl + 8 * e)];
+    for (int e = 0; e < E; ++e) x[e] = r[8 * e];
   }
   // B (column slab, register e holds r = tl + 8e of spectral column b_kc())
   //   -> A (row spectrum distribution of row a_row())
   __device__ __forceinline__ void b_to_a(float2 (&x)[E], float2* sm, cg::cluster_group& cl) const {
     cl.sync();
-    const int kc = b_kc();
+    // ax(tl + 8j, 64q + line) = [274 tl + 68q + line + line/16] + 2192 j
+    const float2* mine = sm + AP * tl + 68 * q + line + (line >> 4);
 #pragma unroll
     for (int d = 0; d < 4; ++d) {
-      float2* dst = cl.map_shared_rank(sm, (unsigned)d);
+      const uint32_t dst = peer_addr(mine, (uint32_t)d);
 #pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const int e = 8 * d + j;
-        dst[ax(tl + 8 * j, kc)] = x[e];  // r = tl + 8e, local row r - 64d = tl + 8j
-      }
+      for (int j = 0; j < 8; ++j) st_peer(dst + 8u * (uint32_t)(8 * AP * j), x[8 * d + j]);
     }
     cl.sync();
+    // ax(line, 4tl + a + 32kB) = [274 line + 4tl + tl/4] + a + 34kB
+    const float2* r = sm + AP * line + 4 * tl + (tl >> 2);
 #pragma unroll
     for (int a = 0; a < 4; ++a)
 #pragma unroll
-      for (int kB = 0; kB < 8; ++kB) x[a * 8 + kB] = sm[ax(line, 4 * tl + a + 32 * kB)];
+      for (int kB = 0; kB < 8; ++kB) x[a * 8 + kB] = r[a + 34 * kB];
   }
 
   // ---- whole 2-D transforms (unnormalised) ----

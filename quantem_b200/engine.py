@@ -95,6 +95,7 @@ class ProblemTensors:
     orthogonalize: bool = True
     loss_type: str = "l2_amplitude"
     grid: int | None = None
+    recompute_every: int | None = None   # 256 x 256 windows: adjoint checkpoint interval (None/0: keep all)
     extra: dict = field(default_factory=dict)
 
     @property
@@ -110,7 +111,8 @@ def batch_step(pt: ProblemTensors, batch_idx: torch.Tensor, optimizers=(), autog
         opt.zero_grad(set_to_none=True)
     probe_o = orthogonalize_probes(pt.probe) if pt.orthogonalize else pt.probe
     loss = ops.batch_loss(pt.obj, probe_o, pt.prop, pt.positions, batch_idx, pt.targets, pt.mask,
-                          pt.num_gpts, pt.mean_intensity, pt.loss_type, grid=pt.grid)
+                          pt.num_gpts, pt.mean_intensity, pt.loss_type, grid=pt.grid,
+                          recompute_every=pt.recompute_every)
     if autograd and (pt.obj.requires_grad or pt.probe.requires_grad):
         loss.backward()
         if pt.obj.grad is not None:

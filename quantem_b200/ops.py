@@ -400,7 +400,8 @@ class _BatchLossFn(torch.autograd.Function):
         if need:
             loss, g_obj_c, g_probe = batch_forward_adjoint(
                 obj_c, probe_c, prop, positions, batch_idx, targets, mask, cfg["num_gpts"],
-                cfg["mean_intensity"], cfg["loss_type"], grid=cfg.get("grid"), variant=cfg.get("variant", "auto"))
+                cfg["mean_intensity"], cfg["loss_type"], grid=cfg.get("grid"), variant=cfg.get("variant", "auto"),
+                recompute_every=cfg.get("recompute_every"))
             ctx.save_for_backward(obj_raw_c, work, g_obj_c, g_probe)
         else:
             loss = batch_forward(obj_c, probe_c, prop, positions, batch_idx, targets, mask, cfg["num_gpts"],
@@ -420,11 +421,12 @@ class _BatchLossFn(torch.autograd.Function):
 
 
 def batch_loss(obj_raw, probe_o, prop, positions, batch_idx, targets, mask, num_gpts, mean_intensity,
-               loss_type="l2_amplitude", grid=None, variant="auto"):
+               loss_type="l2_amplitude", grid=None, variant="auto", recompute_every=None):
     """Differentiable consistency loss of one batch w.r.t. the raw object
-    parameter (hard constraint included) and the orthogonalised probe."""
+    parameter (hard constraint included) and the orthogonalised probe.
+    ``recompute_every`` (256 x 256 windows): adjoint checkpoint interval."""
     cfg = dict(num_gpts=int(num_gpts), mean_intensity=float(mean_intensity), loss_type=loss_type, grid=grid,
-               variant=variant)
+               variant=variant, recompute_every=recompute_every)
     return _BatchLossFn.apply(obj_raw, probe_o, prop, positions, batch_idx, targets, mask, cfg)
 
 
