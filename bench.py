@@ -682,6 +682,65 @@ def run_c4(args):
     }))
 
 
+def run_c5_kernel(args):
+    """One 256^2 cluster forward+adjoint launch over --positions positions (profiling case):
+    16 slices, 6 modes, scan just large enough, every wave kept."""
+    import torch
+
+    from quantem_b200 import ops, synthetic
+
+    dev = torch.device("cuda", 0)
+    side = int(math.ceil(math.sqrt(args.positions)))
+    cfg = synthetic.SyntheticConfig(n=256, slices=16, modes=6, mode_weights=(0.5, 0.2, 0.1, 0.08, 0.07, 0.05),
+                                    scan=(side, side), step_px=6.0, pad_px=131, counts=1e6, seed=0)
+    ds = synthetic.make_dataset(cfg, dev)
+    npos = ds["positions"].shape[0]
+    probe_o = (ds["probes"] * (ds["mean_intensity"] / ds["probes"].abs().square().sum()) ** 0.5).contiguous()
+    obj_c, _ = ops.obj_constrain(torch.ones(ds["obj_shape"], dtype=torch.complex64, device=dev))
+    idx = torch.arange(args.positions, device=dev, dtype=torch.int64)
+    run = lambda: ops.batch_forward_adjoint(obj_c, probe_o, ds["propagators"], ds["positions"], idx,  # noqa: E731
+                                            ds["amplitudes"].contiguous(), torch.ones((256, 256), device=dev),
+                                            npos, ds["mean_intensity"], recompute_every=args.recompute_every)
+    for _ in range(args.warmup):
+        run()
+    ops.PROFILE_EVENTS = []
+    for _ in range(args.steps):
+        run()
+    torch.cuda.synchronize()
+    ms = statistics.median(a.elapsed_time(b) for a, b in ops.PROFILE_EVENTS)
+    ops.PROFILE_EVENTS = None
+    flops = 4 * 6 * 16 * 5 * 256 ** 2 * 16 + 40 * 6 * 16 * 256 ** 2
+    print(json.dumps({"workload": "c5 kernel: 256^2, 16 slices, 6 modes, forward+adjoint",
+                      "positions": args.positions, "recompute_every": args.recompute_every,
+                      "ms_per_launch": round(ms, 3), "positions_per_s": round(args.positions / (ms * 1e-3), 1),
+                      "fp32_tflops": round(flops * args.positions / (ms * 1e-3) / 1e12, 2)}))
+
+
+def run_c4_gemm(args):
+    """The first-layer convolution GEMM of a c4 training step alone (profiling case)."""
+    import torch
+
+    from quantem_b200.core.ml import kernels as kk
+
+    dev = torch.device("cuda", 0)
+    M, K, N = 16 * 32 * 32, 9 * 1024, 32
+    A = torch.randn(M, K, device=dev).to(torch.bfloat16)
+    B = torch.randn(N, K, device=dev).to(torch.bfloat16)
+    C = torch.empty(M, N, device=dev)
+    for _ in range(args.warmup):
+        kk.gemm(A, B, C)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        kk.gemm(A, B, C)
+    e1.record()
+    torch.cuda.synchronize()
+    s_ = e0.elapsed_time(e1) / 1e3 / args.steps
+    byt = 2 * M * K + 2 * N * K + 4 * M * N
+    print(json.dumps({"workload": "c4 first-layer conv GEMM", "M": M, "N": N, "K": K, "ms": round(s_ * 1e3, 4),
+                      "gbs": round(byt / s_ / 1e9, 1), "tflops": round(2 * M * N * K / s_ / 1e12, 2)}))
+
+
 def run_c5(args):
     """Large multislice: 1024x1024x16 object, 6 modes at 256x256 on 4-CTA clusters, 128x128 scan
     (16384 positions, 6 px step, jitter), 1e6 counts, full-batch Adam iterations.  The
@@ -773,6 +832,7 @@ def main():
                     help="c2: the headline multislice mixed-probe iteration; c3: uneven multi-dataset launch; "
                          "c4: learned initialiser vs flat start; c5: 256x256 windows on thread-block clusters")
     ap.add_argument("--c4-objects", type=int, default=20000, help="training objects for --workload c4")
+    ap.add_argument("--recompute-every", type=int, default=0, help="adjoint checkpoint interval (--workload c5)")
     ap.add_argument("--c4-iters", type=int, default=120, help="refinement iterations per arm for --workload c4")
     ap.add_argument("--skip-torch-reference", action="store_true",
                     help="do not time the PyTorch-eager restatement of the reference path")
@@ -785,9 +845,9 @@ def main():
     if args.workload == "c3":
         run_c3(args)
     elif args.workload == "c4":
-        run_c4(args)
+        run_c4_gemm(args) if args.kernel_only else run_c4(args)
     elif args.workload == "c5":
-        run_c5(args)
+        run_c5_kernel(args) if args.kernel_only else run_c5(args)
     elif args.kernel_only:
         run_kernel_only(args)
     elif args.impl == "reference":

@@ -82,7 +82,10 @@ __global__ void __launch_bounds__(512, 1) cluster256_kernel(const BatchParams p)
   double loss_acc = 0.0;
   int nonfinite = 0;
 
-  for (int b = cid; b < p.B; b += ncl) {
+  // each cluster takes a contiguous block of the batch (concurrent positions far apart)
+  const int bchunk = (p.B + ncl - 1) / ncl;
+  const int bend = min(p.B, (cid + 1) * bchunk);
+  for (int b = cid * bchunk; b < bend; ++b) {
     const int64_t gi = p.batch_idx[b];
     if (gi < 0 || gi >= p.npos) {  // the whole cluster skips the position (same b)
       if (tid == 0 && q == 0 && p.status) atomicAdd(p.status, 1 << 20);

@@ -75,7 +75,9 @@ __global__ void __launch_bounds__(4 * N, 1) cluster_batch_kernel(const BatchPara
   double loss_acc = 0.0;
   int nonfinite = 0;
 
-  for (int b = cid; b < p.B; b += ncl) {
+  const int bchunk = (p.B + ncl - 1) / ncl;  // contiguous block of the batch per cluster
+  const int bend = min(p.B, (cid + 1) * bchunk);
+  for (int b = cid * bchunk; b < bend; ++b) {
     const int64_t gi = p.batch_idx[b];
     if (gi < 0 || gi >= p.npos) {  // uniform across the cluster: every CTA skips it
       if (m == 0 && tid == 0 && p.status) atomicAdd(p.status, 1 << 20);

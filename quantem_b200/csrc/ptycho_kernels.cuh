@@ -248,7 +248,12 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
   double loss_acc = 0.0;
   int nonfinite = 0;
 
-  for (int b = cta; b < p.B; b += ncta) {
+  // each CTA takes a contiguous block of the batch: positions processed at the same
+  // time are far apart in the batch order, so raster-ordered batches do not pile
+  // the object-gradient atomics of neighbouring windows onto the same addresses
+  const int bchunk = (p.B + ncta - 1) / ncta;
+  const int bend = min(p.B, (cta + 1) * bchunk);
+  for (int b = cta * bchunk; b < bend; ++b) {
     const int64_t gi = p.batch_idx[b];
     if (gi < 0 || gi >= p.npos) {  // invalid index: skip the position and report it
       if (tid == 0 && p.status) atomicAdd(p.status, 1 << 20);
