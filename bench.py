@@ -684,20 +684,21 @@ def run_c4(args):
 
 def run_c5_kernel(args):
     """One 256^2 cluster forward+adjoint launch over --positions positions (profiling case):
-    16 slices, 6 modes, scan just large enough, every wave kept."""
+    the 1024x1024x16 / 6-mode / 128x128-scan problem, a seeded random subset of the
+    positions (as a shuffled batch of the reconstruction), --recompute-every."""
     import torch
 
     from quantem_b200 import ops, synthetic
 
     dev = torch.device("cuda", 0)
-    side = int(math.ceil(math.sqrt(args.positions)))
     cfg = synthetic.SyntheticConfig(n=256, slices=16, modes=6, mode_weights=(0.5, 0.2, 0.1, 0.08, 0.07, 0.05),
-                                    scan=(side, side), step_px=6.0, pad_px=131, counts=1e6, seed=0)
+                                    scan=(128, 128), step_px=6.0, pad_px=131, counts=1e6, seed=0)
     ds = synthetic.make_dataset(cfg, dev)
     npos = ds["positions"].shape[0]
     probe_o = (ds["probes"] * (ds["mean_intensity"] / ds["probes"].abs().square().sum()) ** 0.5).contiguous()
     obj_c, _ = ops.obj_constrain(torch.ones(ds["obj_shape"], dtype=torch.complex64, device=dev))
-    idx = torch.arange(args.positions, device=dev, dtype=torch.int64)
+    g = torch.Generator().manual_seed(0)
+    idx = torch.randperm(npos, generator=g)[:args.positions].to(dev)
     run = lambda: ops.batch_forward_adjoint(obj_c, probe_o, ds["propagators"], ds["positions"], idx,  # noqa: E731
                                             ds["amplitudes"].contiguous(), torch.ones((256, 256), device=dev),
                                             npos, ds["mean_intensity"], recompute_every=args.recompute_every)

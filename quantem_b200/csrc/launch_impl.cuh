@@ -55,7 +55,12 @@ int launch_serial(const ptycho_batch_args* a, bool adj, cudaStream_t st) {
                           : batch_smem_bytes<N, false>(a->prop_r != nullptr, a->S);
   // the attribute is per device; setting it on every launch keeps multi-device
   // processes correct and costs far less than one launch
-  if (adj) {
+  if (adj && a->analytic) {
+    cudaFuncSetAttribute(fused_batch_kernel<N, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(fused_batch_kernel<N, true, true>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         (int)((smem + 1024) * 100 / (228 * 1024) + 1));
+    fused_batch_kernel<N, true, true><<<a->grid, 4 * N, smem, st>>>(p);
+  } else if (adj) {
     cudaFuncSetAttribute(fused_batch_kernel<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     // smallest shared-memory carve-out that fits: the rest of the 256 KB is L1 for spills
     cudaFuncSetAttribute(fused_batch_kernel<N, true>, cudaFuncAttributePreferredSharedMemoryCarveout,

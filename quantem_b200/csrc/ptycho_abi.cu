@@ -496,6 +496,8 @@ int ptycho_forward_adjoint_multi(const ptycho_batch_args* sets, int nsets, void*
       return fail(rc, "multi: dataset %d: %s", d, why);
     }
     if (sets[d].n != sets[0].n) return fail(PTYCHO_ERR_INVALID, "multi: every dataset needs the same probe window");
+    if (sets[d].n == 256 || sets[d].analytic)
+      return fail(PTYCHO_ERR_UNSUPPORTED, "multi: datasets with n = 64 / 128 and the autograd adjoint only");
     if (sets[d].grid < 1) return fail(PTYCHO_ERR_INVALID, "multi: dataset %d has grid %d", d, sets[d].grid);
     total += sets[d].grid;
   }

@@ -195,8 +195,10 @@ __device__ __forceinline__ void accumulate_probe_grad(const Fft2<N>& f, const fl
 
 // Body of the serial batch kernel for one dataset: CTA `cta` of the `ncta` CTAs
 // that work on this dataset's positions.
-template <int N, bool ADJ>
+template <int N, bool ADJ, bool AN = false>
 __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta, const int ncta) {
+  // AN (compile time): analytic update directions instead of the autograd adjoint,
+  // so the autograd kernel carries none of the analytic code or live values
   using F = Fft2<N>;
   constexpr int E = F::E, D = F::D, G3 = F::G3, T = F::T;
   extern __shared__ float4 smem_raw[];
@@ -302,7 +304,7 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
     float* tile2 = ADJ ? inten + NN : nullptr;
     auto load_far_seed = [&](int mm) {
       const float2* fw = slot + (size_t)(P * S + mm) * NN;
-      if (p.analytic) {
+      if (AN) {
 #pragma unroll
         for (int e = 0; e < E; ++e) {
           const float2 v = fw[e * T + tid];
@@ -360,13 +362,13 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
             atomicAdd(grow + col[j], cmulc(g, ps[j]));  // conj(psi) * g
             x[e0 + j] = cmulc(g, ob[j]);                 // conj(o) * g
           }
-          if (p.analytic) {  // sum_patches(|psi|^2) of this slice and mode (object_models.py:701-703)
+          if (AN) {  // sum_patches(|psi|^2) of this slice and mode (object_models.py:701-703)
             float* nrow = p.an_norm + ((size_t)s * P + m) * HoWo + (size_t)orow * p.Wo;
 #pragma unroll
             for (int j = 0; j < 8; ++j) atomicAdd(nrow + col[j], cabs2(ps[j]));
           }
         }
-        if (p.analytic && s == 0) {
+        if (AN && s == 0) {
           // analytic probe update: sum over positions of the back-propagated
           // gradient at the probe plane, no inverse shift (probe_models.py:774-783)
           float2* pg = pgrad + (size_t)m * NN + (size_t)f.s1_r * N;
@@ -405,7 +407,7 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
         }
 #pragma unroll
         for (int e = 0; e < E; ++e) inten[e * T + tid] = (m == 0 ? 0.f : inten[e * T + tid]) + cabs2(x[e]);
-        if (ADJ && p.analytic) {  // sum_p |Psi_p + 1e-9|^2 (ptychography_base.py:958)
+        if (ADJ && AN) {  // sum_p |Psi_p + 1e-9|^2 (ptychography_base.py:958)
 #pragma unroll
           for (int e = 0; e < E; ++e)
             tile2[e * T + tid] = (m == 0 ? 0.f : tile2[e * T + tid]) + cabs2(make_float2(x[e].x + 1e-9f, x[e].y));
@@ -430,7 +432,7 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
               float dldi;
               const float tv = __ldg(tg + di);
               loss_elem<N>(p, I, tv, __ldg(p.mask + di), loss_acc, dldi);
-              if (ADJ && p.analytic) {
+              if (ADJ && AN) {
                 // factor f and additive fix of the Fourier projection seed
                 const int li = (g * D + e) * T + tid;
                 if (P == 1) {
@@ -485,9 +487,9 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
   if (p.status && nonfinite) atomicAdd(p.status, nonfinite);
 }
 
-template <int N, bool ADJ>
+template <int N, bool ADJ, bool AN = false>
 __global__ void __launch_bounds__(4 * N, 1) fused_batch_kernel(const BatchParams p) {
-  serial_body<N, ADJ>(p, blockIdx.x, gridDim.x);
+  serial_body<N, ADJ, AN>(p, blockIdx.x, gridDim.x);
 }
 
 // Several independent datasets (same probe window N; any S, P, object size,
