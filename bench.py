@@ -463,9 +463,9 @@ def run_kernel_only(args):
 
 def run_c3(args):
     """Uneven multi-dataset workload: six independent datasets (scans 24^2 ... 64^2,
-    slice counts 1..8, one probe mode, 128 x 128 windows) in one persistent launch
-    per iteration, the iteration captured in a CUDA graph, CTA partition from the
-    autotuner.  Compared with the same iteration run eagerly and with one launch
+    slice counts 1..8, one probe mode, 96 x 96 and 128 x 128 windows) in one
+    persistent launch per window size per iteration, the iteration captured in a
+    CUDA graph, CTA partition from the autotuner.  Compared with the same iteration run eagerly and with one launch
     per dataset."""
     import torch
 
@@ -473,18 +473,19 @@ def run_c3(args):
     from quantem_b200.diffractive_imaging.ptycho_utils import SimpleBatcher
 
     dev = torch.device("cuda", 0)
-    specs = [(24, 1), (32, 2), (40, 3), (48, 5), (56, 6), (64, 8)]
+    # (scan, slices, probe window): 96 x 96 and 128 x 128 windows alternate
+    specs = [(24, 1, 96), (32, 2, 128), (40, 3, 96), (48, 5, 128), (56, 6, 96), (64, 8, 128)]
 
     def make():
         probs = []
-        for k, (scan, S) in enumerate(specs):
-            cfg = synthetic.SyntheticConfig(n=128, slices=S, modes=1, mode_weights=(1.0,), scan=(scan, scan),
-                                            step_px=4.0, pad_px=64, seed=100 + k)
+        for k, (scan, S, n) in enumerate(specs):
+            cfg = synthetic.SyntheticConfig(n=n, slices=S, modes=1, mode_weights=(1.0,), scan=(scan, scan),
+                                            step_px=4.0, pad_px=n // 2, seed=100 + k)
             ds = synthetic.make_dataset(cfg, dev)
             obj = torch.ones(ds["obj_shape"], dtype=torch.complex64, device=dev).requires_grad_(True)
             probe = (ds["probes"] * ds["mean_intensity"] ** 0.5).contiguous().requires_grad_(True)
             probs.append(multi.Problem(obj, probe, ds["propagators"], ds["positions"], ds["amplitudes"].contiguous(),
-                                       torch.ones((128, 128), device=dev), ds["mean_intensity"], cfg.step_px))
+                                       torch.ones((n, n), device=dev), ds["mean_intensity"], cfg.step_px))
         return probs
 
     probs = make()
@@ -523,8 +524,8 @@ def run_c3(args):
     for _ in range(args.warmup):
         loop()
     ms_loop = timed(loop, args.steps)
-    print(json.dumps({"workload": "c3: 6 datasets, scans 24^2-64^2, 1-8 slices, 1 mode, 128x128 windows "
-                                  "(96x96 windows of the configuration not built: 128x128 used for all six)",
+    print(json.dumps({"workload": "c3: 6 datasets, scans 24^2-64^2, 1-8 slices, 1 mode, 96x96 and 128x128 "
+                                  "windows (one persistent launch per window size, one CUDA graph)",
                       "positions": npos, "grids": grids, "unit": "positions/s",
                       "graphed_persistent": round(npos / (ms_graph * 1e-3), 1),
                       "eager_persistent": round(npos / (ms_eager * 1e-3), 1),

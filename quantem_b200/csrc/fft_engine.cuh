@@ -24,7 +24,8 @@
 // i.e. two wavefronts per 256-byte warp access, the minimum for 8-byte words.
 //
 // Supported N: 64 (A=16,B=4,C=4,D=16, 256 threads) and 128 (A=32,B=4,C=8,D=16,
-// 512 threads).
+// 512 threads); 96 is a specialisation at the end of this file (192 threads,
+// mixed radix 3 x 2^k).
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -297,6 +298,267 @@ struct Fft2 {
     s3<false>(x);
   }
   // Inverse: registers in S3 layout -> registers in S1 layout (unnormalised).
+  __device__ __forceinline__ void inverse(float2 (&x)[E], float2* sm, const float2* tw) const {
+    s3<true>(x);
+    __syncthreads();
+    write_s3(sm, x);
+    __syncthreads();
+    read_s2_out(sm, x);
+    s2_inv(x, tw);
+    __syncthreads();
+    write_s2_in(sm, x);
+    __syncthreads();
+    read_s1(sm, x);
+    s1<true>(x);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// mixed radix (N = 3 * 2^k) for 96 x 96 windows
+// ---------------------------------------------------------------------------
+// cos(2*pi*m/96) for m = 0..24 (first quadrant), IEEE double rounded to float.
+__device__ __forceinline__ float qcos96(int m) {
+  switch (m) {
+    case 0: return 1.0f;
+    case 1: return 0.9978589232386035f;
+    case 2: return 0.9914448613738104f;
+    case 3: return 0.9807852804032304f;
+    case 4: return 0.9659258262890683f;
+    case 5: return 0.9469301294951057f;
+    case 6: return 0.9238795325112867f;
+    case 7: return 0.8968727415326884f;
+    case 8: return 0.8660254037844387f;
+    case 9: return 0.8314696123025452f;
+    case 10: return 0.7933533402912352f;
+    case 11: return 0.7518398074789774f;
+    case 12: return 0.7071067811865476f;
+    case 13: return 0.6593458151000688f;
+    case 14: return 0.6087614290087207f;
+    case 15: return 0.5555702330196024f;
+    case 16: return 0.5000000000000001f;
+    case 17: return 0.44228869021900125f;
+    case 18: return 0.38268343236508984f;
+    case 19: return 0.3214394653031617f;
+    case 20: return 0.25881904510252074f;
+    case 21: return 0.19509032201612833f;
+    case 22: return 0.1305261922200517f;
+    case 23: return 0.06540312923014327f;
+    default: return 0.0f;
+  }
+}
+// Multiply by w_96^m (forward exp(-2 pi i m/96), inverse its conjugate); m a
+// compile-time constant after unrolling, quarter turns exact.
+template <bool INV>
+__device__ __forceinline__ float2 twmul96(float2 a, int m) {
+  m %= 96;
+  if (m < 0) m += 96;
+  if (m == 0) return a;
+  if (m == 24) return INV ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+  if (m == 48) return make_float2(-a.x, -a.y);
+  if (m == 72) return INV ? make_float2(a.y, -a.x) : make_float2(-a.y, a.x);
+  const int q = m / 24, r = m % 24;
+  float c, s;  // cos / sin(2 pi m / 96)
+  if (q == 0) { c = qcos96(r); s = qcos96(24 - r); }
+  else if (q == 1) { c = -qcos96(24 - r); s = qcos96(r); }
+  else if (q == 2) { c = -qcos96(r); s = -qcos96(24 - r); }
+  else { c = qcos96(24 - r); s = -qcos96(r); }
+  if (!INV) s = -s;
+  return cmul(a, make_float2(c, s));
+}
+// 3-point DFT in place: (a, b, c) -> (X0, X1, X2), w3 = exp(-+2 pi i / 3).
+template <bool INV>
+__device__ __forceinline__ void dft3(float2& a, float2& b, float2& c) {
+  const float h = 0.8660254037844386f;  // sin(pi / 3)
+  const float2 t1 = cadd(b, c);
+  const float2 t2 = make_float2(fmaf(-0.5f, t1.x, a.x), fmaf(-0.5f, t1.y, a.y));
+  const float2 d = csub(b, c);
+  // forward: -i * sin(pi/3) * (b - c); inverse: +i * sin(pi/3) * (b - c)
+  const float2 t3 = INV ? make_float2(-h * d.y, h * d.x) : make_float2(h * d.y, -h * d.x);
+  a = cadd(a, t1);
+  b = cadd(t2, t3);
+  c = csub(t2, t3);
+}
+// In-register N-point DFT for N = 3*M (M a power of two) or a power of two, on
+// x[OFF + STRIDE*i], natural order in and out: three M-point DFTs over the
+// residues of i mod 3, twiddles w_N^(r*k), M three-point DFTs, register rename.
+template <int N, bool INV, int STRIDE = 1, int OFF = 0, int LEN>
+__device__ __forceinline__ void dft_reg_n(float2 (&x)[LEN]) {
+  if constexpr ((N & (N - 1)) == 0) {
+    dft_reg<N, INV, STRIDE, OFF>(x);
+  } else {
+    static_assert(N % 3 == 0 && ((N / 3) & (N / 3 - 1)) == 0 && 96 % N == 0, "N = 3 * 2^k dividing 96");
+    constexpr int M = N / 3;
+    dft_reg<M, INV, 3 * STRIDE, OFF>(x);
+    dft_reg<M, INV, 3 * STRIDE, OFF + STRIDE>(x);
+    dft_reg<M, INV, 3 * STRIDE, OFF + 2 * STRIDE>(x);
+#pragma unroll
+    for (int k = 1; k < M; ++k) {
+      x[OFF + STRIDE * (3 * k + 1)] = twmul96<INV>(x[OFF + STRIDE * (3 * k + 1)], (96 / N) * k);
+      x[OFF + STRIDE * (3 * k + 2)] = twmul96<INV>(x[OFF + STRIDE * (3 * k + 2)], (96 / N) * 2 * k);
+    }
+#pragma unroll
+    for (int k = 0; k < M; ++k)
+      dft3<INV>(x[OFF + STRIDE * (3 * k)], x[OFF + STRIDE * (3 * k + 1)], x[OFF + STRIDE * (3 * k + 2)]);
+    float2 y[N];  // X[k + M j] sits at position 3k + j
+#pragma unroll
+    for (int k = 0; k < M; ++k)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) y[k + M * j] = x[OFF + STRIDE * (3 * k + j)];
+#pragma unroll
+    for (int i = 0; i < N; ++i) x[OFF + STRIDE * i] = y[i];
+  }
+}
+
+// 96 x 96 engine: T = 192 threads (6 warps), E = 48 complex registers each.
+//   columns c = cB + 2*cA (A = 48, B = 2), rows r = rD + 4*rC (C = 24, D = 4)
+//   S1: 48-point DFT over cA for fixed (r, cB)               -> kA
+//   S2: twiddle w96^(cB*kA); 2-point over cB; 24-point over rC; twiddle w96^(rD*kC)
+//   S3: 4-point DFT over rD for 12 (kC, column) groups        -> kD
+// Exchange layouts (float2 index): stage 1<->2 element (r, cB, kA) at r + 100 kA + 4800 cB,
+// stage 2<->3 element (row, col) at 104 row + col; both verified to give two wavefronts per
+// warp access with the lane maps of init().
+template <>
+struct Fft2<96> {
+  static constexpr int N = 96, A = 48, B = 2, C = 24, D = 4;
+  static constexpr int T = 192;
+  static constexpr int E = 48;
+  static constexpr int G3 = 12;
+  static constexpr int SM_FLOAT2 = 9976;
+
+  int s1_r, s1_cB;
+  int s2_rD, s2_kA;
+  int s3_c, s3_kC0;
+
+  __device__ __forceinline__ void init(int tid) {
+    const int lane = tid & 31, w = tid >> 5;
+    s1_r = (lane & 15) + 16 * w;
+    s1_cB = lane >> 4;
+    s2_rD = lane & 3;
+    s2_kA = (lane >> 2) + 8 * w;
+    s3_c = lane + 32 * (w % 3);
+    s3_kC0 = w / 3;
+  }
+  __device__ __forceinline__ int s3_kC(int g) const { return s3_kC0 + 2 * g; }
+  __device__ __forceinline__ int s1_col(int e) const { return s1_cB + B * e; }
+  __device__ __forceinline__ int s3_row(int g, int e) const { return s3_kC(g) + C * e; }
+
+  __device__ __forceinline__ void write_s1(float2* sm, const float2 (&x)[E]) const {
+    float2* w = sm + s1_r + 4800 * s1_cB;
+#pragma unroll
+    for (int e = 0; e < A; ++e) w[100 * e] = x[e];
+  }
+  __device__ __forceinline__ void read_s1(const float2* sm, float2 (&x)[E]) const {
+    const float2* r = sm + s1_r + 4800 * s1_cB;
+#pragma unroll
+    for (int e = 0; e < A; ++e) x[e] = r[100 * e];
+  }
+  // S2 input layout (cB, rC): element (rD + 4 rC, cB, kA)
+  __device__ __forceinline__ void read_s2_in(const float2* sm, float2 (&x)[E]) const {
+    const float2* r = sm + s2_rD + 100 * s2_kA;
+#pragma unroll
+    for (int cB = 0; cB < B; ++cB)
+#pragma unroll
+      for (int rC = 0; rC < C; ++rC) x[cB * C + rC] = r[4 * rC + 4800 * cB];
+  }
+  __device__ __forceinline__ void write_s2_in(float2* sm, const float2 (&x)[E]) const {
+    float2* w = sm + s2_rD + 100 * s2_kA;
+#pragma unroll
+    for (int cB = 0; cB < B; ++cB)
+#pragma unroll
+      for (int rC = 0; rC < C; ++rC) w[4 * rC + 4800 * cB] = x[cB * C + rC];
+  }
+  // S2 output layout (kB, kC): element (row rD + 4 kC, col kA + 48 kB)
+  __device__ __forceinline__ void write_s2_out(float2* sm, const float2 (&x)[E]) const {
+    float2* w = sm + 104 * s2_rD + s2_kA;
+#pragma unroll
+    for (int kB = 0; kB < B; ++kB)
+#pragma unroll
+      for (int kC = 0; kC < C; ++kC) w[416 * kC + 48 * kB] = x[kB * C + kC];
+  }
+  __device__ __forceinline__ void read_s2_out(const float2* sm, float2 (&x)[E]) const {
+    const float2* r = sm + 104 * s2_rD + s2_kA;
+#pragma unroll
+    for (int kB = 0; kB < B; ++kB)
+#pragma unroll
+      for (int kC = 0; kC < C; ++kC) x[kB * C + kC] = r[416 * kC + 48 * kB];
+  }
+  // S3 layout (g, e): element (row e + 4 kC_g, col)
+  __device__ __forceinline__ void read_s3(const float2* sm, float2 (&x)[E]) const {
+    const float2* r = sm + 104 * 4 * s3_kC0 + s3_c;
+#pragma unroll
+    for (int g = 0; g < G3; ++g)
+#pragma unroll
+      for (int e = 0; e < D; ++e) x[g * D + e] = r[104 * (e + 8 * g)];
+  }
+  __device__ __forceinline__ void write_s3(float2* sm, const float2 (&x)[E]) const {
+    float2* w = sm + 104 * 4 * s3_kC0 + s3_c;
+#pragma unroll
+    for (int g = 0; g < G3; ++g)
+#pragma unroll
+      for (int e = 0; e < D; ++e) w[104 * (e + 8 * g)] = x[g * D + e];
+  }
+
+  template <bool INV>
+  __device__ __forceinline__ void s1(float2 (&x)[E]) const { dft_reg_n<A, INV, 1, 0>(x); }
+  template <bool INV, int G>
+  __device__ __forceinline__ void s3_groups(float2 (&x)[E]) const {
+    if constexpr (G < G3) {
+      dft_reg<D, INV, 1, G * D>(x);
+      s3_groups<INV, G + 1>(x);
+    }
+  }
+  template <bool INV>
+  __device__ __forceinline__ void s3(float2 (&x)[E]) const { s3_groups<INV, 0>(x); }
+
+  template <bool INV>
+  __device__ __forceinline__ void s2_core(float2 (&x)[E]) const {
+#pragma unroll
+    for (int rC = 0; rC < C; ++rC) {  // 2-point DFT over cB
+      const float2 a = x[rC], b = x[C + rC];
+      x[rC] = cadd(a, b);
+      x[C + rC] = csub(a, b);
+    }
+    dft_reg_n<C, INV, 1, 0>(x);
+    dft_reg_n<C, INV, 1, C>(x);
+  }
+  __device__ __forceinline__ void s2_fwd(float2 (&x)[E], const float2* tw) const {
+    const float2 w1 = tw[s2_kA];  // w96^(1 * kA)
+#pragma unroll
+    for (int rC = 0; rC < C; ++rC) x[C + rC] = cmul(x[C + rC], w1);
+    s2_core<false>(x);
+#pragma unroll
+    for (int kC = 1; kC < C; ++kC) {
+      const float2 w = tw[s2_rD * kC];  // rD * kC <= 69 < 96
+#pragma unroll
+      for (int kB = 0; kB < B; ++kB) x[kB * C + kC] = cmul(x[kB * C + kC], w);
+    }
+  }
+  __device__ __forceinline__ void s2_inv(float2 (&x)[E], const float2* tw) const {
+#pragma unroll
+    for (int kC = 1; kC < C; ++kC) {
+      const float2 w = tw[s2_rD * kC];
+#pragma unroll
+      for (int kB = 0; kB < B; ++kB) x[kB * C + kC] = cmulc(x[kB * C + kC], w);
+    }
+    s2_core<true>(x);
+    const float2 w1 = tw[s2_kA];
+#pragma unroll
+    for (int rC = 0; rC < C; ++rC) x[C + rC] = cmulc(x[C + rC], w1);
+  }
+
+  __device__ __forceinline__ void forward(float2 (&x)[E], float2* sm, const float2* tw) const {
+    s1<false>(x);
+    __syncthreads();
+    write_s1(sm, x);
+    __syncthreads();
+    read_s2_in(sm, x);
+    s2_fwd(x, tw);
+    __syncthreads();
+    write_s2_out(sm, x);
+    __syncthreads();
+    read_s3(sm, x);
+    s3<false>(x);
+  }
   __device__ __forceinline__ void inverse(float2 (&x)[E], float2* sm, const float2* tw) const {
     s3<true>(x);
     __syncthreads();

@@ -1,0 +1,6 @@
+// Serial-mode batch kernels instantiated for a 96 x 96 probe window (mixed radix 3 x 2^k).
+#include "launch_impl.cuh"
+
+int qb_launch_serial_96(const ptycho_batch_args* a, bool adj, cudaStream_t st) {
+  return qb::launch_serial<96>(a, adj, st);
+}

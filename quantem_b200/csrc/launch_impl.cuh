@@ -59,16 +59,16 @@ int launch_serial(const ptycho_batch_args* a, bool adj, cudaStream_t st) {
     cudaFuncSetAttribute(fused_batch_kernel<N, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaFuncSetAttribute(fused_batch_kernel<N, true, true>, cudaFuncAttributePreferredSharedMemoryCarveout,
                          (int)((smem + 1024) * 100 / (228 * 1024) + 1));
-    fused_batch_kernel<N, true, true><<<a->grid, 4 * N, smem, st>>>(p);
+    fused_batch_kernel<N, true, true><<<a->grid, Fft2<N>::T, smem, st>>>(p);
   } else if (adj) {
     cudaFuncSetAttribute(fused_batch_kernel<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     // smallest shared-memory carve-out that fits: the rest of the 256 KB is L1 for spills
     cudaFuncSetAttribute(fused_batch_kernel<N, true>, cudaFuncAttributePreferredSharedMemoryCarveout,
                          (int)((smem + 1024) * 100 / (228 * 1024) + 1));
-    fused_batch_kernel<N, true><<<a->grid, 4 * N, smem, st>>>(p);
+    fused_batch_kernel<N, true><<<a->grid, Fft2<N>::T, smem, st>>>(p);
   } else {
     cudaFuncSetAttribute(fused_batch_kernel<N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    fused_batch_kernel<N, false><<<a->grid, 4 * N, smem, st>>>(p);
+    fused_batch_kernel<N, false><<<a->grid, Fft2<N>::T, smem, st>>>(p);
   }
   return cudaPeekAtLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_CUDA;
 }
@@ -89,7 +89,7 @@ int launch_multi(const ptycho_batch_args* sets, int nsets, cudaStream_t st) {
   cudaFuncSetAttribute(multi_batch_kernel<N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   cudaFuncSetAttribute(multi_batch_kernel<N, true>, cudaFuncAttributePreferredSharedMemoryCarveout,
                        (int)((smem + 1024) * 100 / (228 * 1024) + 1));
-  multi_batch_kernel<N, true><<<mp.begin[nsets], 4 * N, smem, st>>>(mp);
+  multi_batch_kernel<N, true><<<mp.begin[nsets], Fft2<N>::T, smem, st>>>(mp);
   return cudaPeekAtLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_CUDA;
 }
 

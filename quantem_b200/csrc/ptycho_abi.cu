@@ -312,6 +312,9 @@ int qb_record_error(int code, const char* msg) { return fail(code, "%s", msg); }
 // defined in fused_n{64,128}.cu and cluster_n{64,128}.cu
 int qb_launch_serial_64(const ptycho_batch_args* a, bool adj, cudaStream_t st);
 int qb_launch_serial_128(const ptycho_batch_args* a, bool adj, cudaStream_t st);
+// defined in fused_n96.cu / multi_n96.cu: 96 x 96 windows (serial variant only)
+int qb_launch_serial_96(const ptycho_batch_args* a, bool adj, cudaStream_t st);
+int qb_launch_multi_96(const ptycho_batch_args* sets, int nsets, cudaStream_t st);
 int qb_launch_cluster_64(const ptycho_batch_args* a, bool adj, cudaStream_t st);
 int qb_launch_cluster_128(const ptycho_batch_args* a, bool adj, cudaStream_t st);
 int qb_launch_multi_64(const ptycho_batch_args* sets, int nsets, cudaStream_t st);
@@ -327,10 +330,12 @@ namespace {
 
 int validate_batch(const ptycho_batch_args* a, bool adj) {
   if (!a) return fail(PTYCHO_ERR_INVALID, "args is NULL");
-  if (a->n != 64 && a->n != 128 && a->n != 256)
-    return fail(PTYCHO_ERR_UNSUPPORTED, "probe window n=%d not built (64, 128, 256)", a->n);
+  if (a->n != 64 && a->n != 96 && a->n != 128 && a->n != 256)
+    return fail(PTYCHO_ERR_UNSUPPORTED, "probe window n=%d not built (64, 96, 128, 256)", a->n);
+  if (a->n == 96 && a->variant == PTYCHO_VARIANT_CLUSTER)
+    return fail(PTYCHO_ERR_UNSUPPORTED, "n=96 runs on the serial variant");
   if (a->n == 256) {
-    if (a->analytic) return fail(PTYCHO_ERR_UNSUPPORTED, "the analytic update is built for n = 64, 128");
+    if (a->analytic) return fail(PTYCHO_ERR_UNSUPPORTED, "the analytic update is built for n = 64, 96, 128");
     if (a->out_exit || a->out_waves)
       return fail(PTYCHO_ERR_UNSUPPORTED, "exit-wave / wave outputs are built for n = 64, 128");
     if (a->recompute_every < 0 || a->recompute_every > a->S)
@@ -348,7 +353,9 @@ int validate_batch(const ptycho_batch_args* a, bool adj) {
   if ((a->prop_r == nullptr) != (a->prop_c == nullptr))
     return fail(PTYCHO_ERR_INVALID, "prop_r and prop_c must be given together");
   if (a->prop_r && a->n != 256) {  // n = 256 reads the factors through the L1 cache
-    const size_t need = (size_t)(a->n == 64 ? qb::fused_smem_bytes_sep<64>(a->S) : qb::fused_smem_bytes_sep<128>(a->S));
+    const size_t need = (size_t)(a->n == 64 ? qb::fused_smem_bytes_sep<64>(a->S)
+                                            : (a->n == 96 ? qb::fused_smem_bytes_sep<96>(a->S)
+                                                          : qb::fused_smem_bytes_sep<128>(a->S)));
     if (need + 1024 > 232448)
       return fail(PTYCHO_ERR_UNSUPPORTED, "separable propagators of %d slices do not fit in shared memory; pass prop",
                   a->S);
@@ -372,7 +379,8 @@ int validate_batch(const ptycho_batch_args* a, bool adj) {
 // PTYCHO_VARIANT_CLUSTER or PTYCHO_VARIANT_SERIAL for this configuration, or -1.
 int resolve_variant(const ptycho_batch_args* a) {
   if (a->variant == PTYCHO_VARIANT_SERIAL) return PTYCHO_VARIANT_SERIAL;
-  if (a->variant == PTYCHO_VARIANT_CLUSTER) return (a->P >= 1 && a->P <= 8) ? PTYCHO_VARIANT_CLUSTER : -1;
+  if (a->variant == PTYCHO_VARIANT_CLUSTER)
+    return (a->n != 96 && a->P >= 1 && a->P <= 8) ? PTYCHO_VARIANT_CLUSTER : -1;
   // measured on B200 (8 slices, 4 modes, 128^2): serial 5.9 ms vs cluster 6.9 ms per 592 positions
   if (a->variant == PTYCHO_VARIANT_AUTO) return PTYCHO_VARIANT_SERIAL;
   return -1;
@@ -394,7 +402,8 @@ int run_batch(const ptycho_batch_args* a, void* stream, bool adj) {
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const bool cl = variant == PTYCHO_VARIANT_CLUSTER;
   const int lrc = cl ? (a->n == 64 ? qb_launch_cluster_64(a, adj, st) : qb_launch_cluster_128(a, adj, st))
-                     : (a->n == 64 ? qb_launch_serial_64(a, adj, st) : qb_launch_serial_128(a, adj, st));
+                     : (a->n == 64 ? qb_launch_serial_64(a, adj, st)
+                                   : (a->n == 96 ? qb_launch_serial_96(a, adj, st) : qb_launch_serial_128(a, adj, st)));
   if (lrc) return fail(lrc, "fused_batch_kernel launch: %s", cudaGetErrorString(cudaGetLastError()));
   return PTYCHO_OK;
 }
@@ -432,8 +441,8 @@ int ptycho_workspace_elems(int n, int S, int P, int grid, int64_t* scratch_elems
 int ptycho_batch_plan(const ptycho_batch_args* a, int adjoint, int* variant, int* grid, int64_t* scratch_elems,
                       int64_t* partial_elems, int* partial_parts) {
   if (!a) return fail(PTYCHO_ERR_INVALID, "plan: args is NULL");
-  if (a->n != 64 && a->n != 128 && a->n != 256)
-    return fail(PTYCHO_ERR_UNSUPPORTED, "probe window n=%d not built (64, 128, 256)", a->n);
+  if (a->n != 64 && a->n != 96 && a->n != 128 && a->n != 256)
+    return fail(PTYCHO_ERR_UNSUPPORTED, "probe window n=%d not built (64, 96, 128, 256)", a->n);
   if (a->S < 1 || a->P < 1 || a->B < 0) return fail(PTYCHO_ERR_INVALID, "plan: bad sizes");
   if (a->n == 256) {  // one cluster of 4 CTAs per position; each CTA holds a quarter of every wave
     const int mc = qb_max_clusters_256(adjoint != 0);
@@ -503,7 +512,9 @@ int ptycho_forward_adjoint_multi(const ptycho_batch_args* sets, int nsets, void*
   }
   if (total > 65535) return fail(PTYCHO_ERR_INVALID, "multi: %ld CTAs in total", total);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  const int lrc = sets[0].n == 64 ? qb_launch_multi_64(sets, nsets, st) : qb_launch_multi_128(sets, nsets, st);
+  const int lrc = sets[0].n == 64 ? qb_launch_multi_64(sets, nsets, st)
+                                   : (sets[0].n == 96 ? qb_launch_multi_96(sets, nsets, st)
+                                                      : qb_launch_multi_128(sets, nsets, st));
   if (lrc) return fail(lrc, "multi_batch_kernel launch: %s", cudaGetErrorString(cudaGetLastError()));
   return PTYCHO_OK;
 }
@@ -512,7 +523,7 @@ int ptycho_forward_adjoint(const ptycho_batch_args* a, void* stream) { return ru
 
 int ptycho_fft2(const void* in, void* out, int count, int n, int inverse, float scale, void* stream) {
   if (!in || !out || count < 0) return fail(PTYCHO_ERR_INVALID, "fft2: bad arguments");
-  if (n != 64 && n != 128 && n != 256) return fail(PTYCHO_ERR_UNSUPPORTED, "fft2: n=%d not built", n);
+  if (n != 64 && n != 96 && n != 128 && n != 256) return fail(PTYCHO_ERR_UNSUPPORTED, "fft2: n=%d not built", n);
   if (count == 0) return PTYCHO_OK;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (n == 256) {  // in place is safe: a cluster loads its transform before its first cluster barrier
@@ -526,6 +537,12 @@ int ptycho_fft2(const void* in, void* out, int count, int n, int inverse, float 
     const size_t smem = qb::fft2_smem_bytes<64>();
     if (inverse) qb::fft2_batch_kernel<64, true><<<grid, 256, smem, st>>>(i2, o2, count, scale);
     else qb::fft2_batch_kernel<64, false><<<grid, 256, smem, st>>>(i2, o2, count, scale);
+  } else if (n == 96) {
+    const size_t smem = qb::fft2_smem_bytes<96>();
+    cudaFuncSetAttribute(qb::fft2_batch_kernel<96, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(qb::fft2_batch_kernel<96, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (inverse) qb::fft2_batch_kernel<96, true><<<grid, qb::Fft2<96>::T, smem, st>>>(i2, o2, count, scale);
+    else qb::fft2_batch_kernel<96, false><<<grid, qb::Fft2<96>::T, smem, st>>>(i2, o2, count, scale);
   } else {
     const size_t smem = qb::fft2_smem_bytes<128>();
     cudaFuncSetAttribute(qb::fft2_batch_kernel<128, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

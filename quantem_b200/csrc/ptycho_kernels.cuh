@@ -178,15 +178,17 @@ template <int N>
 __device__ __forceinline__ void accumulate_probe_grad(const Fft2<N>& f, const float2 (&x)[Fft2<N>::E], float2* pg,
                                                       const float2* rowf, const float2* colf) {
   constexpr int D = Fft2<N>::D, G3 = Fft2<N>::G3;
+  constexpr int BT = D < 8 ? D : 8;  // batch of read-modify-writes within one D-point group
+  static_assert(D % BT == 0, "batch must divide the group");
 #pragma unroll
   for (int g = 0; g < G3; ++g)
 #pragma unroll
-    for (int e0 = 0; e0 < D; e0 += 8) {
-      float2 old[8];
+    for (int e0 = 0; e0 < D; e0 += BT) {
+      float2 old[BT];
 #pragma unroll
-      for (int j = 0; j < 8; ++j) old[j] = pg[(size_t)f.s3_row(g, e0 + j) * N + f.s3_c];
+      for (int j = 0; j < BT; ++j) old[j] = pg[(size_t)f.s3_row(g, e0 + j) * N + f.s3_c];
 #pragma unroll
-      for (int j = 0; j < 8; ++j) {
+      for (int j = 0; j < BT; ++j) {
         const int kr = f.s3_row(g, e0 + j), kc = f.s3_c;
         pg[(size_t)kr * N + kc] = cadd(old[j], cmulc(x[g * D + e0 + j], cmul(rowf[kr], colf[kc])));
       }
@@ -201,6 +203,7 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
   // so the autograd kernel carries none of the analytic code or live values
   using F = Fft2<N>;
   constexpr int E = F::E, D = F::D, G3 = F::G3, T = F::T;
+  static_assert(E % 8 == 0, "gathers and scatters go in batches of 8 registers");
   extern __shared__ float4 smem_raw[];
   float2* sm = reinterpret_cast<float2*>(smem_raw);
   float2* tw = sm + F::SM_FLOAT2;
@@ -426,7 +429,7 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
 #pragma unroll
             for (int e = 0; e < D; ++e) {
               const int kr = f.s3_row(g, e), kc = f.s3_c;
-              const int di = ((kr + N / 2) & (N - 1)) * N + ((kc + N / 2) & (N - 1));
+              const int di = ((kr + N / 2) % N) * N + ((kc + N / 2) % N);
               const float I = inten[(g * D + e) * T + tid];
               if (!isfinite(I)) ++nonfinite;
               float dldi;
@@ -488,7 +491,7 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
 }
 
 template <int N, bool ADJ, bool AN = false>
-__global__ void __launch_bounds__(4 * N, 1) fused_batch_kernel(const BatchParams p) {
+__global__ void __launch_bounds__(Fft2<N>::T, 1) fused_batch_kernel(const BatchParams p) {
   serial_body<N, ADJ, AN>(p, blockIdx.x, gridDim.x);
 }
 
@@ -504,7 +507,7 @@ struct MultiParams {
 };
 
 template <int N, bool ADJ>
-__global__ void __launch_bounds__(4 * N, 1) multi_batch_kernel(const __grid_constant__ MultiParams mp) {
+__global__ void __launch_bounds__(Fft2<N>::T, 1) multi_batch_kernel(const __grid_constant__ MultiParams mp) {
   int d = 0;
   while (d + 1 < mp.nd && (int)blockIdx.x >= mp.begin[d + 1]) ++d;
   serial_body<N, ADJ>(mp.d[d], (int)blockIdx.x - mp.begin[d], mp.begin[d + 1] - mp.begin[d]);
@@ -513,7 +516,7 @@ __global__ void __launch_bounds__(4 * N, 1) multi_batch_kernel(const __grid_cons
 // Batched 2-D FFT of (count, N, N) arrays, one CTA per transform, natural layout
 // in and out, result multiplied by `scale`.
 template <int N, bool INV>
-__global__ void __launch_bounds__(4 * N, 1) fft2_batch_kernel(const float2* in, float2* out, int count,
+__global__ void __launch_bounds__(Fft2<N>::T, 1) fft2_batch_kernel(const float2* in, float2* out, int count,
                                                              float scale) {
   using F = Fft2<N>;
   constexpr int E = F::E, D = F::D, G3 = F::G3, T = F::T;

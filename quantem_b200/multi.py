@@ -3,7 +3,8 @@ iterations and the launch autotuner.
 
 A "dataset" is one ptychography problem (object, probe modes, propagators,
 positions, measured amplitudes).  Datasets that share a probe window run in one
-``ptycho_forward_adjoint_multi`` launch whose CTAs are partitioned between them;
+``ptycho_forward_adjoint_multi`` launch whose CTAs are partitioned between them
+(datasets with 96 x 96 and 128 x 128 windows: one launch per window size);
 the partition comes from ``autotune_grids`` (timed candidates, cached per
 problem signature).  ``GraphedMultiIteration`` captures one full iteration of all
 datasets (probe orthogonalisation and its autograd backward, hard constraint,
@@ -50,9 +51,29 @@ class Problem:
         return float(B) * P * (4 * S + 2)  # transforms per position: P(2S + 1) forward + P(2S + 1) adjoint
 
 
+def _window_groups(problems):
+    """Indices of the datasets per probe window (one persistent launch each)."""
+    groups = {}
+    for i, pr in enumerate(problems):
+        groups.setdefault(int(pr.probe.shape[-1]), []).append(i)
+    return list(groups.values())
+
+
 def default_grids(problems, total=None):
-    """CTAs per dataset proportional to its transform count (at least one)."""
+    """CTAs per dataset proportional to its transform count (at least one); each
+    probe-window group (a launch of its own) splits the whole SM count."""
     total = total or ops.sm_count(problems[0].obj.device)
+    groups = _window_groups(problems)
+    if len(groups) > 1:
+        out = [0] * len(problems)
+        for idx in groups:
+            for i, g in zip(idx, _split(([problems[i] for i in idx]), total)):
+                out[i] = g
+        return out
+    return _split(problems, total)
+
+
+def _split(problems, total):
     cost = np.array([p.cost() for p in problems])
     raw = np.maximum(1, np.floor(cost / cost.sum() * total)).astype(int)
     B = np.array([p.signature()[-1] for p in problems])
@@ -64,7 +85,21 @@ def default_grids(problems, total=None):
 
 
 def multi_forward_adjoint(problems, obj_cs, probe_os, grids):
-    """One launch for all datasets; returns per dataset (loss, grad obj_c, grad probe_o)."""
+    """One persistent launch per probe window for all datasets (typically one);
+    returns per dataset (loss, grad obj_c, grad probe_o) in the input order."""
+    groups = _window_groups(problems)
+    if len(groups) > 1:
+        res = [None] * len(problems)
+        for idx in groups:
+            sub = _multi_launch([problems[i] for i in idx], [obj_cs[i] for i in idx], [probe_os[i] for i in idx],
+                                [grids[i] for i in idx])
+            for i, r in zip(idx, sub):
+                res[i] = r
+        return res
+    return _multi_launch(problems, obj_cs, probe_os, grids)
+
+
+def _multi_launch(problems, obj_cs, probe_os, grids):
     n = problems[0].probe.shape[-1]
     args = (_lib.BatchArgs * len(problems))()
     keep, outs = [], []

@@ -14,7 +14,7 @@ import torch
 
 from . import _lib
 
-SUPPORTED_N = (64, 128, 256)
+SUPPORTED_N = (64, 96, 128, 256)
 
 # Adjoint checkpoint interval for 256 x 256 windows (0: keep every slice's wave;
 # k > 0: keep every k-th and recompute the rest in the reverse sweep).
