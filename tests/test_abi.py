@@ -32,9 +32,12 @@ def test_host_side_validation_without_gpu():
     assert lib.ptycho_forward_loss(None, None) == 1
     assert "NULL" in _lib.last_error()
     a = _lib.BatchArgs()
-    a.n = 96
-    assert lib.ptycho_forward_adjoint(ctypes.byref(a), None) == 2  # 96 x 96 window not built
-    assert "96" in _lib.last_error()
+    a.n = 80
+    assert lib.ptycho_forward_adjoint(ctypes.byref(a), None) == 2  # 80 x 80 window not built
+    assert "80" in _lib.last_error()
+    a.n, a.recompute_every, a.S = 256, 5, 3
+    assert lib.ptycho_forward_adjoint(ctypes.byref(a), None) == 1  # checkpoint interval beyond S
+    a.recompute_every = 0
     a.n, a.S, a.P, a.B, a.Ho, a.Wo, a.npos = 128, 2, 1, 4, 64, 64, 4
     assert lib.ptycho_forward_loss(ctypes.byref(a), None) == 1      # missing pointers
     assert lib.ptycho_reduce_loss(None, 1, None, None) == 1
