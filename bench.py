@@ -807,6 +807,43 @@ def run_c5(args):
         "fp32_peak_tflops": (round(fp32, 2) if fp32 else None), "results": out}))
 
 
+def run_preprocess(args):
+    """PtychographyDatasetRaster.preprocess (CoM, plane fit, rotation, intensity
+    normalisation) on the 64x64-scan, 128x128-pattern dataset: host path vs GPU kernels."""
+    import numpy as np
+    import torch
+
+    from quantem_b200 import synthetic
+    from quantem_b200.diffractive_imaging import Dataset4dstem, PtychographyDatasetRaster
+
+    dev = torch.device("cuda", 0)
+    cfg = synthetic.SyntheticConfig(seed=0)
+    ds = synthetic.make_dataset(cfg, dev)
+    # raw 4D data: the simulated counts back in detector (centred) layout order, scan 64 x 64
+    raw = torch.fft.fftshift(ds["intensities"], dim=(-2, -1)).view(64, 64, 128, 128).cpu().numpy()
+    res = {}
+    for where in ("cpu", "cuda"):
+        times = []
+        for _ in range(2 if where == "cpu" else 4):
+            d4 = Dataset4dstem.from_array(raw, sampling=(1.2, 1.2, 1 / 25.6, 1 / 25.6),
+                                          units=("A", "A", "A^-1", "A^-1"))
+            pd = PtychographyDatasetRaster.from_dataset4dstem(d4, verbose=0)
+            torch.cuda.synchronize()
+            t0 = time.time()
+            pd.preprocess(com_fit_function="plane", force_com_rotation=0, force_com_transpose=False,
+                          plot_rotation=False, plot_com=False, probe_energy=300e3, device=where)
+            torch.cuda.synchronize()
+            times.append(time.time() - t0)
+        res[where] = dict(seconds=round(min(times), 4), on=pd._preprocessed_on,
+                          mean_intensity=pd.mean_diffraction_intensity)
+    print(json.dumps({"workload": "dataset preprocess: 64x64 scan, 128x128 patterns (CoM, plane fit, "
+                                  "rotation search, Fourier-shift centring)",
+                      "host_s": res["cpu"]["seconds"], "gpu_s": res["cuda"]["seconds"],
+                      "speedup": round(res["cpu"]["seconds"] / res["cuda"]["seconds"], 1),
+                      "mean_intensity_rel_diff": abs(res["cpu"]["mean_intensity"] - res["cuda"]["mean_intensity"])
+                      / res["cpu"]["mean_intensity"]}))
+
+
 def run_reference(args):
     rank, world, _ = _dist_env()
     if rank != 0:
@@ -830,7 +867,7 @@ def main():
     ap.add_argument("--batch-size", type=int, default=4096)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--kernel-only", action="store_true", help="time only the fused batch kernel")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5"],
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5", "preprocess"],
                     help="c2: the headline multislice mixed-probe iteration; c3: uneven multi-dataset launch; "
                          "c4: learned initialiser vs flat start; c5: 256x256 windows on thread-block clusters")
     ap.add_argument("--c4-objects", type=int, default=20000, help="training objects for --workload c4")
@@ -850,6 +887,8 @@ def main():
         run_c4_gemm(args) if args.kernel_only else run_c4(args)
     elif args.workload == "c5":
         run_c5_kernel(args) if args.kernel_only else run_c5(args)
+    elif args.workload == "preprocess":
+        run_preprocess(args)
     elif args.kernel_only:
         run_kernel_only(args)
     elif args.impl == "reference":

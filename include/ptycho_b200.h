@@ -307,6 +307,35 @@ int ptycho_cnn_bin_features(const float* patterns, int npos, int n, int bin, int
 int ptycho_cnn_mse(const float* pred, const float* target, int64_t n, float* loss, float* dpred32, void* dpred16,
                    double* work, int64_t work_elems, void* stream);
 
+/* ------------------------------------------------------------------------
+ * Dataset preprocessing on the GPU (PtychographyDatasetRaster.preprocess,
+ * dataset_models.py:946-1025).
+ * ------------------------------------------------------------------------ */
+
+/* Centre of mass of npos patterns (nr x nc, FP32), optionally times a detector
+ * mask: com[p] = sum(I r)/sum(I), com[npos + p] = sum(I c)/sum(I) in pixels
+ * (replaces _set_intensities_com, dataset_models.py:1058-1073).  FP64 sums. */
+int ptycho_pattern_com(const float* intensities, const float* mask, int npos, int nr, int nc, double* com,
+                       void* stream);
+
+/* I = max(I, 0), a = sqrt(I) for `count` values: writes the clipped intensities
+ * and amplitudes (either may be NULL), a complex64 copy of a for the Fourier
+ * shift, and sums[0] = sum I, sums[1] = sum a (FP64, fixed order through `work`,
+ * >= 1184 doubles).  First half of the per-position loop of
+ * _normalize_diffraction_intensities (dataset_models.py:1419-1427). */
+int ptycho_pattern_prepare(const float* intensities, int64_t count, float* intensities_out, float* amplitudes_out,
+                           void* amplitudes_c, double* work, int64_t work_elems, double* sums, void* stream);
+
+/* spectra (npos, n, n) complex64 *= exp(-2 pi i (cs_p qc + rs_p qr)), rs = shifts[p],
+ * cs = shifts[npos + p], q = fftfreq(n): the Fourier-shift ramp of shift_array
+ * (ptycho_utils.py:264-271) between ptycho_fft2 forward and inverse. */
+int ptycho_pattern_shift_ramp(void* spectra, const double* shifts, int npos, int n, void* stream);
+
+/* centred amplitudes = fftshift(max(Re(shifted) * scale, 0)) (n even) and their
+ * squares (dataset_models.py:1429-1435). */
+int ptycho_pattern_center(const void* shifted, int npos, int n, float scale, float* centered_amplitudes,
+                          float* centered_intensities, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

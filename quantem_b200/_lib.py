@@ -64,6 +64,10 @@ EXPORTED = (
     "ptycho_cnn_cast_bf16",
     "ptycho_cnn_mse",
     "ptycho_cnn_bin_features",
+    "ptycho_pattern_com",
+    "ptycho_pattern_prepare",
+    "ptycho_pattern_shift_ramp",
+    "ptycho_pattern_center",
 )
 
 _vp = ctypes.c_void_p
@@ -134,6 +138,10 @@ def _declare(lib):
         "ptycho_cnn_cast_bf16": (_int, [_vp, _vp, _i64, _vp]),
         "ptycho_cnn_mse": (_int, [_vp, _vp, _i64, _vp, _vp, _vp, _vp, _i64, _vp]),
         "ptycho_cnn_bin_features": (_int, [_vp, _int, _int, _int, _int, _flt, _vp, _flt, _vp, _int, _vp]),
+        "ptycho_pattern_com": (_int, [_vp, _vp, _int, _int, _int, _vp, _vp]),
+        "ptycho_pattern_prepare": (_int, [_vp, _i64, _vp, _vp, _vp, _vp, _i64, _vp, _vp]),
+        "ptycho_pattern_shift_ramp": (_int, [_vp, _vp, _int, _int, _vp]),
+        "ptycho_pattern_center": (_int, [_vp, _int, _int, _flt, _vp, _vp, _vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

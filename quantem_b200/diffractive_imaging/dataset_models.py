@@ -265,8 +265,14 @@ class PtychographyDatasetRaster(OptimizerMixin):
                    force_com_rotation: float | None = None, force_com_transpose: bool | None = None,
                    bilinear: bool = False, padded_diffraction_intensities_shape=None, obj_padding_px=(0, 0),
                    plot_rotation: bool = True, plot_com: str | bool = True, vectorized: bool = True,
-                   probe_energy: float | None = None):
-        """dataset_models.py:946-1025 (plots are not produced)."""
+                   probe_energy: float | None = None, device=None):
+        """dataset_models.py:946-1025 (plots are not produced).
+
+        ``device`` (default: the dataset's device): on a CUDA device the centre of
+        mass and the intensity normalisation run in the GPU kernels
+        (``ptycho_pattern_*`` + ``ptycho_fft2``) and the targets stay on the device;
+        otherwise they run vectorised on the host.  Only the small CoM fit and the
+        rotation search stay on the host in both cases."""
         if padded_diffraction_intensities_shape is not None:
             raise NotImplementedError("padded diffraction intensities are not part of the B200 path")
         if bilinear:
@@ -275,26 +281,46 @@ class PtychographyDatasetRaster(OptimizerMixin):
                                           force_com_transpose=force_com_transpose, obj_padding_px=obj_padding_px)
         if probe_energy is not None:
             self.probe_energy = probe_energy
+        dev = torch.device(config.validate_device(device if device is not None else self._device)[0])
+        n = int(self.roi_shape[0])
+        from .. import ops
+
+        gpu = dev.type == "cuda" and self.roi_shape[0] == self.roi_shape[1] and n in ops.SUPPORTED_N
+        self._preprocessed_on = "gpu" if gpu else "host"
+        if gpu:
+            self._inten_dev = torch.as_tensor(self.intensities_4d).to(dev, torch.float32).contiguous()
         self._set_intensities_com(self.intensities_4d, com_fit_function)
         self._set_com_relative_rotation(force_com_rotation, force_com_transpose)
         self._normalize_diffraction_intensities()
+        self._inten_dev = None
         self._set_initial_scan_positions_px(obj_padding_px)
         self._set_patch_indices(obj_padding_px)
         self._set_targets("l2_amplitude")
         self._preprocessed = True
 
     def _set_intensities_com(self, intensities, fit_function):
-        """Vectorised centre of mass (dataset_models.py:1027-1112)."""
+        """Vectorised centre of mass (dataset_models.py:1027-1112); on the GPU when
+        preprocess runs there (``ptycho_pattern_com``, FP64 sums)."""
         dt = config.get("dtype_real")
-        kr = np.arange(intensities.shape[-2])
-        kc = np.arange(intensities.shape[-1])
-        krm, kcm = np.meshgrid(kr, kc, indexing="ij")
-        im = intensities.astype(dt)
-        com_r = np.sum(im * krm[None, None], axis=(-2, -1))
-        com_c = np.sum(im * kcm[None, None], axis=(-2, -1))
-        tot = np.sum(im, axis=(-2, -1))
-        com_r /= tot
-        com_c /= tot
+        if getattr(self, "_inten_dev", None) is not None:
+            from .. import _lib, ops
+
+            x = self._inten_dev
+            nr, nc, qr, qc = x.shape
+            com = torch.empty(2 * nr * nc, dtype=torch.float64, device=x.device)
+            _lib.check(_lib.lib().ptycho_pattern_com(ops._p(x), None, nr * nc, qr, qc, ops._p(com), ops._stream()),
+                       "pattern_com")
+            com_r, com_c = com.view(2, nr, nc).cpu().numpy().astype(dt)
+        else:
+            kr = np.arange(intensities.shape[-2])
+            kc = np.arange(intensities.shape[-1])
+            krm, kcm = np.meshgrid(kr, kc, indexing="ij")
+            im = intensities.astype(dt)
+            com_r = np.sum(im * krm[None, None], axis=(-2, -1))
+            com_c = np.sum(im * kcm[None, None], axis=(-2, -1))
+            tot = np.sum(im, axis=(-2, -1))
+            com_r /= tot
+            com_c /= tot
         if fit_function == "none":
             fr, fc = com_r, com_c
         elif fit_function == "no_shift":
@@ -355,6 +381,8 @@ class PtychographyDatasetRaster(OptimizerMixin):
         """Centred target amplitudes (dataset_models.py:1372-1480), vectorised over
         positions: amplitude = sqrt(max(I,0)) Fourier-shifted by -CoM_fit,
         clipped at 0 and fftshifted."""
+        if getattr(self, "_inten_dev", None) is not None:
+            return self._normalize_diffraction_intensities_gpu()
         dt = config.get("dtype_real")
         di = self.intensities_4d.astype(dt)
         inten = np.maximum(di, 0)
@@ -378,6 +406,53 @@ class PtychographyDatasetRaster(OptimizerMixin):
         self._intensities = torch.as_tensor(inten.reshape(-1, *roi))
         self._centered_intensities = torch.as_tensor(centered_i.reshape(-1, *roi))
         self.mean_diffraction_intensity = mean_intensity / npos
+        descan = -1 * self.com_fit.reshape((2, -1)) + self.roi_shape[:, None] / 2
+        self._descan_shifts = torch.as_tensor(descan.T.astype(dt))
+        self._initial_descan_shifts = self._descan_shifts.clone()
+
+    def _normalize_diffraction_intensities_gpu(self, chunk: int = 2048):
+        """GPU version of the normalisation: clip / sqrt / sums (ptycho_pattern_prepare),
+        forward FFT, shift ramp of -CoM_fit (ptycho_pattern_shift_ramp), inverse FFT,
+        clip + fftshift (ptycho_pattern_center), in chunks of ``chunk`` patterns.
+        FP32 transforms (the host path and the reference use FP64 numpy FFTs)."""
+        from .. import _lib, ops
+
+        x = self._inten_dev
+        nr, nc, n, _ = x.shape
+        npos = nr * nc
+        dev = x.device
+        lib, st = _lib.lib(), ops._stream()
+        flat = x.view(npos, n, n)
+        inten = torch.empty_like(flat)
+        amp = torch.empty_like(flat)
+        camp = torch.empty_like(flat)
+        cint = torch.empty_like(flat)
+        shifts = torch.as_tensor(-(np.asarray(self.com_fit, dtype=np.float64).reshape(2, -1) + 0.0), device=dev)
+        work = torch.empty(2 * 592, dtype=torch.float64, device=dev)
+        sums = torch.empty(2, dtype=torch.float64, device=dev)
+        total = torch.zeros(2, dtype=torch.float64, device=dev)
+        for c0 in range(0, npos, chunk):
+            c1 = min(npos, c0 + chunk)
+            m = c1 - c0
+            ac = torch.empty((m, n, n), dtype=torch.complex64, device=dev)
+            _lib.check(lib.ptycho_pattern_prepare(ops._p(flat[c0:c1]), m * n * n, ops._p(inten[c0:c1]),
+                                                  ops._p(amp[c0:c1]), ops._p(ac), ops._p(work), work.numel(),
+                                                  ops._p(sums), st), "pattern_prepare")
+            total += sums
+            ops.fft2(ac, out=ac)
+            sh = shifts[:, c0:c1].contiguous()
+            _lib.check(lib.ptycho_pattern_shift_ramp(ops._p(ac), ops._p(sh), m, n, st), "pattern_shift_ramp")
+            ops.fft2(ac, inverse=True, scale=1.0 / (n * n), out=ac)
+            _lib.check(lib.ptycho_pattern_center(ops._p(ac), m, n, 1.0, ops._p(camp[c0:c1]), ops._p(cint[c0:c1]), st),
+                       "pattern_center")
+        tot = total.cpu().numpy()
+        self._amplitudes = amp
+        self._centered_amplitudes = camp
+        self._intensities = inten
+        self._centered_intensities = cint
+        self.mean_diffraction_intensity = float(tot[0]) / npos
+        self.mean_diffraction_amplitude = float(tot[1]) / npos
+        dt = config.get("dtype_real")
         descan = -1 * self.com_fit.reshape((2, -1)) + self.roi_shape[:, None] / 2
         self._descan_shifts = torch.as_tensor(descan.T.astype(dt))
         self._initial_descan_shifts = self._descan_shifts.clone()

@@ -266,7 +266,7 @@ class Ptychography:
             self.dset.preprocess(com_fit_function=com_fit_function, force_com_rotation=force_com_rotation,
                                  force_com_transpose=force_com_transpose,
                                  padded_diffraction_intensities_shape=padded_diffraction_intensities_shape,
-                                 obj_padding_px=obj_padding_px)
+                                 obj_padding_px=obj_padding_px, device=self.device)
             self.probe_model.set_initial_probe(self.roi_shape, self.reciprocal_sampling,
                                                self.dset.mean_diffraction_intensity, device=self.device)
         self.obj_padding_px = obj_padding_px

@@ -18,7 +18,7 @@ def build_from_golden(z, device="cpu"):
                                   units=("A", "A", "A^-1", "A^-1"))
     pd = PtychographyDatasetRaster.from_dataset4dstem(d4, verbose=0)
     pd.preprocess(com_fit_function="constant", force_com_rotation=0, force_com_transpose=False,
-                  plot_rotation=False, plot_com=False, probe_energy=float(z["energy"]))
+                  plot_rotation=False, plot_com=False, probe_energy=float(z["energy"]), device=device)
     S, P, seed = int(z["S"]), int(z["P"]), int(z["seed"])
     w = z["weights"] if z["weights"].size else None
     obj = ObjectPixelated.from_uniform(num_slices=S, slice_thicknesses=float(z["dz"]), obj_type="complex")
