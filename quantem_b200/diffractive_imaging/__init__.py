@@ -5,7 +5,8 @@ from .detector_models import DetectorPixelated
 from .object_models import ObjectPixelated
 from .probe_models import ProbePixelated
 from .ptychography import Ptychography
+from .ptychography_lite import PtychoLite
 from .ptycho_utils import SimpleBatcher
 
 __all__ = ["Dataset4dstem", "PtychographyDatasetRaster", "DetectorPixelated", "ObjectPixelated", "ProbePixelated",
-           "Ptychography", "SimpleBatcher"]
+           "Ptychography", "PtychoLite", "SimpleBatcher"]
