@@ -228,3 +228,226 @@ class ObjectPixelated(OptimizerMixin):
 
     def backward(self, *args, **kwargs):
         raise NotImplementedError("analytic object gradients: use autograd=True")
+
+
+class ObjectDIP(ObjectPixelated):
+    """Deep-image-prior object (object_models.py:728-1226): the object is the output
+    of a CNN, obj = exp(i * model(model_input (+ noise))[0]) for pure-phase objects,
+    and the network weights are what the optimiser updates.
+
+    The network is ``quantem_b200.core.ml.cnn.CNN2d`` (real-valued, BF16 tcgen05
+    kernels); its output (1, S, H, W) is the phase of every slice.  The complex hard
+    constraint of the fused batch loss applied to exp(i phase) is exactly the
+    reference's pure-phase constraint (unit amplitude, mean phase removed,
+    object_models.py:289-300).  Gradients flow from the fused adjoint through
+    exp and the CNN backward kernels by torch autograd; the pixelated-object
+    gradient rescale (ptychography.py:330-332) is not applied, as in the
+    reference.  Complex-valued networks are not part of the B200 path."""
+
+    def __init__(self, num_slices=1, slice_thicknesses=None, input_noise_std=0.025, device="cuda",
+                 obj_type="pure_phase", rng=None, _token=None):
+        if str(obj_type).lower() != "pure_phase":
+            raise NotImplementedError("ObjectDIP on the B200 path is pure-phase (real CNN2d output = phase)")
+        ObjectPixelated.__init__(self, num_slices, slice_thicknesses, "complex", "dip", device, rng,
+                                 _token=ObjectPixelated._token)
+        self._obj_type_dip = "pure_phase"
+        self._model = None
+        self._model_input = torch.tensor([])
+        self._pretrain_target = torch.tensor([])
+        self._pretrain_losses = []
+        self._pretrain_lrs = []
+        self._pretrained_weights = None
+        if input_noise_std < 0:
+            raise ValueError("input_noise_std must be >= 0")
+        self._input_noise_std = float(input_noise_std)
+        self._gen = None
+
+    @classmethod
+    def from_model(cls, model, model_input, num_slices: int = 1, slice_thicknesses=None,
+                   input_noise_std: float = 0.025, device="cuda", obj_type="pure_phase", rng=None):
+        """object_models.py:768-794."""
+        m = cls(num_slices, slice_thicknesses, input_noise_std, device, obj_type, rng)
+        m._model = model
+        m.model_input = model_input
+        m._set_pretrained_weights()
+        return m
+
+    @classmethod
+    def from_pixelated(cls, model, pixelated: ObjectPixelated, input_noise_std: float = 0.025, device=None):
+        """object_models.py:796-834: input and pre-training target = the pixelated object's phase."""
+        if not isinstance(pixelated, ObjectPixelated):
+            raise ValueError(f"pixelated must be an ObjectPixelated, got {type(pixelated)}")
+        phase = torch.angle(pixelated.obj.detach()).float()
+        m = cls.from_model(model, phase, num_slices=pixelated.num_slices,
+                           slice_thicknesses=pixelated.slice_thicknesses.cpu().numpy() if
+                           pixelated.slice_thicknesses.numel() else None,
+                           input_noise_std=input_noise_std, device=device or pixelated.device,
+                           rng=pixelated._rng_seed)
+        m.pretrain_target = phase
+        return m
+
+    # ------------------------------------------------------------------ state
+    @property
+    def name(self) -> str:
+        return "ObjectDIP"
+
+    @property
+    def obj_type(self) -> str:
+        return "pure_phase"
+
+    @property
+    def model(self):
+        return self._model
+
+    @property
+    def pretrained_weights(self):
+        return self._pretrained_weights
+
+    def _set_pretrained_weights(self):
+        self._pretrained_weights = {k: v.clone() for k, v in self._model.state_dict().items()}
+
+    @property
+    def model_input(self) -> torch.Tensor:
+        return self._model_input
+
+    @model_input.setter
+    def model_input(self, x):
+        x = torch.as_tensor(x).detach().clone().float()
+        if x.shape[-3] != self.num_slices:
+            raise ValueError(f"model_input.shape[-3] {x.shape[-3]} does not match num_slices {self.num_slices}")
+        if x.ndim == 3:
+            x = x[None]
+        elif x.ndim != 4:
+            raise ValueError(f"model_input must be (num_slices, h, w), got shape {tuple(x.shape)}")
+        self._model_input = x.to(self._model.device).contiguous()
+
+    @property
+    def num_slices(self) -> int:
+        return int(self._num_slices_dip) if hasattr(self, "_num_slices_dip") else int(self._obj.shape[0])
+
+    @property
+    def pretrain_target(self) -> torch.Tensor:
+        return self._pretrain_target
+
+    @pretrain_target.setter
+    def pretrain_target(self, t):
+        if t is None:
+            self._pretrain_target = torch.tensor([])
+            return
+        t = torch.as_tensor(t).float()
+        if t.ndim == 4:
+            t = t[0]
+        if tuple(t.shape) != tuple(self.model_input.shape[-3:]):
+            raise ValueError(f"pretrain target {tuple(t.shape)} != model input {tuple(self.model_input.shape[-3:])}")
+        self._pretrain_target = t.to(self._model.device).contiguous()
+
+    @property
+    def pretrain_losses(self) -> np.ndarray:
+        return np.array(self._pretrain_losses)
+
+    @property
+    def pretrain_lrs(self) -> np.ndarray:
+        return np.array(self._pretrain_lrs)
+
+    @property
+    def shape(self):
+        return tuple(int(v) for v in self._model_input.shape[1:])
+
+    @property
+    def params(self):
+        return self._model.flat
+
+    def get_optimization_parameters(self):
+        return [self._model.flat]
+
+    def _noisy_input(self, noise: bool):
+        if not noise or self._input_noise_std <= 0.0:
+            return self._model_input
+        if self._gen is None:
+            self._gen = torch.Generator(device=self._model_input.device).manual_seed(
+                int(self._rng_seed) if self._rng_seed is not None else 0)
+        return self._model_input + torch.randn(self._model_input.shape, generator=self._gen,
+                                               device=self._model_input.device) * self._input_noise_std
+
+    def raw_object(self, noise: bool = True) -> torch.Tensor:
+        """exp(i * model(input (+ noise))[0]) as complex64 (S, H, W), differentiable."""
+        phase = self._model(self._noisy_input(noise))[0]
+        return torch.polar(torch.ones_like(phase), phase)
+
+    @property
+    def _obj(self) -> torch.Tensor:
+        return self.raw_object(noise=True)
+
+    @_obj.setter
+    def _obj(self, v):  # the base constructor stores a placeholder; the network defines the object
+        self._num_slices_dip = int(v.shape[0])
+
+    @property
+    def obj(self) -> torch.Tensor:
+        from .. import ops
+
+        return ops.constrained_object(self.raw_object(noise=False))
+
+    def _initialize_obj(self, shape, sampling=None):
+        if sampling is not None:
+            self._sampling = (float(sampling[0]), float(sampling[1]))
+        if tuple(int(s) for s in shape) != tuple(self._model_input.shape[1:]):
+            raise ValueError(f"shape {tuple(shape)} does not match model_input {tuple(self._model_input.shape)}")
+
+    def reset(self):
+        """Back to the pre-trained weights (object_models.py:1032-1034)."""
+        self._model.load_state_dict(self._pretrained_weights)
+        if self._optimizer is not None:
+            self.set_optimizer(self._optimizer_params)
+
+    def to(self, device):
+        dev, _ = config.validate_device(device)
+        if torch.device(dev) != self._model.device:
+            raise NotImplementedError("the CNN2d lives on the device it was built on")
+        self._device = dev
+        return self
+
+    def forward(self, patch_indices: torch.Tensor) -> torch.Tensor:
+        o = self._obj.reshape(self.num_slices, -1)
+        return torch.complex(o.real[:, patch_indices], o.imag[:, patch_indices])
+
+    # ------------------------------------------------------------------ pre-training
+    def pretrain(self, model_input=None, pretrain_target=None, reset: bool = False, num_iters: int = 100,
+                 optimizer_params: dict | None = None, scheduler_params: dict | None = None, loss_fn="l2",
+                 apply_constraints: bool = False, show: bool = False, device=None):
+        """Fit the network output to the target phase (object_models.py:1047-1154)."""
+        from ..core.ml.cnn import mse_loss
+
+        if str(loss_fn).lower() not in ("l2", "mse"):
+            raise NotImplementedError("pre-training loss: l2")
+        if apply_constraints:
+            raise NotImplementedError("pre-training with the hard constraint applied is not part of the B200 path")
+        if optimizer_params is not None:
+            self.set_optimizer(optimizer_params)
+        if self._optimizer is None:
+            self.set_optimizer({"type": "adam", "lr": 1e-3})
+        if scheduler_params is not None:
+            self.set_scheduler(scheduler_params, num_iters)
+        if reset:
+            self._model._init_params(0)
+            self._pretrain_losses, self._pretrain_lrs = [], []
+        if model_input is not None:
+            self.model_input = model_input
+        if pretrain_target is not None:
+            self.pretrain_target = pretrain_target
+        if self._pretrain_target.numel() == 0:
+            raise ValueError("No pretrain target set. Provide pretrain_target or set it beforehand.")
+        self._model.train()
+        opt = self._optimizer
+        for _ in range(num_iters):
+            out = self._model(self._noisy_input(True))[0]
+            loss = mse_loss(out, self._pretrain_target)
+            opt.zero_grad(set_to_none=True)
+            loss.backward()
+            opt.step()
+            if self._scheduler is not None:
+                self.step_scheduler(float(loss.item()))
+            self._pretrain_losses.append(float(loss.item()))
+            self._pretrain_lrs.append(opt.param_groups[0]["lr"])
+        self._set_pretrained_weights()
+        return self

@@ -487,15 +487,18 @@ class Ptychography:
                 idx = torch.as_tensor(np.asarray(bi, dtype=np.int64)).to(dev, non_blocking=True)
                 if autograd:
                     probe_o = self.probe_model.probe
-                    loss = ops.batch_loss(self.obj_model._obj, probe_o, prop, pos, idx, tg, mask,
+                    obj_raw = self.obj_model._obj  # a leaf (pixelated) or a network output (DIP)
+                    loss = ops.batch_loss(obj_raw, probe_o, prop, pos, idx, tg, mask,
                                           self.dset.num_gpts, self.dset.mean_diffraction_intensity, loss_type)
-                    if self.obj_model._obj.requires_grad or self.probe_model._probe.requires_grad:
+                    if obj_raw.requires_grad or self.probe_model._probe.requires_grad:
                         loss.backward()
-                        if self.obj_model._obj.grad is not None:
-                            # ptychography.py:330-332
-                            self.obj_model._obj.grad.mul_(self.dset.upsample_factor ** 2 / 2)
+                        if obj_raw.is_leaf and obj_raw.grad is not None:
+                            # pixelated objects only (ptychography.py:330-332)
+                            obj_raw.grad.mul_(self.dset.upsample_factor ** 2 / 2)
                 else:
                     # analytic update directions (ptychography.py:339-348), no autograd graph
+                    if type(self.obj_model).__name__ == "ObjectDIP":
+                        raise NotImplementedError("the analytic update applies to pixelated objects (autograd=True)")
                     with torch.no_grad():
                         probe_o = self.probe_model.probe.detach().contiguous()
                         obj_c, _ = ops.obj_constrain(self.obj_model._obj.detach().contiguous())
