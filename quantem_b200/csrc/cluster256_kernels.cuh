@@ -125,8 +125,9 @@ __global__ void __launch_bounds__(512, 1) cluster256_kernel(const BatchParams p)
     };
     auto load_far_seed = [&](int mm) {
       const float2* fw = far_slot(mm);
+      load_pairs<E, T>(fw, tid, x);
 #pragma unroll
-      for (int i = 0; i < E; ++i) x[i] = cscale(fw[i * T + tid], 2.0f * inten[i * T + tid]);
+      for (int i = 0; i < E; ++i) x[i] = cscale(x[i], 2.0f * inten[i * T + tid]);
     };
     auto apply_prop = [&](int s, bool conj) {
       if (p.prop_r) {
@@ -165,19 +166,16 @@ __global__ void __launch_bounds__(512, 1) cluster256_kernel(const BatchParams p)
       if (ADJ && ck > 0) {
         if (!bwd && s % ck == 0) {  // Fourier checkpoint of the wave entering slice s
           float2* cp = ckpt_slot(m, s / ck);
-#pragma unroll
-          for (int i = 0; i < E; ++i) cp[i * T + tid] = x[i];
+          store_pairs<E, T>(cp, tid, x);
         } else if (bwd && !rec && (s < seg_lo || s > seg_hi)) {
           // recompute the incident waves of the segment that ends at slice s
-#pragma unroll
-          for (int i = 0; i < E; ++i) gsave[i * T + tid] = x[i];
+          store_pairs<E, T>(gsave, tid, x);
           seg_lo = (s / ck) * ck;
           seg_hi = s;
           srec = seg_lo;
           rec = true;
           const float2* cp = ckpt_slot(m, s / ck);
-#pragma unroll
-          for (int i = 0; i < E; ++i) x[i] = cp[i * T + tid];
+          load_pairs<E, T>(cp, tid, x);
         }
       }
       f.inverse(x, sm, tw, cl);
@@ -188,12 +186,10 @@ __global__ void __launch_bounds__(512, 1) cluster256_kernel(const BatchParams p)
         if (ADJ) {
           float2* wv = rec ? seg_slot(srec - seg_lo) : (ck == 0 ? wave_slot(m, s) : nullptr);
           if (wv) {
-#pragma unroll
-            for (int e = 0; e < E; ++e) wv[e * T + tid] = x[e];
+            store_pairs<E, T>(wv, tid, x);
           }
           if (rec && srec == seg_hi) {  // segment complete: resume the reverse sweep at slice seg_hi
-#pragma unroll
-            for (int i = 0; i < E; ++i) x[i] = gsave[i * T + tid];
+            load_pairs<E, T>(gsave, tid, x);
             rec = false;
             continue;
           }
@@ -209,9 +205,14 @@ __global__ void __launch_bounds__(512, 1) cluster256_kernel(const BatchParams p)
           float2 ps[4], ob[4];
           int col[4];
 #pragma unroll
+          for (int j = 0; j < 4; j += 2) {
+            const float4 v = reinterpret_cast<const float4*>(wv)[((e0 + j) >> 1) * T + tid];
+            ps[j] = make_float2(v.x, v.y);
+            ps[j + 1] = make_float2(v.z, v.w);
+          }
+#pragma unroll
           for (int j = 0; j < 4; ++j) {
             col[j] = colmap[f.a_col(e0 + j)];
-            ps[j] = wv[(e0 + j) * T + tid];
             ob[j] = __ldg(orow_ptr + col[j]);
           }
 #pragma unroll
@@ -239,8 +240,7 @@ __global__ void __launch_bounds__(512, 1) cluster256_kernel(const BatchParams p)
         for (int i = 0; i < E; ++i) x[i] = cscale(x[i], inv_n);  // orthonormal detector FFT
         if (ADJ) {
           float2* fw = far_slot(m);
-#pragma unroll
-          for (int i = 0; i < E; ++i) fw[i * T + tid] = x[i];
+          store_pairs<E, T>(fw, tid, x);
         }
 #pragma unroll
         for (int i = 0; i < E; ++i) inten[i * T + tid] = (m == 0 ? 0.f : inten[i * T + tid]) + cabs2(x[i]);

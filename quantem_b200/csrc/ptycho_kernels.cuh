@@ -69,6 +69,27 @@ __device__ __forceinline__ int wrap_index(int x, int n) {
   return x < 0 ? x + n : x;
 }
 
+// Saved per-thread register arrays (waves, far fields, checkpoints) are stored
+// thread-major with the register pair (e, e+1) packed into one 16-byte word:
+// element e of thread tid lives in word (e / 2) * T + tid, so a warp moves 512
+// contiguous bytes per access and a thread issues E / 2 vector accesses.
+template <int E, int T>
+__device__ __forceinline__ void store_pairs(float2* dst, int tid, const float2 (&x)[E]) {
+  float4* d = reinterpret_cast<float4*>(dst) + tid;
+#pragma unroll
+  for (int e = 0; e < E; e += 2) d[(e >> 1) * T] = make_float4(x[e].x, x[e].y, x[e + 1].x, x[e + 1].y);
+}
+template <int E, int T>
+__device__ __forceinline__ void load_pairs(const float2* src, int tid, float2 (&x)[E]) {
+  const float4* s = reinterpret_cast<const float4*>(src) + tid;
+#pragma unroll
+  for (int e = 0; e < E; e += 2) {
+    const float4 v = s[(e >> 1) * T];
+    x[e] = make_float2(v.x, v.y);
+    x[e + 1] = make_float2(v.z, v.w);
+  }
+}
+
 // shared-memory bytes used by fused_batch_kernel<N, *> (without the separable
 // propagator factors, which add 2 * N * (S-1) float2 when used)
 template <int N>
@@ -241,6 +262,11 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
   const size_t HoWo = (size_t)p.Ho * p.Wo;
   float2* slot = ADJ ? p.scratch + (size_t)cta * (size_t)(P * S + P + 1) * NN : nullptr;
   float* inten = ADJ ? reinterpret_cast<float*>(slot + (size_t)(P * S + P) * NN) : inten_sm;
+  // Per-thread saved data (waves, far fields, intensities) is thread-major with the
+  // register pair (e, e+1) packed into one word: one 16-byte (waves) or 8-byte
+  // (intensities) access per pair.  Element e of this thread lives in pair word
+  // (e / 2) * T + tid, half e % 2.
+  float2* inten2 = reinterpret_cast<float2*>(inten);
   float2* pgrad = ADJ ? p.probe_grad_part + (size_t)cta * (size_t)P * NN : nullptr;
   if (ADJ) {
     for (int m = 0; m < P; ++m)
@@ -309,14 +335,22 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
       const float2* fw = slot + (size_t)(P * S + mm) * NN;
       if (AN) {
 #pragma unroll
-        for (int e = 0; e < E; ++e) {
-          const float2 v = fw[e * T + tid];
-          const float fm1 = inten[e * T + tid] - 1.0f;
-          x[e] = make_float2(fmaf(v.x, fm1, tile2[e * T + tid]), v.y * fm1);
+        for (int e = 0; e < E; e += 2) {
+          const float4 v = reinterpret_cast<const float4*>(fw)[(e >> 1) * T + tid];
+          const float2 in = inten2[(e >> 1) * T + tid];
+          const float2 fx = reinterpret_cast<const float2*>(tile2)[(e >> 1) * T + tid];
+          const float fm0 = in.x - 1.0f, fm1 = in.y - 1.0f;
+          x[e] = make_float2(fmaf(v.x, fm0, fx.x), v.y * fm0);
+          x[e + 1] = make_float2(fmaf(v.z, fm1, fx.y), v.w * fm1);
         }
       } else {
 #pragma unroll
-        for (int e = 0; e < E; ++e) x[e] = cscale(fw[e * T + tid], 2.0f * inten[e * T + tid]);
+        for (int e = 0; e < E; e += 2) {
+          const float4 v = reinterpret_cast<const float4*>(fw)[(e >> 1) * T + tid];
+          const float2 in = inten2[(e >> 1) * T + tid];
+          x[e] = make_float2(v.x * 2.0f * in.x, v.y * 2.0f * in.x);
+          x[e + 1] = make_float2(v.z * 2.0f * in.y, v.w * 2.0f * in.y);
+        }
       }
     };
     int m = 0, s = 0;
@@ -331,8 +365,7 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
         for (int e = 0; e < E; ++e) x[e] = cscale(x[e], inv_n2);
         if (ADJ) {
           float2* wv = slot + (size_t)(m * S + s) * NN;
-#pragma unroll
-          for (int e = 0; e < E; ++e) wv[e * T + tid] = x[e];
+          store_pairs<E, T>(wv, tid, x);
         }
         if (p.out_waves) {
           float2* ow = p.out_waves + (((size_t)s * P + m) * p.B + b) * NN + (size_t)f.s1_r * N;
@@ -354,9 +387,14 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
           float2 ps[8], ob[8];
           int col[8];
 #pragma unroll
+          for (int j = 0; j < 8; j += 2) {
+            const float4 v = reinterpret_cast<const float4*>(wv)[((e0 + j) >> 1) * T + tid];
+            ps[j] = make_float2(v.x, v.y);
+            ps[j + 1] = make_float2(v.z, v.w);
+          }
+#pragma unroll
           for (int j = 0; j < 8; ++j) {
             col[j] = colmap[f.s1_col(e0 + j)];
-            ps[j] = wv[(e0 + j) * T + tid];
             ob[j] = __ldg(orow_ptr + col[j]);
           }
 #pragma unroll
@@ -405,15 +443,21 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
         for (int e = 0; e < E; ++e) x[e] = cscale(x[e], inv_n);  // orthonormal detector FFT
         if (ADJ) {
           float2* fw = slot + (size_t)(P * S + m) * NN;
-#pragma unroll
-          for (int e = 0; e < E; ++e) fw[e * T + tid] = x[e];
+          store_pairs<E, T>(fw, tid, x);
         }
 #pragma unroll
-        for (int e = 0; e < E; ++e) inten[e * T + tid] = (m == 0 ? 0.f : inten[e * T + tid]) + cabs2(x[e]);
+        for (int e = 0; e < E; e += 2) {
+          const float2 old = m == 0 ? make_float2(0.f, 0.f) : inten2[(e >> 1) * T + tid];
+          inten2[(e >> 1) * T + tid] = make_float2(old.x + cabs2(x[e]), old.y + cabs2(x[e + 1]));
+        }
         if (ADJ && AN) {  // sum_p |Psi_p + 1e-9|^2 (ptychography_base.py:958)
+          float2* t2 = reinterpret_cast<float2*>(tile2);
 #pragma unroll
-          for (int e = 0; e < E; ++e)
-            tile2[e * T + tid] = (m == 0 ? 0.f : tile2[e * T + tid]) + cabs2(make_float2(x[e].x + 1e-9f, x[e].y));
+          for (int e = 0; e < E; e += 2) {
+            const float2 old = m == 0 ? make_float2(0.f, 0.f) : t2[(e >> 1) * T + tid];
+            t2[(e >> 1) * T + tid] = make_float2(old.x + cabs2(make_float2(x[e].x + 1e-9f, x[e].y)),
+                                                 old.y + cabs2(make_float2(x[e + 1].x + 1e-9f, x[e + 1].y)));
+          }
         }
         if (m < P - 1) {
           ++m;
@@ -430,14 +474,14 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
             for (int e = 0; e < D; ++e) {
               const int kr = f.s3_row(g, e), kc = f.s3_c;
               const int di = ((kr + N / 2) % N) * N + ((kc + N / 2) % N);
-              const float I = inten[(g * D + e) * T + tid];
+              const int li = 2 * (((g * D + e) >> 1) * T + tid) + ((g * D + e) & 1);
+              const float I = inten[li];
               if (!isfinite(I)) ++nonfinite;
               float dldi;
               const float tv = __ldg(tg + di);
               loss_elem<N>(p, I, tv, __ldg(p.mask + di), loss_acc, dldi);
               if (ADJ && AN) {
                 // factor f and additive fix of the Fourier projection seed
-                const int li = (g * D + e) * T + tid;
                 if (P == 1) {
                   dldi = I > 0.f ? tv / sqrtf(I) : 0.f;   // t exp(i angle(Psi)) = Psi t / |Psi|
                   tile2[li] = I > 0.f ? 0.f : tv;        // angle(0) = 0
@@ -447,7 +491,7 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
                   tile2[li] = 0.f;
                 }
               }
-              inten[(g * D + e) * T + tid] = dldi;
+              inten[li] = dldi;
               if (p.out_intensity) p.out_intensity[(size_t)b * NN + di] = I;
             }
         }
