@@ -858,6 +858,120 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def reference_torch_gpu(cfg, device, steps, warmup, batch_size, ref_dir=None, verbose=False):
+    """Positions/s of the reference's own PyTorch iteration on `device`.
+
+    Runs quantem's ``Ptychography.reconstruct`` (ptychography.py:146-308) unmodified:
+    autograd, probe orthogonalisation, Adam on object (lr 5e-3) and probe (lr 1e-3),
+    on a dataset simulated for `cfg` and set up through the reference's own
+    ``Dataset4dstem`` / ``PtychographyDatasetRaster.preprocess`` /
+    ``ObjectPixelated.from_uniform`` / ``ProbePixelated.from_params`` /
+    ``Ptychography.from_models``.  The package is imported from ``ref_dir``
+    (default ``baseline/_ref``, filled by ``baseline/install_reference.sh``) with the
+    oracle's import shim, which stubs the plotting / IO packages it imports at module
+    level.  The batch starts at `batch_size` and is halved while the GPU runs out of
+    memory; the batch used is reported.  Timed: ``reconstruct(num_iters=steps)`` as one
+    call between CUDA events (one end-of-call ``gc.collect`` / ``empty_cache`` per
+    `steps` iterations)."""
+    import numpy as np
+    import torch
+
+    from oracle.quantem_shim import import_reference
+    from quantem_b200 import synthetic
+
+    ref_dir = ref_dir or os.path.join(ROOT, "baseline", "_ref")
+    if not os.path.isdir(os.path.join(ref_dir, "quantem")):
+        return {"unavailable": f"reference package not installed under {os.path.relpath(ref_dir, ROOT)} "
+                               "(baseline/install_reference.sh)"}
+    import_reference(ref_dir)
+    from quantem.core.datastructures.dataset4dstem import Dataset4dstem
+    from quantem.diffractive_imaging.dataset_models import PtychographyDatasetRaster
+    from quantem.diffractive_imaging.detector_models import DetectorPixelated
+    from quantem.diffractive_imaging.object_models import ObjectPixelated
+    from quantem.diffractive_imaging.probe_models import ProbePixelated
+    from quantem.diffractive_imaging.ptychography import Ptychography
+
+    dev = torch.device(device)
+    ds = synthetic.make_dataset(cfg, dev)
+    nr, nc = cfg.scan
+    data = ds["intensities"].cpu().numpy().reshape(nr, nc, cfg.n, cfg.n)
+    rs = 1.0 / (cfg.n * cfg.pixel)
+    t0 = time.perf_counter()
+    d4 = Dataset4dstem.from_array(data, sampling=(cfg.step_px * cfg.pixel, cfg.step_px * cfg.pixel, rs, rs),
+                                  units=("A", "A", "A^-1", "A^-1"))
+    pd = PtychographyDatasetRaster.from_dataset4dstem(d4, verbose=0)
+    pd.preprocess(com_fit_function="constant", force_com_rotation=0, force_com_transpose=False,
+                  plot_rotation=False, plot_com=False, probe_energy=cfg.energy)
+    obj_model = ObjectPixelated.from_uniform(num_slices=cfg.slices, slice_thicknesses=cfg.slice_thickness,
+                                             obj_type="complex")
+    probe_model = ProbePixelated.from_params(
+        probe_params={"energy": cfg.energy, "defocus": cfg.defocus, "semiangle_cutoff": cfg.semiangle},
+        num_probes=cfg.modes, rng=cfg.seed + 1, initial_probe_weights=list(cfg.mode_weights))
+    pt = Ptychography.from_models(dset=pd, obj_model=obj_model, probe_model=probe_model,
+                                  detector_model=DetectorPixelated(), device="cpu", verbose=0, rng=cfg.seed + 2)
+    pt.preprocess(obj_padding_px=(cfg.pad_px, cfg.pad_px))
+    pd.scan_positions_px = pd.scan_positions_px.detach() + torch.as_tensor(
+        np.random.default_rng(cfg.seed).uniform(-cfg.jitter_px, cfg.jitter_px, (pd.num_gpts, 2)).astype(np.float32))
+    setup_s = time.perf_counter() - t0
+    dev_arg = "gpu" if dev.type == "cuda" else "cpu"
+    opt = {"object": {"type": "adam", "lr": 5e-3}, "probe": {"type": "adam", "lr": 1e-3}}
+    sync = torch.cuda.synchronize if dev.type == "cuda" else (lambda: None)
+
+    bs = batch_size
+    while True:
+        try:
+            pt.reconstruct(num_iters=1, reset=True, optimizer_params=opt, batch_size=bs, device=dev_arg)
+            sync()
+            break
+        except torch.OutOfMemoryError:
+            if dev.type == "cuda":
+                torch.cuda.empty_cache()
+            bs //= 2
+            if bs < 1:
+                return {"unavailable": "out of memory at batch 1"}
+    if warmup > 1:
+        pt.reconstruct(num_iters=warmup - 1, batch_size=bs)
+    sync()
+    if dev.type == "cuda":
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        pt.reconstruct(num_iters=steps, batch_size=bs)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+    else:
+        t1 = time.perf_counter()
+        pt.reconstruct(num_iters=steps, batch_size=bs)
+        ms = (time.perf_counter() - t1) * 1e3 / steps
+    npos = pd.num_gpts
+    losses = [float(x) for x in pt.iter_losses]
+    if verbose:
+        print(f"reference setup {setup_s:.1f} s, batch {bs}, {ms:.1f} ms/iteration", file=sys.stderr)
+    return {"value": round(npos / (ms * 1e-3), 1), "unit": "positions/s", "batch_size": bs,
+            "ms_per_step": round(ms, 2), "positions": npos, "setup_s": round(setup_s, 1),
+            "final_loss": losses[-1] if losses else None,
+            "what": "quantem Ptychography.reconstruct (reference PyTorch path, autograd, Adam) on this device"}
+
+
+def run_reference_torch_gpu(args):
+    rank, world, _ = _dist_env()
+    if rank != 0:
+        return
+    from quantem_b200 import synthetic
+
+    res = reference_torch_gpu(synthetic.SyntheticConfig(seed=0), "cuda:0", args.steps, args.warmup,
+                              args.batch_size)
+    line = {"metric": METRIC, "unit": "positions/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64/f32",
+            "data": "synthetic", "impl": "reference", "device": "gpu",
+            "config": {"workload": WORKLOAD, "parallelism": "replicas1"}}
+    if "unavailable" in res:
+        line["unavailable"] = res["unavailable"]
+    else:
+        line.update(value=res["value"], ms_per_step=res["ms_per_step"], reference_torch_gpu=res)
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -873,6 +987,9 @@ def main():
     ap.add_argument("--c4-objects", type=int, default=20000, help="training objects for --workload c4")
     ap.add_argument("--recompute-every", type=int, default=0, help="adjoint checkpoint interval (--workload c5)")
     ap.add_argument("--c4-iters", type=int, default=120, help="refinement iterations per arm for --workload c4")
+    ap.add_argument("--torch-gpu", action="store_true",
+                    help="with --impl reference: time the reference's own PyTorch iteration on the GPU "
+                         "(package under baseline/_ref) instead of the CPU oracle port")
     ap.add_argument("--skip-torch-reference", action="store_true",
                     help="do not time the PyTorch-eager restatement of the reference path")
     ap.add_argument("--positions", type=int, default=296, help="positions per launch with --kernel-only")
@@ -892,7 +1009,7 @@ def main():
     elif args.kernel_only:
         run_kernel_only(args)
     elif args.impl == "reference":
-        run_reference(args)
+        run_reference_torch_gpu(args) if args.torch_gpu else run_reference(args)
     else:
         run_ours(args)
 
