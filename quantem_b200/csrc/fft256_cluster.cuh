@@ -83,9 +83,21 @@ struct Fft256C {
     }
   }
 
+  // Split cluster barrier: the first barrier of a cluster exchange only has to
+  // order every CTA's last reads of its own buffer before the peers' remote
+  // stores, so each thread arrives right after those reads and waits just before
+  // its own remote stores; the register work in between hides the barrier.
+  static __device__ __forceinline__ void cluster_arrive() {
+    asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+  }
+  static __device__ __forceinline__ void cluster_wait() {
+    asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
+  }
+
   // ---- 256-point transform along the line: x[e] = element tl + 8e in, natural
   //      frequency k = 4*tl + a + 32*kB in register a*8 + kB out ----
-  template <bool INV>
+  // ARRIVE: arrive on the cluster barrier after the last read of the buffer
+  template <bool INV, bool ARRIVE = false>
   __device__ __forceinline__ void line_fwd(float2 (&x)[E], float2* sm, const float2* tw) const {
     dft_reg<32, INV>(x);
     {
@@ -107,11 +119,12 @@ struct Fft256C {
 #pragma unroll
         for (int t = 0; t < 8; ++t) x[a * 8 + t] = r[8 * a + t];
     }
+    if (ARRIVE) cluster_arrive();
     dft8_groups<INV, 0>(x);
   }
   // inverse direction of line_fwd's data flow: frequency distribution in,
   // element tl + 8e out (INV selects the conjugate transform)
-  template <bool INV>
+  template <bool INV, bool ARRIVE = false>
   __device__ __forceinline__ void line_bwd(float2 (&x)[E], float2* sm, const float2* tw) const {
     dft8_groups<INV, 0>(x);
     __syncthreads();
@@ -128,6 +141,7 @@ struct Fft256C {
 #pragma unroll
       for (int k1 = 0; k1 < 32; ++k1) x[k1] = r[33 * (k1 >> 2) + 8 * (k1 & 3)];
     }
+    if (ARRIVE) cluster_arrive();
     {
       const float2* twr = tw + 33 * tl;
 #pragma unroll
@@ -150,8 +164,9 @@ struct Fft256C {
   }
   // A (row spectrum, register a*8+kB holds kc = 4tl + a + 32kB of row a_row())
   //   -> B (column slab, register e holds r = tl + 8e of spectral column b_kc())
+  // (the caller arrived on the cluster barrier after its last read of sm)
   __device__ __forceinline__ void a_to_b(float2 (&x)[E], float2* sm, cg::cluster_group& cl) const {
-    cl.sync();  // every CTA of the cluster is done reading its buffer
+    cluster_wait();  // every CTA of the cluster is done reading its buffer
     // bx(4tl + a + 32x, 64q + line) = [1042 tl + 64q + line] + 260a + 8336x
     const float2* mine = sm + 1042 * tl + 64 * q + line;
 #pragma unroll
@@ -170,7 +185,7 @@ struct Fft256C {
   // B (column slab, register e holds r = tl + 8e of spectral column b_kc())
   //   -> A (row spectrum distribution of row a_row())
   __device__ __forceinline__ void b_to_a(float2 (&x)[E], float2* sm, cg::cluster_group& cl) const {
-    cl.sync();
+    cluster_wait();  // arrived after the caller's last read of sm
     // ax(tl + 8j, 64q + line) = [274 tl + 68q + line + line/16] + 2192 j
     const float2* mine = sm + AP * tl + 68 * q + line + (line >> 4);
 #pragma unroll
@@ -191,13 +206,13 @@ struct Fft256C {
   // ---- whole 2-D transforms (unnormalised) ----
   // layout A real space -> layout B spectrum
   __device__ __forceinline__ void forward(float2 (&x)[E], float2* sm, const float2* tw, cg::cluster_group& cl) const {
-    line_fwd<false>(x, sm, tw);
+    line_fwd<false, true>(x, sm, tw);
     a_to_b(x, sm, cl);
     line_fwd<false>(x, sm, tw);
   }
   // layout B spectrum -> layout A real space
   __device__ __forceinline__ void inverse(float2 (&x)[E], float2* sm, const float2* tw, cg::cluster_group& cl) const {
-    line_bwd<true>(x, sm, tw);
+    line_bwd<true, true>(x, sm, tw);
     b_to_a(x, sm, cl);
     line_bwd<true>(x, sm, tw);
   }

@@ -5,8 +5,8 @@ from .detector_models import DetectorPixelated
 from .object_models import ObjectDIP, ObjectPixelated
 from .probe_models import ProbePixelated
 from .ptychography import Ptychography
-from .ptychography_lite import PtychoLite
+from .ptychography_lite import PtychoLite, PtychoLiteDIP
 from .ptycho_utils import SimpleBatcher
 
 __all__ = ["Dataset4dstem", "PtychographyDatasetRaster", "DetectorPixelated", "ObjectPixelated", "ObjectDIP", "ProbePixelated",
-           "Ptychography", "PtychoLite", "SimpleBatcher"]
+           "Ptychography", "PtychoLite", "PtychoLiteDIP", "SimpleBatcher"]

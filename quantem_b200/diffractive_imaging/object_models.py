@@ -402,7 +402,12 @@ class ObjectDIP(ObjectPixelated):
 
     def to(self, device):
         dev, _ = config.validate_device(device)
-        if torch.device(dev) != self._model.device:
+
+        def norm(d):
+            d = torch.device(d)
+            return torch.device("cuda", torch.cuda.current_device()) if d.type == "cuda" and d.index is None else d
+
+        if norm(dev) != norm(self._model.device):
             raise NotImplementedError("the CNN2d lives on the device it was built on")
         self._device = dev
         return self
