@@ -1,15 +1,16 @@
-"""Import shim for the reference package (quantem 0.1.8) — TEST INFRASTRUCTURE ONLY.
+"""Import shim for the reference package (quantem 0.1.8).
 
 The reference's ptychography modules import plotting / IO / hyper-parameter
 packages at module import time (matplotlib, zarr, h5py, optuna, skimage, ...)
 that are absent from this image, although the ptychography iteration never
 calls them.  ``import_reference(path)`` installs permissive stand-in modules
 for exactly those names, patches ``importlib.metadata.version("quantem")`` and
-puts the reference's ``src`` directory first on ``sys.path``.
+puts ``path`` (a directory holding the ``quantem`` package: the reference's
+``src`` or the ``baseline/_ref`` install) first on ``sys.path``.
 
-Only the golden-fixture generator under ``tests/golden/`` uses this, and only in
-a container where the reference source tree is mounted.  Nothing in the
-product package imports it.
+Users: the golden-fixture generators under ``tests/golden/`` and the timing of
+the reference's own PyTorch iteration in ``bench.py``.  Nothing in the product
+package imports it.
 """
 from __future__ import annotations
 

@@ -12,7 +12,9 @@ synthetic inputs simulated with this package's forward kernels.
 ``--impl ours`` times the CUDA path (device-resident ``value``; ``e2e`` through
 the public reconstruct call with the measured data copied from pinned host
 memory every step).  ``--impl reference`` times the CPU oracle port of the
-reference algorithm on the host cores on a bounded sample of the same workload.
+reference algorithm on the host cores on a bounded sample of the same workload;
+``--impl reference --torch-gpu`` times the reference's own PyTorch iteration on
+the GPU (also reported in the default line as ``reference_torch_gpu``).
 With ``--gpus N`` (torchrun), every rank reconstructs its own dataset: N
 independent replicas, no collective.
 """
@@ -309,6 +311,15 @@ def run_ours(args):
                      "frac": round(ach / fp32, 4), "peak_source": "measured (own FMA probe)"}
     cpu = cpu_baseline_sample(args)
     torch_ref = torch_eager_reference(pt, args.batch_size) if not args.skip_torch_reference else None
+    ref_gpu = None
+    if not args.skip_torch_reference:
+        try:
+            from quantem_b200 import synthetic
+
+            ref_gpu = reference_torch_gpu(synthetic.SyntheticConfig(seed=0), device, 3, 3, args.batch_size)
+        except Exception as exc:  # the reference is a baseline here: report, never fail the bench
+            ref_gpu = {"unavailable": f"{type(exc).__name__}: {exc}"[:300]}
+        torch.cuda.empty_cache()
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": "positions/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
@@ -324,6 +335,7 @@ def run_ours(args):
         "roofline": roofline, "roofline_fp32": fp32_roof,
         "cpu_baseline": cpu,
         "torch_eager_reference_gpu": torch_ref,
+        "reference_torch_gpu": ref_gpu,
         "clocks": clk.summary(),
         "final_loss": float(losses[-1].item()),
     }
@@ -905,15 +917,15 @@ def reference_torch_gpu(cfg, device, steps, warmup, batch_size, ref_dir=None, ve
     ``ObjectPixelated.from_uniform`` / ``ProbePixelated.from_params`` /
     ``Ptychography.from_models``.  The package is imported from ``ref_dir``
     (default ``baseline/_ref``, filled by ``baseline/install_reference.sh``) with the
-    oracle's import shim, which stubs the plotting / IO packages it imports at module
-    level.  The batch starts at `batch_size` and is halved while the GPU runs out of
+    import shim in ``baseline/reference_import.py``, which stubs the plotting / IO
+    packages it imports at module level.  The batch starts at `batch_size` and is halved while the GPU runs out of
     memory; the batch used is reported.  Timed: ``reconstruct(num_iters=steps)`` as one
     call between CUDA events (one end-of-call ``gc.collect`` / ``empty_cache`` per
     `steps` iterations)."""
     import numpy as np
     import torch
 
-    from oracle.quantem_shim import import_reference
+    from baseline.reference_import import import_reference
     from quantem_b200 import synthetic
 
     ref_dir = ref_dir or os.path.join(ROOT, "baseline", "_ref")
@@ -1028,7 +1040,8 @@ def main():
                     help="with --impl reference: time the reference's own PyTorch iteration on the GPU "
                          "(package under baseline/_ref) instead of the CPU oracle port")
     ap.add_argument("--skip-torch-reference", action="store_true",
-                    help="do not time the PyTorch-eager restatement of the reference path")
+                    help="do not time the PyTorch-eager restatement of the reference path nor the "
+                         "reference's own PyTorch iteration on the GPU")
     ap.add_argument("--positions", type=int, default=296, help="positions per launch with --kernel-only")
     ap.add_argument("--variant", default="auto", choices=["auto", "serial", "cluster"],
                     help="mapping of probe modes onto CTAs (--kernel-only)")

@@ -29,7 +29,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 from oracle import ptycho_oracle as O  # noqa: E402
-from oracle.quantem_shim import import_reference  # noqa: E402
+from baseline.reference_import import import_reference  # noqa: E402
 
 
 def _c64(x):

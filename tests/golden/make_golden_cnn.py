@@ -24,7 +24,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
-from oracle.quantem_shim import import_reference  # noqa: E402
+from baseline.reference_import import import_reference  # noqa: E402
 
 CASES = {
     # name: (in_ch, out_ch, start_filters, num_layers, num_per_layer, skip, batchnorm, B, H, W)
