@@ -198,3 +198,35 @@ def test_analytic_update_matches_reference(cuda_device, case):
     assert abs(loss.item() - float(z["batch_loss"])) / float(z["batch_loss"]) < TOL_I
     assert rel(g_obj.cpu().numpy(), z["grad_obj_an"]) < TOL_G
     assert rel(g_probe.cpu().numpy(), z["grad_probe_an"]) < TOL_G
+
+
+@pytest.mark.parametrize("n", [64, 96])
+@pytest.mark.parametrize("loss_type", O.LOSS_TYPES)
+def test_loss_types_match_fp64_oracle(cuda_device, n, loss_type):
+    """Every consistency loss of the reference (ptychography_base.py:908-932) through the
+    fused forward + adjoint kernel, with a partial detector mask: loss, object and probe
+    gradients against the FP64 oracle, whose losses are pinned to the reference's own
+    error_estimate (tests/golden/loss_types.npz)."""
+    from quantem_b200 import ops
+
+    rng = np.random.default_rng(23)
+    S, P, Ho, B, npos, mean_i = 2, 2, 160, 6, 300, 20.0
+    obj = np.exp(1j * 0.3 * rng.standard_normal((S, Ho, Ho))) * (1 - 0.2 * rng.random((S, Ho, Ho)))
+    probe = rng.standard_normal((P, n, n)) + 1j * rng.standard_normal((P, n, n))
+    probe *= np.exp(-((np.fft.fftfreq(n) * n)[:, None] ** 2 + (np.fft.fftfreq(n) * n)[None] ** 2) / 150.0)
+    props = O.propagators((n, n), (0.2, 0.2), 300e3, [20.0] * (S - 1))
+    positions = rng.uniform(0, Ho, size=(B, 2)).astype(np.float32).astype(np.float64)
+    targets = np.abs(rng.standard_normal((B, n, n))) * (2.0 if "amplitude" in loss_type else 6.0)
+    mask = (rng.random((n, n)) > 0.15).astype(np.float64)
+    obj_c = O.constrain_object(obj)
+    loss_o, g_obj_o, g_probe_o, _ = O.batch_loss_and_grads(obj_c, probe, positions, props, targets, mask, npos,
+                                                           mean_i, loss_type)
+    dev = cuda_device
+    args = (_t(obj_c.astype(np.complex64), dev), _t(probe.astype(np.complex64), dev),
+            _t(props.astype(np.complex64), dev), _t(positions, dev, torch.float32),
+            torch.arange(B, device=dev, dtype=torch.int64), _t(targets, dev, torch.float32),
+            _t(mask, dev, torch.float32), npos, mean_i)
+    loss, g_obj, g_probe = ops.batch_forward_adjoint(*args, loss_type=loss_type)
+    assert abs(loss.item() - loss_o) / abs(loss_o) < TOL_I
+    assert rel(g_obj.cpu().numpy(), g_obj_o) < TOL_G
+    assert rel(g_probe.cpu().numpy(), g_probe_o) < TOL_G

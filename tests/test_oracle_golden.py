@@ -88,3 +88,15 @@ def test_oracle_analytic_update_matches_reference(case):
                                              orthogonalize=bool(z["orthogonalize"]))
     assert rel(g_obj, z["grad_obj_an"]) < 5e-6
     assert rel(g_probe, z["grad_probe_an"]) < 5e-6
+
+
+@pytest.mark.parametrize("loss_type", O.LOSS_TYPES)
+def test_oracle_loss_types_match_reference(loss_type):
+    """All five consistency losses and their dL/dI against the reference's own
+    error_estimate (ptychography_base.py:908-932), fixture tests/golden/loss_types.npz."""
+    z = load_golden("loss_types")
+    inten, mask = z["intensity"], z["mask"]
+    loss, dldi_cc = O.loss_and_seed(np.fft.ifftshift(inten, axes=(-2, -1)), z[f"{loss_type}_targets"], mask,
+                                    int(z["num_gpts"]), float(z["mean_intensity"]), loss_type)
+    assert abs(loss - float(z[f"{loss_type}_loss"])) <= 1e-12 * abs(float(z[f"{loss_type}_loss"]))
+    assert rel(np.fft.fftshift(dldi_cc, axes=(-2, -1)), z[f"{loss_type}_dldi"]) < 1e-12
