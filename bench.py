@@ -310,6 +310,10 @@ def run_ours(args):
         fp32_roof = {"bound": "fp32", "achieved": round(ach, 2), "peak": round(fp32, 2), "unit": "TFLOP/s",
                      "frac": round(ach / fp32, 4), "peak_source": "measured (own FMA probe)"}
     cpu = cpu_baseline_sample(args)
+    try:  # the oracle as the checker: FP32 CUDA path against an FP64 run on a bounded sample
+        accuracy = accuracy_vs_fp64(pt)
+    except Exception as exc:
+        accuracy = {"unavailable": f"{type(exc).__name__}: {exc}"[:300]}
     torch_ref = torch_eager_reference(pt, args.batch_size) if not args.skip_torch_reference else None
     ref_gpu = None
     if not args.skip_torch_reference:
@@ -334,6 +338,7 @@ def run_ours(args):
         "gpu_launches": launches_per_batch * nbatches,
         "roofline": roofline, "roofline_fp32": fp32_roof,
         "cpu_baseline": cpu,
+        "accuracy_vs_fp64": accuracy,
         "torch_eager_reference_gpu": torch_ref,
         "reference_torch_gpu": ref_gpu,
         "clocks": clk.summary(),
@@ -479,6 +484,83 @@ def cpu_baseline_sample(args, positions=8):
     return {"value": round(rate, 2), "unit": "positions/s", "cores": ncores, "kind": "port",
             "sample": f"{reps} x {positions}-position batches of the same geometry, forward+loss+adjoint "
                       f"(optimizer step excluded), complex64, scipy.fft workers={ncores}"}
+
+
+def accuracy_vs_fp64(pt, nsub=16, iters=3):
+    """Accuracy of the FP32 CUDA path against an FP64 run of the oracle (the checker)
+    on a bounded sample of the workload: `nsub` positions spread over the scan.
+
+    * forward intensities at the bench's current object and probe: relative L2;
+    * `iters` full iterations (forward, loss, adjoint, object-gradient rescale, Adam
+      on object lr 5e-3 and probe lr 1e-3, probe orthogonalisation) on those positions
+      from the flat object: relative L2 of the first object gradient and phase NRMSE
+      of the constrained object (mean phase removed) against the FP64 run.  Adam
+      moves every pixel by about lr on its first steps whatever the size of its
+      gradient, so pixels the sample barely reaches carry most of the phase error."""
+    import torch
+
+    from oracle import ptycho_oracle as O
+    from quantem_b200 import engine, ops
+    from quantem_b200.diffractive_imaging.ptycho_utils import orthogonalize_probes
+
+    dev = pt.obj.device
+    idx = (torch.arange(nsub, device=dev) * (pt.num_gpts // nsub)).to(torch.int64)
+    kr, kc = pt.prop
+    props64 = (kr.cpu().numpy().astype(np.complex128)[:, :, None] * kc.cpu().numpy().astype(np.complex128)[:, None, :])
+    pos = pt.positions[idx].double().cpu().numpy()
+    tg = pt.targets[idx].double().cpu().numpy()
+    mask = pt.mask.double().cpu().numpy()
+    mean_i, up = float(pt.mean_intensity), float(pt.upsample_factor)
+    # forward intensities at the current state
+    with torch.no_grad():
+        obj_c, _ = ops.obj_constrain(pt.obj.detach())
+        probe_o = orthogonalize_probes(pt.probe.detach())
+        out = ops.batch_forward(obj_c, probe_o, pt.prop, pt.positions, idx, pt.targets, pt.mask, pt.num_gpts,
+                                pt.mean_intensity)
+    st = O.forward(obj_c.cpu().numpy().astype(np.complex128), probe_o.cpu().numpy().astype(np.complex128), pos,
+                   props64)
+    i64 = O.detector_intensities(st)
+    i32 = out["intensity"].double().cpu().numpy()
+    inten_rel = float(np.linalg.norm(i32 - i64) / np.linalg.norm(i64))
+    # a few iterations from the flat object, FP32 CUDA vs FP64 oracle
+    S, Ho, Wo = pt.obj.shape
+    probe0 = pt.probe.detach().clone()
+    sub = engine.ProblemTensors(
+        obj=torch.ones((S, Ho, Wo), dtype=torch.complex64, device=dev).requires_grad_(True),
+        probe=probe0.clone().requires_grad_(True), prop=pt.prop, positions=pt.positions[idx].contiguous(),
+        targets=pt.targets[idx].contiguous(), mask=pt.mask, mean_intensity=pt.mean_intensity, upsample_factor=up)
+    opts = [engine.make_optimizer([sub.obj], {"type": "adam", "lr": 5e-3}),
+            engine.make_optimizer([sub.probe], {"type": "adam", "lr": 1e-3})]
+    all_idx = torch.arange(nsub, device=dev, dtype=torch.int64)
+    o64 = np.ones((S, Ho, Wo), np.complex128)
+    p64 = probe0.cpu().numpy().astype(np.complex128)
+    adam = {}
+
+    def adam_step(key, x, g, lr, t):  # torch.optim.Adam on the real and imaginary parts
+        m, v = adam.get(key, (np.zeros_like(x), np.zeros_like(x)))
+        m = 0.9 * m + 0.1 * g
+        v = 0.999 * v + 0.001 * (g.real ** 2 + 1j * g.imag ** 2)
+        adam[key] = (m, v)
+        den = lambda a: np.sqrt(a) / np.sqrt(1 - 0.999 ** t) + 1e-8  # noqa: E731
+        return x - lr / (1 - 0.9 ** t) * (m.real / den(v.real) + 1j * m.imag / den(v.imag))
+
+    grad_rel = None
+    for t in range(1, iters + 1):
+        engine.batch_step(sub, all_idx, opts)
+        if t == 1:
+            g32 = sub.obj.grad.detach().cpu().numpy().astype(np.complex128)
+        _, g_o, g_p, _ = O.full_gradients(o64, p64, pos, props64, tg, mask, nsub, mean_i, up)
+        if t == 1:
+            grad_rel = float(np.linalg.norm(g32 - g_o) / np.linalg.norm(g_o))
+        o64 = adam_step("o", o64, g_o, 5e-3, t)
+        p64 = adam_step("p", p64, g_p, 1e-3, t)
+    ph64 = np.angle(O.constrain_object(o64))
+    ph32 = np.angle(O.constrain_object(sub.obj.detach().cpu().numpy().astype(np.complex128)))
+    d64 = ph64 - ph64.mean()
+    nrmse = float(np.linalg.norm((ph32 - ph32.mean()) - d64) / np.linalg.norm(d64))
+    return {"forward_intensity_rel_l2": inten_rel, "first_object_gradient_rel_l2": grad_rel,
+            "phase_nrmse_after_iters": nrmse, "iters": iters,
+            "sample": f"{nsub} positions spread over the scan; FP64 oracle (numpy/scipy) vs FP32 CUDA"}
 
 
 def run_kernel_only(args):
