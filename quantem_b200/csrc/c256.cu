@@ -1,4 +1,7 @@
 // 256 x 256 probe windows: cluster batch kernel and cluster FFT launches.
+// Complex arithmetic on packed FP32 pairs in this translation unit (fft_engine.cuh).
+#define QB_F32X2_ADD 1
+#define QB_F32X2_MUL 1
 #include "cluster256_kernels.cuh"
 #include "launch_impl.cuh"
 

@@ -35,8 +35,37 @@ namespace qb {
 // ---------------------------------------------------------------------------
 // complex helpers
 // ---------------------------------------------------------------------------
+// Complex arithmetic.  With QB_F32X2_ADD / QB_F32X2_MUL set (per translation unit,
+// before this header) it runs on sm_100's packed FP32 pairs, one instruction for the
+// real and imaginary parts, with the same roundings as the scalar forms
+//   a * b       = (fma(a.x, b.x, -(a.y b.y)), fma(a.x, b.y, a.y b.x))
+//   a * conj(b) = (fma(a.x, b.x, a.y b.y),    fma(a.y, b.x, -(a.x b.y)))
+// so results are bit-identical either way.  The packed operands live in aligned
+// register pairs, which costs registers: it pays in the 256^2 cluster kernels and
+// not in the 128^2 batch kernel, whose 512 threads already sit at 128 registers.
+#ifndef QB_F32X2_ADD
+#define QB_F32X2_ADD 0
+#endif
+#ifndef QB_F32X2_MUL
+#define QB_F32X2_MUL 0
+#endif
+#if QB_F32X2_ADD
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+#else
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+#endif
+#if QB_F32X2_MUL
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return __ffma2_rn(make_float2(a.x, a.x), b, __fmul2_rn(make_float2(a.y, a.y), make_float2(-b.y, b.x)));
+}
+// a * conj(b)
+__device__ __forceinline__ float2 cmulc(float2 a, float2 b) {
+  return __ffma2_rn(a, make_float2(b.x, b.x), __fmul2_rn(make_float2(a.y, -a.x), make_float2(b.y, b.y)));
+}
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return __fmul2_rn(a, make_float2(s, s)); }
+#else
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
 }
@@ -44,8 +73,9 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
 __device__ __forceinline__ float2 cmulc(float2 a, float2 b) {
   return make_float2(fmaf(a.x, b.x, a.y * b.y), fmaf(a.y, b.x, -a.x * b.y));
 }
-__device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
 __device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+#endif
+__device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
 __device__ __forceinline__ float cabs2(float2 a) { return fmaf(a.x, a.x, a.y * a.y); }
 
 // cos(2*pi*m/64) for m = 0..16 (first quadrant), IEEE double rounded to float.
