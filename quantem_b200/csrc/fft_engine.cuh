@@ -41,8 +41,9 @@ namespace qb {
 //   a * b       = (fma(a.x, b.x, -(a.y b.y)), fma(a.x, b.y, a.y b.x))
 //   a * conj(b) = (fma(a.x, b.x, a.y b.y),    fma(a.y, b.x, -(a.x b.y)))
 // so results are bit-identical either way.  The packed operands live in aligned
-// register pairs, which costs registers: it pays in the 256^2 cluster kernels and
-// not in the 128^2 batch kernel, whose 512 threads already sit at 128 registers.
+// register pairs, which costs registers: packed products pay in the 64^2, 96^2 and
+// 256^2 kernels but not in the 128^2 batch kernel, whose 512 threads already sit at
+// 128 registers (it packs only its additions).
 #ifndef QB_F32X2_ADD
 #define QB_F32X2_ADD 0
 #endif
