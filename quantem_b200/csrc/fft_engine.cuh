@@ -77,6 +77,18 @@ __device__ __forceinline__ float2 cmulc(float2 a, float2 b) {
 __device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
 #endif
 __device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
+// Packed products whatever the switches above say; QB_F32X2_S2 uses them for the
+// twiddle multiplies of the 2-D engine's middle stage only (no extra spills in the
+// 128^2 batch kernel, unlike packed products everywhere).
+__device__ __forceinline__ float2 pcmul(float2 a, float2 b) {
+  return __ffma2_rn(make_float2(a.x, a.x), b, __fmul2_rn(make_float2(a.y, a.y), make_float2(-b.y, b.x)));
+}
+__device__ __forceinline__ float2 pcmulc(float2 a, float2 b) {
+  return __ffma2_rn(a, make_float2(b.x, b.x), __fmul2_rn(make_float2(a.y, -a.x), make_float2(b.y, b.y)));
+}
+#ifndef QB_F32X2_S2
+#define QB_F32X2_S2 0
+#endif
 __device__ __forceinline__ float cabs2(float2 a) { return fmaf(a.x, a.x, a.y * a.y); }
 
 // cos(2*pi*m/64) for m = 0..16 (first quadrant), IEEE double rounded to float.
@@ -266,14 +278,14 @@ struct Fft2 {
     for (int cB = 1; cB < B; ++cB) {
       const float2 w = tw[(cB * s2_kA) & (N - 1)];
 #pragma unroll
-      for (int rC = 0; rC < C; ++rC) x[cB * C + rC] = cmul(x[cB * C + rC], w);
+      for (int rC = 0; rC < C; ++rC) x[cB * C + rC] = QB_F32X2_S2 ? pcmul(x[cB * C + rC], w) : cmul(x[cB * C + rC], w);
     }
     s2_core<false>(x);
 #pragma unroll
     for (int kC = 1; kC < C; ++kC) {
       const float2 w = tw[(s2_rD * kC) & (N - 1)];
 #pragma unroll
-      for (int kB = 0; kB < B; ++kB) x[kB * C + kC] = cmul(x[kB * C + kC], w);
+      for (int kB = 0; kB < B; ++kB) x[kB * C + kC] = QB_F32X2_S2 ? pcmul(x[kB * C + kC], w) : cmul(x[kB * C + kC], w);
     }
   }
   // S2 inverse: (kB, kC) on entry, (cB, rC) on exit.
@@ -282,14 +294,14 @@ struct Fft2 {
     for (int kC = 1; kC < C; ++kC) {
       const float2 w = tw[(s2_rD * kC) & (N - 1)];
 #pragma unroll
-      for (int kB = 0; kB < B; ++kB) x[kB * C + kC] = cmulc(x[kB * C + kC], w);
+      for (int kB = 0; kB < B; ++kB) x[kB * C + kC] = QB_F32X2_S2 ? pcmulc(x[kB * C + kC], w) : cmulc(x[kB * C + kC], w);
     }
     s2_core<true>(x);
 #pragma unroll
     for (int cB = 1; cB < B; ++cB) {
       const float2 w = tw[(cB * s2_kA) & (N - 1)];
 #pragma unroll
-      for (int rC = 0; rC < C; ++rC) x[cB * C + rC] = cmulc(x[cB * C + rC], w);
+      for (int rC = 0; rC < C; ++rC) x[cB * C + rC] = QB_F32X2_S2 ? pcmulc(x[cB * C + rC], w) : cmulc(x[cB * C + rC], w);
     }
   }
   // B-point DFT along index 0 (stride C) and C-point DFT along index 1 (stride 1).
