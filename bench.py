@@ -134,13 +134,13 @@ def _init_dist(world, backend):
     return None
 
 
-def build_problem(seed, device, batch_size):
+def build_problem(seed, device, batch_size, cfg=None):
     import torch
 
     from quantem_b200 import engine, synthetic
     from quantem_b200.diffractive_imaging.ptycho_utils import SimpleBatcher
 
-    cfg = synthetic.SyntheticConfig(seed=seed)
+    cfg = cfg or synthetic.SyntheticConfig(seed=seed)
     ds = synthetic.make_dataset(cfg, device)
     S, Ho, Wo = ds["obj_shape"]
     obj = torch.ones((S, Ho, Wo), dtype=torch.complex64, device=device).requires_grad_(True)
@@ -561,6 +561,58 @@ def accuracy_vs_fp64(pt, nsub=16, iters=3):
     return {"forward_intensity_rel_l2": inten_rel, "first_object_gradient_rel_l2": grad_rel,
             "phase_nrmse_after_iters": nrmse, "iters": iters,
             "sample": f"{nsub} positions spread over the scan; FP64 oracle (numpy/scipy) vs FP32 CUDA"}
+
+
+def c1_config():
+    """Single-slice, single-mode configuration: 256^2 object with 200 Gaussian atoms
+    (sigma 1.5 px, peak 0.3 rad), 64^2 probe (300 kV, 20 mrad, 200 A defocus, 0.2 A
+    pixels), 16 x 16 raster with 4 px step, 1e5 counts per pattern."""
+    from quantem_b200 import synthetic
+
+    return synthetic.SyntheticConfig(n=64, slices=1, modes=1, mode_weights=(1.0,), scan=(16, 16), step_px=4.0,
+                                     jitter_px=0.0, pad_px=98, peak_phase=0.3, atom_density=200 / 256 ** 2,
+                                     sigma_px=1.5, counts=1e5, seed=0)
+
+
+def run_c1(args):
+    """The single-slice, single-mode configuration (256 positions, 20 iterations of the
+    amplitude loss, Adam, full batch): the fused path on the GPU against the reference's
+    own PyTorch iteration on the GPU and on the host cores (package under baseline/_ref)."""
+    import torch
+
+    from quantem_b200 import engine
+
+    dev = torch.device("cuda", 0)
+    iters = 20
+    cfg = c1_config()
+    _, _, pt, opts, batcher = build_problem(0, dev, None, cfg=cfg)
+    for _ in range(args.warmup):
+        engine.run_iteration(pt, batcher, opts)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(iters):
+        loss = engine.run_iteration(pt, batcher, opts)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / iters
+    npos = pt.num_gpts
+    ours = {"positions_per_s": round(npos / (ms * 1e-3), 1), "ms_per_iteration": round(ms, 4),
+            "final_loss": float(loss)}
+    ref = {}
+    torch.set_num_threads(os.cpu_count() or 1)
+    for name, d in (("gpu", "cuda:0"), ("cpu", "cpu")):
+        try:
+            ref[name] = reference_torch_gpu(cfg, d, iters, args.warmup, npos)
+        except Exception as exc:  # a baseline: report, never fail the bench
+            ref[name] = {"unavailable": f"{type(exc).__name__}: {exc}"[:300]}
+    print(json.dumps({"metric": METRIC, "value": ours["positions_per_s"], "unit": "positions/s",
+                      "higher_is_better": True, "data": "synthetic", "dtype": "c64/f32",
+                      "config": {"workload": "single slice, single mode: 256x256 object, 64x64 probe, 16x16 scan, "
+                                             "4 px step, 1e5 counts, 20 iterations, batch 256, Adam",
+                                 "iterations": iters},
+                      "ours": ours, "reference_torch_gpu": ref.get("gpu"), "reference_torch_cpu": ref.get("cpu"),
+                      "cpu_threads": os.cpu_count()}))
 
 
 def run_kernel_only(args):
@@ -1023,7 +1075,9 @@ def reference_torch_gpu(cfg, device, steps, warmup, batch_size, ref_dir=None, ve
     from quantem.diffractive_imaging.ptychography import Ptychography
 
     dev = torch.device(device)
-    ds = synthetic.make_dataset(cfg, dev)
+    # the data are simulated with this package's forward kernels (on the GPU) in every case
+    sim_dev = torch.device("cuda", torch.cuda.current_device()) if torch.cuda.is_available() else dev
+    ds = synthetic.make_dataset(cfg, sim_dev)
     nr, nc = cfg.scan
     data = ds["intensities"].cpu().numpy().reshape(nr, nc, cfg.n, cfg.n)
     rs = 1.0 / (cfg.n * cfg.pixel)
@@ -1112,7 +1166,7 @@ def main():
     ap.add_argument("--batch-size", type=int, default=4096)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--kernel-only", action="store_true", help="time only the fused batch kernel")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "c5", "preprocess"],
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5", "preprocess"],
                     help="c2: the headline multislice mixed-probe iteration; c3: uneven multi-dataset launch; "
                          "c4: learned initialiser vs flat start; c5: 256x256 windows on thread-block clusters")
     ap.add_argument("--c4-objects", type=int, default=20000, help="training objects for --workload c4")
@@ -1130,7 +1184,9 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.workload == "c3":
+    if args.workload == "c1":
+        run_c1(args)
+    elif args.workload == "c3":
         run_c3(args)
     elif args.workload == "c4":
         run_c4_gemm(args) if args.kernel_only else run_c4(args)
