@@ -512,6 +512,7 @@ class Ptychography:
                 total += loss.detach()
                 nb += 1
             total_loss = float((total / max(nb, 1)).item())
+            ops.check_status(dev)  # out-of-range batch indices / non-finite intensities since the last check
             val_loss = None
             if batcher.has_validation:
                 vl, vb = 0.0, 0

@@ -8,6 +8,7 @@ and raise ``RuntimeError`` if the library is unavailable (no CPU fallback).
 from __future__ import annotations
 
 import ctypes
+import warnings
 from dataclasses import dataclass
 
 import torch
@@ -178,6 +179,39 @@ def workspace(device) -> Workspace:
     if key not in _WORKSPACES:
         _WORKSPACES[key] = Workspace(device)
     return _WORKSPACES[key]
+
+
+# Status word written by the batch kernels (one int32 per device workspace):
+# bits 0-19 count non-finite predicted intensities, bits 20-27 count batch indices
+# outside [0, npos) (those positions are skipped).
+STATUS_NONFINITE_MASK = (1 << 20) - 1
+STATUS_INVALID_SHIFT = 20
+
+
+def read_status(device=None, reset: bool = True) -> dict:
+    """Read (and by default clear) the batch kernels' status word of ``device``:
+    ``{"nonfinite": n, "invalid_indices": k, "raw": v}``.  One 4-byte device-to-host
+    copy, which waits for the work queued before it."""
+    dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+    ws = workspace(dev)
+    v = int(ws.status.item())
+    if reset and v:
+        ws.status.zero_()
+    return {"nonfinite": v & STATUS_NONFINITE_MASK, "invalid_indices": (v >> STATUS_INVALID_SHIFT) & 0xFF, "raw": v}
+
+
+def check_status(device=None) -> dict:
+    """Raise ``RuntimeError`` if a batch index was out of range since the last check
+    (the kernels skip such positions); warn when predicted intensities were non-finite
+    (the loss is then non-finite too, as in the reference).  Clears the word."""
+    st = read_status(device, reset=True)
+    if st["invalid_indices"]:
+        raise RuntimeError(f"{st['invalid_indices']} batch position(s) had an index outside [0, num positions); "
+                           "they were skipped by the batch kernel")
+    if st["nonfinite"]:
+        warnings.warn(f"{st['nonfinite']} predicted intensities were not finite (NaN / inf in the object or probe)",
+                      RuntimeWarning, stacklevel=2)
+    return st
 
 
 def default_grid(B: int, device=None) -> int:

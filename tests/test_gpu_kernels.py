@@ -230,3 +230,39 @@ def test_loss_types_match_fp64_oracle(cuda_device, n, loss_type):
     assert abs(loss.item() - loss_o) / abs(loss_o) < TOL_I
     assert rel(g_obj.cpu().numpy(), g_obj_o) < TOL_G
     assert rel(g_probe.cpu().numpy(), g_probe_o) < TOL_G
+
+
+def test_status_word_reports_invalid_indices_and_nonfinite(cuda_device):
+    """The batch kernels skip positions whose index is outside [0, npos) and count them,
+    and count non-finite predicted intensities; ops.check_status surfaces both."""
+    import warnings
+
+    from quantem_b200 import ops
+
+    rng = np.random.default_rng(5)
+    S, P, n, Ho, B, npos = 2, 1, 64, 96, 3, 3
+    obj = np.exp(1j * 0.2 * rng.standard_normal((S, Ho, Ho)))
+    probe = (rng.standard_normal((P, n, n)) + 1j * rng.standard_normal((P, n, n))) * 0.5
+    props = O.propagators((n, n), (0.2, 0.2), 300e3, [20.0] * (S - 1))
+    pos = rng.uniform(0, Ho, (npos, 2))
+    tg = np.abs(rng.standard_normal((npos, n, n)))
+    dev = cuda_device
+    args = dict(prop=_t(props.astype(np.complex64), dev), positions=_t(pos, dev, torch.float32),
+                targets=_t(tg, dev, torch.float32), mask=torch.ones((n, n), device=dev), num_gpts=npos,
+                mean_intensity=2.0)
+    obj_t, probe_t = _t(O.constrain_object(obj).astype(np.complex64), dev), _t(probe.astype(np.complex64), dev)
+    ops.read_status(dev)  # start clean
+    ops.batch_forward_adjoint(obj_t, probe_t, batch_idx=torch.tensor([0, 5, 1], device=dev), **args)
+    st = ops.read_status(dev, reset=False)
+    assert st["invalid_indices"] == 1 and st["nonfinite"] == 0
+    with pytest.raises(RuntimeError, match="outside"):
+        ops.check_status(dev)
+    assert ops.read_status(dev)["raw"] == 0  # cleared by the check
+    bad = obj_t.clone()
+    bad[0, 0:Ho, 0:Ho] = float("nan")
+    ops.batch_forward_adjoint(bad, probe_t, batch_idx=torch.arange(B, device=dev), **args)
+    with warnings.catch_warnings(record=True) as w:
+        warnings.simplefilter("always")
+        st = ops.check_status(dev)
+    assert st["nonfinite"] > 0 and st["invalid_indices"] == 0
+    assert any("not finite" in str(x.message) for x in w)
