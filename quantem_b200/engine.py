@@ -133,3 +133,67 @@ def run_iteration(pt: ProblemTensors, batcher: SimpleBatcher, optimizers=(), dev
         total += batch_step(pt, idx, optimizers)
         nb += 1
     return total / max(nb, 1)
+
+
+class GraphedIteration:
+    """One full-batch iteration of one dataset (forward, loss, fused adjoint, object-
+    gradient rescale, Adam on object and probe, probe orthogonalisation) captured in a
+    CUDA graph and replayed: the launch sequence of ``batch_step`` without the host's
+    per-launch cost.
+
+    The batch is every position in a fixed order (``batch_idx``, default a seeded
+    permutation, so that positions processed at the same time stay far apart); the
+    loss and gradients of a full batch do not depend on the order.  The optimisers
+    keep their step count and learning rate on the device (``multi.CapturableAdam``,
+    same update as torch.optim.Adam), so each replay advances the bias corrections."""
+
+    def __init__(self, pt: ProblemTensors, lr_obj: float = 5e-3, lr_probe: float = 1e-3, batch_idx=None,
+                 seed: int = 0):
+        from .multi import CapturableAdam
+
+        self.pt = pt
+        dev = pt.obj.device
+        if batch_idx is None:
+            g = torch.Generator().manual_seed(seed)
+            batch_idx = torch.randperm(pt.num_gpts, generator=g)
+        self.batch_idx = batch_idx.to(dev, torch.int64).contiguous()
+        self.opts = [CapturableAdam([pt.obj], lr=lr_obj), CapturableAdam([pt.probe], lr=lr_probe)]
+        self.graph = None
+        self.static_loss = None
+
+    def _step(self):
+        pt = self.pt
+        pt.obj.grad = None
+        pt.probe.grad = None
+        probe_o = orthogonalize_probes(pt.probe) if pt.orthogonalize else pt.probe
+        loss = ops.batch_loss(pt.obj, probe_o, pt.prop, pt.positions, self.batch_idx, pt.targets, pt.mask,
+                              pt.num_gpts, pt.mean_intensity, pt.loss_type, grid=pt.grid,
+                              recompute_every=pt.recompute_every)
+        loss.backward()
+        pt.obj.grad.mul_(pt.upsample_factor ** 2 / 2)  # ptychography.py:330-332
+        for o in self.opts:
+            o.step()
+        return loss.detach()
+
+    def run_eager(self):
+        return self._step()
+
+    def capture(self, warmup: int = 3):
+        """Warm up on a side stream (workspaces sized, kernels loaded), then capture."""
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            for _ in range(warmup):
+                self._step()
+        torch.cuda.current_stream().wait_stream(s)
+        self.pt.obj.grad = None
+        self.pt.probe.grad = None
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self.static_loss = self._step()
+        return self
+
+    def replay(self):
+        """One iteration; returns the batch loss (a device tensor overwritten by the next replay)."""
+        self.graph.replay()
+        return self.static_loss

@@ -98,3 +98,48 @@ def test_reconstruct_analytic_matches_oracle(cuda_device, case):
         probe = probe - lr * g_probe
     assert rel(pt.obj_model._obj.detach().cpu().numpy(), obj) < 1e-5
     assert rel(pt.probe_model._probe.detach().cpu().numpy(), probe) < 1e-5
+
+
+def test_graphed_iteration_matches_eager(cuda_device):
+    """engine.GraphedIteration (the full-batch iteration captured in a CUDA graph, device-side
+    Adam step counts) follows the eager batch_step + torch-style Adam trajectory."""
+    from quantem_b200 import engine
+
+    rng = np.random.default_rng(9)
+    S, P, n, Ho, npos = 2, 2, 64, 128, 24
+    dev = cuda_device
+    obj0 = torch.tensor(np.exp(1j * 0.1 * rng.standard_normal((S, Ho, Ho))), dtype=torch.complex64, device=dev)
+    probe0 = torch.tensor((rng.standard_normal((P, n, n)) + 1j * rng.standard_normal((P, n, n))) * 0.3,
+                          dtype=torch.complex64, device=dev)
+    props = torch.tensor(O.propagators((n, n), (0.2, 0.2), 300e3, [20.0] * (S - 1)), dtype=torch.complex64,
+                         device=dev)
+    pos = torch.tensor(rng.uniform(32, 96, (npos, 2)), dtype=torch.float32, device=dev)
+    tg = torch.tensor(np.abs(rng.standard_normal((npos, n, n))) * 2, dtype=torch.float32, device=dev)
+    mask = torch.ones((n, n), device=dev)
+
+    def problem():
+        return engine.ProblemTensors(obj=obj0.clone().requires_grad_(True), probe=probe0.clone().requires_grad_(True),
+                                     prop=props, positions=pos, targets=tg, mask=mask, mean_intensity=4.0,
+                                     upsample_factor=2.0)
+
+    pe = problem()
+    opts = [engine.make_optimizer([pe.obj], {"type": "adam", "lr": 5e-3}),
+            engine.make_optimizer([pe.probe], {"type": "adam", "lr": 1e-3})]
+    idx = torch.arange(npos, device=dev)
+    le, ge = [], None
+    for k in range(4):
+        le.append(float(engine.batch_step(pe, idx, opts)))
+        if k == 0:
+            ge = (pe.obj.grad.detach().cpu().numpy(), pe.probe.grad.detach().cpu().numpy())
+    pg = problem()
+    it = engine.GraphedIteration(pg, batch_idx=idx).capture(warmup=0)
+    lg, gg = [], None
+    for k in range(4):
+        lg.append(float(it.replay()))
+        if k == 0:
+            gg = (pg.obj.grad.detach().cpu().numpy(), pg.probe.grad.detach().cpu().numpy())
+    # the first step's gradients to the gradient tolerance, the loss trajectory to 1e-5 (the
+    # parameters themselves are not compared: Adam's first steps move every pixel by about
+    # lr whatever the size of its gradient, so weakly lit pixels follow rounding noise)
+    assert rel(gg[0], ge[0]) < 1e-4 and rel(gg[1], ge[1]) < 1e-4
+    np.testing.assert_allclose(lg, le, rtol=1e-5)
