@@ -266,3 +266,33 @@ def test_status_word_reports_invalid_indices_and_nonfinite(cuda_device):
         st = ops.check_status(dev)
     assert st["nonfinite"] > 0 and st["invalid_indices"] == 0
     assert any("not finite" in str(x.message) for x in w)
+
+
+@pytest.mark.parametrize("n", [128, 256])
+@pytest.mark.parametrize("B", [1, 2])
+def test_small_batches_at_the_object_edge(cuda_device, n, B):
+    """Batches smaller than the grid (one or two positions) whose windows wrap around the
+    object's edges (periodic patch indices, dataset_models.py:514-535): loss and
+    gradients against the FP64 oracle."""
+    from quantem_b200 import ops
+
+    rng = np.random.default_rng(31 + n + B)
+    S, P, Ho = 2, 2, n + 64
+    obj = np.exp(1j * 0.3 * rng.standard_normal((S, Ho, Ho))) * (1 - 0.2 * rng.random((S, Ho, Ho)))
+    probe = rng.standard_normal((P, n, n)) + 1j * rng.standard_normal((P, n, n))
+    probe *= np.exp(-((np.fft.fftfreq(n) * n)[:, None] ** 2 + (np.fft.fftfreq(n) * n)[None] ** 2) / (n * 2.0))
+    props = O.propagators((n, n), (0.2, 0.2), 300e3, [20.0] * (S - 1))
+    edge = np.array([[1.3, Ho - 2.6], [Ho - 0.4, 3.7]])[:B].astype(np.float32).astype(np.float64)  # both edges
+    targets = np.abs(rng.standard_normal((B, n, n))) * 2
+    obj_c = O.constrain_object(obj)
+    npos, mean_i = 50, 10.0
+    loss_o, g_obj_o, g_probe_o, _ = O.batch_loss_and_grads(obj_c, probe, edge, props, targets, np.ones((n, n)),
+                                                           npos, mean_i)
+    dev = cuda_device
+    loss, g_obj, g_probe = ops.batch_forward_adjoint(
+        _t(obj_c.astype(np.complex64), dev), _t(probe.astype(np.complex64), dev), _t(props.astype(np.complex64), dev),
+        _t(edge, dev, torch.float32), torch.arange(B, device=dev, dtype=torch.int64), _t(targets, dev, torch.float32),
+        torch.ones((n, n), device=dev), npos, mean_i)
+    assert abs(loss.item() - loss_o) / abs(loss_o) < TOL_I
+    assert rel(g_obj.cpu().numpy(), g_obj_o) < TOL_G
+    assert rel(g_probe.cpu().numpy(), g_probe_o) < TOL_G
