@@ -77,3 +77,32 @@ def test_c256_batch_matches_fp64_oracle(cuda_device, recompute_every, separable)
     assert abs(loss.item() - loss_o) / loss_o < TOL_I
     assert rel(g_obj.cpu().numpy(), g_obj_o) < TOL_G
     assert rel(g_probe.cpu().numpy(), g_probe_o) < TOL_G
+
+
+@pytest.mark.parametrize("S,P,recompute_every", [(1, 1, 0), (1, 2, 1), (3, 1, 2), (4, 2, 3)])
+def test_c256_slice_and_mode_counts(cuda_device, S, P, recompute_every):
+    """Single-slice and single-mode 256^2 batches, and checkpoint intervals that do not
+    divide the slice count: loss and gradients against the FP64 oracle."""
+    from quantem_b200 import ops
+
+    rng = np.random.default_rng(100 + 10 * S + P)
+    n, Ho, B, npos, mean_i = 256, 384, 3, 64, 20.0
+    obj = np.exp(1j * 0.3 * rng.standard_normal((S, Ho, Ho))) * (1 - 0.2 * rng.random((S, Ho, Ho)))
+    probe = rng.standard_normal((P, n, n)) + 1j * rng.standard_normal((P, n, n))
+    probe *= np.exp(-((np.fft.fftfreq(n) * n)[:, None] ** 2 + (np.fft.fftfreq(n) * n)[None] ** 2) / 800.0)
+    props = O.propagators((n, n), (0.2, 0.2), 300e3, [20.0] * (S - 1))
+    pos = rng.uniform(0, Ho, size=(B, 2)).astype(np.float32).astype(np.float64)
+    targets = np.abs(rng.standard_normal((B, n, n))) * 3
+    obj_c = O.constrain_object(obj)
+    loss_o, g_obj_o, g_probe_o, _ = O.batch_loss_and_grads(obj_c, probe, pos, props, targets, np.ones((n, n)),
+                                                           npos, mean_i)
+    dev = cuda_device
+    prop = _t(props.astype(np.complex64), dev) if S > 1 else torch.zeros((0, n, n), dtype=torch.complex64,
+                                                                           device=dev)
+    loss, g_obj, g_probe = ops.batch_forward_adjoint(
+        _t(obj_c.astype(np.complex64), dev), _t(probe.astype(np.complex64), dev), prop, _t(pos, dev, torch.float32),
+        torch.arange(B, device=dev, dtype=torch.int64), _t(targets, dev, torch.float32), torch.ones((n, n), device=dev),
+        npos, mean_i, recompute_every=recompute_every)
+    assert abs(loss.item() - loss_o) / abs(loss_o) < TOL_I
+    assert rel(g_obj.cpu().numpy(), g_obj_o) < TOL_G
+    assert rel(g_probe.cpu().numpy(), g_probe_o) < TOL_G
