@@ -336,6 +336,23 @@ int ptycho_pattern_shift_ramp(void* spectra, const double* shifts, int npos, int
 int ptycho_pattern_center(const void* shifted, int npos, int n, float scale, float* centered_amplitudes,
                           float* centered_intensities, void* stream);
 
+/* ---- probe-mode orthogonalisation (ProbePixelated._probe_orthogonalization_constraint,
+ * probe_models.py:484-525): modified Gram-Schmidt with the running vector, every mode
+ * rescaled to its original norm, modes sorted by descending intensity; one CTA. ---- */
+
+/* complex64 elements of the work buffer for P modes of nn elements (1 <= P <= 16). */
+int64_t ptycho_probe_ortho_work_elems(int P, int64_t nn);
+
+/* out (P, nn) = sorted orthogonalised modes of probe (P, nn), complex64; `work` keeps
+ * what the gradient needs.  out must not alias probe. */
+int ptycho_probe_orthogonalize(const void* probe, void* out, int P, int64_t nn, void* work, int64_t work_elems,
+                               void* stream);
+
+/* grad_probe = gradient w.r.t. probe of a real loss whose gradient w.r.t. the sorted
+ * output is grad_sorted (torch convention); `work` from the matching forward call. */
+int ptycho_probe_orthogonalize_vjp(const void* probe, const void* grad_sorted, void* grad_probe, int P, int64_t nn,
+                                   void* work, int64_t work_elems, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

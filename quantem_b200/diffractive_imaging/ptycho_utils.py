@@ -102,13 +102,52 @@ class SimpleBatcher:
         return int(ceil(len(self.val_indices) / self.batch_size)) if self.has_validation else 0
 
 
+class _OrthogonalizeProbes(torch.autograd.Function):
+    """The orthogonalisation on the GPU: one ``ptycho_probe_orthogonalize`` launch
+    forward, one ``ptycho_probe_orthogonalize_vjp`` launch backward."""
+
+    @staticmethod
+    def forward(ctx, probe):
+        from .. import _lib, ops
+
+        probe = probe.detach().contiguous()
+        P = probe.shape[0]
+        nn = probe[0].numel()
+        lib = _lib.lib()
+        we = int(lib.ptycho_probe_ortho_work_elems(P, nn))
+        work = torch.empty(we, dtype=torch.complex64, device=probe.device)
+        out = torch.empty_like(probe)
+        _lib.check(lib.ptycho_probe_orthogonalize(ops._p(probe), ops._p(out), P, nn, ops._p(work), we, ops._stream()),
+                   "probe_orthogonalize")
+        ctx.save_for_backward(probe, work)
+        return out
+
+    @staticmethod
+    def backward(ctx, grad_out):
+        from .. import _lib, ops
+
+        probe, work = ctx.saved_tensors
+        P = probe.shape[0]
+        nn = probe[0].numel()
+        g = grad_out.contiguous()
+        grad = torch.empty_like(probe)
+        _lib.check(_lib.lib().ptycho_probe_orthogonalize_vjp(ops._p(probe), ops._p(g), ops._p(grad), P, nn,
+                                                             ops._p(work), work.numel(), ops._stream()),
+                   "probe_orthogonalize_vjp")
+        return grad
+
+
 def orthogonalize_probes(start_probe: torch.Tensor) -> torch.Tensor:
     """Mixed-state Gram-Schmidt with norm restore and intensity sort.
 
     probe_models.py:484-525: modified Gram-Schmidt on the running vector,
     each mode rescaled to its original norm, modes sorted by descending
-    real-space intensity.  Differentiable (runs as tensor ops of (P, n, n)).
+    real-space intensity.  Differentiable.  CUDA complex64 stacks run on the
+    orthogonalisation kernels (forward and gradient, one launch each); host
+    tensors (set-up code) use the same steps as tensor ops.
     """
+    if start_probe.is_cuda and start_probe.dtype == torch.complex64 and 1 <= start_probe.shape[0] <= 16:
+        return _OrthogonalizeProbes.apply(start_probe)
     n_probes = start_probe.shape[0]
     original_norms = torch.sqrt(
         torch.sum(start_probe.real.square() + start_probe.imag.square(), dim=(-2, -1), keepdim=True))

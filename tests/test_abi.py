@@ -9,7 +9,7 @@ from tests.conftest import ROOT
 
 def _declared():
     txt = open(os.path.join(ROOT, "include", "ptycho_b200.h")).read()
-    return sorted(set(re.findall(r"^int\s+(ptycho_\w+)\s*\(", txt, flags=re.M)))
+    return sorted(set(re.findall(r"^(?:int|int64_t)\s+(ptycho_\w+)\s*\(", txt, flags=re.M)))
 
 
 def test_library_exports_every_declared_symbol():

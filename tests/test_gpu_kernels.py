@@ -327,3 +327,24 @@ def test_rectangular_object(cuda_device, n):
     assert abs(loss.item() - loss_o) / abs(loss_o) < TOL_I
     assert rel(g_obj.cpu().numpy(), g_obj_o) < TOL_G
     assert rel(g_probe.cpu().numpy(), g_probe_o) < TOL_G
+
+
+@pytest.mark.parametrize("P,n", [(1, 64), (2, 96), (4, 128), (6, 256)])
+def test_probe_orthogonalization_kernels_match_fp64_oracle(cuda_device, P, n):
+    """ptycho_probe_orthogonalize / _vjp (probe_models.py:484-525) against the FP64 oracle's
+    Gram-Schmidt and its reverse mode, through orthogonalize_probes and torch autograd."""
+    from quantem_b200.diffractive_imaging.ptycho_utils import orthogonalize_probes
+
+    rng = np.random.default_rng(P * 1000 + n)
+    probe = (rng.standard_normal((P, n, n)) + 1j * rng.standard_normal((P, n, n))) * rng.uniform(0.2, 2.0, (P, 1, 1))
+    probe = probe.astype(np.complex64).astype(np.complex128)
+    gs = (rng.standard_normal((P, n, n)) + 1j * rng.standard_normal((P, n, n)))
+    out_o, order_o, cache = O.gram_schmidt(probe)
+    g_o = O.gram_schmidt_vjp(cache, gs)
+    pt = torch.tensor(probe, dtype=torch.complex64, device=cuda_device, requires_grad=True)
+    out = orthogonalize_probes(pt)
+    assert rel(out.detach().cpu().numpy(), out_o) < TOL_I
+    # a real loss whose gradient w.r.t. the output is gs (torch convention)
+    loss = torch.sum(torch.real(torch.conj(torch.tensor(gs, dtype=torch.complex64, device=cuda_device)) * out))
+    loss.backward()
+    assert rel(pt.grad.cpu().numpy(), g_o) < TOL_G
