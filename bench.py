@@ -336,6 +336,10 @@ def run_ours(args):
     torch_ref = torch_eager_reference(pt, args.batch_size) if not args.skip_torch_reference else None
     ref_gpu = None
     if not args.skip_torch_reference:
+        import gc
+
+        gc.collect()  # hand the reference a clean allocator (graph pools, workspaces released)
+        torch.cuda.empty_cache()
         try:
             from quantem_b200 import synthetic
 
