@@ -336,17 +336,7 @@ def run_ours(args):
     torch_ref = torch_eager_reference(pt, args.batch_size) if not args.skip_torch_reference else None
     ref_gpu = None
     if not args.skip_torch_reference:
-        import gc
-
-        gc.collect()  # hand the reference a clean allocator (graph pools, workspaces released)
-        torch.cuda.empty_cache()
-        try:
-            from quantem_b200 import synthetic
-
-            ref_gpu = reference_torch_gpu(synthetic.SyntheticConfig(seed=0), device, 3, 3, args.batch_size)
-        except Exception as exc:  # the reference is a baseline here: report, never fail the bench
-            ref_gpu = {"unavailable": f"{type(exc).__name__}: {exc}"[:300]}
-        torch.cuda.empty_cache()
+        ref_gpu = reference_torch_gpu_subprocess(local, args.batch_size)
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": "positions/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
@@ -1162,6 +1152,29 @@ def reference_torch_gpu(cfg, device, steps, warmup, batch_size, ref_dir=None, ve
             "ms_per_step": round(ms, 2), "positions": npos, "setup_s": round(setup_s, 1),
             "final_loss": losses[-1] if losses else None,
             "what": "quantem Ptychography.reconstruct (reference PyTorch path, autograd, Adam) on this device"}
+
+
+def reference_torch_gpu_subprocess(local_device: int, batch_size: int, steps: int = 3, warmup: int = 3):
+    """``reference_torch_gpu`` in a fresh process on the same GPU (its own allocator and host
+    threads, nothing of this process's state), via ``bench.py --impl reference --torch-gpu``."""
+    env = {k: v for k, v in os.environ.items()
+           if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK", "LOCAL_WORLD_SIZE", "MASTER_ADDR", "MASTER_PORT",
+                        "GROUP_RANK", "ROLE_RANK", "TORCHELASTIC_RUN_ID")}
+    visible = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if visible:
+        env["CUDA_VISIBLE_DEVICES"] = visible.split(",")[local_device]
+    else:
+        env["CUDA_VISIBLE_DEVICES"] = str(local_device)
+    cmd = [sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--torch-gpu", "--steps", str(steps),
+           "--warmup", str(warmup), "--batch-size", str(batch_size)]
+    try:
+        out = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=900)
+        line = json.loads(out.stdout.strip().splitlines()[-1])
+    except Exception as exc:  # the reference is a baseline here: report, never fail the bench
+        return {"unavailable": f"{type(exc).__name__}: {exc}"[:300]}
+    if "unavailable" in line:
+        return {"unavailable": line["unavailable"]}
+    return line.get("reference_torch_gpu", line)
 
 
 def run_reference_torch_gpu(args):
