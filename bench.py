@@ -231,7 +231,10 @@ def run_ours(args):
     ops.PROFILE_EVENTS = None
     ms_eager = t0.elapsed_time(t1) / args.steps
     fused_ms = [a.elapsed_time(b) for a, b in fused_events]
-    launches_per_batch = 13  # ours per batch: probe orthogonalisation + its gradient, object constraint (2) and its VJP (2), probe FFT, fused batch kernel, loss and partial reductions, probe-gradient FFT, two Adam steps
+    # ours per batch: probe orthogonalisation and its gradient, object constraint (2) and its
+    # VJP (2), probe FFT, fused batch kernel, loss and partial reductions, probe-gradient FFT,
+    # two Adam steps
+    launches_per_batch = 13
     nbatches = len(batcher) * args.steps
 
     # ---- the same full-batch iteration captured in a CUDA graph and replayed ----
