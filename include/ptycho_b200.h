@@ -20,6 +20,10 @@
  *   ptycho_obj_constrain_vjp autograd of the same constraint
  *   ptycho_fft2              torch.fft.fft2/ifft2 of the probe stack
  *                            (ptycho_utils.py:133-135) and of the probe gradient
+ *   ptycho_probe_orthogonalize,
+ *   ptycho_probe_orthogonalize_vjp
+ *                            probe_models.py:484-525 (_probe_orthogonalization_constraint)
+ *                            and its autograd
  *   ptycho_reduce_partials,
  *   ptycho_reduce_loss       deterministic reductions of per-CTA partials
  *   ptycho_adam_step,
