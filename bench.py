@@ -618,13 +618,9 @@ def run_c1(args):
     npos = pt.num_gpts
     ours = {"positions_per_s": round(npos / (ms * 1e-3), 1), "ms_per_iteration": round(ms, 4),
             "final_loss": float(loss)}
-    ref = {}
-    torch.set_num_threads(os.cpu_count() or 1)
-    for name, d in (("gpu", "cuda:0"), ("cpu", "cpu")):
-        try:
-            ref[name] = reference_torch_gpu(cfg, d, iters, args.warmup, npos)
-        except Exception as exc:  # a baseline: report, never fail the bench
-            ref[name] = {"unavailable": f"{type(exc).__name__}: {exc}"[:300]}
+    ref = {name: reference_torch_gpu_subprocess(0, npos, steps=iters, warmup=args.warmup,
+                                                 extra=["--workload", "c1", "--ref-device", name])
+           for name in ("gpu", "cpu")}
     print(json.dumps({"metric": METRIC, "value": ours["positions_per_s"], "unit": "positions/s",
                       "higher_is_better": True, "data": "synthetic", "dtype": "c64/f32",
                       "config": {"workload": "single slice, single mode: 256x256 object, 64x64 probe, 16x16 scan, "
@@ -1157,7 +1153,8 @@ def reference_torch_gpu(cfg, device, steps, warmup, batch_size, ref_dir=None, ve
             "what": "quantem Ptychography.reconstruct (reference PyTorch path, autograd, Adam) on this device"}
 
 
-def reference_torch_gpu_subprocess(local_device: int, batch_size: int, steps: int = 3, warmup: int = 3):
+def reference_torch_gpu_subprocess(local_device: int, batch_size: int, steps: int = 3, warmup: int = 3,
+                                   extra=()):
     """``reference_torch_gpu`` in a fresh process on the same GPU (its own allocator and host
     threads, nothing of this process's state), via ``bench.py --impl reference --torch-gpu``."""
     env = {k: v for k, v in os.environ.items()
@@ -1169,7 +1166,7 @@ def reference_torch_gpu_subprocess(local_device: int, batch_size: int, steps: in
     else:
         env["CUDA_VISIBLE_DEVICES"] = str(local_device)
     cmd = [sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--torch-gpu", "--steps", str(steps),
-           "--warmup", str(warmup), "--batch-size", str(batch_size)]
+           "--warmup", str(warmup), "--batch-size", str(batch_size), *extra]
     try:
         out = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=900)
         line = json.loads(out.stdout.strip().splitlines()[-1])
@@ -1184,14 +1181,21 @@ def run_reference_torch_gpu(args):
     rank, world, _ = _dist_env()
     if rank != 0:
         return
+    import torch
+
     from quantem_b200 import synthetic
 
-    res = reference_torch_gpu(synthetic.SyntheticConfig(seed=0), "cuda:0", args.steps, args.warmup,
-                              args.batch_size)
+    c1 = args.workload == "c1"
+    cfg = c1_config() if c1 else synthetic.SyntheticConfig(seed=0)
+    device = "cuda:0" if args.ref_device == "gpu" else "cpu"
+    if device == "cpu":
+        torch.set_num_threads(os.cpu_count() or 1)
+    res = reference_torch_gpu(cfg, device, args.steps, args.warmup,
+                              cfg.scan[0] * cfg.scan[1] if c1 else args.batch_size)
     line = {"metric": METRIC, "unit": "positions/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64/f32",
-            "data": "synthetic", "impl": "reference", "device": "gpu",
-            "config": {"workload": WORKLOAD, "parallelism": "replicas1"}}
+            "data": "synthetic", "impl": "reference", "device": args.ref_device,
+            "config": {"workload": "c1" if c1 else WORKLOAD, "parallelism": "replicas1"}}
     if "unavailable" in res:
         line["unavailable"] = res["unavailable"]
     else:
@@ -1217,6 +1221,8 @@ def main():
     ap.add_argument("--torch-gpu", action="store_true",
                     help="with --impl reference: time the reference's own PyTorch iteration on the GPU "
                          "(package under baseline/_ref) instead of the CPU oracle port")
+    ap.add_argument("--ref-device", default="gpu", choices=["gpu", "cpu"],
+                    help="with --impl reference --torch-gpu: the device the reference's iteration runs on")
     ap.add_argument("--skip-torch-reference", action="store_true",
                     help="do not time the PyTorch-eager restatement of the reference path nor the "
                          "reference's own PyTorch iteration on the GPU")
@@ -1226,7 +1232,9 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.workload == "c1":
+    if args.impl == "reference" and args.torch_gpu:
+        run_reference_torch_gpu(args)
+    elif args.workload == "c1":
         run_c1(args)
     elif args.workload == "c3":
         run_c3(args)
