@@ -15,6 +15,7 @@ from __future__ import annotations
 
 import ctypes
 import time
+import warnings
 
 import numpy as np
 import torch
@@ -245,6 +246,24 @@ class MultiIteration:
     def replay(self):
         self.graph.replay()
         return self.static_losses
+
+    def check_status(self):
+        """Read and clear every dataset's status word (one small copy each, which waits for
+        the queued work): raise on out-of-range batch indices, warn on non-finite predicted
+        intensities, like ``ops.check_status`` for single-dataset launches."""
+        out = []
+        for d, p in enumerate(self.problems):
+            v = int(p.ws.status.item())
+            if v:
+                p.ws.status.zero_()
+            bad, nonfinite = (v >> ops.STATUS_INVALID_SHIFT) & 0xFF, v & ops.STATUS_NONFINITE_MASK
+            if bad:
+                raise RuntimeError(f"dataset {d}: {bad} batch position(s) had an index outside [0, num positions)")
+            if nonfinite:
+                warnings.warn(f"dataset {d}: {nonfinite} predicted intensities were not finite", RuntimeWarning,
+                              stacklevel=2)
+            out.append({"nonfinite": nonfinite, "invalid_indices": bad, "raw": v})
+        return out
 
 
 def autotune_grids(problems, total=None, trials=2, cache={}):

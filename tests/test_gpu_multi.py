@@ -63,6 +63,8 @@ def test_graphed_iteration_matches_eager(cuda_device):
     for pa, pb in zip(a, b):
         assert rel(pb.obj.detach().cpu().numpy(), pa.obj.detach().cpu().numpy()) < 1e-5
         assert rel(pb.probe.detach().cpu().numpy(), pa.probe.detach().cpu().numpy()) < 1e-5
+    st = gb.check_status()  # clean data: no skipped positions, finite intensities
+    assert len(st) == len(b) and all(x["raw"] == 0 for x in st)
 
 
 def test_autotune_returns_valid_partition(cuda_device):
