@@ -42,6 +42,17 @@ def test_host_side_validation_without_gpu():
     assert lib.ptycho_forward_loss(ctypes.byref(a), None) == 1      # missing pointers
     assert lib.ptycho_reduce_loss(None, 1, None, None) == 1
     assert lib.ptycho_fft2(None, None, 1, 128, 0, 1.0, None) == 1
+    # probe orthogonalisation: mode count and work size are checked before the launch
+    dummy = ctypes.c_void_p(16)  # never dereferenced: the calls fail validation
+    we = lib.ptycho_probe_ortho_work_elems(4, 128 * 128)
+    assert we >= 2 * 4 * 128 * 128
+    assert lib.ptycho_probe_orthogonalize(dummy, dummy, 17, 128 * 128, dummy, we, None) == 1
+    assert "P <= 16" in _lib.last_error()
+    assert lib.ptycho_probe_orthogonalize(dummy, ctypes.c_void_p(32), 4, 128 * 128, dummy, we - 1, None) == 1
+    assert "work" in _lib.last_error()
+    assert lib.ptycho_probe_orthogonalize(dummy, dummy, 4, 128 * 128, ctypes.c_void_p(64), we, None) == 1
+    assert "alias" in _lib.last_error()
+    assert lib.ptycho_probe_orthogonalize_vjp(None, dummy, dummy, 4, 128 * 128, dummy, we, None) == 1
     buf = ctypes.create_string_buffer(8)
     assert lib.ptycho_get_last_error(buf, 8) == 0 and len(buf.value) <= 7
 
