@@ -18,6 +18,9 @@
  *   ptycho_forward_adjoint   the above plus loss.backward() of ptychography.py:326-328
  *   ptycho_obj_constrain     object_models.py:289-300 (apply_hard_constraints, complex)
  *   ptycho_obj_constrain_vjp autograd of the same constraint
+ *   ptycho_obj_transmission, object_models.py:289-339 for complex, pure-phase and
+ *   ptycho_obj_transmission_vjp potential objects (+ exp(i V), object_models.py:252-256)
+ *                            and their autograd
  *   ptycho_fft2              torch.fft.fft2/ifft2 of the probe stack
  *                            (ptycho_utils.py:133-135) and of the probe gradient
  *   ptycho_probe_orthogonalize,
@@ -76,7 +79,10 @@ typedef struct ptycho_batch_args {
   float* out_intensity;      /* optional float32 (B, N, N): predicted intensities, detector layout */
   void* out_exit;            /* optional complex64 (P, B, N, N): exit waves */
   void* out_waves;           /* optional complex64 (S, P, B, N, N): wave entering each slice */
-  int* status;               /* optional int32: incremented by the count of non-finite intensities */
+  int* status;               /* optional int32 status word: bits 0-19 count non-finite predicted
+                                intensities, bits 20-30 count batch indices outside [0, npos)
+                                (those positions are skipped); each field saturates at its
+                                maximum instead of carrying into the next */
   const void* prop_r;        /* optional complex64 (S-1, N): separable propagator factors, */
   const void* prop_c;        /*   K_s[kr][kc] = prop_r[s][kr] * prop_c[s][kc] (kept in shared memory) */
   int n, S, P, B, Ho, Wo, npos, grid;
@@ -154,6 +160,31 @@ int ptycho_obj_constrain(const void* obj, void* out, int64_t count, double* work
 int ptycho_obj_constrain_vjp(const void* obj, const void* grad_c, void* grad_raw, int64_t count,
                              double* work, int nwork, const float* scale, void* stream);
 
+/* Object types of ptycho_obj_transmission (object_models.py:123-136). */
+#define PTYCHO_OBJ_COMPLEX 0    /* complex64 object, amplitude clamped to [0, 1] */
+#define PTYCHO_OBJ_PURE_PHASE 1 /* complex64 object, amplitude dropped */
+#define PTYCHO_OBJ_POTENTIAL 2  /* float32 potential V, transmission exp(i V) */
+
+/* Transmission the batch kernels multiply by, from the raw object of any type:
+ * apply_hard_constraints (object_models.py:289-339) followed by the exp(i V) of
+ * _get_obj_patches for potentials (object_models.py:252-256).
+ *   complex:    out = clamp(|o|,0,1) exp(i(angle(o) - mean angle))   (= ptycho_obj_constrain)
+ *   pure phase: out = exp(i(angle(o) - mean angle))
+ *   potential:  V' = V - offset, clamped at 0 when `positivity`; out = exp(i V'); offset =
+ *               baseline_factor * min(V) when `fix_baseline`, else 0.
+ * obj: complex64 (complex, pure phase) or float32 (potential), `count` elements; out:
+ * complex64.  work: float64 scratch of nwork >= 2 * ptycho_reduce_blocks() elements,
+ * reused by the matching _vjp call. */
+int ptycho_obj_transmission(const void* obj, void* out, int64_t count, int obj_type, int positivity,
+                            int fix_baseline, float baseline_factor, double* work, int nwork, void* stream);
+
+/* Gradient of ptycho_obj_transmission w.r.t. the raw object (torch convention; float32
+ * for potentials, the offset is detached as in the reference), scaled by the device
+ * float scale[0] (NULL means 1).  Same arguments and `work` as the forward call. */
+int ptycho_obj_transmission_vjp(const void* obj, const void* grad_t, void* grad_raw, int64_t count, int obj_type,
+                                int positivity, int fix_baseline, float baseline_factor, double* work, int nwork,
+                                const float* scale, void* stream);
+
 /* Blocks used by the reductions (size of `work` is 2x this). */
 int ptycho_reduce_blocks(void);
 
@@ -209,8 +240,10 @@ int ptycho_fp32_fma_probe(float* out, int iters, int blocks, void* stream);
  * device float *out_loss.  Nothing is allocated or freed.  a->grid above
  * PTYCHO_NOALLOC_MAX_GRID is rejected with PTYCHO_ERR_INVALID.  The first call
  * on a device looks up the array's device address (cudaGetSymbolAddress), so
- * make that first call before any stream capture.  All calls on a device share
- * the array: calls that overlap on the GPU race. */
+ * make that first call before any stream capture.  That address is cached for
+ * the life of the process, so a device reset (cudaDeviceReset, or a new primary
+ * context) between calls is not supported.  All calls on a device share the
+ * array: calls that overlap on the GPU race. */
 int ptycho_forward_loss_noalloc(const ptycho_batch_args* a, float* out_loss, void* stream);
 
 
@@ -353,7 +386,8 @@ int ptycho_probe_orthogonalize(const void* probe, void* out, int P, int64_t nn, 
                                void* stream);
 
 /* grad_probe = gradient w.r.t. probe of a real loss whose gradient w.r.t. the sorted
- * output is grad_sorted (torch convention); `work` from the matching forward call. */
+ * output is grad_sorted (torch convention); `work` from the matching forward call.
+ * grad_probe must not alias probe, grad_sorted or work (PTYCHO_ERR_INVALID). */
 int ptycho_probe_orthogonalize_vjp(const void* probe, const void* grad_sorted, void* grad_probe, int P, int64_t nn,
                                    void* work, int64_t work_elems, void* stream);
 

@@ -88,7 +88,7 @@ __global__ void __launch_bounds__(512, 1) cluster256_kernel(const BatchParams p)
   for (int b = cid * bchunk; b < bend; ++b) {
     const int64_t gi = p.batch_idx[b];
     if (gi < 0 || gi >= p.npos) {  // the whole cluster skips the position (same b)
-      if (tid == 0 && q == 0 && p.status) atomicAdd(p.status, 1 << 20);
+      if (tid == 0 && q == 0) status_add_invalid(p.status, 1);
       continue;
     }
     const float py = p.positions[2 * gi], px = p.positions[2 * gi + 1];
@@ -320,7 +320,7 @@ __global__ void __launch_bounds__(512, 1) cluster256_kernel(const BatchParams p)
     // l1/l2: sum / (B / num_gpts) / mean_I ; poisson: sum / mean_I
     p.loss_part[blockIdx.x] = t * (double)(p.loss_type == LOSS_POISSON ? p.inv_mean_intensity : p.loss_scale);
   }
-  if (nonfinite && p.status) atomicAdd(p.status, nonfinite);
+  status_add_nonfinite(p.status, nonfinite);
   cl.sync();  // no CTA leaves while a peer may still write into its shared memory
 }
 

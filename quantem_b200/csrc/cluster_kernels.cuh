@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(4 * N, 1) cluster_batch_kernel(const BatchPara
   for (int b = cid * bchunk; b < bend; ++b) {
     const int64_t gi = p.batch_idx[b];
     if (gi < 0 || gi >= p.npos) {  // uniform across the cluster: every CTA skips it
-      if (m == 0 && tid == 0 && p.status) atomicAdd(p.status, 1 << 20);
+      if (m == 0 && tid == 0) status_add_invalid(p.status, 1);
       continue;
     }
     const float py = p.positions[2 * gi], px = p.positions[2 * gi + 1];
@@ -234,7 +234,7 @@ __global__ void __launch_bounds__(4 * N, 1) cluster_batch_kernel(const BatchPara
     for (int w = 0; w < T / 32; ++w) t += red[w];
     p.loss_part[blockIdx.x] = t * (double)(p.loss_type == LOSS_POISSON ? p.inv_mean_intensity : p.loss_scale);
   }
-  if (p.status && nonfinite) atomicAdd(p.status, nonfinite);
+  status_add_nonfinite(p.status, nonfinite);
   cluster.sync();  // no CTA exits while another may still read its shared memory
 }
 

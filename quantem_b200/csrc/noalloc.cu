@@ -15,7 +15,10 @@
 //   * all calls on a device share the one array: two calls that overlap on the
 //     GPU (different streams, no ordering between them) race on it.  Every CTA of
 //     a call overwrites its own slot before the final sum reads it, so nothing
-//     needs clearing between calls.
+//     needs clearing between calls;
+//   * the array's device address is looked up on a device's first call and
+//     cached for the life of the process: a device reset (cudaDeviceReset, or a
+//     new primary context) between calls is not supported.
 #include <cuda_runtime.h>
 
 #include <mutex>

@@ -262,6 +262,9 @@ int ptycho_probe_orthogonalize_vjp(const void* probe, const void* grad_sorted, v
   if (work_elems < ptycho_probe_ortho_work_elems(P, nn))
     return fail(PTYCHO_ERR_INVALID, "probe_orthogonalize_vjp: work needs %lld complex elements",
                 (long long)ptycho_probe_ortho_work_elems(P, nn));
+  // the kernel reads probe and grad_sorted while it writes grad_probe (restrict pointers)
+  if (grad_probe == probe || grad_probe == grad_sorted || grad_probe == work)
+    return fail(PTYCHO_ERR_INVALID, "probe_orthogonalize_vjp: grad_probe must not alias probe, grad_sorted or work");
   probe_ortho_vjp_kernel<<<1, kThreads, 0, static_cast<cudaStream_t>(stream)>>>(
       static_cast<const float2*>(probe), static_cast<const float2*>(grad_sorted), static_cast<float2*>(grad_probe), P,
       nn, static_cast<float2*>(work));

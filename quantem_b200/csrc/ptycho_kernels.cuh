@@ -63,11 +63,97 @@ struct BatchParams {
   int ckpt;                   // 256^2 cluster kernel: checkpoint interval of the adjoint (0 = keep all waves)
 };
 
+// Status word of the batch kernels: bits 0-19 count non-finite predicted
+// intensities, bits 20-30 count batch indices outside [0, npos).  Each field
+// saturates at its maximum instead of carrying into the next one (a NaN object at
+// thousands of positions x 128^2 pixels would otherwise overflow the first field
+// into the second).  A bounded compare-and-swap loop; it runs only on error paths.
+constexpr int kStatusNonfiniteBits = 20;
+constexpr int kStatusInvalidShift = 20;
+constexpr int kStatusInvalidBits = 11;
+__device__ __forceinline__ void status_add(int* st, int shift, int bits, int n) {
+  if (!st || n <= 0) return;
+  const unsigned fmask = (1u << bits) - 1u;
+  unsigned old = *reinterpret_cast<volatile unsigned*>(st);
+  for (int it = 0; it < 4096; ++it) {
+    const unsigned cur = (old >> shift) & fmask;
+    const unsigned add = (unsigned)n < fmask - cur ? (unsigned)n : fmask - cur;
+    if (add == 0) return;
+    const unsigned want = old + (add << shift);
+    const unsigned seen = atomicCAS(reinterpret_cast<unsigned*>(st), old, want);
+    if (seen == old) return;
+    old = seen;
+  }
+}
+__device__ __forceinline__ void status_add_nonfinite(int* st, int n) { status_add(st, 0, kStatusNonfiniteBits, n); }
+__device__ __forceinline__ void status_add_invalid(int* st, int n) {
+  status_add(st, kStatusInvalidShift, kStatusInvalidBits, n);
+}
+
 __device__ __forceinline__ int fsigned(int k, int n) { return k < n / 2 ? k : k - n; }
 __device__ __forceinline__ int wrap_index(int x, int n) {
   x %= n;
   return x < 0 ? x + n : x;
 }
+
+// ---- experimental switches (defaults = current behaviour) ----
+#ifndef QB_LIFO
+#define QB_LIFO 0
+#endif
+#ifndef QB_OBJ_HINT
+#define QB_OBJ_HINT 0
+#endif
+#ifndef QB_DISCARD
+#define QB_DISCARD 0
+#endif
+#ifndef QB_PREFETCH
+#define QB_PREFETCH 0
+#endif
+#ifndef QB_PF_ELEMS
+#define QB_PF_ELEMS 16
+#endif
+constexpr int kPrefetchElems = QB_PF_ELEMS;  // object values per thread staged by cp.async
+
+__device__ __forceinline__ uint64_t evict_last_policy() {
+  uint64_t pol;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+__device__ __forceinline__ float2 ld_obj(const float2* ptr, uint64_t pol) {
+#if QB_OBJ_HINT
+  float2 v;
+  asm("ld.global.nc.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;" : "=f"(v.x), "=f"(v.y) : "l"(ptr), "l"(pol));
+  return v;
+#else
+  (void)pol;
+  return __ldg(ptr);
+#endif
+}
+__device__ __forceinline__ float ld_stream(const float* ptr) {
+#if QB_OBJ_HINT
+  return __ldcs(ptr);
+#else
+  return __ldg(ptr);
+#endif
+}
+// drop the L2 lines of a saved wave word range that no one reads again (no write-back)
+__device__ __forceinline__ void discard_pairs(const float4* warp_base_word) {
+#if QB_DISCARD
+  __syncwarp();
+  const int lane = threadIdx.x & 31;
+  if ((lane & 7) == 0)
+    asm volatile("discard.global.L2 [%0], 128;" ::"l"(reinterpret_cast<const char*>(warp_base_word) + lane * 16)
+                 : "memory");
+#else
+  (void)warp_base_word;
+#endif
+}
+__device__ __forceinline__ void cp_async8(float2* dst, const float2* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // Saved per-thread register arrays (waves, far fields, checkpoints) are stored
 // thread-major with the register pair (e, e+1) packed into one 16-byte word:
@@ -106,7 +192,8 @@ constexpr size_t fused_smem_bytes_sep(int S) {
 // to the L1 cache hold the register spills of the 512-thread CTA.
 template <int N, bool ADJ>
 constexpr size_t batch_smem_bytes(bool sep, int S) {
-  return (sep ? fused_smem_bytes_sep<N>(S) : fused_smem_bytes<N>()) - (ADJ ? sizeof(float) * (size_t)N * N : 0);
+  return (sep ? fused_smem_bytes_sep<N>(S) : fused_smem_bytes<N>()) - (ADJ ? sizeof(float) * (size_t)N * N : 0) +
+         (QB_PREFETCH && ADJ ? sizeof(float2) * (size_t)kPrefetchElems * 4 * N : 0);
 }
 
 template <int N>
@@ -180,15 +267,15 @@ __device__ __forceinline__ void apply_prop(const Fft2<N>& f, float2 (&x)[Fft2<N>
 // x (S1 layout) *= o (CONJ: conj(o)) for the object row orow_ptr, columns through
 // colmap.  Loads go in batches of 8 so that a batch is in flight at once while
 // the wave occupies half of the register file.
-template <int N, bool CONJ>
+template <int N, bool CONJ, int E0 = 0>
 __device__ __forceinline__ void gather_mul(const Fft2<N>& f, float2 (&x)[Fft2<N>::E], const float2* orow_ptr,
-                                           const int* colmap) {
+                                           const int* colmap, uint64_t pol = 0) {
   constexpr int E = Fft2<N>::E;
 #pragma unroll
-  for (int e0 = 0; e0 < E; e0 += 8) {
+  for (int e0 = E0; e0 < E; e0 += 8) {
     float2 ob[8];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) ob[j] = __ldg(orow_ptr + colmap[f.s1_col(e0 + j)]);
+    for (int j = 0; j < 8; ++j) ob[j] = ld_obj(orow_ptr + colmap[f.s1_col(e0 + j)], pol);
 #pragma unroll
     for (int j = 0; j < 8; ++j) x[e0 + j] = CONJ ? cmulc(x[e0 + j], ob[j]) : cmul(x[e0 + j], ob[j]);
   }
@@ -239,6 +326,11 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
   float2* sKr = reinterpret_cast<float2*>(colmap + N);
   float2* sKc = sKr + (size_t)N * (p.S > 1 ? p.S - 1 : 0);
   const bool sep = p.prop_r != nullptr;
+  // per-thread staging of the next real-space step's first object values (thread-major)
+  float2* pf = (sep ? sKc : sKr) + (sep ? (size_t)N * (p.S > 1 ? p.S - 1 : 0) : 0);
+  constexpr bool PF = QB_PREFETCH && ADJ;
+  bool pf_ready = false;
+  const uint64_t pol = QB_OBJ_HINT ? evict_last_policy() : 0;
   __shared__ double red[32];
 
   const int tid = threadIdx.x;
@@ -287,7 +379,7 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
   for (int b = cta * bchunk; b < bend; ++b) {
     const int64_t gi = p.batch_idx[b];
     if (gi < 0 || gi >= p.npos) {  // invalid index: skip the position and report it
-      if (tid == 0 && p.status) atomicAdd(p.status, 1 << 20);
+      if (tid == 0) status_add_invalid(p.status, 1);
       continue;
     }
     const float py = p.positions[2 * gi], px = p.positions[2 * gi + 1];
@@ -311,6 +403,20 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
     }
     __syncthreads();
     const int orow = rowmap[f.s1_r];
+    pf_ready = false;
+    // stage the object values e < kPrefetchElems of slice ns for the next real-space step
+    auto prefetch = [&](int ns) {
+      if (!PF) return;
+      if (ns < 0) {
+        pf_ready = false;
+        return;
+      }
+      const float2* nrow = p.obj + (size_t)ns * HoWo + (size_t)orow * p.Wo;
+#pragma unroll
+      for (int e = 0; e < kPrefetchElems; ++e) cp_async8(pf + e * T + tid, nrow + colmap[f.s1_col(e)]);
+      cp_async_commit();
+      pf_ready = true;
+    };
 
     // One loop with a single inverse and a single forward transform site walks
     // the forward chains of all modes, the loss, and (ADJ) the reverse chains.
@@ -351,6 +457,8 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
           x[e] = make_float2(v.x * 2.0f * in.x, v.y * 2.0f * in.x);
           x[e + 1] = make_float2(v.z * 2.0f * in.y, v.w * 2.0f * in.y);
         }
+#pragma unroll
+        for (int e = 0; e < E; e += 2) discard_pairs(reinterpret_cast<const float4*>(fw) + (e >> 1) * T + (tid & ~31));
       }
     };
     int m = 0, s = 0;
@@ -372,7 +480,16 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
 #pragma unroll
           for (int e = 0; e < E; ++e) ow[f.s1_col(e)] = x[e];
         }
-        gather_mul<N, false>(f, x, orow_ptr, colmap);
+        if (PF && pf_ready) {
+          cp_async_wait_all();
+#pragma unroll
+          for (int e = 0; e < kPrefetchElems; ++e) x[e] = cmul(x[e], pf[e * T + tid]);
+          gather_mul<N, false, kPrefetchElems>(f, x, orow_ptr, colmap, pol);
+        } else {
+          gather_mul<N, false>(f, x, orow_ptr, colmap, pol);
+        }
+        // next real-space step: next slice, next mode's first slice, or the adjoint's last slice
+        prefetch(s < S - 1 ? s + 1 : (m < P - 1 ? 0 : (ADJ ? S - 1 : -1)));
         if (s == S - 1 && p.out_exit) {
           float2* oe = p.out_exit + ((size_t)m * p.B + b) * NN + (size_t)f.s1_r * N;
 #pragma unroll
@@ -382,6 +499,7 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
         const float sc = first_bwd ? inv_n : inv_n2;  // adjoint of the orthonormal FFT, or of a propagation
         const float2* wv = slot + (size_t)(m * S + s) * NN;
         float2* grow = p.grad_obj + (size_t)s * HoWo + (size_t)orow * p.Wo;
+        if (PF && pf_ready) cp_async_wait_all();
 #pragma unroll
         for (int e0 = 0; e0 < E; e0 += 8) {
           float2 ps[8], ob[8];
@@ -395,7 +513,11 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
 #pragma unroll
           for (int j = 0; j < 8; ++j) {
             col[j] = colmap[f.s1_col(e0 + j)];
-            ob[j] = __ldg(orow_ptr + col[j]);
+            if (PF && e0 < kPrefetchElems) {
+              ob[j] = pf_ready ? pf[(e0 + j) * T + tid] : ld_obj(orow_ptr + col[j], pol);
+            } else {
+              ob[j] = ld_obj(orow_ptr + col[j], pol);
+            }
           }
 #pragma unroll
           for (int j = 0; j < 8; ++j) {
@@ -403,11 +525,20 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
             atomicAdd(grow + col[j], cmulc(g, ps[j]));  // conj(psi) * g
             x[e0 + j] = cmulc(g, ob[j]);                 // conj(o) * g
           }
+          if (!AN) {
+#pragma unroll
+            for (int j = 0; j < 8; j += 2)
+              discard_pairs(reinterpret_cast<const float4*>(wv) + ((e0 + j) >> 1) * T + (tid & ~31));
+          }
           if (AN) {  // sum_patches(|psi|^2) of this slice and mode (object_models.py:701-703)
             float* nrow = p.an_norm + ((size_t)s * P + m) * HoWo + (size_t)orow * p.Wo;
 #pragma unroll
             for (int j = 0; j < 8; ++j) atomicAdd(nrow + col[j], cabs2(ps[j]));
           }
+        }
+        {
+          const bool more = QB_LIFO ? m > 0 : m < P - 1;
+          prefetch(s > 0 ? s - 1 : (more ? S - 1 : -1));
         }
         if (AN && s == 0) {
           // analytic probe update: sum over positions of the back-propagated
@@ -421,8 +552,8 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
 #pragma unroll
             for (int j = 0; j < 8; ++j) pg[f.s1_col(e0 + j)] = cadd(old[j], x[e0 + j]);
           }
-          if (m < P - 1) {
-            ++m;
+          if (QB_LIFO ? m > 0 : m < P - 1) {
+            m += QB_LIFO ? -1 : 1;
             s = S - 1;
             first_bwd = true;
             load_far_seed(m);
@@ -478,7 +609,7 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
               const float I = inten[li];
               if (!isfinite(I)) ++nonfinite;
               float dldi;
-              const float tv = __ldg(tg + di);
+              const float tv = ld_stream(tg + di);
               loss_elem<N>(p, I, tv, __ldg(p.mask + di), loss_acc, dldi);
               if (ADJ && AN) {
                 // factor f and additive fix of the Fourier projection seed
@@ -498,9 +629,9 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
         if (!ADJ) break;
         bwd = true;
         first_bwd = true;
-        m = 0;
+        m = QB_LIFO ? P - 1 : 0;
         s = S - 1;
-        load_far_seed(0);
+        load_far_seed(m);
         continue;
       }
       first_bwd = false;
@@ -510,8 +641,8 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
         continue;
       }
       accumulate_probe_grad<N>(f, x, pgrad + (size_t)m * NN, rowf, colf);
-      if (m < P - 1) {
-        ++m;
+      if (QB_LIFO ? m > 0 : m < P - 1) {
+        m += QB_LIFO ? -1 : 1;
         s = S - 1;
         first_bwd = true;
         load_far_seed(m);
@@ -531,7 +662,7 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
     // l1/l2: sum / (B / num_gpts) / mean_I ; poisson: sum / mean_I
     p.loss_part[cta] = t * (double)(p.loss_type == LOSS_POISSON ? p.inv_mean_intensity : p.loss_scale);
   }
-  if (p.status && nonfinite) atomicAdd(p.status, nonfinite);
+  status_add_nonfinite(p.status, nonfinite);
 }
 
 template <int N, bool ADJ, bool AN = false>

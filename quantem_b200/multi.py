@@ -251,18 +251,22 @@ class MultiIteration:
         """Read and clear every dataset's status word (one small copy each, which waits for
         the queued work): raise on out-of-range batch indices, warn on non-finite predicted
         intensities, like ``ops.check_status`` for single-dataset launches."""
+        # every word is read and cleared before anything is raised, so no dataset's
+        # count is left behind for the next check
         out = []
-        for d, p in enumerate(self.problems):
+        for p in self.problems:
             v = int(p.ws.status.item())
             if v:
                 p.ws.status.zero_()
-            bad, nonfinite = (v >> ops.STATUS_INVALID_SHIFT) & 0xFF, v & ops.STATUS_NONFINITE_MASK
-            if bad:
-                raise RuntimeError(f"dataset {d}: {bad} batch position(s) had an index outside [0, num positions)")
-            if nonfinite:
-                warnings.warn(f"dataset {d}: {nonfinite} predicted intensities were not finite", RuntimeWarning,
-                              stacklevel=2)
-            out.append({"nonfinite": nonfinite, "invalid_indices": bad, "raw": v})
+            out.append(ops.decode_status(v))
+        for d, st in enumerate(out):
+            if st["nonfinite"]:
+                warnings.warn(f"dataset {d}: {st['nonfinite']} predicted intensities were not finite",
+                              RuntimeWarning, stacklevel=2)
+        bad = [(d, st["invalid_indices"]) for d, st in enumerate(out) if st["invalid_indices"]]
+        if bad:
+            raise RuntimeError("batch position(s) with an index outside [0, num positions): "
+                               + ", ".join(f"dataset {d}: {k}" for d, k in bad))
         return out
 
 

@@ -126,6 +126,83 @@ def constrained_object(obj: torch.Tensor) -> torch.Tensor:
     return _ObjConstrainFn.apply(obj)
 
 
+OBJ_TYPES = {"complex": 0, "pure_phase": 1, "potential": 2}
+
+
+@dataclass(frozen=True)
+class ObjSpec:
+    """How a raw object becomes the transmission the batch kernels multiply by
+    (object_models.py:289-339, 252-256): the object type and the potential's
+    positivity / baseline constraints."""
+
+    obj_type: str = "complex"
+    positivity: bool = True
+    fix_baseline: bool = False
+    baseline_factor: float = 1.0
+
+    def __post_init__(self):
+        if self.obj_type not in OBJ_TYPES:
+            raise ValueError(f"object type must be one of {list(OBJ_TYPES)}, got {self.obj_type!r}")
+
+    @property
+    def raw_dtype(self):
+        return torch.float32 if self.obj_type == "potential" else torch.complex64
+
+
+COMPLEX_OBJECT = ObjSpec()
+
+
+def _spec_args(spec: ObjSpec):
+    return (OBJ_TYPES[spec.obj_type], int(bool(spec.positivity)), int(bool(spec.fix_baseline)),
+            float(spec.baseline_factor))
+
+
+def obj_transmission(obj: torch.Tensor, spec: ObjSpec = COMPLEX_OBJECT, work: torch.Tensor | None = None,
+                     out: torch.Tensor | None = None):
+    """Transmission (complex64) of a raw object of any type; returns (out, work)."""
+    _req(obj, "obj", spec.raw_dtype)
+    work = new_constraint_work(obj.device) if work is None else work
+    out = torch.empty(obj.shape, dtype=torch.complex64, device=obj.device) if out is None else out
+    _lib.check(_lib.lib().ptycho_obj_transmission(_p(obj), _p(out), obj.numel(), *_spec_args(spec), _p(work),
+                                                  work.numel(), _stream()), "obj_transmission")
+    return out, work
+
+
+def obj_transmission_vjp(obj: torch.Tensor, grad_t: torch.Tensor, work: torch.Tensor, spec: ObjSpec = COMPLEX_OBJECT,
+                         scale: torch.Tensor | None = None, out: torch.Tensor | None = None):
+    """Gradient w.r.t. the raw object (its own dtype) of a loss whose gradient w.r.t. the
+    transmission is ``grad_t``; ``work`` from the matching ``obj_transmission`` call."""
+    _req(obj, "obj", spec.raw_dtype)
+    _req(grad_t, "grad_t", torch.complex64)
+    out = torch.empty_like(obj) if out is None else out
+    if scale is not None:
+        scale = scale.detach().to(torch.float32).contiguous()
+    _lib.check(_lib.lib().ptycho_obj_transmission_vjp(_p(obj), _p(grad_t), _p(out), obj.numel(), *_spec_args(spec),
+                                                      _p(work), work.numel(), _p(scale), _stream()),
+               "obj_transmission_vjp")
+    return out
+
+
+class _ObjTransmissionFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, obj, spec):
+        out, work = obj_transmission(obj.detach().contiguous(), spec)
+        ctx.spec = spec
+        ctx.save_for_backward(obj, work)
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        obj, work = ctx.saved_tensors
+        return obj_transmission_vjp(obj.detach().contiguous(), g.contiguous().to(torch.complex64), work,
+                                    ctx.spec), None
+
+
+def object_transmission(obj: torch.Tensor, spec: ObjSpec = COMPLEX_OBJECT) -> torch.Tensor:
+    """Differentiable transmission of a raw object of any type (CUDA kernels)."""
+    return _ObjTransmissionFn.apply(obj, spec)
+
+
 # ----------------------------------------------------------------------------
 # batch kernels
 # ----------------------------------------------------------------------------
@@ -182,10 +259,18 @@ def workspace(device) -> Workspace:
 
 
 # Status word written by the batch kernels (one int32 per device workspace):
-# bits 0-19 count non-finite predicted intensities, bits 20-27 count batch indices
-# outside [0, npos) (those positions are skipped).
+# bits 0-19 count non-finite predicted intensities, bits 20-30 count batch indices
+# outside [0, npos) (those positions are skipped).  Each field saturates at its
+# maximum, so a large non-finite count never reads as bad indices.
 STATUS_NONFINITE_MASK = (1 << 20) - 1
 STATUS_INVALID_SHIFT = 20
+STATUS_INVALID_MASK = (1 << 11) - 1
+
+
+def decode_status(v: int) -> dict:
+    """Split a raw status word into its two counters."""
+    return {"nonfinite": v & STATUS_NONFINITE_MASK,
+            "invalid_indices": (v >> STATUS_INVALID_SHIFT) & STATUS_INVALID_MASK, "raw": v}
 
 
 def read_status(device=None, reset: bool = True) -> dict:
@@ -197,7 +282,7 @@ def read_status(device=None, reset: bool = True) -> dict:
     v = int(ws.status.item())
     if reset and v:
         ws.status.zero_()
-    return {"nonfinite": v & STATUS_NONFINITE_MASK, "invalid_indices": (v >> STATUS_INVALID_SHIFT) & 0xFF, "raw": v}
+    return decode_status(v)
 
 
 def check_status(device=None) -> dict:
@@ -429,7 +514,9 @@ class _BatchLossFn(torch.autograd.Function):
     def forward(ctx, obj_raw, probe_o, prop, positions, batch_idx, targets, mask, cfg):
         obj_raw_c = obj_raw.detach().contiguous()
         probe_c = probe_o.detach().contiguous()
-        obj_c, work = obj_constrain(obj_raw_c)
+        spec = cfg.get("obj_spec") or COMPLEX_OBJECT
+        ctx.spec = spec
+        obj_c, work = obj_transmission(obj_raw_c, spec)
         need = ctx.needs_input_grad[0] or ctx.needs_input_grad[1]
         if need:
             loss, g_obj_c, g_probe = batch_forward_adjoint(
@@ -449,18 +536,19 @@ class _BatchLossFn(torch.autograd.Function):
         gout = gout.detach().to(torch.float32).reshape(1).contiguous()
         g_obj = None
         if ctx.needs_input_grad[0]:
-            g_obj = obj_constrain_vjp(obj_raw, g_obj_c, work, scale=gout)
+            g_obj = obj_transmission_vjp(obj_raw, g_obj_c, work, ctx.spec, scale=gout)
         g_pr = g_probe * gout if ctx.needs_input_grad[1] else None
         return g_obj, g_pr, None, None, None, None, None, None
 
 
 def batch_loss(obj_raw, probe_o, prop, positions, batch_idx, targets, mask, num_gpts, mean_intensity,
-               loss_type="l2_amplitude", grid=None, variant="auto", recompute_every=None):
+               loss_type="l2_amplitude", grid=None, variant="auto", recompute_every=None, obj_spec=None):
     """Differentiable consistency loss of one batch w.r.t. the raw object
-    parameter (hard constraint included) and the orthogonalised probe.
-    ``recompute_every`` (256 x 256 windows): adjoint checkpoint interval."""
+    parameter (hard constraint and, for potentials, exp(i V) included) and the
+    orthogonalised probe.  ``obj_spec`` (default: complex object) names the object
+    type; ``recompute_every`` (256 x 256 windows): adjoint checkpoint interval."""
     cfg = dict(num_gpts=int(num_gpts), mean_intensity=float(mean_intensity), loss_type=loss_type, grid=grid,
-               variant=variant, recompute_every=recompute_every)
+               variant=variant, recompute_every=recompute_every, obj_spec=obj_spec)
     return _BatchLossFn.apply(obj_raw, probe_o, prop, positions, batch_idx, targets, mask, cfg)
 
 

@@ -2,7 +2,7 @@
 
 Run in a container where the reference source tree is mounted:
 
-    python tests/golden/make_golden_cnn.py /root/reference/src
+    python tests/golden/make_golden_cnn.py <reference checkout>/src
 
 Builds the reference's ``quantem.core.ml.cnn.CNN2d`` (UNet topology of
 core/ml/cnn.py:17-212 with the blocks of core/ml/blocks.py) for a few small
@@ -66,7 +66,9 @@ def run_case(name, cfg):
 
 
 def main():
-    src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src"
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {os.path.relpath(__file__)} <reference source dir (the one holding quantem/)>")
+    src = sys.argv[1]
     import_reference(src)
     for name, cfg in CASES.items():
         run_case(name, cfg)

@@ -2,7 +2,7 @@
 
 Run in a container where the reference source tree is mounted:
 
-    python tests/golden/make_golden_loss.py /root/reference/src
+    python tests/golden/make_golden_loss.py <reference checkout>/src
 
 Calls the reference's own ``PtychographyBase.error_estimate``
 (ptychography_base.py:908-932) on seeded predicted intensities, targets and a
@@ -53,4 +53,6 @@ def main(src):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src")
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {os.path.relpath(__file__)} <reference source dir (the one holding quantem/)>")
+    main(sys.argv[1])

@@ -53,6 +53,11 @@ def test_host_side_validation_without_gpu():
     assert lib.ptycho_probe_orthogonalize(dummy, dummy, 4, 128 * 128, ctypes.c_void_p(64), we, None) == 1
     assert "alias" in _lib.last_error()
     assert lib.ptycho_probe_orthogonalize_vjp(None, dummy, dummy, 4, 128 * 128, dummy, we, None) == 1
+    # the gradient output must not alias any input of the VJP
+    a1, a2, a3 = ctypes.c_void_p(16), ctypes.c_void_p(48), ctypes.c_void_p(80)
+    for gp in (a1, a2, a3):  # grad_probe == probe, == grad_sorted, == work
+        assert lib.ptycho_probe_orthogonalize_vjp(a1, a2, gp, 4, 128 * 128, a3, we, None) == 1
+        assert "alias" in _lib.last_error()
     buf = ctypes.create_string_buffer(8)
     assert lib.ptycho_get_last_error(buf, 8) == 0 and len(buf.value) <= 7
 

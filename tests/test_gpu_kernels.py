@@ -268,6 +268,34 @@ def test_status_word_reports_invalid_indices_and_nonfinite(cuda_device):
     assert any("not finite" in str(x.message) for x in w)
 
 
+def test_status_word_saturates_without_reporting_bad_indices(cuda_device):
+    """A NaN object over more than 2^20 predicted pixels (80 positions x 128^2) fills the
+    non-finite field of the status word to its maximum; the count must not carry into
+    the invalid-index field, so check_status warns and does not raise."""
+    import warnings
+
+    from quantem_b200 import ops
+
+    rng = np.random.default_rng(9)
+    S, P, n, Ho, B = 1, 1, 128, 256, 80
+    dev = cuda_device
+    obj = torch.full((S, Ho, Ho), float("nan"), dtype=torch.complex64, device=dev)
+    probe = _t(((rng.standard_normal((P, n, n)) + 1j * rng.standard_normal((P, n, n))) * 0.5).astype(np.complex64),
+               dev)
+    pos = _t(rng.uniform(0, Ho, (B, 2)), dev, torch.float32)
+    tg = _t(np.abs(rng.standard_normal((B, n, n))), dev, torch.float32)
+    ops.read_status(dev)  # start clean
+    ops.batch_forward_adjoint(obj, probe, torch.empty((0, n, n), dtype=torch.complex64, device=dev), pos,
+                              torch.arange(B, device=dev), tg, torch.ones((n, n), device=dev), B, 2.0)
+    st = ops.read_status(dev, reset=False)
+    assert B * n * n > ops.STATUS_NONFINITE_MASK
+    assert st["nonfinite"] == ops.STATUS_NONFINITE_MASK and st["invalid_indices"] == 0
+    with warnings.catch_warnings(record=True):
+        warnings.simplefilter("always")
+        ops.check_status(dev)  # warns, does not raise
+    assert ops.read_status(dev)["raw"] == 0
+
+
 @pytest.mark.parametrize("n", [128, 256])
 @pytest.mark.parametrize("B", [1, 2])
 def test_small_batches_at_the_object_edge(cuda_device, n, B):
