@@ -2,7 +2,7 @@
 
 Run in a container where the reference source tree is mounted:
 
-    python tests/golden/make_golden.py /root/reference/src
+    python tests/golden/make_golden.py <reference checkout>/src
 
 For each seeded case this records the reference's own set-up products
 (targets, mean intensity, scan positions, object shape, initial probe,
@@ -30,6 +30,7 @@ sys.path.insert(0, ROOT)
 
 from oracle import ptycho_oracle as O  # noqa: E402
 from baseline.reference_import import import_reference  # noqa: E402
+from tests.golden.c2small import perturbed_object  # noqa: E402
 
 
 def _c64(x):
@@ -49,7 +50,7 @@ def simulate_data(true_obj, probes, positions_px, props, counts, rng):
 
 
 def run_case(name, *, H, S, P, nscan, step_px, pad, dz, counts, jitter, batch, iters,
-             weights=None, seed=0, opt=None, orthogonalize=True, keep_data=True):
+             weights=None, seed=0, opt=None, orthogonalize=True, keep_data=True, obj_type="complex"):
     import torch
     from quantem.core.datastructures.dataset4dstem import Dataset4dstem
     from quantem.diffractive_imaging.complex_probe import real_space_probe
@@ -86,7 +87,7 @@ def run_case(name, *, H, S, P, nscan, step_px, pad, dz, counts, jitter, batch, i
     pd = PtychographyDatasetRaster.from_dataset4dstem(d4, verbose=0)
     pd.preprocess(com_fit_function="constant", force_com_rotation=0, force_com_transpose=False,
                   plot_rotation=False, plot_com=False, probe_energy=energy)
-    obj_model = ObjectPixelated.from_uniform(num_slices=S, slice_thicknesses=dz, obj_type="complex")
+    obj_model = ObjectPixelated.from_uniform(num_slices=S, slice_thicknesses=dz, obj_type=obj_type)
     probe_model = ProbePixelated.from_params(
         probe_params={"energy": energy, "defocus": 200.0, "semiangle_cutoff": 20.0},
         num_probes=P, rng=seed + 1, initial_probe_weights=weights)
@@ -100,7 +101,7 @@ def run_case(name, *, H, S, P, nscan, step_px, pad, dz, counts, jitter, batch, i
 
     out = dict(
         H=H, S=S, P=P, nscan=nscan, step_px=step_px, pad=pad, dz=dz, px=px, energy=energy,
-        jitter=int(jitter), batch=batch, iters=iters, seed=seed, counts=counts,
+        jitter=int(jitter), batch=batch, iters=iters, seed=seed, counts=counts, obj_type=obj_type,
         weights=np.asarray(weights if weights is not None else [], dtype=np.float64),
         orthogonalize=int(orthogonalize),
         data=data if keep_data else np.zeros(0, np.float32),
@@ -121,10 +122,14 @@ def run_case(name, *, H, S, P, nscan, step_px, pad, dz, counts, jitter, batch, i
     pt.constraints = constraints
     with torch.no_grad():
         shp = tuple(obj_model._obj.shape)
-        amp = 1.0 - 0.3 * rng.random(shp)
-        ph = 0.4 * rng.standard_normal(shp)
-        obj_model._obj.data = torch.tensor(amp * np.exp(1j * ph), dtype=torch.complex64)
-    out["obj_perturbed"] = _c64(obj_model._obj.detach().numpy())
+        if obj_type == "potential":
+            # a real potential with negative values, so that the positivity clamp acts
+            obj_model._obj.data = torch.tensor(0.05 + 0.1 * rng.standard_normal(shp), dtype=torch.float32)
+        else:
+            amp = 1.0 - 0.3 * rng.random(shp)
+            ph = 0.4 * rng.standard_normal(shp)
+            obj_model._obj.data = torch.tensor(amp * np.exp(1j * ph), dtype=torch.complex64)
+    out["obj_perturbed"] = obj_model._obj.detach().numpy().copy()
     bi = np.arange(min(batch, pd.num_gpts))
     obj_model._obj.grad = None
     probe_model._probe.grad = None
@@ -141,12 +146,12 @@ def run_case(name, *, H, S, P, nscan, step_px, pad, dz, counts, jitter, batch, i
         batch_indices=bi,
         batch_intensities=_f32(inten.detach().numpy()),
         batch_loss=np.float64(loss.item()),
-        grad_obj=_c64(obj_model._obj.grad.numpy()),
+        grad_obj=obj_model._obj.grad.numpy().copy(),
         grad_probe=_c64(probe_model._probe.grad.numpy()),
         probe_ortho=_c64(probe_model.probe.detach().numpy()),
     )
 
-    # --- analytic (autograd=False) update directions at the same state ---
+    # --- analytic (autograd=False) update directions at the same state (complex objects) ---
     with torch.no_grad():
         obj_model._obj.grad = None
         probe_model._probe.grad = None
@@ -157,7 +162,7 @@ def run_case(name, *, H, S, P, nscan, step_px, pad, dz, counts, jitter, batch, i
         inten = pt.detector_model.forward(ov)
         loss_an, tg = pt.error_estimate(inten, bi)
         pt.backward(loss_an, False, op, prop, ov, patch_indices, tg)
-    out.update(grad_obj_an=_c64(obj_model._obj.grad.numpy()),
+    out.update(grad_obj_an=obj_model._obj.grad.numpy().copy(),
                grad_probe_an=_c64(probe_model._probe.grad.numpy()))
 
     # --- a few reconstruct iterations from the same state ---
@@ -169,7 +174,7 @@ def run_case(name, *, H, S, P, nscan, step_px, pad, dz, counts, jitter, batch, i
     pt.reconstruct(num_iters=iters, batch_size=batch, optimizer_params=opt,
                    constraints=constraints, device="cpu")
     out.update(
-        recon_obj=_c64(obj_model._obj.detach().numpy()),
+        recon_obj=obj_model._obj.detach().numpy().copy(),
         recon_probe=_c64(probe_model._probe.detach().numpy()),
         recon_losses=np.asarray(pt._iter_losses, dtype=np.float64),
         recon_rng_seed=np.int64(seed + 3),
@@ -177,6 +182,138 @@ def run_case(name, *, H, S, P, nscan, step_px, pad, dz, counts, jitter, batch, i
     path = os.path.join(HERE, f"{name}.npz")
     np.savez_compressed(path, **out)
     print(f"wrote {path}: obj {tuple(pt.obj_shape_full)} N={pd.num_gpts} losses={out['recon_losses']}")
+
+
+def c2small_case(name="c2small", nscan=3, batch=5, iters=3, seed=41):
+    """The headline geometry at a small scan: 8 slices of 20 A, 4 probe modes at 128^2 with
+    mode weights 0.7/0.15/0.1/0.05, a 512^2 object, +-0.5 px jitter, and two windows that
+    wrap around both object edges (positions 1 and 3 moved next to opposite corners).
+    Object-sized arrays are stored on sampled pixels only (flat row-major indices of one
+    slice, the same for every slice): the batch's autograd object gradient on every
+    pixel a window touches plus 4096 random untouched ones (``grad_idx``; off the windows
+    only the constraint's mean-phase term acts), and the object after ``iters`` Adam
+    iterations on 8192 touched plus 4096 untouched pixels (``recon_idx``)."""
+    import torch
+    from quantem.core.datastructures.dataset4dstem import Dataset4dstem
+    from quantem.diffractive_imaging.complex_probe import real_space_probe
+    from quantem.diffractive_imaging.dataset_models import PtychographyDatasetRaster
+    from quantem.diffractive_imaging.detector_models import DetectorPixelated
+    from quantem.diffractive_imaging.object_models import ObjectPixelated
+    from quantem.diffractive_imaging.probe_models import ProbePixelated
+    from quantem.diffractive_imaging.ptychography import Ptychography
+
+    H, S, P, step_px, dz, counts = 128, 8, 4, 6, 20.0, 1e5
+    weights = [0.7, 0.15, 0.1, 0.05]
+    rng = np.random.default_rng(seed)
+    px, energy = 0.2, 300e3
+    rs = 1.0 / (H * px)
+    ext = (nscan - 1) * step_px
+    pad = (512 - ext) // 2
+    obj_hw = ext + 2 * pad
+    assert obj_hw == 512
+    probe1 = real_space_probe(gpts=(H, H), sampling=(px, px), energy=energy, semiangle_cutoff=20.0,
+                              aberration_coefs={"C10": -200.0}).numpy().astype(np.complex128)
+    probes = np.stack([probe1 * np.sqrt(w) * np.exp(2j * np.pi * k * np.arange(H)[None, :] / H)
+                       for k, w in enumerate(weights)])
+    phase = np.stack([O.gaussian_atom_phase((obj_hw, obj_hw), obj_hw * obj_hw // 400, 1.5, 0.1, rng)
+                      for _ in range(S)])
+    true_obj = np.exp(1j * phase)
+    grid = np.stack(np.meshgrid(np.arange(nscan), np.arange(nscan), indexing="ij"), -1).reshape(-1, 2)
+    pos_true = grid * step_px + pad + rng.uniform(-0.5, 0.5, size=(nscan * nscan, 2))
+    props_true = O.propagators((H, H), (px, px), energy, [dz] * (S - 1))
+    data = simulate_data(true_obj, probes, pos_true, props_true, counts, rng)
+
+    d4 = Dataset4dstem.from_array(data.reshape(nscan, nscan, H, H), sampling=(step_px * px, step_px * px, rs, rs),
+                                  units=("A", "A", "A^-1", "A^-1"))
+    pd = PtychographyDatasetRaster.from_dataset4dstem(d4, verbose=0)
+    pd.preprocess(com_fit_function="constant", force_com_rotation=0, force_com_transpose=False,
+                  plot_rotation=False, plot_com=False, probe_energy=energy)
+    obj_model = ObjectPixelated.from_uniform(num_slices=S, slice_thicknesses=dz, obj_type="complex")
+    probe_model = ProbePixelated.from_params(
+        probe_params={"energy": energy, "defocus": 200.0, "semiangle_cutoff": 20.0},
+        num_probes=P, rng=seed + 1, initial_probe_weights=weights)
+    pt = Ptychography.from_models(dset=pd, obj_model=obj_model, probe_model=probe_model,
+                                  detector_model=DetectorPixelated(), device="cpu", verbose=0, rng=seed + 2)
+    pt.preprocess(obj_padding_px=(pad, pad))
+    assert tuple(pt.obj_shape_full) == (S, 512, 512), pt.obj_shape_full
+    jit = rng.uniform(-0.5, 0.5, size=(pd.num_gpts, 2)).astype(np.float32)
+    pos = pd.scan_positions_px.detach().numpy() + jit
+    pos[1] = (3.4, 509.2)    # window wraps the top and right edges
+    pos[3] = (508.6, 4.1)    # window wraps the bottom and left edges
+    pd.scan_positions_px = torch.tensor(pos.astype(np.float32))
+
+    out = dict(
+        H=H, S=S, P=P, nscan=nscan, step_px=step_px, pad=pad, dz=dz, px=px, energy=energy, jitter=1,
+        batch=batch, iters=iters, seed=seed, counts=counts, weights=np.asarray(weights, dtype=np.float64),
+        orthogonalize=1, data=data,
+        targets=_f32(pd.targets.numpy()),
+        mean_intensity=np.float64(pd.mean_diffraction_intensity),
+        positions=_f32(pd.scan_positions_px.detach().numpy()),
+        initial_positions=_f32(pd.initial_scan_positions_px.numpy()),
+        obj_shape=np.asarray(pt.obj_shape_full),
+        obj_padding_px=np.asarray(pt.obj_padding_px),
+        upsample_factor=np.float64(pd.upsample_factor),
+        probe_init=_c64(probe_model._probe.detach().numpy()),
+        propagators=_c64(pt._propagators.numpy()),
+        sampling=np.asarray(pt.sampling, dtype=np.float64),
+    )
+    # windows of every position, one slice (the gradient vanishes elsewhere)
+    origins, _ = O.split_positions(out["positions"].astype(np.float64))
+    rows, cols = O.patch_rows_cols(origins, (H, H), (512, 512))
+    touched = np.unique((rows[:, :, None] * 512 + cols[:, None, :]).ravel()).astype(np.int32)
+    untouched = np.setdiff1d(np.arange(512 * 512, dtype=np.int32), touched)
+    srng = np.random.default_rng(seed + 4)
+    grad_idx = np.sort(np.concatenate([touched, srng.choice(untouched, 4096, replace=False)])).astype(np.int32)
+    recon_idx = np.sort(np.concatenate([srng.choice(touched, 8192, replace=False),
+                                        srng.choice(untouched, 4096, replace=False)])).astype(np.int32)
+    out.update(touched_count=np.int64(touched.size), grad_idx=grad_idx, recon_idx=recon_idx)
+
+    constraints = {"probe": {"orthogonalize_probe": True}}
+    pt.constraints = constraints
+    perturb_seed = seed + 100
+    obj0 = perturbed_object((S, 512, 512), perturb_seed)
+    with torch.no_grad():
+        obj_model._obj.data = torch.tensor(obj0)
+    out["perturb_seed"] = np.int64(perturb_seed)
+    out["obj_perturbed_abs_sum"] = np.float64(np.abs(obj0.astype(np.complex128)).sum())
+    bi = np.arange(batch)
+    obj_model._obj.grad = None
+    probe_model._probe.grad = None
+    pt.dset._set_targets("l2_amplitude")
+    pt.compute_propagator_arrays()
+    patch_indices, _pos, frac, descan = pt.dset.forward(bi, pt.obj_padding_px)
+    sp = probe_model.forward(frac)
+    op = obj_model.forward(patch_indices)
+    prop, ov = pt.forward_operator(op, sp, descan)
+    inten = pt.detector_model.forward(ov)
+    loss, tg = pt.error_estimate(inten, bi)
+    pt.backward(loss, True, op, prop, ov, patch_indices, tg)
+    g_obj = obj_model._obj.grad.numpy().reshape(S, -1)
+    out.update(
+        batch_indices=bi,
+        batch_intensities=_f32(inten.detach().numpy()),
+        batch_loss=np.float64(loss.item()),
+        grad_obj_sampled=_c64(g_obj[:, grad_idx]),
+        grad_probe=_c64(probe_model._probe.grad.numpy()),
+        probe_ortho=_c64(probe_model.probe.detach().numpy()),
+    )
+    with torch.no_grad():
+        obj_model._obj.grad = None
+        probe_model._probe.grad = None
+    pt.rng = seed + 3
+    pt.reconstruct(num_iters=iters, batch_size=batch, optimizer_params={"object": {"type": "adam"},
+                                                                         "probe": {"type": "adam"}},
+                   constraints=constraints, device="cpu")
+    rec = obj_model._obj.detach().numpy().reshape(S, -1)
+    out.update(
+        recon_obj_sampled=_c64(rec[:, recon_idx]),
+        recon_probe=_c64(probe_model._probe.detach().numpy()),
+        recon_losses=np.asarray(pt._iter_losses, dtype=np.float64),
+        recon_rng_seed=np.int64(seed + 3),
+    )
+    path = os.path.join(HERE, f"{name}.npz")
+    np.savez_compressed(path, **out)
+    print(f"wrote {path}: N={pd.num_gpts} touched={touched.size} losses={out['recon_losses']}")
 
 
 def whitenoise_case():
@@ -237,6 +374,12 @@ def main(src):
     if os.environ.get("GOLDEN_ONLY") == "whitenoise":
         whitenoise_case()
         return
+    if os.environ.get("GOLDEN_ONLY") == "c2small":
+        c2small_case()
+        return
+    if os.environ.get("GOLDEN_ONLY") == "objtypes":
+        objtype_cases()
+        return
     run_case("single64", H=64, S=1, P=1, nscan=6, step_px=4, pad=32, dz=20.0, counts=1e5,
              jitter=False, batch=12, iters=3, seed=11)
     run_case("mixed64", H=64, S=3, P=3, nscan=5, step_px=6, pad=32, dz=20.0, counts=1e5,
@@ -245,7 +388,20 @@ def main(src):
              jitter=True, batch=9, iters=2, weights=[0.7, 0.15, 0.1, 0.05], seed=31,
              keep_data=False)
     whitenoise_case()
+    c2small_case()
+    objtype_cases()
+
+
+def objtype_cases():
+    """The pure-phase and potential object types (object_models.py:87, 123-136,
+    289-339, 252-256) at the mixed64 geometry, default constraints (positivity on)."""
+    run_case("purephase64", H=64, S=2, P=2, nscan=5, step_px=6, pad=32, dz=20.0, counts=1e5,
+             jitter=True, batch=10, iters=2, weights=[0.8, 0.2], seed=51, obj_type="pure_phase")
+    run_case("potential64", H=64, S=2, P=2, nscan=5, step_px=6, pad=32, dz=20.0, counts=1e5,
+             jitter=True, batch=10, iters=2, weights=[0.8, 0.2], seed=61, obj_type="potential")
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src")
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {os.path.relpath(__file__)} <reference source dir (the one holding quantem/)>")
+    main(sys.argv[1])

@@ -32,7 +32,7 @@ def build_from_golden(z, device="cpu"):
     return pt
 
 
-@pytest.mark.parametrize("case", ["single64", "mixed64"])
+@pytest.mark.parametrize("case", ["single64", "mixed64", "c2small"])
 def test_setup_matches_reference(case):
     z = load_golden(case)
     pt = build_from_golden(z)
@@ -76,8 +76,8 @@ def test_gram_schmidt_matches_oracle():
 def test_unsupported_options_raise():
     from quantem_b200.diffractive_imaging import ObjectPixelated
 
-    with pytest.raises(NotImplementedError):
-        ObjectPixelated.from_uniform(num_slices=1, obj_type="potential")
+    with pytest.raises(ValueError, match="Object type"):
+        ObjectPixelated.from_uniform(num_slices=1, obj_type="absorption")
     o = ObjectPixelated.from_uniform(num_slices=1)
     with pytest.raises(NotImplementedError):
         o.add_constraint("tv_weight_xy", 0.1)

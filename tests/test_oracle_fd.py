@@ -1,0 +1,90 @@
+"""FP64 central finite differences of the oracle's batch loss against its adjoint.
+
+The loss is a function of the raw object (through the hard constraint, with its
+mean-phase term) and of the raw probe modes (through Gram-Schmidt and the intensity
+sort).  For random complex directions d the directional derivative
+dL/dt (x + t d) at t = 0 equals Re<g, d> for a gradient g in torch's convention
+(dL/dRe + i dL/dIm).  In FP64 a central difference with t ~ 1e-6 of the parameter
+scale agrees with it to ~1e-8 relative (truncation ~t^2, rounding ~1e-16 / t).
+
+The check is made at the fixtures' start object with its amplitude scaled by 0.999:
+the hard constraint clamps |o| to 1, and the start objects (amplitude 1 - 0.3 U[0,1))
+hold a few pixels within 1e-6 of that kink, where a difference quotient straddles two
+branches (measured: up to 1.5e-3 relative at t = 1e-6 on the unscaled c2small start)."""
+import numpy as np
+import pytest
+
+from oracle import ptycho_oracle as O
+from tests.conftest import load_golden
+
+
+def _loss(z, obj_raw, probe_raw):
+    bi = z["batch_indices"]
+    H = int(z["H"])
+    S = int(z["S"])
+    props = z["propagators"].astype(np.complex128) if S > 1 else np.zeros((0, H, H))
+    obj_c = O.constrain_object(obj_raw)
+    probe_o = O.gram_schmidt(probe_raw)[0] if int(z["orthogonalize"]) else probe_raw
+    st = O.forward(obj_c, probe_o, z["positions"].astype(np.float64)[bi], props)
+    loss, _ = O.loss_and_seed(st.intensity, z["targets"].astype(np.float64)[bi], np.ones((H, H)),
+                              z["positions"].shape[0], float(z["mean_intensity"]))
+    return loss
+
+
+def _grads(z, obj_raw, probe_raw):
+    bi = z["batch_indices"]
+    H = int(z["H"])
+    S = int(z["S"])
+    props = z["propagators"].astype(np.complex128) if S > 1 else np.zeros((0, H, H))
+    loss, g_obj, g_probe, _ = O.full_gradients(
+        obj_raw, probe_raw, z["positions"].astype(np.float64)[bi], props, z["targets"].astype(np.float64)[bi],
+        np.ones((H, H)), z["positions"].shape[0], float(z["mean_intensity"]), 1.0,
+        orthogonalize=bool(int(z["orthogonalize"])))
+    return loss, g_obj * 2.0, g_probe  # undo the upsample_factor^2 / 2 rescale (factor 1 here)
+
+
+def fd_directional(z, obj_raw, probe_raw, d_obj, d_probe, t):
+    """Central difference of the loss along (d_obj, d_probe)."""
+    lp = _loss(z, obj_raw + t * d_obj, probe_raw + t * d_probe)
+    lm = _loss(z, obj_raw - t * d_obj, probe_raw - t * d_probe)
+    return (lp - lm) / (2 * t)
+
+
+def random_directions(rng, obj_raw, probe_raw, which):
+    """Unit-scale complex directions (scaled to the parameters' RMS) for the object, the
+    probe, or both."""
+    def rnd(x):
+        d = rng.standard_normal(x.shape) + 1j * rng.standard_normal(x.shape)
+        return d * (np.sqrt(np.mean(np.abs(x) ** 2)) / np.sqrt(np.mean(np.abs(d) ** 2)))
+
+    d_obj = rnd(obj_raw) if which in ("obj", "both") else np.zeros_like(obj_raw)
+    d_probe = rnd(probe_raw) if which in ("probe", "both") else np.zeros_like(probe_raw)
+    return d_obj, d_probe
+
+
+def _inner(g, d):
+    return float(np.sum(g.real * d.real + g.imag * d.imag))
+
+
+@pytest.mark.parametrize("case", ["single64", "mixed64", "c2small"])
+@pytest.mark.parametrize("which", ["obj", "probe", "both"])
+def test_oracle_adjoint_matches_fp64_finite_differences(case, which):
+    if case == "c2small":
+        from tests.golden.c2small import load_c2small
+
+        z = load_c2small()
+    else:
+        z = load_golden(case)
+    obj_raw = z["obj_perturbed"].astype(np.complex128) * 0.999  # away from the |o| = 1 clamp
+    probe_raw = z["probe_init"].astype(np.complex128)
+    _, g_obj, g_probe = _grads(z, obj_raw, probe_raw)
+    loss = _loss(z, obj_raw, probe_raw)
+    t = 1e-6
+    rng = np.random.default_rng(hash((case, which)) % 2**32)
+    for _ in range(2):
+        d_obj, d_probe = random_directions(rng, obj_raw, probe_raw, which)
+        adj = _inner(g_obj, d_obj) + _inner(g_probe, d_probe)
+        fd = fd_directional(z, obj_raw, probe_raw, d_obj, d_probe, t)
+        # 1e-7 relative plus the difference quotient's own rounding floor, eps |L| / t
+        # (random directions in ~10^5 dimensions cancel much of <g, d>)
+        assert abs(fd - adj) <= 1e-7 * abs(adj) + 4 * np.finfo(np.float64).eps * abs(loss) / t, (fd, adj)

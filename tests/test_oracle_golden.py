@@ -7,7 +7,15 @@ from oracle import ptycho_oracle as O
 from tests.conftest import load_golden, rel
 
 
-@pytest.mark.parametrize("case", ["single64", "mixed64", "mixed128"])
+def obj_type_of(z):
+    return str(z["obj_type"]) if "obj_type" in z else "complex"
+
+
+def fp64(x):
+    return x.astype(np.complex128) if np.iscomplexobj(x) else x.astype(np.float64)
+
+
+@pytest.mark.parametrize("case", ["single64", "mixed64", "mixed128", "purephase64", "potential64"])
 def test_oracle_matches_reference_batch(case):
     z = load_golden(case)
     S = int(z["S"])
@@ -16,9 +24,9 @@ def test_oracle_matches_reference_batch(case):
     pos = z["positions"].astype(np.float64)[bi]
     mask = np.ones(z["targets"].shape[1:])
     loss, g_obj, g_probe, st = O.full_gradients(
-        z["obj_perturbed"].astype(np.complex128), z["probe_init"].astype(np.complex128), pos, props,
+        fp64(z["obj_perturbed"]), z["probe_init"].astype(np.complex128), pos, props,
         z["targets"].astype(np.float64)[bi], mask, z["positions"].shape[0], float(z["mean_intensity"]),
-        float(z["upsample_factor"]), orthogonalize=bool(z["orthogonalize"]))
+        float(z["upsample_factor"]), orthogonalize=bool(z["orthogonalize"]), obj_type=obj_type_of(z))
     assert rel(O.detector_intensities(st), z["batch_intensities"]) < 2e-6
     assert abs(loss - float(z["batch_loss"])) / float(z["batch_loss"]) < 2e-6
     assert rel(g_obj, z["grad_obj"]) < 5e-6
@@ -100,3 +108,39 @@ def test_oracle_loss_types_match_reference(loss_type):
                                     int(z["num_gpts"]), float(z["mean_intensity"]), loss_type)
     assert abs(loss - float(z[f"{loss_type}_loss"])) <= 1e-12 * abs(float(z[f"{loss_type}_loss"]))
     assert rel(np.fft.fftshift(dldi_cc, axes=(-2, -1)), z[f"{loss_type}_dldi"]) < 1e-12
+
+
+def test_oracle_matches_reference_c2small():
+    """The headline geometry (8 slices, 4 modes with weights 0.7/0.15/0.1/0.05 at 128^2,
+    512^2 object, two windows wrapping both edges): the reference's batch intensities,
+    loss and autograd gradients (object gradient on the sampled pixels)."""
+    from tests.golden.c2small import load_c2small, sampled
+
+    z = load_c2small()
+    bi = z["batch_indices"]
+    H = int(z["H"])
+    loss, g_obj, g_probe, st = O.full_gradients(
+        z["obj_perturbed"].astype(np.complex128), z["probe_init"].astype(np.complex128),
+        z["positions"].astype(np.float64)[bi], z["propagators"].astype(np.complex128),
+        z["targets"].astype(np.float64)[bi], np.ones((H, H)), z["positions"].shape[0], float(z["mean_intensity"]),
+        float(z["upsample_factor"]), orthogonalize=True)
+    assert rel(O.detector_intensities(st), z["batch_intensities"]) < 2e-6
+    assert abs(loss - float(z["batch_loss"])) / float(z["batch_loss"]) < 2e-6
+    assert rel(sampled(g_obj, z["grad_idx"]), z["grad_obj_sampled"]) < 5e-6
+    assert rel(g_probe, z["grad_probe"]) < 5e-6
+
+
+@pytest.mark.parametrize("case", ["purephase64", "potential64"])
+def test_oracle_reconstruct_matches_reference_object_types(case):
+    """Two Adam iterations of the reference's reconstruct for pure-phase and potential
+    objects: loss trajectory and final parameters against the FP64 oracle."""
+    z = load_golden(case)
+    H = int(z["H"])
+    obj, probe, losses = O.reconstruct(fp64(z["obj_perturbed"]), z["probe_init"].astype(np.complex128),
+                                       z["positions"].astype(np.float64), z["propagators"].astype(np.complex128),
+                                       z["targets"].astype(np.float64), np.ones((H, H)), float(z["mean_intensity"]),
+                                       float(z["upsample_factor"]), int(z["iters"]), int(z["batch"]),
+                                       np.random.default_rng(int(z["recon_rng_seed"])), obj_type=obj_type_of(z))
+    np.testing.assert_allclose(losses, z["recon_losses"], rtol=2e-6)
+    assert rel(obj, z["recon_obj"]) < 1e-5
+    assert rel(probe, z["recon_probe"]) < 1e-5
