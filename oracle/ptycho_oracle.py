@@ -182,6 +182,55 @@ def constrain_object_vjp(obj: np.ndarray, grad_out: np.ndarray) -> np.ndarray:
     return (g_mag * sgn + g_ph * dang).astype(obj.dtype)
 
 
+def object_transmission(obj: np.ndarray, obj_type: str = "complex", positivity: bool = True,
+                        fix_baseline: bool = False, baseline_factor: float = 1.0) -> np.ndarray:
+    """Transmission multiplied into the wave, for every object type:
+    apply_hard_constraints (object_models.py:289-339, no FOV mask) followed by the
+    exp(i V) of _get_obj_patches for real potentials (object_models.py:252-256).
+
+    complex: ``constrain_object``; pure_phase: exp(i (angle(o) - mean angle));
+    potential: V' = V - offset (offset = factor * min V when the baseline is fixed),
+    clamped at 0 with positivity, transmission exp(i V')."""
+    if obj_type == "complex":
+        return constrain_object(obj)
+    if obj_type == "pure_phase":
+        ph = np.angle(obj)
+        return np.exp(1j * (ph - ph.mean())).astype(obj.dtype)
+    if obj_type == "potential":
+        v = obj - (obj.min() * baseline_factor if fix_baseline else 0.0)
+        if positivity:
+            v = np.maximum(v, 0.0)
+        cdt = np.complex128 if obj.dtype == np.float64 else np.complex64
+        return np.exp(1j * v).astype(cdt)
+    raise ValueError(obj_type)
+
+
+def object_transmission_vjp(obj: np.ndarray, grad_t: np.ndarray, obj_type: str = "complex",
+                            positivity: bool = True, fix_baseline: bool = False,
+                            baseline_factor: float = 1.0) -> np.ndarray:
+    """VJP of ``object_transmission`` w.r.t. the raw object (torch convention).
+
+    pure_phase: the amplitude does not enter, g = g_phi * i o / |o|^2 with g_phi the
+    mean-removed Im(G conj(e)); potential: dL/dV = Re(conj(G) i t) where the clamp
+    passes (V - offset >= 0, inclusive like torch.clamp) -- the offset is detached."""
+    if obj_type == "complex":
+        return constrain_object_vjp(obj, grad_t)
+    if obj_type == "pure_phase":
+        mag = np.abs(obj)
+        th = np.angle(obj) - np.angle(obj).mean()
+        g_th = (grad_t * np.exp(-1j * th)).imag
+        g_ph = g_th - g_th.mean()
+        safe = np.where(mag == 0, 1.0, mag)
+        dang = np.where(mag == 0, 0.0, 1j * obj / safe**2)
+        return (g_ph * dang).astype(obj.dtype)
+    if obj_type == "potential":
+        v = obj - (obj.min() * baseline_factor if fix_baseline else 0.0)
+        passes = (v >= 0.0) if positivity else np.ones(v.shape, bool)
+        t = np.exp(1j * (np.maximum(v, 0.0) if positivity else v))
+        return np.where(passes, (np.conj(grad_t) * 1j * t).real, 0.0).astype(obj.dtype)
+    raise ValueError(obj_type)
+
+
 def gram_schmidt(probe: np.ndarray):
     """Mixed-state probe orthogonalisation + intensity sort; probe_models.py:484-525.
 
@@ -358,18 +407,19 @@ def batch_loss_and_grads(obj_c, probe_o, positions_px, props, targets, mask, num
 
 def full_gradients(obj_raw, probe_raw, positions_px, props, targets, mask, num_gpts,
                    mean_intensity, upsample_factor, orthogonalize=True,
-                   loss_type="l2_amplitude"):
+                   loss_type="l2_amplitude", obj_type="complex"):
     """Loss and gradients w.r.t. the raw parameters, as Ptychography.backward
     leaves them (autograd branch, ptychography.py:326-332): the object gradient
-    is scaled by upsample_factor**2 / 2."""
-    obj_c = constrain_object(obj_raw)
+    is scaled by upsample_factor**2 / 2.  ``obj_type``: complex, pure_phase or
+    potential (default constraints: positivity on, baseline not fixed)."""
+    obj_c = object_transmission(obj_raw, obj_type)
     if orthogonalize:
         probe_o, _, cache = gram_schmidt(probe_raw)
     else:
         probe_o, cache = probe_raw, None
     loss, g_obj_c, g_probe_o, st = batch_loss_and_grads(
         obj_c, probe_o, positions_px, props, targets, mask, num_gpts, mean_intensity, loss_type)
-    g_obj = constrain_object_vjp(obj_raw, g_obj_c) * (upsample_factor**2 / 2)
+    g_obj = object_transmission_vjp(obj_raw, g_obj_c, obj_type) * (upsample_factor**2 / 2)
     g_probe = gram_schmidt_vjp(cache, g_probe_o) if orthogonalize else g_probe_o
     return loss, g_obj, g_probe, st
 
@@ -451,7 +501,7 @@ def gaussian_atom_phase(shape, n_atoms, sigma_px, peak_rad, rng):
 
 def reconstruct(obj_raw, probe_raw, positions_px, props, targets, mask, mean_intensity, upsample_factor,
                 num_iters, batch_size, rng, lr_obj=5e-3, lr_probe=1e-3, orthogonalize=True,
-                loss_type="l2_amplitude"):
+                loss_type="l2_amplitude", obj_type="complex"):
     """Adam iterations of Ptychography.reconstruct (ptychography.py:208-245) on
     the given state; batches from a numpy generator like SimpleBatcher.
     Returns (obj, probe, per-iteration mean batch losses)."""
@@ -464,7 +514,8 @@ def reconstruct(obj_raw, probe_raw, positions_px, props, targets, mask, mean_int
         tot, nb = 0.0, 0
         for bi in batch_order(rng, npos, batch_size):
             loss, g_obj, g_probe, _ = full_gradients(obj, probe, positions_px[bi], props, targets[bi], mask, npos,
-                                                     mean_intensity, upsample_factor, orthogonalize, loss_type)
+                                                     mean_intensity, upsample_factor, orthogonalize, loss_type,
+                                                     obj_type)
             adam_step(obj, g_obj, so, lr_obj)
             adam_step(probe, g_probe, sp, lr_probe)
             tot += loss

@@ -40,6 +40,8 @@ EXPORTED = (
     "ptycho_reduce_loss",
     "ptycho_obj_constrain",
     "ptycho_obj_constrain_vjp",
+    "ptycho_obj_transmission",
+    "ptycho_obj_transmission_vjp",
     "ptycho_reduce_blocks",
     "ptycho_adam_step",
     "ptycho_sgd_step",
@@ -116,6 +118,8 @@ def _declare(lib):
         "ptycho_reduce_loss": (_int, [_vp, _int, _vp, _vp]),
         "ptycho_obj_constrain": (_int, [_vp, _vp, _i64, _vp, _int, _vp]),
         "ptycho_obj_constrain_vjp": (_int, [_vp, _vp, _vp, _i64, _vp, _int, _vp, _vp]),
+        "ptycho_obj_transmission": (_int, [_vp, _vp, _i64, _int, _int, _int, _flt, _vp, _int, _vp]),
+        "ptycho_obj_transmission_vjp": (_int, [_vp, _vp, _vp, _i64, _int, _int, _int, _flt, _vp, _int, _vp, _vp]),
         "ptycho_reduce_blocks": (_int, []),
         "ptycho_adam_step": (_int, [_vp, _vp, _vp, _vp, _i64, _flt, _vp, _flt, _flt, _flt, _flt, _int, _flt, _flt,
                                     _vp]),

@@ -70,6 +70,8 @@ __global__ void angle_sum_kernel(const float2* __restrict__ obj, int64_t n, doub
   if (threadIdx.x == 0) part[blockIdx.x] = t;
 }
 
+// PURE: pure-phase objects (amplitude fixed at 1, object_models.py:292-298)
+template <bool PURE>
 __global__ void constrain_apply_kernel(const float2* __restrict__ obj, float2* __restrict__ out, int64_t n,
                                        const double* part, int nparts) {
   __shared__ double red[32];
@@ -77,7 +79,7 @@ __global__ void constrain_apply_kernel(const float2* __restrict__ obj, float2* _
   const float mean = (float)(sum_partials(part, nparts, red, &bc) / (double)n);
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const float2 o = obj[i];
-    const float amp = fminf(fmaxf(hypotf(o.x, o.y), 0.0f), 1.0f);
+    const float amp = PURE ? 1.0f : fminf(fmaxf(hypotf(o.x, o.y), 0.0f), 1.0f);
     const float ph = atan2f(o.y, o.x) - mean;
     float s, c;
     sincosf(ph, &s, &c);
@@ -86,6 +88,7 @@ __global__ void constrain_apply_kernel(const float2* __restrict__ obj, float2* _
 }
 
 // g_theta = clamp(|o|) * Im(G conj(e^{i theta})) summed over the object
+template <bool PURE>
 __global__ void vjp_sum_kernel(const float2* __restrict__ obj, const float2* __restrict__ gc, int64_t n,
                                const double* part_fwd, int nparts, double* part) {
   __shared__ double red[32];
@@ -94,7 +97,7 @@ __global__ void vjp_sum_kernel(const float2* __restrict__ obj, const float2* __r
   double v = 0.0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const float2 o = obj[i], g = gc[i];
-    const float amp = fminf(fmaxf(hypotf(o.x, o.y), 0.0f), 1.0f);
+    const float amp = PURE ? 1.0f : fminf(fmaxf(hypotf(o.x, o.y), 0.0f), 1.0f);
     float s, c;
     sincosf(atan2f(o.y, o.x) - mean, &s, &c);
     v += (double)(amp * (g.y * c - g.x * s));
@@ -103,6 +106,7 @@ __global__ void vjp_sum_kernel(const float2* __restrict__ obj, const float2* __r
   if (threadIdx.x == 0) part[blockIdx.x] = t;
 }
 
+template <bool PURE>
 __global__ void vjp_apply_kernel(const float2* __restrict__ obj, const float2* __restrict__ gc,
                                  float2* __restrict__ gout, int64_t n, const double* part_fwd,
                                  const double* part_g, int nparts, const float* scale) {
@@ -115,13 +119,14 @@ __global__ void vjp_apply_kernel(const float2* __restrict__ obj, const float2* _
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const float2 o = obj[i], g = gc[i];
     const float mag = hypotf(o.x, o.y);
-    const float amp = fminf(fmaxf(mag, 0.0f), 1.0f);
+    const float amp = PURE ? 1.0f : fminf(fmaxf(mag, 0.0f), 1.0f);
     float s, c;
     sincosf(atan2f(o.y, o.x) - mean, &s, &c);
     const float g_amp = g.x * c + g.y * s;            // Re(G conj(e))
     const float g_th = amp * (g.y * c - g.x * s);      // amp * Im(G conj(e))
     const float g_ph = g_th - gmean;
-    const float g_mag = (mag >= 0.0f && mag <= 1.0f) ? g_amp : 0.0f;
+    // the amplitude of a pure-phase object does not enter its transmission
+    const float g_mag = (!PURE && mag >= 0.0f && mag <= 1.0f) ? g_amp : 0.0f;
     float2 r = make_float2(0.f, 0.f);
     if (mag != 0.0f) {
       const float inv = 1.0f / mag;
@@ -130,6 +135,68 @@ __global__ void vjp_apply_kernel(const float2* __restrict__ obj, const float2* _
       r.y = g_mag * o.y * inv + g_ph * o.x * inv * inv;
     }
     gout[i] = make_float2(r.x * sc, r.y * sc);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// potential objects (object_models.py:301-320, 252-256): V' = V - offset, clamped
+// at 0 with positivity; transmission t = exp(i V').  The baseline offset (when
+// fixed) is factor * min(V), detached from the gradient as in the reference.
+// ---------------------------------------------------------------------------
+__global__ void potential_min_kernel(const float* __restrict__ v, int64_t n, double* part) {
+  __shared__ float red[32];
+  float m = INFINITY;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    m = fminf(m, v[i]);
+  for (int o = 16; o > 0; o >>= 1) m = fminf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) red[w] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int i = 1; i < (int)(blockDim.x >> 5); ++i) m = fminf(m, red[i]);
+    part[blockIdx.x] = (double)fminf(m, red[0]);
+  }
+}
+
+// offset of the potential: factor * min over the per-block minima (0 when not fixed)
+__device__ __forceinline__ float potential_offset(const double* part, int nparts, float factor) {
+  if (!part) return 0.0f;
+  __shared__ float bc;
+  if (threadIdx.x == 0) {
+    double m = part[0];
+    for (int i = 1; i < nparts; ++i) m = fmin(m, part[i]);
+    bc = (float)m * factor;
+  }
+  __syncthreads();
+  return bc;
+}
+
+__global__ void potential_apply_kernel(const float* __restrict__ v, float2* __restrict__ out, int64_t n,
+                                       int positivity, const double* part, int nparts, float factor) {
+  const float off = potential_offset(part, nparts, factor);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    float x = v[i] - off;
+    if (positivity) x = fmaxf(x, 0.0f);
+    float s, c;
+    sincosf(x, &s, &c);
+    out[i] = make_float2(c, s);
+  }
+}
+
+// dL/dV = Re(conj(G) i t) where the clamp passes (V - offset >= 0, as torch.clamp's gradient)
+__global__ void potential_vjp_kernel(const float* __restrict__ v, const float2* __restrict__ gc,
+                                     float* __restrict__ gout, int64_t n, int positivity, const double* part,
+                                     int nparts, float factor, const float* scale) {
+  const float off = potential_offset(part, nparts, factor);
+  const float sc = scale ? *scale : 1.0f;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    float x = v[i] - off;
+    const bool pass = !positivity || x >= 0.0f;
+    if (positivity) x = fmaxf(x, 0.0f);
+    float s, c;
+    sincosf(x, &s, &c);
+    const float2 g = gc[i];
+    gout[i] = pass ? sc * (g.y * c - g.x * s) : 0.0f;
   }
 }
 
@@ -575,8 +642,8 @@ int ptycho_obj_constrain(const void* obj, void* out, int64_t count, double* work
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const float2* o = static_cast<const float2*>(obj);
   angle_sum_kernel<<<kReduceBlocks, kReduceThreads, 0, st>>>(o, count, work);
-  constrain_apply_kernel<<<kReduceBlocks, kReduceThreads, 0, st>>>(o, static_cast<float2*>(out), count, work,
-                                                                   kReduceBlocks);
+  constrain_apply_kernel<false><<<kReduceBlocks, kReduceThreads, 0, st>>>(o, static_cast<float2*>(out), count, work,
+                                                                          kReduceBlocks);
   return check_launch("obj_constrain");
 }
 
@@ -588,10 +655,71 @@ int ptycho_obj_constrain_vjp(const void* obj, const void* grad_c, void* grad_raw
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const float2* o = static_cast<const float2*>(obj);
   const float2* g = static_cast<const float2*>(grad_c);
-  vjp_sum_kernel<<<kReduceBlocks, kReduceThreads, 0, st>>>(o, g, count, work, kReduceBlocks, work + kReduceBlocks);
-  vjp_apply_kernel<<<kReduceBlocks, kReduceThreads, 0, st>>>(o, g, static_cast<float2*>(grad_raw), count, work,
-                                                             work + kReduceBlocks, kReduceBlocks, scale);
+  vjp_sum_kernel<false><<<kReduceBlocks, kReduceThreads, 0, st>>>(o, g, count, work, kReduceBlocks,
+                                                                   work + kReduceBlocks);
+  vjp_apply_kernel<false><<<kReduceBlocks, kReduceThreads, 0, st>>>(o, g, static_cast<float2*>(grad_raw), count, work,
+                                                                    work + kReduceBlocks, kReduceBlocks, scale);
   return check_launch("obj_constrain_vjp");
+}
+
+int ptycho_obj_transmission(const void* obj, void* out, int64_t count, int obj_type, int positivity,
+                            int fix_baseline, float baseline_factor, double* work, int nwork, void* stream) {
+  if (!obj || !out || !work || count < 1) return fail(PTYCHO_ERR_INVALID, "obj_transmission: bad arguments");
+  if (nwork < 2 * kReduceBlocks) return fail(PTYCHO_ERR_INVALID, "obj_transmission: work too small (%d)", nwork);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  switch (obj_type) {
+    case PTYCHO_OBJ_COMPLEX:
+      return ptycho_obj_constrain(obj, out, count, work, nwork, stream);
+    case PTYCHO_OBJ_PURE_PHASE: {
+      const float2* o = static_cast<const float2*>(obj);
+      angle_sum_kernel<<<kReduceBlocks, kReduceThreads, 0, st>>>(o, count, work);
+      constrain_apply_kernel<true><<<kReduceBlocks, kReduceThreads, 0, st>>>(o, static_cast<float2*>(out), count,
+                                                                             work, kReduceBlocks);
+      return check_launch("obj_transmission (pure phase)");
+    }
+    case PTYCHO_OBJ_POTENTIAL: {
+      const float* v = static_cast<const float*>(obj);
+      if (fix_baseline) potential_min_kernel<<<kReduceBlocks, kReduceThreads, 0, st>>>(v, count, work);
+      potential_apply_kernel<<<kReduceBlocks, kReduceThreads, 0, st>>>(
+          v, static_cast<float2*>(out), count, positivity, fix_baseline ? work : nullptr, kReduceBlocks,
+          baseline_factor);
+      return check_launch("obj_transmission (potential)");
+    }
+    default:
+      return fail(PTYCHO_ERR_INVALID, "obj_transmission: unknown object type %d", obj_type);
+  }
+}
+
+int ptycho_obj_transmission_vjp(const void* obj, const void* grad_t, void* grad_raw, int64_t count, int obj_type,
+                                int positivity, int fix_baseline, float baseline_factor, double* work, int nwork,
+                                const float* scale, void* stream) {
+  if (!obj || !grad_t || !grad_raw || !work || count < 1)
+    return fail(PTYCHO_ERR_INVALID, "obj_transmission_vjp: bad arguments");
+  if (nwork < 2 * kReduceBlocks) return fail(PTYCHO_ERR_INVALID, "obj_transmission_vjp: work too small");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const float2* g = static_cast<const float2*>(grad_t);
+  switch (obj_type) {
+    case PTYCHO_OBJ_COMPLEX:
+      return ptycho_obj_constrain_vjp(obj, grad_t, grad_raw, count, work, nwork, scale, stream);
+    case PTYCHO_OBJ_PURE_PHASE: {
+      const float2* o = static_cast<const float2*>(obj);
+      vjp_sum_kernel<true><<<kReduceBlocks, kReduceThreads, 0, st>>>(o, g, count, work, kReduceBlocks,
+                                                                     work + kReduceBlocks);
+      vjp_apply_kernel<true><<<kReduceBlocks, kReduceThreads, 0, st>>>(o, g, static_cast<float2*>(grad_raw), count,
+                                                                       work, work + kReduceBlocks, kReduceBlocks,
+                                                                       scale);
+      return check_launch("obj_transmission_vjp (pure phase)");
+    }
+    case PTYCHO_OBJ_POTENTIAL: {
+      // `work` holds the per-block minima of the matching forward call when the baseline is fixed
+      potential_vjp_kernel<<<kReduceBlocks, kReduceThreads, 0, st>>>(
+          static_cast<const float*>(obj), g, static_cast<float*>(grad_raw), count, positivity,
+          fix_baseline ? work : nullptr, kReduceBlocks, baseline_factor, scale);
+      return check_launch("obj_transmission_vjp (potential)");
+    }
+    default:
+      return fail(PTYCHO_ERR_INVALID, "obj_transmission_vjp: unknown object type %d", obj_type);
+  }
 }
 
 int ptycho_adam_step(float* param, const float* grad, float* exp_avg, float* exp_avg_sq, int64_t count, float lr,

@@ -25,8 +25,10 @@ class ObjectPixelated(OptimizerMixin):
         "q_highpass": None,
     }
     # constraints whose non-default values need operations outside the B200 path
+    # (fix_potential_baseline: the reference takes the baseline from the background of the
+    # probe-overlap FOV mask its preprocess builds, which this path does not build)
     _UNSUPPORTED = ("identical_slices", "apply_fov_mask", "tv_weight_z", "tv_weight_xy", "surface_zero_weight",
-                    "gaussian_sigma", "q_lowpass", "q_highpass")
+                    "gaussian_sigma", "q_lowpass", "q_highpass", "fix_potential_baseline")
     _token = object()
 
     def __init__(self, num_slices=1, slice_thicknesses=None, obj_type="complex", initialize_mode="uniform",
@@ -34,13 +36,10 @@ class ObjectPixelated(OptimizerMixin):
         if _token is not self._token:
             raise RuntimeError("Use a factory method to instantiate this class.")
         OptimizerMixin.__init__(self)
-        t = str(obj_type).lower()
-        if t != "complex":
-            raise NotImplementedError(f"obj_type {obj_type!r}: the B200 path implements complex objects")
-        self._obj_type = "complex"
+        self._obj_type = self._process_obj_type(obj_type)
         self._device = config.validate_device(device)[0]
         self._initialize_mode = initialize_mode
-        self._obj = torch.ones(num_slices, 1, 1, dtype=torch.complex64)
+        self._obj = torch.ones(num_slices, 1, 1, dtype=self.dtype)
         self._initial_obj = None
         self.slice_thicknesses = slice_thicknesses
         self._constraints = dict(self.DEFAULT_CONSTRAINTS)
@@ -60,10 +59,24 @@ class ObjectPixelated(OptimizerMixin):
 
     @classmethod
     def from_array(cls, initial_obj, slice_thicknesses=None, device="cpu", obj_type="complex", rng=None):
-        arr = torch.as_tensor(initial_obj).to(torch.complex64)
+        arr = torch.as_tensor(initial_obj)
         m = cls(arr.shape[0], slice_thicknesses, obj_type, "array", device, rng, _token=cls._token)
-        m._initial_obj = arr
+        if m.obj_type == "potential" and arr.is_complex():
+            raise TypeError("a potential object is real: pass a real initial_obj")
+        m._initial_obj = arr.to(m.dtype)
         return m
+
+    @staticmethod
+    def _process_obj_type(obj_type) -> str:
+        """object_models.py:123-136 (same spellings accepted)."""
+        t = str(obj_type).lower()
+        if t in ("potential", "potentials"):
+            return "potential"
+        if t in ("pure_phase", "purephase", "pure phase"):
+            return "pure_phase"
+        if t == "complex":
+            return "complex"
+        raise ValueError(f"Object type should be 'potential', 'complex', or 'pure_phase', got {obj_type}")
 
     # ------------------------------------------------------------ properties
     @property
@@ -72,7 +85,17 @@ class ObjectPixelated(OptimizerMixin):
 
     @property
     def dtype(self):
-        return torch.complex64
+        """float32 for potentials, complex64 otherwise (object_models.py:85-89)."""
+        return torch.float32 if self._obj_type == "potential" else torch.complex64
+
+    def transmission_spec(self):
+        """What the batch kernels need to turn the raw object into its transmission."""
+        from .. import ops
+
+        c = self._constraints
+        return ops.ObjSpec(self._obj_type, positivity=bool(c.get("positivity", True)),
+                           fix_baseline=bool(c.get("fix_potential_baseline", False)),
+                           baseline_factor=float(c.get("fix_potential_baseline_factor", 1.0)))
 
     @property
     def device(self):
@@ -159,19 +182,20 @@ class ObjectPixelated(OptimizerMixin):
         shape = tuple(int(x) for x in shape)
         if self._obj.numel() > self.num_slices and tuple(self._obj.shape) == shape:
             return
-        if self._initialize_mode == "uniform":
-            arr = torch.ones(shape, dtype=torch.complex64)
+        potential = self._obj_type == "potential"
+        if self._initialize_mode == "uniform":  # object_models.py:660-664
+            arr = torch.zeros(shape, dtype=torch.float32) if potential else torch.ones(shape, dtype=torch.complex64)
         elif self._initialize_mode == "random":
             g = torch.Generator().manual_seed(int(self._rng_seed % 2**32) if self._rng_seed is not None else 0)
             ph = (torch.randn(shape, dtype=torch.float32, generator=g) - 0.5) * 1e-6
-            arr = torch.exp(1.0j * ph).to(torch.complex64)
+            arr = ph if potential else torch.exp(1.0j * ph).to(torch.complex64)
         elif self._initialize_mode == "array":
             arr = self._initial_obj
             if tuple(arr.shape) != shape:
                 raise ValueError(f"initial object shape {tuple(arr.shape)} != reconstruction shape {shape}")
         else:
             raise ValueError(f"Invalid initialize mode: {self._initialize_mode}")
-        self._initial_obj = arr.to(torch.complex64)
+        self._initial_obj = arr.to(self.dtype)
         self.reset()
 
     def reset(self):
@@ -216,14 +240,31 @@ class ObjectPixelated(OptimizerMixin):
     # ------------------------------------------------------------ compute
     @property
     def obj(self) -> torch.Tensor:
-        """Hard-constrained object (differentiable, CUDA kernels)."""
+        """Hard-constrained object (object_models.py:289-339; differentiable): the complex
+        or pure-phase object from the CUDA constraint kernels, or the real potential
+        V - offset clamped at 0."""
         from .. import ops
 
-        return ops.constrained_object(self._obj)
+        if self._obj_type == "complex":
+            return ops.constrained_object(self._obj)
+        if self._obj_type == "pure_phase":
+            return ops.object_transmission(self._obj, self.transmission_spec())
+        spec = self.transmission_spec()
+        v = self._obj
+        if spec.fix_baseline:
+            v = v - v.min().detach() * spec.baseline_factor
+        return torch.clamp(v, min=0.0) if spec.positivity else v
+
+    def transmission(self) -> torch.Tensor:
+        """exp(i V') for potentials, the constrained object otherwise (complex64,
+        differentiable, CUDA kernels): what multiplies the wave in every slice."""
+        from .. import ops
+
+        return ops.object_transmission(self._obj, self.transmission_spec())
 
     def forward(self, patch_indices: torch.Tensor) -> torch.Tensor:
         """(S, B, H, W) object patches at the given flat indices (object_models.py:252-265)."""
-        o = self.obj.reshape(self.num_slices, -1)
+        o = self.transmission().reshape(self.num_slices, -1)
         return torch.complex(o.real[:, patch_indices], o.imag[:, patch_indices])
 
     def backward(self, *args, **kwargs):
