@@ -112,6 +112,7 @@ class PtychographyDatasetRaster(OptimizerMixin):
         self.detector_mask = detector_mask
         self._constraints = dict(self.DEFAULT_CONSTRAINTS)
         self._targets = None
+        self._targets_on_host = False
         self._patch_indices = None
         self._last_patch_positions_px = None
 
@@ -236,6 +237,27 @@ class PtychographyDatasetRaster(OptimizerMixin):
     def constraints(self) -> dict:
         return self._constraints
 
+    @property
+    def targets_on_host(self) -> bool:
+        return self._targets_on_host
+
+    def keep_targets_on_host(self, enable: bool = True):
+        """Keep the measured targets in pinned host memory whatever device the dataset
+        moves to.  ``Ptychography.reconstruct`` then copies them to the GPU once per
+        iteration, double-buffered on a copy stream so that the copy for the next
+        iteration overlaps the current one (for data that should not stay resident in
+        device memory).  Not part of the reference API."""
+        self._targets_on_host = bool(enable)
+        if isinstance(self._targets, torch.Tensor):
+            self._targets = self._host_or_device(self._targets)
+        return self
+
+    def _host_or_device(self, t: torch.Tensor) -> torch.Tensor:
+        if self._targets_on_host:
+            t = t.detach().cpu().contiguous()
+            return t if not torch.cuda.is_available() or t.is_pinned() else t.pin_memory()
+        return t.to(self._device).contiguous()
+
     def add_constraint(self, key, value):
         if key not in self.DEFAULT_CONSTRAINTS:
             raise KeyError(f"Unknown dataset constraint {key!r}")
@@ -257,7 +279,7 @@ class PtychographyDatasetRaster(OptimizerMixin):
                      "_targets", "_centered_amplitudes", "_amplitudes", "_centered_intensities", "_intensities"):
             v = getattr(self, name, None)
             if isinstance(v, torch.Tensor):
-                setattr(self, name, v.to(dev))
+                setattr(self, name, self._host_or_device(v) if name == "_targets" else v.to(dev))
         return self
 
     # ---------------------------------------------------------- preprocessing
@@ -521,7 +543,7 @@ class PtychographyDatasetRaster(OptimizerMixin):
             t = self._centered_intensities
         else:
             raise ValueError(f"Unknown loss type {loss_type}")
-        self._targets = t.clone().to(self._device).contiguous()
+        self._targets = self._host_or_device(t.clone())
 
     # --------------------------------------------------------- per batch
     def apply_hard_constraints(self, obj_padding_px):

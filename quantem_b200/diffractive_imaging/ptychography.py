@@ -22,6 +22,7 @@ from .detector_models import DetectorPixelated
 from .object_models import ObjectPixelated
 from .probe_models import ProbePixelated
 from .ptycho_utils import SimpleBatcher
+from ..engine import HostTargetStream
 
 
 def adjust_padding_power2(pad, shape, power2_level):
@@ -413,12 +414,17 @@ class Ptychography:
         return prop, self.dset.scan_positions_px.contiguous(), self.dset.targets, \
             self.dset.detector_mask.to(dev).contiguous()
 
+    def _device_targets(self, tg):
+        """Targets on the device (a one-off copy when the dataset keeps them on the host)."""
+        return tg if tg.device.type == "cuda" else tg.to(self._device, non_blocking=True)
+
     def forward_intensities(self, batch_indices, loss_type="l2_amplitude"):
         """Predicted detector intensities (B, H, W) and batch loss, no gradients."""
         prop, pos, tg, mask = self._batch_tensors()
+        tg = self._device_targets(tg)
         bi = torch.as_tensor(np.asarray(batch_indices, dtype=np.int64), device=self._device)
         with torch.no_grad():
-            obj_c = self.obj_model.obj.detach().contiguous()
+            obj_c = self.obj_model.transmission().detach().contiguous()
             probe_o = self.probe_model.probe.detach().contiguous()
         out = ops.batch_forward(obj_c, probe_o, prop, pos, bi, tg, mask, self.dset.num_gpts,
                                 self.dset.mean_diffraction_intensity, loss_type)
@@ -430,9 +436,10 @@ class Ptychography:
         if batch_indices is None:
             raise ValueError("forward_operator on the B200 path takes batch_indices (positions are gathered in-kernel)")
         prop, pos, tg, mask = self._batch_tensors()
+        tg = self._device_targets(tg)
         bi = torch.as_tensor(np.asarray(batch_indices, dtype=np.int64), device=self._device)
         with torch.no_grad():
-            out = ops.batch_forward(self.obj_model.obj.detach().contiguous(),
+            out = ops.batch_forward(self.obj_model.transmission().detach().contiguous(),
                                     self.probe_model.probe.detach().contiguous(), prop, pos, bi, tg, mask,
                                     self.dset.num_gpts, self.dset.mean_diffraction_intensity,
                                     want_intensity=False, want_exit=True, want_waves=True)
@@ -476,9 +483,16 @@ class Ptychography:
         prop, _, tg, mask = self._batch_tensors()
         opts = [o for o in (self.obj_model.optimizer, self.probe_model.optimizer) if o is not None]
         dev = torch.device(self._device)
+        # targets kept in host memory (dset.keep_targets_on_host): one double-buffered copy per iteration
+        stream = HostTargetStream(tg, dev) if tg.device.type != "cuda" and num_iters > 0 else None
+        self.last_h2d_bytes_per_iter = stream.bytes_per_copy if stream is not None else 0
         for a0 in range(num_iters):
             total = torch.zeros((), dtype=torch.float32, device=dev)
             nb = 0
+            if stream is not None:
+                tg = stream.acquire()
+                if a0 + 1 < num_iters:
+                    stream.prefetch_next()
             for bi in batcher:
                 for o in opts:
                     o.zero_grad(set_to_none=True)
@@ -489,7 +503,8 @@ class Ptychography:
                     probe_o = self.probe_model.probe
                     obj_raw = self.obj_model._obj  # a leaf (pixelated) or a network output (DIP)
                     loss = ops.batch_loss(obj_raw, probe_o, prop, pos, idx, tg, mask,
-                                          self.dset.num_gpts, self.dset.mean_diffraction_intensity, loss_type)
+                                          self.dset.num_gpts, self.dset.mean_diffraction_intensity, loss_type,
+                                          obj_spec=self.obj_model.transmission_spec())
                     if obj_raw.requires_grad or self.probe_model._probe.requires_grad:
                         loss.backward()
                         if obj_raw.is_leaf and obj_raw.grad is not None:
@@ -499,6 +514,9 @@ class Ptychography:
                     # analytic update directions (ptychography.py:339-348), no autograd graph
                     if type(self.obj_model).__name__ == "ObjectDIP":
                         raise NotImplementedError("the analytic update applies to pixelated objects (autograd=True)")
+                    if self.obj_model.obj_type != "complex":
+                        raise NotImplementedError("the analytic update of this path covers complex objects; "
+                                                  "use autograd=True for pure-phase and potential objects")
                     with torch.no_grad():
                         probe_o = self.probe_model.probe.detach().contiguous()
                         obj_c, _ = ops.obj_constrain(self.obj_model._obj.detach().contiguous())
@@ -511,6 +529,8 @@ class Ptychography:
                     o.step()
                 total += loss.detach()
                 nb += 1
+            if stream is not None:
+                stream.release()
             total_loss = float((total / max(nb, 1)).item())
             ops.check_status(dev)  # out-of-range batch indices / non-finite intensities since the last check
             val_loss = None
@@ -544,12 +564,50 @@ class Ptychography:
             else:
                 self._iter_lrs[key] = [0.0] * (self.num_iters - 1) + [opts[key].param_groups[0]["lr"]]
 
+    # ------------------------------------------------------------ checkpoint / resume
+    def state_dict(self, save_raw_data: bool = False, skip=()) -> dict:
+        """The reconstruction's resumable state (quantem_b200.diffractive_imaging.checkpoint)."""
+        from . import checkpoint
+
+        return checkpoint.state_dict(self, save_raw_data=save_raw_data, skip=skip)
+
+    def save(self, path, mode: Literal["w", "o"] = "w", store: Literal["auto", "zip", "dir"] = "auto", skip=(),
+             compression_level: int | None = 4, save_raw_data: bool = False, verbose: int | bool = True):
+        """Save the reconstruction (ptychography.py:376-480): object, probe, optimiser and
+        scheduler states, generator state, histories and the dataset's preprocessing
+        parameters and positions; the 4D-STEM array too with ``save_raw_data``.  One
+        ``torch.save`` file (``store`` and ``compression_level`` are accepted for API
+        compatibility; the reference's zarr store is not used).  ``mode`` "w" refuses to
+        replace an existing file, "o" overwrites."""
+        from pathlib import Path
+
+        from . import checkpoint
+
+        if self.verbose and verbose:
+            print(f"Saving ptychography object to {Path(path).resolve()}")
+        checkpoint.save(self, path, mode=mode, save_raw_data=save_raw_data, skip=skip)
+
+    @classmethod
+    def from_file(cls, path, dset=None, device=None, verbose=None, auto_reload_dataset: bool = True):
+        """Load a reconstruction saved by ``save`` (ptychography.py:481-588).  Without
+        ``dset`` the dataset is rebuilt from the stored raw data and preprocessed with the
+        stored parameters; a given ``dset`` is used as is (preprocessed with the stored
+        parameters if it is not yet).  Training continues exactly where it stopped."""
+        from . import checkpoint
+
+        if dset is None and not auto_reload_dataset:
+            raise ValueError("this path needs a dataset: pass dset= or keep auto_reload_dataset=True")
+        return checkpoint.load(cls, path, dset=dset, device=device, verbose=verbose)
+
     # ------------------------------------------------------------ results
     @property
     def obj(self) -> np.ndarray:
-        """Constrained object with the mean phase removed (ptychography_base.py:312-318)."""
+        """Constrained object with the mean phase removed (ptychography_base.py:312-318);
+        the constrained real potential for potential objects."""
         with torch.no_grad():
             o = self.obj_model.obj.detach().cpu().numpy()
+        if self.obj_model.obj_type == "potential":
+            return o
         ph = np.angle(o)
         return np.abs(o) * np.exp(1j * (ph - ph.mean()))
 
@@ -561,6 +619,8 @@ class Ptychography:
     @property
     def obj_cropped(self) -> np.ndarray:
         c = self._crop_rotate_obj_fov(self.obj)
+        if self.obj_model.obj_type == "potential":
+            return c
         ph = np.angle(c)
         return np.abs(c) * np.exp(1j * (ph - ph.mean()))
 

@@ -197,3 +197,47 @@ class GraphedIteration:
         """One iteration; returns the batch loss (a device tensor overwritten by the next replay)."""
         self.graph.replay()
         return self.static_loss
+
+
+class HostTargetStream:
+    """Per-iteration host-to-device copies of a host array (the measured targets),
+    double-buffered: the copy for iteration k + 1 runs on a copy stream into the second
+    device buffer while iteration k computes on the current stream.  The first copy is
+    exposed.  ``acquire()`` returns this iteration's buffer (the current stream waits
+    for its copy), ``prefetch_next()`` starts the next copy once that buffer is free,
+    ``release()`` marks the end of this iteration's use of its buffer."""
+
+    def __init__(self, host: torch.Tensor, device):
+        self.host = host if host.is_pinned() else host.pin_memory()
+        self.device = torch.device(device)
+        self.stream = torch.cuda.Stream(device=self.device)
+        self.buf = [torch.empty(host.shape, dtype=host.dtype, device=self.device) for _ in range(2)]
+        for b in self.buf:
+            b.record_stream(self.stream)
+        self.ready = [torch.cuda.Event(), torch.cuda.Event()]
+        self.free = [None, None]
+        self.k = 0
+        self.bytes_per_copy = host.numel() * host.element_size()
+        self._issue(0)
+
+    def _issue(self, i):
+        with torch.cuda.stream(self.stream):
+            if self.free[i] is not None:
+                self.stream.wait_event(self.free[i])
+            self.buf[i].copy_(self.host, non_blocking=True)
+            self.ready[i].record(self.stream)
+
+    def acquire(self) -> torch.Tensor:
+        i = self.k % 2
+        torch.cuda.current_stream(self.device).wait_event(self.ready[i])
+        return self.buf[i]
+
+    def prefetch_next(self):
+        self._issue((self.k + 1) % 2)
+
+    def release(self):
+        i = self.k % 2
+        ev = torch.cuda.Event()
+        ev.record(torch.cuda.current_stream(self.device))
+        self.free[i] = ev
+        self.k += 1

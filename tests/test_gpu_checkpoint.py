@@ -1,0 +1,60 @@
+"""Resume on the GPU: 2 iterations, save, load, 2 more iterations equal 4 uninterrupted
+iterations.  The object gradient is accumulated with float atomics, whose order varies
+from run to run, so two uninterrupted runs may already differ in the last bits; the
+resumed run must sit within that run-to-run spread (and match exactly when the
+uninterrupted runs do)."""
+import numpy as np
+import pytest
+import torch
+
+from tests.conftest import load_golden, rel
+from tests.test_host_setup import build_from_golden
+
+pytestmark = pytest.mark.gpu
+
+OPT = {"object": {"type": "adam"}, "probe": {"type": "adam"}}
+
+
+def _fresh(z):
+    pt = build_from_golden(z, device="gpu")
+    dev = torch.device("cuda", 0)
+    pt.dset.scan_positions_px = torch.as_tensor(z["positions"])
+    pt.obj_model._obj = torch.as_tensor(z["obj_perturbed"]).to(dev).requires_grad_(True)
+    pt.probe_model._probe = torch.as_tensor(z["probe_init"]).to(dev).requires_grad_(True)
+    pt.rng = int(z["recon_rng_seed"])
+    return pt
+
+
+def _state(pt):
+    return (pt.obj_model._obj.detach().cpu().numpy(), pt.probe_model._probe.detach().cpu().numpy(),
+            np.asarray(pt.iter_losses))
+
+
+@pytest.mark.parametrize("raw", [True, False])
+def test_resume_equals_uninterrupted(cuda_device, tmp_path, raw):
+    from quantem_b200.diffractive_imaging import Ptychography
+
+    z = load_golden("mixed64")
+    bs = 7  # 25 positions: 4 batches per iteration, the last one short
+    runs = []
+    for _ in range(2):
+        pt = _fresh(z)
+        pt.reconstruct(num_iters=4, batch_size=bs, optimizer_params=OPT, device="gpu")
+        runs.append(_state(pt))
+    pt = _fresh(z)
+    pt.reconstruct(num_iters=2, batch_size=bs, optimizer_params=OPT, device="gpu")
+    path = tmp_path / "mid.pt"
+    pt.save(path, save_raw_data=raw, verbose=False)
+    q = Ptychography.from_file(path, dset=None if raw else _fresh(z).dset, device="gpu")
+    del pt
+    assert q.num_iters == 2
+    q.reconstruct(num_iters=2, device="gpu")
+    obj, probe, losses = _state(q)
+    (obj_a, probe_a, losses_a), (obj_b, probe_b, losses_b) = runs
+    assert losses.shape == (4,)
+    spread = max(rel(obj_b, obj_a), rel(probe_b, probe_a))
+    if spread == 0.0:
+        np.testing.assert_array_equal(losses, losses_a)
+    np.testing.assert_allclose(losses, losses_a, rtol=1e-6)
+    assert rel(obj, obj_a) <= 3 * spread + 1e-6
+    assert rel(probe, probe_a) <= 3 * spread + 1e-6
