@@ -9,12 +9,15 @@ counts/pattern Poisson data, l2_amplitude loss, Adam on object and probe, batch
 = all 4096 positions (the reference's default batch size).  Data are seeded
 synthetic inputs simulated with this package's forward kernels.
 
-``--impl ours`` times the CUDA path (device-resident ``value``; ``e2e`` through
-the public reconstruct call with the measured data copied from pinned host
-memory every step).  ``--impl reference`` times the CPU oracle port of the
-reference algorithm on the host cores on a bounded sample of the same workload;
-``--impl reference --torch-gpu`` times the reference's own PyTorch iteration on
-the GPU (also reported in the default line as ``reference_torch_gpu``).
+``--impl ours`` times the CUDA path: ``value`` is the device-resident iteration
+replayed from a CUDA graph; ``e2e`` is ``Ptychography.reconstruct`` of the drop-in
+API on a dataset built from host arrays whose targets stay in pinned host memory
+and are copied to the GPU every iteration.  ``--impl reference`` times the
+reference's own ``Ptychography.reconstruct(device="cpu")`` (package under
+``baseline/_ref``) on the host cores on a bounded sample of the same geometry (an
+8 x 8 sub-scan, 64 positions, batch 64); ``--impl reference --torch-gpu`` times the
+reference's own PyTorch iteration on the GPU (also reported in the default line as
+``reference_torch_gpu``).
 With ``--gpus N`` (torchrun), every rank reconstructs its own dataset: N
 independent replicas, no collective.
 """
@@ -163,6 +166,44 @@ def build_problem(seed, device, batch_size, cfg=None):
     return cfg, ds, pt, opts, batcher
 
 
+def build_dropin(cfg, device, seed):
+    """The drop-in API set up the way a user of the reference would: a host
+    ``Dataset4dstem`` of the simulated patterns, ``PtychographyDatasetRaster.preprocess``
+    (on the GPU), ``ObjectPixelated.from_uniform``, ``ProbePixelated.from_params`` with
+    the configuration's mode weights, ``Ptychography.from_models(...).preprocess(...)``,
+    jittered positions.  The targets stay in pinned host memory
+    (``keep_targets_on_host``), so every ``reconstruct`` iteration copies them to the
+    GPU."""
+    import torch
+
+    from quantem_b200 import synthetic
+    from quantem_b200.diffractive_imaging import (Dataset4dstem, DetectorPixelated, ObjectPixelated,
+                                                  ProbePixelated, Ptychography, PtychographyDatasetRaster)
+
+    ds = synthetic.make_dataset(cfg, device)
+    nr, nc = cfg.scan
+    data = ds["intensities"].cpu().numpy().reshape(nr, nc, cfg.n, cfg.n)
+    del ds
+    rs = 1.0 / (cfg.n * cfg.pixel)
+    d4 = Dataset4dstem.from_array(data, sampling=(cfg.step_px * cfg.pixel, cfg.step_px * cfg.pixel, rs, rs),
+                                  units=("A", "A", "A^-1", "A^-1"))
+    pd = PtychographyDatasetRaster.from_dataset4dstem(d4, verbose=0)
+    pd.preprocess(com_fit_function="constant", force_com_rotation=0, force_com_transpose=False,
+                  plot_rotation=False, plot_com=False, probe_energy=cfg.energy, device="gpu")
+    obj = ObjectPixelated.from_uniform(num_slices=cfg.slices, slice_thicknesses=cfg.slice_thickness,
+                                       obj_type="complex")
+    probe = ProbePixelated.from_params(probe_params={"energy": cfg.energy, "defocus": cfg.defocus,
+                                                     "semiangle_cutoff": cfg.semiangle},
+                                       num_probes=cfg.modes, rng=seed + 1, initial_probe_weights=list(cfg.mode_weights))
+    pt = Ptychography.from_models(dset=pd, obj_model=obj, probe_model=probe, detector_model=DetectorPixelated(),
+                                  device="gpu", verbose=0, rng=seed + 2)
+    pt.preprocess(obj_padding_px=(cfg.pad_px, cfg.pad_px))
+    jit = np.random.default_rng(seed).uniform(-cfg.jitter_px, cfg.jitter_px, (pd.num_gpts, 2)).astype(np.float32)
+    pd.scan_positions_px = pd.scan_positions_px.detach() + torch.as_tensor(jit, device=pd.scan_positions_px.device)
+    pd.keep_targets_on_host(True)
+    return pt
+
+
 def fp32_peak_tflops(device):
     """FP32 FMA throughput of this GPU (own microbenchmark kernel), TFLOP/s."""
     import ctypes
@@ -256,60 +297,27 @@ def run_ours(args):
         del git
     ms = ms_graph if ms_graph is not None else ms_eager
 
-    # ---- end to end through the public call with host buffers ----
-    host_t = ds["amplitudes"].cpu().pin_memory()
-    host_p = pt.positions.cpu().pin_memory()
-    loss_host = torch.empty(1, dtype=torch.float32).pin_memory()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
+    # ---- end to end through the drop-in API: Ptychography.reconstruct on a dataset whose
+    # targets stay in pinned host memory and are copied to the GPU every iteration; the
+    # loss and the status word are read back every iteration ----
+    drop = build_dropin(cfg, device, 1234 + rank)
+    opt = {"object": {"type": "adam", "lr": 5e-3}, "probe": {"type": "adam", "lr": 1e-3}}
+    drop.reconstruct(num_iters=args.warmup, batch_size=args.batch_size, optimizer_params=opt, device="gpu")
     torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
-    for _ in range(args.steps):
-        pt.targets.copy_(host_t, non_blocking=True)
-        pt.positions.copy_(host_p, non_blocking=True)
-        l = engine.run_iteration(pt, batcher, opts)
-        loss_host.copy_(l.reshape(1), non_blocking=True)
+    drop.reconstruct(num_iters=args.steps, batch_size=args.batch_size, device="gpu")
     e1.record()
     torch.cuda.synchronize()
-    e2e_serial_ms = e0.elapsed_time(e1) / args.steps
-
-    # pipelined: step k+1's inputs are copied on a copy stream into the other half of
-    # a double buffer while step k computes; every step still copies its own inputs
-    # inside the timed region, and the first copy is exposed
-    tbuf = [pt.targets, torch.empty_like(pt.targets)]
-    pbuf = [pt.positions, torch.empty_like(pt.positions)]
-    cstream = torch.cuda.Stream(device=device)
-    ready = [torch.cuda.Event(), torch.cuda.Event()]
-    freed = [torch.cuda.Event(), torch.cuda.Event()]
-    main = torch.cuda.current_stream(device)
-
-    def upload(i, after=None):
-        with torch.cuda.stream(cstream):
-            if after is not None:
-                cstream.wait_event(after)
-            tbuf[i].copy_(host_t, non_blocking=True)
-            pbuf[i].copy_(host_p, non_blocking=True)
-            ready[i].record(cstream)
-
-    torch.cuda.synchronize()
-    e0.record(main)
-    upload(0)
-    for k in range(args.steps):
-        i = k % 2
-        if k + 1 < args.steps:
-            upload(1 - i, freed[1 - i] if k >= 1 else None)
-        main.wait_event(ready[i])
-        pt.targets, pt.positions = tbuf[i], pbuf[i]
-        l = engine.run_iteration(pt, batcher, opts)
-        freed[i].record(main)
-        loss_host.copy_(l.reshape(1), non_blocking=True)
-    e1.record(main)
-    torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1) / args.steps
-    pt.targets, pt.positions = tbuf[0], pbuf[0]
-    del tbuf[1], pbuf[1]
+    h2d = drop.last_h2d_bytes_per_iter + drop.dset.num_gpts * 8  # targets + batch indices
+    e2e_final_loss = float(drop.iter_losses[-1])
+    del drop
+    torch.cuda.empty_cache()
 
-    ms, ms_eager, e2e_ms, e2e_serial_ms = max_over_ranks([ms, ms_eager, e2e_ms, e2e_serial_ms], dist, device)
+    ms, ms_eager, e2e_ms = max_over_ranks([ms, ms_eager, e2e_ms], dist, device)
     if rank != 0:
         if dist:
             dist.destroy_process_group()
@@ -319,19 +327,26 @@ def run_ours(args):
     hbm_peak, peak_kind = _peaks()
     fused_avg_ms = statistics.mean(fused_ms) if fused_ms else None
     pos_per_launch = args.batch_size if args.batch_size else npos
-    roofline = None
+    # The binding roof of this FFT path is the FP32 CUDA-core pipe (no GEMM: tensor cores do
+    # not apply); its peak is measured in the same run by the library's FMA probe kernel
+    # (MEASURED_PEAKS.json carries HBM and BF16 figures only).  The HBM roof is reported
+    # beside it.
+    roofline = roofline_hbm = None
+    fp32 = fp32_peak_tflops(device)
     if fused_avg_ms:
         achieved = BYTES_PER_POS * pos_per_launch / (fused_avg_ms * 1e-3) / 1e9
-        roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
-                    "frac": round(achieved / hbm_peak, 4), "traffic": _ncu_traffic(), "peak_source": peak_kind,
-                    "kernel": "fused_batch_kernel<128,adjoint>", "kernel_ms": round(fused_avg_ms, 4)}
-    fp32 = fp32_peak_tflops(device)
-    fp32_roof = None
+        roofline_hbm = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
+                        "frac": round(achieved / hbm_peak, 4), "traffic": _ncu_traffic(),
+                        "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                        else "fallback 6650 GB/s", "bytes_per_position": BYTES_PER_POS}
     if fused_avg_ms and fp32:
         ach = FLOPS_PER_POS * pos_per_launch / (fused_avg_ms * 1e-3) / 1e12
-        fp32_roof = {"bound": "fp32", "achieved": round(ach, 2), "peak": round(fp32, 2), "unit": "TFLOP/s",
-                     "frac": round(ach / fp32, 4), "peak_source": "measured (own FMA probe)"}
-    cpu = cpu_baseline_sample(args)
+        roofline = {"bound": "fp32", "achieved": round(ach, 2), "peak": round(fp32, 2), "unit": "TFLOP/s",
+                    "frac": round(ach / fp32, 4), "traffic": _ncu_traffic(),
+                    "peak_source": "measured in this run (ptycho_fp32_fma_probe: 148 x 4 CTAs of FMA chains)",
+                    "flops_per_position": FLOPS_PER_POS, "positions_per_launch": pos_per_launch,
+                    "kernel": "fused_batch_kernel<128,adjoint>", "kernel_ms": round(fused_avg_ms, 4)}
+    cpu = reference_cpu_subprocess(local, steps=2, warmup=1)
     try:  # the oracle as the checker: FP32 CUDA path against an FP64 run on a bounded sample
         accuracy = accuracy_vs_fp64(pt)
     except Exception as exc:
@@ -339,7 +354,7 @@ def run_ours(args):
     torch_ref = torch_eager_reference(pt, args.batch_size) if not args.skip_torch_reference else None
     ref_gpu = None
     if not args.skip_torch_reference:
-        ref_gpu = reference_torch_gpu_subprocess(local, args.batch_size)
+        ref_gpu = reference_torch_gpu_subprocess(local, args.batch_size, steps=10, warmup=3)
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": "positions/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
@@ -349,12 +364,15 @@ def run_ours(args):
         "config": {"workload": WORKLOAD, "global_batch": pos_per_launch * world, "positions": npos,
                    "object": [cfg.slices, 512, 512], "probe": [cfg.modes, cfg.n, cfg.n],
                    "parallelism": f"replicas{world}", "l2": "inputs larger than L2 (targets 256 MiB/step)"},
-        "e2e": {"value": round(e2e, 1), "unit": "positions/s", "h2d_bytes_per_step": int(host_t.numel() * 4
-                                                                                          + host_p.numel() * 4),
-                "d2h_bytes_per_step": 4, "pipelined": "inputs of step k+1 copied on a copy stream during step k",
-                "serial_value": round(npos * world / (e2e_serial_ms * 1e-3), 1)},
+        "e2e": {"value": round(e2e, 1), "unit": "positions/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": 8,
+                "path": "quantem_b200.diffractive_imaging.Ptychography.reconstruct(num_iters=steps, device='gpu') "
+                        "on a host Dataset4dstem preprocessed through the drop-in API; targets in pinned host "
+                        "memory copied to the GPU every iteration (double-buffered on a copy stream), loss and "
+                        "status word read back every iteration",
+                "final_loss": e2e_final_loss},
         "gpu_launches": launches_per_batch * nbatches,
-        "roofline": roofline, "roofline_fp32": fp32_roof,
+        "roofline": roofline, "roofline_hbm": roofline_hbm,
         "cpu_baseline": cpu,
         "accuracy_vs_fp64": accuracy,
         "torch_eager_reference_gpu": torch_ref,
@@ -1042,17 +1060,89 @@ def run_preprocess(args):
                       / res["cpu"]["mean_intensity"]}))
 
 
+def _cpu_model():
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
+def reference_cpu_config():
+    """The bounded CPU sample of the headline geometry: an 8 x 8 sub-scan (64 positions,
+    6 px step, +-0.5 px jitter) with the padding that keeps the object at 512 x 512 x 8;
+    4 modes at 128^2, 1e5 counts."""
+    from quantem_b200 import synthetic
+
+    return synthetic.SyntheticConfig(seed=0, scan=(8, 8), pad_px=235)
+
+
+def reference_cpu_sample(steps, warmup):
+    """The reference's own ``Ptychography.reconstruct(device="cpu")`` (autograd, Adam,
+    probe orthogonalisation; package under baseline/_ref) on every host core, over the
+    bounded sample of ``reference_cpu_config`` with batch 64 (one batch per iteration).
+    Falls back to the oracle port (kind "port") when the reference package is absent."""
+    import torch
+
+    ncores = os.cpu_count() or 1
+    torch.set_num_threads(ncores)
+    cfg = reference_cpu_config()
+    npos = cfg.scan[0] * cfg.scan[1]
+    if torch.cuda.is_available():  # the sample's data are simulated with this package's CUDA kernels
+        try:
+            res = reference_torch_gpu(cfg, "cpu", steps, warmup, npos)
+        except Exception as exc:  # a reported baseline: report why, never fail the bench
+            res = {"unavailable": f"{type(exc).__name__}: {exc}"[:300]}
+    else:
+        res = {"unavailable": "no CUDA device to simulate the sample's data"}
+    if "unavailable" not in res:
+        return {"value": res["value"], "unit": "positions/s", "cores": torch.get_num_threads(), "kind": "reference",
+                "cpu_model": _cpu_model(), "ms_per_step": res["ms_per_step"],
+                "sample": f"quantem Ptychography.reconstruct(device='cpu') from baseline/_ref, {steps} timed "
+                          f"iterations after {warmup} warm-up: {npos} positions (8x8 sub-scan) of the 512x512x8 "
+                          "object / 4 modes at 128^2 geometry, batch 64, autograd + Adam + probe "
+                          "orthogonalisation, complex64, torch threads = host cores"}
+    port = cpu_baseline_sample(argparse.Namespace(cpu_seconds=15.0))
+    port["reference_unavailable"] = res["unavailable"]
+    return port
+
+
+def reference_cpu_subprocess(local_device: int, steps: int, warmup: int):
+    """``reference_cpu_sample`` in a fresh process (its own torch threads and allocator)."""
+    env = {k: v for k, v in os.environ.items()
+           if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK", "LOCAL_WORLD_SIZE", "MASTER_ADDR", "MASTER_PORT",
+                        "GROUP_RANK", "ROLE_RANK", "TORCHELASTIC_RUN_ID")}
+    visible = os.environ.get("CUDA_VISIBLE_DEVICES")
+    env["CUDA_VISIBLE_DEVICES"] = visible.split(",")[local_device] if visible else str(local_device)
+    cmd = [sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--cpu-sample",
+           "--steps", str(steps), "--warmup", str(warmup)]
+    try:
+        out = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=900)
+        line = json.loads(out.stdout.strip().splitlines()[-1])
+    except Exception as exc:  # a reported baseline: never fail the bench over it
+        return {"unavailable": f"{type(exc).__name__}: {exc}"[:300]}
+    return line.get("cpu_baseline", line)
+
+
 def run_reference(args):
+    """``--impl reference``: the reference's own CPU iteration (see reference_cpu_sample),
+    rank 0 only; the other ranks exit without work."""
     rank, world, _ = _dist_env()
     if rank != 0:
         return
-    cpu = cpu_baseline_sample(args)
+    cpu = reference_cpu_sample(args.steps, args.warmup)
     line = {"metric": METRIC, "value": cpu["value"], "unit": "positions/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "c64/f32", "data": "synthetic", "impl": "reference",
-            "config": {"workload": WORKLOAD, "parallelism": "host cores"},
+            "config": {"workload": WORKLOAD, "parallelism": "host cores",
+                       "sample": "64 positions (8x8 sub-scan) per step, batch 64"},
             "cpu_baseline": cpu, "e2e": {"value": cpu["value"], "unit": "positions/s",
                                           "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if "ms_per_step" in cpu:
+        line["ms_per_step"] = cpu["ms_per_step"]
     print(json.dumps(line))
 
 
@@ -1227,10 +1317,13 @@ def main():
                     help="do not time the PyTorch-eager restatement of the reference path nor the "
                          "reference's own PyTorch iteration on the GPU")
     ap.add_argument("--positions", type=int, default=296, help="positions per launch with --kernel-only")
+    ap.add_argument("--cpu-sample", action="store_true",
+                    help="with --impl reference: the bounded reference CPU sample for the cpu_baseline key "
+                         "(keeps the given --warmup)")
     ap.add_argument("--variant", default="auto", choices=["auto", "serial", "cluster"],
                     help="mapping of probe modes onto CTAs (--kernel-only)")
     args = ap.parse_args()
-    if args.warmup < 3:
+    if args.warmup < 3 and not args.cpu_sample:
         args.warmup = 3
     if args.impl == "reference" and args.torch_gpu:
         run_reference_torch_gpu(args)
