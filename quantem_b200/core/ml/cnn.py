@@ -664,3 +664,178 @@ class _MSEFn(torch.autograd.Function):
     def backward(ctx, g):
         (dp,) = ctx.saved_tensors
         return dp * g, None
+
+
+class ComplexCNN2d(torch.nn.Module):
+    """The reference's CNN2d with ``dtype=torch.complex64`` (complex convolutions,
+    ComplexBatchNorm2D, Complex_ReLU, complex pooling) on the B200 kernels.
+
+    It runs as a real ``CNN2d`` with doubled channels whose tensors hold the real parts
+    followed by the imaginary parts and whose weights have the block structure
+    [[A, -B], [B, A]] of a complex weight A + iB (``complex_map``).  The complex
+    parameters live in one flat FP32 tensor (``self.flat``: every complex tensor as its
+    real view, batch-norm parameters as they are); each forward writes the real
+    network's weights as a signed gather of it, and the gradient of the real weights
+    flows back through the same gather (so dA and dB sum the two blocks each feeds).
+    ``state_dict`` / ``load_state_dict`` use the reference's names, complex dtypes and
+    layouts (``real_bn`` / ``imag_bn`` batch-norm halves)."""
+
+    def __init__(self, in_channels: int, out_channels: int | None = None, start_filters: int = 16,
+                 num_layers: int = 3, num_per_layer: int = 2, use_skip_connections: bool = True,
+                 dtype: torch.dtype = torch.complex64, dropout: float = 0, activation="relu",
+                 final_activation="identity", use_batchnorm: bool = True, device="cuda", seed: int | None = 0):
+        super().__init__()
+        from .complex_map import complex_to_real_state
+
+        if not dtype.is_complex:
+            raise ValueError("ComplexCNN2d takes a complex dtype (use CNN2d for real networks)")
+        self.in_channels = int(in_channels)
+        self.out_channels = int(out_channels) if out_channels is not None else int(in_channels)
+        self.start_filters = int(start_filters)
+        self.num_layers = int(num_layers)
+        self.use_skip_connections = bool(use_skip_connections)
+        self.dtype = dtype
+        self.device = torch.device(device)
+        self.real = CNN2d(2 * self.in_channels, 2 * self.out_channels, start_filters=2 * self.start_filters,
+                          num_layers=num_layers, num_per_layer=num_per_layer,
+                          use_skip_connections=use_skip_connections, dtype=torch.float32, dropout=dropout,
+                          activation=activation, final_activation=final_activation, use_batchnorm=use_batchnorm,
+                          device=device, seed=seed)
+        # the reference's complex state-dict template, from the real network's
+        self.template = self._complex_template(self.real.state_dict())
+        self.keys = [k for k, v in self.template.items()
+                     if not k.endswith(("running_mean", "running_var", "num_batches_tracked"))]
+        self.offsets = {}
+        off = 0
+        for k in self.keys:
+            t = self.template[k]
+            n = t.numel() * (2 if t.is_complex() else 1)
+            self.offsets[k] = (off, n)
+            off += n
+        if off >= 2 ** 24:
+            raise ValueError("network too large for the float32 index map of ComplexCNN2d")
+        self.flat = torch.nn.Parameter(torch.zeros(off, device=self.device))
+        # signed gather map: real flat element e = sign[e] * self.flat[src[e]]
+        probe_sd = {}
+        for k, t in self.template.items():
+            if k in self.offsets:
+                o, n = self.offsets[k]
+                idx = torch.arange(o + 1, o + n + 1, dtype=torch.float64)
+                probe_sd[k] = torch.view_as_complex(idx.view(*t.shape, 2)) if t.is_complex() else idx.view(t.shape)
+            else:
+                probe_sd[k] = t.clone().double() if t.is_floating_point() else t.clone()
+        self.real.load_state_dict(complex_to_real_state(probe_sd, self.use_skip_connections))
+        code = self.real.flat.data.clone()
+        self.src = (code.abs().round().long() - 1).clamp(min=0)
+        self.sign = torch.sign(code)
+        for pref, (rm, rv) in self.real.running.items():
+            rm.zero_()
+            rv.fill_(1.0)
+        self.real.num_batches_tracked = 0
+        self._init_params(seed)
+
+    @staticmethod
+    def _complex_template(rsd: dict) -> dict:
+        """Complex state-dict entries (names, shapes, dtypes) of the real network's."""
+        bn_prefixes = {k[: -len(".running_mean")] for k in rsd if k.endswith(".running_mean")}
+        out = {}
+        for k, v in rsd.items():
+            pref = k.rsplit(".", 1)[0]
+            field = k.rsplit(".", 1)[1]
+            if pref in bn_prefixes:
+                if field == "num_batches_tracked":
+                    for half in ("real_bn", "imag_bn"):
+                        out[f"{pref}.{half}.{field}"] = v.clone()
+                else:
+                    C = v.shape[0] // 2
+                    for half in ("real_bn", "imag_bn"):
+                        out[f"{pref}.{half}.{field}"] = torch.zeros(C, dtype=torch.float32)
+            elif field == "bias":
+                out[k] = torch.zeros(v.shape[0] // 2, dtype=torch.complex64)
+            elif ".upsample2x." in k:
+                out[k] = torch.zeros((v.shape[0] // 2, v.shape[1] // 2) + tuple(v.shape[2:]), dtype=torch.complex64)
+            else:
+                out[k] = torch.zeros((v.shape[0] // 2, v.shape[1] // 2) + tuple(v.shape[2:]), dtype=torch.complex64)
+        return out
+
+    def _init_params(self, seed):
+        """torch's default initialisation of complex Conv2d / ConvTranspose2d (real and
+        imaginary parts uniform in +-1/sqrt(fan_in)) and of the batch norms (1, 0)."""
+        g = torch.Generator().manual_seed(0 if seed is None else int(seed))
+        flat = torch.zeros(self.flat.numel())
+        for k in self.keys:
+            t = self.template[k]
+            o, n = self.offsets[k]
+            if not t.is_complex():  # batch norm: weight 1, bias 0
+                flat[o:o + n] = 1.0 if k.endswith(".weight") else 0.0
+                continue
+            wkey = k[: -len(".bias")] + ".weight" if k.endswith(".bias") else k
+            w = self.template[wkey]
+            fan_in = (w.shape[0] if ".upsample2x." in wkey else w.shape[1]) * int(math.prod(w.shape[2:]))
+            bound = 1.0 / math.sqrt(fan_in)
+            flat[o:o + n] = (torch.rand(n, generator=g) * 2 - 1) * bound
+        self.flat.data.copy_(flat.to(self.device))
+
+    def _real_flat(self) -> torch.Tensor:
+        return self.sign * self.flat[self.src]
+
+    def train(self, mode: bool = True):
+        self.training = bool(mode)
+        self.real.train(mode)
+        return self
+
+    def eval(self):
+        return self.train(False)
+
+    def forward(self, x: torch.Tensor) -> torch.Tensor:
+        """x: (B, in_channels, H, W) complex; returns (B, out_channels, H, W) complex64."""
+        if not x.is_complex():
+            raise TypeError("ComplexCNN2d takes a complex input")
+        if not x.is_cuda:
+            raise RuntimeError("ComplexCNN2d runs on the CUDA kernels only (no CPU fallback)")
+        xr = torch.cat([x.real, x.imag], dim=1).float().contiguous()
+        w = self._real_flat()
+        self.real.flat.data.copy_(w.detach())
+        y = _CNNFn.apply(xr, w, self.real, None)
+        C = self.out_channels
+        return torch.complex(y[:, :C], y[:, C:])
+
+    __call__ = forward
+
+    def state_dict(self, *args, **kwargs):
+        from .complex_map import real_to_complex_state
+
+        self.real.flat.data.copy_(self._real_flat().detach())
+        return real_to_complex_state(self.real.state_dict(), self.template, self.use_skip_connections)
+
+    def load_state_dict(self, sd, strict: bool = True):
+        from .complex_map import complex_to_real_state
+
+        flat = torch.zeros(self.flat.numel())
+        for k in self.keys:
+            if k not in sd:
+                if strict:
+                    raise KeyError(f"missing key {k}")
+                continue
+            o, n = self.offsets[k]
+            v = torch.as_tensor(sd[k])
+            flat[o:o + n] = (torch.view_as_real(v.to(torch.complex64)) if v.is_complex() else v.float()).reshape(-1)
+        self.flat.data.copy_(flat.to(self.device))
+        full = dict(self.template)
+        full.update({k: torch.as_tensor(v) for k, v in sd.items()})
+        self.real.load_state_dict(complex_to_real_state(full, self.use_skip_connections), strict=False)
+        self.real.flat.data.copy_(self._real_flat().detach())
+        self.real.sync_weights()
+
+    def named_gradients(self) -> dict:
+        """Gradients of the last backward under the reference's names (complex tensors
+        in torch's convention dL/dRe + i dL/dIm)."""
+        if self.flat.grad is None:
+            return {}
+        out = {}
+        for k in self.keys:
+            o, n = self.offsets[k]
+            t = self.template[k]
+            g = self.flat.grad[o:o + n]
+            out[k] = torch.view_as_complex(g.view(*t.shape, 2).contiguous()) if t.is_complex() else g.view(t.shape)
+        return out

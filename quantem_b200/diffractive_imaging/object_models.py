@@ -277,21 +277,24 @@ class ObjectDIP(ObjectPixelated):
     and the network weights are what the optimiser updates.
 
     The network is ``quantem_b200.core.ml.cnn.CNN2d`` (real-valued, BF16 tcgen05
-    kernels); its output (1, S, H, W) is the phase of every slice.  The complex hard
-    constraint of the fused batch loss applied to exp(i phase) is exactly the
-    reference's pure-phase constraint (unit amplitude, mean phase removed,
-    object_models.py:289-300).  Gradients flow from the fused adjoint through
-    exp and the CNN backward kernels by torch autograd; the pixelated-object
-    gradient rescale (ptychography.py:330-332) is not applied, as in the
-    reference.  Complex-valued networks are not part of the B200 path."""
+    kernels).  With a real network (pure-phase or potential objects) its output
+    (1, S, H, W) is the phase / potential of every slice and the transmission is
+    exp(i output); with a complex network (``ComplexCNN2d``, complex objects, the
+    reference's default) the output is the complex object itself.  As in the
+    reference's ObjectDIP.forward (object_models.py:990-1008) the network output enters
+    the patches without the hard constraint (for a real network exp(i phase) goes through
+    the complex constraint kernel, which at unit amplitude only removes the mean phase:
+    a global phase that changes neither the loss nor its gradient); ``obj`` applies the
+    hard constraint of the object type.  Gradients flow from the fused adjoint into the
+    CNN backward kernels by torch autograd; the pixelated-object gradient rescale
+    (ptychography.py:330-332) is not applied, as in the reference."""
 
     def __init__(self, num_slices=1, slice_thicknesses=None, input_noise_std=0.025, device="cuda",
-                 obj_type="pure_phase", rng=None, _token=None):
-        if str(obj_type).lower() != "pure_phase":
-            raise NotImplementedError("ObjectDIP on the B200 path is pure-phase (real CNN2d output = phase)")
+                 obj_type="complex", rng=None, _token=None):
+        t = ObjectPixelated._process_obj_type(obj_type)
         ObjectPixelated.__init__(self, num_slices, slice_thicknesses, "complex", "dip", device, rng,
                                  _token=ObjectPixelated._token)
-        self._obj_type_dip = "pure_phase"
+        self._obj_type_dip = t
         self._model = None
         self._model_input = torch.tensor([])
         self._pretrain_target = torch.tensor([])
@@ -305,27 +308,53 @@ class ObjectDIP(ObjectPixelated):
 
     @classmethod
     def from_model(cls, model, model_input, num_slices: int = 1, slice_thicknesses=None,
-                   input_noise_std: float = 0.025, device="cuda", obj_type="pure_phase", rng=None):
+                   input_noise_std: float = 0.025, device="cuda", obj_type="complex", rng=None):
         """object_models.py:768-794."""
         m = cls(num_slices, slice_thicknesses, input_noise_std, device, obj_type, rng)
         m._model = model
+        if m.is_complex_model and m._obj_type_dip != "complex":
+            raise ValueError("a complex network (ComplexCNN2d) describes a complex object")
         m.model_input = model_input
         m._set_pretrained_weights()
         return m
 
     @classmethod
     def from_pixelated(cls, model, pixelated: ObjectPixelated, input_noise_std: float = 0.025, device=None):
-        """object_models.py:796-834: input and pre-training target = the pixelated object's phase."""
+        """object_models.py:796-834: input and pre-training target = the pixelated object
+        with a complex network; with a real network its potential (potential objects) or
+        its phase (pure-phase objects, and complex objects, whose transmission then is
+        exp(i output): the reference casts a complex object to the real network's dtype
+        here, keeping only its real part, which this path does not reproduce)."""
         if not isinstance(pixelated, ObjectPixelated):
             raise ValueError(f"pixelated must be an ObjectPixelated, got {type(pixelated)}")
-        phase = torch.angle(pixelated.obj.detach()).float()
-        m = cls.from_model(model, phase, num_slices=pixelated.num_slices,
+        complex_model = "complex" in str(getattr(model, "dtype", ""))
+        obj = pixelated.obj.detach()
+        if complex_model:
+            if pixelated.obj_type != "complex":
+                raise ValueError("a complex network (ComplexCNN2d) describes a complex object")
+            target = obj.clone()
+        elif pixelated.obj_type == "potential":
+            target = obj.float().clone()
+        else:
+            target = torch.angle(obj).float()
+        m = cls.from_model(model, target, num_slices=pixelated.num_slices,
                            slice_thicknesses=pixelated.slice_thicknesses.cpu().numpy() if
                            pixelated.slice_thicknesses.numel() else None,
                            input_noise_std=input_noise_std, device=device or pixelated.device,
-                           rng=pixelated._rng_seed)
-        m.pretrain_target = phase
+                           obj_type=pixelated.obj_type, rng=pixelated._rng_seed)
+        m.pretrain_target = target
         return m
+
+    @property
+    def is_complex_model(self) -> bool:
+        return "complex" in str(getattr(self._model, "dtype", ""))
+
+    def transmission_spec(self):
+        """Complex network: the output is the transmission (no hard constraint, as the
+        reference's DIP forward); real network: exp(i output) through the complex kernel."""
+        from .. import ops
+
+        return ops.ObjSpec("complex", hard_constraint=not self.is_complex_model)
 
     # ------------------------------------------------------------------ state
     @property
@@ -334,7 +363,7 @@ class ObjectDIP(ObjectPixelated):
 
     @property
     def obj_type(self) -> str:
-        return "pure_phase"
+        return self._obj_type_dip
 
     @property
     def model(self):
@@ -353,7 +382,8 @@ class ObjectDIP(ObjectPixelated):
 
     @model_input.setter
     def model_input(self, x):
-        x = torch.as_tensor(x).detach().clone().float()
+        x = torch.as_tensor(x).detach().clone()
+        x = x.to(torch.complex64) if self.is_complex_model else x.float()
         if x.shape[-3] != self.num_slices:
             raise ValueError(f"model_input.shape[-3] {x.shape[-3]} does not match num_slices {self.num_slices}")
         if x.ndim == 3:
@@ -375,7 +405,8 @@ class ObjectDIP(ObjectPixelated):
         if t is None:
             self._pretrain_target = torch.tensor([])
             return
-        t = torch.as_tensor(t).float()
+        t = torch.as_tensor(t)
+        t = t.to(torch.complex64) if self.is_complex_model else t.float()
         if t.ndim == 4:
             t = t[0]
         if tuple(t.shape) != tuple(self.model_input.shape[-3:]):
@@ -407,13 +438,18 @@ class ObjectDIP(ObjectPixelated):
         if self._gen is None:
             self._gen = torch.Generator(device=self._model_input.device).manual_seed(
                 int(self._rng_seed) if self._rng_seed is not None else 0)
+        # torch.randn of a complex dtype: real and imaginary parts each N(0, 1/2)
         return self._model_input + torch.randn(self._model_input.shape, generator=self._gen,
-                                               device=self._model_input.device) * self._input_noise_std
+                                               device=self._model_input.device,
+                                               dtype=self._model_input.dtype) * self._input_noise_std
 
     def raw_object(self, noise: bool = True) -> torch.Tensor:
-        """exp(i * model(input (+ noise))[0]) as complex64 (S, H, W), differentiable."""
-        phase = self._model(self._noisy_input(noise))[0]
-        return torch.polar(torch.ones_like(phase), phase)
+        """The network's object as complex64 (S, H, W), differentiable: its output for a
+        complex network, exp(i output) for a real one."""
+        out = self._model(self._noisy_input(noise))[0]
+        if self.is_complex_model:
+            return out.contiguous()
+        return torch.polar(torch.ones_like(out), out)
 
     @property
     def _obj(self) -> torch.Tensor:
@@ -425,8 +461,12 @@ class ObjectDIP(ObjectPixelated):
 
     @property
     def obj(self) -> torch.Tensor:
+        """The network's object with the hard constraint of its type (object_models.py:985-991)."""
         from .. import ops
 
+        if self._obj_type_dip == "potential":
+            v = self._model(self._noisy_input(False))[0]
+            return torch.clamp(v, min=0.0) if self._constraints.get("positivity", True) else v
         return ops.constrained_object(self.raw_object(noise=False))
 
     def _initialize_obj(self, shape, sampling=None):
@@ -485,9 +525,12 @@ class ObjectDIP(ObjectPixelated):
             raise ValueError("No pretrain target set. Provide pretrain_target or set it beforehand.")
         self._model.train()
         opt = self._optimizer
+        tgt = torch.view_as_real(self._pretrain_target) if self.is_complex_model else self._pretrain_target
         for _ in range(num_iters):
             out = self._model(self._noisy_input(True))[0]
-            loss = mse_loss(out, self._pretrain_target)
+            if self.is_complex_model:  # complex_l2: mean over the real and the imaginary parts
+                out = torch.view_as_real(out)
+            loss = mse_loss(out, tgt)
             opt.zero_grad(set_to_none=True)
             loss.backward()
             opt.step()

@@ -105,13 +105,13 @@ def _lite_reconstruct(pt, num_iters, reset, lr_obj, learn_probe, lr_probe, batch
 
 class PtychoLiteDIP(Ptychography):
     """Deep-image-prior variant of PtychoLite (ptychography_lite.py:255-427) on the B200
-    path: the object becomes an ``ObjectDIP`` (CNN2d on the BF16 tcgen05 kernels,
-    pure phase), optionally pre-trained on the PtychoLite object's phase, and the
+    path: the object becomes an ``ObjectDIP`` on the BF16 tcgen05 kernels -- a complex
+    network (``ComplexCNN2d``) for complex objects, a real ``CNN2d`` otherwise, as the
+    reference chooses -- optionally pre-trained on the PtychoLite object, and the
     network weights are optimised through the fused forward / adjoint kernels.
 
-    The probe stays the PtychoLite's pixelated probe: the reference's probe DIP is a
-    complex-valued CNN, which is not part of this path (``pretrain_probe`` therefore
-    has nothing to pre-train).  Complex objects are represented by their phase."""
+    The probe stays the PtychoLite's pixelated probe (the reference's probe DIP is not
+    built here, so ``pretrain_probe`` has nothing to pre-train)."""
 
     @classmethod
     def from_ptycholite(cls, ptycholite: PtychoLite, pretrain_iters: int | None = None, pretrain_lr: float = 1e-3,
@@ -122,7 +122,7 @@ class PtychoLiteDIP(Ptychography):
         """ptychography_lite.py:263-370: CNN2d object model from the pixelated object,
         optional pre-training (AdamW, plateau scheduler), ``from_models`` with the same
         dataset / probe / detector and ``preprocess`` with the same padding."""
-        from ..core.ml.cnn import CNN2d
+        from ..core.ml.cnn import CNN2d, ComplexCNN2d
         from .object_models import ObjectDIP
 
         if log_dir is not None:
@@ -130,8 +130,9 @@ class PtychoLiteDIP(Ptychography):
         if str(device).lower() == "cpu":
             raise ValueError("PtychoLiteDIP runs its CNN on the GPU kernels: device must be 'gpu' or 'cuda'")
         S = ptycholite.obj_model.num_slices
-        net = CNN2d(in_channels=S, out_channels=S, num_layers=cnn_num_layers,
-                    device=torch.device("cuda", torch.cuda.current_device()))
+        dev = torch.device("cuda", torch.cuda.current_device())
+        kind = ComplexCNN2d if ptycholite.obj_model.obj_type == "complex" else CNN2d
+        net = kind(in_channels=S, out_channels=S, num_layers=cnn_num_layers, device=dev)
         obj_model = ObjectDIP.from_pixelated(net, ptycholite.obj_model)
         if pretrain_iters is not None and pretrain_object:
             obj_model.pretrain(reset=True, num_iters=pretrain_iters,

@@ -139,6 +139,10 @@ class ObjSpec:
     positivity: bool = True
     fix_baseline: bool = False
     baseline_factor: float = 1.0
+    # False: the raw complex object is the transmission as it is (the reference's
+    # ObjectDIP.forward feeds the network output to the patches without the hard
+    # constraint, object_models.py:990-1008)
+    hard_constraint: bool = True
 
     def __post_init__(self):
         if self.obj_type not in OBJ_TYPES:
@@ -162,6 +166,10 @@ def obj_transmission(obj: torch.Tensor, spec: ObjSpec = COMPLEX_OBJECT, work: to
     """Transmission (complex64) of a raw object of any type; returns (out, work)."""
     _req(obj, "obj", spec.raw_dtype)
     work = new_constraint_work(obj.device) if work is None else work
+    if not spec.hard_constraint:
+        if spec.obj_type != "complex":
+            raise ValueError("an unconstrained transmission is a complex object")
+        return (obj if out is None else out.copy_(obj)), work
     out = torch.empty(obj.shape, dtype=torch.complex64, device=obj.device) if out is None else out
     _lib.check(_lib.lib().ptycho_obj_transmission(_p(obj), _p(out), obj.numel(), *_spec_args(spec), _p(work),
                                                   work.numel(), _stream()), "obj_transmission")
@@ -174,6 +182,9 @@ def obj_transmission_vjp(obj: torch.Tensor, grad_t: torch.Tensor, work: torch.Te
     transmission is ``grad_t``; ``work`` from the matching ``obj_transmission`` call."""
     _req(obj, "obj", spec.raw_dtype)
     _req(grad_t, "grad_t", torch.complex64)
+    if not spec.hard_constraint:  # identity transmission
+        g = grad_t if scale is None else grad_t * scale.detach().to(torch.float32)
+        return g.clone() if out is None else out.copy_(g)
     out = torch.empty_like(obj) if out is None else out
     if scale is not None:
         scale = scale.detach().to(torch.float32).contiguous()

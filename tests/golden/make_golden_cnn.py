@@ -65,13 +65,78 @@ def run_case(name, cfg):
     print(name, "params", sum(p.numel() for p in net.parameters()))
 
 
+def _to_fp64(net):
+    """complex parameters / buffers to complex128, real ones to float64 (Module.double()
+    leaves complex tensors alone and Module.to(complex128) would make the batch norms
+    complex)."""
+    import torch
+
+    for mod in net.modules():
+        for name, t in list(mod._parameters.items()) + list(mod._buffers.items()):
+            if t is None:
+                continue
+            if t.is_complex():
+                t.data = t.data.to(torch.complex128)
+            elif t.is_floating_point():
+                t.data = t.data.double()
+    return net
+
+
+def run_complex_case(name, cfg):
+    """A complex CNN2d (dtype=complex64: complex convolutions, ComplexBatchNorm2D,
+    Complex_ReLU, complex pooling), run in complex128: the loss is
+    Re(sum(conj(dy) * y)), so every recorded gradient follows torch's complex
+    convention (dL/dRe + i dL/dIm)."""
+    import torch
+    from quantem.core.ml.cnn import CNN2d
+
+    cin, cout, sf, L, npl, skip, bn, B, H, W = cfg
+    torch.manual_seed(4321 + len(name))
+    net = _to_fp64(CNN2d(cin, cout, start_filters=sf, num_layers=L, num_per_layer=npl, use_skip_connections=skip,
+                         use_batchnorm=bn, dtype=torch.complex64))
+    net.train()
+    g = torch.Generator().manual_seed(77)
+
+    def crandn(*shape):
+        return torch.complex(torch.randn(*shape, generator=g, dtype=torch.float64),
+                             torch.randn(*shape, generator=g, dtype=torch.float64))
+
+    x = crandn(B, cin, H, W).requires_grad_(True)
+    dy = crandn(B, cout, H, W)
+    sd0 = {k: v.detach().clone() for k, v in net.state_dict().items()}
+    y = net(x)
+    (torch.conj(dy) * y).real.sum().backward()
+    out = {"x": x.detach().numpy(), "dy": dy.numpy(), "y_train": y.detach().numpy(),
+           "dx": x.grad.numpy(), "config": np.array(cfg[:5] + (int(skip), int(bn)), dtype=np.int64)}
+    for k, v in sd0.items():
+        out["sd/" + k] = v.numpy()
+    for k, p in net.named_parameters():
+        out["grad/" + k] = p.grad.numpy() if p.grad is not None else np.zeros(tuple(p.shape), p.detach().numpy().dtype)
+    for k, v in net.state_dict().items():
+        if "running" in k:
+            out["after/" + k] = v.numpy()
+    net.eval()
+    with torch.no_grad():
+        out["y_eval"] = net(x.detach()).numpy()
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+    print(name, "params", sum(p.numel() for p in net.parameters()))
+
+
+COMPLEX_CASES = {
+    "cnn_complex_unet2": (2, 2, 8, 2, 2, True, True, 2, 16, 16),
+}
+
+
 def main():
     if len(sys.argv) != 2:
         sys.exit(f"usage: python {os.path.relpath(__file__)} <reference source dir (the one holding quantem/)>")
     src = sys.argv[1]
     import_reference(src)
-    for name, cfg in CASES.items():
-        run_case(name, cfg)
+    if os.environ.get("GOLDEN_ONLY") != "complex":
+        for name, cfg in CASES.items():
+            run_case(name, cfg)
+    for name, cfg in COMPLEX_CASES.items():
+        run_complex_case(name, cfg)
 
 
 if __name__ == "__main__":

@@ -45,3 +45,43 @@ def test_bf16_rounding():
     assert r[2] == 1.0078125
     assert abs(r[3] + 3.140625) < 1e-12
     assert np.isinf(r[6])
+
+
+def test_complex_cnn_is_the_real_network_with_block_weights():
+    """The reference's complex CNN2d (tests/golden/cnn_complex_unet2.npz) equals the real
+    CNN2d with doubled channels and [[A, -B], [B, A]] weights
+    (quantem_b200.core.ml.complex_map): the FP64 oracle run on that real network
+    reproduces the complex outputs, input and parameter gradients and running
+    statistics of the reference to 1e-12."""
+    import torch
+
+    from quantem_b200.core.ml.complex_map import complex_to_real_state, real_grads_to_complex
+
+    z = load_golden("cnn_complex_unet2")
+    cfg = [int(c) for c in z["config"]]
+    cin, cout, sf, L, npl, skip, bn = cfg
+    sd = {k[3:]: torch.as_tensor(z[k]) for k in z if k.startswith("sd/")}
+    rsd = {k: v.numpy() for k, v in complex_to_real_state(sd, bool(skip)).items()}
+    net = CNN2dOracle(rsd, 2 * cin, 2 * cout, 2 * sf, L, npl, use_skip_connections=bool(skip),
+                      use_batchnorm=bool(bn))
+    x = z["x"]
+    y = net.forward(np.concatenate([x.real, x.imag], axis=1), training=True)
+    assert _rel(y[:, :cout] + 1j * y[:, cout:], z["y_train"]) < 1e-12
+    dy = z["dy"]
+    dx, grads = net.backward(np.concatenate([dy.real, dy.imag], axis=1))
+    assert _rel(dx[:, :cin] + 1j * dx[:, cin:], z["dx"]) < 1e-12
+    cg = real_grads_to_complex({k: torch.as_tensor(v) for k, v in grads.items()}, sd, bool(skip))
+    gscale = np.sqrt(sum(np.linalg.norm(z[k]) ** 2 for k in z if k.startswith("grad/")))
+    for k in z:
+        if k.startswith("grad/"):
+            assert np.linalg.norm(cg[k[5:]].numpy() - z[k]) <= 1e-12 * gscale, k
+    back = {}
+    for k in z:
+        if k.startswith("after/"):
+            name = k[6:]
+            pref, half, field = name.rsplit(".", 2)
+            full = net.sd[f"{pref}.{field}"]
+            C = full.shape[0] // 2
+            assert _rel(full[:C] if half == "real_bn" else full[C:], z[k]) < 1e-12, k
+    y_eval = net.forward(np.concatenate([x.real, x.imag], axis=1), training=False)
+    assert _rel(y_eval[:, :cout] + 1j * y_eval[:, cout:], z["y_eval"]) < 1e-12

@@ -33,6 +33,12 @@ def _rel(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
 
+def _crel(a, b):
+    a = np.asarray(a, dtype=np.complex128)
+    b = np.asarray(b, dtype=np.complex128)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
 def _cfg(z):
     c = [int(v) for v in z["config"]]
     return dict(in_channels=c[0], out_channels=c[1], start_filters=c[2], num_layers=c[3], num_per_layer=c[4],
@@ -243,3 +249,53 @@ def test_cnn_training_reduces_loss(cuda_device):
         opt.step()
         losses.append(float(loss.item()))
     assert losses[-1] < 0.5 * losses[0]
+
+
+def test_complex_cnn_matches_reference(cuda_device):
+    """ComplexCNN2d (the reference's dtype=complex64 CNN2d on the tcgen05 kernels, as a
+    real network with block weights) against the reference's own complex network,
+    with the same bar as the real networks (1.5x the exact BF16 model's distance to
+    FP64 + 5e-3); the exact BF16 model is the oracle on the real-equivalent network."""
+    from quantem_b200.core.ml.cnn import ComplexCNN2d
+    from quantem_b200.core.ml.complex_map import complex_to_real_state, real_grads_to_complex
+
+    z = load_golden("cnn_complex_unet2")
+    c = [int(v) for v in z["config"]]
+    cin, cout, sf, L, npl, skip, bn = c
+    sd = {k[3:]: torch.as_tensor(z[k]) for k in z if k.startswith("sd/")}
+    net = ComplexCNN2d(cin, cout, start_filters=sf, num_layers=L, num_per_layer=npl, use_skip_connections=bool(skip),
+                       use_batchnorm=bool(bn), device=cuda_device)
+    net.load_state_dict(sd)
+    back = net.state_dict()
+    for k, v in sd.items():  # the state round trip (weights through the FP32 master copy)
+        if v.dtype != torch.int64:
+            assert _crel(back[k].numpy(), v.numpy().astype(back[k].numpy().dtype)) < 1e-7, k
+    net.train()
+    x = torch.as_tensor(z["x"], dtype=torch.complex64, device=cuda_device).requires_grad_(True)
+    y = net(x)
+    dy = torch.as_tensor(z["dy"], dtype=torch.complex64, device=cuda_device)
+    (torch.conj(dy) * y).real.sum().backward()
+    torch.cuda.synchronize()
+    y = y.detach().cpu().numpy()
+    dx = x.grad.cpu().numpy()
+    g = {k: v.cpu().numpy() for k, v in net.named_gradients().items()}
+    keys = sorted(k[5:] for k in z if k.startswith("grad/"))
+    rsd = {k: v.numpy() for k, v in complex_to_real_state(sd, bool(skip)).items()}
+    orc = CNN2dOracle(rsd, 2 * cin, 2 * cout, 2 * sf, L, npl, use_skip_connections=bool(skip),
+                      use_batchnorm=bool(bn), emulate_bf16=True)
+    xs = np.concatenate([z["x"].real, z["x"].imag], axis=1)
+    yo = orc.forward(xs, training=True)
+    dxo, go = orc.backward(np.concatenate([z["dy"].real, z["dy"].imag], axis=1))
+    yo = yo[:, :cout] + 1j * yo[:, cout:]
+    dxo = dxo[:, :cin] + 1j * dxo[:, cin:]
+    gco = {k: v.numpy() for k, v in real_grads_to_complex({k: torch.as_tensor(v) for k, v in go.items()}, sd,
+                                                          bool(skip)).items()}
+    bar = lambda model_err: 1.5 * model_err + 5e-3  # noqa: E731
+
+    def flat(d):
+        return np.concatenate([np.asarray(d[k]).astype(np.complex128).ravel() for k in keys])
+
+    gref = flat({k: z["grad/" + k] for k in keys})
+    assert _crel(y, z["y_train"]) < bar(_crel(yo, z["y_train"]))
+    assert _crel(dx, z["dx"]) < bar(_crel(dxo, z["dx"]))
+    assert _crel(flat(g), gref) < bar(_crel(flat(gco), gref))

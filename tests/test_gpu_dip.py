@@ -72,3 +72,61 @@ def test_dip_pretrain_and_reconstruct(cuda_device):
     assert losses.shape == (3,) and np.all(np.isfinite(losses))
     assert losses[-1] < losses[0]
     assert float((net.flat.detach() - w0).abs().max()) > 0  # the network weights are what moved
+
+
+def test_complex_dip_chain_matches_fp64_oracle(cuda_device):
+    """A complex network's output is the transmission itself (no hard constraint in the
+    reference's DIP forward): dL/d(output) through the fused adjoint equals the oracle's
+    batch gradient at that object."""
+    from quantem_b200 import ops
+
+    rng = np.random.default_rng(33)
+    S, P, n, Ho, B = 2, 2, 64, 96, 6
+    z = (1.1 - 0.4 * rng.random((S, Ho, Ho))) * np.exp(1j * 0.4 * rng.standard_normal((S, Ho, Ho)))
+    probe = rng.standard_normal((P, n, n)) + 1j * rng.standard_normal((P, n, n))
+    probe *= np.exp(-((np.fft.fftfreq(n) * n)[:, None] ** 2 + (np.fft.fftfreq(n) * n)[None] ** 2) / 100.0)
+    props = O.propagators((n, n), (0.2, 0.2), 300e3, [20.0] * (S - 1))
+    pos = rng.uniform(0, Ho, size=(B, 2)).astype(np.float32).astype(np.float64)
+    tg = np.abs(rng.standard_normal((B, n, n))) * 3
+    loss_o, g_o, _, _ = O.batch_loss_and_grads(z, probe, pos, props, tg, np.ones((n, n)), 400, 30.0)
+    dev = cuda_device
+    zt = torch.tensor(z.astype(np.complex64), device=dev, requires_grad=True)
+    loss = ops.batch_loss(zt, torch.as_tensor(probe.astype(np.complex64), device=dev),
+                          torch.as_tensor(props.astype(np.complex64), device=dev),
+                          torch.as_tensor(pos, dtype=torch.float32, device=dev),
+                          torch.arange(B, device=dev, dtype=torch.int64),
+                          torch.as_tensor(tg, dtype=torch.float32, device=dev), torch.ones((n, n), device=dev),
+                          400, 30.0, obj_spec=ops.ObjSpec("complex", hard_constraint=False))
+    loss.backward()
+    assert abs(loss.item() - loss_o) / loss_o < 1e-5
+    assert rel(zt.grad.cpu().numpy(), g_o) < 1e-4
+
+
+def test_complex_dip_pretrain_and_reconstruct(cuda_device):
+    """PtychoLiteDIP-style use with the reference's default complex object: a complex
+    network (ComplexCNN2d) pre-trained on the pixelated complex object, then optimised
+    through Ptychography.reconstruct."""
+    from quantem_b200.core.ml.cnn import ComplexCNN2d
+    from quantem_b200.diffractive_imaging import ObjectDIP, Ptychography
+
+    z = load_golden("mixed64")
+    base = build_from_golden(z, device="cuda")
+    base.reconstruct(num_iters=2, optimizer_params={"object": {"type": "adam", "lr": 5e-3},
+                                                    "probe": {"type": "adam", "lr": 1e-3}}, batch_size=8)
+    S = base.obj_model.num_slices
+    net = ComplexCNN2d(S, S, start_filters=8, num_layers=3, device=cuda_device, seed=4)
+    dip = ObjectDIP.from_pixelated(net, base.obj_model, input_noise_std=0.0)
+    assert dip.obj_type == "complex" and dip.model_input.dtype == torch.complex64
+    dip.pretrain(num_iters=60, optimizer_params={"type": "adam", "lr": 3e-3})
+    pl = dip.pretrain_losses
+    assert pl[-1] < 0.2 * pl[0]
+    assert tuple(dip.obj.shape) == tuple(base.obj_model.shape) and dip.obj.dtype == torch.complex64
+    pt = Ptychography.from_models(dset=base.dset, obj_model=dip, probe_model=base.probe_model,
+                                  detector_model=base.detector_model, device="gpu", verbose=0, rng=3)
+    pt.preprocess(obj_padding_px=base.obj_padding_px)
+    w0 = net.flat.detach().clone()
+    pt.reconstruct(num_iters=3, optimizer_params={"object": {"type": "adam", "lr": 1e-3}}, batch_size=8)
+    losses = np.asarray(pt.iter_losses)
+    assert losses.shape == (3,) and np.all(np.isfinite(losses))
+    assert losses[-1] < losses[0]
+    assert float((net.flat.detach() - w0).abs().max()) > 0
