@@ -72,6 +72,10 @@ def test_ptycholite_dip_from_ptycholite(cuda_device):
 
     dip = PtychoLiteDIP.from_ptycholite(lite, pretrain_iters=40, pretrain_lr=3e-3, device="gpu", verbose=0)
     assert isinstance(dip.obj_model, ObjectDIP)
+    # a complex PtychoLite object gets a complex network, as in the reference
+    from quantem_b200.core.ml.cnn import ComplexCNN2d
+
+    assert isinstance(dip.obj_model.model, ComplexCNN2d) and dip.obj_model.obj_type == "complex"
     assert dip.probe_model is lite.probe_model and dip.dset is lite.dset
     assert tuple(dip.obj_model.obj.shape) == tuple(lite.obj_model.obj.shape)
     pl = dip.obj_model.pretrain_losses
