@@ -959,6 +959,16 @@ def run_c4_gemm(args):
                       "gbs": round(byt / s_ / 1e9, 1), "tflops": round(2 * M * N * K / s_ / 1e12, 2)}))
 
 
+def c5_config(scan=(128, 128)):
+    """Large multislice: 1024 x 1024 x 16 object, 6 modes at 256^2, 6 px raster step with
+    +-0.5 px jitter, 1e6 counts; the padding keeps the object at 1024^2 for any scan."""
+    from quantem_b200 import synthetic
+
+    pad = (1024 - (scan[0] - 1) * 6) // 2
+    return synthetic.SyntheticConfig(n=256, slices=16, modes=6, mode_weights=(0.5, 0.2, 0.1, 0.08, 0.07, 0.05),
+                                     scan=scan, step_px=6.0, pad_px=pad, counts=1e6, seed=0)
+
+
 def run_c5(args):
     """Large multislice: 1024x1024x16 object, 6 modes at 256x256 on 4-CTA clusters, 128x128 scan
     (16384 positions, 6 px step, jitter), 1e6 counts, full-batch Adam iterations.  The
@@ -970,8 +980,7 @@ def run_c5(args):
     from quantem_b200.diffractive_imaging.ptycho_utils import SimpleBatcher
 
     dev = torch.device("cuda", 0)
-    cfg = synthetic.SyntheticConfig(n=256, slices=16, modes=6, mode_weights=(0.5, 0.2, 0.1, 0.08, 0.07, 0.05),
-                                    scan=(128, 128), step_px=6.0, pad_px=131, counts=1e6, seed=0)
+    cfg = c5_config()
     t0 = time.time()
     ds = synthetic.make_dataset(cfg, dev)
     torch.cuda.synchronize()
@@ -1014,8 +1023,15 @@ def run_c5(args):
             "scratch_gb": round(ws.scratch.numel() * 8 / 1e9, 3)}
         del pt, opts, obj, probe
         torch.cuda.empty_cache()
+    del ds
+    torch.cuda.empty_cache()
+    # the reference's own iteration at this geometry, in a fresh process, on a 32 x 32 sub-scan
+    # (1024 positions; same object, probe and slices), the batch halved from 1024 until it fits
+    ref = None if args.skip_torch_reference else reference_torch_gpu_subprocess(
+        0, 1024, steps=2, warmup=1, extra=["--workload", "c5"])
     print(json.dumps({
         "metric": METRIC, "value": out["recompute_every_4"]["positions_per_s"], "unit": "positions/s",
+        "reference_torch_gpu": ref,
         "higher_is_better": True, "data": "synthetic",
         "config": {"workload": "c5: 1024x1024x16 object, 6 modes at 256x256 (4-CTA cluster FFT), 128x128 scan, "
                                "16384 positions, full batch, Adam", "simulate_s": round(sim_s, 2)},
@@ -1276,7 +1292,8 @@ def run_reference_torch_gpu(args):
     from quantem_b200 import synthetic
 
     c1 = args.workload == "c1"
-    cfg = c1_config() if c1 else synthetic.SyntheticConfig(seed=0)
+    c5 = args.workload == "c5"
+    cfg = c1_config() if c1 else (c5_config(scan=(32, 32)) if c5 else synthetic.SyntheticConfig(seed=0))
     device = "cuda:0" if args.ref_device == "gpu" else "cpu"
     if device == "cpu":
         torch.set_num_threads(os.cpu_count() or 1)
@@ -1285,7 +1302,8 @@ def run_reference_torch_gpu(args):
     line = {"metric": METRIC, "unit": "positions/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64/f32",
             "data": "synthetic", "impl": "reference", "device": args.ref_device,
-            "config": {"workload": "c1" if c1 else WORKLOAD, "parallelism": "replicas1"}}
+            "config": {"workload": "c1" if c1 else ("c5 geometry, 32x32 sub-scan" if c5 else WORKLOAD),
+                       "parallelism": "replicas1"}}
     if "unavailable" in res:
         line["unavailable"] = res["unavailable"]
     else:

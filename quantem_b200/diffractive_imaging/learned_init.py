@@ -9,10 +9,12 @@ iterative reconstruction (ptychography.py:146-308) refines it.
   GPU (``ptycho_cnn_bin_features``), giving (n/bin)^2 channels per scan position
   on the (scan rows x scan columns) grid; per-channel mean and a global scale,
   fixed from the first training batch, normalise them.
-* Output: sub x sub channels per scan position (sub = scan step in pixels), the
-  projected phase sum_s phi_s on the sub x sub object pixels around the
-  position (rows p - sub/2 ... p + sub/2 - 1); depth-to-space gives a
-  (sub*rows, sub*cols) phase map covering the scanned field of view.
+* Output: S x sub x sub channels per scan position (sub = scan step in pixels):
+  the phase phi_s of every slice on the sub x sub object pixels around the
+  position (rows p - sub/2 ... p + sub/2 - 1); depth-to-space gives one
+  (sub*rows, sub*cols) phase map per slice covering the scanned field of view.
+  (``per_slice=False``: the projected phase sum_s phi_s only, split evenly over
+  the slices at use.)
 * Training pairs come from the method's own forward model: random
   Gaussian-atom multislice objects (atom density and peak phase drawn per
   object), simulated through ``ptycho_forward_loss`` with the experiment's probe
@@ -20,8 +22,8 @@ iterative reconstruction (ptychography.py:146-308) refines it.
   simulates fresh objects (nothing is stored), so N training objects cost N
   forward simulations.  The network trains with the tcgen05 BF16 kernels and the
   fused Adam step.
-* Use: ``initial_object`` splits the predicted projected phase evenly over the
-  slices.  The plain reconstruction is the fallback and the judge: the forward
+* Use: ``initial_object`` sets every slice to exp(i phi_s) of its predicted phase.
+  The plain reconstruction is the fallback and the judge: the forward
   model's loss on the measured data is evaluated for the learned and the flat
   start, and the flat object is returned when the learned one fits worse.
 """
@@ -55,6 +57,7 @@ class LearnedInitConfig:
     lr: float = 1e-3
     batch_objects: int = 16
     zero_mean_target: bool = True    # the reconstruction fixes the mean phase: learn the structure only
+    per_slice: bool = True           # predict every slice's phase (else the projected phase)
 
 
 class LearnedInitializer:
@@ -76,8 +79,9 @@ class LearnedInitializer:
             raise ValueError("probe size must equal cfg.n and be divisible by cfg.bin")
         self.C = (c.n // c.bin) ** 2
         self.sub = int(c.step_px)
-        self.net = CNN2d(self.C, self.sub * self.sub, start_filters=c.start_filters, num_layers=c.num_layers,
-                         num_per_layer=c.num_per_layer, device=self.device, seed=seed)
+        self.depth = self.S if c.per_slice else 1  # phase maps predicted per position
+        self.net = CNN2d(self.C, self.depth * self.sub * self.sub, start_filters=c.start_filters,
+                         num_layers=c.num_layers, num_per_layer=c.num_per_layer, device=self.device, seed=seed)
         self.opt = FusedAdam([self.net.flat], lr=c.lr)
         self.gen = torch.Generator(device=self.device).manual_seed(seed + 1)
         self.feat_mean = None
@@ -95,7 +99,7 @@ class LearnedInitializer:
 
     def simulate(self, nobj: int):
         """Fresh training pairs: (BF16 feature rows (nobj*crop^2, C), FP32 targets
-        (nobj, sub^2, crop, crop))."""
+        (nobj, depth*sub^2, crop, crop), depth = S per-slice maps or 1 projected map)."""
         c = self.cfg
         crop = c.scan_crop
         pad, ho = self._crop_geometry(crop)
@@ -107,7 +111,8 @@ class LearnedInitializer:
         mask = torch.ones((c.n, c.n), device=dev)
         dummy = torch.zeros((npos, c.n, c.n), device=dev)
         rows = torch.empty((nobj * npos, self.C), dtype=torch.bfloat16, device=dev)
-        targets = torch.empty((nobj, self.sub * self.sub, crop, crop), device=dev)
+        D = self.depth
+        targets = torch.empty((nobj, D * self.sub * self.sub, crop, crop), device=dev)
         off = torch.arange(self.sub, device=dev) - self.sub // 2
         ti = (nominal[:, 0].long().view(crop, crop, 1, 1) + off.view(1, 1, -1, 1))
         tj = (nominal[:, 1].long().view(crop, crop, 1, 1) + off.view(1, 1, 1, -1))
@@ -128,11 +133,11 @@ class LearnedInitializer:
             else:
                 inten = inten * (1e5 / inten.sum(dim=(-2, -1)).mean())
             self._features(inten.contiguous(), rows[b * npos:(b + 1) * npos])
-            proj = phase.sum(0).float()
-            t = proj[ti, tj]  # (crop, crop, sub, sub)
+            maps = phase.float() if c.per_slice else phase.sum(0, keepdim=True).float()  # (D, ho, ho)
+            t = maps[:, ti, tj]  # (D, crop, crop, sub, sub)
             if c.zero_mean_target:
-                t = t - t.mean()
-            targets[b] = t.permute(2, 3, 0, 1).reshape(self.sub * self.sub, crop, crop)
+                t = t - t.mean(dim=(1, 2, 3, 4), keepdim=True)
+            targets[b] = t.permute(0, 3, 4, 1, 2).reshape(D * self.sub * self.sub, crop, crop)
         return rows, targets
 
     def _features(self, patterns: torch.Tensor, out: torch.Tensor, amplitudes: bool = False):
@@ -179,15 +184,19 @@ class LearnedInitializer:
         return self.history
 
     @torch.no_grad()
-    def evaluate(self, nobj: int = 8, batch_stats: bool = False) -> float:
+    def evaluate(self, nobj: int = 8, batch_stats: bool = False, projected: bool = True) -> float:
         """Mean phase NRMSE (mean-removed) of the prediction on fresh simulated crops
-        (eval-mode batch norm unless ``batch_stats``)."""
+        (eval-mode batch norm unless ``batch_stats``): of the projected phase (the sum
+        of the per-slice maps) with ``projected``, else of all per-slice maps."""
         c = self.cfg
         rows, tgt = self.simulate(nobj)
         if not batch_stats:
             self.net.eval()
         pred = self.net(rows, rows=(nobj, c.scan_crop, c.scan_crop))
         self.net.train()
+        if projected and self.depth > 1:
+            shp = (nobj, self.depth, self.sub * self.sub, c.scan_crop, c.scan_crop)
+            pred, tgt = pred.reshape(shp).sum(1), tgt.reshape(shp).sum(1)
         p = pred.reshape(nobj, -1).double()
         t = tgt.reshape(nobj, -1).double()
         d = (p - p.mean(1, keepdim=True)) - (t - t.mean(1, keepdim=True))
@@ -196,8 +205,9 @@ class LearnedInitializer:
     # ------------------------------------------------------------------ inference
     @torch.no_grad()
     def predict_phase_map(self, patterns: torch.Tensor, scan: tuple, amplitudes: bool = True) -> torch.Tensor:
-        """(sub*rows, sub*cols) projected phase over the scanned field from the
-        measured patterns (npos, n, n) in detector layout, raster order."""
+        """(depth, sub*rows, sub*cols) phase maps over the scanned field (per slice, or the
+        projected phase) from the measured patterns (npos, n, n) in detector layout,
+        raster order."""
         rows_n, cols_n = scan
         f = 2 ** self.cfg.num_layers
         if rows_n % f or cols_n % f:
@@ -205,26 +215,31 @@ class LearnedInitializer:
         self.net.eval()
         x = torch.empty((rows_n * cols_n, self.C), dtype=torch.bfloat16, device=self.device)
         self._features(patterns.float().contiguous(), x, amplitudes=amplitudes)
-        out = self.net(x, rows=(1, rows_n, cols_n))[0]  # (sub^2, rows, cols)
-        s = self.sub
-        return out.view(s, s, rows_n, cols_n).permute(2, 0, 3, 1).reshape(rows_n * s, cols_n * s)
+        out = self.net(x, rows=(1, rows_n, cols_n))[0]  # (depth*sub^2, rows, cols)
+        s, D = self.sub, self.depth
+        return out.view(D, s, s, rows_n, cols_n).permute(0, 3, 1, 4, 2).reshape(D, rows_n * s, cols_n * s)
 
     @torch.no_grad()
     def initial_object(self, patterns: torch.Tensor, scan: tuple, obj_shape: tuple, origin_px: tuple,
                        amplitudes: bool = True, judge: dict | None = None) -> torch.Tensor:
-        """Complex (S, Ho, Wo) start: exp(i phi / S) per slice inside the scanned
-        field (scan position (0, 0) at object pixel ``origin_px``), 1 elsewhere.
+        """Complex (S, Ho, Wo) start: exp(i phi_s) for every slice (exp(i phi / S) from a
+        projected-phase network) inside the scanned field (scan position (0, 0) at
+        object pixel ``origin_px``), 1 elsewhere.
 
         ``judge`` (optional dict with positions, targets, probe, prop, mask,
         mean_intensity, batch of indices) makes the plain forward model decide:
         the flat object is returned when its data loss is lower."""
         S, Ho, Wo = obj_shape
         ph = self.predict_phase_map(patterns, scan, amplitudes)
-        full = torch.zeros((Ho, Wo), device=self.device)
+        if ph.shape[0] not in (1, S):
+            raise ValueError(f"the network predicts {ph.shape[0]} slices, the object has {S}")
+        full = torch.zeros((ph.shape[0], Ho, Wo), device=self.device)
         r0 = int(origin_px[0]) - self.sub // 2
         c0 = int(origin_px[1]) - self.sub // 2
-        full[r0:r0 + ph.shape[0], c0:c0 + ph.shape[1]] = ph
-        obj = torch.exp(1j * (full / S)).to(torch.complex64).expand(S, Ho, Wo).contiguous()
+        full[:, r0:r0 + ph.shape[1], c0:c0 + ph.shape[2]] = ph
+        if ph.shape[0] == 1:
+            full = (full / S).expand(S, Ho, Wo)
+        obj = torch.exp(1j * full).to(torch.complex64).contiguous()
         self.used_learned = True
         if judge is not None:
             flat = torch.ones_like(obj)
