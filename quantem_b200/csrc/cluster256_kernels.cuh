@@ -49,6 +49,7 @@ __global__ void __launch_bounds__(512, 1) cluster256_kernel(const BatchParams p)
   int* colmap = rowmap + N;
   float* inten = reinterpret_cast<float*>(colmap + N);
   __shared__ double red[32];
+  __shared__ int nfred[32];  // per-warp non-finite counts
 
   const int tid = threadIdx.x;
   const int q = (int)cl.block_rank();
@@ -312,15 +313,22 @@ __global__ void __launch_bounds__(512, 1) cluster256_kernel(const BatchParams p)
   }
 
   for (int o = 16; o > 0; o >>= 1) loss_acc += __shfl_xor_sync(0xffffffffu, loss_acc, o);
-  if ((tid & 31) == 0) red[tid >> 5] = loss_acc;
+  // one status update per CTA: per-thread updates of a shared word contend and can drop counts
+  const int nf_warp = __reduce_add_sync(0xffffffffu, nonfinite);
+  if ((tid & 31) == 0) {
+    red[tid >> 5] = loss_acc;
+    nfred[tid >> 5] = nf_warp;
+  }
   __syncthreads();
   if (tid == 0) {
+    int nf = 0;
+    for (int w = 0; w < T / 32; ++w) nf += nfred[w];
+    status_add_nonfinite(p.status, nf);
     double t = 0.0;
     for (int w = 0; w < T / 32; ++w) t += red[w];
     // l1/l2: sum / (B / num_gpts) / mean_I ; poisson: sum / mean_I
     p.loss_part[blockIdx.x] = t * (double)(p.loss_type == LOSS_POISSON ? p.inv_mean_intensity : p.loss_scale);
   }
-  status_add_nonfinite(p.status, nonfinite);
   cl.sync();  // no CTA leaves while a peer may still write into its shared memory
 }
 

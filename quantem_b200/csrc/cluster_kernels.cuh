@@ -42,6 +42,7 @@ __global__ void __launch_bounds__(4 * N, 1) cluster_batch_kernel(const BatchPara
   float2* sKc = sKr + (size_t)N * (p.S > 1 ? p.S - 1 : 0);
   const bool sep = p.prop_r != nullptr;
   __shared__ double red[32];
+  __shared__ int nfred[32];  // per-warp non-finite counts
 
   const int tid = threadIdx.x;
   F f;
@@ -139,7 +140,7 @@ __global__ void __launch_bounds__(4 * N, 1) cluster_batch_kernel(const BatchPara
 #pragma unroll
           for (int e = 0; e < E; ++e) ow[f.s1_col(e)] = x[e];
         }
-        gather_mul<N, false>(f, x, orow_ptr, colmap);
+        gather_mul<N, false>(f, x, orow_ptr, colmap, evict_last_policy());
         if (s == S - 1 && p.out_exit) {
           float2* oe = p.out_exit + ((size_t)m * p.B + b) * NN + (size_t)f.s1_r * N;
 #pragma unroll
@@ -169,7 +170,7 @@ __global__ void __launch_bounds__(4 * N, 1) cluster_batch_kernel(const BatchPara
           atomicAdd(grow_s + (size_t)rowmap[r] * p.Wo + colmap[c], a);
         }
         cluster.sync();  // all tiles read before any exchange buffer is reused
-        gather_mul<N, true>(f, x, orow_ptr, colmap);
+        gather_mul<N, true>(f, x, orow_ptr, colmap, evict_last_policy());
       }
       f.forward(x, sm, tw);
       // ---------------- Fourier space (S3 layout) ----------------
@@ -227,14 +228,21 @@ __global__ void __launch_bounds__(4 * N, 1) cluster_batch_kernel(const BatchPara
   }
 
   for (int o = 16; o > 0; o >>= 1) loss_acc += __shfl_xor_sync(0xffffffffu, loss_acc, o);
-  if ((tid & 31) == 0) red[tid >> 5] = loss_acc;
+  // one status update per CTA: per-thread updates of a shared word contend and can drop counts
+  const int nf_warp = __reduce_add_sync(0xffffffffu, nonfinite);
+  if ((tid & 31) == 0) {
+    red[tid >> 5] = loss_acc;
+    nfred[tid >> 5] = nf_warp;
+  }
   __syncthreads();
   if (tid == 0) {
+    int nf = 0;
+    for (int w = 0; w < T / 32; ++w) nf += nfred[w];
+    status_add_nonfinite(p.status, nf);
     double t = 0.0;
     for (int w = 0; w < T / 32; ++w) t += red[w];
     p.loss_part[blockIdx.x] = t * (double)(p.loss_type == LOSS_POISSON ? p.inv_mean_intensity : p.loss_scale);
   }
-  status_add_nonfinite(p.status, nonfinite);
   cluster.sync();  // no CTA exits while another may still read its shared memory
 }
 

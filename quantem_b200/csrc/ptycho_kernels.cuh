@@ -96,64 +96,20 @@ __device__ __forceinline__ int wrap_index(int x, int n) {
   return x < 0 ? x + n : x;
 }
 
-// ---- experimental switches (defaults = current behaviour) ----
-#ifndef QB_LIFO
-#define QB_LIFO 0
-#endif
-#ifndef QB_OBJ_HINT
-#define QB_OBJ_HINT 0
-#endif
-#ifndef QB_DISCARD
-#define QB_DISCARD 0
-#endif
-#ifndef QB_PREFETCH
-#define QB_PREFETCH 0
-#endif
-#ifndef QB_PF_ELEMS
-#define QB_PF_ELEMS 16
-#endif
-constexpr int kPrefetchElems = QB_PF_ELEMS;  // object values per thread staged by cp.async
-
+// Object patches are re-read by every mode and slice of a position and by the
+// neighbouring positions of the batch: keep them in L2 (evict-last policy) while the
+// saved waves and the measured targets stream through it.  Measured on the full
+// 4096-position batch: 29.58 -> 29.29 ms (with the reversed adjoint mode order).
 __device__ __forceinline__ uint64_t evict_last_policy() {
   uint64_t pol;
   asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
   return pol;
 }
 __device__ __forceinline__ float2 ld_obj(const float2* ptr, uint64_t pol) {
-#if QB_OBJ_HINT
   float2 v;
   asm("ld.global.nc.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;" : "=f"(v.x), "=f"(v.y) : "l"(ptr), "l"(pol));
   return v;
-#else
-  (void)pol;
-  return __ldg(ptr);
-#endif
 }
-__device__ __forceinline__ float ld_stream(const float* ptr) {
-#if QB_OBJ_HINT
-  return __ldcs(ptr);
-#else
-  return __ldg(ptr);
-#endif
-}
-// drop the L2 lines of a saved wave word range that no one reads again (no write-back)
-__device__ __forceinline__ void discard_pairs(const float4* warp_base_word) {
-#if QB_DISCARD
-  __syncwarp();
-  const int lane = threadIdx.x & 31;
-  if ((lane & 7) == 0)
-    asm volatile("discard.global.L2 [%0], 128;" ::"l"(reinterpret_cast<const char*>(warp_base_word) + lane * 16)
-                 : "memory");
-#else
-  (void)warp_base_word;
-#endif
-}
-__device__ __forceinline__ void cp_async8(float2* dst, const float2* src) {
-  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // Saved per-thread register arrays (waves, far fields, checkpoints) are stored
 // thread-major with the register pair (e, e+1) packed into one 16-byte word:
@@ -192,8 +148,7 @@ constexpr size_t fused_smem_bytes_sep(int S) {
 // to the L1 cache hold the register spills of the 512-thread CTA.
 template <int N, bool ADJ>
 constexpr size_t batch_smem_bytes(bool sep, int S) {
-  return (sep ? fused_smem_bytes_sep<N>(S) : fused_smem_bytes<N>()) - (ADJ ? sizeof(float) * (size_t)N * N : 0) +
-         (QB_PREFETCH && ADJ ? sizeof(float2) * (size_t)kPrefetchElems * 4 * N : 0);
+  return (sep ? fused_smem_bytes_sep<N>(S) : fused_smem_bytes<N>()) - (ADJ ? sizeof(float) * (size_t)N * N : 0);
 }
 
 template <int N>
@@ -267,12 +222,12 @@ __device__ __forceinline__ void apply_prop(const Fft2<N>& f, float2 (&x)[Fft2<N>
 // x (S1 layout) *= o (CONJ: conj(o)) for the object row orow_ptr, columns through
 // colmap.  Loads go in batches of 8 so that a batch is in flight at once while
 // the wave occupies half of the register file.
-template <int N, bool CONJ, int E0 = 0>
+template <int N, bool CONJ>
 __device__ __forceinline__ void gather_mul(const Fft2<N>& f, float2 (&x)[Fft2<N>::E], const float2* orow_ptr,
-                                           const int* colmap, uint64_t pol = 0) {
+                                           const int* colmap, uint64_t pol) {
   constexpr int E = Fft2<N>::E;
 #pragma unroll
-  for (int e0 = E0; e0 < E; e0 += 8) {
+  for (int e0 = 0; e0 < E; e0 += 8) {
     float2 ob[8];
 #pragma unroll
     for (int j = 0; j < 8; ++j) ob[j] = ld_obj(orow_ptr + colmap[f.s1_col(e0 + j)], pol);
@@ -326,12 +281,9 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
   float2* sKr = reinterpret_cast<float2*>(colmap + N);
   float2* sKc = sKr + (size_t)N * (p.S > 1 ? p.S - 1 : 0);
   const bool sep = p.prop_r != nullptr;
-  // per-thread staging of the next real-space step's first object values (thread-major)
-  float2* pf = (sep ? sKc : sKr) + (sep ? (size_t)N * (p.S > 1 ? p.S - 1 : 0) : 0);
-  constexpr bool PF = QB_PREFETCH && ADJ;
-  bool pf_ready = false;
-  const uint64_t pol = QB_OBJ_HINT ? evict_last_policy() : 0;
+  const uint64_t pol = evict_last_policy();
   __shared__ double red[32];
+  __shared__ int nfred[32];  // per-warp non-finite counts
 
   const int tid = threadIdx.x;
   F f;
@@ -403,20 +355,6 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
     }
     __syncthreads();
     const int orow = rowmap[f.s1_r];
-    pf_ready = false;
-    // stage the object values e < kPrefetchElems of slice ns for the next real-space step
-    auto prefetch = [&](int ns) {
-      if (!PF) return;
-      if (ns < 0) {
-        pf_ready = false;
-        return;
-      }
-      const float2* nrow = p.obj + (size_t)ns * HoWo + (size_t)orow * p.Wo;
-#pragma unroll
-      for (int e = 0; e < kPrefetchElems; ++e) cp_async8(pf + e * T + tid, nrow + colmap[f.s1_col(e)]);
-      cp_async_commit();
-      pf_ready = true;
-    };
 
     // One loop with a single inverse and a single forward transform site walks
     // the forward chains of all modes, the loss, and (ADJ) the reverse chains.
@@ -457,8 +395,6 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
           x[e] = make_float2(v.x * 2.0f * in.x, v.y * 2.0f * in.x);
           x[e + 1] = make_float2(v.z * 2.0f * in.y, v.w * 2.0f * in.y);
         }
-#pragma unroll
-        for (int e = 0; e < E; e += 2) discard_pairs(reinterpret_cast<const float4*>(fw) + (e >> 1) * T + (tid & ~31));
       }
     };
     int m = 0, s = 0;
@@ -480,16 +416,7 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
 #pragma unroll
           for (int e = 0; e < E; ++e) ow[f.s1_col(e)] = x[e];
         }
-        if (PF && pf_ready) {
-          cp_async_wait_all();
-#pragma unroll
-          for (int e = 0; e < kPrefetchElems; ++e) x[e] = cmul(x[e], pf[e * T + tid]);
-          gather_mul<N, false, kPrefetchElems>(f, x, orow_ptr, colmap, pol);
-        } else {
-          gather_mul<N, false>(f, x, orow_ptr, colmap, pol);
-        }
-        // next real-space step: next slice, next mode's first slice, or the adjoint's last slice
-        prefetch(s < S - 1 ? s + 1 : (m < P - 1 ? 0 : (ADJ ? S - 1 : -1)));
+        gather_mul<N, false>(f, x, orow_ptr, colmap, pol);
         if (s == S - 1 && p.out_exit) {
           float2* oe = p.out_exit + ((size_t)m * p.B + b) * NN + (size_t)f.s1_r * N;
 #pragma unroll
@@ -499,7 +426,6 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
         const float sc = first_bwd ? inv_n : inv_n2;  // adjoint of the orthonormal FFT, or of a propagation
         const float2* wv = slot + (size_t)(m * S + s) * NN;
         float2* grow = p.grad_obj + (size_t)s * HoWo + (size_t)orow * p.Wo;
-        if (PF && pf_ready) cp_async_wait_all();
 #pragma unroll
         for (int e0 = 0; e0 < E; e0 += 8) {
           float2 ps[8], ob[8];
@@ -513,11 +439,7 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
 #pragma unroll
           for (int j = 0; j < 8; ++j) {
             col[j] = colmap[f.s1_col(e0 + j)];
-            if (PF && e0 < kPrefetchElems) {
-              ob[j] = pf_ready ? pf[(e0 + j) * T + tid] : ld_obj(orow_ptr + col[j], pol);
-            } else {
-              ob[j] = ld_obj(orow_ptr + col[j], pol);
-            }
+            ob[j] = ld_obj(orow_ptr + col[j], pol);
           }
 #pragma unroll
           for (int j = 0; j < 8; ++j) {
@@ -525,20 +447,11 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
             atomicAdd(grow + col[j], cmulc(g, ps[j]));  // conj(psi) * g
             x[e0 + j] = cmulc(g, ob[j]);                 // conj(o) * g
           }
-          if (!AN) {
-#pragma unroll
-            for (int j = 0; j < 8; j += 2)
-              discard_pairs(reinterpret_cast<const float4*>(wv) + ((e0 + j) >> 1) * T + (tid & ~31));
-          }
           if (AN) {  // sum_patches(|psi|^2) of this slice and mode (object_models.py:701-703)
             float* nrow = p.an_norm + ((size_t)s * P + m) * HoWo + (size_t)orow * p.Wo;
 #pragma unroll
             for (int j = 0; j < 8; ++j) atomicAdd(nrow + col[j], cabs2(ps[j]));
           }
-        }
-        {
-          const bool more = QB_LIFO ? m > 0 : m < P - 1;
-          prefetch(s > 0 ? s - 1 : (more ? S - 1 : -1));
         }
         if (AN && s == 0) {
           // analytic probe update: sum over positions of the back-propagated
@@ -552,8 +465,8 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
 #pragma unroll
             for (int j = 0; j < 8; ++j) pg[f.s1_col(e0 + j)] = cadd(old[j], x[e0 + j]);
           }
-          if (QB_LIFO ? m > 0 : m < P - 1) {
-            m += QB_LIFO ? -1 : 1;
+          if (m > 0) {
+            --m;
             s = S - 1;
             first_bwd = true;
             load_far_seed(m);
@@ -609,7 +522,7 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
               const float I = inten[li];
               if (!isfinite(I)) ++nonfinite;
               float dldi;
-              const float tv = ld_stream(tg + di);
+              const float tv = __ldcs(tg + di);  // targets stream through L2 once per iteration
               loss_elem<N>(p, I, tv, __ldg(p.mask + di), loss_acc, dldi);
               if (ADJ && AN) {
                 // factor f and additive fix of the Fourier projection seed
@@ -629,7 +542,7 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
         if (!ADJ) break;
         bwd = true;
         first_bwd = true;
-        m = QB_LIFO ? P - 1 : 0;
+        m = P - 1;  // last mode first: its far field and deepest waves are the most recent in L2
         s = S - 1;
         load_far_seed(m);
         continue;
@@ -641,8 +554,8 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
         continue;
       }
       accumulate_probe_grad<N>(f, x, pgrad + (size_t)m * NN, rowf, colf);
-      if (QB_LIFO ? m > 0 : m < P - 1) {
-        m += QB_LIFO ? -1 : 1;
+      if (m > 0) {
+        --m;
         s = S - 1;
         first_bwd = true;
         load_far_seed(m);
@@ -654,15 +567,22 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
 
   // ------------------------------ loss reduction ------------------------------
   for (int o = 16; o > 0; o >>= 1) loss_acc += __shfl_xor_sync(0xffffffffu, loss_acc, o);
-  if ((tid & 31) == 0) red[tid >> 5] = loss_acc;
+  // one status update per CTA: per-thread updates of a shared word contend and can drop counts
+  const int nf_warp = __reduce_add_sync(0xffffffffu, nonfinite);
+  if ((tid & 31) == 0) {
+    red[tid >> 5] = loss_acc;
+    nfred[tid >> 5] = nf_warp;
+  }
   __syncthreads();
   if (tid == 0) {
+    int nf = 0;
+    for (int w = 0; w < T / 32; ++w) nf += nfred[w];
+    status_add_nonfinite(p.status, nf);
     double t = 0.0;
     for (int w = 0; w < T / 32; ++w) t += red[w];
     // l1/l2: sum / (B / num_gpts) / mean_I ; poisson: sum / mean_I
     p.loss_part[cta] = t * (double)(p.loss_type == LOSS_POISSON ? p.inv_mean_intensity : p.loss_scale);
   }
-  status_add_nonfinite(p.status, nonfinite);
 }
 
 template <int N, bool ADJ, bool AN = false>

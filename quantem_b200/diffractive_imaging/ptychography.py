@@ -22,7 +22,6 @@ from .detector_models import DetectorPixelated
 from .object_models import ObjectPixelated
 from .probe_models import ProbePixelated
 from .ptycho_utils import SimpleBatcher
-from ..engine import HostTargetStream
 
 
 def adjust_padding_power2(pad, shape, power2_level):
@@ -484,6 +483,8 @@ class Ptychography:
         opts = [o for o in (self.obj_model.optimizer, self.probe_model.optimizer) if o is not None]
         dev = torch.device(self._device)
         # targets kept in host memory (dset.keep_targets_on_host): one double-buffered copy per iteration
+        from ..engine import HostTargetStream  # engine imports this package's utilities
+
         stream = HostTargetStream(tg, dev) if tg.device.type != "cuda" and num_iters > 0 else None
         self.last_h2d_bytes_per_iter = stream.bytes_per_copy if stream is not None else 0
         for a0 in range(num_iters):

@@ -269,7 +269,8 @@ def test_complex_cnn_matches_reference(cuda_device):
     back = net.state_dict()
     for k, v in sd.items():  # the state round trip (weights through the FP32 master copy)
         if v.dtype != torch.int64:
-            assert _crel(back[k].numpy(), v.numpy().astype(back[k].numpy().dtype)) < 1e-7, k
+            b = back[k].detach().cpu().numpy()
+            assert _crel(b, v.numpy().astype(b.dtype)) < 1e-7, k
     net.train()
     x = torch.as_tensor(z["x"], dtype=torch.complex64, device=cuda_device).requires_grad_(True)
     y = net(x)
