@@ -250,6 +250,7 @@ class PtychographyDatasetRaster(OptimizerMixin):
         self._targets_on_host = bool(enable)
         if isinstance(self._targets, torch.Tensor):
             self._targets = self._host_or_device(self._targets)
+            self._targets_kind = getattr(self, "_targets_kind", None)
         return self
 
     def _host_or_device(self, t: torch.Tensor) -> torch.Tensor:
@@ -538,12 +539,18 @@ class PtychographyDatasetRaster(OptimizerMixin):
     def _set_targets(self, loss_type):
         """dataset_models.py:225-242 (descan is not learned on this path)."""
         if "amplitude" in loss_type:
-            t = self._centered_amplitudes
+            t, kind = self._centered_amplitudes, "amplitude"
         elif "intensity" in loss_type or loss_type == "poisson":
-            t = self._centered_intensities
+            t, kind = self._centered_intensities, "intensity"
         else:
             raise ValueError(f"Unknown loss type {loss_type}")
+        # host-resident targets are built once per kind: a fresh pinned copy of the whole
+        # stack on every reconstruct call would cost more than the iterations it feeds
+        if (self._targets_on_host and isinstance(self._targets, torch.Tensor) and self._targets.device.type == "cpu"
+                and getattr(self, "_targets_kind", None) == kind):
+            return
         self._targets = self._host_or_device(t.clone())
+        self._targets_kind = kind
 
     # --------------------------------------------------------- per batch
     def apply_hard_constraints(self, obj_padding_px):

@@ -143,3 +143,31 @@ def test_graphed_iteration_matches_eager(cuda_device):
     # lr whatever the size of its gradient, so weakly lit pixels follow rounding noise)
     assert rel(gg[0], ge[0]) < 1e-4 and rel(gg[1], ge[1]) < 1e-4
     np.testing.assert_allclose(lg, le, rtol=1e-5)
+
+
+def test_host_resident_targets_match_device_targets(cuda_device):
+    """dset.keep_targets_on_host: the targets stay in pinned host memory and reconstruct
+    copies them to the GPU every iteration; the trajectory equals the device-resident one
+    (up to the order of the float atomics), and the pinned copy is built once, not per call."""
+    z = load_golden("mixed64")
+    runs = []
+    for host in (False, True):
+        pt = build_from_golden(z, device="gpu")
+        pt.dset.scan_positions_px = torch.as_tensor(z["positions"])
+        pt.obj_model._obj = torch.as_tensor(z["obj_perturbed"]).to(cuda_device).requires_grad_(True)
+        pt.probe_model._probe = torch.as_tensor(z["probe_init"]).to(cuda_device).requires_grad_(True)
+        pt.rng = int(z["recon_rng_seed"])
+        if host:
+            pt.dset.keep_targets_on_host(True)
+        pt.reconstruct(num_iters=2, batch_size=int(z["batch"]),
+                       optimizer_params={"object": {"type": "adam"}, "probe": {"type": "adam"}}, device="gpu")
+        if host:
+            tg = pt.dset.targets
+            assert tg.device.type == "cpu" and tg.is_pinned()
+            assert pt.last_h2d_bytes_per_iter == tg.numel() * 4
+        pt.reconstruct(num_iters=2, batch_size=int(z["batch"]), device="gpu")
+        if host:
+            assert pt.dset.targets is tg  # kept across reconstruct calls
+        runs.append((np.asarray(pt.iter_losses), pt.obj_model._obj.detach().cpu().numpy()))
+    np.testing.assert_allclose(runs[1][0], runs[0][0], rtol=1e-6)
+    assert rel(runs[1][1], runs[0][1]) < 1e-5
