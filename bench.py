@@ -183,6 +183,7 @@ def build_dropin(cfg, device, seed):
     ds = synthetic.make_dataset(cfg, device)
     nr, nc = cfg.scan
     data = ds["intensities"].cpu().numpy().reshape(nr, nc, cfg.n, cfg.n)
+    positions = ds["positions"]
     del ds
     rs = 1.0 / (cfg.n * cfg.pixel)
     d4 = Dataset4dstem.from_array(data, sampling=(cfg.step_px * cfg.pixel, cfg.step_px * cfg.pixel, rs, rs),
@@ -198,8 +199,7 @@ def build_dropin(cfg, device, seed):
     pt = Ptychography.from_models(dset=pd, obj_model=obj, probe_model=probe, detector_model=DetectorPixelated(),
                                   device="gpu", verbose=0, rng=seed + 2)
     pt.preprocess(obj_padding_px=(cfg.pad_px, cfg.pad_px))
-    jit = np.random.default_rng(seed).uniform(-cfg.jitter_px, cfg.jitter_px, (pd.num_gpts, 2)).astype(np.float32)
-    pd.scan_positions_px = pd.scan_positions_px.detach() + torch.as_tensor(jit, device=pd.scan_positions_px.device)
+    pd.scan_positions_px = positions.float().to(pd.scan_positions_px.device).contiguous()  # simulated positions
     pd.keep_targets_on_host(True)
     return pt
 
@@ -1221,8 +1221,8 @@ def _reference_setup(cfg, dev, ref_dir=None, probe_known=False):
     pt = Ptychography.from_models(dset=pd, obj_model=obj_model, probe_model=probe_model,
                                   detector_model=DetectorPixelated(), device="cpu", verbose=0, rng=cfg.seed + 2)
     pt.preprocess(obj_padding_px=(cfg.pad_px, cfg.pad_px))
-    pd.scan_positions_px = pd.scan_positions_px.detach() + torch.as_tensor(
-        np.random.default_rng(cfg.seed).uniform(-cfg.jitter_px, cfg.jitter_px, (pd.num_gpts, 2)).astype(np.float32))
+    # the positions the data were simulated at (raster + the simulation's jitter)
+    pd.scan_positions_px = ds["positions"].float().cpu().contiguous()
     if probe_known:
         known = (ds["probes"] * (ds["mean_intensity"] / ds["probes"].abs().square().sum()) ** 0.5).cpu()
         with torch.no_grad():
@@ -1367,11 +1367,13 @@ def reference_torch_gpu_subprocess(local_device: int, batch_size: int, steps: in
         env["CUDA_VISIBLE_DEVICES"] = str(local_device)
     cmd = [sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--torch-gpu", "--steps", str(steps),
            "--warmup", str(warmup), "--batch-size", str(batch_size), *extra]
+    out = None
     try:
-        out = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=900)
+        out = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=1800)
         line = json.loads(out.stdout.strip().splitlines()[-1])
     except Exception as exc:  # the reference is a baseline here: report, never fail the bench
-        return {"unavailable": f"{type(exc).__name__}: {exc}"[:300]}
+        err = out.stderr.strip().splitlines()[-1] if out is not None and out.stderr.strip() else ""
+        return {"unavailable": f"{type(exc).__name__}: {exc}; {err}"[:400]}
     if "unavailable" in line:
         return {"unavailable": line["unavailable"]}
     return line.get("reference_torch_gpu", line)

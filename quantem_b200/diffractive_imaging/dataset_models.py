@@ -255,6 +255,8 @@ class PtychographyDatasetRaster(OptimizerMixin):
 
     def _host_or_device(self, t: torch.Tensor) -> torch.Tensor:
         if self._targets_on_host:
+            if t.device.type == "cpu" and t.is_contiguous() and (not torch.cuda.is_available() or t.is_pinned()):
+                return t  # already where it belongs: no new tensor, no copy
             t = t.detach().cpu().contiguous()
             return t if not torch.cuda.is_available() or t.is_pinned() else t.pin_memory()
         return t.to(self._device).contiguous()
