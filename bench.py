@@ -1224,7 +1224,10 @@ def _reference_setup(cfg, dev, ref_dir=None, probe_known=False):
     # the positions the data were simulated at (raster + the simulation's jitter)
     pd.scan_positions_px = ds["positions"].float().cpu().contiguous()
     if probe_known:
-        known = (ds["probes"] * (ds["mean_intensity"] / ds["probes"].abs().square().sum()) ** 0.5).cpu()
+        # the simulation's mode shapes at the reference's own intensity scale (its targets are
+        # normalised by its preprocessing, and its initial probe is scaled to match them)
+        ref_scale = float(probe_model._probe.detach().abs().square().sum())
+        known = (ds["probes"] * (ref_scale / float(ds["probes"].abs().square().sum())) ** 0.5).cpu()
         with torch.no_grad():
             probe_model._probe.data = known.to(probe_model._probe.dtype).clone()
             probe_model._initial_probe = known.clone()
@@ -1256,10 +1259,23 @@ def reference_torch_gpu(cfg, device, steps, warmup, batch_size, ref_dir=None, ve
     sync = torch.cuda.synchronize if dev.type == "cuda" else (lambda: None)
 
     bs = batch_size
-    while True:
+    while True:  # the whole warm-up and timed run at one batch; halved while the GPU runs out of memory
         try:
             pt.reconstruct(num_iters=1, reset=True, optimizer_params=opt, batch_size=bs, device=dev_arg)
+            if warmup > 1:
+                pt.reconstruct(num_iters=warmup - 1, batch_size=bs)
             sync()
+            if dev.type == "cuda":
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                pt.reconstruct(num_iters=steps, batch_size=bs)
+                e1.record()
+                torch.cuda.synchronize()
+                ms = e0.elapsed_time(e1) / steps
+            else:
+                t1 = time.perf_counter()
+                pt.reconstruct(num_iters=steps, batch_size=bs)
+                ms = (time.perf_counter() - t1) * 1e3 / steps
             break
         except torch.OutOfMemoryError:
             if dev.type == "cuda":
@@ -1267,20 +1283,6 @@ def reference_torch_gpu(cfg, device, steps, warmup, batch_size, ref_dir=None, ve
             bs //= 2
             if bs < 1:
                 return {"unavailable": "out of memory at batch 1"}
-    if warmup > 1:
-        pt.reconstruct(num_iters=warmup - 1, batch_size=bs)
-    sync()
-    if dev.type == "cuda":
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        pt.reconstruct(num_iters=steps, batch_size=bs)
-        e1.record()
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / steps
-    else:
-        t1 = time.perf_counter()
-        pt.reconstruct(num_iters=steps, batch_size=bs)
-        ms = (time.perf_counter() - t1) * 1e3 / steps
     npos = pd.num_gpts
     losses = [float(x) for x in pt.iter_losses]
     if verbose:

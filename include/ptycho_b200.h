@@ -97,6 +97,11 @@ typedef struct ptycho_batch_args {
   int recompute_every;       /* n = 256 adjoint: 0 keeps every slice's incident wave; k > 0 keeps the
                                 wave entering every k-th slice and recomputes the others in the
                                 reverse sweep (smaller scratch, S - S/k extra propagations per mode) */
+  float* grad_positions;     /* optional float32 (B, 2), adjoint launch: dL/d(scan position) (row, column)
+                                of every batch entry, summed over the modes (serial variant, n < 256,
+                                autograd adjoint).  Positions enter through the fractional probe shift
+                                only (dataset_models.py:1487-1490, ptycho_utils.py:128-176); entries
+                                whose index is invalid are left untouched.  ABI version 2. */
 } ptycho_batch_args;
 
 enum {

@@ -305,6 +305,8 @@ class ForwardState:
     waves: list = field(default_factory=list)  # incoming wave at each slice, (P, B, H, W)
     far: np.ndarray = None       # orthonormal far field (P, B, H, W)
     intensity: np.ndarray = None  # corner-centred sum over modes (B, H, W)
+    g_probe_plane: np.ndarray = None  # set by adjoint: dL/d(shifted probe) (P, B, H, W)
+    probe_o: np.ndarray = None        # set by full_gradients: the orthogonalised probe used
 
 
 def forward(obj_c: np.ndarray, probe_o: np.ndarray, positions_px: np.ndarray,
@@ -394,7 +396,24 @@ def adjoint(obj_c, probe_o, props, st: ForwardState, dL_dI: np.ndarray):
     acc = np.sum(fft2(g) * np.conj(st.ramp)[None], axis=1)
     g_probe = ifft2(acc)
     g_obj = scatter_patches(g_patch, st.rows, st.cols, obj_c.shape)
+    st.g_probe_plane = g  # (P, B, H, W): gradient w.r.t. the shifted probe, for position gradients
     return g_obj, g_probe
+
+
+def position_gradients(probe_o, st: ForwardState, g_probe_plane: np.ndarray) -> np.ndarray:
+    """dL/d(scan position) (B, 2) of the batch: the positions enter only through the
+    fractional shift of the probe (dataset_models.py:1487-1490, ptycho_utils.py:128-176;
+    the rounded part only picks the patch).  With Y = fft2(probe) * ramp(frac) and
+    psi0 = ifft2(Y), G_Y = fft2(g) / (H W) for the probe-plane gradient g, and
+    dL/dfrac_r = sum over modes and frequencies of Re(conj(G_Y) (-2 pi i k_r) Y)."""
+    H, W = probe_o.shape[-2:]
+    kr = np.fft.fftfreq(H, d=1.0)[None, None, :, None]
+    kc = np.fft.fftfreq(W, d=1.0)[None, None, None, :]
+    Y = fft2(probe_o)[:, None] * st.ramp[None]            # (P, B, H, W)
+    t = np.conj(fft2(g_probe_plane) / (H * W)) * Y
+    gr = np.sum(np.real(-2j * np.pi * kr * t), axis=(0, 2, 3))
+    gc = np.sum(np.real(-2j * np.pi * kc * t), axis=(0, 2, 3))
+    return np.stack([gr, gc], axis=-1)
 
 
 def batch_loss_and_grads(obj_c, probe_o, positions_px, props, targets, mask, num_gpts,
@@ -419,6 +438,7 @@ def full_gradients(obj_raw, probe_raw, positions_px, props, targets, mask, num_g
         probe_o, cache = probe_raw, None
     loss, g_obj_c, g_probe_o, st = batch_loss_and_grads(
         obj_c, probe_o, positions_px, props, targets, mask, num_gpts, mean_intensity, loss_type)
+    st.probe_o = probe_o
     g_obj = object_transmission_vjp(obj_raw, g_obj_c, obj_type) * (upsample_factor**2 / 2)
     g_probe = gram_schmidt_vjp(cache, g_probe_o) if orthogonalize else g_probe_o
     return loss, g_obj, g_probe, st
@@ -501,26 +521,37 @@ def gaussian_atom_phase(shape, n_atoms, sigma_px, peak_rad, rng):
 
 def reconstruct(obj_raw, probe_raw, positions_px, props, targets, mask, mean_intensity, upsample_factor,
                 num_iters, batch_size, rng, lr_obj=5e-3, lr_probe=1e-3, orthogonalize=True,
-                loss_type="l2_amplitude", obj_type="complex"):
+                loss_type="l2_amplitude", obj_type="complex", lr_positions=None):
     """Adam iterations of Ptychography.reconstruct (ptychography.py:208-245) on
-    the given state; batches from a numpy generator like SimpleBatcher.
-    Returns (obj, probe, per-iteration mean batch losses)."""
+    the given state; batches from a numpy generator like SimpleBatcher.  With
+    ``lr_positions`` the scan positions are a parameter too (a dataset optimiser,
+    dataset_models.py:98-110): Adam over the whole (N, 2) array, the gradient zero
+    outside the batch.  Returns (obj, probe, per-iteration mean batch losses), plus the
+    positions with ``lr_positions``."""
     obj = obj_raw.copy()
     probe = probe_raw.copy()
-    so, sp = AdamState(), AdamState()
+    pos = positions_px.astype(np.float64).copy()
+    so, sp, spos = AdamState(), AdamState(), AdamState()
     npos = positions_px.shape[0]
     losses = []
     for _ in range(num_iters):
         tot, nb = 0.0, 0
         for bi in batch_order(rng, npos, batch_size):
-            loss, g_obj, g_probe, _ = full_gradients(obj, probe, positions_px[bi], props, targets[bi], mask, npos,
-                                                     mean_intensity, upsample_factor, orthogonalize, loss_type,
-                                                     obj_type)
+            loss, g_obj, g_probe, st = full_gradients(obj, probe, pos[bi], props, targets[bi], mask, npos,
+                                                      mean_intensity, upsample_factor, orthogonalize, loss_type,
+                                                      obj_type)
+            if lr_positions is not None:
+                g_pos = np.zeros_like(pos)
+                g_pos[bi] = position_gradients(st.probe_o, st, st.g_probe_plane)
             adam_step(obj, g_obj, so, lr_obj)
             adam_step(probe, g_probe, sp, lr_probe)
+            if lr_positions is not None:
+                adam_step(pos, g_pos, spos, lr_positions)
             tot += loss
             nb += 1
         losses.append(tot / nb)
+    if lr_positions is not None:
+        return obj, probe, np.array(losses), pos
     return obj, probe, np.array(losses)
 
 

@@ -92,7 +92,7 @@ class BatchArgs(ctypes.Structure):
         ("n", _int), ("S", _int), ("P", _int), ("B", _int), ("Ho", _int), ("Wo", _int),
         ("npos", _int), ("grid", _int), ("loss_type", _int),
         ("loss_scale", _flt), ("inv_mean_intensity", _flt), ("variant", _int),
-        ("analytic", _int), ("an_norm", _vp), ("recompute_every", _int),
+        ("analytic", _int), ("an_norm", _vp), ("recompute_every", _int), ("grad_positions", _vp),
     ]
 
 

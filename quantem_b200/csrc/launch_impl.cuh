@@ -39,6 +39,7 @@ inline BatchParams to_params(const ptycho_batch_args* a) {
   p.analytic = a->analytic;
   p.an_norm = a->an_norm;
   p.ckpt = a->recompute_every;
+  p.grad_positions = a->grad_positions;
   return p;
 }
 

@@ -458,11 +458,16 @@ int run_batch(const ptycho_batch_args* a, void* stream, bool adj) {
   if (rc) return rc;
   if (a->B == 0) return PTYCHO_OK;
   if (a->n == 256) {
+    if (a->grad_positions)
+      return fail(PTYCHO_ERR_UNSUPPORTED, "position gradients are not built for 256 x 256 windows");
     const int lrc = qb_launch_c256(a, adj, static_cast<cudaStream_t>(stream));
     if (lrc) return fail(lrc, "cluster256_kernel launch: %s", cudaGetErrorString(cudaGetLastError()));
     return PTYCHO_OK;
   }
-  const int variant = a->analytic ? PTYCHO_VARIANT_SERIAL : resolve_variant(a);
+  if (a->grad_positions && (!adj || a->analytic))
+    return fail(PTYCHO_ERR_UNSUPPORTED, "position gradients come from the autograd adjoint launch");
+  // position gradients are summed over the modes inside one CTA: serial variant
+  const int variant = (a->analytic || a->grad_positions) ? PTYCHO_VARIANT_SERIAL : resolve_variant(a);
   if (variant < 0) return fail(PTYCHO_ERR_UNSUPPORTED, "variant %d not available for P=%d", a->variant, a->P);
   if (variant == PTYCHO_VARIANT_CLUSTER && a->grid % a->P != 0)
     return fail(PTYCHO_ERR_INVALID, "cluster launch: grid %d is not a multiple of P=%d", a->grid, a->P);
@@ -486,7 +491,7 @@ int ptycho_get_last_error(char* buf, size_t len) {
   return PTYCHO_OK;
 }
 
-int ptycho_abi_version(void) { return 1; }
+int ptycho_abi_version(void) { return 2; }  // 2: ptycho_batch_args.grad_positions
 
 int ptycho_sm_count(int* out) {
   if (!out) return fail(PTYCHO_ERR_INVALID, "out is NULL");

@@ -61,6 +61,7 @@ struct BatchParams {
   int analytic;               // 0: autograd adjoint; 1: analytic update (ptychography.py:339-372), serial kernel
   float* an_norm;             // (S, P, Ho, Wo) scatter of |psi|^2 for the analytic normalisation
   int ckpt;                   // 256^2 cluster kernel: checkpoint interval of the adjoint (0 = keep all waves)
+  float* grad_positions;      // optional (B, 2) dL/d(position), serial autograd adjoint only
 };
 
 // Status word of the batch kernels: bits 0-19 count non-finite predicted
@@ -284,6 +285,7 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
   const uint64_t pol = evict_last_policy();
   __shared__ double red[32];
   __shared__ int nfred[32];  // per-warp non-finite counts
+  __shared__ float posred[32][2];  // per-warp position-gradient partials
 
   const int tid = threadIdx.x;
   F f;
@@ -554,6 +556,45 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
         continue;
       }
       accumulate_probe_grad<N>(f, x, pgrad + (size_t)m * NN, rowf, colf);
+      if (p.grad_positions) {
+        // positions enter through the probe shift Y = probe_hat * ramp(frac) only; x = N^2 dL/dY
+        // here, so dL/dfrac = (2 pi / N^2) sum_k fftfreq(k) Im(conj(x_k) Y_k), summed over the modes
+        const float2* ph = p.probe_hat + (size_t)m * NN;
+        float gr = 0.f, gc = 0.f;
+#pragma unroll
+        for (int g = 0; g < G3; ++g)
+#pragma unroll
+          for (int e = 0; e < D; ++e) {
+            const int kr = f.s3_row(g, e), kc = f.s3_c;
+            const float2 y = cmul(cmul(__ldg(ph + (size_t)kr * N + kc), rowf[kr]), colf[kc]);
+            const float2 xv = x[g * D + e];
+            const float im = xv.x * y.y - xv.y * y.x;
+            gr = fmaf((float)fsigned(kr, N), im, gr);
+            gc = fmaf((float)fsigned(kc, N), im, gc);
+          }
+        for (int o = 16; o > 0; o >>= 1) {
+          gr += __shfl_xor_sync(0xffffffffu, gr, o);
+          gc += __shfl_xor_sync(0xffffffffu, gc, o);
+        }
+        if ((tid & 31) == 0) {
+          posred[tid >> 5][0] = gr;
+          posred[tid >> 5][1] = gc;
+        }
+        __syncthreads();
+        if (tid == 0) {  // fixed-order sum over warps, accumulated over the modes of this position
+          float sr = 0.f, sc = 0.f;
+          for (int w = 0; w < T / 32; ++w) {
+            sr += posred[w][0];
+            sc += posred[w][1];
+          }
+          const float k = 6.283185307179586f / ((float)N * (float)N * (float)N);  // 2 pi / N^2, fftfreq = k / N
+          float* out = p.grad_positions + 2 * (size_t)b;
+          const bool first = m == P - 1;  // the reverse chains run last mode first
+          out[0] = (first ? 0.f : out[0]) + k * sr;
+          out[1] = (first ? 0.f : out[1]) + k * sc;
+        }
+        __syncthreads();
+      }
       if (m > 0) {
         --m;
         s = S - 1;

@@ -86,7 +86,7 @@ def _dataset_state(dset, save_raw_data):
              "initial_scan_positions_px": _cpu(dset.initial_scan_positions_px),
              "probe_energy": dset.probe_energy, "targets_on_host": dset.targets_on_host,
              "learn_descan": dset.learn_descan, "learn_scan_positions": dset.learn_scan_positions,
-             "raw": None}
+             "raw": None, **{"optim": _opt_state(dset)}}
     if save_raw_data:
         mask = dset.detector_mask
         state["raw"] = {"array": np.asarray(dset.intensities_4d),
@@ -207,6 +207,8 @@ def from_state(cls, state, dset=None, device=None, verbose=None):
     pt.compute_propagator_arrays()
     _restore_opt_state(obj, os_)
     _restore_opt_state(probe, pr)
+    if ds.get("optim"):  # learned scan positions (dataset optimiser)
+        _restore_opt_state(dset, ds["optim"])
     gen = getattr(np.random, ps["rng_bit_generator"])()
     gen.state = ps["rng_state"]
     pt._rng = np.random.Generator(gen)

@@ -213,7 +213,17 @@ class PtychographyDatasetRaster(OptimizerMixin):
                             else np.asarray(positions), dtype=getattr(torch, config.get("dtype_real")))
         if tuple(t.shape) != (self.num_gpts, 2):
             raise ValueError(f"scan_positions_px must have shape {(self.num_gpts, 2)}")
-        self._scan_positions_px = t.to(self._device).contiguous()
+        self._set_positions(t)
+
+    def _set_positions(self, t: torch.Tensor):
+        """New position values; kept in the same tensor while an optimiser holds it (the
+        reference assigns ``.data`` of its position parameter, dataset_models.py:146-154)."""
+        cur = self._scan_positions_px
+        if self.has_optimizer() and isinstance(cur, torch.Tensor) and cur.shape == t.shape:
+            with torch.no_grad():
+                cur.data = t.detach().to(cur.device, cur.dtype).contiguous()
+        else:
+            self._scan_positions_px = t.detach().to(self._device).contiguous()
 
     @property
     def initial_scan_positions_px(self) -> torch.Tensor:
@@ -267,13 +277,28 @@ class PtychographyDatasetRaster(OptimizerMixin):
         self._constraints[key] = value
 
     def get_optimization_parameters(self):
-        raise NotImplementedError("learning scan positions / descan is not part of the B200 path")
+        """The scan positions when they are learned (dataset_models.py:98-110).  Learned descan
+        shifts are not built on this path: a dataset optimiser needs ``learn_descan=False``."""
+        if self.learn_descan:
+            raise NotImplementedError("learned descan shifts are not part of the B200 path: create the dataset "
+                                      "with learn_descan=False to learn the scan positions")
+        if not self.learn_scan_positions:
+            raise RuntimeError("No parameters to optimize for dataset: learn_descan and learn_scan_positions "
+                               "are both False")
+        self._scan_positions_px = self._scan_positions_px.detach().contiguous().requires_grad_(True)
+        return [self._scan_positions_px]
+
+    def remove_optimizer(self):
+        super().remove_optimizer()
+        self._scan_positions_px = self._scan_positions_px.detach()
 
     def reset_iter_constraint_losses(self):
         pass
 
     def reset(self):
-        self._scan_positions_px = self._initial_scan_positions_px.clone().to(self._device)
+        self._set_positions(self._initial_scan_positions_px.clone())
+        if self._optimizer is not None:
+            self.set_optimizer(self._optimizer_params)
 
     def to(self, device):
         dev, _ = config.validate_device(device)
@@ -282,7 +307,9 @@ class PtychographyDatasetRaster(OptimizerMixin):
                      "_targets", "_centered_amplitudes", "_amplitudes", "_centered_intensities", "_intensities"):
             v = getattr(self, name, None)
             if isinstance(v, torch.Tensor):
-                setattr(self, name, self._host_or_device(v) if name == "_targets" else v.to(dev))
+                setattr(self, name, self._host_or_device(v) if name == "_targets" else v.detach().to(dev))
+        if self._optimizer is not None:  # the positions may be new tensors now
+            self.set_optimizer(self._optimizer_params)
         return self
 
     # ---------------------------------------------------------- preprocessing
@@ -563,7 +590,7 @@ class PtychographyDatasetRaster(OptimizerMixin):
             pos = torch.minimum(torch.maximum(pos, torch.zeros_like(shp)), shp - 1)
         if self._constraints.get("center_scan_positions", False):
             pos = pos - pos.mean(dim=0, keepdim=True) + shp / 2
-        self._scan_positions_px = pos.contiguous()
+        self._set_positions(pos)
 
     def forward(self, batch_indices, obj_padding_px):
         """(patch_indices, positions_px, positions_px_fractional, None) of a batch."""

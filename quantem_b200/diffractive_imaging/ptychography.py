@@ -323,8 +323,7 @@ class Ptychography:
             elif k == "probe":
                 self.probe_model.optimizer_params = v
             elif k == "dataset":
-                if v.get("type", "adam") != "none":
-                    raise NotImplementedError("learning scan positions / descan is not part of the B200 path")
+                self.dset.optimizer_params = v
             else:
                 raise ValueError(f"key to be optimized, {k}, not in allowed keys: {self.OPTIMIZABLE_VALS}")
 
@@ -335,11 +334,14 @@ class Ptychography:
             out["object"] = self.obj_model.optimizer
         if self.probe_model.has_optimizer():
             out["probe"] = self.probe_model.optimizer
+        if self.dset.has_optimizer():
+            out["dataset"] = self.dset.optimizer
         return out
 
     def set_optimizers(self):
+        models = {"object": self.obj_model, "probe": self.probe_model, "dataset": self.dset}
         for key, params in self.optimizer_params.items():
-            (self.obj_model if key == "object" else self.probe_model).set_optimizer(params)
+            models[key].set_optimizer(params)
 
     @property
     def scheduler_params(self) -> dict:
@@ -366,10 +368,13 @@ class Ptychography:
                 self.obj_model.set_scheduler(sp, num_iter)
             elif key == "probe":
                 self.probe_model.set_scheduler(sp, num_iter)
+            elif key == "dataset":
+                self.dset.set_scheduler(sp, num_iter)
 
     def step_schedulers(self, loss=None):
         self.obj_model.step_scheduler(loss)
         self.probe_model.step_scheduler(loss)
+        self.dset.step_scheduler(loss)
 
     @property
     def constraints(self) -> dict:
@@ -400,6 +405,7 @@ class Ptychography:
         self._iter_losses, self._iter_val_losses, self._iter_lrs, self._snapshots = [], [], {}, []
         self.obj_model.reset_optimizer()
         self.probe_model.reset_optimizer()
+        self.dset.reset_optimizer()
 
     # ------------------------------------------------------------ forward model API
     def _batch_tensors(self):
@@ -480,7 +486,7 @@ class Ptychography:
         batcher = SimpleBatcher(self.dset.num_gpts, self.batch_size, rng=self.rng, val_ratio=self.val_ratio,
                                 val_mode=self.val_mode)
         prop, _, tg, mask = self._batch_tensors()
-        opts = [o for o in (self.obj_model.optimizer, self.probe_model.optimizer) if o is not None]
+        opts = [o for o in (self.obj_model.optimizer, self.probe_model.optimizer, self.dset.optimizer) if o is not None]
         dev = torch.device(self._device)
         # targets kept in host memory (dset.keep_targets_on_host): one double-buffered copy per iteration
         from ..engine import HostTargetStream  # engine imports this package's utilities

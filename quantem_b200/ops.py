@@ -430,12 +430,14 @@ def batch_forward(obj_c, probe_o, prop, positions, batch_idx, targets, mask, num
 
 def batch_forward_adjoint(obj_c, probe_o, prop, positions, batch_idx, targets, mask, num_gpts, mean_intensity,
                           loss_type="l2_amplitude", probe_hat=None, grid=None, grad_obj=None,
-                          grad_probe=None, variant="auto", recompute_every=None):
+                          grad_probe=None, variant="auto", recompute_every=None, grad_positions=None):
     """Fused forward + loss + adjoint of one batch.
 
     Returns (loss 0-d tensor, grad w.r.t. the constrained object (S,Ho,Wo),
     grad w.r.t. the orthogonalised probe (P,n,n)), torch gradient convention.
-    ``grad_obj`` (if given) is accumulated into, not cleared.
+    ``grad_obj`` (if given) is accumulated into, not cleared.  ``grad_positions``
+    (optional float32 (B, 2), zero-filled by the caller) receives dL/d(position) of
+    every batch entry (the serial kernel runs then).
     """
     geom = _check_batch_inputs(obj_c, probe_o, prop, positions, batch_idx, targets, mask)
     B = int(batch_idx.numel())
@@ -453,7 +455,13 @@ def batch_forward_adjoint(obj_c, probe_o, prop, positions, batch_idx, targets, m
         return loss, grad_obj, grad_probe
     a = _batch_args(geom, obj_c, probe_hat, prop, positions, batch_idx, targets, mask, B, loss_type,
                     loss_scale_of(loss_type, B, num_gpts, mean_intensity), 1.0 / mean_intensity,
-                    grad_obj=grad_obj, variant=variant, recompute_every=recompute_every)
+                    grad_obj=grad_obj, variant="serial" if grad_positions is not None else variant,
+                    recompute_every=recompute_every)
+    if grad_positions is not None:
+        _req(grad_positions, "grad_positions", torch.float32, dev)
+        if tuple(grad_positions.shape) != (B, 2):
+            raise ValueError(f"grad_positions must be ({B}, 2)")
+        a.grad_positions = grad_positions.data_ptr()
     grid_v, parts, ws = plan_and_bind(a, dev, adjoint=True, grid=grid)
     lib = _lib.lib()
     st = _stream()
@@ -528,28 +536,39 @@ class _BatchLossFn(torch.autograd.Function):
         spec = cfg.get("obj_spec") or COMPLEX_OBJECT
         ctx.spec = spec
         obj_c, work = obj_transmission(obj_raw_c, spec)
-        need = ctx.needs_input_grad[0] or ctx.needs_input_grad[1]
+        need = ctx.needs_input_grad[0] or ctx.needs_input_grad[1] or ctx.needs_input_grad[3]
+        ctx.npos = int(positions.shape[0])
         if need:
+            g_pos = (torch.zeros((int(batch_idx.numel()), 2), dtype=torch.float32, device=positions.device)
+                     if ctx.needs_input_grad[3] else None)
             loss, g_obj_c, g_probe = batch_forward_adjoint(
-                obj_c, probe_c, prop, positions, batch_idx, targets, mask, cfg["num_gpts"],
+                obj_c, probe_c, prop, positions.detach(), batch_idx, targets, mask, cfg["num_gpts"],
                 cfg["mean_intensity"], cfg["loss_type"], grid=cfg.get("grid"), variant=cfg.get("variant", "auto"),
-                recompute_every=cfg.get("recompute_every"))
-            ctx.save_for_backward(obj_raw_c, work, g_obj_c, g_probe)
+                recompute_every=cfg.get("recompute_every"), grad_positions=g_pos)
+            ctx.save_for_backward(obj_raw_c, work, g_obj_c, g_probe, batch_idx,
+                                  g_pos if g_pos is not None else torch.empty(0, device=positions.device))
         else:
-            loss = batch_forward(obj_c, probe_c, prop, positions, batch_idx, targets, mask, cfg["num_gpts"],
+            loss = batch_forward(obj_c, probe_c, prop, positions.detach(), batch_idx, targets, mask, cfg["num_gpts"],
                                  cfg["mean_intensity"], cfg["loss_type"], want_intensity=False,
                                  grid=cfg.get("grid"), variant=cfg.get("variant", "auto"))["loss"]
         return loss
 
     @staticmethod
     def backward(ctx, gout):
-        obj_raw, work, g_obj_c, g_probe = ctx.saved_tensors
+        obj_raw, work, g_obj_c, g_probe, batch_idx, g_pos = ctx.saved_tensors
         gout = gout.detach().to(torch.float32).reshape(1).contiguous()
         g_obj = None
         if ctx.needs_input_grad[0]:
             g_obj = obj_transmission_vjp(obj_raw, g_obj_c, work, ctx.spec, scale=gout)
         g_pr = g_probe * gout if ctx.needs_input_grad[1] else None
-        return g_obj, g_pr, None, None, None, None, None, None
+        g_positions = None
+        if ctx.needs_input_grad[3]:  # per batch entry -> per scan position (repeated indices add up)
+            g_positions = torch.zeros((ctx.npos, 2), dtype=torch.float32, device=g_pos.device)
+            # the kernel skips out-of-range indices (and reports them): route them to row 0 with a zero gradient
+            valid = (batch_idx >= 0) & (batch_idx < ctx.npos)
+            g_positions.index_add_(0, torch.where(valid, batch_idx, torch.zeros_like(batch_idx)),
+                                   g_pos * gout * valid[:, None])
+        return g_obj, g_pr, None, g_positions, None, None, None, None
 
 
 def batch_loss(obj_raw, probe_o, prop, positions, batch_idx, targets, mask, num_gpts, mean_intensity,

@@ -88,3 +88,39 @@ def test_oracle_adjoint_matches_fp64_finite_differences(case, which):
         # 1e-7 relative plus the difference quotient's own rounding floor, eps |L| / t
         # (random directions in ~10^5 dimensions cancel much of <g, d>)
         assert abs(fd - adj) <= 1e-7 * abs(adj) + 4 * np.finfo(np.float64).eps * abs(loss) / t, (fd, adj)
+
+
+@pytest.mark.parametrize("case", ["single64", "mixed64", "c2small"])
+def test_oracle_position_gradients_match_fp64_finite_differences(case):
+    """dL/d(scan positions): only the fractional shift of the probe depends on a position
+    (the rounded part picks the patch), so a central difference of 1e-6 px, far from the
+    rounding boundaries of the fixture positions, checks O.position_gradients."""
+    if case == "c2small":
+        from tests.golden.c2small import load_c2small
+
+        z = load_c2small()
+    else:
+        z = load_golden(case)
+    H, S = int(z["H"]), int(z["S"])
+    props = z["propagators"].astype(np.complex128) if S > 1 else np.zeros((0, H, H))
+    bi = z["batch_indices"]
+    obj_c = O.constrain_object(z["obj_perturbed"].astype(np.complex128))
+    probe_o = O.gram_schmidt(z["probe_init"].astype(np.complex128))[0] if int(z["orthogonalize"]) else \
+        z["probe_init"].astype(np.complex128)
+    pos = z["positions"].astype(np.float64)[bi]
+    tg = z["targets"].astype(np.float64)[bi]
+    args = (props, tg, np.ones((H, H)), z["positions"].shape[0], float(z["mean_intensity"]))
+    loss, _, _, st = O.batch_loss_and_grads(obj_c, probe_o, pos, *args)
+    gpos = O.position_gradients(probe_o, st, st.g_probe_plane)
+    frac = pos - np.round(pos)
+    assert np.abs(np.abs(frac) - 0.5).min() > 1e-3  # no position sits on a rounding boundary
+    rng = np.random.default_rng(5)
+    d = rng.standard_normal(pos.shape)
+    t = 1e-6
+
+    def lossat(p):
+        return O.batch_loss_and_grads(obj_c, probe_o, p, *args)[0]
+
+    fd = (lossat(pos + t * d) - lossat(pos - t * d)) / (2 * t)
+    adj = float(np.sum(gpos * d))
+    assert abs(fd - adj) <= 1e-6 * abs(adj) + 4 * np.finfo(np.float64).eps * abs(loss) / t, (fd, adj)

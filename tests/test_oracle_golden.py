@@ -144,3 +144,32 @@ def test_oracle_reconstruct_matches_reference_object_types(case):
     np.testing.assert_allclose(losses, z["recon_losses"], rtol=2e-6)
     assert rel(obj, z["recon_obj"]) < 1e-5
     assert rel(probe, z["recon_probe"]) < 1e-5
+
+
+def test_oracle_position_gradients_and_learned_positions_match_reference():
+    """Learned scan positions (fixture positions64, made by the reference with a dataset
+    optimiser and learn_descan=False): the batch's autograd position gradient, and 3 Adam
+    iterations moving object, probe and positions."""
+    z = load_golden("positions64")
+    H = int(z["H"])
+    bi = z["batch_indices"]
+    props = z["propagators"].astype(np.complex128)
+    loss, _, _, st = O.full_gradients(
+        z["obj_perturbed"].astype(np.complex128), z["probe_init"].astype(np.complex128),
+        z["positions"].astype(np.float64)[bi], props, z["targets"].astype(np.float64)[bi], np.ones((H, H)),
+        z["positions"].shape[0], float(z["mean_intensity"]), float(z["upsample_factor"]), orthogonalize=True)
+    assert abs(loss - float(z["batch_loss"])) / float(z["batch_loss"]) < 2e-6
+    g = O.position_gradients(st.probe_o, st, st.g_probe_plane)
+    ref = z["grad_positions"][bi]
+    assert np.abs(z["grad_positions"][len(bi):]).max() == 0.0  # positions outside the batch get none
+    assert rel(g, ref) < 1e-5  # the reference's float32 ramp and FFTs
+    obj, probe, losses, pos = O.reconstruct(
+        z["obj_perturbed"].astype(np.complex128), z["probe_init"].astype(np.complex128),
+        z["positions"].astype(np.float64), props, z["targets"].astype(np.float64), np.ones((H, H)),
+        float(z["mean_intensity"]), float(z["upsample_factor"]), int(z["iters"]), int(z["batch"]),
+        np.random.default_rng(int(z["recon_rng_seed"])), lr_positions=1e-2)
+    np.testing.assert_allclose(losses, z["recon_losses"], rtol=1e-5)
+    moved_ref = z["recon_positions"] - z["positions"]
+    assert np.abs(moved_ref).max() > 0.02
+    assert rel(pos - z["positions"], moved_ref) < 1e-3  # Adam's sign-like steps on float32 gradients
+    assert rel(obj, z["recon_obj"]) < 1e-4
