@@ -1336,8 +1336,8 @@ def reference_c4_curve(counts, iters, batch=256):
     for it in range(1, iters + 1):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        if it == 1:
-            pt.reconstruct(num_iters=1, reset=True, optimizer_params=opt, scheduler_params=sched, batch_size=batch,
+        if it == 1:  # no reset: it would put the raster positions back in place of the simulated ones
+            pt.reconstruct(num_iters=1, optimizer_params=opt, scheduler_params=sched, batch_size=batch,
                            device="gpu")
         else:
             pt.reconstruct(num_iters=1, batch_size=batch, device="gpu")
