@@ -189,7 +189,7 @@ def build_dropin(cfg, device, seed):
     d4 = Dataset4dstem.from_array(data, sampling=(cfg.step_px * cfg.pixel, cfg.step_px * cfg.pixel, rs, rs),
                                   units=("A", "A", "A^-1", "A^-1"))
     pd = PtychographyDatasetRaster.from_dataset4dstem(d4, verbose=0)
-    pd.preprocess(com_fit_function="constant", force_com_rotation=0, force_com_transpose=False,
+    pd.preprocess(com_fit_function="no_shift", force_com_rotation=0, force_com_transpose=False,
                   plot_rotation=False, plot_com=False, probe_energy=cfg.energy, device="gpu")
     obj = ObjectPixelated.from_uniform(num_slices=cfg.slices, slice_thicknesses=cfg.slice_thickness,
                                        obj_type="complex")
@@ -760,13 +760,20 @@ def _bf16_peak():
         return 1590.0, "fallback"
 
 
+# held-out test objects of the learned-initialiser benchmark (peak phase per atom [rad], atoms / px^2
+# / slice): the multislice problem's own object and two denser, stronger draws from the training range
+C4_OBJECTS = {"c2": (0.1, 0.003), "mid": (0.25, 0.006), "strong": (0.4, 0.008)}
+
+
 def run_c4(args):
     """Learned initialiser: train the CNN2d (5 levels, 32 base filters, BF16 tcgen05
     kernels) on objects simulated by the forward kernel, then compare the time to a
     phase NRMSE target of the plain reconstruction from a flat start and from the
     learned start, on the 512x512x8 / 4-mode / 128^2 / 64x64-scan problem at the
-    configured dose (1e5 counts) and noiseless.  Probe known and fixed in both arms,
-    Adam lr 5e-3 decaying 0.97 per iteration, batch 256."""
+    configured dose (1e5 counts) and noiseless, for the held-out objects of
+    ``C4_OBJECTS``.  Probe known and fixed in both arms, Adam lr 5e-3 decaying 0.97 per
+    iteration, batch 256.  Targets: NRMSE 1e-2 and 1.05 x the best NRMSE the flat start
+    reaches in the run (the plain method's own plateau)."""
     import torch
 
     from quantem_b200 import engine, ops, synthetic
@@ -813,7 +820,7 @@ def run_c4(args):
     # the reference's own reconstruction of the same data (fresh process, GPU): its best phase
     # NRMSE is the target both arms are timed to
     ref = {}
-    for dose, counts in (("1e5", 1e5), ("noiseless", 1e12)):
+    for dose, counts in (() if args.skip_torch_reference else (("1e5", 1e5), ("noiseless", 1e12))):
         try:
             env = dict(os.environ)
             cmd = [sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--torch-gpu", "--workload",
@@ -822,72 +829,83 @@ def run_c4(args):
             ref[dose] = json.loads(o.stdout.strip().splitlines()[-1])["reference_torch_gpu"]
         except Exception as exc:
             ref[dose] = {"unavailable": f"{type(exc).__name__}: {exc}"[:300]}
-    thresholds = [0.5, 0.3, 0.1, 0.05, 0.02, 0.01]
-    for dose in ref:
-        if "best_nrmse" in ref[dose]:
-            thresholds.append(round(ref[dose]["best_nrmse"] * 1.05, 5))
+    base_thresholds = [0.5, 0.3, 0.1, 0.05, 0.02, 0.01]
     results = {}
-    for dose in ("1e5", "noiseless"):
-        dcfg = synthetic.SyntheticConfig(seed=0, counts=1e5 if dose == "1e5" else 1e12)
-        ds = synthetic.make_dataset(dcfg, dev)
-        truth = proj_phase(ds["obj"])
-        lo, hi = dcfg.pad_px, dcfg.pad_px + int((dcfg.scan[0] - 1) * dcfg.step_px)
-        crop = (slice(lo, hi), slice(lo, hi))
-        S, Ho, Wo = ds["obj_shape"]
-        probe = (ds["probes"] * (ds["mean_intensity"] / ds["probes"].abs().square().sum()) ** 0.5).contiguous()
-        arms = {}
-        for arm in ("plain", "learned"):
-            torch.cuda.synchronize()
-            t0 = time.time()
-            if arm == "learned":
-                judge = dict(probe=probe, prop=ds["propagators"], positions=ds["positions"],
-                             targets=ds["amplitudes"].contiguous(), mask=torch.ones((dcfg.n, dcfg.n), device=dev),
-                             mean_intensity=ds["mean_intensity"],
-                             batch=torch.arange(0, ds["positions"].shape[0], 4, device=dev))
-                o0 = li.initial_object(ds["amplitudes"], dcfg.scan, (S, Ho, Wo), (dcfg.pad_px, dcfg.pad_px),
-                                       judge=judge)
-            else:
-                o0 = torch.ones((S, Ho, Wo), dtype=torch.complex64, device=dev)
-            torch.cuda.synchronize()
-            elapsed = time.time() - t0
-            obj = o0.clone().requires_grad_(True)
-            pt = engine.ProblemTensors(obj=obj, probe=probe.clone().requires_grad_(True), prop=ds["propagators"],
-                                       positions=ds["positions"], targets=ds["amplitudes"].contiguous(),
-                                       mask=torch.ones((dcfg.n, dcfg.n), device=dev),
-                                       mean_intensity=ds["mean_intensity"], upsample_factor=dcfg.step_px)
-            opt = engine.make_optimizer([obj], {"type": "adam", "lr": 5e-3})
-            sched = torch.optim.lr_scheduler.ExponentialLR(opt, 0.97)
-            bt = SimpleBatcher(pt.num_gpts, 256, rng=0)
-            with torch.no_grad():
-                curve = [(0, round(elapsed, 4), round(nrmse(proj_phase(ops.constrained_object(obj.detach()))[crop],
-                                                           truth[crop]), 5))]
-            for it in range(1, args.c4_iters + 1):
-                s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                s0.record()
-                engine.run_iteration(pt, bt, [opt])
-                s1.record()
-                sched.step()
+    for oname, (peak, density) in C4_OBJECTS.items():
+        results[oname] = {}
+        for dose in ("1e5", "noiseless"):
+            thresholds = list(base_thresholds)
+            if oname == "c2" and "best_nrmse" in ref.get(dose, {}):
+                thresholds.append(round(ref[dose]["best_nrmse"] * 1.05, 5))
+            dcfg = synthetic.SyntheticConfig(seed=0, counts=1e5 if dose == "1e5" else 1e12, peak_phase=peak,
+                                             atom_density=density)
+            ds = synthetic.make_dataset(dcfg, dev)
+            truth = proj_phase(ds["obj"])
+            true_sum = ds["obj"].angle().sum(0)  # unwrapped projected phase
+            lo, hi = dcfg.pad_px, dcfg.pad_px + int((dcfg.scan[0] - 1) * dcfg.step_px)
+            crop = (slice(lo, hi), slice(lo, hi))
+            S, Ho, Wo = ds["obj_shape"]
+            probe = (ds["probes"] * (ds["mean_intensity"] / ds["probes"].abs().square().sum()) ** 0.5).contiguous()
+            arms = {}
+            for arm in ("plain", "learned"):
                 torch.cuda.synchronize()
-                elapsed += s0.elapsed_time(s1) / 1e3
+                t0 = time.time()
+                if arm == "learned":
+                    judge = dict(probe=probe, prop=ds["propagators"], positions=ds["positions"],
+                                 targets=ds["amplitudes"].contiguous(), mask=torch.ones((dcfg.n, dcfg.n), device=dev),
+                                 mean_intensity=ds["mean_intensity"],
+                                 batch=torch.arange(0, ds["positions"].shape[0], 4, device=dev))
+                    o0 = li.initial_object(ds["amplitudes"], dcfg.scan, (S, Ho, Wo), (dcfg.pad_px, dcfg.pad_px),
+                                           judge=judge)
+                else:
+                    o0 = torch.ones((S, Ho, Wo), dtype=torch.complex64, device=dev)
+                torch.cuda.synchronize()
+                elapsed = time.time() - t0
+                obj = o0.clone().requires_grad_(True)
+                pt = engine.ProblemTensors(obj=obj, probe=probe.clone().requires_grad_(True), prop=ds["propagators"],
+                                           positions=ds["positions"], targets=ds["amplitudes"].contiguous(),
+                                           mask=torch.ones((dcfg.n, dcfg.n), device=dev),
+                                           mean_intensity=ds["mean_intensity"], upsample_factor=dcfg.step_px)
+                opt = engine.make_optimizer([obj], {"type": "adam", "lr": 5e-3})
+                sched = torch.optim.lr_scheduler.ExponentialLR(opt, 0.97)
+                bt = SimpleBatcher(pt.num_gpts, 256, rng=0)
                 with torch.no_grad():
-                    curve.append((it, round(elapsed, 4),
-                                  round(nrmse(proj_phase(ops.constrained_object(obj.detach()))[crop], truth[crop]), 5)))
-            reach = {}
-            for th in thresholds:
-                hit = next((c for c in curve if c[2] <= th), None)
-                reach[str(th)] = None if hit is None else hit[1]
-            arms[arm] = dict(time_to_nrmse_s=reach, start_nrmse=curve[0][2], best_nrmse=min(c[2] for c in curve),
-                             final_nrmse=curve[-1][2], curve=curve[:: max(1, len(curve) // 12)],
-                             used_learned_start=(getattr(li, "used_learned", None) if arm == "learned" else None))
-        results[dose] = arms
-    tp = results["noiseless"]["plain"]["time_to_nrmse_s"]["0.01"]
-    tl = results["noiseless"]["learned"]["time_to_nrmse_s"]["0.01"]
+                    err = lambda: round(nrmse(proj_phase(ops.constrained_object(obj.detach()))[crop],  # noqa: E731
+                                              truth[crop]), 5)
+                    curve = [(0, round(elapsed, 4), err())]
+                for it in range(1, args.c4_iters + 1):
+                    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    s0.record()
+                    engine.run_iteration(pt, bt, [opt])
+                    s1.record()
+                    sched.step()
+                    torch.cuda.synchronize()
+                    elapsed += s0.elapsed_time(s1) / 1e3
+                    with torch.no_grad():
+                        curve.append((it, round(elapsed, 4), err()))
+                if arm == "plain":
+                    thresholds.append(round(1.05 * min(c[2] for c in curve), 5))
+                reach = {}
+                for th in thresholds:
+                    hit = next((c for c in curve if c[2] <= th), None)
+                    reach[str(th)] = None if hit is None else hit[1]
+                arms[arm] = dict(time_to_nrmse_s=reach, start_nrmse=curve[0][2], best_nrmse=min(c[2] for c in curve),
+                                 final_nrmse=curve[-1][2], curve=curve[:: max(1, len(curve) // 12)],
+                                 used_learned_start=(getattr(li, "used_learned", None) if arm == "learned" else None))
+            key = str(thresholds[-1])  # 1.05 x the flat start's best
+            tp, tl = arms["plain"]["time_to_nrmse_s"][key], arms["learned"]["time_to_nrmse_s"][key]
+            arms["to_plain_best"] = {"target_nrmse": float(key), "plain_s": tp, "learned_s": tl,
+                                     "ratio": round(tl / tp, 4) if (tp and tl) else None}
+            arms["max_abs_projected_phase"] = round(float(true_sum.abs().max()), 3)
+            results[oname][dose] = arms
+    tp = results["c2"]["noiseless"]["plain"]["time_to_nrmse_s"]["0.01"]
+    tl = results["c2"]["noiseless"]["learned"]["time_to_nrmse_s"]["0.01"]
     # at the benchmark dose: both arms timed to within 5 % of the best NRMSE the reference reaches
     vs_ref = None
     if "best_nrmse" in ref.get("1e5", {}):
         key = str(round(ref["1e5"]["best_nrmse"] * 1.05, 5))
-        rp = results["1e5"]["plain"]["time_to_nrmse_s"].get(key)
-        rl = results["1e5"]["learned"]["time_to_nrmse_s"].get(key)
+        rp = results["c2"]["1e5"]["plain"]["time_to_nrmse_s"].get(key)
+        rl = results["c2"]["1e5"]["learned"]["time_to_nrmse_s"].get(key)
         vs_ref = {"target_nrmse": float(key), "plain_s": rp, "learned_s": rl,
                   "ratio": round(rl / rp, 4) if (rp and rl) else None}
     print(json.dumps({
@@ -898,6 +916,7 @@ def run_c4(args):
         "time_to_reference_best_1e5": vs_ref,
         "config": {"workload": "c4: CNN2d 5 levels x 32 filters on 32x32-binned patterns of a 64x64 scan -> "
                                "projected phase; refinement 512x512x8, 4 modes at 128x128",
+                   "objects": {k: {"peak_phase": v[0], "atom_density": v[1]} for k, v in C4_OBJECTS.items()},
                    "training_objects": nobj, "refine_iterations": args.c4_iters, "probe": "known, fixed"},
         "cnn": {"train_s": round(train_s, 2), "objects_per_s": round(nobj / train_s, 1),
                 "held_out_phase_nrmse": round(held_out, 4),
@@ -1211,7 +1230,10 @@ def _reference_setup(cfg, dev, ref_dir=None, probe_known=False):
     d4 = Dataset4dstem.from_array(data, sampling=(cfg.step_px * cfg.pixel, cfg.step_px * cfg.pixel, rs, rs),
                                   units=("A", "A", "A^-1", "A^-1"))
     pd = PtychographyDatasetRaster.from_dataset4dstem(d4, verbose=0)
-    pd.preprocess(com_fit_function="constant", force_com_rotation=0, force_com_transpose=False,
+    # the simulated patterns are centred exactly: "no_shift" keeps them as simulated (a fitted
+    # centre of mass would shift every pattern by its sub-pixel mean offset, a descan error the
+    # reconstruction then fits with a phase ramp)
+    pd.preprocess(com_fit_function="no_shift", force_com_rotation=0, force_com_transpose=False,
                   plot_rotation=False, plot_com=False, probe_energy=cfg.energy)
     obj_model = ObjectPixelated.from_uniform(num_slices=cfg.slices, slice_thicknesses=cfg.slice_thickness,
                                              obj_type="complex")
