@@ -102,6 +102,21 @@ typedef struct ptycho_batch_args {
                                 autograd adjoint).  Positions enter through the fractional probe shift
                                 only (dataset_models.py:1487-1490, ptycho_utils.py:128-176); entries
                                 whose index is invalid are left untouched.  ABI version 2. */
+  const float* descan;       /* optional float32 (npos, 2): descan shifts [px] (row, column).  The exit
+                                wave is multiplied by exp(-2 pi i (fftfreq(r) d_r + fftfreq(c) d_c)) on
+                                the real-space grid before the detector (ptychography_base.py:903-905,
+                                ptycho_utils.py:156-176).  Serial variant, n < 256.  ABI version 3. */
+  float* grad_descan;        /* optional float32 (B, 2), adjoint launch with descan: dL/d(descan shift)
+                                of every batch entry, summed over the modes (autograd adjoint).
+                                ABI version 3. */
+  float* grad_prop;          /* optional float32 (S-1, 2), zero-filled by the caller, S <= 17; adjoint
+                                launch: accumulates, over the batch and the modes, sum_k fftfreq_index(k)
+                                Im(conj(dL/dZ_s(k)) Z_s(k)) along rows / columns for the propagated
+                                wave Z_s = K_s fft2(chi_s) of every slice.  A per-axis phase ramp
+                                exp(-2 pi i a_s fftfreq_index) of K_s changes the loss at the rate
+                                2 pi times this sum (the probe tilt, probe_models.py:418-425).  The
+                                adjoint then needs the larger scratch that ptycho_batch_plan reports
+                                for these arguments.  ABI version 3. */
 } ptycho_batch_args;
 
 enum {
@@ -119,7 +134,8 @@ int ptycho_abi_version(void);
 /* Number of SMs of the current device. */
 int ptycho_sm_count(int* out);
 
-/* Number of complex64 elements of scratch / partial buffers for a batch launch. */
+/* Number of complex64 elements of scratch / partial buffers for a batch launch
+ * without grad_prop (ptycho_batch_plan sizes every launch). */
 int ptycho_workspace_elems(int n, int S, int P, int grid, int64_t* scratch_elems,
                            int64_t* partial_elems);
 

@@ -307,14 +307,21 @@ class ForwardState:
     intensity: np.ndarray = None  # corner-centred sum over modes (B, H, W)
     g_probe_plane: np.ndarray = None  # set by adjoint: dL/d(shifted probe) (P, B, H, W)
     probe_o: np.ndarray = None        # set by full_gradients: the orthogonalised probe used
+    descan_ramp: np.ndarray = None    # (B, H, W) descan ramp of the exit wave, or None
+    exit: np.ndarray = None           # exit wave (P, B, H, W) after the descan ramp
+    g_exit: np.ndarray = None         # set by adjoint: dL/d(exit) (P, B, H, W)
+    prop_sums: np.ndarray = None      # set by adjoint: (S-1, 2) sum_k fftfreq_idx(k) Im(conj(G_Z) Z)
 
 
 def forward(obj_c: np.ndarray, probe_o: np.ndarray, positions_px: np.ndarray,
-            props: np.ndarray) -> ForwardState:
+            props: np.ndarray, descan: np.ndarray | None = None) -> ForwardState:
     """Batch forward model.
 
     probe shift: ptycho_utils.py:128-139 (fft2 -> ramp -> ifft2), probe_models.py:718-720;
     multislice: ptychography_base.py:934-947, 970-989;
+    descan (optional, (B, 2) px): the exit wave times the translation ramp of the
+    descan shift evaluated on the real-space grid (ptychography_base.py:903-905,
+    ptycho_utils.py:156-176), which moves the far field by -descan pixels;
     detector: detector_models.py:22-30 (orthonormal FFT, |.|^2 summed over modes).
     The returned intensity is corner-centred (before the detector fftshift).
     """
@@ -333,6 +340,10 @@ def forward(obj_c: np.ndarray, probe_o: np.ndarray, positions_px: np.ndarray,
             psi = ifft2(fft2(chi) * props[s][None, None])
         else:
             psi = chi
+    if descan is not None:
+        st.descan_ramp = translation_ramp(np.asarray(descan, dtype=np.float64), (H, W), probe_o.dtype)
+        psi = psi * st.descan_ramp[None]
+    st.exit = psi
     st.far = fft2(psi, norm="ortho")
     st.intensity = np.sum(st.far.real**2 + st.far.imag**2, axis=0)
     return st
@@ -385,12 +396,25 @@ def adjoint(obj_c, probe_o, props, st: ForwardState, dL_dI: np.ndarray):
     H, W = probe_o.shape[-2:]
     g_far = 2.0 * st.far * dL_dI[None]
     g = ifft2(g_far, norm="ortho")  # adjoint of the orthonormal FFT
+    st.g_exit = g
+    if st.descan_ramp is not None:
+        g = g * np.conj(st.descan_ramp)[None]
     g_patch = np.zeros_like(st.patches)
+    fr = fftfreq_index(H).astype(np.float64)[:, None]
+    fc = fftfreq_index(W).astype(np.float64)[None, :]
+    st.prop_sums = np.zeros((max(S - 1, 0), 2))
     for s in reversed(range(S)):
         psi = st.waves[s]
         g_patch[s] = np.sum(np.conj(psi) * g, axis=0)
         g = np.conj(st.patches[s])[None] * g
         if s > 0:
+            # propagator sensitivity: Z = fft2(chi_{s-1}) K_{s-1} enters w_s = ifft2(Z), so
+            # dL/dZ = fft2(g) / (H W) (torch convention) and sum_k k Im(conj(dL/dZ) Z) carries
+            # every per-axis phase ramp of K (the tilt terms of probe_models.py:418-425)
+            gz = fft2(g) / (H * W)
+            z = fft2(st.patches[s - 1][None] * st.waves[s - 1]) * props[s - 1][None, None]
+            im = np.imag(np.conj(gz) * z)
+            st.prop_sums[s - 1] = (np.sum(fr * im), np.sum(fc * im))
             g = ifft2(fft2(g) * np.conj(props[s - 1])[None, None])
     # probe shift adjoint: ifft2(sum_b conj(ramp_b) * fft2(g_b))
     acc = np.sum(fft2(g) * np.conj(st.ramp)[None], axis=1)
@@ -416,9 +440,37 @@ def position_gradients(probe_o, st: ForwardState, g_probe_plane: np.ndarray) -> 
     return np.stack([gr, gc], axis=-1)
 
 
+def descan_gradients(st: ForwardState) -> np.ndarray:
+    """dL/d(descan shift) (B, 2): the exit wave is E = Y ramp(d) with
+    ramp = exp(-2 pi i (fftfreq_r d_r + fftfreq_c d_c)) on the real-space grid, so
+    dL/dd_r = sum over modes and pixels of 2 pi fftfreq_r Im(conj(dL/dE) E)."""
+    H, W = st.exit.shape[-2:]
+    kr = np.fft.fftfreq(H, d=1.0)[None, None, :, None]
+    kc = np.fft.fftfreq(W, d=1.0)[None, None, None, :]
+    im = np.imag(np.conj(st.g_exit) * st.exit)
+    return np.stack([np.sum(2 * np.pi * kr * im, axis=(0, 2, 3)), np.sum(2 * np.pi * kc * im, axis=(0, 2, 3))], -1)
+
+
+def tilt_gradients(st: ForwardState, tilt_mrad, slice_thicknesses, sampling, roi_shape) -> np.ndarray:
+    """dL/d(probe tilt) (2,) [1/mrad] of a batch.  K_s carries exp(-2 pi i dz_s tan(theta/1e3) k)
+    per axis (probe_models.py:418-425), so dL/dtheta = sum_s 2 pi dz_s sec^2(theta/1e3)/1e3
+    sum_k k Im(conj(dL/dZ_s) Z_s).  The reference multiplies the ramp in only when
+    theta != 0 (probe_models.py:418, 421), so a zero tilt has a zero gradient."""
+    dz = np.broadcast_to(np.atleast_1d(np.asarray(slice_thicknesses, dtype=np.float64)), (st.prop_sums.shape[0],))
+    out = np.zeros(2)
+    for a in range(2):
+        th = float(tilt_mrad[a])
+        if th == 0.0 or st.prop_sums.shape[0] == 0:
+            continue
+        k_unit = 1.0 / (int(roi_shape[a]) * float(sampling[a]))  # fftfreq(n, d) = index / (n d)
+        sec2 = 1.0 / math.cos(th / 1e3) ** 2
+        out[a] = float(np.sum(2 * np.pi * dz * st.prop_sums[:, a])) * k_unit * sec2 / 1e3
+    return out
+
+
 def batch_loss_and_grads(obj_c, probe_o, positions_px, props, targets, mask, num_gpts,
-                         mean_intensity, loss_type="l2_amplitude"):
-    st = forward(obj_c, probe_o, positions_px, props)
+                         mean_intensity, loss_type="l2_amplitude", descan=None):
+    st = forward(obj_c, probe_o, positions_px, props, descan)
     loss, dI = loss_and_seed(st.intensity, targets, mask, num_gpts, mean_intensity, loss_type)
     g_obj, g_probe = adjoint(obj_c, probe_o, props, st, dI)
     return loss, g_obj, g_probe, st
@@ -426,18 +478,20 @@ def batch_loss_and_grads(obj_c, probe_o, positions_px, props, targets, mask, num
 
 def full_gradients(obj_raw, probe_raw, positions_px, props, targets, mask, num_gpts,
                    mean_intensity, upsample_factor, orthogonalize=True,
-                   loss_type="l2_amplitude", obj_type="complex"):
+                   loss_type="l2_amplitude", obj_type="complex", descan=None):
     """Loss and gradients w.r.t. the raw parameters, as Ptychography.backward
     leaves them (autograd branch, ptychography.py:326-332): the object gradient
     is scaled by upsample_factor**2 / 2.  ``obj_type``: complex, pure_phase or
-    potential (default constraints: positivity on, baseline not fixed)."""
+    potential (default constraints: positivity on, baseline not fixed).  ``descan``:
+    (B, 2) descan shifts of the batch or None; ``descan_gradients(st)`` and
+    ``tilt_gradients(st, ...)`` read the returned state."""
     obj_c = object_transmission(obj_raw, obj_type)
     if orthogonalize:
         probe_o, _, cache = gram_schmidt(probe_raw)
     else:
         probe_o, cache = probe_raw, None
     loss, g_obj_c, g_probe_o, st = batch_loss_and_grads(
-        obj_c, probe_o, positions_px, props, targets, mask, num_gpts, mean_intensity, loss_type)
+        obj_c, probe_o, positions_px, props, targets, mask, num_gpts, mean_intensity, loss_type, descan)
     st.probe_o = probe_o
     g_obj = object_transmission_vjp(obj_raw, g_obj_c, obj_type) * (upsample_factor**2 / 2)
     g_probe = gram_schmidt_vjp(cache, g_probe_o) if orthogonalize else g_probe_o
@@ -521,38 +575,61 @@ def gaussian_atom_phase(shape, n_atoms, sigma_px, peak_rad, rng):
 
 def reconstruct(obj_raw, probe_raw, positions_px, props, targets, mask, mean_intensity, upsample_factor,
                 num_iters, batch_size, rng, lr_obj=5e-3, lr_probe=1e-3, orthogonalize=True,
-                loss_type="l2_amplitude", obj_type="complex", lr_positions=None):
+                loss_type="l2_amplitude", obj_type="complex", lr_positions=None, descan=None, lr_descan=None,
+                tilt=None, prop_geometry=None):
     """Adam iterations of Ptychography.reconstruct (ptychography.py:208-245) on
     the given state; batches from a numpy generator like SimpleBatcher.  With
     ``lr_positions`` the scan positions are a parameter too (a dataset optimiser,
     dataset_models.py:98-110): Adam over the whole (N, 2) array, the gradient zero
-    outside the batch.  Returns (obj, probe, per-iteration mean batch losses), plus the
-    positions with ``lr_positions``."""
+    outside the batch.  ``descan`` ((N, 2) start) applies descan shifts, learned with
+    Adam at ``lr_descan`` (the same dataset optimiser).  ``tilt`` ((2,) mrad start, with
+    ``prop_geometry`` = (roi_shape, sampling, energy, slice_thicknesses)) learns the probe
+    tilt in the probe's Adam (lr_probe; probe_models.py:295-304), the propagators
+    recomputed from it for every batch.  Returns (obj, probe, per-iteration mean batch
+    losses), plus the positions with ``lr_positions``, plus a dict with "descan" / "tilt"
+    when either is given."""
     obj = obj_raw.copy()
     probe = probe_raw.copy()
     pos = positions_px.astype(np.float64).copy()
-    so, sp, spos = AdamState(), AdamState(), AdamState()
+    dsc = None if descan is None else np.asarray(descan, dtype=np.float64).copy()
+    th = None if tilt is None else np.asarray(tilt, dtype=np.float64).copy()
+    so, sp, spos, sdsc, sth = AdamState(), AdamState(), AdamState(), AdamState(), AdamState()
     npos = positions_px.shape[0]
     losses = []
     for _ in range(num_iters):
         tot, nb = 0.0, 0
         for bi in batch_order(rng, npos, batch_size):
+            if th is not None:
+                roi, samp, energy, dz = prop_geometry
+                props = propagators(roi, samp, energy, dz, tilt_mrad=tuple(th))
             loss, g_obj, g_probe, st = full_gradients(obj, probe, pos[bi], props, targets[bi], mask, npos,
                                                       mean_intensity, upsample_factor, orthogonalize, loss_type,
-                                                      obj_type)
+                                                      obj_type, descan=None if dsc is None else dsc[bi])
             if lr_positions is not None:
                 g_pos = np.zeros_like(pos)
                 g_pos[bi] = position_gradients(st.probe_o, st, st.g_probe_plane)
+            if dsc is not None and lr_descan is not None:
+                g_dsc = np.zeros_like(dsc)
+                g_dsc[bi] = descan_gradients(st)
+            if th is not None:
+                g_th = tilt_gradients(st, th, prop_geometry[3], prop_geometry[1], prop_geometry[0])
             adam_step(obj, g_obj, so, lr_obj)
             adam_step(probe, g_probe, sp, lr_probe)
+            if th is not None:
+                adam_step(th, g_th, sth, lr_probe)
             if lr_positions is not None:
                 adam_step(pos, g_pos, spos, lr_positions)
+            if dsc is not None and lr_descan is not None:
+                adam_step(dsc, g_dsc, sdsc, lr_descan)
             tot += loss
             nb += 1
         losses.append(tot / nb)
+    res = (obj, probe, np.array(losses))
     if lr_positions is not None:
-        return obj, probe, np.array(losses), pos
-    return obj, probe, np.array(losses)
+        res = res + (pos,)
+    if dsc is not None or th is not None:
+        res = res + ({"descan": dsc, "tilt": th},)
+    return res
 
 
 # ----------------------------------------------------------------------------

@@ -93,6 +93,7 @@ class BatchArgs(ctypes.Structure):
         ("npos", _int), ("grid", _int), ("loss_type", _int),
         ("loss_scale", _flt), ("inv_mean_intensity", _flt), ("variant", _int),
         ("analytic", _int), ("an_norm", _vp), ("recompute_every", _int), ("grad_positions", _vp),
+        ("descan", _vp), ("grad_descan", _vp), ("grad_prop", _vp),
     ]
 
 

@@ -40,6 +40,9 @@ inline BatchParams to_params(const ptycho_batch_args* a) {
   p.an_norm = a->an_norm;
   p.ckpt = a->recompute_every;
   p.grad_positions = a->grad_positions;
+  p.descan = a->descan;
+  p.grad_descan = a->grad_descan;
+  p.grad_prop = a->grad_prop;
   return p;
 }
 
@@ -48,12 +51,35 @@ size_t batch_smem(const ptycho_batch_args* a) {
   return a->prop_r ? fused_smem_bytes_sep<N>(a->S) : fused_smem_bytes<N>();
 }
 
+// the serial kernel with its optional extensions compiled in (descan, position / descan /
+// propagator gradients)
+inline bool wants_ext(const ptycho_batch_args* a) {
+  return a->descan || a->grad_descan || a->grad_prop || a->grad_positions;
+}
+
+template <int N, bool ADJ>
+void launch_ext(const BatchParams& p, int grid, size_t smem, cudaStream_t st) {
+  cudaFuncSetAttribute(fused_batch_kernel<N, ADJ, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)smem);
+  if (ADJ)
+    cudaFuncSetAttribute(fused_batch_kernel<N, ADJ, false, true>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         (int)((smem + 1024) * 100 / (228 * 1024) + 1));
+  fused_batch_kernel<N, ADJ, false, true><<<grid, Fft2<N>::T, smem, st>>>(p);
+}
+
 // one CTA per position, modes in sequence
 template <int N>
 int launch_serial(const ptycho_batch_args* a, bool adj, cudaStream_t st) {
   const BatchParams p = to_params(a);
   const size_t smem = adj ? batch_smem_bytes<N, true>(a->prop_r != nullptr, a->S)
                           : batch_smem_bytes<N, false>(a->prop_r != nullptr, a->S);
+  if (wants_ext(a) && !a->analytic) {
+    if (adj)
+      launch_ext<N, true>(p, a->grid, smem, st);
+    else
+      launch_ext<N, false>(p, a->grid, smem, st);
+    return cudaPeekAtLastError() == cudaSuccess ? PTYCHO_OK : PTYCHO_ERR_CUDA;
+  }
   // the attribute is per device; setting it on every launch keeps multi-device
   // processes correct and costs far less than one launch
   if (adj && a->analytic) {

@@ -8,6 +8,7 @@
 
 #include "ptycho_b200.h"
 #include "cluster256_kernels.cuh"
+#include "launch_impl.cuh"
 #include "ptycho_kernels.cuh"
 
 namespace {
@@ -434,6 +435,12 @@ int validate_batch(const ptycho_batch_args* a, bool adj) {
   for (const void* q : ptrs)
     if (q && !aligned(q, 8)) return fail(PTYCHO_ERR_INVALID, "complex buffer not 8-byte aligned");
   if (a->loss_type < 0 || a->loss_type > 4) return fail(PTYCHO_ERR_INVALID, "bad loss type %d", a->loss_type);
+  if ((a->grad_descan || a->grad_prop) && (!adj || a->analytic))
+    return fail(PTYCHO_ERR_UNSUPPORTED, "descan / propagator gradients come from the autograd adjoint launch");
+  if (a->grad_descan && !a->descan) return fail(PTYCHO_ERR_INVALID, "grad_descan needs the descan shifts");
+  if (a->grad_prop && a->S > 17)
+    return fail(PTYCHO_ERR_UNSUPPORTED, "propagator gradients are built for up to 17 slices (S=%d)", a->S);
+  if (a->descan && a->analytic) return fail(PTYCHO_ERR_UNSUPPORTED, "descan shifts with the analytic update");
   if (a->analytic) {
     if (!adj) return fail(PTYCHO_ERR_INVALID, "analytic is an adjoint-launch option");
     if (!a->an_norm) return fail(PTYCHO_ERR_INVALID, "analytic update needs an_norm");
@@ -460,14 +467,16 @@ int run_batch(const ptycho_batch_args* a, void* stream, bool adj) {
   if (a->n == 256) {
     if (a->grad_positions)
       return fail(PTYCHO_ERR_UNSUPPORTED, "position gradients are not built for 256 x 256 windows");
+    if (a->descan || a->grad_descan || a->grad_prop)
+      return fail(PTYCHO_ERR_UNSUPPORTED, "descan shifts and propagator gradients are not built for 256 x 256 windows");
     const int lrc = qb_launch_c256(a, adj, static_cast<cudaStream_t>(stream));
     if (lrc) return fail(lrc, "cluster256_kernel launch: %s", cudaGetErrorString(cudaGetLastError()));
     return PTYCHO_OK;
   }
   if (a->grad_positions && (!adj || a->analytic))
     return fail(PTYCHO_ERR_UNSUPPORTED, "position gradients come from the autograd adjoint launch");
-  // position gradients are summed over the modes inside one CTA: serial variant
-  const int variant = (a->analytic || a->grad_positions) ? PTYCHO_VARIANT_SERIAL : resolve_variant(a);
+  // the extensions (descan, position / descan / propagator gradients) live in the serial kernel
+  const int variant = (a->analytic || qb::wants_ext(a)) ? PTYCHO_VARIANT_SERIAL : resolve_variant(a);
   if (variant < 0) return fail(PTYCHO_ERR_UNSUPPORTED, "variant %d not available for P=%d", a->variant, a->P);
   if (variant == PTYCHO_VARIANT_CLUSTER && a->grid % a->P != 0)
     return fail(PTYCHO_ERR_INVALID, "cluster launch: grid %d is not a multiple of P=%d", a->grid, a->P);
@@ -491,7 +500,8 @@ int ptycho_get_last_error(char* buf, size_t len) {
   return PTYCHO_OK;
 }
 
-int ptycho_abi_version(void) { return 2; }  // 2: ptycho_batch_args.grad_positions
+// 2: ptycho_batch_args.grad_positions; 3: descan, grad_descan, grad_prop
+int ptycho_abi_version(void) { return 3; }
 
 int ptycho_sm_count(int* out) {
   if (!out) return fail(PTYCHO_ERR_INVALID, "out is NULL");
@@ -530,7 +540,7 @@ int ptycho_batch_plan(const ptycho_batch_args* a, int adjoint, int* variant, int
     if (partial_parts) *partial_parts = ncl;
     return PTYCHO_OK;
   }
-  const int v = a->analytic ? PTYCHO_VARIANT_SERIAL : resolve_variant(a);
+  const int v = (a->analytic || qb::wants_ext(a)) ? PTYCHO_VARIANT_SERIAL : resolve_variant(a);
   if (v < 0) return fail(PTYCHO_ERR_UNSUPPORTED, "variant %d not available for P=%d", a->variant, a->P);
   int sms = 0, dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -551,7 +561,8 @@ int ptycho_batch_plan(const ptycho_batch_args* a, int adjoint, int* variant, int
   } else {
     g = B < sms ? B : sms;
     parts = g;
-    scr = (int64_t)g * (a->P * a->S + a->P + 1) * nn;  // waves, far fields, intensity tile
+    // waves, far fields, intensity tile (+ the Fourier waves after each propagation)
+    scr = (int64_t)g * (a->P * a->S + a->P + 1 + (a->grad_prop ? a->P * (a->S - 1) : 0)) * nn;
     part = (int64_t)g * a->P * nn;
   }
   if (variant) *variant = v;
@@ -579,6 +590,9 @@ int ptycho_forward_adjoint_multi(const ptycho_batch_args* sets, int nsets, void*
     if (sets[d].n != sets[0].n) return fail(PTYCHO_ERR_INVALID, "multi: every dataset needs the same probe window");
     if (sets[d].n == 256 || sets[d].analytic)
       return fail(PTYCHO_ERR_UNSUPPORTED, "multi: datasets with n = 64 / 128 and the autograd adjoint only");
+    if (qb::wants_ext(&sets[d]))
+      return fail(PTYCHO_ERR_UNSUPPORTED,
+                  "multi: descan shifts and position / descan / propagator gradients run on ptycho_forward_adjoint");
     if (sets[d].grid < 1) return fail(PTYCHO_ERR_INVALID, "multi: dataset %d has grid %d", d, sets[d].grid);
     total += sets[d].grid;
   }

@@ -62,6 +62,9 @@ struct BatchParams {
   float* an_norm;             // (S, P, Ho, Wo) scatter of |psi|^2 for the analytic normalisation
   int ckpt;                   // 256^2 cluster kernel: checkpoint interval of the adjoint (0 = keep all waves)
   float* grad_positions;      // optional (B, 2) dL/d(position), serial autograd adjoint only
+  const float* descan;        // optional (npos, 2) descan shifts [px] applied to the exit wave
+  float* grad_descan;         // optional (B, 2) dL/d(descan), serial autograd adjoint only
+  float* grad_prop;           // optional (S-1, 2) propagator sensitivities, serial autograd adjoint only
 };
 
 // Status word of the batch kernels: bits 0-19 count non-finite predicted
@@ -237,6 +240,22 @@ __device__ __forceinline__ void gather_mul(const Fft2<N>& f, float2 (&x)[Fft2<N>
   }
 }
 
+// Descan (ptychography_base.py:903-905): the exit wave (S1 layout) times the
+// translation ramp of the descan shift (dr, dc) evaluated on the real-space grid,
+// exp(-2 pi i (fftfreq(r) dr + fftfreq(c) dc)) (ptycho_utils.py:156-176); CONJ: its
+// conjugate, for the adjoint.
+template <int N, bool CONJ>
+__device__ __forceinline__ void descan_mul(const Fft2<N>& f, float2 (&x)[Fft2<N>::E], float dr, float dc) {
+  constexpr int E = Fft2<N>::E;
+  const float ar = (float)fsigned(f.s1_r, N) * dr;
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    float sn, cs;
+    sincospif(-2.0f * (ar + (float)fsigned(f.s1_col(e), N) * dc) / (float)N, &sn, &cs);
+    x[e] = CONJ ? cmulc(x[e], make_float2(cs, sn)) : cmul(x[e], make_float2(cs, sn));
+  }
+}
+
 // Fourier-space probe-gradient partial (S3 layout): pg += conj(ramp) * x, batched RMW.
 template <int N>
 __device__ __forceinline__ void accumulate_probe_grad(const Fft2<N>& f, const float2 (&x)[Fft2<N>::E], float2* pg,
@@ -261,7 +280,9 @@ __device__ __forceinline__ void accumulate_probe_grad(const Fft2<N>& f, const fl
 
 // Body of the serial batch kernel for one dataset: CTA `cta` of the `ncta` CTAs
 // that work on this dataset's positions.
-template <int N, bool ADJ, bool AN = false>
+// EXT: the optional extensions (descan shifts, position / descan / propagator gradients)
+// are compiled in; the default kernel carries none of their code or registers.
+template <int N, bool ADJ, bool AN = false, bool EXT = false>
 __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta, const int ncta) {
   // AN (compile time): analytic update directions instead of the autograd adjoint,
   // so the autograd kernel carries none of the analytic code or live values
@@ -285,7 +306,8 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
   const uint64_t pol = evict_last_policy();
   __shared__ double red[32];
   __shared__ int nfred[32];  // per-warp non-finite counts
-  __shared__ float posred[32][2];  // per-warp position-gradient partials
+  __shared__ float posred[32][2];  // per-warp position / descan gradient partials
+  __shared__ float propred[2 * 16];  // EXT: this CTA's propagator sensitivities (S <= 17)
 
   const int tid = threadIdx.x;
   F f;
@@ -306,7 +328,15 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
   const size_t NN = (size_t)N * N;
   const int S = p.S, P = p.P;
   const size_t HoWo = (size_t)p.Ho * p.Wo;
-  float2* slot = ADJ ? p.scratch + (size_t)cta * (size_t)(P * S + P + 1) * NN : nullptr;
+  // scratch slots per CTA: P*S incident waves, P far fields, the intensity tile and (EXT
+  // with propagator sensitivities) the P*(S-1) Fourier-space waves after each propagation
+  const bool want_prop = EXT && ADJ && p.grad_prop != nullptr;
+  const size_t nslot = (size_t)(P * S + P + 1) + (want_prop ? (size_t)P * (S - 1) : 0);
+  float2* slot = ADJ ? p.scratch + (size_t)cta * nslot * NN : nullptr;
+  float2* zslot = want_prop ? slot + (size_t)(P * S + P + 1) * NN : nullptr;
+  if (want_prop) {
+    for (int k = tid; k < 2 * 16; k += T) propred[k] = 0.f;
+  }
   float* inten = ADJ ? reinterpret_cast<float*>(slot + (size_t)(P * S + P) * NN) : inten_sm;
   // Per-thread saved data (waves, far fields, intensities) is thread-major with the
   // register pair (e, e+1) packed into one word: one 16-byte (waves) or 8-byte
@@ -419,6 +449,7 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
           for (int e = 0; e < E; ++e) ow[f.s1_col(e)] = x[e];
         }
         gather_mul<N, false>(f, x, orow_ptr, colmap, pol);
+        if (EXT && s == S - 1 && p.descan) descan_mul<N, false>(f, x, __ldg(p.descan + 2 * gi), __ldg(p.descan + 2 * gi + 1));
         if (s == S - 1 && p.out_exit) {
           float2* oe = p.out_exit + ((size_t)m * p.B + b) * NN + (size_t)f.s1_r * N;
 #pragma unroll
@@ -428,6 +459,10 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
         const float sc = first_bwd ? inv_n : inv_n2;  // adjoint of the orthonormal FFT, or of a propagation
         const float2* wv = slot + (size_t)(m * S + s) * NN;
         float2* grow = p.grad_obj + (size_t)s * HoWo + (size_t)orow * p.Wo;
+        // the exit wave carries the descan ramp: its gradient times conj(ramp) is the
+        // gradient of the last slice's transmitted wave
+        if (EXT && first_bwd && p.descan)
+          descan_mul<N, true>(f, x, __ldg(p.descan + 2 * gi), __ldg(p.descan + 2 * gi + 1));
 #pragma unroll
         for (int e0 = 0; e0 < E; e0 += 8) {
           float2 ps[8], ob[8];
@@ -454,6 +489,43 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
 #pragma unroll
             for (int j = 0; j < 8; ++j) atomicAdd(nrow + col[j], cabs2(ps[j]));
           }
+        }
+        if (EXT && first_bwd && p.grad_descan) {
+          // x = dL/dw of the last slice's incident wave w, so conj(x) w = conj(dL/dE) E for the
+          // exit wave E: dL/d(descan) = (2 pi / N) sum fftfreq_index Im(conj(x) w), summed over the modes
+          float gr = 0.f, gc = 0.f;
+#pragma unroll
+          for (int e = 0; e < E; e += 2) {
+            const float4 v = reinterpret_cast<const float4*>(wv)[(e >> 1) * T + tid];
+            const float im0 = x[e].x * v.y - x[e].y * v.x;
+            const float im1 = x[e + 1].x * v.w - x[e + 1].y * v.z;
+            gc = fmaf((float)fsigned(f.s1_col(e), N), im0, gc);
+            gc = fmaf((float)fsigned(f.s1_col(e + 1), N), im1, gc);
+            gr += im0 + im1;
+          }
+          gr *= (float)fsigned(f.s1_r, N);
+          for (int o = 16; o > 0; o >>= 1) {
+            gr += __shfl_xor_sync(0xffffffffu, gr, o);
+            gc += __shfl_xor_sync(0xffffffffu, gc, o);
+          }
+          if ((tid & 31) == 0) {
+            posred[tid >> 5][0] = gr;
+            posred[tid >> 5][1] = gc;
+          }
+          __syncthreads();
+          if (tid == 0) {  // fixed-order sum over warps, accumulated over the modes of this position
+            float sr = 0.f, scc = 0.f;
+            for (int w = 0; w < T / 32; ++w) {
+              sr += posred[w][0];
+              scc += posred[w][1];
+            }
+            const float k = 6.283185307179586f / (float)N;
+            float* out = p.grad_descan + 2 * (size_t)b;
+            const bool first = m == P - 1;  // the reverse chains run last mode first
+            out[0] = (first ? 0.f : out[0]) + k * sr;
+            out[1] = (first ? 0.f : out[1]) + k * scc;
+          }
+          __syncthreads();
         }
         if (AN && s == 0) {
           // analytic probe update: sum over positions of the back-propagated
@@ -482,6 +554,7 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
       if (!bwd) {
         if (s < S - 1) {
           apply_prop<N, false>(f, x, p, s, sep, sKr, sKc);
+          if (want_prop) store_pairs<E, T>(zslot + (size_t)(m * (S - 1) + s) * NN, tid, x);  // Z_s = K_s fft2(chi_s)
           ++s;
           continue;
         }
@@ -551,12 +624,40 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
       }
       first_bwd = false;
       if (s > 0) {
+        if (want_prop) {
+          // x = N^2 dL/dZ for Z = K_{s-1} fft2(chi_{s-1}) (w_s = ifft2(Z)): sum over this thread's
+          // frequencies of fftfreq_index * Im(conj(dL/dZ) Z), the sensitivity of the loss to a
+          // phase ramp of the propagator along each axis (the probe tilt, probe_models.py:418-425)
+          const float2* zw = zslot + (size_t)(m * (S - 1) + s - 1) * NN;
+          float gr = 0.f, gc = 0.f;
+#pragma unroll
+          for (int g = 0; g < G3; ++g)
+#pragma unroll
+            for (int e = 0; e < D; e += 2) {
+              const int i = g * D + e;
+              const float4 v = reinterpret_cast<const float4*>(zw)[(i >> 1) * T + tid];
+              const float im0 = x[i].x * v.y - x[i].y * v.x;
+              const float im1 = x[i + 1].x * v.w - x[i + 1].y * v.z;
+              gr = fmaf((float)fsigned(f.s3_row(g, e), N), im0, gr);
+              gr = fmaf((float)fsigned(f.s3_row(g, e + 1), N), im1, gr);
+              gc += im0 + im1;
+            }
+          gc *= (float)fsigned(f.s3_c, N);
+          for (int o = 16; o > 0; o >>= 1) {
+            gr += __shfl_xor_sync(0xffffffffu, gr, o);
+            gc += __shfl_xor_sync(0xffffffffu, gc, o);
+          }
+          if ((tid & 31) == 0) {
+            atomicAdd(&propred[2 * (s - 1)], gr * inv_n2);
+            atomicAdd(&propred[2 * (s - 1) + 1], gc * inv_n2);
+          }
+        }
         apply_prop<N, true>(f, x, p, s - 1, sep, sKr, sKc);
         --s;
         continue;
       }
       accumulate_probe_grad<N>(f, x, pgrad + (size_t)m * NN, rowf, colf);
-      if (p.grad_positions) {
+      if (EXT && p.grad_positions) {
         // positions enter through the probe shift Y = probe_hat * ramp(frac) only; x = N^2 dL/dY
         // here, so dL/dfrac = (2 pi / N^2) sum_k fftfreq(k) Im(conj(x_k) Y_k), summed over the modes
         const float2* ph = p.probe_hat + (size_t)m * NN;
@@ -624,11 +725,12 @@ __device__ __forceinline__ void serial_body(const BatchParams& p, const int cta,
     // l1/l2: sum / (B / num_gpts) / mean_I ; poisson: sum / mean_I
     p.loss_part[cta] = t * (double)(p.loss_type == LOSS_POISSON ? p.inv_mean_intensity : p.loss_scale);
   }
+  if (want_prop && tid < 2 * (S - 1)) atomicAdd(p.grad_prop + tid, propred[tid]);  // after the barrier above
 }
 
-template <int N, bool ADJ, bool AN = false>
+template <int N, bool ADJ, bool AN = false, bool EXT = false>
 __global__ void __launch_bounds__(Fft2<N>::T, 1) fused_batch_kernel(const BatchParams p) {
-  serial_body<N, ADJ, AN>(p, blockIdx.x, gridDim.x);
+  serial_body<N, ADJ, AN, EXT>(p, blockIdx.x, gridDim.x);
 }
 
 // Several independent datasets (same probe window N; any S, P, object size,

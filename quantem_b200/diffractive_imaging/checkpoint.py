@@ -73,7 +73,8 @@ def _object_state(obj):
 
 def _probe_state(probe):
     return {"class": type(probe).__name__, "num_probes": probe.num_probes, "probe_params": dict(probe.probe_params),
-            "probe_tilt": probe.probe_tilt.tolist(), "from_params": probe._from_params,
+            "probe_tilt": probe.probe_tilt.tolist(), "initial_probe_tilt": probe._initial_probe_tilt.tolist(),
+            "learn_probe_tilt": probe.learn_probe_tilt, "from_params": probe._from_params,
             "roi_shape": None if probe.roi_shape is None else [int(x) for x in probe.roi_shape],
             "initial_probe_weights": _cpu(probe.initial_probe_weights), "rng_seed": probe._rng_seed,
             "constraints": dict(probe.constraints), "probe": _cpu(probe._probe),
@@ -84,6 +85,7 @@ def _dataset_state(dset, save_raw_data):
     state = {"preprocessing_params": dict(dset._preprocessing_params), "constraints": dict(dset.constraints),
              "scan_positions_px": _cpu(dset.scan_positions_px),
              "initial_scan_positions_px": _cpu(dset.initial_scan_positions_px),
+             "descan_shifts": _cpu(dset.descan_shifts), "initial_descan_shifts": _cpu(dset.initial_descan_shifts),
              "probe_energy": dset.probe_energy, "targets_on_host": dset.targets_on_host,
              "learn_descan": dset.learn_descan, "learn_scan_positions": dset.learn_scan_positions,
              "raw": None, **{"optim": _opt_state(dset)}}
@@ -166,7 +168,8 @@ def from_state(cls, state, dset=None, device=None, verbose=None):
     th = os_["slice_thicknesses"]
     obj = ObjectPixelated(os_["num_slices"], th if th else None, os_["obj_type"], os_["initialize_mode"],
                           "cpu", os_["rng_seed"], _token=ObjectPixelated._token)
-    probe = ProbePixelated(pr["num_probes"], pr["probe_params"], tuple(pr["probe_tilt"]), False, pr["roi_shape"],
+    probe = ProbePixelated(pr["num_probes"], pr["probe_params"], tuple(pr["probe_tilt"]),
+                           bool(pr.get("learn_probe_tilt", False)), pr["roi_shape"],
                            torch.complex64, "cpu", pr["rng_seed"], pr["initial_probe_weights"], None,
                            _from_params=pr["from_params"], _token=ProbePixelated._token)
     if pr["initial_probe"] is not None:
@@ -185,10 +188,15 @@ def from_state(cls, state, dset=None, device=None, verbose=None):
         obj.mask = os_["mask"]
     probe._initial_probe = pr["initial_probe"].clone()
     probe._probe = pr["probe"].clone().requires_grad_(True)
+    if "initial_probe_tilt" in pr:
+        probe._initial_probe_tilt = torch.tensor(pr["initial_probe_tilt"], dtype=torch.float32)
     probe.constraints = pr["constraints"]
     dset._constraints = dict(ds["constraints"])
     dset._initial_scan_positions_px = ds["initial_scan_positions_px"].clone()
     dset.scan_positions_px = ds["scan_positions_px"].clone()
+    if "descan_shifts" in ds:
+        dset.descan_shifts = ds["descan_shifts"].clone()
+        dset.initial_descan_shifts = ds["initial_descan_shifts"].clone()
     dset._set_patch_indices(pt.obj_padding_px)
     if ds["targets_on_host"]:
         dset.keep_targets_on_host(True)

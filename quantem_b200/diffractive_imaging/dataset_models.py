@@ -231,7 +231,70 @@ class PtychographyDatasetRaster(OptimizerMixin):
 
     @property
     def descan_shifts(self) -> torch.Tensor:
+        """Descan shifts [px] (num_positions, 2): with ``learn_descan`` and a dataset
+        optimiser, the exit wave of every position is multiplied by their translation
+        ramp (ptychography_base.py:903-905) and the targets are the uncentred patterns."""
         return self._descan_shifts
+
+    @descan_shifts.setter
+    def descan_shifts(self, shifts):
+        t = torch.as_tensor(shifts.detach().cpu().numpy() if isinstance(shifts, torch.Tensor)
+                            else np.asarray(shifts), dtype=getattr(torch, config.get("dtype_real")))
+        if tuple(t.shape) != (self.num_gpts, 2):
+            raise ValueError(f"descan_shifts must have shape {(self.num_gpts, 2)}")
+        self._set_descan(t)
+
+    def _set_descan(self, t: torch.Tensor):
+        """New descan values, kept in the same tensor while an optimiser holds it
+        (dataset_models.py:121-132 assigns ``.data``)."""
+        cur = self._descan_shifts
+        if self.has_optimizer() and isinstance(cur, torch.Tensor) and cur.shape == t.shape:
+            with torch.no_grad():
+                cur.data = t.detach().to(cur.device, cur.dtype).contiguous()
+        else:
+            self._descan_shifts = t.detach().to(self._device).contiguous()
+
+    @property
+    def initial_descan_shifts(self) -> torch.Tensor:
+        """Descan shifts the dataset resets to (dataset_models.py:189-202)."""
+        return self._initial_descan_shifts
+
+    @initial_descan_shifts.setter
+    def initial_descan_shifts(self, shifts):
+        t = torch.as_tensor(shifts.detach().cpu().numpy() if isinstance(shifts, torch.Tensor)
+                            else np.asarray(shifts), dtype=getattr(torch, config.get("dtype_real")))
+        if tuple(t.shape) != (self.num_gpts, 2):
+            raise ValueError(f"initial_descan_shifts must have shape {(self.num_gpts, 2)}")
+        self._initial_descan_shifts = t.to(self._device)
+
+    @property
+    def descan_learned(self) -> bool:
+        """Descan shifts enter the forward model (dataset_models.py:232, 1495): learned and
+        a dataset optimiser is set."""
+        return self.learn_descan and self.has_optimizer()
+
+    def apply_descan_constraints(self, descan: torch.Tensor) -> torch.Tensor | None:
+        """dataset_models.py:588-595: ``descan_shifts_constant`` replaces the shifts by zeros
+        (no gradient reaches them); None stands for those zeros here."""
+        if self._constraints.get("descan_shifts_constant", False):
+            return None
+        return descan
+
+    def batch_descan(self) -> torch.Tensor | None:
+        """The (num_positions, 2) descan shifts the batch kernels apply, or None."""
+        if not self.descan_learned:
+            return None
+        return self.apply_descan_constraints(self._descan_shifts)
+
+    def apply_soft_constraints(self, descan_shifts: torch.Tensor) -> torch.Tensor:
+        """dataset_models.py:564-586: ``descan_tv_weight`` * the mean absolute difference of
+        consecutive shifts (raster order), averaged over the two axes, when descan is
+        learned; zero otherwise."""
+        w = float(self._constraints.get("descan_tv_weight", 0.0))
+        if w <= 0 or not self.descan_learned:
+            return torch.zeros((), dtype=getattr(torch, config.get("dtype_real")), device=descan_shifts.device)
+        return w * (torch.mean(torch.abs(descan_shifts[:, 0].diff())) +
+                    torch.mean(torch.abs(descan_shifts[:, 1].diff()))) / 2
 
     @property
     def positions_px_fractional(self) -> torch.Tensor:
@@ -277,33 +340,39 @@ class PtychographyDatasetRaster(OptimizerMixin):
         self._constraints[key] = value
 
     def get_optimization_parameters(self):
-        """The scan positions when they are learned (dataset_models.py:98-110).  Learned descan
-        shifts are not built on this path: a dataset optimiser needs ``learn_descan=False``."""
+        """The descan shifts and the scan positions, each when learned, in that order
+        (dataset_models.py:98-110)."""
+        params = []
         if self.learn_descan:
-            raise NotImplementedError("learned descan shifts are not part of the B200 path: create the dataset "
-                                      "with learn_descan=False to learn the scan positions")
-        if not self.learn_scan_positions:
+            self._descan_shifts = self._descan_shifts.detach().contiguous().requires_grad_(True)
+            params.append(self._descan_shifts)
+        if self.learn_scan_positions:
+            self._scan_positions_px = self._scan_positions_px.detach().contiguous().requires_grad_(True)
+            params.append(self._scan_positions_px)
+        if not params:
             raise RuntimeError("No parameters to optimize for dataset: learn_descan and learn_scan_positions "
                                "are both False")
-        self._scan_positions_px = self._scan_positions_px.detach().contiguous().requires_grad_(True)
-        return [self._scan_positions_px]
+        return params
 
     def remove_optimizer(self):
         super().remove_optimizer()
         self._scan_positions_px = self._scan_positions_px.detach()
+        self._descan_shifts = self._descan_shifts.detach()
 
     def reset_iter_constraint_losses(self):
         pass
 
     def reset(self):
         self._set_positions(self._initial_scan_positions_px.clone())
+        self._set_descan(self._initial_descan_shifts.clone())
         if self._optimizer is not None:
             self.set_optimizer(self._optimizer_params)
 
     def to(self, device):
         dev, _ = config.validate_device(device)
         self._device = dev
-        for name in ("_scan_positions_px", "_initial_scan_positions_px", "_descan_shifts", "_detector_mask",
+        for name in ("_scan_positions_px", "_initial_scan_positions_px", "_descan_shifts", "_initial_descan_shifts",
+                     "_detector_mask",
                      "_targets", "_centered_amplitudes", "_amplitudes", "_centered_intensities", "_intensities"):
             v = getattr(self, name, None)
             if isinstance(v, torch.Tensor):
@@ -566,11 +635,13 @@ class PtychographyDatasetRaster(OptimizerMixin):
         return self._patch_indices
 
     def _set_targets(self, loss_type):
-        """dataset_models.py:225-242 (descan is not learned on this path)."""
+        """dataset_models.py:225-242: the centred patterns, or the uncentred ones while the
+        descan shifts are learned (they then carry the pattern offsets)."""
+        raw = self.descan_learned
         if "amplitude" in loss_type:
-            t, kind = self._centered_amplitudes, "amplitude"
+            t, kind = (self._amplitudes, "amplitude_raw") if raw else (self._centered_amplitudes, "amplitude")
         elif "intensity" in loss_type or loss_type == "poisson":
-            t, kind = self._centered_intensities, "intensity"
+            t, kind = (self._intensities, "intensity_raw") if raw else (self._centered_intensities, "intensity")
         else:
             raise ValueError(f"Unknown loss type {loss_type}")
         # host-resident targets are built once per kind: a fresh pinned copy of the whole
@@ -593,7 +664,8 @@ class PtychographyDatasetRaster(OptimizerMixin):
         self._set_positions(pos)
 
     def forward(self, batch_indices, obj_padding_px):
-        """(patch_indices, positions_px, positions_px_fractional, None) of a batch."""
+        """(patch_indices, positions_px, positions_px_fractional, descan shifts or None) of a
+        batch (dataset_models.py:1482-1499)."""
         self.apply_hard_constraints(obj_padding_px)
         bi = torch.as_tensor(np.asarray(batch_indices), device=self.scan_positions_px.device)
         positions = self.scan_positions_px[bi]
@@ -601,4 +673,5 @@ class PtychographyDatasetRaster(OptimizerMixin):
         if not torch.equal(torch.round(self._last_patch_positions_px.to(positions.device)),
                            torch.round(self.scan_positions_px)):
             self._set_patch_indices(obj_padding_px)
-        return self.patch_indices.to(positions.device)[bi], positions, frac, None
+        descan = self.batch_descan()
+        return self.patch_indices.to(positions.device)[bi], positions, frac, (None if descan is None else descan[bi])

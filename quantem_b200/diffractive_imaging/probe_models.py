@@ -59,14 +59,13 @@ class ProbePixelated(OptimizerMixin):
         if _token is not self._token:
             raise RuntimeError("Use a factory method to instantiate this class.")
         OptimizerMixin.__init__(self)
-        if learn_probe_tilt:
-            raise NotImplementedError("learning the probe tilt is not part of the B200 path")
         self.num_probes = int(num_probes)
         self._device = config.validate_device(device)[0]
         self._probe_params = dict(self.DEFAULT_PROBE_PARAMS)
         self.probe_params = dict(probe_params or {})
-        self.probe_tilt = torch.tensor(probe_tilt, dtype=torch.float32)
-        self.learn_probe_tilt = False
+        self._probe_tilt = torch.as_tensor(probe_tilt, dtype=torch.float32).detach().clone().reshape(2)
+        self._initial_probe_tilt = self._probe_tilt.clone()
+        self.learn_probe_tilt = bool(learn_probe_tilt)
         self._roi_shape = None if roi_shape is None else np.asarray(roi_shape, dtype=int)
         self.rng = rng
         self.initial_probe_weights = initial_probe_weights
@@ -176,7 +175,29 @@ class ProbePixelated(OptimizerMixin):
         self._constraints[key] = value
 
     @property
+    def probe_tilt(self) -> torch.Tensor:
+        """Probe tilt [mrad] (row, column) of the propagators (probe_models.py:118-131,
+        418-425); a parameter of the probe optimiser with ``learn_probe_tilt``."""
+        return self._probe_tilt
+
+    @probe_tilt.setter
+    def probe_tilt(self, tilt):
+        t = torch.as_tensor(tilt.detach().cpu() if isinstance(tilt, torch.Tensor) else tilt,
+                            dtype=torch.float32).reshape(2)
+        if self.has_optimizer() and isinstance(getattr(self, "_probe_tilt", None), torch.Tensor):
+            with torch.no_grad():
+                self._probe_tilt.data = t.to(self._probe_tilt.device)
+        else:
+            self._probe_tilt = t.to(self._device)
+
+    @property
     def params(self):
+        """The tilt (when learned) and the probe modes (probe_models.py:299-304, 699-703)."""
+        if self.learn_probe_tilt:
+            t = self._probe_tilt
+            if not (t.is_leaf and t.requires_grad and t.device == torch.device(self._device)):
+                self._probe_tilt = t.detach().to(self._device).contiguous().requires_grad_(True)
+            return [self._probe_tilt, self._probe]
         return [self._probe]
 
     @property
@@ -184,7 +205,11 @@ class ProbePixelated(OptimizerMixin):
         return self._initial_probe
 
     def get_optimization_parameters(self):
-        return [self._probe]
+        return self.params
+
+    def remove_optimizer(self):
+        super().remove_optimizer()
+        self._probe_tilt = self._probe_tilt.detach()
 
     # ------------------------------------------------------------ set-up
     def set_initial_probe(self, roi_shape, reciprocal_sampling, mean_diffraction_intensity, device=None):
@@ -239,6 +264,7 @@ class ProbePixelated(OptimizerMixin):
 
     def reset(self):
         self._probe = self._initial_probe.clone().to(self._device).requires_grad_(True)
+        self._probe_tilt = self._initial_probe_tilt.clone().to(self._device)
         if self._optimizer is not None:
             self.set_optimizer(self._optimizer_params)
 
@@ -247,9 +273,18 @@ class ProbePixelated(OptimizerMixin):
         self._device = dev
         if self._probe is not None and self._probe.device != torch.device(dev):
             self._probe = self._probe.detach().to(dev).requires_grad_(True)
+            self._probe_tilt = self._probe_tilt.detach().to(dev)
             if self._optimizer is not None:
                 self.set_optimizer(self._optimizer_params)
+        else:
+            self._probe_tilt = self._probe_tilt.to(dev)
         return self
+
+    def prop_geometry(self, sampling, slice_thicknesses):
+        """(n, sampling, energy, slice thicknesses) from which the batch kernels build the
+        separable propagators of a learned tilt (ops.batch_loss)."""
+        return (int(self._roi_shape[0]), tuple(float(x) for x in sampling), self.probe_params["energy"],
+                tuple(float(x) for x in np.atleast_1d(np.asarray(slice_thicknesses, dtype=float))))
 
     def reset_iter_constraint_losses(self):
         pass

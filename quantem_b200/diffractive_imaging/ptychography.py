@@ -416,8 +416,17 @@ class Ptychography:
         if self.num_slices == 1:
             n = int(self.roi_shape[0])
             prop = torch.zeros((0, n, n), dtype=torch.complex64, device=dev)
+        elif self.probe_model.learn_probe_tilt:  # the propagators follow the current tilt
+            prop = ops.separable_propagators_t(self._prop_geometry(), self.probe_model.probe_tilt.detach())
         return prop, self.dset.scan_positions_px.contiguous(), self.dset.targets, \
             self.dset.detector_mask.to(dev).contiguous()
+
+    def _prop_geometry(self):
+        return self.probe_model.prop_geometry(self.sampling, self.slice_thicknesses)
+
+    def _batch_descan(self):
+        d = self.dset.batch_descan()
+        return None if d is None else d.detach().contiguous()
 
     def _device_targets(self, tg):
         """Targets on the device (a one-off copy when the dataset keeps them on the host)."""
@@ -432,7 +441,7 @@ class Ptychography:
             obj_c = self.obj_model.transmission().detach().contiguous()
             probe_o = self.probe_model.probe.detach().contiguous()
         out = ops.batch_forward(obj_c, probe_o, prop, pos, bi, tg, mask, self.dset.num_gpts,
-                                self.dset.mean_diffraction_intensity, loss_type)
+                                self.dset.mean_diffraction_intensity, loss_type, descan=self._batch_descan())
         return out["intensity"], out["loss"]
 
     def forward_operator(self, obj_patches=None, shifted_input_probes=None, descan=None, batch_indices=None):
@@ -447,7 +456,8 @@ class Ptychography:
             out = ops.batch_forward(self.obj_model.transmission().detach().contiguous(),
                                     self.probe_model.probe.detach().contiguous(), prop, pos, bi, tg, mask,
                                     self.dset.num_gpts, self.dset.mean_diffraction_intensity,
-                                    want_intensity=False, want_exit=True, want_waves=True)
+                                    want_intensity=False, want_exit=True, want_waves=True,
+                                    descan=self._batch_descan())
         return out["waves"], out["exit"]
 
     # ------------------------------------------------------------ reconstruction
@@ -509,10 +519,18 @@ class Ptychography:
                 if autograd:
                     probe_o = self.probe_model.probe
                     obj_raw = self.obj_model._obj  # a leaf (pixelated) or a network output (DIP)
+                    # learned descan shifts and probe tilt enter the kernels as differentiable inputs
+                    descan = self.dset.batch_descan()
+                    tilt = self.probe_model.probe_tilt
+                    tilt = tilt if (tilt.requires_grad and self.num_slices > 1) else None
                     loss = ops.batch_loss(obj_raw, probe_o, prop, pos, idx, tg, mask,
                                           self.dset.num_gpts, self.dset.mean_diffraction_intensity, loss_type,
-                                          obj_spec=self.obj_model.transmission_spec())
-                    if obj_raw.requires_grad or self.probe_model._probe.requires_grad:
+                                          obj_spec=self.obj_model.transmission_spec(), descan=descan, tilt=tilt,
+                                          prop_geometry=self._prop_geometry() if tilt is not None else None)
+                    if descan is not None and self.dset.constraints.get("descan_tv_weight", 0) > 0:
+                        loss = loss + self.dset.apply_soft_constraints(descan)  # ptychography.py:125-140
+                    if (obj_raw.requires_grad or self.probe_model._probe.requires_grad or pos.requires_grad
+                            or (descan is not None and descan.requires_grad) or tilt is not None):
                         loss.backward()
                         if obj_raw.is_leaf and obj_raw.grad is not None:
                             # pixelated objects only (ptychography.py:330-332)
@@ -524,6 +542,8 @@ class Ptychography:
                     if self.obj_model.obj_type != "complex":
                         raise NotImplementedError("the analytic update of this path covers complex objects; "
                                                   "use autograd=True for pure-phase and potential objects")
+                    if self.dset.batch_descan() is not None:
+                        raise NotImplementedError("learned descan shifts need autograd=True")
                     with torch.no_grad():
                         probe_o = self.probe_model.probe.detach().contiguous()
                         obj_c, _ = ops.obj_constrain(self.obj_model._obj.detach().contiguous())

@@ -11,6 +11,7 @@ import ctypes
 import warnings
 from dataclasses import dataclass
 
+import numpy as np
 import torch
 
 from . import _lib
@@ -316,8 +317,13 @@ def default_grid(B: int, device=None) -> int:
 
 def _batch_args(geom, obj_c, probe_hat, prop, positions, batch_idx, targets, mask, B, loss_type, loss_scale,
                 inv_mean, grad_obj=None, out_intensity=None, out_exit=None, out_waves=None, variant="auto",
-                recompute_every=None):
+                recompute_every=None, descan=None):
     a = _lib.BatchArgs()
+    if descan is not None:
+        _req(descan, "descan", torch.float32, positions.device)
+        if tuple(descan.shape) != tuple(positions.shape):
+            raise ValueError(f"descan shifts must be {tuple(positions.shape)} like the positions")
+        a.descan = descan.data_ptr()
     a.recompute_every = int(RECOMPUTE_EVERY if recompute_every is None else recompute_every)
     a.obj = obj_c.data_ptr()
     a.probe_hat = probe_hat.data_ptr()
@@ -357,7 +363,8 @@ def plan_and_bind(a, device, adjoint: bool, grid=None):
             raise ValueError("an explicit grid is only accepted with variant='serial'")
         grid_v = parts_v = int(grid)
         nn = a.n * a.n
-        se.value, pe.value = grid_v * (a.P * a.S + a.P + 1) * nn, grid_v * a.P * nn
+        slots = a.P * a.S + a.P + 1 + (a.P * (a.S - 1) if a.grad_prop else 0)
+        se.value, pe.value = grid_v * slots * nn, grid_v * a.P * nn
     ws = workspace(device).ensure(se.value if adjoint else 0, pe.value if adjoint else 0, grid_v)
     a.grid = grid_v
     a.scratch = ws.scratch.data_ptr() if adjoint else None
@@ -400,8 +407,9 @@ def loss_scale_of(loss_type: str, B: int, num_gpts: int, mean_intensity: float) 
 
 def batch_forward(obj_c, probe_o, prop, positions, batch_idx, targets, mask, num_gpts, mean_intensity,
                   loss_type="l2_amplitude", want_intensity=True, want_exit=False, want_waves=False,
-                  probe_hat=None, grid=None, variant="auto"):
-    """Forward model + loss of one batch with no gradients.
+                  probe_hat=None, grid=None, variant="auto", descan=None):
+    """Forward model + loss of one batch with no gradients.  ``descan`` (optional
+    float32 (npos, 2)): descan shifts applied to the exit waves.
 
     Returns dict(loss=0-d tensor, intensity=(B,n,n) detector layout or None,
     exit=(P,B,n,n) or None, waves=(S,P,B,n,n) or None).
@@ -417,7 +425,7 @@ def batch_forward(obj_c, probe_o, prop, positions, batch_idx, targets, mask, num
              if want_waves else None)
     a = _batch_args(geom, obj_c, probe_hat, prop, positions, batch_idx, targets, mask, B, loss_type,
                     loss_scale_of(loss_type, max(B, 1), num_gpts, mean_intensity), 1.0 / mean_intensity,
-                    out_intensity=out_i, out_exit=out_e, out_waves=out_w, variant=variant)
+                    out_intensity=out_i, out_exit=out_e, out_waves=out_w, variant=variant, descan=descan)
     grid_v, _, ws = plan_and_bind(a, dev, adjoint=False, grid=grid)
     loss = torch.empty((), dtype=torch.float32, device=dev)
     if B == 0:
@@ -430,14 +438,19 @@ def batch_forward(obj_c, probe_o, prop, positions, batch_idx, targets, mask, num
 
 def batch_forward_adjoint(obj_c, probe_o, prop, positions, batch_idx, targets, mask, num_gpts, mean_intensity,
                           loss_type="l2_amplitude", probe_hat=None, grid=None, grad_obj=None,
-                          grad_probe=None, variant="auto", recompute_every=None, grad_positions=None):
+                          grad_probe=None, variant="auto", recompute_every=None, grad_positions=None,
+                          descan=None, grad_descan=None, grad_prop=None):
     """Fused forward + loss + adjoint of one batch.
 
     Returns (loss 0-d tensor, grad w.r.t. the constrained object (S,Ho,Wo),
     grad w.r.t. the orthogonalised probe (P,n,n)), torch gradient convention.
     ``grad_obj`` (if given) is accumulated into, not cleared.  ``grad_positions``
     (optional float32 (B, 2), zero-filled by the caller) receives dL/d(position) of
-    every batch entry (the serial kernel runs then).
+    every batch entry (the serial kernel runs then).  ``descan`` (float32 (npos, 2))
+    applies descan shifts to the exit waves; ``grad_descan`` (float32 (B, 2)) receives
+    dL/d(descan) of every batch entry; ``grad_prop`` (float32 (S-1, 2), zero-filled)
+    accumulates the propagator sensitivities sum_k fftfreq_index(k) Im(conj(dL/dZ_s) Z_s)
+    along rows and columns (the probe-tilt gradient's per-slice factors).
     """
     geom = _check_batch_inputs(obj_c, probe_o, prop, positions, batch_idx, targets, mask)
     B = int(batch_idx.numel())
@@ -453,15 +466,19 @@ def batch_forward_adjoint(obj_c, probe_o, prop, positions, batch_idx, targets, m
         loss.zero_()
         grad_probe.zero_()
         return loss, grad_obj, grad_probe
+    ext = grad_positions is not None or descan is not None or grad_descan is not None or grad_prop is not None
     a = _batch_args(geom, obj_c, probe_hat, prop, positions, batch_idx, targets, mask, B, loss_type,
                     loss_scale_of(loss_type, B, num_gpts, mean_intensity), 1.0 / mean_intensity,
-                    grad_obj=grad_obj, variant="serial" if grad_positions is not None else variant,
-                    recompute_every=recompute_every)
-    if grad_positions is not None:
-        _req(grad_positions, "grad_positions", torch.float32, dev)
-        if tuple(grad_positions.shape) != (B, 2):
-            raise ValueError(f"grad_positions must be ({B}, 2)")
-        a.grad_positions = grad_positions.data_ptr()
+                    grad_obj=grad_obj, variant="serial" if ext else variant,
+                    recompute_every=recompute_every, descan=descan)
+    for name, t, shape in (("grad_positions", grad_positions, (B, 2)), ("grad_descan", grad_descan, (B, 2)),
+                           ("grad_prop", grad_prop, (max(geom.S - 1, 0), 2))):
+        if t is None:
+            continue
+        _req(t, name, torch.float32, dev)
+        if tuple(t.shape) != shape:
+            raise ValueError(f"{name} must be {shape}")
+        setattr(a, name, t.data_ptr())
     grid_v, parts, ws = plan_and_bind(a, dev, adjoint=True, grid=grid)
     lib = _lib.lib()
     st = _stream()
@@ -527,59 +544,126 @@ def batch_analytic(obj_c, probe_o, prop, positions, batch_idx, targets, mask, nu
 
 
 class _BatchLossFn(torch.autograd.Function):
-    """loss(obj_raw, probe_o) of one batch; gradients from the fused adjoint kernel."""
+    """loss(obj_raw, probe_o, positions, descan, tilt) of one batch; gradients from the
+    fused adjoint kernel."""
 
     @staticmethod
-    def forward(ctx, obj_raw, probe_o, prop, positions, batch_idx, targets, mask, cfg):
+    def forward(ctx, obj_raw, probe_o, prop, positions, batch_idx, targets, mask, descan, tilt, cfg):
         obj_raw_c = obj_raw.detach().contiguous()
         probe_c = probe_o.detach().contiguous()
         spec = cfg.get("obj_spec") or COMPLEX_OBJECT
         ctx.spec = spec
         obj_c, work = obj_transmission(obj_raw_c, spec)
-        need = ctx.needs_input_grad[0] or ctx.needs_input_grad[1] or ctx.needs_input_grad[3]
+        ng = ctx.needs_input_grad
+        need = ng[0] or ng[1] or ng[3] or ng[7] or ng[8]
         ctx.npos = int(positions.shape[0])
+        dsc = None if descan is None else descan.detach().contiguous()
+        dev = positions.device
+        if tilt is not None:
+            prop = separable_propagators_t(cfg["prop_geometry"], tilt.detach())
+        B = int(batch_idx.numel())
+        empty = torch.empty(0, device=dev)
         if need:
-            g_pos = (torch.zeros((int(batch_idx.numel()), 2), dtype=torch.float32, device=positions.device)
-                     if ctx.needs_input_grad[3] else None)
+            g_pos = torch.zeros((B, 2), dtype=torch.float32, device=dev) if ng[3] else None
+            g_dsc = torch.zeros((B, 2), dtype=torch.float32, device=dev) if ng[7] else None
+            S = int(obj_raw.shape[0])
+            g_prop = torch.zeros((max(S - 1, 0), 2), dtype=torch.float32, device=dev) if ng[8] else None
             loss, g_obj_c, g_probe = batch_forward_adjoint(
                 obj_c, probe_c, prop, positions.detach(), batch_idx, targets, mask, cfg["num_gpts"],
                 cfg["mean_intensity"], cfg["loss_type"], grid=cfg.get("grid"), variant=cfg.get("variant", "auto"),
-                recompute_every=cfg.get("recompute_every"), grad_positions=g_pos)
+                recompute_every=cfg.get("recompute_every"), grad_positions=g_pos, descan=dsc, grad_descan=g_dsc,
+                grad_prop=g_prop)
             ctx.save_for_backward(obj_raw_c, work, g_obj_c, g_probe, batch_idx,
-                                  g_pos if g_pos is not None else torch.empty(0, device=positions.device))
+                                  g_pos if g_pos is not None else empty, g_dsc if g_dsc is not None else empty,
+                                  g_prop if g_prop is not None else empty,
+                                  tilt.detach() if tilt is not None else empty)
+            ctx.prop_geometry = cfg.get("prop_geometry")
         else:
             loss = batch_forward(obj_c, probe_c, prop, positions.detach(), batch_idx, targets, mask, cfg["num_gpts"],
                                  cfg["mean_intensity"], cfg["loss_type"], want_intensity=False,
-                                 grid=cfg.get("grid"), variant=cfg.get("variant", "auto"))["loss"]
+                                 grid=cfg.get("grid"), variant=cfg.get("variant", "auto"), descan=dsc)["loss"]
         return loss
 
     @staticmethod
+    def _per_position(ctx, g_batch, batch_idx, gout):
+        """Per batch entry -> per scan position (repeated indices add up); the kernel skips
+        out-of-range indices (and reports them): route them to row 0 with a zero gradient."""
+        out = torch.zeros((ctx.npos, 2), dtype=torch.float32, device=g_batch.device)
+        valid = (batch_idx >= 0) & (batch_idx < ctx.npos)
+        out.index_add_(0, torch.where(valid, batch_idx, torch.zeros_like(batch_idx)), g_batch * gout * valid[:, None])
+        return out
+
+    @staticmethod
     def backward(ctx, gout):
-        obj_raw, work, g_obj_c, g_probe, batch_idx, g_pos = ctx.saved_tensors
+        obj_raw, work, g_obj_c, g_probe, batch_idx, g_pos, g_dsc, g_prop, tilt = ctx.saved_tensors
         gout = gout.detach().to(torch.float32).reshape(1).contiguous()
-        g_obj = None
-        if ctx.needs_input_grad[0]:
-            g_obj = obj_transmission_vjp(obj_raw, g_obj_c, work, ctx.spec, scale=gout)
-        g_pr = g_probe * gout if ctx.needs_input_grad[1] else None
-        g_positions = None
-        if ctx.needs_input_grad[3]:  # per batch entry -> per scan position (repeated indices add up)
-            g_positions = torch.zeros((ctx.npos, 2), dtype=torch.float32, device=g_pos.device)
-            # the kernel skips out-of-range indices (and reports them): route them to row 0 with a zero gradient
-            valid = (batch_idx >= 0) & (batch_idx < ctx.npos)
-            g_positions.index_add_(0, torch.where(valid, batch_idx, torch.zeros_like(batch_idx)),
-                                   g_pos * gout * valid[:, None])
-        return g_obj, g_pr, None, g_positions, None, None, None, None
+        ng = ctx.needs_input_grad
+        g_obj = obj_transmission_vjp(obj_raw, g_obj_c, work, ctx.spec, scale=gout) if ng[0] else None
+        g_pr = g_probe * gout if ng[1] else None
+        g_positions = _BatchLossFn._per_position(ctx, g_pos, batch_idx, gout) if ng[3] else None
+        g_descan = _BatchLossFn._per_position(ctx, g_dsc, batch_idx, gout) if ng[7] else None
+        g_tilt = None
+        if ng[8]:
+            g_tilt = tilt_gradient(g_prop, tilt, ctx.prop_geometry) * gout
+        return g_obj, g_pr, None, g_positions, None, None, None, g_descan, g_tilt, None
 
 
 def batch_loss(obj_raw, probe_o, prop, positions, batch_idx, targets, mask, num_gpts, mean_intensity,
-               loss_type="l2_amplitude", grid=None, variant="auto", recompute_every=None, obj_spec=None):
+               loss_type="l2_amplitude", grid=None, variant="auto", recompute_every=None, obj_spec=None,
+               descan=None, tilt=None, prop_geometry=None):
     """Differentiable consistency loss of one batch w.r.t. the raw object
-    parameter (hard constraint and, for potentials, exp(i V) included) and the
-    orthogonalised probe.  ``obj_spec`` (default: complex object) names the object
-    type; ``recompute_every`` (256 x 256 windows): adjoint checkpoint interval."""
+    parameter (hard constraint and, for potentials, exp(i V) included), the
+    orthogonalised probe, the scan positions (when they require grad), the descan
+    shifts ``descan`` (float32 (npos, 2), optional) and the probe tilt ``tilt`` (float32
+    (2,) mrad, optional: the propagators are then built from it, ``prop_geometry`` =
+    (n, sampling, energy, slice thicknesses), and ``prop`` is ignored).  ``obj_spec``
+    (default: complex object) names the object type; ``recompute_every`` (256 x 256
+    windows): adjoint checkpoint interval."""
+    if tilt is not None and prop_geometry is None:
+        raise ValueError("a probe tilt needs prop_geometry = (n, sampling, energy, slice thicknesses)")
     cfg = dict(num_gpts=int(num_gpts), mean_intensity=float(mean_intensity), loss_type=loss_type, grid=grid,
-               variant=variant, recompute_every=recompute_every, obj_spec=obj_spec)
-    return _BatchLossFn.apply(obj_raw, probe_o, prop, positions, batch_idx, targets, mask, cfg)
+               variant=variant, recompute_every=recompute_every, obj_spec=obj_spec, prop_geometry=prop_geometry)
+    return _BatchLossFn.apply(obj_raw, probe_o, prop, positions, batch_idx, targets, mask, descan, tilt, cfg)
+
+
+def separable_propagators_t(prop_geometry, tilt: torch.Tensor):
+    """``separable_propagators`` with the tilt given as a device tensor (2,) [mrad], so a
+    learned tilt needs no device-to-host read: Kr_s = exp(-i pi lambda dz_s kr^2 -
+    2 pi i dz_s tan(theta_r / 1e3) kr), Kc likewise (probe_models.py:406-425).  The
+    factors are evaluated in float32 on the tilt's device."""
+    import math
+
+    from .diffractive_imaging.complex_probe import electron_wavelength_angstrom
+
+    n, sampling, energy, dz = prop_geometry
+    dev = tilt.device
+    dz = torch.as_tensor(np.asarray(dz, dtype=np.float64), device=dev).reshape(-1)
+    lam = electron_wavelength_angstrom(energy)
+    t = torch.tan(tilt.to(torch.float64) / 1e3)
+    out = []
+    for ax in range(2):
+        k = torch.fft.fftfreq(int(n), float(sampling[ax]), dtype=torch.float64, device=dev)
+        ph = -math.pi * lam * dz[:, None] * k[None] ** 2 - 2 * math.pi * dz[:, None] * t[ax] * k[None]
+        out.append(torch.polar(torch.ones_like(ph), ph).to(torch.complex64).contiguous())
+    return tuple(out)
+
+
+def tilt_gradient(prop_sums: torch.Tensor, tilt: torch.Tensor, prop_geometry) -> torch.Tensor:
+    """dL/d(probe tilt) (2,) from the kernel's propagator sensitivities (S-1, 2):
+    K_s carries exp(-2 pi i dz_s tan(theta / 1e3) k) per axis, k = index / (n d), so
+    dL/dtheta = sum_s 2 pi dz_s sec^2(theta / 1e3) / 1e3 / (n d) * prop_sums[s].  The
+    reference adds the tilt ramp only for a nonzero tilt (probe_models.py:418, 421), so
+    a zero tilt gets a zero gradient."""
+    import math
+
+    n, sampling, _, dz = prop_geometry
+    dev = prop_sums.device
+    dz = torch.as_tensor(np.asarray(dz, dtype=np.float64), device=dev).reshape(-1, 1)
+    d = torch.as_tensor([float(sampling[0]), float(sampling[1])], dtype=torch.float64, device=dev)
+    th = tilt.to(torch.float64)
+    coef = 2 * math.pi * dz / (1e3 * int(n) * d[None]) / torch.cos(th / 1e3)[None] ** 2
+    g = (coef * prop_sums.to(torch.float64)).sum(0) * (th != 0)
+    return g.to(torch.float32)
 
 
 def separable_propagators(n, sampling, energy, slice_thicknesses, tilt_mrad=(0.0, 0.0), device="cuda"):

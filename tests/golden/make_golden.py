@@ -419,6 +419,122 @@ def positions_case(name="positions64", seed=71):
           f"moved={np.abs(out['recon_positions'] - out['positions']).max():.3g}")
 
 
+def descan_tilt_case(name="descantilt64", seed=83):
+    """Learned descan shifts (dataset_models.py:30-120, 225-242, 1482-1499;
+    ptychography_base.py:892-906) and a learned probe tilt (probe_models.py:56-131,
+    295-304, 376-427).  Data simulated with per-position descan shifts of up to 0.6 px
+    and a (1.0, -1.5) mrad tilt; the reference starts from zero descan and a
+    (0.5, -0.5) mrad tilt (a zero tilt would get no gradient: the reference adds the
+    ramp only for a nonzero tilt).  Records one batch's autograd gradients, the descan
+    and tilt ones included, with the dataset optimiser set (so the targets are the
+    uncentred amplitudes), and 3 Adam iterations of object, probe (+ tilt) and dataset
+    (descan; scan positions not learned)."""
+    import torch
+    from quantem.core.datastructures.dataset4dstem import Dataset4dstem
+    from quantem.diffractive_imaging.complex_probe import real_space_probe
+    from quantem.diffractive_imaging.dataset_models import PtychographyDatasetRaster
+    from quantem.diffractive_imaging.detector_models import DetectorPixelated
+    from quantem.diffractive_imaging.object_models import ObjectPixelated
+    from quantem.diffractive_imaging.probe_models import ProbePixelated
+    from quantem.diffractive_imaging.ptychography import Ptychography
+
+    H, S, P, nscan, step_px, pad, dz, counts, batch, iters = 64, 3, 2, 5, 6, 32, 20.0, 1e5, 10, 3
+    weights = [0.8, 0.2]
+    tilt_true, tilt_start = (1.0, -1.5), (0.5, -0.5)
+    rng = np.random.default_rng(seed)
+    px, energy = 0.2, 300e3
+    rs = 1.0 / (H * px)
+    probe1 = real_space_probe(gpts=(H, H), sampling=(px, px), energy=energy, semiangle_cutoff=20.0,
+                              aberration_coefs={"C10": -200.0}).numpy().astype(np.complex128)
+    probes = np.stack([probe1 * np.sqrt(w) * np.exp(2j * np.pi * k * np.arange(H)[None, :] / H)
+                       for k, w in enumerate(weights)])
+    ext = (nscan - 1) * step_px
+    obj_hw = int(ext + 2 * pad)
+    obj_hw += (-obj_hw) % 8
+    phase = np.stack([O.gaussian_atom_phase((obj_hw, obj_hw), obj_hw * obj_hw // 400, 1.5, 0.1, rng)
+                      for _ in range(S)])
+    grid = np.stack(np.meshgrid(np.arange(nscan), np.arange(nscan), indexing="ij"), -1).reshape(-1, 2)
+    pos = (grid * step_px + pad).astype(np.float64)
+    descan_true = rng.uniform(-0.6, 0.6, size=(nscan * nscan, 2))
+    props_true = O.propagators((H, H), (px, px), energy, [dz] * (S - 1), tilt_mrad=tilt_true)
+    st = O.forward(np.exp(1j * phase), probes, pos, props_true, descan=descan_true)
+    inten = O.detector_intensities(st)
+    inten = inten / inten.sum(axis=(-2, -1), keepdims=True).mean() * counts
+    data = rng.poisson(inten).astype(np.float32)
+    d4 = Dataset4dstem.from_array(data.reshape(nscan, nscan, H, H), sampling=(step_px * px, step_px * px, rs, rs),
+                                  units=("A", "A", "A^-1", "A^-1"))
+    pd = PtychographyDatasetRaster.from_dataset4dstem(d4, verbose=0, learn_descan=True, learn_scan_positions=False)
+    pd.preprocess(com_fit_function="constant", force_com_rotation=0, force_com_transpose=False,
+                  plot_rotation=False, plot_com=False, probe_energy=energy)
+    obj_model = ObjectPixelated.from_uniform(num_slices=S, slice_thicknesses=dz, obj_type="complex")
+    probe_model = ProbePixelated.from_params(
+        probe_params={"energy": energy, "defocus": 200.0, "semiangle_cutoff": 20.0},
+        num_probes=P, rng=seed + 1, initial_probe_weights=weights, probe_tilt=tilt_start, learn_probe_tilt=True)
+    pt = Ptychography.from_models(dset=pd, obj_model=obj_model, probe_model=probe_model,
+                                  detector_model=DetectorPixelated(), device="cpu", verbose=0, rng=seed + 2)
+    pt.preprocess(obj_padding_px=(pad, pad))
+    # start the descan shifts off zero so the batch gradient is not the trivial one
+    with torch.no_grad():
+        pd.descan_shifts = torch.tensor(rng.uniform(-0.3, 0.3, size=(pd.num_gpts, 2)), dtype=torch.float32)
+    opt = {"object": {"type": "adam"}, "probe": {"type": "adam"}, "dataset": {"type": "adam", "lr": 1e-2}}
+    constraints = {"probe": {"orthogonalize_probe": True}}
+    pt.constraints = constraints
+    pt.optimizer_params = {k: dict(v) for k, v in opt.items()}
+    pt.set_optimizers()
+    pt.dset._set_targets("l2_amplitude")  # the uncentred amplitudes: descan is learned
+    out = dict(H=H, S=S, P=P, nscan=nscan, step_px=step_px, pad=pad, dz=dz, px=px, energy=energy, jitter=0,
+               batch=batch, iters=iters, seed=seed, counts=counts, weights=np.asarray(weights, dtype=np.float64),
+               orthogonalize=1, data=data, targets=_f32(pd.targets.numpy()),
+               centered_targets=_f32(pd.centered_amplitudes.numpy()),
+               mean_intensity=np.float64(pd.mean_diffraction_intensity),
+               positions=_f32(pd.scan_positions_px.detach().numpy()),
+               descan=_f32(pd.descan_shifts.detach().numpy()), descan_true=descan_true.astype(np.float32),
+               tilt=np.asarray(tilt_start, dtype=np.float64), tilt_true=np.asarray(tilt_true, dtype=np.float64),
+               obj_shape=np.asarray(pt.obj_shape_full), obj_padding_px=np.asarray(pt.obj_padding_px),
+               upsample_factor=np.float64(pd.upsample_factor),
+               probe_init=_c64(probe_model._probe.detach().numpy()),
+               sampling=np.asarray(pt.sampling, dtype=np.float64))
+    pt.compute_propagator_arrays()
+    out["propagators"] = _c64(pt._propagators.detach().numpy())
+    with torch.no_grad():
+        shp = tuple(obj_model._obj.shape)
+        amp = 1.0 - 0.3 * rng.random(shp)
+        ph = 0.4 * rng.standard_normal(shp)
+        obj_model._obj.data = torch.tensor(amp * np.exp(1j * ph), dtype=torch.complex64)
+    out["obj_perturbed"] = obj_model._obj.detach().numpy().copy()
+    bi = np.arange(batch)
+    for prm in (obj_model._obj, probe_model._probe, probe_model._probe_tilt, pd._descan_shifts):
+        prm.grad = None
+    patch_indices, _pos, frac, descan = pt.dset.forward(bi, pt.obj_padding_px)
+    assert descan is not None
+    sp = probe_model.forward(frac)
+    op = obj_model.forward(patch_indices)
+    prop, ov = pt.forward_operator(op, sp, descan)
+    inten = pt.detector_model.forward(ov)
+    loss, tg = pt.error_estimate(inten, bi)
+    pt.backward(loss, True, op, prop, ov, patch_indices, tg)
+    out.update(batch_indices=bi, batch_loss=np.float64(loss.item()),
+               batch_intensities=_f32(inten.detach().numpy()),
+               grad_descan=pd._descan_shifts.grad.numpy().astype(np.float64).copy(),
+               grad_tilt=probe_model._probe_tilt.grad.numpy().astype(np.float64).copy(),
+               grad_obj=obj_model._obj.grad.numpy().copy(), grad_probe=_c64(probe_model._probe.grad.numpy()))
+    for prm in (obj_model._obj, probe_model._probe, probe_model._probe_tilt, pd._descan_shifts):
+        prm.grad = None
+    pt.rng = seed + 3
+    pt.reconstruct(num_iters=iters, batch_size=batch, optimizer_params={k: dict(v) for k, v in opt.items()},
+                   constraints=constraints, device="cpu")
+    out.update(recon_obj=obj_model._obj.detach().numpy().copy(), recon_probe=_c64(probe_model._probe.detach().numpy()),
+               recon_descan=pd.descan_shifts.detach().numpy().astype(np.float32).copy(),
+               recon_tilt=probe_model.probe_tilt.detach().numpy().astype(np.float64).copy(),
+               recon_positions=pd.scan_positions_px.detach().numpy().astype(np.float32).copy(),
+               recon_losses=np.asarray(pt._iter_losses, dtype=np.float64), recon_rng_seed=np.int64(seed + 3))
+    path = os.path.join(HERE, f"{name}.npz")
+    np.savez_compressed(path, **out)
+    print(f"wrote {path}: losses={out['recon_losses']} grad_tilt={out['grad_tilt']} "
+          f"|grad_descan|={np.abs(out['grad_descan']).max():.3g} tilt {out['tilt']} -> {out['recon_tilt']} "
+          f"descan moved={np.abs(out['recon_descan'] - out['descan']).max():.3g}")
+
+
 def whitenoise_case():
     """The reference gradient test's fixture (test_ptychography.py:19-212), restated."""
     import torch
@@ -486,6 +602,9 @@ def main(src):
     if os.environ.get("GOLDEN_ONLY") == "positions":
         positions_case()
         return
+    if os.environ.get("GOLDEN_ONLY") == "descantilt":
+        descan_tilt_case()
+        return
     run_case("single64", H=64, S=1, P=1, nscan=6, step_px=4, pad=32, dz=20.0, counts=1e5,
              jitter=False, batch=12, iters=3, seed=11)
     run_case("mixed64", H=64, S=3, P=3, nscan=5, step_px=6, pad=32, dz=20.0, counts=1e5,
@@ -497,6 +616,7 @@ def main(src):
     c2small_case()
     objtype_cases()
     positions_case()
+    descan_tilt_case()
 
 
 def objtype_cases():

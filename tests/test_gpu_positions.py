@@ -105,6 +105,8 @@ def test_reconstruct_learns_positions_like_reference(cuda_device):
     moved64 = pos64 - z["positions"]
     assert rel(moved, moved64) < max(3 * rel(z["recon_positions"] - z["positions"], moved64), 1e-3)
     assert rel(pt.obj_model._obj.detach().cpu().numpy(), obj64) < max(3 * rel(z["recon_obj"], obj64), 1e-5)
-    with pytest.raises(NotImplementedError, match="descan"):
-        pd2 = PtychographyDatasetRaster.from_dataset4dstem(d4, verbose=0)  # learn_descan defaults to True
-        pd2.set_optimizer({"type": "adam", "lr": 1e-3})
+    # the reference's defaults learn the descan shifts and the positions together
+    pd2 = PtychographyDatasetRaster.from_dataset4dstem(d4, verbose=0)
+    pd2.set_optimizer({"type": "adam", "lr": 1e-3})
+    assert [tuple(p.shape) for p in pd2.optimizer.param_groups[0]["params"]] == [(nscan * nscan, 2)] * 2
+    assert pd2.optimizer.param_groups[0]["params"][0] is pd2.descan_shifts

@@ -173,3 +173,43 @@ def test_oracle_position_gradients_and_learned_positions_match_reference():
     assert np.abs(moved_ref).max() > 0.02
     assert rel(pos - z["positions"], moved_ref) < 1e-3  # Adam's sign-like steps on float32 gradients
     assert rel(obj, z["recon_obj"]) < 1e-4
+
+
+def test_oracle_descan_and_tilt_gradients_and_learning_match_reference():
+    """Learned descan shifts and probe tilt (fixture descantilt64, made by the reference with
+    a dataset optimiser over the descan shifts and learn_probe_tilt=True): the batch's
+    autograd descan and tilt gradients against the uncentred targets, and 3 Adam
+    iterations moving object, probe, tilt and descan."""
+    z = load_golden("descantilt64")
+    H, S = int(z["H"]), int(z["S"])
+    bi = z["batch_indices"]
+    geom = ((H, H), tuple(z["sampling"]), float(z["energy"]), [float(z["dz"])] * (S - 1))
+    props = O.propagators(*geom, tilt_mrad=tuple(z["tilt"]))
+    assert rel(props, z["propagators"]) < 1e-6  # the reference's complex64 propagators at the start tilt
+    loss, g_obj, g_probe, st = O.full_gradients(
+        z["obj_perturbed"].astype(np.complex128), z["probe_init"].astype(np.complex128),
+        z["positions"].astype(np.float64)[bi], props, z["targets"].astype(np.float64)[bi], np.ones((H, H)),
+        z["positions"].shape[0], float(z["mean_intensity"]), float(z["upsample_factor"]), orthogonalize=True,
+        descan=z["descan"].astype(np.float64)[bi])
+    assert abs(loss - float(z["batch_loss"])) / float(z["batch_loss"]) < 2e-6
+    assert rel(np.fft.fftshift(st.intensity, axes=(-2, -1)), z["batch_intensities"]) < 2e-6
+    assert rel(g_obj, z["grad_obj"]) < 5e-6
+    assert rel(g_probe, z["grad_probe"]) < 5e-6
+    gd = O.descan_gradients(st)
+    assert np.abs(z["grad_descan"][len(bi):]).max() == 0.0
+    assert rel(gd, z["grad_descan"][bi]) < 1e-5
+    gt = O.tilt_gradients(st, tuple(z["tilt"]), geom[3], geom[1], geom[0])
+    assert rel(gt, z["grad_tilt"]) < 1e-5
+    obj, probe, losses, learned = O.reconstruct(
+        z["obj_perturbed"].astype(np.complex128), z["probe_init"].astype(np.complex128),
+        z["positions"].astype(np.float64), props, z["targets"].astype(np.float64), np.ones((H, H)),
+        float(z["mean_intensity"]), float(z["upsample_factor"]), int(z["iters"]), int(z["batch"]),
+        np.random.default_rng(int(z["recon_rng_seed"])), descan=z["descan"], lr_descan=1e-2,
+        tilt=z["tilt"], prop_geometry=geom)
+    np.testing.assert_allclose(losses, z["recon_losses"], rtol=1e-5)
+    moved = z["recon_descan"] - z["descan"]
+    assert np.abs(moved).max() > 0.02
+    assert rel(learned["descan"] - z["descan"], moved) < 1e-3
+    assert rel(learned["tilt"] - z["tilt"], z["recon_tilt"] - z["tilt"]) < 1e-3
+    assert rel(obj, z["recon_obj"]) < 1e-4
+    assert np.array_equal(z["recon_positions"], z["positions"])  # scan positions not learned
