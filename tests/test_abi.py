@@ -74,3 +74,38 @@ def test_product_has_no_cpu_fallback():
         ops.fft2(x)
     with pytest.raises(RuntimeError, match="CUDA"):
         ops.obj_constrain(x)
+
+
+def test_extension_arguments_are_validated_without_gpu():
+    """Descan shifts and the descan / propagator gradients (ABI 3): rejected, before any
+    CUDA call, where they are not built or are inconsistent."""
+    from quantem_b200 import _lib
+
+    lib = _lib.lib()
+    assert lib.ptycho_abi_version() >= 3
+    a = _lib.BatchArgs()
+    d = ctypes.c_void_p(256)  # never dereferenced: every call below fails validation
+    for f in ("obj", "probe_hat", "prop", "positions", "batch_idx", "targets", "mask", "loss_part", "grad_obj",
+              "probe_grad_part", "scratch"):
+        setattr(a, f, d)
+    a.n, a.S, a.P, a.B, a.Ho, a.Wo, a.npos, a.grid = 128, 3, 2, 4, 256, 256, 4, 4
+    a.grad_descan = d
+    assert lib.ptycho_forward_adjoint(ctypes.byref(a), None) == 1  # grad_descan without descan
+    assert "descan" in _lib.last_error()
+    a.descan = d
+    assert lib.ptycho_forward_loss(ctypes.byref(a), None) == 2     # gradients need the adjoint launch
+    a.grad_descan = None
+    a.grad_prop, a.S = d, 18
+    assert lib.ptycho_forward_adjoint(ctypes.byref(a), None) == 2  # propagator gradients up to 17 slices
+    assert "17" in _lib.last_error()
+    a.grad_prop, a.S = None, 3
+    a.analytic, a.an_norm = 1, d
+    assert lib.ptycho_forward_adjoint(ctypes.byref(a), None) == 2  # descan with the analytic update
+    a.analytic, a.an_norm = 0, None
+    a.n = 256
+    assert lib.ptycho_forward_loss(ctypes.byref(a), None) == 2     # not built for 256 x 256 windows
+    assert "256" in _lib.last_error()
+    sets = (_lib.BatchArgs * 1)(a)
+    sets[0].n = 128
+    assert lib.ptycho_forward_adjoint_multi(sets, 1, None) == 2    # not in the multi-dataset launch
+    assert "multi" in _lib.last_error()
