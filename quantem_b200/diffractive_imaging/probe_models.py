@@ -312,7 +312,7 @@ class ProbePixelated(OptimizerMixin):
         lam = electron_wavelength_angstrom(energy)
         dz = torch.as_tensor(np.asarray(slice_thicknesses), dtype=k2.dtype)
         props = torch.exp((-1.0j * torch.pi * lam * dz[:, None, None]) * k2)
-        tr, tc = (float(x) for x in self.probe_tilt)
+        tr, tc = (float(x) for x in self.probe_tilt.detach())
         if tr != 0:
             props = props * torch.exp(1.0j * (-2 * math.pi * dz[:, None, None] * math.tan(tr / 1e3)) * kr[None, :, None])
         if tc != 0:
@@ -325,7 +325,7 @@ class ProbePixelated(OptimizerMixin):
 
         return ops.separable_propagators(int(self._roi_shape[0]), sampling, self.probe_params["energy"],
                                          np.asarray(slice_thicknesses, dtype=float),
-                                         tuple(float(x) for x in self.probe_tilt), device=device)
+                                         tuple(float(x) for x in self.probe_tilt.detach()), device=device)
 
     def forward(self, fract_positions: torch.Tensor) -> torch.Tensor:
         """(P, B, H, W) sub-pixel shifted probes (ptycho_utils.py:128-176)."""
