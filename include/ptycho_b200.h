@@ -145,6 +145,64 @@ int ptycho_workspace_elems(int n, int S, int P, int grid, int64_t* scratch_elems
 int ptycho_batch_plan(const ptycho_batch_args* a, int adjoint, int* variant, int* grid, int64_t* scratch_elems,
                       int64_t* partial_elems, int* partial_parts);
 
+/* ---- optional object constraints (object_models.py:273-480) and the FOV mask
+ * (ptychography_base.py:191-216).  Objects are (S, Ho, Wo) complex64 or float32,
+ * hw = Ho * Wo, count = S * hw; masks are float32 (Ho, Wo).  work: float64 scratch of
+ * ptycho_obj_constraint_work_elems() elements.  Every reduction is fixed-order. ---- */
+
+/* float64 elements of the work buffer the functions below need. */
+int ptycho_obj_constraint_work_elems(void);
+
+/* out (Ho, Wo) = sum over positions of intensity (n, n) placed at each position's
+ * wrapped patch window (rounded half to even), as the reference's probe overlap with
+ * |probe mode 0|^2 (ptychography_base.py:201-216). */
+int ptycho_probe_overlap(const float* intensity, int n, const float* positions, int npos, int Ho, int Wo, float* out,
+                         void* stream);
+
+/* Hard constraint of complex (pure = 0) or pure-phase (pure = 1) objects with the FOV
+ * mask m: amp m exp(i (angle - mean angle) m) m (object_models.py:292-300, 322-323; the
+ * amplitude carries the mask twice, as in the reference), and its VJP w.r.t. the raw
+ * object (grad_raw must not alias obj or grad_c). */
+int ptycho_obj_constrain_fov(const void* obj, const float* mask, int64_t hw, void* out, int64_t count, int pure,
+                             double* work, int nwork, void* stream);
+int ptycho_obj_constrain_fov_vjp(const void* obj, const float* mask, int64_t hw, const void* grad_c, void* grad_raw,
+                                 int64_t count, int pure, double* work, int nwork, void* stream);
+
+/* Potential hard constraint (object_models.py:301-323): out = (V - offset), clamped at 0
+ * with positivity, times apply_mask (may be NULL).  With fix_baseline the offset is
+ * factor * the mean of V over the background pixels of baseline_mask (mask < 0.5 max), or
+ * factor * min V when baseline_mask is NULL or has no background.  The VJP treats the
+ * offset as a constant (detached, as in the reference). */
+int ptycho_obj_potential_base(const float* v, const float* baseline_mask, const float* apply_mask, int64_t hw,
+                              float* out, int64_t count, int positivity, int fix_baseline, float factor,
+                              double* work, int nwork, void* stream);
+int ptycho_obj_potential_base_vjp(const float* v, const float* baseline_mask, const float* apply_mask, int64_t hw,
+                                  const float* grad_out, float* grad_v, int64_t count, int positivity,
+                                  int fix_baseline, float factor, double* work, int nwork, void* stream);
+
+/* Transmission exp(i V) of a real potential (object_models.py:252-256) and its VJP
+ * dL/dV = Re(conj(G) i t). */
+int ptycho_phase_exp(const float* v, void* out, int64_t count, void* stream);
+int ptycho_phase_exp_vjp(const float* v, const void* grad_t, float* grad_v, int64_t count, void* stream);
+
+/* Gaussian blur of every slice (object_models.py:437-479): zero-padded 'same'
+ * correlation with the odd tap vector (<= 255 taps) along the rows, then the columns;
+ * complex objects blur their real and imaginary parts.  Self-adjoint, so it is its own
+ * VJP.  tmp: a buffer of the object's size, aliasing neither in nor out. */
+int ptycho_obj_blur(const void* in, void* out, void* tmp, int S, int Ho, int Wo, int is_complex, const float* taps,
+                    int ntaps, void* stream);
+
+/* identical_slices (object_models.py:330-333): every slice replaced by the mean over the
+ * slices (the reference averages in place under no_grad: its VJP is the identity). */
+int ptycho_obj_slice_mean(const void* in, void* out, int S, int64_t hw, int is_complex, void* stream);
+
+/* Soft constraints of the hard-constrained object (object_models.py:341-435): kind 0
+ * complex (TV and surface terms of phase and amplitude), 1 pure phase (phase terms), 2
+ * real potential.  Writes the loss (device float) and its gradient w.r.t. obj (torch
+ * convention; zero at zero-magnitude pixels). */
+int ptycho_obj_soft_loss(const void* obj, int S, int Ho, int Wo, int kind, float tv_weight_z, float tv_weight_xy,
+                         float surface_zero_weight, double* work, int nwork, float* loss, void* grad, void* stream);
+
 /* Forward model + loss of one batch (no gradients). */
 int ptycho_forward_loss(const ptycho_batch_args* a, void* stream);
 

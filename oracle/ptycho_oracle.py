@@ -231,6 +231,211 @@ def object_transmission_vjp(obj: np.ndarray, grad_t: np.ndarray, obj_type: str =
     raise ValueError(obj_type)
 
 
+# ----------------------------------------------------------------------------
+# optional object constraints (object_models.py:273-480) and the FOV mask
+# (ptychography_base.py:191-216)
+# ----------------------------------------------------------------------------
+
+def probe_overlap(probe0_intensity: np.ndarray, positions_px: np.ndarray, obj_shape_2d) -> np.ndarray:
+    """sum over positions of |probe mode 0|^2 placed at each position's patch window
+    (ptychography_base.py:201-216, ptycho_utils.py:215-236; unshifted probe, rounded
+    positions, wrapped windows)."""
+    H, W = probe0_intensity.shape
+    origins, _ = split_positions(np.asarray(positions_px, dtype=np.float64))
+    rows, cols = patch_rows_cols(origins, (H, W), obj_shape_2d)
+    out = np.zeros(tuple(int(x) for x in obj_shape_2d), dtype=np.float64)
+    for b in range(origins.shape[0]):
+        np.add.at(out, (rows[b][:, None], cols[b][None, :]), probe0_intensity)
+    return out
+
+
+def fov_mask(overlap: np.ndarray, obj_padding_px, gaussian_sigma: float = 2.0) -> np.ndarray:
+    """ptychography_base.py:191-199: overlap > 0.3 max, binary closing (5 iterations),
+    binary dilation (min(32, min(padding) // 4) iterations), Gaussian filter."""
+    import scipy.ndimage as ndi
+
+    ov = overlap > overlap.max() * 0.3
+    ov = ndi.binary_closing(ov, iterations=5)
+    ov = ndi.binary_dilation(ov, iterations=min(32, int(np.min(obj_padding_px)) // 4))
+    return ndi.gaussian_filter(ov.astype(np.float32), sigma=gaussian_sigma)
+
+
+def gaussian_taps(sigma: float) -> np.ndarray:
+    """The normalised float32 Gaussian of object_models.py:445-451."""
+    k = int(2 * math.ceil(3 * sigma) + 1)
+    if k % 2 == 0:
+        k += 1
+    ax = np.arange(-k // 2 + 1.0, k // 2 + 1.0, dtype=np.float32)
+    g = np.exp(-0.5 * (ax / np.float32(sigma)) ** 2).astype(np.float32)
+    return (g / g.sum()).astype(np.float32)
+
+
+def blur(x: np.ndarray, taps: np.ndarray) -> np.ndarray:
+    """object_models.py:437-479: zero-padded 'same' correlation with the taps along the
+    rows, then along the columns, of every slice (real and imaginary parts separately).
+    Self-adjoint (symmetric taps, symmetric zero padding): the VJP is the same blur."""
+    import scipy.ndimage as ndi
+
+    t = np.asarray(taps, dtype=np.float64)
+
+    def one(a):
+        a = ndi.correlate1d(a, t, axis=-2, mode="constant", cval=0.0)
+        return ndi.correlate1d(a, t, axis=-1, mode="constant", cval=0.0)
+
+    if np.iscomplexobj(x):
+        return one(x.real) + 1j * one(x.imag)
+    return one(x)
+
+
+def constrain_object_ext(obj: np.ndarray, obj_type: str, mask=None, positivity: bool = True,
+                         fix_baseline: bool = False, baseline_factor: float = 1.0, taps=None,
+                         identical: bool = False) -> np.ndarray:
+    """ObjectConstraints.apply_hard_constraints (object_models.py:289-339) with the FOV mask
+    (apply_fov_mask, the mask (H, W) applied to every slice), the Gaussian blur and identical
+    slices: complex / pure phase -> amp mask exp(i (angle - mean angle) mask) times the mask
+    again (the reference multiplies the amplitude by the mask twice); potential -> V - offset
+    (offset = factor * mean of V over the background pixels, mask < 0.5 max mask, or factor *
+    min V without a background), clamped at 0, times the mask.  Returns the complex object or
+    the real potential before exp(i V)."""
+    m = None if mask is None else np.asarray(mask, dtype=np.float64)[None]
+    if obj_type in ("complex", "pure_phase"):
+        amp = np.clip(np.abs(obj), 0.0, 1.0) if obj_type == "complex" else np.ones(obj.shape)
+        ph = np.angle(obj) - np.angle(obj).mean()
+        out = amp * np.exp(1j * ph) if m is None else amp * m * np.exp(1j * ph * m) * m
+    elif obj_type == "potential":
+        off = 0.0
+        if fix_baseline:
+            if m is not None:
+                bg = np.broadcast_to(m < 0.5 * m.max(), obj.shape)
+                off = obj[bg].mean() if bg.any() else obj.min()
+            else:
+                off = obj.min()
+            off = off * baseline_factor
+        out = obj - off
+        if positivity:
+            out = np.maximum(out, 0.0)
+        if m is not None:
+            out = out * m
+    else:
+        raise ValueError(obj_type)
+    if taps is not None:
+        out = blur(out, taps)
+    if identical and out.shape[0] > 1:
+        out = np.broadcast_to(out.mean(axis=0, keepdims=True), out.shape).copy()
+    return out
+
+
+def constrain_object_ext_vjp(obj: np.ndarray, grad_out: np.ndarray, obj_type: str, mask=None,
+                             positivity: bool = True, fix_baseline: bool = False, baseline_factor: float = 1.0,
+                             taps=None, identical: bool = False) -> np.ndarray:
+    """VJP of ``constrain_object_ext`` w.r.t. the raw object (torch convention).  Identical
+    slices pass the gradient straight through (the reference averages in place under
+    no_grad), the blur is self-adjoint, the potential's offset is detached."""
+    g = np.asarray(grad_out)
+    if taps is not None:
+        g = blur(g, taps)
+    m = None if mask is None else np.asarray(mask, dtype=np.float64)[None]
+    if obj_type in ("complex", "pure_phase"):
+        mag = np.abs(obj)
+        amp = np.clip(mag, 0.0, 1.0) if obj_type == "complex" else np.ones(obj.shape)
+        th = np.angle(obj) - np.angle(obj).mean()
+        mm = np.ones(obj.shape) if m is None else np.broadcast_to(m, obj.shape)
+        A = amp * (mm if m is None else mm * mm)
+        e = np.exp(1j * th * mm)
+        g_amp = (mm * mm if m is not None else 1.0) * (np.conj(e) * g).real
+        g_th = mm * A * (np.conj(e) * g).imag
+        g_ph = g_th - g_th.mean()
+        passes = (mag >= 0.0) & (mag <= 1.0) if obj_type == "complex" else np.zeros(obj.shape, bool)
+        g_mag = np.where(passes, g_amp, 0.0)
+        safe = np.where(mag == 0, 1.0, mag)
+        r = np.where(mag == 0, 0.0, g_mag * obj / safe + g_ph * 1j * obj / safe**2)
+        return r
+    if obj_type == "potential":
+        off = 0.0
+        if fix_baseline:
+            if m is not None:
+                bg = np.broadcast_to(m < 0.5 * m.max(), obj.shape)
+                off = obj[bg].mean() if bg.any() else obj.min()
+            else:
+                off = obj.min()
+            off = off * baseline_factor
+        v = obj - off
+        passes = (v >= 0.0) if positivity else np.ones(v.shape, bool)
+        gg = np.real(g) * (1.0 if m is None else m)
+        return np.where(passes, gg, 0.0)
+    raise ValueError(obj_type)
+
+
+def phase_exp_vjp(v: np.ndarray, grad_t: np.ndarray) -> np.ndarray:
+    """dL/dV of t = exp(i V) (object_models.py:252-256): Re(conj(G) i t)."""
+    return (np.conj(grad_t) * 1j * np.exp(1j * v)).real
+
+
+def soft_constraint_loss(obj2: np.ndarray, obj_type: str, tv_weight_z: float = 0.0, tv_weight_xy: float = 0.0,
+                         surface_zero_weight: float = 0.0):
+    """Soft constraints of the hard-constrained object (object_models.py:341-435): TV of
+    the phase (and, for complex objects, the amplitude) or of the potential, along z with
+    tv_weight_z and along rows / columns with tv_weight_xy, each term w * mean |diff|,
+    divided by the number of weighted dimensions; surface-zero terms on the first and last
+    slices (3 slices or more).  Returns (loss, gradient w.r.t. obj2 in torch convention)."""
+    S = obj2.shape[0]
+    w = (tv_weight_z, tv_weight_xy) if S > 1 else (0.0, tv_weight_xy)
+    loss = 0.0
+    cplx = np.iscomplexobj(obj2)
+    g_ph = np.zeros(obj2.shape)
+    g_amp = np.zeros(obj2.shape)
+    g_real = np.zeros(obj2.shape)
+
+    def tv(a, g):
+        nonlocal loss
+        ws = [w[0] if (d == 0) else w[1] for d in range(3)]
+        nd = sum(1 for x in ws if x > 0)
+        if nd == 0:
+            return
+        for d in range(3):
+            if ws[d] <= 0:
+                continue
+            df = np.diff(a, axis=d)
+            loss += ws[d] * np.mean(np.abs(df)) / nd
+            sg = np.sign(df) * ws[d] / (df.size * nd)
+            pad_hi = [(0, 0)] * 3
+            pad_lo = [(0, 0)] * 3
+            pad_hi[d] = (1, 0)
+            pad_lo[d] = (0, 1)
+            g += np.pad(sg, pad_hi) - np.pad(sg, pad_lo)
+
+    if any(w):
+        if cplx:
+            tv(np.angle(obj2), g_ph)
+            if obj_type == "complex":
+                tv(np.abs(obj2), g_amp)
+        else:
+            tv(obj2, g_real)
+    if surface_zero_weight and S >= 3:
+        sw = surface_zero_weight
+        for k in (0, S - 1):
+            if cplx:
+                ang = np.angle(obj2[k])
+                ph = np.abs(ang)
+                u = ph - ph.mean()
+                n = u.size
+                if obj_type == "complex":
+                    loss += sw * np.mean(1.0 - np.abs(obj2[k]))
+                    g_amp[k] += -sw / n
+                loss += sw * np.mean(np.abs(u))
+                su = np.sign(u)
+                g_ph[k] += sw * (su - su.mean()) / n * np.sign(ang)
+            else:
+                loss += sw * np.mean(np.abs(obj2[k]))
+                g_real[k] += sw * np.sign(obj2[k]) / obj2[k].size
+    if cplx:
+        a = np.abs(obj2)
+        safe = np.where(a == 0, 1.0, a)
+        grad = np.where(a == 0, 0.0, g_amp * obj2 / safe + 1j * g_ph * obj2 / safe**2)
+        return float(loss), grad
+    return float(loss), g_real
+
+
 def gram_schmidt(probe: np.ndarray):
     """Mixed-state probe orthogonalisation + intensity sort; probe_models.py:484-525.
 
@@ -476,16 +681,34 @@ def batch_loss_and_grads(obj_c, probe_o, positions_px, props, targets, mask, num
     return loss, g_obj, g_probe, st
 
 
+def _ext_args(obj_constraints: dict, obj_mask):
+    c = obj_constraints
+    return dict(mask=obj_mask if c.get("apply_fov_mask") else None, positivity=c.get("positivity", True),
+                fix_baseline=c.get("fix_potential_baseline", False),
+                baseline_factor=c.get("fix_potential_baseline_factor", 1.0),
+                taps=gaussian_taps(c["gaussian_sigma"]) if c.get("gaussian_sigma") is not None else None,
+                identical=c.get("identical_slices", False))
+
+
 def full_gradients(obj_raw, probe_raw, positions_px, props, targets, mask, num_gpts,
                    mean_intensity, upsample_factor, orthogonalize=True,
-                   loss_type="l2_amplitude", obj_type="complex", descan=None):
+                   loss_type="l2_amplitude", obj_type="complex", descan=None, obj_constraints=None,
+                   obj_mask=None):
     """Loss and gradients w.r.t. the raw parameters, as Ptychography.backward
     leaves them (autograd branch, ptychography.py:326-332): the object gradient
     is scaled by upsample_factor**2 / 2.  ``obj_type``: complex, pure_phase or
     potential (default constraints: positivity on, baseline not fixed).  ``descan``:
     (B, 2) descan shifts of the batch or None; ``descan_gradients(st)`` and
-    ``tilt_gradients(st, ...)`` read the returned state."""
-    obj_c = object_transmission(obj_raw, obj_type)
+    ``tilt_gradients(st, ...)`` read the returned state.  ``obj_constraints`` (a dict of the
+    reference's object constraints) with ``obj_mask`` (the FOV mask) selects the full hard
+    constraint (``constrain_object_ext``) and adds the soft-constraint loss, as the
+    reference's batch loss does (ptychography.py:229-231)."""
+    if obj_constraints is not None:
+        ext = _ext_args(obj_constraints, obj_mask)
+        obj2 = constrain_object_ext(obj_raw, obj_type, **ext)
+        obj_c = np.exp(1j * obj2) if obj_type == "potential" else obj2
+    else:
+        obj_c = object_transmission(obj_raw, obj_type)
     if orthogonalize:
         probe_o, _, cache = gram_schmidt(probe_raw)
     else:
@@ -493,7 +716,17 @@ def full_gradients(obj_raw, probe_raw, positions_px, props, targets, mask, num_g
     loss, g_obj_c, g_probe_o, st = batch_loss_and_grads(
         obj_c, probe_o, positions_px, props, targets, mask, num_gpts, mean_intensity, loss_type, descan)
     st.probe_o = probe_o
-    g_obj = object_transmission_vjp(obj_raw, g_obj_c, obj_type) * (upsample_factor**2 / 2)
+    if obj_constraints is not None:
+        c = obj_constraints
+        g2 = phase_exp_vjp(obj2, g_obj_c) if obj_type == "potential" else g_obj_c
+        if c.get("tv_weight_z", 0) or c.get("tv_weight_xy", 0) or c.get("surface_zero_weight", 0):
+            soft, g_soft = soft_constraint_loss(obj2, obj_type, c.get("tv_weight_z", 0), c.get("tv_weight_xy", 0),
+                                                c.get("surface_zero_weight", 0))
+            loss = loss + soft
+            g2 = g2 + g_soft
+        g_obj = constrain_object_ext_vjp(obj_raw, g2, obj_type, **ext) * (upsample_factor**2 / 2)
+    else:
+        g_obj = object_transmission_vjp(obj_raw, g_obj_c, obj_type) * (upsample_factor**2 / 2)
     g_probe = gram_schmidt_vjp(cache, g_probe_o) if orthogonalize else g_probe_o
     return loss, g_obj, g_probe, st
 
@@ -576,7 +809,7 @@ def gaussian_atom_phase(shape, n_atoms, sigma_px, peak_rad, rng):
 def reconstruct(obj_raw, probe_raw, positions_px, props, targets, mask, mean_intensity, upsample_factor,
                 num_iters, batch_size, rng, lr_obj=5e-3, lr_probe=1e-3, orthogonalize=True,
                 loss_type="l2_amplitude", obj_type="complex", lr_positions=None, descan=None, lr_descan=None,
-                tilt=None, prop_geometry=None):
+                tilt=None, prop_geometry=None, obj_constraints=None, obj_mask=None):
     """Adam iterations of Ptychography.reconstruct (ptychography.py:208-245) on
     the given state; batches from a numpy generator like SimpleBatcher.  With
     ``lr_positions`` the scan positions are a parameter too (a dataset optimiser,
@@ -604,7 +837,8 @@ def reconstruct(obj_raw, probe_raw, positions_px, props, targets, mask, mean_int
                 props = propagators(roi, samp, energy, dz, tilt_mrad=tuple(th))
             loss, g_obj, g_probe, st = full_gradients(obj, probe, pos[bi], props, targets[bi], mask, npos,
                                                       mean_intensity, upsample_factor, orthogonalize, loss_type,
-                                                      obj_type, descan=None if dsc is None else dsc[bi])
+                                                      obj_type, descan=None if dsc is None else dsc[bi],
+                                                      obj_constraints=obj_constraints, obj_mask=obj_mask)
             if lr_positions is not None:
                 g_pos = np.zeros_like(pos)
                 g_pos[bi] = position_gradients(st.probe_o, st, st.g_probe_plane)

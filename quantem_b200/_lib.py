@@ -73,6 +73,17 @@ EXPORTED = (
     "ptycho_probe_ortho_work_elems",
     "ptycho_probe_orthogonalize",
     "ptycho_probe_orthogonalize_vjp",
+    "ptycho_obj_constraint_work_elems",
+    "ptycho_probe_overlap",
+    "ptycho_obj_constrain_fov",
+    "ptycho_obj_constrain_fov_vjp",
+    "ptycho_obj_potential_base",
+    "ptycho_obj_potential_base_vjp",
+    "ptycho_phase_exp",
+    "ptycho_phase_exp_vjp",
+    "ptycho_obj_blur",
+    "ptycho_obj_slice_mean",
+    "ptycho_obj_soft_loss",
 )
 
 _vp = ctypes.c_void_p
@@ -153,6 +164,18 @@ def _declare(lib):
         "ptycho_probe_ortho_work_elems": (_i64, [_int, _i64]),
         "ptycho_probe_orthogonalize": (_int, [_vp, _vp, _int, _i64, _vp, _i64, _vp]),
         "ptycho_probe_orthogonalize_vjp": (_int, [_vp, _vp, _vp, _int, _i64, _vp, _i64, _vp]),
+        "ptycho_obj_constraint_work_elems": (_int, []),
+        "ptycho_probe_overlap": (_int, [_vp, _int, _vp, _int, _int, _int, _vp, _vp]),
+        "ptycho_obj_constrain_fov": (_int, [_vp, _vp, _i64, _vp, _i64, _int, _vp, _int, _vp]),
+        "ptycho_obj_constrain_fov_vjp": (_int, [_vp, _vp, _i64, _vp, _vp, _i64, _int, _vp, _int, _vp]),
+        "ptycho_obj_potential_base": (_int, [_vp, _vp, _vp, _i64, _vp, _i64, _int, _int, _flt, _vp, _int, _vp]),
+        "ptycho_obj_potential_base_vjp": (_int, [_vp, _vp, _vp, _i64, _vp, _vp, _i64, _int, _int, _flt, _vp, _int,
+                                                 _vp]),
+        "ptycho_phase_exp": (_int, [_vp, _vp, _i64, _vp]),
+        "ptycho_phase_exp_vjp": (_int, [_vp, _vp, _vp, _i64, _vp]),
+        "ptycho_obj_blur": (_int, [_vp, _vp, _vp, _int, _int, _int, _int, _vp, _int, _vp]),
+        "ptycho_obj_slice_mean": (_int, [_vp, _vp, _int, _i64, _int, _vp]),
+        "ptycho_obj_soft_loss": (_int, [_vp, _int, _int, _int, _int, _flt, _flt, _flt, _vp, _int, _vp, _vp, _vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

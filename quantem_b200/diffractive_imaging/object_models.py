@@ -24,11 +24,9 @@ class ObjectPixelated(OptimizerMixin):
         "surface_zero_weight": 0, "gaussian_sigma": None, "butterworth_order": 4, "q_lowpass": None,
         "q_highpass": None,
     }
-    # constraints whose non-default values need operations outside the B200 path
-    # (fix_potential_baseline: the reference takes the baseline from the background of the
-    # probe-overlap FOV mask its preprocess builds, which this path does not build)
-    _UNSUPPORTED = ("identical_slices", "apply_fov_mask", "tv_weight_z", "tv_weight_xy", "surface_zero_weight",
-                    "gaussian_sigma", "q_lowpass", "q_highpass", "fix_potential_baseline")
+    # constraints whose non-default values are not built: the Butterworth filters need an
+    # object-sized 2-D FFT (object_models.py:481-520)
+    _UNSUPPORTED = ("q_lowpass", "q_highpass")
     _token = object()
 
     def __init__(self, num_slices=1, slice_thicknesses=None, obj_type="complex", initialize_mode="uniform",
@@ -87,6 +85,37 @@ class ObjectPixelated(OptimizerMixin):
     def dtype(self):
         """float32 for potentials, complex64 otherwise (object_models.py:85-89)."""
         return torch.float32 if self._obj_type == "potential" else torch.complex64
+
+    def _ext_constraints(self) -> bool:
+        """Whether the optional hard constraints are active (FOV mask, Gaussian blur, identical
+        slices, a potential baseline taken from the FOV mask's background)."""
+        c = self._constraints
+        return bool((c.get("apply_fov_mask") and self._mask is not None) or c.get("gaussian_sigma") is not None
+                    or (c.get("identical_slices") and self.num_slices > 1)
+                    or (self._obj_type == "potential" and c.get("fix_potential_baseline")))
+
+    @property
+    def has_soft_constraints(self) -> bool:
+        c = self._constraints
+        return bool(c.get("tv_weight_z", 0) or c.get("tv_weight_xy", 0) or c.get("surface_zero_weight", 0))
+
+    def _mask_on_device(self):
+        m = self._mask
+        if m is None:
+            return None
+        if m.device != torch.device(self._obj.device) or m.dtype != torch.float32 or not m.is_contiguous():
+            self._mask = m = m.to(self._obj.device, torch.float32).contiguous()
+        return m
+
+    def batch_object(self):
+        """(tensor, ObjSpec) for the batch kernels: the raw object and its transmission spec,
+        or, with the optional hard constraints active, the transmission itself (computed by
+        the constraint kernels, differentiable) with an identity spec."""
+        from .. import ops
+
+        if self._ext_constraints():
+            return self.transmission(), ops.ObjSpec("complex", hard_constraint=False)
+        return self._obj, self.transmission_spec()
 
     def transmission_spec(self):
         """What the batch kernels need to turn the raw object into its transmission."""
@@ -173,7 +202,13 @@ class ObjectPixelated(OptimizerMixin):
 
     @mask.setter
     def mask(self, m):
-        self._mask = None if m is None else torch.as_tensor(m)
+        """The probe-overlap FOV mask (Ho, Wo) (the reference stores it expanded over the
+        slices; a (S, Ho, Wo) mask is reduced to its first slice)."""
+        if m is None:
+            self._mask = None
+            return
+        t = torch.as_tensor(np.asarray(m) if not isinstance(m, torch.Tensor) else m.detach(), dtype=torch.float32)
+        self._mask = (t[0] if t.ndim == 3 else t).contiguous()
 
     # ------------------------------------------------------------ state
     def _initialize_obj(self, shape, sampling=None):
@@ -235,7 +270,15 @@ class ObjectPixelated(OptimizerMixin):
         pass
 
     def apply_soft_constraints(self, obj, mask=None):
-        return torch.zeros((), device=self._obj.device)
+        """Soft constraints of the hard-constrained object (object_models.py:341-358): TV
+        along z and in-plane and the surface-zero terms, by the constraint kernels."""
+        from .. import ops
+
+        if not self.has_soft_constraints:
+            return torch.zeros((), device=self._obj.device)
+        c = self._constraints
+        return ops.soft_constraint_loss(obj, self._obj_type, c.get("tv_weight_z", 0), c.get("tv_weight_xy", 0),
+                                        c.get("surface_zero_weight", 0))
 
     # ------------------------------------------------------------ compute
     @property
@@ -245,6 +288,8 @@ class ObjectPixelated(OptimizerMixin):
         V - offset clamped at 0."""
         from .. import ops
 
+        if self._ext_constraints():
+            return ops.constrained_object_ext(self._obj, self._obj_type, self._constraints, self._mask_on_device())
         if self._obj_type == "complex":
             return ops.constrained_object(self._obj)
         if self._obj_type == "pure_phase":
@@ -260,6 +305,8 @@ class ObjectPixelated(OptimizerMixin):
         differentiable, CUDA kernels): what multiplies the wave in every slice."""
         from .. import ops
 
+        if self._ext_constraints():
+            return ops.transmission_of(self.obj)
         return ops.object_transmission(self._obj, self.transmission_spec())
 
     def forward(self, patch_indices: torch.Tensor) -> torch.Tensor:
@@ -288,6 +335,10 @@ class ObjectDIP(ObjectPixelated):
     hard constraint of the object type.  Gradients flow from the fused adjoint into the
     CNN backward kernels by torch autograd; the pixelated-object gradient rescale
     (ptychography.py:330-332) is not applied, as in the reference."""
+
+    # the DIP network's output takes only the default hard constraints on this path
+    _UNSUPPORTED = ("identical_slices", "apply_fov_mask", "tv_weight_z", "tv_weight_xy", "surface_zero_weight",
+                    "gaussian_sigma", "q_lowpass", "q_highpass", "fix_potential_baseline")
 
     def __init__(self, num_slices=1, slice_thicknesses=None, input_noise_std=0.025, device="cuda",
                  obj_type="complex", rng=None, _token=None):

@@ -273,10 +273,44 @@ class Ptychography:
         self.dset._set_initial_scan_positions_px(self.obj_padding_px)
         self.dset._set_patch_indices(self.obj_padding_px)
         self.compute_propagator_arrays()
+        self._set_obj_fov_mask()
         self._preprocessed = True
         self.val_ratio = float(val_ratio)
         self.val_mode = val_mode
         return self
+
+    def _get_probe_overlap(self) -> np.ndarray:
+        """Sum over positions of |probe mode 0|^2 at each patch window (ptychography_base.py:
+        201-216): the overlap kernel on CUDA devices, a host sum during a host set-up."""
+        with torch.no_grad():
+            inten = self.probe_model.probe[0].detach().abs().square().to(torch.float32).contiguous()
+        pos = self.dset.scan_positions_px.detach().to(torch.float32).contiguous()
+        shape = tuple(int(x) for x in self.obj_shape_full[-2:])
+        if inten.device.type == "cuda":
+            return ops.probe_overlap(inten, pos.to(inten.device), shape).cpu().numpy()
+        n = int(inten.shape[-1])
+        fr = np.fft.fftfreq(n, d=1.0 / n).astype(np.int64)
+        org = np.round(pos.numpy().astype(np.float64)).astype(np.int64)
+        rows = (org[:, 0][:, None] + fr[None]) % shape[0]
+        cols = (org[:, 1][:, None] + fr[None]) % shape[1]
+        out = np.zeros(shape, dtype=np.float32)
+        a = inten.numpy()
+        for b in range(org.shape[0]):
+            np.add.at(out, (rows[b][:, None], cols[b][None, :]), a)
+        return out
+
+    def _set_obj_fov_mask(self, gaussian_sigma: float = 2.0):
+        """The probe-overlap FOV mask (ptychography_base.py:191-199): overlap > 0.3 max,
+        binary closing (5 iterations), binary dilation (min(32, min padding // 4)
+        iterations), Gaussian filter; used by ``apply_fov_mask`` and by a fixed potential
+        baseline."""
+        overlap = self._get_probe_overlap()
+        ov = overlap > overlap.max() * 0.3
+        ov = ndi.binary_closing(ov, iterations=5)
+        ov = ndi.binary_dilation(ov, iterations=min(32, int(np.min(self.obj_padding_px)) // 4))
+        ov = ndi.gaussian_filter(ov.astype(np.float32), sigma=gaussian_sigma)
+        self.obj_fov_mask = ov
+        self.obj_model.mask = ov
 
     def compute_propagator_arrays(self):
         """Propagators like the reference (complex64, probe_models.py:376-427) plus
@@ -510,6 +544,7 @@ class Ptychography:
                 tg = stream.acquire()
                 if a0 + 1 < num_iters:
                     stream.prefetch_next()
+            consistency = torch.zeros((), dtype=torch.float32, device=dev)
             for bi in batcher:
                 for o in opts:
                     o.zero_grad(set_to_none=True)
@@ -518,23 +553,30 @@ class Ptychography:
                 idx = torch.as_tensor(np.asarray(bi, dtype=np.int64)).to(dev, non_blocking=True)
                 if autograd:
                     probe_o = self.probe_model.probe
-                    obj_raw = self.obj_model._obj  # a leaf (pixelated) or a network output (DIP)
+                    leaf = self.obj_model._obj  # a leaf (pixelated) or a network output (DIP)
+                    # the raw object and its transmission spec, or the transmission of the
+                    # optional constraint chain with an identity spec
+                    obj_raw, obj_spec = self.obj_model.batch_object()
                     # learned descan shifts and probe tilt enter the kernels as differentiable inputs
                     descan = self.dset.batch_descan()
                     tilt = self.probe_model.probe_tilt
                     tilt = tilt if (tilt.requires_grad and self.num_slices > 1) else None
-                    loss = ops.batch_loss(obj_raw, probe_o, prop, pos, idx, tg, mask,
-                                          self.dset.num_gpts, self.dset.mean_diffraction_intensity, loss_type,
-                                          obj_spec=self.obj_model.transmission_spec(), descan=descan, tilt=tilt,
-                                          prop_geometry=self._prop_geometry() if tilt is not None else None)
+                    closs = ops.batch_loss(obj_raw, probe_o, prop, pos, idx, tg, mask,
+                                           self.dset.num_gpts, self.dset.mean_diffraction_intensity, loss_type,
+                                           obj_spec=obj_spec, descan=descan, tilt=tilt,
+                                           prop_geometry=self._prop_geometry() if tilt is not None else None)
+                    loss = closs
+                    # soft constraints join the batch loss (ptychography.py:125-140, 229-231)
+                    if self.obj_model.has_soft_constraints:
+                        loss = loss + self.obj_model.apply_soft_constraints(self.obj_model.obj)
                     if descan is not None and self.dset.constraints.get("descan_tv_weight", 0) > 0:
-                        loss = loss + self.dset.apply_soft_constraints(descan)  # ptychography.py:125-140
+                        loss = loss + self.dset.apply_soft_constraints(descan)
                     if (obj_raw.requires_grad or self.probe_model._probe.requires_grad or pos.requires_grad
                             or (descan is not None and descan.requires_grad) or tilt is not None):
                         loss.backward()
-                        if obj_raw.is_leaf and obj_raw.grad is not None:
+                        if leaf.is_leaf and leaf.grad is not None:
                             # pixelated objects only (ptychography.py:330-332)
-                            obj_raw.grad.mul_(self.dset.upsample_factor ** 2 / 2)
+                            leaf.grad.mul_(self.dset.upsample_factor ** 2 / 2)
                 else:
                     # analytic update directions (ptychography.py:339-348), no autograd graph
                     if type(self.obj_model).__name__ == "ObjectDIP":
@@ -544,6 +586,8 @@ class Ptychography:
                                                   "use autograd=True for pure-phase and potential objects")
                     if self.dset.batch_descan() is not None:
                         raise NotImplementedError("learned descan shifts need autograd=True")
+                    if self.obj_model._ext_constraints() or self.obj_model.has_soft_constraints:
+                        raise NotImplementedError("the optional object constraints need autograd=True")
                     with torch.no_grad():
                         probe_o = self.probe_model.probe.detach().contiguous()
                         obj_c, _ = ops.obj_constrain(self.obj_model._obj.detach().contiguous())
@@ -552,13 +596,20 @@ class Ptychography:
                             self.dset.mean_diffraction_intensity, loss_type)
                     self.obj_model._obj.grad = g_obj
                     self.probe_model._probe.grad = g_probe
+                    closs = loss
                 for o in opts:
                     o.step()
                 total += loss.detach()
+                consistency += closs.detach()
                 nb += 1
             if stream is not None:
                 stream.release()
             total_loss = float((total / max(nb, 1)).item())
+            # the logger receives the consistency loss alone (ptychography.py:284-292)
+            consistency_loss = total_loss
+            if self.logger is not None and (self.obj_model.has_soft_constraints or
+                                            self.dset.constraints.get("descan_tv_weight", 0) > 0):
+                consistency_loss = float((consistency / max(nb, 1)).item())
             ops.check_status(dev)  # out-of-range batch indices / non-finite intensities since the last check
             val_loss = None
             if batcher.has_validation:
@@ -575,8 +626,8 @@ class Ptychography:
             if self._store_snapshots and (a0 % self._store_snapshot_every) == 0:
                 self._snapshots.append(dict(iteration=self.num_iters, obj=self.obj, probe=self.probe))
             if self.logger is not None:
-                self.logger.log_iter(self.obj_model, self.probe_model, self.dset, self.num_iters - 1, total_loss,
-                                     nb, self._get_current_lrs())
+                self.logger.log_iter(self.obj_model, self.probe_model, self.dset, self.num_iters - 1,
+                                     consistency_loss, nb, self._get_current_lrs())
         return self
 
     def _get_current_lrs(self):

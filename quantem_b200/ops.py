@@ -689,6 +689,218 @@ def separable_propagators(n, sampling, energy, slice_thicknesses, tilt_mrad=(0.0
 
 
 # ----------------------------------------------------------------------------
+# optional object constraints (object_models.py:273-480) and the FOV mask
+# ----------------------------------------------------------------------------
+
+def _cwork(device) -> torch.Tensor:
+    return torch.empty(int(_lib.lib().ptycho_obj_constraint_work_elems()), dtype=torch.float64, device=device)
+
+
+def probe_overlap(intensity: torch.Tensor, positions: torch.Tensor, obj_shape_2d) -> torch.Tensor:
+    """(Ho, Wo) float32: sum over positions of ``intensity`` (n, n) placed at each
+    position's wrapped patch window (ptychography_base.py:201-216)."""
+    dev = intensity.device
+    _req(intensity, "intensity", torch.float32, dev)
+    _req(positions, "positions", torch.float32, dev)
+    Ho, Wo = (int(x) for x in obj_shape_2d)
+    out = torch.empty((Ho, Wo), dtype=torch.float32, device=dev)
+    _lib.check(_lib.lib().ptycho_probe_overlap(_p(intensity), int(intensity.shape[-1]), _p(positions),
+                                               int(positions.shape[0]), Ho, Wo, _p(out), _stream()), "probe_overlap")
+    return out
+
+
+def gaussian_taps(sigma: float, device) -> torch.Tensor:
+    """The normalised float32 Gaussian of object_models.py:445-451."""
+    import math
+
+    k = int(2 * math.ceil(3 * sigma) + 1)
+    if k % 2 == 0:
+        k += 1
+    ax = np.arange(-k // 2 + 1.0, k // 2 + 1.0, dtype=np.float32)
+    g = np.exp(-0.5 * (ax / np.float32(sigma)) ** 2).astype(np.float32)
+    return torch.as_tensor(g / g.sum(), dtype=torch.float32, device=device)
+
+
+class _FovConstrainFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, obj, mask, pure):
+        o = obj.detach().contiguous()
+        m = mask.detach().contiguous()
+        out = torch.empty_like(o)
+        work = _cwork(o.device)
+        _lib.check(_lib.lib().ptycho_obj_constrain_fov(_p(o), _p(m), m.numel(), _p(out), o.numel(), int(pure),
+                                                       _p(work), work.numel(), _stream()), "obj_constrain_fov")
+        ctx.save_for_backward(o, m)
+        ctx.pure = pure
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        o, m = ctx.saved_tensors
+        g = g.detach().to(torch.complex64).contiguous()
+        out = torch.empty_like(o)
+        work = _cwork(o.device)
+        _lib.check(_lib.lib().ptycho_obj_constrain_fov_vjp(_p(o), _p(m), m.numel(), _p(g), _p(out), o.numel(),
+                                                           int(ctx.pure), _p(work), work.numel(), _stream()),
+                   "obj_constrain_fov_vjp")
+        return out, None, None
+
+
+class _PotentialBaseFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, v, bmask, amask, positivity, fix, factor):
+        v = v.detach().contiguous()
+        out = torch.empty_like(v)
+        work = _cwork(v.device)
+        hw = int(v.shape[-2] * v.shape[-1])
+        _lib.check(_lib.lib().ptycho_obj_potential_base(
+            _p(v), _p(bmask) if bmask is not None else None, _p(amask) if amask is not None else None, hw, _p(out),
+            v.numel(), int(positivity), int(fix), float(factor), _p(work), work.numel(), _stream()),
+            "obj_potential_base")
+        ctx.save_for_backward(v, *(t for t in (bmask, amask) if t is not None))
+        ctx.has = (bmask is not None, amask is not None)
+        ctx.args = (int(positivity), int(fix), float(factor))
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        saved = list(ctx.saved_tensors)
+        v = saved.pop(0)
+        bmask = saved.pop(0) if ctx.has[0] else None
+        amask = saved.pop(0) if ctx.has[1] else None
+        g = g.detach().to(torch.float32).contiguous()
+        out = torch.empty_like(v)
+        work = _cwork(v.device)
+        hw = int(v.shape[-2] * v.shape[-1])
+        _lib.check(_lib.lib().ptycho_obj_potential_base_vjp(
+            _p(v), _p(bmask) if bmask is not None else None, _p(amask) if amask is not None else None, hw, _p(g),
+            _p(out), v.numel(), *ctx.args, _p(work), work.numel(), _stream()), "obj_potential_base_vjp")
+        return out, None, None, None, None, None
+
+
+class _PhaseExpFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, v):
+        v = v.detach().contiguous()
+        out = torch.empty(v.shape, dtype=torch.complex64, device=v.device)
+        _lib.check(_lib.lib().ptycho_phase_exp(_p(v), _p(out), v.numel(), _stream()), "phase_exp")
+        ctx.save_for_backward(v)
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        (v,) = ctx.saved_tensors
+        g = g.detach().to(torch.complex64).contiguous()
+        out = torch.empty_like(v)
+        _lib.check(_lib.lib().ptycho_phase_exp_vjp(_p(v), _p(g), _p(out), v.numel(), _stream()), "phase_exp_vjp")
+        return out
+
+
+def _blur(x: torch.Tensor, taps: torch.Tensor) -> torch.Tensor:
+    x = x.contiguous()
+    out = torch.empty_like(x)
+    tmp = torch.empty_like(x)
+    S, Ho, Wo = (int(d) for d in x.shape)
+    _lib.check(_lib.lib().ptycho_obj_blur(_p(x), _p(out), _p(tmp), S, Ho, Wo, int(x.is_complex()), _p(taps),
+                                          int(taps.numel()), _stream()), "obj_blur")
+    return out
+
+
+class _BlurFn(torch.autograd.Function):
+    """Zero-padded separable Gaussian blur: self-adjoint, so the VJP is the same blur."""
+
+    @staticmethod
+    def forward(ctx, x, taps):
+        ctx.save_for_backward(taps)
+        return _blur(x.detach(), taps)
+
+    @staticmethod
+    def backward(ctx, g):
+        (taps,) = ctx.saved_tensors
+        return _blur(g.detach(), taps), None
+
+
+class _SliceMeanFn(torch.autograd.Function):
+    """identical_slices: every slice replaced by the slice mean; the reference does it in
+    place under no_grad, so the gradient passes straight through."""
+
+    @staticmethod
+    def forward(ctx, x):
+        x = x.detach().contiguous()
+        out = torch.empty_like(x)
+        S = int(x.shape[0])
+        _lib.check(_lib.lib().ptycho_obj_slice_mean(_p(x), _p(out), S, x[0].numel(), int(x.is_complex()),
+                                                    _stream()), "obj_slice_mean")
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        return g
+
+
+def constrained_object_ext(obj_raw: torch.Tensor, obj_type: str, constraints: dict, mask=None) -> torch.Tensor:
+    """ObjectConstraints.apply_hard_constraints (object_models.py:289-339) with the optional
+    constraints: the FOV mask (``apply_fov_mask``, ``mask`` (Ho, Wo)), the potential's
+    baseline from the mask's background (``fix_potential_baseline``), ``gaussian_sigma`` and
+    ``identical_slices`` (Butterworth filters are not built).  Differentiable; returns the
+    complex object, or the real potential before exp(i V)."""
+    c = constraints
+    use_mask = bool(c.get("apply_fov_mask")) and mask is not None
+    if obj_type in ("complex", "pure_phase"):
+        if use_mask:
+            out = _FovConstrainFn.apply(obj_raw, mask, obj_type == "pure_phase")
+        else:
+            out = object_transmission(obj_raw, ObjSpec(obj_type))
+    elif obj_type == "potential":
+        fix = bool(c.get("fix_potential_baseline", False))
+        out = _PotentialBaseFn.apply(obj_raw, mask if fix else None, mask if use_mask else None,
+                                     bool(c.get("positivity", True)), fix,
+                                     float(c.get("fix_potential_baseline_factor", 1.0)))
+    else:
+        raise ValueError(f"unknown object type {obj_type!r}")
+    if c.get("gaussian_sigma") is not None:
+        out = _BlurFn.apply(out, gaussian_taps(float(c["gaussian_sigma"]), out.device))
+    if c.get("identical_slices") and out.shape[0] > 1:
+        out = _SliceMeanFn.apply(out)
+    return out
+
+
+def transmission_of(obj2: torch.Tensor) -> torch.Tensor:
+    """What multiplies the wave: the complex object itself, exp(i V) of a potential
+    (object_models.py:252-256)."""
+    return obj2 if obj2.is_complex() else _PhaseExpFn.apply(obj2)
+
+
+class _SoftLossFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, obj2, kind, wz, wxy, ws):
+        o = obj2.detach().contiguous()
+        S, Ho, Wo = (int(d) for d in o.shape)
+        loss = torch.empty((), dtype=torch.float32, device=o.device)
+        grad = torch.empty_like(o)
+        work = _cwork(o.device)
+        _lib.check(_lib.lib().ptycho_obj_soft_loss(_p(o), S, Ho, Wo, int(kind), float(wz), float(wxy), float(ws),
+                                                   _p(work), work.numel(), _p(loss), _p(grad), _stream()),
+                   "obj_soft_loss")
+        ctx.save_for_backward(grad)
+        return loss
+
+    @staticmethod
+    def backward(ctx, g):
+        (grad,) = ctx.saved_tensors
+        return grad * g.to(torch.float32), None, None, None, None
+
+
+def soft_constraint_loss(obj2: torch.Tensor, obj_type: str, tv_weight_z=0.0, tv_weight_xy=0.0,
+                         surface_zero_weight=0.0) -> torch.Tensor:
+    """Soft constraints of the hard-constrained object (object_models.py:341-435): TV along z
+    and in-plane, surface-zero terms; a differentiable scalar (zero gradient at zero-magnitude
+    pixels, where the reference's autograd gives NaN)."""
+    kind = {"complex": 0, "pure_phase": 1, "potential": 2}[obj_type]
+    return _SoftLossFn.apply(obj2, kind, float(tv_weight_z), float(tv_weight_xy), float(surface_zero_weight))
+
+
+# ----------------------------------------------------------------------------
 # optimiser steps
 # ----------------------------------------------------------------------------
 

@@ -1,0 +1,189 @@
+"""Optional object constraints on the CUDA path (object_models.py:273-480) and the FOV
+mask (ptychography_base.py:191-216): every constraint kernel and its VJP against the FP64
+oracle, the constrained object, soft loss and batch gradients against the reference's own
+(fixtures objcons_*64), and the drop-in reconstruction with the constraints active against
+the reference's run."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import ptycho_oracle as O
+from tests.conftest import load_golden, rel
+from tests.test_oracle_golden import OBJCONS_CASES
+
+pytestmark = pytest.mark.gpu
+
+
+def _t(x, dev, dtype=None):
+    return torch.as_tensor(np.ascontiguousarray(x), device=dev, dtype=dtype)
+
+
+def _mask(rng, H, W):
+    m = np.zeros((H, W))
+    m[H // 5:4 * H // 5, W // 6:5 * W // 6] = 1.0
+    import scipy.ndimage as ndi
+
+    return ndi.gaussian_filter(m, 2.0) * (1 - 0.1 * rng.random((H, W)))
+
+
+@pytest.mark.parametrize("obj_type", ["complex", "pure_phase", "potential"])
+def test_constraint_kernels_match_fp64_oracle(cuda_device, obj_type):
+    from quantem_b200 import ops
+
+    dev = cuda_device
+    rng = np.random.default_rng({"complex": 1, "pure_phase": 2, "potential": 3}[obj_type])
+    S, H, W = 3, 48, 40
+    m = _mask(rng, H, W)
+    if obj_type == "potential":
+        raw = 0.05 + 0.1 * rng.standard_normal((S, H, W))
+        cons = {"fix_potential_baseline": True, "apply_fov_mask": True, "gaussian_sigma": 1.3,
+                "identical_slices": True}
+    else:
+        raw = (1 - 0.3 * rng.random((S, H, W))) * np.exp(0.5j * rng.standard_normal((S, H, W)))
+        cons = {"apply_fov_mask": True, "gaussian_sigma": 0.8}
+    raw32 = raw.astype(np.float32 if obj_type == "potential" else np.complex64)
+    x = _t(raw32, dev).requires_grad_(True)
+    obj2 = ops.constrained_object_ext(x, obj_type, cons, _t(m, dev, torch.float32))
+    ext = O._ext_args(cons, m.astype(np.float32).astype(np.float64))
+    ref2 = O.constrain_object_ext(raw32.astype(np.complex128 if obj_type != "potential" else np.float64), obj_type,
+                                  **ext)
+    assert rel(obj2.detach().cpu().numpy(), ref2) < 2e-5
+    t = ops.transmission_of(obj2)
+    G = rng.standard_normal(t.shape) + 1j * rng.standard_normal(t.shape)
+    (t.conj() * _t(G.astype(np.complex64), dev)).real.sum().backward()  # dL/dt = G (torch convention)
+    g2 = O.phase_exp_vjp(ref2, G) if obj_type == "potential" else G
+    g_ref = O.constrain_object_ext_vjp(raw32.astype(np.complex128 if obj_type != "potential" else np.float64),
+                                       g2, obj_type, **ext)
+    assert rel(x.grad.cpu().numpy(), g_ref) < 1e-4
+
+
+@pytest.mark.parametrize("obj_type", ["complex", "pure_phase", "potential"])
+def test_soft_constraint_kernel_matches_fp64_oracle(cuda_device, obj_type):
+    from quantem_b200 import ops
+
+    dev = cuda_device
+    rng = np.random.default_rng(11)
+    S, H, W = 4, 40, 56
+    if obj_type == "potential":
+        o = 0.2 * rng.standard_normal((S, H, W))
+    else:
+        o = (0.4 + 0.6 * rng.random((S, H, W))) * np.exp(1.0j * rng.standard_normal((S, H, W)))
+    o32 = o.astype(np.float32 if obj_type == "potential" else np.complex64)
+    x = _t(o32, dev).requires_grad_(True)
+    loss = ops.soft_constraint_loss(x, obj_type, 0.03, 0.05, 0.02)
+    loss.backward()
+    l_ref, g_ref = O.soft_constraint_loss(o32.astype(np.float64 if obj_type == "potential" else np.complex128),
+                                          obj_type, 0.03, 0.05, 0.02)
+    assert abs(loss.item() - l_ref) / abs(l_ref) < 1e-5
+    assert rel(x.grad.cpu().numpy(), g_ref) < 1e-4
+
+
+def test_blur_is_self_adjoint_and_slice_mean_passes_gradients(cuda_device):
+    from quantem_b200 import ops
+
+    dev = cuda_device
+    g = torch.Generator(device="cpu").manual_seed(3)
+    a = torch.randn((2, 33, 47), generator=g).to(dev)
+    b = torch.randn((2, 33, 47), generator=g).to(dev)
+    taps = ops.gaussian_taps(1.7, dev)
+    assert abs((ops._blur(a, taps) * b).sum().item() - (a * ops._blur(b, taps)).sum().item()) < 1e-3
+    ref = O.blur(a.cpu().double().numpy(), taps.cpu().numpy())
+    assert rel(ops._blur(a, taps).cpu().numpy(), ref) < 1e-6
+    x = a.clone().requires_grad_(True)
+    y = ops._SliceMeanFn.apply(x)
+    assert torch.allclose(y[0], a.mean(0), atol=1e-6) and torch.equal(y[0], y[1])
+    y.sum().backward()
+    assert torch.equal(x.grad, torch.ones_like(a))
+
+
+def test_probe_overlap_kernel_matches_reference(cuda_device):
+    from quantem_b200 import ops
+
+    z = load_golden("objcons_complex64")
+    dev = cuda_device
+    probe_o = O.gram_schmidt(z["probe_init"].astype(np.complex128))[0]
+    inten = _t((np.abs(probe_o[0]) ** 2).astype(np.float32), dev)
+    ov = ops.probe_overlap(inten, _t(z["positions"], dev, torch.float32), z["obj_shape"][-2:])
+    assert rel(ov.cpu().numpy(), z["probe_overlap"]) < 1e-5
+
+
+def _dropin(z, dev, obj_type):
+    from quantem_b200.diffractive_imaging import (Dataset4dstem, DetectorPixelated, ObjectPixelated,
+                                                  ProbePixelated, Ptychography, PtychographyDatasetRaster)
+
+    H, nscan = int(z["H"]), int(z["nscan"])
+    px, step = float(z["px"]), float(z["step_px"])
+    rs = 1.0 / (H * px)
+    d4 = Dataset4dstem.from_array(z["data"].reshape(nscan, nscan, H, H), sampling=(step * px, step * px, rs, rs),
+                                  units=("A", "A", "A^-1", "A^-1"))
+    pd = PtychographyDatasetRaster.from_dataset4dstem(d4, verbose=0)
+    pd.preprocess(com_fit_function="constant", force_com_rotation=0, force_com_transpose=False,
+                  probe_energy=float(z["energy"]), device="gpu")
+    obj = ObjectPixelated.from_uniform(num_slices=int(z["S"]), slice_thicknesses=float(z["dz"]), obj_type=obj_type)
+    probe = ProbePixelated.from_params(probe_params={"energy": float(z["energy"]), "defocus": 200.0,
+                                                     "semiangle_cutoff": 20.0},
+                                       num_probes=int(z["P"]), rng=92, initial_probe_weights=list(z["weights"]))
+    pt = Ptychography.from_models(dset=pd, obj_model=obj, probe_model=probe, detector_model=DetectorPixelated(),
+                                  device="gpu", verbose=0, rng=93)
+    pt.preprocess(obj_padding_px=(int(z["pad"]), int(z["pad"])))
+    pt.probe_model._probe = torch.as_tensor(z["probe_init"]).to(dev).requires_grad_(True)
+    pt._set_obj_fov_mask()  # from the reference's initial probe
+    pt.obj_model._obj = torch.as_tensor(z["obj_perturbed"]).to(dev).requires_grad_(True)
+    return pt
+
+
+@pytest.mark.parametrize("case", sorted(OBJCONS_CASES))
+def test_constrained_object_and_batch_gradients_match_reference(cuda_device, case):
+    from quantem_b200 import ops
+    from quantem_b200.diffractive_imaging.ptycho_utils import orthogonalize_probes
+
+    obj_type, cons = OBJCONS_CASES[case]
+    z = load_golden(f"objcons_{case}64")
+    dev = cuda_device
+    pt = _dropin(z, dev, obj_type)
+    assert np.abs(pt.obj_model.mask.cpu().numpy() - z["fov_mask"]).max() < 1e-5
+    pt.constraints = {"object": dict(cons)}
+    om = pt.obj_model
+    obj2 = om.obj
+    assert rel(obj2.detach().cpu().numpy(), z["obj_constrained"]) < 2e-5
+    soft = om.apply_soft_constraints(obj2)
+    assert abs(soft.item() - float(z["soft_loss"])) <= 1e-5 * max(float(z["soft_loss"]), 1e-3)
+    H = int(z["H"])
+    probe = _t(z["probe_init"], dev).requires_grad_(True)
+    obj_in, spec = om.batch_object()
+    loss = ops.batch_loss(obj_in, orthogonalize_probes(probe), _t(z["propagators"], dev),
+                          _t(z["positions"], dev, torch.float32), _t(z["batch_indices"].astype(np.int64), dev),
+                          _t(z["targets"], dev, torch.float32), torch.ones((H, H), device=dev),
+                          int(z["positions"].shape[0]), float(z["mean_intensity"]), obj_spec=spec)
+    total = loss + om.apply_soft_constraints(om.obj)
+    total.backward()
+    assert abs(total.item() - float(z["batch_total_loss"])) / float(z["batch_total_loss"]) < 1e-5
+    up = float(z["upsample_factor"]) ** 2 / 2
+    assert rel(om._obj.grad.cpu().numpy() * up, z["grad_obj"]) < 2e-4
+    assert rel(probe.grad.cpu().numpy(), z["grad_probe"]) < 1e-4
+
+
+@pytest.mark.parametrize("case", sorted(OBJCONS_CASES))
+def test_reconstruct_with_object_constraints_like_reference(cuda_device, case):
+    """Two Adam iterations through Ptychography.reconstruct with the constraints: loss
+    trajectory against the reference's, the object against the FP64 oracle within 3x the
+    reference's own float32 drift from it."""
+    obj_type, cons = OBJCONS_CASES[case]
+    z = load_golden(f"objcons_{case}64")
+    dev = cuda_device
+    pt = _dropin(z, dev, obj_type)
+    pt.rng = int(z["recon_rng_seed"])
+    pt.reconstruct(num_iters=int(z["iters"]), batch_size=int(z["batch"]),
+                   optimizer_params={"object": {"type": "adam"}, "probe": {"type": "adam"}},
+                   constraints={"object": dict(cons), "probe": {"orthogonalize_probe": True}}, device="gpu")
+    np.testing.assert_allclose(pt.iter_losses, z["recon_losses"], rtol=1e-4)
+    H = int(z["H"])
+    raw = z["obj_perturbed"].astype(np.complex128 if obj_type != "potential" else np.float64)
+    obj64, _, _ = O.reconstruct(
+        raw, z["probe_init"].astype(np.complex128), z["positions"].astype(np.float64),
+        z["propagators"].astype(np.complex128), z["targets"].astype(np.float64), np.ones((H, H)),
+        float(z["mean_intensity"]), float(z["upsample_factor"]), int(z["iters"]), int(z["batch"]),
+        np.random.default_rng(int(z["recon_rng_seed"])), obj_type=obj_type, obj_constraints=cons,
+        obj_mask=z["fov_mask"].astype(np.float64))
+    got = pt.obj_model._obj.detach().cpu().numpy()
+    assert rel(got, obj64) < max(3 * rel(z["recon_obj"], obj64), 1e-5)

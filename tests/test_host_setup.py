@@ -79,5 +79,20 @@ def test_unsupported_options_raise():
     with pytest.raises(ValueError, match="Object type"):
         ObjectPixelated.from_uniform(num_slices=1, obj_type="absorption")
     o = ObjectPixelated.from_uniform(num_slices=1)
-    with pytest.raises(NotImplementedError):
-        o.add_constraint("tv_weight_xy", 0.1)
+    o.add_constraint("tv_weight_xy", 0.1)  # built: TV, surface-zero, FOV mask, blur, identical slices
+    with pytest.raises(NotImplementedError, match="q_lowpass"):
+        o.add_constraint("q_lowpass", 0.5)  # the Butterworth filters are not
+    with pytest.raises(KeyError):
+        o.add_constraint("no_such_constraint", 1)
+
+
+@pytest.mark.parametrize("case", ["complex", "potential"])
+def test_fov_mask_matches_reference(case):
+    """The probe-overlap FOV mask Ptychography.preprocess builds (ptychography_base.py:
+    191-216), on the host set-up path, against the reference's own (fixtures objcons_*)."""
+    z = load_golden(f"objcons_{case}64")
+    pt = build_from_golden(z)
+    pt.probe_model._probe = torch.as_tensor(z["probe_init"]).requires_grad_(True)
+    pt._set_obj_fov_mask()
+    np.testing.assert_allclose(pt._get_probe_overlap(), z["probe_overlap"], rtol=1e-5, atol=1e-3)
+    assert np.abs(pt.obj_model.mask.numpy() - z["fov_mask"]).max() < 1e-5

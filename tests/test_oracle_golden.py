@@ -213,3 +213,52 @@ def test_oracle_descan_and_tilt_gradients_and_learning_match_reference():
     assert rel(learned["tilt"] - z["tilt"], z["recon_tilt"] - z["tilt"]) < 1e-3
     assert rel(obj, z["recon_obj"]) < 1e-4
     assert np.array_equal(z["recon_positions"], z["positions"])  # scan positions not learned
+
+
+OBJCONS_CASES = {
+    "complex": ("complex", {"gaussian_sigma": 1.0, "tv_weight_xy": 0.05, "tv_weight_z": 0.02,
+                            "surface_zero_weight": 0.01}),
+    "complexfov": ("complex", {"apply_fov_mask": True, "gaussian_sigma": 1.0}),
+    "potential": ("potential", {"fix_potential_baseline": True, "apply_fov_mask": True, "identical_slices": True,
+                                "tv_weight_xy": 0.05}),
+    "pure_phase": ("pure_phase", {"gaussian_sigma": 0.7, "identical_slices": True, "tv_weight_xy": 0.04}),
+}
+
+
+@pytest.mark.parametrize("case", sorted(OBJCONS_CASES))
+def test_oracle_object_constraints_match_reference(case):
+    """Optional object constraints (fixtures objcons_*64, made by the reference): the
+    probe-overlap FOV mask, the hard-constrained object, the soft-constraint loss, one
+    batch's total loss and raw-object / probe gradients, and 2 Adam iterations."""
+    obj_type, cons = OBJCONS_CASES[case]
+    z = load_golden(f"objcons_{case}64")
+    H = int(z["H"])
+    probe_o = O.gram_schmidt(z["probe_init"].astype(np.complex128))[0]
+    ov = O.probe_overlap(np.abs(probe_o[0]) ** 2, z["positions"].astype(np.float64), z["obj_shape"][-2:])
+    assert rel(ov, z["probe_overlap"]) < 1e-5
+    mask = O.fov_mask(ov, z["obj_padding_px"])
+    assert np.abs(mask - z["fov_mask"]).max() < 1e-5
+    raw = z["obj_perturbed"].astype(np.complex128 if obj_type != "potential" else np.float64)
+    ext = O._ext_args(cons, mask)
+    obj2 = O.constrain_object_ext(raw, obj_type, **ext)
+    assert rel(obj2, z["obj_constrained"]) < 1e-5
+    soft, _ = O.soft_constraint_loss(obj2, obj_type, cons.get("tv_weight_z", 0), cons.get("tv_weight_xy", 0),
+                                     cons.get("surface_zero_weight", 0))
+    assert abs(soft - float(z["soft_loss"])) <= 1e-5 * max(abs(float(z["soft_loss"])), 1e-3)
+    bi = z["batch_indices"]
+    props = z["propagators"].astype(np.complex128)
+    args = (props, z["targets"].astype(np.float64)[bi], np.ones((H, H)), z["positions"].shape[0],
+            float(z["mean_intensity"]), float(z["upsample_factor"]))
+    loss, g_obj, g_probe, _ = O.full_gradients(raw, z["probe_init"].astype(np.complex128),
+                                               z["positions"].astype(np.float64)[bi], *args, obj_type=obj_type,
+                                               obj_constraints=cons, obj_mask=mask)
+    assert abs(loss - float(z["batch_total_loss"])) / float(z["batch_total_loss"]) < 2e-6
+    assert rel(g_obj, z["grad_obj"]) < 5e-5
+    assert rel(g_probe, z["grad_probe"]) < 5e-6
+    obj, probe, losses = O.reconstruct(
+        raw, z["probe_init"].astype(np.complex128), z["positions"].astype(np.float64), props,
+        z["targets"].astype(np.float64), np.ones((H, H)), float(z["mean_intensity"]), float(z["upsample_factor"]),
+        int(z["iters"]), int(z["batch"]), np.random.default_rng(int(z["recon_rng_seed"])), obj_type=obj_type,
+        obj_constraints=cons, obj_mask=mask)
+    np.testing.assert_allclose(losses, z["recon_losses"], rtol=2e-5)
+    assert rel(obj, z["recon_obj"]) < 2e-4
