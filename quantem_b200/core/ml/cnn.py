@@ -639,7 +639,7 @@ class _CNNFn(torch.autograd.Function):
         run = ctx.run
         ctx.run = None
         grad = torch.zeros_like(run.net.flat.data)
-        dx = run.backward(dy.float().contiguous(), grad, ctx.needs_x)
+        dx = run.backward(dy.float().resolve_neg().contiguous(), grad, ctx.needs_x)
         return dx, grad, None, None
 
 
@@ -651,8 +651,8 @@ def mse_loss(pred: torch.Tensor, target: torch.Tensor) -> torch.Tensor:
 class _MSEFn(torch.autograd.Function):
     @staticmethod
     def forward(ctx, pred, target):
-        p = pred.float().contiguous()
-        t = target.float().contiguous()
+        p = pred.float().resolve_neg().contiguous()
+        t = target.float().resolve_neg().contiguous()
         loss = torch.empty(1, device=p.device)
         work = torch.empty(296, dtype=torch.float64, device=p.device)
         dp = torch.empty_like(p)

@@ -110,7 +110,7 @@ class _OrthogonalizeProbes(torch.autograd.Function):
     def forward(ctx, probe):
         from .. import _lib, ops
 
-        probe = probe.detach().contiguous()
+        probe = ops.dense(probe.detach())
         P = probe.shape[0]
         nn = probe[0].numel()
         lib = _lib.lib()
@@ -129,7 +129,7 @@ class _OrthogonalizeProbes(torch.autograd.Function):
         probe, work = ctx.saved_tensors
         P = probe.shape[0]
         nn = probe[0].numel()
-        g = grad_out.contiguous()
+        g = ops.dense(grad_out.to(torch.complex64))
         grad = torch.empty_like(probe)
         _lib.check(_lib.lib().ptycho_probe_orthogonalize_vjp(ops._p(probe), ops._p(g), ops._p(grad), P, nn,
                                                              ops._p(work), work.numel(), ops._stream()),

@@ -161,7 +161,7 @@ class _MultiLossFn(torch.autograd.Function):
         nd = ctx.nd
         t = ctx.saved_tensors
         objs, works, gcs, gps = t[:nd], t[nd:2 * nd], t[2 * nd:3 * nd], t[3 * nd:]
-        gout = gout.detach().to(torch.float32).contiguous()
+        gout = ops.dense(gout.detach().to(torch.float32))
         g_objs = [ops.obj_constrain_vjp(o, gc, w, scale=gout[d:d + 1]) for d, (o, gc, w) in
                   enumerate(zip(objs, gcs, works))]
         g_probes = [gp * gout[d] for d, gp in enumerate(gps)]

@@ -36,9 +36,17 @@ def _p(t):
     return None if t is None else ctypes.c_void_p(t.data_ptr())
 
 
+def dense(t: torch.Tensor) -> torch.Tensor:
+    """t with its lazy conjugate / negative bits applied and contiguous: the memory the
+    kernels read (autograd hands complex gradients in as lazy conjugate views)."""
+    return t.resolve_conj().resolve_neg().contiguous()
+
+
 def _req(t: torch.Tensor, name: str, dtype: torch.dtype, device=None):
     if not isinstance(t, torch.Tensor):
         raise TypeError(f"{name} must be a torch.Tensor")
+    if t.is_conj() or t.is_neg():
+        raise ValueError(f"{name} is a lazy conjugate / negative view; pass ops.dense({name})")
     if not t.is_cuda:
         raise RuntimeError(f"{name} must be a CUDA tensor (the B200 path has no CPU fallback)")
     if t.dtype != dtype:
@@ -112,14 +120,14 @@ def obj_constrain_vjp(obj: torch.Tensor, grad_c: torch.Tensor, work: torch.Tenso
 class _ObjConstrainFn(torch.autograd.Function):
     @staticmethod
     def forward(ctx, obj):
-        out, work = obj_constrain(obj.detach().contiguous())
+        out, work = obj_constrain(dense(obj.detach()))
         ctx.save_for_backward(obj, work)
         return out
 
     @staticmethod
     def backward(ctx, g):
         obj, work = ctx.saved_tensors
-        return obj_constrain_vjp(obj.detach().contiguous(), g.contiguous().to(torch.complex64), work)
+        return obj_constrain_vjp(dense(obj.detach()), dense(g.to(torch.complex64)), work)
 
 
 def constrained_object(obj: torch.Tensor) -> torch.Tensor:
@@ -198,7 +206,7 @@ def obj_transmission_vjp(obj: torch.Tensor, grad_t: torch.Tensor, work: torch.Te
 class _ObjTransmissionFn(torch.autograd.Function):
     @staticmethod
     def forward(ctx, obj, spec):
-        out, work = obj_transmission(obj.detach().contiguous(), spec)
+        out, work = obj_transmission(dense(obj.detach()), spec)
         ctx.spec = spec
         ctx.save_for_backward(obj, work)
         return out
@@ -206,8 +214,7 @@ class _ObjTransmissionFn(torch.autograd.Function):
     @staticmethod
     def backward(ctx, g):
         obj, work = ctx.saved_tensors
-        return obj_transmission_vjp(obj.detach().contiguous(), g.contiguous().to(torch.complex64), work,
-                                    ctx.spec), None
+        return obj_transmission_vjp(dense(obj.detach()), dense(g.to(torch.complex64)), work, ctx.spec), None
 
 
 def object_transmission(obj: torch.Tensor, spec: ObjSpec = COMPLEX_OBJECT) -> torch.Tensor:
@@ -549,15 +556,15 @@ class _BatchLossFn(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, obj_raw, probe_o, prop, positions, batch_idx, targets, mask, descan, tilt, cfg):
-        obj_raw_c = obj_raw.detach().contiguous()
-        probe_c = probe_o.detach().contiguous()
+        obj_raw_c = dense(obj_raw.detach())
+        probe_c = dense(probe_o.detach())
         spec = cfg.get("obj_spec") or COMPLEX_OBJECT
         ctx.spec = spec
         obj_c, work = obj_transmission(obj_raw_c, spec)
         ng = ctx.needs_input_grad
         need = ng[0] or ng[1] or ng[3] or ng[7] or ng[8]
         ctx.npos = int(positions.shape[0])
-        dsc = None if descan is None else descan.detach().contiguous()
+        dsc = None if descan is None else dense(descan.detach())
         dev = positions.device
         if tilt is not None:
             prop = separable_propagators_t(cfg["prop_geometry"], tilt.detach())
@@ -596,7 +603,7 @@ class _BatchLossFn(torch.autograd.Function):
     @staticmethod
     def backward(ctx, gout):
         obj_raw, work, g_obj_c, g_probe, batch_idx, g_pos, g_dsc, g_prop, tilt = ctx.saved_tensors
-        gout = gout.detach().to(torch.float32).reshape(1).contiguous()
+        gout = dense(gout.detach().to(torch.float32).reshape(1))
         ng = ctx.needs_input_grad
         g_obj = obj_transmission_vjp(obj_raw, g_obj_c, work, ctx.spec, scale=gout) if ng[0] else None
         g_pr = g_probe * gout if ng[1] else None
@@ -724,8 +731,8 @@ def gaussian_taps(sigma: float, device) -> torch.Tensor:
 class _FovConstrainFn(torch.autograd.Function):
     @staticmethod
     def forward(ctx, obj, mask, pure):
-        o = obj.detach().contiguous()
-        m = mask.detach().contiguous()
+        o = dense(obj.detach())
+        m = dense(mask.detach())
         out = torch.empty_like(o)
         work = _cwork(o.device)
         _lib.check(_lib.lib().ptycho_obj_constrain_fov(_p(o), _p(m), m.numel(), _p(out), o.numel(), int(pure),
@@ -737,7 +744,7 @@ class _FovConstrainFn(torch.autograd.Function):
     @staticmethod
     def backward(ctx, g):
         o, m = ctx.saved_tensors
-        g = g.detach().to(torch.complex64).contiguous()
+        g = dense(g.detach().to(torch.complex64))
         out = torch.empty_like(o)
         work = _cwork(o.device)
         _lib.check(_lib.lib().ptycho_obj_constrain_fov_vjp(_p(o), _p(m), m.numel(), _p(g), _p(out), o.numel(),
@@ -749,7 +756,7 @@ class _FovConstrainFn(torch.autograd.Function):
 class _PotentialBaseFn(torch.autograd.Function):
     @staticmethod
     def forward(ctx, v, bmask, amask, positivity, fix, factor):
-        v = v.detach().contiguous()
+        v = dense(v.detach())
         out = torch.empty_like(v)
         work = _cwork(v.device)
         hw = int(v.shape[-2] * v.shape[-1])
@@ -768,7 +775,7 @@ class _PotentialBaseFn(torch.autograd.Function):
         v = saved.pop(0)
         bmask = saved.pop(0) if ctx.has[0] else None
         amask = saved.pop(0) if ctx.has[1] else None
-        g = g.detach().to(torch.float32).contiguous()
+        g = dense(g.detach().to(torch.float32))
         out = torch.empty_like(v)
         work = _cwork(v.device)
         hw = int(v.shape[-2] * v.shape[-1])
@@ -781,7 +788,7 @@ class _PotentialBaseFn(torch.autograd.Function):
 class _PhaseExpFn(torch.autograd.Function):
     @staticmethod
     def forward(ctx, v):
-        v = v.detach().contiguous()
+        v = dense(v.detach())
         out = torch.empty(v.shape, dtype=torch.complex64, device=v.device)
         _lib.check(_lib.lib().ptycho_phase_exp(_p(v), _p(out), v.numel(), _stream()), "phase_exp")
         ctx.save_for_backward(v)
@@ -790,14 +797,14 @@ class _PhaseExpFn(torch.autograd.Function):
     @staticmethod
     def backward(ctx, g):
         (v,) = ctx.saved_tensors
-        g = g.detach().to(torch.complex64).contiguous()
+        g = dense(g.detach().to(torch.complex64))
         out = torch.empty_like(v)
         _lib.check(_lib.lib().ptycho_phase_exp_vjp(_p(v), _p(g), _p(out), v.numel(), _stream()), "phase_exp_vjp")
         return out
 
 
 def _blur(x: torch.Tensor, taps: torch.Tensor) -> torch.Tensor:
-    x = x.contiguous()
+    x = dense(x)
     out = torch.empty_like(x)
     tmp = torch.empty_like(x)
     S, Ho, Wo = (int(d) for d in x.shape)
@@ -826,7 +833,7 @@ class _SliceMeanFn(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, x):
-        x = x.detach().contiguous()
+        x = dense(x.detach())
         out = torch.empty_like(x)
         S = int(x.shape[0])
         _lib.check(_lib.lib().ptycho_obj_slice_mean(_p(x), _p(out), S, x[0].numel(), int(x.is_complex()),
@@ -874,7 +881,7 @@ def transmission_of(obj2: torch.Tensor) -> torch.Tensor:
 class _SoftLossFn(torch.autograd.Function):
     @staticmethod
     def forward(ctx, obj2, kind, wz, wxy, ws):
-        o = obj2.detach().contiguous()
+        o = dense(obj2.detach())
         S, Ho, Wo = (int(d) for d in o.shape)
         loss = torch.empty((), dtype=torch.float32, device=o.device)
         grad = torch.empty_like(o)

@@ -109,3 +109,19 @@ def test_extension_arguments_are_validated_without_gpu():
     sets[0].n = 128
     assert lib.ptycho_forward_adjoint_multi(sets, 1, None) == 2    # not in the multi-dataset launch
     assert "multi" in _lib.last_error()
+
+
+def test_lazy_conjugate_views_are_rejected_or_resolved():
+    """Kernels read raw memory: a lazily conjugated tensor (autograd hands complex
+    gradients in that form) is either resolved by ops.dense or refused by the argument
+    checks, never read with its conjugate bit dropped."""
+    import pytest
+    import torch
+
+    from quantem_b200 import ops
+
+    z = torch.tensor([1 + 2j, 3 - 1j], dtype=torch.complex64)
+    with pytest.raises(ValueError, match="conjugate"):
+        ops._req(z.conj(), "x", torch.complex64)
+    d = ops.dense(z.conj())
+    assert not d.is_conj() and torch.equal(d, torch.tensor([1 - 2j, 3 + 1j], dtype=torch.complex64))
