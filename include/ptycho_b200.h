@@ -192,6 +192,16 @@ int ptycho_phase_exp_vjp(const float* v, const void* grad_t, float* grad_v, int6
 int ptycho_obj_blur(const void* in, void* out, void* tmp, int S, int Ho, int Wo, int is_complex, const float* taps,
                     int ntaps, void* stream);
 
+/* Butterworth filter (object_models.py:481-520): per slice, mean removed, ifft2(fft2(x)
+ * env), mean added back (the real part for a real potential, is_real = 1); env: float32
+ * (Ho, Wo) envelope on the fftfreq grid.  The 2-D transform is a direct DFT along each
+ * axis (object sides <= 6144).  tmp: complex64 2 * S * Ho * Wo; means: complex64 2 * S.
+ * The filter is self-adjoint: the VJP is P g - mean(P g) + mean(g) per slice. */
+int ptycho_obj_butterworth(const void* in, void* out, int S, int Ho, int Wo, int is_real, const float* env, void* tmp,
+                           void* means, void* stream);
+int ptycho_obj_butterworth_vjp(const void* grad_out, void* grad_in, int S, int Ho, int Wo, int is_real,
+                               const float* env, void* tmp, void* means, void* stream);
+
 /* identical_slices (object_models.py:330-333): every slice replaced by the mean over the
  * slices (the reference averages in place under no_grad: its VJP is the identity). */
 int ptycho_obj_slice_mean(const void* in, void* out, int S, int64_t hw, int is_complex, void* stream);

@@ -287,9 +287,41 @@ def blur(x: np.ndarray, taps: np.ndarray) -> np.ndarray:
     return one(x)
 
 
+def butterworth_env(shape, sampling, q_lowpass=None, q_highpass=None, order: int = 4) -> np.ndarray:
+    """The float32 Butterworth envelope of object_models.py:495-507 on the (H, W) frequency
+    grid of the object (fftfreq with the object sampling, |q| radial)."""
+    qx = np.fft.fftfreq(int(shape[0]), float(sampling[0])).astype(np.float32)
+    qy = np.fft.fftfreq(int(shape[1]), float(sampling[1])).astype(np.float32)
+    qya, qxa = np.meshgrid(qy, qx, indexing="xy")
+    qra = np.sqrt(qxa**2 + qya**2).astype(np.float32)
+    env = np.ones_like(qra)
+    if q_highpass:
+        env = env * (1 - 1 / (1 + (qra / np.float32(q_highpass)) ** (2 * order)))
+    if q_lowpass:
+        env = env * (1 / (1 + (qra / np.float32(q_lowpass)) ** (2 * order)))
+    return env.astype(np.float32)
+
+
+def butterworth(x: np.ndarray, env: np.ndarray) -> np.ndarray:
+    """object_models.py:509-520: per slice, mean removed, ifft2(fft2(x) env), mean added
+    back; the real part for a real (potential) input."""
+    mu = x.mean(axis=(-2, -1), keepdims=True)
+    y = np.fft.ifft2(np.fft.fft2(x - mu) * env) + mu
+    return y.real if not np.iscomplexobj(x) else y
+
+
+def butterworth_vjp(g: np.ndarray, env: np.ndarray, real: bool) -> np.ndarray:
+    """VJP of ``butterworth``: the filter P = ifft2 env fft2 is self-adjoint (a real,
+    radially symmetric envelope), so g_x = P g - mean(P g) + mean(g) per slice (real part
+    for a real input)."""
+    pg = np.fft.ifft2(np.fft.fft2(g) * env)
+    out = pg - pg.mean(axis=(-2, -1), keepdims=True) + g.mean(axis=(-2, -1), keepdims=True)
+    return out.real if real else out
+
+
 def constrain_object_ext(obj: np.ndarray, obj_type: str, mask=None, positivity: bool = True,
                          fix_baseline: bool = False, baseline_factor: float = 1.0, taps=None,
-                         identical: bool = False) -> np.ndarray:
+                         identical: bool = False, butter_env=None) -> np.ndarray:
     """ObjectConstraints.apply_hard_constraints (object_models.py:289-339) with the FOV mask
     (apply_fov_mask, the mask (H, W) applied to every slice), the Gaussian blur and identical
     slices: complex / pure phase -> amp mask exp(i (angle - mean angle) mask) times the mask
@@ -320,6 +352,8 @@ def constrain_object_ext(obj: np.ndarray, obj_type: str, mask=None, positivity: 
         raise ValueError(obj_type)
     if taps is not None:
         out = blur(out, taps)
+    if butter_env is not None:
+        out = butterworth(out, butter_env)
     if identical and out.shape[0] > 1:
         out = np.broadcast_to(out.mean(axis=0, keepdims=True), out.shape).copy()
     return out
@@ -327,11 +361,13 @@ def constrain_object_ext(obj: np.ndarray, obj_type: str, mask=None, positivity: 
 
 def constrain_object_ext_vjp(obj: np.ndarray, grad_out: np.ndarray, obj_type: str, mask=None,
                              positivity: bool = True, fix_baseline: bool = False, baseline_factor: float = 1.0,
-                             taps=None, identical: bool = False) -> np.ndarray:
+                             taps=None, identical: bool = False, butter_env=None) -> np.ndarray:
     """VJP of ``constrain_object_ext`` w.r.t. the raw object (torch convention).  Identical
     slices pass the gradient straight through (the reference averages in place under
     no_grad), the blur is self-adjoint, the potential's offset is detached."""
     g = np.asarray(grad_out)
+    if butter_env is not None:
+        g = butterworth_vjp(g, butter_env, real=obj_type == "potential")
     if taps is not None:
         g = blur(g, taps)
     m = None if mask is None else np.asarray(mask, dtype=np.float64)[None]
@@ -681,19 +717,23 @@ def batch_loss_and_grads(obj_c, probe_o, positions_px, props, targets, mask, num
     return loss, g_obj, g_probe, st
 
 
-def _ext_args(obj_constraints: dict, obj_mask):
+def _ext_args(obj_constraints: dict, obj_mask, obj_shape_2d=None, sampling=None):
     c = obj_constraints
+    env = None
+    if c.get("q_lowpass") or c.get("q_highpass"):
+        env = butterworth_env(obj_shape_2d, sampling, c.get("q_lowpass"), c.get("q_highpass"),
+                              int(c.get("butterworth_order", 4)))
     return dict(mask=obj_mask if c.get("apply_fov_mask") else None, positivity=c.get("positivity", True),
                 fix_baseline=c.get("fix_potential_baseline", False),
                 baseline_factor=c.get("fix_potential_baseline_factor", 1.0),
                 taps=gaussian_taps(c["gaussian_sigma"]) if c.get("gaussian_sigma") is not None else None,
-                identical=c.get("identical_slices", False))
+                identical=c.get("identical_slices", False), butter_env=env)
 
 
 def full_gradients(obj_raw, probe_raw, positions_px, props, targets, mask, num_gpts,
                    mean_intensity, upsample_factor, orthogonalize=True,
                    loss_type="l2_amplitude", obj_type="complex", descan=None, obj_constraints=None,
-                   obj_mask=None):
+                   obj_mask=None, obj_sampling=None):
     """Loss and gradients w.r.t. the raw parameters, as Ptychography.backward
     leaves them (autograd branch, ptychography.py:326-332): the object gradient
     is scaled by upsample_factor**2 / 2.  ``obj_type``: complex, pure_phase or
@@ -704,7 +744,7 @@ def full_gradients(obj_raw, probe_raw, positions_px, props, targets, mask, num_g
     constraint (``constrain_object_ext``) and adds the soft-constraint loss, as the
     reference's batch loss does (ptychography.py:229-231)."""
     if obj_constraints is not None:
-        ext = _ext_args(obj_constraints, obj_mask)
+        ext = _ext_args(obj_constraints, obj_mask, obj_raw.shape[-2:], obj_sampling)
         obj2 = constrain_object_ext(obj_raw, obj_type, **ext)
         obj_c = np.exp(1j * obj2) if obj_type == "potential" else obj2
     else:
@@ -809,7 +849,7 @@ def gaussian_atom_phase(shape, n_atoms, sigma_px, peak_rad, rng):
 def reconstruct(obj_raw, probe_raw, positions_px, props, targets, mask, mean_intensity, upsample_factor,
                 num_iters, batch_size, rng, lr_obj=5e-3, lr_probe=1e-3, orthogonalize=True,
                 loss_type="l2_amplitude", obj_type="complex", lr_positions=None, descan=None, lr_descan=None,
-                tilt=None, prop_geometry=None, obj_constraints=None, obj_mask=None):
+                tilt=None, prop_geometry=None, obj_constraints=None, obj_mask=None, obj_sampling=None):
     """Adam iterations of Ptychography.reconstruct (ptychography.py:208-245) on
     the given state; batches from a numpy generator like SimpleBatcher.  With
     ``lr_positions`` the scan positions are a parameter too (a dataset optimiser,
@@ -838,7 +878,8 @@ def reconstruct(obj_raw, probe_raw, positions_px, props, targets, mask, mean_int
             loss, g_obj, g_probe, st = full_gradients(obj, probe, pos[bi], props, targets[bi], mask, npos,
                                                       mean_intensity, upsample_factor, orthogonalize, loss_type,
                                                       obj_type, descan=None if dsc is None else dsc[bi],
-                                                      obj_constraints=obj_constraints, obj_mask=obj_mask)
+                                                      obj_constraints=obj_constraints, obj_mask=obj_mask,
+                                                      obj_sampling=obj_sampling)
             if lr_positions is not None:
                 g_pos = np.zeros_like(pos)
                 g_pos[bi] = position_gradients(st.probe_o, st, st.g_probe_plane)

@@ -84,6 +84,8 @@ EXPORTED = (
     "ptycho_obj_blur",
     "ptycho_obj_slice_mean",
     "ptycho_obj_soft_loss",
+    "ptycho_obj_butterworth",
+    "ptycho_obj_butterworth_vjp",
 )
 
 _vp = ctypes.c_void_p
@@ -176,6 +178,8 @@ def _declare(lib):
         "ptycho_obj_blur": (_int, [_vp, _vp, _vp, _int, _int, _int, _int, _vp, _int, _vp]),
         "ptycho_obj_slice_mean": (_int, [_vp, _vp, _int, _i64, _int, _vp]),
         "ptycho_obj_soft_loss": (_int, [_vp, _int, _int, _int, _int, _flt, _flt, _flt, _vp, _int, _vp, _vp, _vp]),
+        "ptycho_obj_butterworth": (_int, [_vp, _vp, _int, _int, _int, _int, _vp, _vp, _vp, _vp]),
+        "ptycho_obj_butterworth_vjp": (_int, [_vp, _vp, _int, _int, _int, _int, _vp, _vp, _vp, _vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

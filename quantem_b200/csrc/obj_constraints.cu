@@ -465,6 +465,139 @@ __global__ void loss_from_partials_kernel(const double* __restrict__ part, float
   if (threadIdx.x == 0) *out = (float)t;
 }
 
+int check(const char* what);
+int grid_for(int64_t n);
+
+// ---------------------------------------------------------------- Butterworth filter
+// object_models.py:481-520: per slice, mean removed, ifft2(fft2(x) env), mean added back.
+// The 2-D transform is a direct DFT along the rows, a transpose, a direct DFT along the
+// (former) columns and a transpose back: O(H W (H + W)) per slice, exact for any object
+// size (no object-sized FFT is built on this path); the twiddles come from a per-line
+// table of w^j, j < n, indexed by (k c) mod n.
+
+// per-slice mean of a complex (or real, REAL) plane, one block per slice
+template <bool REAL>
+__global__ void plane_mean_kernel(const float* __restrict__ in, int64_t hw, float2* __restrict__ means) {
+  __shared__ double red[32];
+  const int s = blockIdx.x;
+  double re = 0.0, im = 0.0;
+  for (int64_t p = threadIdx.x; p < hw; p += blockDim.x) {
+    if (REAL) {
+      re += (double)in[(int64_t)s * hw + p];
+    } else {
+      const float2 v = reinterpret_cast<const float2*>(in)[(int64_t)s * hw + p];
+      re += (double)v.x;
+      im += (double)v.y;
+    }
+  }
+  const double tr = block_sum_d(re, red);
+  const double ti = block_sum_d(im, red);
+  if (threadIdx.x == 0) means[s] = make_float2((float)(tr / (double)hw), (float)(ti / (double)hw));
+}
+
+// out (complex) = in - mean of its slice
+template <bool REAL>
+__global__ void center_kernel(const float* __restrict__ in, int64_t hw, int64_t n, const float2* __restrict__ means,
+                              float2* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const float2 m = means[i / hw];
+    const float2 v = REAL ? make_float2(in[i], 0.f) : reinterpret_cast<const float2*>(in)[i];
+    out[i] = make_float2(v.x - m.x, v.y - m.y);
+  }
+}
+
+// DFT of every line of length n (lines contiguous): out[l, k] = scale sum_c x[l, c] w^(+-k c)
+template <bool INV>
+__global__ void dft_lines_kernel(const float2* __restrict__ in, float2* __restrict__ out, int n, float scale) {
+  extern __shared__ float2 sh[];
+  float2* x = sh;
+  float2* tw = sh + n;
+  const int64_t line = blockIdx.x;
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    x[j] = in[line * n + j];
+    double sn, cs;
+    sincospi((INV ? 2.0 : -2.0) * (double)j / (double)n, &sn, &cs);
+    tw[j] = make_float2((float)cs, (float)sn);
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    float ar = 0.f, ai = 0.f;
+    int idx = 0;
+    for (int c = 0; c < n; ++c) {
+      const float2 v = x[c], w = tw[idx];
+      ar = fmaf(v.x, w.x, fmaf(-v.y, w.y, ar));
+      ai = fmaf(v.x, w.y, fmaf(v.y, w.x, ai));
+      idx += k;
+      if (idx >= n) idx -= n;
+    }
+    out[line * n + k] = make_float2(ar * scale, ai * scale);
+  }
+}
+
+// (S, H, W) -> (S, W, H), 32 x 32 tiles through shared memory
+__global__ void transpose_c_kernel(const float2* __restrict__ in, float2* __restrict__ out, int H, int W) {
+  __shared__ float2 t[32][33];
+  const int64_t s = blockIdx.z;
+  const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+  for (int dy = threadIdx.y; dy < 32; dy += blockDim.y) {
+    const int r = r0 + dy, c = c0 + threadIdx.x;
+    if (r < H && c < W) t[dy][threadIdx.x] = in[(s * H + r) * W + c];
+  }
+  __syncthreads();
+  for (int dy = threadIdx.y; dy < 32; dy += blockDim.y) {
+    const int c = c0 + dy, r = r0 + threadIdx.x;
+    if (r < H && c < W) out[(s * W + c) * H + r] = t[threadIdx.x][dy];
+  }
+}
+
+// x (S, W, H) transposed spectrum *= env[kh, kw]
+__global__ void env_mul_t_kernel(float2* __restrict__ x, const float* __restrict__ env, int H, int W, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t p = i % ((int64_t)H * W);
+    const int kw = (int)(p / H), kh = (int)(p % H);
+    const float e = env[(int64_t)kh * W + kw];
+    x[i] = make_float2(x[i].x * e, x[i].y * e);
+  }
+}
+
+// out = y + add[slice] - sub[slice] (the real part for REAL): forward y + mean(x), VJP
+// y - mean(y) + mean(g)
+template <bool REAL>
+__global__ void butter_finish_kernel(const float2* __restrict__ y, int64_t hw, int64_t n,
+                                     const float2* __restrict__ add, const float2* __restrict__ sub,
+                                     float* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t s = i / hw;
+    float2 v = y[i];
+    v.x += add[s].x - (sub ? sub[s].x : 0.f);
+    v.y += add[s].y - (sub ? sub[s].y : 0.f);
+    if (REAL)
+      out[i] = v.x;
+    else
+      reinterpret_cast<float2*>(out)[i] = v;
+  }
+}
+
+// y (in a) = ifft2(env fft2(a)) of (S, H, W) complex planes; b: scratch of the same size
+int butter_core(float2* a, float2* b, int S, int H, int W, const float* env, cudaStream_t st) {
+  const size_t smw = sizeof(float2) * 2 * (size_t)W, smh = sizeof(float2) * 2 * (size_t)H;
+  cudaFuncSetAttribute(dft_lines_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)(smw > smh ? smw : smh));
+  cudaFuncSetAttribute(dft_lines_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)(smw > smh ? smw : smh));
+  const dim3 tb(32, 8);
+  const dim3 tg_hw((W + 31) / 32, (H + 31) / 32, S), tg_wh((H + 31) / 32, (W + 31) / 32, S);
+  const int64_t n = (int64_t)S * H * W;
+  dft_lines_kernel<false><<<S * H, kThreads, smw, st>>>(a, b, W, 1.0f);       // along W
+  transpose_c_kernel<<<tg_hw, tb, 0, st>>>(b, a, H, W);                     // (S, W, H)
+  dft_lines_kernel<false><<<S * W, kThreads, smh, st>>>(a, b, H, 1.0f);       // along H
+  env_mul_t_kernel<<<grid_for(n), kThreads, 0, st>>>(b, env, H, W, n);
+  dft_lines_kernel<true><<<S * W, kThreads, smh, st>>>(b, a, H, 1.0f / (float)H);
+  transpose_c_kernel<<<tg_wh, tb, 0, st>>>(a, b, W, H);                     // (S, H, W)
+  dft_lines_kernel<true><<<S * H, kThreads, smw, st>>>(b, a, W, 1.0f / (float)W);
+  return check("butterworth dft");
+}
+
 int check(const char* what) {
   const cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? PTYCHO_OK : qb_record_error(PTYCHO_ERR_CUDA, what);
@@ -595,6 +728,65 @@ int ptycho_obj_slice_mean(const void* in, void* out, int S, int64_t hw, int is_c
   slice_mean_kernel<<<grid_for(plane), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(
       static_cast<const float*>(in), static_cast<float*>(out), S, plane);
   return check("slice_mean_kernel");
+}
+
+int ptycho_obj_butterworth(const void* in, void* out, int S, int Ho, int Wo, int is_real, const float* env, void* tmp,
+                           void* means, void* stream) {
+  if (!in || !out || !env || !tmp || !means || S < 1 || Ho < 1 || Wo < 1 || Ho > 6144 || Wo > 6144)
+    return qb_record_error(PTYCHO_ERR_INVALID, "obj_butterworth: bad arguments (object sides <= 6144)");
+  if (tmp == in || tmp == out) return qb_record_error(PTYCHO_ERR_INVALID, "obj_butterworth: tmp aliases in or out");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int64_t hw = (int64_t)Ho * Wo, n = (int64_t)S * hw;
+  float2* a = static_cast<float2*>(tmp);
+  float2* b = a + n;
+  float2* mu = static_cast<float2*>(means);
+  const float* x = static_cast<const float*>(in);
+  if (is_real) {
+    plane_mean_kernel<true><<<S, kThreads, 0, st>>>(x, hw, mu);
+    center_kernel<true><<<grid_for(n), kThreads, 0, st>>>(x, hw, n, mu, a);
+  } else {
+    plane_mean_kernel<false><<<S, kThreads, 0, st>>>(x, hw, mu);
+    center_kernel<false><<<grid_for(n), kThreads, 0, st>>>(x, hw, n, mu, a);
+  }
+  int rc = butter_core(a, b, S, Ho, Wo, env, st);
+  if (rc) return rc;
+  if (is_real)
+    butter_finish_kernel<true><<<grid_for(n), kThreads, 0, st>>>(a, hw, n, mu, nullptr, static_cast<float*>(out));
+  else
+    butter_finish_kernel<false><<<grid_for(n), kThreads, 0, st>>>(a, hw, n, mu, nullptr, static_cast<float*>(out));
+  return check("butter_finish_kernel");
+}
+
+int ptycho_obj_butterworth_vjp(const void* grad_out, void* grad_in, int S, int Ho, int Wo, int is_real,
+                               const float* env, void* tmp, void* means, void* stream) {
+  if (!grad_out || !grad_in || !env || !tmp || !means || S < 1 || Ho < 1 || Wo < 1 || Ho > 6144 || Wo > 6144)
+    return qb_record_error(PTYCHO_ERR_INVALID, "obj_butterworth_vjp: bad arguments (object sides <= 6144)");
+  if (tmp == grad_out || tmp == grad_in)
+    return qb_record_error(PTYCHO_ERR_INVALID, "obj_butterworth_vjp: tmp aliases a gradient");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int64_t hw = (int64_t)Ho * Wo, n = (int64_t)S * hw;
+  float2* a = static_cast<float2*>(tmp);
+  float2* b = a + n;
+  float2* mg = static_cast<float2*>(means);  // mean of g
+  float2* my = mg + S;                      // mean of P g (zero while g is copied into a)
+  const float* g = static_cast<const float*>(grad_out);
+  if (cudaMemsetAsync(my, 0, sizeof(float2) * (size_t)S, st) != cudaSuccess)
+    return qb_record_error(PTYCHO_ERR_CUDA, "obj_butterworth_vjp: memset");
+  if (is_real) {
+    plane_mean_kernel<true><<<S, kThreads, 0, st>>>(g, hw, mg);
+    center_kernel<true><<<grid_for(n), kThreads, 0, st>>>(g, hw, n, my, a);  // my zeroed below first
+  } else {
+    plane_mean_kernel<false><<<S, kThreads, 0, st>>>(g, hw, mg);
+    center_kernel<false><<<grid_for(n), kThreads, 0, st>>>(g, hw, n, my, a);
+  }
+  int rc = butter_core(a, b, S, Ho, Wo, env, st);
+  if (rc) return rc;
+  plane_mean_kernel<false><<<S, kThreads, 0, st>>>(reinterpret_cast<const float*>(a), hw, my);
+  if (is_real)
+    butter_finish_kernel<true><<<grid_for(n), kThreads, 0, st>>>(a, hw, n, mg, my, static_cast<float*>(grad_in));
+  else
+    butter_finish_kernel<false><<<grid_for(n), kThreads, 0, st>>>(a, hw, n, mg, my, static_cast<float*>(grad_in));
+  return check("butter_finish_kernel");
 }
 
 int ptycho_obj_soft_loss(const void* obj, int S, int Ho, int Wo, int kind, float tv_weight_z, float tv_weight_xy,

@@ -24,9 +24,8 @@ class ObjectPixelated(OptimizerMixin):
         "surface_zero_weight": 0, "gaussian_sigma": None, "butterworth_order": 4, "q_lowpass": None,
         "q_highpass": None,
     }
-    # constraints whose non-default values are not built: the Butterworth filters need an
-    # object-sized 2-D FFT (object_models.py:481-520)
-    _UNSUPPORTED = ("q_lowpass", "q_highpass")
+    # every optional constraint of the reference is built for pixelated objects
+    _UNSUPPORTED = ()
     _token = object()
 
     def __init__(self, num_slices=1, slice_thicknesses=None, obj_type="complex", initialize_mode="uniform",
@@ -91,6 +90,7 @@ class ObjectPixelated(OptimizerMixin):
         slices, a potential baseline taken from the FOV mask's background)."""
         c = self._constraints
         return bool((c.get("apply_fov_mask") and self._mask is not None) or c.get("gaussian_sigma") is not None
+                    or c.get("q_lowpass") or c.get("q_highpass")
                     or (c.get("identical_slices") and self.num_slices > 1)
                     or (self._obj_type == "potential" and c.get("fix_potential_baseline")))
 
@@ -289,7 +289,8 @@ class ObjectPixelated(OptimizerMixin):
         from .. import ops
 
         if self._ext_constraints():
-            return ops.constrained_object_ext(self._obj, self._obj_type, self._constraints, self._mask_on_device())
+            return ops.constrained_object_ext(self._obj, self._obj_type, self._constraints, self._mask_on_device(),
+                                              self._sampling)
         if self._obj_type == "complex":
             return ops.constrained_object(self._obj)
         if self._obj_type == "pure_phase":

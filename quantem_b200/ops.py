@@ -827,6 +827,58 @@ class _BlurFn(torch.autograd.Function):
         return _blur(g.detach(), taps), None
 
 
+_ENV_CACHE: dict = {}
+
+
+def butterworth_env(shape, sampling, q_lowpass, q_highpass, order, device) -> torch.Tensor:
+    """The float32 Butterworth envelope (H, W) of object_models.py:495-507 (cached)."""
+    key = (tuple(int(x) for x in shape), tuple(float(x) for x in sampling), q_lowpass, q_highpass, int(order),
+           str(device))
+    env = _ENV_CACHE.get(key)
+    if env is None:
+        qx = np.fft.fftfreq(key[0][0], key[1][0]).astype(np.float32)
+        qy = np.fft.fftfreq(key[0][1], key[1][1]).astype(np.float32)
+        qya, qxa = np.meshgrid(qy, qx, indexing="xy")
+        qra = np.sqrt(qxa ** 2 + qya ** 2).astype(np.float32)
+        e = np.ones_like(qra)
+        if q_highpass:
+            e = e * (1 - 1 / (1 + (qra / np.float32(q_highpass)) ** (2 * order)))
+        if q_lowpass:
+            e = e * (1 / (1 + (qra / np.float32(q_lowpass)) ** (2 * order)))
+        env = torch.as_tensor(e.astype(np.float32), device=device).contiguous()
+        if len(_ENV_CACHE) > 16:
+            _ENV_CACHE.clear()
+        _ENV_CACHE[key] = env
+    return env
+
+
+def _butter(x: torch.Tensor, env: torch.Tensor, vjp: bool) -> torch.Tensor:
+    x = dense(x)
+    S, Ho, Wo = (int(d) for d in x.shape)
+    out = torch.empty_like(x)
+    tmp = torch.empty((2, S, Ho, Wo), dtype=torch.complex64, device=x.device)
+    means = torch.empty((2, S), dtype=torch.complex64, device=x.device)
+    fn = _lib.lib().ptycho_obj_butterworth_vjp if vjp else _lib.lib().ptycho_obj_butterworth
+    _lib.check(fn(_p(x), _p(out), S, Ho, Wo, int(not x.is_complex()), _p(env), _p(tmp), _p(means), _stream()),
+               "obj_butterworth" + ("_vjp" if vjp else ""))
+    return out
+
+
+class _ButterworthFn(torch.autograd.Function):
+    """The Butterworth filter of object_models.py:481-520 (per-slice mean kept, real part
+    for potentials); self-adjoint up to the mean handling."""
+
+    @staticmethod
+    def forward(ctx, x, env):
+        ctx.save_for_backward(env)
+        return _butter(x.detach(), env, vjp=False)
+
+    @staticmethod
+    def backward(ctx, g):
+        (env,) = ctx.saved_tensors
+        return _butter(g.detach(), env, vjp=True), None
+
+
 class _SliceMeanFn(torch.autograd.Function):
     """identical_slices: every slice replaced by the slice mean; the reference does it in
     place under no_grad, so the gradient passes straight through."""
@@ -845,12 +897,14 @@ class _SliceMeanFn(torch.autograd.Function):
         return g
 
 
-def constrained_object_ext(obj_raw: torch.Tensor, obj_type: str, constraints: dict, mask=None) -> torch.Tensor:
+def constrained_object_ext(obj_raw: torch.Tensor, obj_type: str, constraints: dict, mask=None,
+                           sampling=None) -> torch.Tensor:
     """ObjectConstraints.apply_hard_constraints (object_models.py:289-339) with the optional
     constraints: the FOV mask (``apply_fov_mask``, ``mask`` (Ho, Wo)), the potential's
-    baseline from the mask's background (``fix_potential_baseline``), ``gaussian_sigma`` and
-    ``identical_slices`` (Butterworth filters are not built).  Differentiable; returns the
-    complex object, or the real potential before exp(i V)."""
+    baseline from the mask's background (``fix_potential_baseline``), ``gaussian_sigma``, the
+    Butterworth filters (``q_lowpass`` / ``q_highpass`` with ``butterworth_order``; needs the
+    object ``sampling`` [A]) and ``identical_slices``.  Differentiable; returns the complex
+    object, or the real potential before exp(i V)."""
     c = constraints
     use_mask = bool(c.get("apply_fov_mask")) and mask is not None
     if obj_type in ("complex", "pure_phase"):
@@ -867,6 +921,12 @@ def constrained_object_ext(obj_raw: torch.Tensor, obj_type: str, constraints: di
         raise ValueError(f"unknown object type {obj_type!r}")
     if c.get("gaussian_sigma") is not None:
         out = _BlurFn.apply(out, gaussian_taps(float(c["gaussian_sigma"]), out.device))
+    if c.get("q_lowpass") or c.get("q_highpass"):
+        if sampling is None:
+            raise ValueError("the Butterworth filters need the object sampling")
+        env = butterworth_env(out.shape[-2:], sampling, c.get("q_lowpass"), c.get("q_highpass"),
+                              int(c.get("butterworth_order", 4)), out.device)
+        out = _ButterworthFn.apply(out, env)
     if c.get("identical_slices") and out.shape[0] > 1:
         out = _SliceMeanFn.apply(out)
     return out

@@ -564,6 +564,8 @@ def objconstraints_cases(seed=91):
         ("potential", "potential", {"fix_potential_baseline": True, "apply_fov_mask": True,
                                     "identical_slices": True, "tv_weight_xy": 0.05}),
         ("pure_phase", "pure_phase", {"gaussian_sigma": 0.7, "identical_slices": True, "tv_weight_xy": 0.04}),
+        ("butter_complex", "complex", {"q_lowpass": 1.5, "q_highpass": 0.05, "butterworth_order": 3}),
+        ("butter_potential", "potential", {"q_lowpass": 1.2, "gaussian_sigma": 0.8}),
     ]
     for k, (name, obj_type, cons) in enumerate(cases):
         rng = np.random.default_rng(seed + k)
@@ -610,6 +612,7 @@ def objconstraints_cases(seed=91):
                    probe_init=_c64(probe_model._probe.detach().numpy()), propagators=_c64(pt._propagators.numpy()),
                    sampling=np.asarray(pt.sampling, dtype=np.float64),
                    fov_mask=np.asarray(obj_model.mask[0].detach().numpy(), dtype=np.float32),
+                   obj_sampling=np.asarray(obj_model.sampling, dtype=np.float64),
                    probe_overlap=np.asarray(pt._get_probe_overlap(), dtype=np.float64))
         out["obj_perturbed"] = obj_model._obj.detach().numpy().copy()
         obj2 = obj_model.obj

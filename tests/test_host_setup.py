@@ -79,9 +79,8 @@ def test_unsupported_options_raise():
     with pytest.raises(ValueError, match="Object type"):
         ObjectPixelated.from_uniform(num_slices=1, obj_type="absorption")
     o = ObjectPixelated.from_uniform(num_slices=1)
-    o.add_constraint("tv_weight_xy", 0.1)  # built: TV, surface-zero, FOV mask, blur, identical slices
-    with pytest.raises(NotImplementedError, match="q_lowpass"):
-        o.add_constraint("q_lowpass", 0.5)  # the Butterworth filters are not
+    o.add_constraint("tv_weight_xy", 0.1)  # every optional constraint is built for pixelated objects
+    o.add_constraint("q_lowpass", 0.5)
     with pytest.raises(KeyError):
         o.add_constraint("no_such_constraint", 1)
 

@@ -222,6 +222,8 @@ OBJCONS_CASES = {
     "potential": ("potential", {"fix_potential_baseline": True, "apply_fov_mask": True, "identical_slices": True,
                                 "tv_weight_xy": 0.05}),
     "pure_phase": ("pure_phase", {"gaussian_sigma": 0.7, "identical_slices": True, "tv_weight_xy": 0.04}),
+    "butter_complex": ("complex", {"q_lowpass": 1.5, "q_highpass": 0.05, "butterworth_order": 3}),
+    "butter_potential": ("potential", {"q_lowpass": 1.2, "gaussian_sigma": 0.8}),
 }
 
 
@@ -239,7 +241,8 @@ def test_oracle_object_constraints_match_reference(case):
     mask = O.fov_mask(ov, z["obj_padding_px"])
     assert np.abs(mask - z["fov_mask"]).max() < 1e-5
     raw = z["obj_perturbed"].astype(np.complex128 if obj_type != "potential" else np.float64)
-    ext = O._ext_args(cons, mask)
+    smp = tuple(z["obj_sampling"])
+    ext = O._ext_args(cons, mask, raw.shape[-2:], smp)
     obj2 = O.constrain_object_ext(raw, obj_type, **ext)
     assert rel(obj2, z["obj_constrained"]) < 1e-5
     soft, _ = O.soft_constraint_loss(obj2, obj_type, cons.get("tv_weight_z", 0), cons.get("tv_weight_xy", 0),
@@ -251,7 +254,7 @@ def test_oracle_object_constraints_match_reference(case):
             float(z["mean_intensity"]), float(z["upsample_factor"]))
     loss, g_obj, g_probe, _ = O.full_gradients(raw, z["probe_init"].astype(np.complex128),
                                                z["positions"].astype(np.float64)[bi], *args, obj_type=obj_type,
-                                               obj_constraints=cons, obj_mask=mask)
+                                               obj_constraints=cons, obj_mask=mask, obj_sampling=smp)
     assert abs(loss - float(z["batch_total_loss"])) / float(z["batch_total_loss"]) < 2e-6
     assert rel(g_obj, z["grad_obj"]) < 5e-5
     assert rel(g_probe, z["grad_probe"]) < 5e-6
@@ -259,6 +262,6 @@ def test_oracle_object_constraints_match_reference(case):
         raw, z["probe_init"].astype(np.complex128), z["positions"].astype(np.float64), props,
         z["targets"].astype(np.float64), np.ones((H, H)), float(z["mean_intensity"]), float(z["upsample_factor"]),
         int(z["iters"]), int(z["batch"]), np.random.default_rng(int(z["recon_rng_seed"])), obj_type=obj_type,
-        obj_constraints=cons, obj_mask=mask)
+        obj_constraints=cons, obj_mask=mask, obj_sampling=smp)
     np.testing.assert_allclose(losses, z["recon_losses"], rtol=2e-5)
     assert rel(obj, z["recon_obj"]) < 2e-4
