@@ -682,6 +682,7 @@ int ptycho_obj_potential_base_vjp(const float* v, const float* baseline_mask, co
                                   int fix_baseline, float factor, double* work, int nwork, void* stream) {
   if (!v || !grad_out || !grad_v || !work || count < 1 || hw < 1 || count % hw || nwork < 5 * kBlocks)
     return qb_record_error(PTYCHO_ERR_INVALID, "obj_potential_base_vjp: bad arguments");
+  if (grad_v == v) return qb_record_error(PTYCHO_ERR_INVALID, "obj_potential_base_vjp: grad_v aliases v");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (fix_baseline) {
     if (baseline_mask) mask_max_kernel<<<kBlocks, kThreads, 0, st>>>(baseline_mask, hw, work);
@@ -702,6 +703,7 @@ int ptycho_phase_exp(const float* v, void* out, int64_t count, void* stream) {
 
 int ptycho_phase_exp_vjp(const float* v, const void* grad_t, float* grad_v, int64_t count, void* stream) {
   if (!v || !grad_t || !grad_v || count < 0) return qb_record_error(PTYCHO_ERR_INVALID, "phase_exp_vjp: bad arguments");
+  if (grad_v == v) return qb_record_error(PTYCHO_ERR_INVALID, "phase_exp_vjp: grad_v aliases v");
   if (count == 0) return PTYCHO_OK;
   phase_exp_vjp_kernel<<<grid_for(count), kThreads, 0, static_cast<cudaStream_t>(stream)>>>(
       v, static_cast<const float2*>(grad_t), grad_v, count);
