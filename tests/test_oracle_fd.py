@@ -199,3 +199,48 @@ def test_oracle_tilt_gradients_match_fp64_finite_differences(case):
         assert abs(fd - g[a]) <= 1e-6 * abs(g[a]) + 4 * np.finfo(np.float64).eps * abs(loss) / t, (a, fd, g[a])
     _, _, _, st0 = lossat((0.0, 0.0))
     assert np.all(O.tilt_gradients(st0, (0.0, 0.0), dz, (px, px), (H, H)) == 0.0)
+
+
+@pytest.mark.parametrize("obj_type", ["complex", "pure_phase", "potential"])
+def test_oracle_constraint_chain_vjp_matches_fp64_finite_differences(obj_type):
+    """The optional hard constraints (FOV mask, Gaussian blur, Butterworth filter; not
+    identical slices, whose gradient is straight-through by design, nor the potential's
+    fixed baseline, whose offset is detached by design, both as in the reference) and the
+    soft-constraint loss: their VJPs against central differences."""
+    import scipy.ndimage as ndi
+
+    rng = np.random.default_rng(17)
+    S, H, W = 3, 24, 20
+    m = np.zeros((H, W))
+    m[4:20, 3:17] = 1.0
+    m = ndi.gaussian_filter(m, 1.5)
+    if obj_type == "potential":
+        x = 0.05 + 0.1 * rng.standard_normal((S, H, W))
+        x = x + 0.5  # away from the positivity clamp's kink
+        cons = {"apply_fov_mask": True, "gaussian_sigma": 0.9, "q_lowpass": 1.4}
+    else:
+        x = (0.5 + 0.4 * rng.random((S, H, W))) * np.exp(0.7j * rng.standard_normal((S, H, W)))
+        cons = {"apply_fov_mask": True, "gaussian_sigma": 0.9, "q_lowpass": 1.4, "q_highpass": 0.1}
+    ext = O._ext_args(cons, m, (H, W), (0.2, 0.2))
+    cplx = np.iscomplexobj(x)
+    G = rng.standard_normal(x.shape) + (1j * rng.standard_normal(x.shape) if cplx else 0)
+
+    def L(v):
+        y = O.constrain_object_ext(v, obj_type, **ext)
+        return float(np.sum((np.conj(y) * G).real))
+
+    g = O.constrain_object_ext_vjp(x, G, obj_type, **ext)
+    d = rng.standard_normal(x.shape) + (1j * rng.standard_normal(x.shape) if cplx else 0)
+    t = 1e-6
+    fd = (L(x + t * d) - L(x - t * d)) / (2 * t)
+    adj = float(np.sum((np.conj(g) * d).real))
+    assert abs(fd - adj) <= 1e-6 * abs(adj) + 1e-8, (fd, adj)
+    # soft constraints, at an object without zero-magnitude pixels (the phase of a zero pixel
+    # has no derivative; both the kernels and the oracle give it a zero gradient there)
+    y = x if obj_type == "potential" else x * np.exp(0.3j)
+    loss, gs = O.soft_constraint_loss(y, obj_type, 0.03, 0.05, 0.02)
+    dy = rng.standard_normal(y.shape) + (1j * rng.standard_normal(y.shape) if np.iscomplexobj(y) else 0)
+    ls = lambda v: O.soft_constraint_loss(v, obj_type, 0.03, 0.05, 0.02)[0]  # noqa: E731
+    fd = (ls(y + t * dy) - ls(y - t * dy)) / (2 * t)
+    adj = float(np.sum((np.conj(gs) * dy).real))
+    assert abs(fd - adj) <= 1e-5 * abs(adj) + 1e-8, (fd, adj)
