@@ -495,17 +495,25 @@ class ObjectDIP(ObjectPixelated):
                                                device=self._model_input.device,
                                                dtype=self._model_input.dtype) * self._input_noise_std
 
-    def raw_object(self, noise: bool = True) -> torch.Tensor:
+    def raw_object(self, noise: bool = True, masked: bool = False) -> torch.Tensor:
         """The network's object as complex64 (S, H, W), differentiable: its output for a
-        complex network, exp(i output) for a real one."""
+        complex network, exp(i output) for a real one.  ``masked``: the output times the
+        probe-overlap FOV mask first, as the reference's DIP forward does whenever the mask
+        is set (object_models.py:1005-1007; Ptychography.preprocess sets it)."""
         out = self._model(self._noisy_input(noise))[0]
+        if masked and self._mask is not None:
+            m = self._mask
+            if m.device != out.device:
+                self._mask = m = m.to(out.device).contiguous()
+            out = out * m
         if self.is_complex_model:
             return out.contiguous()
         return torch.polar(torch.ones_like(out), out)
 
     @property
     def _obj(self) -> torch.Tensor:
-        return self.raw_object(noise=True)
+        """What the batch kernels take: the (noisy-input) network output, FOV-masked."""
+        return self.raw_object(noise=True, masked=True)
 
     @_obj.setter
     def _obj(self, v):  # the base constructor stores a placeholder; the network defines the object

@@ -130,3 +130,27 @@ def test_complex_dip_pretrain_and_reconstruct(cuda_device):
     assert losses.shape == (3,) and np.all(np.isfinite(losses))
     assert losses[-1] < losses[0]
     assert float((net.flat.detach() - w0).abs().max()) > 0
+
+
+def test_dip_batch_object_carries_the_fov_mask(cuda_device):
+    """The reference's DIP forward multiplies the network output by the probe-overlap FOV
+    mask whenever Ptychography.preprocess has set it (object_models.py:1005-1007); the
+    object the batch kernels take does the same, while ``obj`` stays unmasked."""
+    from quantem_b200.core.ml.cnn import CNN2d
+    from quantem_b200.diffractive_imaging import ObjectDIP, Ptychography
+
+    z = load_golden("mixed64")
+    base = build_from_golden(z, device="cuda")
+    S = base.obj_model.num_slices
+    net = CNN2d(S, S, start_filters=8, num_layers=3, device=cuda_device, seed=2)
+    dip = ObjectDIP.from_pixelated(net, base.obj_model, input_noise_std=0.0)
+    pt = Ptychography.from_models(dset=base.dset, obj_model=dip, probe_model=base.probe_model,
+                                  detector_model=base.detector_model, device="gpu", verbose=0, rng=3)
+    pt.preprocess(obj_padding_px=base.obj_padding_px)
+    m = dip.mask
+    assert m is not None and float(m.min()) < 0.5 and float(m.max()) > 0.5
+    with torch.no_grad():
+        out = net(dip._noisy_input(False))[0]
+        want = torch.polar(torch.ones_like(out), out * m.to(out.device))
+        assert torch.allclose(dip._obj, want, atol=1e-6)
+        assert not torch.allclose(dip._obj, torch.polar(torch.ones_like(out), out), atol=1e-3)
