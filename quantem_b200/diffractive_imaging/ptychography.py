@@ -554,9 +554,15 @@ class Ptychography:
                 if autograd:
                     probe_o = self.probe_model.probe
                     leaf = self.obj_model._obj  # a leaf (pixelated) or a network output (DIP)
-                    # the raw object and its transmission spec, or the transmission of the
-                    # optional constraint chain with an identity spec
-                    obj_raw, obj_spec = self.obj_model.batch_object()
+                    # the raw object and its transmission spec, or (optional / soft constraints)
+                    # the hard-constrained object computed once, its transmission taken by the
+                    # batch kernels with an identity spec and the object by the soft terms
+                    soft_obj = None
+                    if self.obj_model.has_soft_constraints:  # pixelated objects (DIP objects refuse them)
+                        soft_obj = self.obj_model.obj
+                        obj_raw, obj_spec = ops.transmission_of(soft_obj), ops.ObjSpec("complex", hard_constraint=False)
+                    else:
+                        obj_raw, obj_spec = self.obj_model.batch_object()
                     # learned descan shifts and probe tilt enter the kernels as differentiable inputs
                     descan = self.dset.batch_descan()
                     tilt = self.probe_model.probe_tilt
@@ -568,7 +574,8 @@ class Ptychography:
                     loss = closs
                     # soft constraints join the batch loss (ptychography.py:125-140, 229-231)
                     if self.obj_model.has_soft_constraints:
-                        loss = loss + self.obj_model.apply_soft_constraints(self.obj_model.obj)
+                        loss = loss + self.obj_model.apply_soft_constraints(
+                            soft_obj if soft_obj is not None else self.obj_model.obj)
                     if descan is not None and self.dset.constraints.get("descan_tv_weight", 0) > 0:
                         loss = loss + self.dset.apply_soft_constraints(descan)
                     if (obj_raw.requires_grad or self.probe_model._probe.requires_grad or pos.requires_grad
