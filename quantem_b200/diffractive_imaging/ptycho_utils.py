@@ -102,6 +102,26 @@ class SimpleBatcher:
         return int(ceil(len(self.val_indices) / self.batch_size)) if self.has_validation else 0
 
 
+def device_batches(batcher: SimpleBatcher, device):
+    """The batches of one pass of ``batcher`` (same generator calls, same boundaries) as
+    int64 index tensors on ``device``: the pass's whole order goes up in one pinned,
+    asynchronous copy, so no batch waits for a pageable host copy (which would drain the
+    stream before every batch)."""
+    batches = list(batcher)
+    if not batches:
+        return
+    order = torch.from_numpy(np.ascontiguousarray(np.concatenate(batches), dtype=np.int64))
+    dev = torch.device(device)
+    if dev.type == "cuda":
+        order = order.pin_memory().to(dev, non_blocking=True)
+    else:
+        order = order.to(dev)
+    start = 0
+    for b in batches:
+        yield order[start:start + len(b)]
+        start += len(b)
+
+
 class _OrthogonalizeProbes(torch.autograd.Function):
     """The orthogonalisation on the GPU: one ``ptycho_probe_orthogonalize`` launch
     forward, one ``ptycho_probe_orthogonalize_vjp`` launch backward."""

@@ -21,7 +21,7 @@ from .dataset_models import PtychographyDatasetRaster
 from .detector_models import DetectorPixelated
 from .object_models import ObjectPixelated
 from .probe_models import ProbePixelated
-from .ptycho_utils import SimpleBatcher
+from .ptycho_utils import SimpleBatcher, device_batches
 
 
 def adjust_padding_power2(pad, shape, power2_level):
@@ -545,12 +545,11 @@ class Ptychography:
                 if a0 + 1 < num_iters:
                     stream.prefetch_next()
             consistency = torch.zeros((), dtype=torch.float32, device=dev)
-            for bi in batcher:
+            for idx in device_batches(batcher, dev):
                 for o in opts:
                     o.zero_grad(set_to_none=True)
                 self.dset.apply_hard_constraints(self.obj_padding_px)
                 pos = self.dset.scan_positions_px.contiguous()
-                idx = torch.as_tensor(np.asarray(bi, dtype=np.int64)).to(dev, non_blocking=True)
                 if autograd:
                     probe_o = self.probe_model.probe
                     leaf = self.obj_model._obj  # a leaf (pixelated) or a network output (DIP)

@@ -10,11 +10,10 @@ from __future__ import annotations
 
 from dataclasses import dataclass, field
 
-import numpy as np
 import torch
 
 from . import ops
-from .diffractive_imaging.ptycho_utils import SimpleBatcher, orthogonalize_probes
+from .diffractive_imaging.ptycho_utils import SimpleBatcher, device_batches, orthogonalize_probes
 
 
 class FusedAdam(torch.optim.Optimizer):
@@ -128,8 +127,7 @@ def run_iteration(pt: ProblemTensors, batcher: SimpleBatcher, optimizers=(), dev
     device = pt.obj.device if device is None else device
     total = torch.zeros((), dtype=torch.float32, device=device)
     nb = 0
-    for bi in batcher:
-        idx = torch.as_tensor(np.asarray(bi, dtype=np.int64)).to(device, non_blocking=True)
+    for idx in device_batches(batcher, device):
         total += batch_step(pt, idx, optimizers)
         nb += 1
     return total / max(nb, 1)
