@@ -92,7 +92,7 @@ class ObjectPixelated(OptimizerMixin):
         return bool((c.get("apply_fov_mask") and self._mask is not None) or c.get("gaussian_sigma") is not None
                     or c.get("q_lowpass") or c.get("q_highpass")
                     or (c.get("identical_slices") and self.num_slices > 1)
-                    or (self._obj_type == "potential" and c.get("fix_potential_baseline")))
+                    or (self.obj_type == "potential" and c.get("fix_potential_baseline")))
 
     @property
     def has_soft_constraints(self) -> bool:
@@ -277,7 +277,7 @@ class ObjectPixelated(OptimizerMixin):
         if not self.has_soft_constraints:
             return torch.zeros((), device=self._obj.device)
         c = self._constraints
-        return ops.soft_constraint_loss(obj, self._obj_type, c.get("tv_weight_z", 0), c.get("tv_weight_xy", 0),
+        return ops.soft_constraint_loss(obj, self.obj_type, c.get("tv_weight_z", 0), c.get("tv_weight_xy", 0),
                                         c.get("surface_zero_weight", 0))
 
     # ------------------------------------------------------------ compute
@@ -337,9 +337,9 @@ class ObjectDIP(ObjectPixelated):
     CNN backward kernels by torch autograd; the pixelated-object gradient rescale
     (ptychography.py:330-332) is not applied, as in the reference."""
 
-    # the DIP network's output takes only the default hard constraints on this path
-    _UNSUPPORTED = ("identical_slices", "apply_fov_mask", "tv_weight_z", "tv_weight_xy", "surface_zero_weight",
-                    "gaussian_sigma", "q_lowpass", "q_highpass", "fix_potential_baseline")
+    # the optional constraints act on ``obj`` (and through it on the soft terms), as in the
+    # reference, whose DIP forward feeds the masked network output to the patches
+    _UNSUPPORTED = ()
 
     def __init__(self, num_slices=1, slice_thicknesses=None, input_noise_std=0.025, device="cuda",
                  obj_type="complex", rng=None, _token=None):
@@ -519,11 +519,29 @@ class ObjectDIP(ObjectPixelated):
     def _obj(self, v):  # the base constructor stores a placeholder; the network defines the object
         self._num_slices_dip = int(v.shape[0])
 
-    @property
-    def obj(self) -> torch.Tensor:
-        """The network's object with the hard constraint of its type (object_models.py:985-991)."""
+    def batch_object(self):
+        """The masked network output and its spec: the reference's DIP forward applies no
+        hard constraint, optional or not (object_models.py:990-1008)."""
+        return self._obj, self.transmission_spec()
+
+    def transmission(self) -> torch.Tensor:
         from .. import ops
 
+        return ops.object_transmission(self._obj, self.transmission_spec())
+
+    @property
+    def obj(self) -> torch.Tensor:
+        """The network's object with the hard constraint of its type (object_models.py:975-983),
+        the optional constraints included."""
+        from .. import ops
+
+        if self._ext_constraints():
+            x = (self._model(self._noisy_input(False))[0] if self._obj_type_dip == "potential"
+                 else self.raw_object(noise=False))
+            m = self._mask
+            if m is not None and m.device != x.device:
+                self._mask = m = m.to(x.device).contiguous()
+            return ops.constrained_object_ext(x, self._obj_type_dip, self._constraints, m, self._sampling)
         if self._obj_type_dip == "potential":
             v = self._model(self._noisy_input(False))[0]
             return torch.clamp(v, min=0.0) if self._constraints.get("positivity", True) else v

@@ -557,7 +557,7 @@ class Ptychography:
                     # the hard-constrained object computed once, its transmission taken by the
                     # batch kernels with an identity spec and the object by the soft terms
                     soft_obj = None
-                    if self.obj_model.has_soft_constraints:  # pixelated objects (DIP objects refuse them)
+                    if self.obj_model.has_soft_constraints and type(self.obj_model) is ObjectPixelated:
                         soft_obj = self.obj_model.obj
                         obj_raw, obj_spec = ops.transmission_of(soft_obj), ops.ObjSpec("complex", hard_constraint=False)
                     else:

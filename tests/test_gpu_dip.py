@@ -160,3 +160,32 @@ def test_dip_batch_object_carries_the_fov_mask(cuda_device):
         want = torch.polar(torch.ones_like(out), out * m.to(out.device))
         assert torch.allclose(dip._obj, want, atol=1e-6)
         assert not torch.allclose(dip._obj, torch.polar(torch.ones_like(out), out), atol=1e-3)
+
+
+def test_dip_optional_constraints_act_on_obj_and_soft_terms(cuda_device):
+    """On a DIP object the optional hard constraints shape ``obj`` (and the soft terms that
+    read it) while the batch path keeps the masked network output, as the reference's DIP
+    does (object_models.py:975-1008); checked against the FP64 oracle's constraint chain."""
+    from quantem_b200.core.ml.cnn import CNN2d
+    from quantem_b200.diffractive_imaging import ObjectDIP, Ptychography
+
+    z = load_golden("mixed64")
+    base = build_from_golden(z, device="cuda")
+    S = base.obj_model.num_slices
+    net = CNN2d(S, S, start_filters=8, num_layers=3, device=cuda_device, seed=5)
+    dip = ObjectDIP.from_pixelated(net, base.obj_model, input_noise_std=0.0)
+    pt = Ptychography.from_models(dset=base.dset, obj_model=dip, probe_model=base.probe_model,
+                                  detector_model=base.detector_model, device="gpu", verbose=0, rng=3)
+    pt.preprocess(obj_padding_px=base.obj_padding_px)
+    cons = {"gaussian_sigma": 1.2, "apply_fov_mask": True, "tv_weight_xy": 0.05}
+    pt.constraints = {"object": dict(cons)}
+    with torch.no_grad():
+        raw = dip.raw_object(noise=False).cpu().numpy().astype(np.complex128)
+        want = O.constrain_object_ext(raw, "pure_phase", **O._ext_args(cons, dip.mask.cpu().numpy().astype(np.float64)))
+        assert rel(dip.obj.cpu().numpy(), want) < 2e-5
+        out = net(dip._noisy_input(False))[0]
+        assert torch.allclose(dip.batch_object()[0], torch.polar(torch.ones_like(out), out * dip.mask), atol=1e-6)
+    w0 = net.flat.detach().clone()
+    pt.reconstruct(num_iters=2, optimizer_params={"object": {"type": "adam", "lr": 1e-3}}, batch_size=8)
+    assert np.all(np.isfinite(pt.iter_losses))
+    assert float((net.flat.detach() - w0).abs().max()) > 0
