@@ -181,7 +181,9 @@ def test_dip_optional_constraints_act_on_obj_and_soft_terms(cuda_device):
     pt.constraints = {"object": dict(cons)}
     with torch.no_grad():
         raw = dip.raw_object(noise=False).cpu().numpy().astype(np.complex128)
-        want = O.constrain_object_ext(raw, "pure_phase", **O._ext_args(cons, dip.mask.cpu().numpy().astype(np.float64)))
+        assert dip.obj_type == "complex"  # a real network on a complex object: exp(i output)
+        ext = O._ext_args(cons, dip.mask.cpu().numpy().astype(np.float64))
+        want = O.constrain_object_ext(raw, "complex", **ext)
         assert rel(dip.obj.cpu().numpy(), want) < 2e-5
         out = net(dip._noisy_input(False))[0]
         assert torch.allclose(dip.batch_object()[0], torch.polar(torch.ones_like(out), out * dip.mask), atol=1e-6)
