@@ -73,7 +73,8 @@ def _object_state(obj):
 
 def _probe_state(probe):
     return {"class": type(probe).__name__, "num_probes": probe.num_probes, "probe_params": dict(probe.probe_params),
-            "probe_tilt": probe.probe_tilt.detach().cpu().tolist(), "initial_probe_tilt": probe._initial_probe_tilt.tolist(),
+            "probe_tilt": probe.probe_tilt.detach().cpu().tolist(),
+            "initial_probe_tilt": probe._initial_probe_tilt.tolist(),
             "learn_probe_tilt": probe.learn_probe_tilt, "from_params": probe._from_params,
             "roi_shape": None if probe.roi_shape is None else [int(x) for x in probe.roi_shape],
             "initial_probe_weights": _cpu(probe.initial_probe_weights), "rng_seed": probe._rng_seed,
