@@ -537,7 +537,9 @@ class Ptychography:
 
         stream = HostTargetStream(tg, dev) if tg.device.type != "cuda" and num_iters > 0 else None
         self.last_h2d_bytes_per_iter = stream.bytes_per_copy if stream is not None else 0
+        nvtx = torch.cuda.nvtx  # profiler ranges (iteration, batch); no cost without a profiler
         for a0 in range(num_iters):
+            nvtx.range_push(f"reconstruct iteration {self.num_iters}")
             total = torch.zeros((), dtype=torch.float32, device=dev)
             nb = 0
             if stream is not None:
@@ -546,6 +548,7 @@ class Ptychography:
                     stream.prefetch_next()
             consistency = torch.zeros((), dtype=torch.float32, device=dev)
             for idx in device_batches(batcher, dev):
+                nvtx.range_push("batch")
                 for o in opts:
                     o.zero_grad(set_to_none=True)
                 self.dset.apply_hard_constraints(self.obj_padding_px)
@@ -608,6 +611,7 @@ class Ptychography:
                 total += loss.detach()
                 consistency += closs.detach()
                 nb += 1
+                nvtx.range_pop()
             if stream is not None:
                 stream.release()
             total_loss = float((total / max(nb, 1)).item())
@@ -634,6 +638,7 @@ class Ptychography:
             if self.logger is not None:
                 self.logger.log_iter(self.obj_model, self.probe_model, self.dset, self.num_iters - 1,
                                      consistency_loss, nb, self._get_current_lrs())
+            nvtx.range_pop()
         return self
 
     def _get_current_lrs(self):
