@@ -891,7 +891,8 @@ def run_c4(args):
                     reach[str(th)] = None if hit is None else hit[1]
                 arms[arm] = dict(time_to_nrmse_s=reach, start_nrmse=curve[0][2], best_nrmse=min(c[2] for c in curve),
                                  final_nrmse=curve[-1][2], curve=curve[:: max(1, len(curve) // 12)],
-                                 used_learned_start=(getattr(li, "used_learned", None) if arm == "learned" else None))
+                                 used_learned_start=(getattr(li, "used_learned", None) if arm == "learned" else None),
+                                 judge_scale=(getattr(li, "judge_scale", None) if arm == "learned" else None))
             key = str(thresholds[-1])  # 1.05 x the flat start's best
             tp, tl = arms["plain"]["time_to_nrmse_s"][key], arms["learned"]["time_to_nrmse_s"][key]
             arms["to_plain_best"] = {"target_nrmse": float(key), "plain_s": tp, "learned_s": tl,

@@ -224,6 +224,9 @@ class LearnedInitializer:
         s, D = self.sub, self.depth
         return out.view(D, s, s, rows_n, cols_n).permute(0, 3, 1, 4, 2).reshape(D, rows_n * s, cols_n * s)
 
+    # scalings of the predicted phase the judge compares (0 = the flat start)
+    JUDGE_SCALES = (1.0, 0.75, 0.5, 0.25, 0.0)
+
     @torch.no_grad()
     def initial_object(self, patterns: torch.Tensor, scan: tuple, obj_shape: tuple, origin_px: tuple,
                        amplitudes: bool = True, judge: dict | None = None) -> torch.Tensor:
@@ -232,8 +235,11 @@ class LearnedInitializer:
         object pixel ``origin_px``), 1 elsewhere.
 
         ``judge`` (optional dict with positions, targets, probe, prop, mask,
-        mean_intensity, batch of indices) makes the plain forward model decide:
-        the flat object is returned when its data loss is lower."""
+        mean_intensity, batch of indices) makes the plain forward model decide: its data
+        loss is evaluated for the prediction scaled by each of ``JUDGE_SCALES`` (a noisy
+        prediction of a weak object fits the data better shrunk towards zero) and the
+        best-fitting start is returned, the flat object (scale 0) included.  The chosen
+        scale is ``judge_scale``; ``used_learned`` is False when the flat start won."""
         S, Ho, Wo = obj_shape
         ph = self.predict_phase_map(patterns, scan, amplitudes)
         if ph.shape[0] not in (1, S):
@@ -244,19 +250,21 @@ class LearnedInitializer:
         full[:, r0:r0 + ph.shape[1], c0:c0 + ph.shape[2]] = ph
         if ph.shape[0] == 1:
             full = (full / S).expand(S, Ho, Wo)
-        obj = torch.exp(1j * full).to(torch.complex64).contiguous()
         self.used_learned = True
-        if judge is not None:
-            flat = torch.ones_like(obj)
-            losses = []
-            for cand in (obj, flat):
-                oc = ops.constrained_object(cand)
-                out = ops.batch_forward(oc, judge["probe"], judge["prop"], judge["positions"], judge["batch"],
-                                        judge["targets"], judge["mask"], judge["positions"].shape[0],
-                                        judge["mean_intensity"], want_intensity=False)
-                losses.append(float(out["loss"]))
-            self.judge_losses = tuple(losses)
-            if losses[0] > losses[1]:
-                self.used_learned = False
-                return flat
-        return obj
+        self.judge_scale = 1.0
+        if judge is None:
+            return torch.exp(1j * full).to(torch.complex64).contiguous()
+        losses = []
+        for a in self.JUDGE_SCALES:
+            cand = torch.exp(1j * (a * full)).to(torch.complex64).contiguous()
+            oc = ops.constrained_object(cand)
+            out = ops.batch_forward(oc, judge["probe"], judge["prop"], judge["positions"], judge["batch"],
+                                    judge["targets"], judge["mask"], judge["positions"].shape[0],
+                                    judge["mean_intensity"], want_intensity=False)
+            losses.append(out["loss"])
+        losses = [float(x) for x in torch.stack(losses).cpu()]  # one read-back for all candidates
+        self.judge_losses = tuple(losses)
+        best = min(range(len(losses)), key=lambda i: losses[i])
+        self.judge_scale = float(self.JUDGE_SCALES[best])
+        self.used_learned = self.judge_scale > 0.0
+        return torch.exp(1j * (self.judge_scale * full)).to(torch.complex64).contiguous()
