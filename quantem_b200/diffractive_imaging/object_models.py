@@ -80,6 +80,11 @@ class ObjectPixelated(OptimizerMixin):
     def obj_type(self) -> str:
         return self._obj_type
 
+    @obj_type.setter
+    def obj_type(self, t) -> None:
+        """object_models.py:105-107 (the parameter keeps its dtype until re-initialised)."""
+        self._obj_type = self._process_obj_type(t)
+
     @property
     def dtype(self):
         """float32 for potentials, complex64 otherwise (object_models.py:85-89)."""

@@ -441,6 +441,213 @@ class Ptychography:
         self.probe_model.reset_optimizer()
         self.dset.reset_optimizer()
 
+    # ------------------------------------------------------------ reference API surface
+    @property
+    def autograd(self) -> bool:
+        """ptychography.py:84-90 (``reconstruct(autograd=...)`` selects the update)."""
+        return getattr(self, "_autograd", True)
+
+    @autograd.setter
+    def autograd(self, autograd: bool) -> None:
+        self._autograd = bool(autograd)
+
+    @property
+    def iter_recon_types(self) -> np.ndarray:
+        """ptychography_base.py:403-408 (the reference records none)."""
+        return np.array(getattr(self, "_iter_recon_types", []))
+
+    @property
+    def reciprocal_units(self) -> list[str]:
+        return ["A^-1", "A^-1"]
+
+    @property
+    def angular_sampling(self) -> np.ndarray:
+        """Detector sampling in mrad (ptychography_base.py:672-694)."""
+        from .complex_probe import electron_wavelength_angstrom
+
+        sampling = np.asarray(self.dset.detector_sampling, dtype=float)
+        units = self.dset.detector_units
+        if units[0] == "mrad":
+            return sampling
+        if units[0] == "A^-1":
+            energy = self.probe_model.probe_params.get("energy")
+            if energy is None:
+                raise ValueError("dc units given in A^-1 but no energy defined to convert to mrad")
+            return sampling * electron_wavelength_angstrom(energy) * 1e3
+        if units[0] == "pixels":
+            raise ValueError("dset Q units given in pixels, needs calibration")
+        raise NotImplementedError(f"Unknown dset Q units: {units}")
+
+    @property
+    def angular_units(self) -> list[str]:
+        return ["mrad", "mrad"]
+
+    @property
+    def store_snapshots(self) -> bool:
+        return self._store_snapshots
+
+    @store_snapshots.setter
+    def store_snapshots(self, val) -> None:
+        if val is not None:
+            self._store_snapshots = bool(val)
+
+    @property
+    def store_snapshot_every(self) -> int:
+        return self._store_snapshot_every
+
+    @store_snapshot_every.setter
+    def store_snapshot_every(self, val) -> None:
+        if val is not None:
+            self._store_snapshot_every = int(val)
+
+    def get_snapshot_by_iter(self, iteration: int, closest: bool = False, cropped: bool = False) -> dict:
+        """ptychography_base.py:444-493: the snapshot at ``iteration`` (or the closest one), its
+        object optionally cropped to the field of view with the mean phase removed."""
+        if len(self._snapshots) == 0:
+            raise ValueError("No snapshots available. Use store_snapshots=True during reconstruction.")
+        iteration = int(iteration)
+        if closest:
+            snp = min(self._snapshots, key=lambda x: abs(x["iteration"] - iteration))
+        else:
+            for snp in self._snapshots:
+                if snp["iteration"] == iteration:
+                    break
+            else:
+                raise ValueError(f"No snapshot found at iteration: {iteration}, "
+                                 "to return the closest snapshot, set closest=True")
+        if cropped:
+            snp = dict(snp)
+            c = self._crop_rotate_obj_fov(snp["obj"])
+            if self.obj_type == "pure_phase":
+                ph = np.angle(c)
+                c = np.exp(1j * (ph - ph.mean()))
+            if self.obj_type in ("pure_phase", "complex"):
+                ph = np.angle(c)
+                c = np.abs(c) * np.exp(1j * (ph - ph.mean()))
+            snp["obj"] = c
+        return snp
+
+    @property
+    def obj_type(self) -> str:
+        return self.obj_model.obj_type
+
+    def set_obj_type(self, t, force: bool = False) -> None:
+        """ptychography_base.py:249-255: only before training unless forced."""
+        new = ObjectPixelated._process_obj_type(t)
+        if self.num_iters > 0 and new != self.obj_model.obj_type and not force:
+            raise ValueError("Cannot change object type after training. Run with reset=True or rerun preprocess.")
+        self.obj_model.obj_type = new
+
+    def get_probe_intensities(self, probe=None) -> np.ndarray:
+        """Relative intensities of the probe modes (ptychography_base.py:864-877)."""
+        if probe is None:
+            probe = self.probe
+        probe = probe.detach().cpu().numpy() if isinstance(probe, torch.Tensor) else np.asarray(probe)
+        if probe.ndim == 2:
+            return np.array([1.0])
+        inten = np.abs(probe) ** 2
+        return inten.sum(axis=(-2, -1)) / inten.sum()
+
+    def estimate_intensities(self, overlap_array: torch.Tensor) -> torch.Tensor:
+        """sum over modes of |orthonormal fft2(exit waves)|^2, corner-centred
+        (ptychography_base.py:963-968); exit waves (P, B, n, n) complex64 on the GPU, n one of the
+        built window sizes."""
+        ov = ops.dense(overlap_array.detach().to(torch.complex64))
+        n = int(ov.shape[-1])
+        far = ops.fft2(ov.reshape(-1, n, n), scale=1.0 / n).reshape(ov.shape)
+        return far.abs().square().sum(0)
+
+    def estimate_amplitudes(self, overlap_array: torch.Tensor, corner_centered: bool = False) -> torch.Tensor:
+        """sqrt of the mode sum of |orthonormal fft2(exit waves) + 1e-9|^2, fftshifted unless
+        ``corner_centered`` (ptychography_base.py:949-961)."""
+        ov = ops.dense(overlap_array.detach().to(torch.complex64))
+        n = int(ov.shape[-1])
+        far = ops.fft2(ov.reshape(-1, n, n), scale=1.0 / n).reshape(ov.shape)
+        amps = torch.sqrt((far + 1e-9).abs().square().sum(0))
+        return amps if corner_centered else torch.fft.fftshift(amps, dim=(-2, -1))
+
+    def error_estimate(self, pred_intensities: torch.Tensor, batch_indices, loss_type="l2_amplitude"):
+        """The consistency loss of predicted (detector-layout) intensities against the batch's
+        targets and those targets (ptychography_base.py:908-932): an analysis helper; the
+        reconstruction computes the same loss inside the fused batch kernel."""
+        dev = pred_intensities.device
+        bi = torch.as_tensor(np.asarray(batch_indices, dtype=np.int64), device=self.dset.targets.device)
+        targets = self.dset.targets[bi].to(dev)
+        mask = self.dset.detector_mask.to(dev)
+        preds = torch.sqrt(pred_intensities + 1e-9) if "amplitude" in loss_type else pred_intensities
+        diff = preds * mask - targets * mask
+        if "l1" in loss_type:
+            error = torch.sum(torch.abs(diff)) / (diff.shape[0] / self.dset.num_gpts)
+        elif "l2" in loss_type:
+            error = torch.sum(torch.abs(diff) ** 2) / (diff.shape[0] / self.dset.num_gpts)
+        elif loss_type == "poisson":
+            error = torch.sum(preds - targets * torch.log(preds + 1e-6))
+        else:
+            raise ValueError(f"Unknown loss type {loss_type}, should be 'l1' or 'l2'")
+        return error / self.dset.mean_diffraction_intensity, targets
+
+    def backward(self, loss: torch.Tensor, autograd: bool = True, *args):
+        """ptychography.py:317-348 for a loss from ``ops.batch_loss``: autograd, then the
+        pixelated-object gradient rescale; the analytic update runs inside ``reconstruct``."""
+        if not autograd:
+            raise NotImplementedError("the analytic update is fused into reconstruct(autograd=False)")
+        loss.backward()
+        leaf = self.obj_model._obj
+        if type(self.obj_model) is ObjectPixelated and leaf.grad is not None:
+            leaf.grad.mul_(self.dset.upsample_factor ** 2 / 2)
+
+    @property
+    def schedulers(self) -> dict:
+        out = {}
+        for key, m in (("object", self.obj_model), ("probe", self.probe_model), ("dataset", self.dset)):
+            if getattr(m, "scheduler", None) is not None:
+                out[key] = m.scheduler
+        return out
+
+    def remove_optimizer(self, key: str) -> None:
+        {"object": self.obj_model, "probe": self.probe_model, "dataset": self.dset}[key].remove_optimizer()
+
+    def step_optimizers(self) -> None:
+        for o in self.optimizers.values():
+            o.step()
+
+    def zero_grad_all(self) -> None:
+        for o in self.optimizers.values():
+            o.zero_grad(set_to_none=True)
+
+    def clone(self, device="cpu"):
+        """A deep copy of the reconstruction (ptychography.py:595-629), moved to ``device``."""
+        import copy
+
+        lg = self.logger
+        self.logger = None  # loggers hold writers; the reference clones them separately
+        try:
+            cloned = copy.deepcopy(self)
+        finally:
+            self.logger = lg
+        if lg is not None:
+            cloned.logger = lg.clone() if hasattr(lg, "clone") else lg
+        cloned.to(device)
+        return cloned
+
+    @classmethod
+    def from_ptychography(cls, ptycho, obj_model=None, probe_model=None, logger=None):
+        """ptychography.py:61-81: a reset clone of ``ptycho``, optionally with new models."""
+        tmp = ptycho.logger
+        ptycho.logger = None
+        try:
+            cloned = ptycho.clone(ptycho.device)
+        finally:
+            ptycho.logger = tmp
+        if obj_model is not None:
+            cloned._obj_model = obj_model
+        if probe_model is not None:
+            cloned._probe_model = probe_model
+        if logger is not None:
+            cloned.logger = logger
+        cloned.reset_recon()
+        return cloned
+
     # ------------------------------------------------------------ forward model API
     def _batch_tensors(self):
         dev = torch.device(self._device)

@@ -95,3 +95,35 @@ def test_fov_mask_matches_reference(case):
     pt._set_obj_fov_mask()
     np.testing.assert_allclose(pt._get_probe_overlap(), z["probe_overlap"], rtol=1e-5, atol=1e-3)
     assert np.abs(pt.obj_model.mask.numpy() - z["fov_mask"]).max() < 1e-5
+
+
+def test_reference_api_surface_on_the_host():
+    """Members of the reference's Ptychography that need no GPU: units, snapshots, object
+    type, probe intensities, optimiser bookkeeping, clone."""
+    z = load_golden("mixed64")
+    pt = build_from_golden(z)
+    assert pt.reciprocal_units == ["A^-1", "A^-1"] and pt.angular_units == ["mrad", "mrad"]
+    from quantem_b200.diffractive_imaging.complex_probe import electron_wavelength_angstrom
+
+    np.testing.assert_allclose(pt.angular_sampling,
+                               np.asarray(pt.dset.detector_sampling) * electron_wavelength_angstrom(float(z["energy"])) * 1e3)
+    assert pt.iter_recon_types.size == 0 and pt.autograd
+    pt.store_snapshots = True
+    pt.store_snapshot_every = 2
+    assert pt.store_snapshots and pt.store_snapshot_every == 2
+    with pytest.raises(ValueError, match="No snapshots"):
+        pt.get_snapshot_by_iter(0)
+    o = pt.obj_model._obj.detach().numpy()  # snapshot objects are host arrays
+    pt._snapshots = [dict(iteration=0, obj=o, probe=pt.probe), dict(iteration=4, obj=o, probe=pt.probe)]
+    assert pt.get_snapshot_by_iter(3, closest=True)["iteration"] == 4
+    assert pt.get_snapshot_by_iter(0, cropped=True)["obj"].shape == pt._crop_rotate_obj_fov(o).shape
+    w = pt.get_probe_intensities()
+    assert w.shape == (int(z["P"]),) and abs(w.sum() - 1) < 1e-6
+    assert pt.obj_type == "complex"
+    pt.set_obj_type("pure_phase")
+    assert pt.obj_type == "pure_phase"
+    pt.set_obj_type("complex")
+    assert pt.schedulers == {}
+    c = pt.clone()
+    assert c is not pt and c.obj_model is not pt.obj_model
+    assert torch.equal(c.obj_model._obj.detach(), pt.obj_model._obj.detach())
