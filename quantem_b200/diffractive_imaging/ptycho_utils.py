@@ -102,24 +102,27 @@ class SimpleBatcher:
         return int(ceil(len(self.val_indices) / self.batch_size)) if self.has_validation else 0
 
 
-def device_batches(batcher: SimpleBatcher, device):
+def device_batches(batcher: SimpleBatcher, device) -> list[torch.Tensor]:
     """The batches of one pass of ``batcher`` (same generator calls, same boundaries) as
     int64 index tensors on ``device``: the pass's whole order goes up in one pinned,
     asynchronous copy, so no batch waits for a pageable host copy (which would drain the
-    stream before every batch)."""
+    stream before every batch).  The copy is issued here, before the caller's loop: a pinned
+    copy runs on a copy engine, so a caller that streams other data up on a side stream
+    issues this one first, or it queues behind that transfer."""
     batches = list(batcher)
     if not batches:
-        return
+        return []
     order = torch.from_numpy(np.ascontiguousarray(np.concatenate(batches), dtype=np.int64))
     dev = torch.device(device)
     if dev.type == "cuda":
         order = order.pin_memory().to(dev, non_blocking=True)
     else:
         order = order.to(dev)
-    start = 0
+    out, start = [], 0
     for b in batches:
-        yield order[start:start + len(b)]
+        out.append(order[start:start + len(b)])
         start += len(b)
+    return out
 
 
 class _OrthogonalizeProbes(torch.autograd.Function):

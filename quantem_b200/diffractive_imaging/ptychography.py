@@ -749,12 +749,14 @@ class Ptychography:
             nvtx.range_push(f"reconstruct iteration {self.num_iters}")
             total = torch.zeros((), dtype=torch.float32, device=dev)
             nb = 0
+            # the batch order goes up before the next targets copy takes the copy engine
+            batches = device_batches(batcher, dev)
             if stream is not None:
                 tg = stream.acquire()
                 if a0 + 1 < num_iters:
                     stream.prefetch_next()
             consistency = torch.zeros((), dtype=torch.float32, device=dev)
-            for idx in device_batches(batcher, dev):
+            for idx in batches:
                 nvtx.range_push("batch")
                 for o in opts:
                     o.zero_grad(set_to_none=True)

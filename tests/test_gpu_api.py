@@ -1,0 +1,73 @@
+"""The reference's analysis members of ``Ptychography`` on the GPU: far-field intensity
+and amplitude estimates from exit waves (ptychography_base.py:949-968), the consistency
+error of predicted intensities (ptychography_base.py:908-932) and ``backward``
+(ptychography.py:317-348), against torch FP32 restatements and the fused batch kernel."""
+import numpy as np
+import pytest
+import torch
+
+from tests.conftest import load_golden, rel
+from tests.test_host_setup import build_from_golden
+
+pytestmark = pytest.mark.gpu
+
+
+def _problem(dev, case="mixed64"):
+    z = load_golden(case)
+    pt = build_from_golden(z, device="gpu")
+    pt.dset.scan_positions_px = torch.as_tensor(z["positions"])
+    pt.obj_model._obj = torch.as_tensor(z["obj_perturbed"]).to(dev).requires_grad_(True)
+    pt.probe_model._probe = torch.as_tensor(z["probe_init"]).to(dev).requires_grad_(True)
+    return z, pt
+
+
+@pytest.mark.parametrize("case", ["single64", "mixed64"])
+def test_estimates_and_error_match_the_batch_kernel(cuda_device, case):
+    z, pt = _problem(cuda_device, case)
+    batch = np.arange(0, pt.dset.num_gpts, 3)
+    _, exits = pt.forward_operator(batch_indices=batch)
+    ex = exits.detach()
+    ref = torch.fft.fft2(ex, norm="ortho")
+    inten = pt.estimate_intensities(ex)
+    assert rel(inten.cpu().numpy(), ref.abs().square().sum(0).cpu().numpy()) < 1e-5
+    amps = pt.estimate_amplitudes(ex)
+    ref_amps = torch.fft.fftshift(torch.sqrt((ref + 1e-9).abs().square().sum(0)), dim=(-2, -1))
+    assert rel(amps.cpu().numpy(), ref_amps.cpu().numpy()) < 1e-5
+    assert rel(pt.estimate_amplitudes(ex, corner_centered=True).cpu().numpy(),
+               torch.fft.ifftshift(ref_amps, dim=(-2, -1)).cpu().numpy()) < 1e-5
+    # the fused kernel's predicted intensities are in the detector layout (the reference's
+    # DetectorPixelated fftshifts the corner-centred estimate), and its batch loss is the
+    # error estimate of those intensities
+    pred, loss = pt.forward_intensities(batch)
+    det = torch.fft.fftshift(inten, dim=(-2, -1))
+    assert rel(pred.cpu().numpy(), det.cpu().numpy()) < 1e-5
+    err, targets = pt.error_estimate(det, batch)
+    assert targets.shape == det.shape
+    assert abs(float(err) - float(loss)) <= 1e-4 * abs(float(loss))
+    for lt in ("l1_amplitude", "l2_intensity", "l1_intensity", "poisson"):
+        err_lt, _ = pt.error_estimate(pred, batch, loss_type=lt)
+        _, loss_lt = pt.forward_intensities(batch, loss_type=lt)
+        assert abs(float(err_lt) - float(loss_lt)) <= 1e-4 * abs(float(loss_lt))
+
+
+def test_backward_rescales_the_pixelated_object_gradient(cuda_device):
+    from quantem_b200 import ops
+
+    z, pt = _problem(cuda_device)
+    prop, pos, tg, mask = pt._batch_tensors()
+    bi = torch.arange(0, pt.dset.num_gpts, 2, device=cuda_device)
+    obj, probe = pt.obj_model._obj, pt.probe_model._probe
+
+    def loss():
+        return ops.batch_loss(obj, probe, prop, pos, bi, tg, mask, pt.dset.num_gpts,
+                              pt.dset.mean_diffraction_intensity, "l2_amplitude")
+
+    loss().backward()
+    g_obj, g_probe = obj.grad.clone(), probe.grad.clone()
+    obj.grad = probe.grad = None
+    pt.backward(loss())
+    # the object gradient is a scatter-add whose float32 atomics land in any order
+    assert rel(obj.grad.cpu().numpy(), (g_obj * (pt.dset.upsample_factor ** 2 / 2)).cpu().numpy()) < 1e-5
+    assert rel(probe.grad.cpu().numpy(), g_probe.cpu().numpy()) < 1e-5
+    with pytest.raises(NotImplementedError):
+        pt.backward(loss(), autograd=False)
