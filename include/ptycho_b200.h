@@ -27,6 +27,10 @@
  *   ptycho_probe_orthogonalize_vjp
  *                            probe_models.py:484-525 (_probe_orthogonalization_constraint)
  *                            and its autograd
+ *   ptycho_probe_center,
+ *   ptycho_probe_center_vjp  probe_models.py:467-482 (_probe_center_of_mass_constraint)
+ *                            and its autograd
+ *   ptycho_probe_tv          probe_models.py:460-466 (_probe_tv_constraint) and its gradient
  *   ptycho_reduce_partials,
  *   ptycho_reduce_loss       deterministic reductions of per-CTA partials
  *   ptycho_adam_step,
@@ -479,6 +483,38 @@ int ptycho_probe_orthogonalize(const void* probe, void* out, int P, int64_t nn, 
  * grad_probe must not alias probe, grad_sorted or work (PTYCHO_ERR_INVALID). */
 int ptycho_probe_orthogonalize_vjp(const void* probe, const void* grad_sorted, void* grad_probe, int P, int64_t nn,
                                    void* work, int64_t work_elems, void* stream);
+
+/* ---- optional probe constraints (replace ProbeConstraints, probe_models.py:430-482) ---- */
+
+/* Complex elements of the `work` buffer of ptycho_probe_center / _vjp for P modes of n x n. */
+int64_t ptycho_probe_center_work_elems(int P, int n);
+
+/* The centre-of-mass constraint (`center_probe`, probe_models.py:467-482, with
+ * fourier_shift_expand, ptycho_utils.py:128-139): for every mode the centre of mass of
+ * |probe|^2 on the fftshifted grid minus n / 2 is computed (float64) and the mode is
+ * Fourier-shifted by minus it: out = ifft2(fft2(probe) exp(2 pi i (k_r c_r + k_c c_c))),
+ * k = fftfreq(n).  probe, out: (P, n, n) complex64, 1 <= P <= 16, n in {64, 96, 128, 256}.
+ * `work` (ptycho_probe_center_work_elems complex elements) keeps the shifted spectrum and the
+ * centres of mass for ptycho_probe_center_vjp.  out must not alias probe or work. */
+int ptycho_probe_center(const void* probe, void* out, int P, int n, void* work, int64_t work_elems, void* stream);
+
+/* grad_probe = gradient w.r.t. probe (torch convention) of a real loss whose gradient w.r.t.
+ * the centred probe is grad_out: the adjoint of the shift plus the path through the centre
+ * of mass.  `work` from the matching ptycho_probe_center call, unchanged since.  grad_probe
+ * must not alias probe or work (PTYCHO_ERR_INVALID); it may alias grad_out. */
+int ptycho_probe_center_vjp(const void* probe, const void* grad_out, void* grad_probe, int P, int n, void* work,
+                            int64_t work_elems, void* stream);
+
+/* float64 elements of the `work` buffer of ptycho_probe_tv. */
+int ptycho_probe_tv_work_elems(void);
+
+/* The probe TV soft loss (`tv_weight`, probe_models.py:460-466): loss[0] = weight x
+ * (mean |probe[..., c + 1] - probe[..., c]| + mean |probe[..., r + 1, :] - probe[..., r, :]|)
+ * over all P modes of n x n (n >= 2); with grad (nullable) its gradient, weight / (P n (n - 1))
+ * x the sum of d / |d| over the differences touching each element with the sign of its
+ * position in d (0 where d = 0).  grad must not alias probe.  Deterministic. */
+int ptycho_probe_tv(const void* probe, int P, int n, float weight, float* loss, void* grad, double* work, int nwork,
+                    void* stream);
 
 #ifdef __cplusplus
 }

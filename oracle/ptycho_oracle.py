@@ -533,6 +533,90 @@ def gram_schmidt_vjp(cache, grad_sorted: np.ndarray) -> np.ndarray:
     return g_flat.reshape(grad_sorted.shape)
 
 
+def center_probe(probe: np.ndarray):
+    """Probe centre-of-mass constraint; probe_models.py:467-482.
+
+    Per mode: the centre of mass of |psi|^2 on the fftshifted grid, minus n // 2, and the
+    mode Fourier-shifted by minus that offset (fourier_shift_expand with expand_dim=False,
+    ptycho_utils.py:128-139; the ramp's frequencies are float32 fftfreq values,
+    ptycho_utils.py:166-170).  An unshifted row y sits at (y + n // 2) mod n after the
+    fftshift.  Returns (centred probe, cache for ``center_probe_vjp``)."""
+    P, nr, nc = probe.shape
+    inten = probe.real**2 + probe.imag**2
+    wr = ((np.arange(nr) + nr // 2) % nr).astype(np.float64)
+    wc = ((np.arange(nc) + nc // 2) % nc).astype(np.float64)
+    tot = inten.sum(axis=(-2, -1))
+    com = np.stack([(inten * wr[None, :, None]).sum(axis=(-2, -1)) / tot - nr // 2,
+                    (inten * wc[None, None, :]).sum(axis=(-2, -1)) / tot - nc // 2], axis=-1)
+    kr = np.fft.fftfreq(nr).astype(np.float32).astype(np.float64)
+    kc = np.fft.fftfreq(nc).astype(np.float32).astype(np.float64)
+    # shift by -com: exp(-2 pi i (kr (-com_r) + kc (-com_c)))
+    ramp = np.exp(2j * np.pi * (kr[None, :, None] * com[:, 0, None, None] + kc[None, None, :] * com[:, 1, None, None]))
+    spec = fft2(probe) * ramp
+    cache = dict(probe=probe, spec=spec, ramp=ramp, com=com, tot=tot, wr=wr, wc=wc, kr=kr, kc=kc)
+    return ifft2(spec), cache
+
+
+def center_probe_vjp(cache, g: np.ndarray) -> np.ndarray:
+    """Reverse mode of ``center_probe`` (torch gradient convention): the adjoint of the
+    fixed shift, ifft2(fft2(g) conj(ramp)), plus the path through the centre of mass,
+    dL/dcom = Re (1/n^2) sum_k conj(fft2(g)) spec 2 pi i k and dcom/d|psi|^2 = (w - n // 2
+    - com) / sum |psi|^2, with d|psi|^2 -> 2 psi."""
+    probe, spec, ramp, com, tot, wr, wc, kr, kc = (cache[k] for k in
+                                                   ("probe", "spec", "ramp", "com", "tot", "wr", "wc", "kr", "kc"))
+    P, nr, nc = probe.shape
+    G = fft2(g)
+    g_lin = ifft2(G * np.conj(ramp))
+    cross = np.conj(G) * spec * (2j * np.pi) / (nr * nc)
+    d_com_r = (cross * kr[None, :, None]).sum(axis=(-2, -1)).real
+    d_com_c = (cross * kc[None, None, :]).sum(axis=(-2, -1)).real
+    d_inten = (d_com_r[:, None, None] * (wr[None, :, None] - nr // 2 - com[:, 0, None, None])
+               + d_com_c[:, None, None] * (wc[None, None, :] - nc // 2 - com[:, 1, None, None])) / tot[:, None, None]
+    return g_lin + 2.0 * probe * d_inten
+
+
+def probe_tv_loss(probe: np.ndarray, weight: float):
+    """Probe total-variation soft constraint; probe_models.py:460-466: weight times the sum
+    over the last two axes of mean |diff(probe)|.  Returns (loss, gradient); the gradient of
+    |d| is d / |d| and 0 where d = 0 (torch's convention)."""
+    if not weight:
+        return 0.0, np.zeros_like(probe)
+    loss, g = 0.0, np.zeros_like(probe)
+    for axis in (-1, -2):
+        d = np.diff(probe, axis=axis)
+        a = np.abs(d)
+        loss += a.mean()
+        s = np.where(a > 0, d / np.where(a > 0, a, 1.0), 0.0) / d.size
+        hi = [slice(None)] * probe.ndim
+        lo = [slice(None)] * probe.ndim
+        hi[axis], lo[axis] = slice(1, None), slice(None, -1)
+        g[tuple(hi)] += s
+        g[tuple(lo)] -= s
+    return float(weight * loss), weight * g
+
+
+def constrain_probe(probe_raw: np.ndarray, probe_constraints: dict | None = None):
+    """The probe's hard constraints in the reference's order (probe_models.py:452-458):
+    Gram-Schmidt + sort when ``orthogonalize_probe`` (default on), then the centre-of-mass
+    shift when ``center_probe``.  Returns (probe, cache for ``constrain_probe_vjp``)."""
+    c = {"orthogonalize_probe": True} if probe_constraints is None else probe_constraints
+    p, gs_cache, ctr_cache = probe_raw, None, None
+    if c.get("orthogonalize_probe", True):
+        p, _, gs_cache = gram_schmidt(p)
+    if c.get("center_probe", False):
+        p, ctr_cache = center_probe(p)
+    return p, (gs_cache, ctr_cache)
+
+
+def constrain_probe_vjp(cache, g: np.ndarray) -> np.ndarray:
+    gs_cache, ctr_cache = cache
+    if ctr_cache is not None:
+        g = center_probe_vjp(ctr_cache, g)
+    if gs_cache is not None:
+        g = gram_schmidt_vjp(gs_cache, g)
+    return g
+
+
 # ----------------------------------------------------------------------------
 # forward model and loss
 # ----------------------------------------------------------------------------
@@ -733,7 +817,7 @@ def _ext_args(obj_constraints: dict, obj_mask, obj_shape_2d=None, sampling=None)
 def full_gradients(obj_raw, probe_raw, positions_px, props, targets, mask, num_gpts,
                    mean_intensity, upsample_factor, orthogonalize=True,
                    loss_type="l2_amplitude", obj_type="complex", descan=None, obj_constraints=None,
-                   obj_mask=None, obj_sampling=None):
+                   obj_mask=None, obj_sampling=None, probe_constraints=None):
     """Loss and gradients w.r.t. the raw parameters, as Ptychography.backward
     leaves them (autograd branch, ptychography.py:326-332): the object gradient
     is scaled by upsample_factor**2 / 2.  ``obj_type``: complex, pure_phase or
@@ -742,20 +826,24 @@ def full_gradients(obj_raw, probe_raw, positions_px, props, targets, mask, num_g
     ``tilt_gradients(st, ...)`` read the returned state.  ``obj_constraints`` (a dict of the
     reference's object constraints) with ``obj_mask`` (the FOV mask) selects the full hard
     constraint (``constrain_object_ext``) and adds the soft-constraint loss, as the
-    reference's batch loss does (ptychography.py:229-231)."""
+    reference's batch loss does (ptychography.py:229-231).  ``probe_constraints`` (a dict of
+    the reference's probe constraints; replaces ``orthogonalize``) adds the centre-of-mass
+    shift and the probe TV soft loss on the hard-constrained probe (ptychography.py:134)."""
     if obj_constraints is not None:
         ext = _ext_args(obj_constraints, obj_mask, obj_raw.shape[-2:], obj_sampling)
         obj2 = constrain_object_ext(obj_raw, obj_type, **ext)
         obj_c = np.exp(1j * obj2) if obj_type == "potential" else obj2
     else:
         obj_c = object_transmission(obj_raw, obj_type)
-    if orthogonalize:
-        probe_o, _, cache = gram_schmidt(probe_raw)
-    else:
-        probe_o, cache = probe_raw, None
+    pc = {"orthogonalize_probe": bool(orthogonalize)} if probe_constraints is None else probe_constraints
+    probe_o, pcache = constrain_probe(probe_raw, pc)
     loss, g_obj_c, g_probe_o, st = batch_loss_and_grads(
         obj_c, probe_o, positions_px, props, targets, mask, num_gpts, mean_intensity, loss_type, descan)
     st.probe_o = probe_o
+    if pc.get("tv_weight", 0):
+        tv, g_tv = probe_tv_loss(probe_o, pc["tv_weight"])
+        loss = loss + tv
+        g_probe_o = g_probe_o + g_tv
     if obj_constraints is not None:
         c = obj_constraints
         g2 = phase_exp_vjp(obj2, g_obj_c) if obj_type == "potential" else g_obj_c
@@ -767,7 +855,7 @@ def full_gradients(obj_raw, probe_raw, positions_px, props, targets, mask, num_g
         g_obj = constrain_object_ext_vjp(obj_raw, g2, obj_type, **ext) * (upsample_factor**2 / 2)
     else:
         g_obj = object_transmission_vjp(obj_raw, g_obj_c, obj_type) * (upsample_factor**2 / 2)
-    g_probe = gram_schmidt_vjp(cache, g_probe_o) if orthogonalize else g_probe_o
+    g_probe = constrain_probe_vjp(pcache, g_probe_o)
     return loss, g_obj, g_probe, st
 
 
@@ -849,7 +937,8 @@ def gaussian_atom_phase(shape, n_atoms, sigma_px, peak_rad, rng):
 def reconstruct(obj_raw, probe_raw, positions_px, props, targets, mask, mean_intensity, upsample_factor,
                 num_iters, batch_size, rng, lr_obj=5e-3, lr_probe=1e-3, orthogonalize=True,
                 loss_type="l2_amplitude", obj_type="complex", lr_positions=None, descan=None, lr_descan=None,
-                tilt=None, prop_geometry=None, obj_constraints=None, obj_mask=None, obj_sampling=None):
+                tilt=None, prop_geometry=None, obj_constraints=None, obj_mask=None, obj_sampling=None,
+                probe_constraints=None):
     """Adam iterations of Ptychography.reconstruct (ptychography.py:208-245) on
     the given state; batches from a numpy generator like SimpleBatcher.  With
     ``lr_positions`` the scan positions are a parameter too (a dataset optimiser,
@@ -879,7 +968,7 @@ def reconstruct(obj_raw, probe_raw, positions_px, props, targets, mask, mean_int
                                                       mean_intensity, upsample_factor, orthogonalize, loss_type,
                                                       obj_type, descan=None if dsc is None else dsc[bi],
                                                       obj_constraints=obj_constraints, obj_mask=obj_mask,
-                                                      obj_sampling=obj_sampling)
+                                                      obj_sampling=obj_sampling, probe_constraints=probe_constraints)
             if lr_positions is not None:
                 g_pos = np.zeros_like(pos)
                 g_pos[bi] = position_gradients(st.probe_o, st, st.g_probe_plane)

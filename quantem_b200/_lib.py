@@ -73,6 +73,11 @@ EXPORTED = (
     "ptycho_probe_ortho_work_elems",
     "ptycho_probe_orthogonalize",
     "ptycho_probe_orthogonalize_vjp",
+    "ptycho_probe_center_work_elems",
+    "ptycho_probe_center",
+    "ptycho_probe_center_vjp",
+    "ptycho_probe_tv_work_elems",
+    "ptycho_probe_tv",
     "ptycho_obj_constraint_work_elems",
     "ptycho_probe_overlap",
     "ptycho_obj_constrain_fov",
@@ -166,6 +171,11 @@ def _declare(lib):
         "ptycho_probe_ortho_work_elems": (_i64, [_int, _i64]),
         "ptycho_probe_orthogonalize": (_int, [_vp, _vp, _int, _i64, _vp, _i64, _vp]),
         "ptycho_probe_orthogonalize_vjp": (_int, [_vp, _vp, _vp, _int, _i64, _vp, _i64, _vp]),
+        "ptycho_probe_center_work_elems": (_i64, [_int, _int]),
+        "ptycho_probe_center": (_int, [_vp, _vp, _int, _int, _vp, _i64, _vp]),
+        "ptycho_probe_center_vjp": (_int, [_vp, _vp, _vp, _int, _int, _vp, _i64, _vp]),
+        "ptycho_probe_tv_work_elems": (_int, []),
+        "ptycho_probe_tv": (_int, [_vp, _int, _int, _flt, _vp, _vp, _vp, _int, _vp]),
         "ptycho_obj_constraint_work_elems": (_int, []),
         "ptycho_probe_overlap": (_int, [_vp, _int, _vp, _int, _int, _int, _vp, _vp]),
         "ptycho_obj_constrain_fov": (_int, [_vp, _vp, _i64, _vp, _i64, _int, _vp, _int, _vp]),

@@ -17,7 +17,7 @@ import torch
 from ..core import config
 from ..core.optim import OptimizerMixin
 from .complex_probe import POLAR_ALIASES, POLAR_SYMBOLS, electron_wavelength_angstrom, real_space_probe
-from .ptycho_utils import orthogonalize_probes
+from .ptycho_utils import center_probe, orthogonalize_probes, probe_tv_loss
 
 
 def _standardise_aberrations(params: dict, max_order: int | None = 5) -> dict:
@@ -170,8 +170,6 @@ class ProbePixelated(OptimizerMixin):
     def add_constraint(self, key, value):
         if key not in self.DEFAULT_CONSTRAINTS:
             raise KeyError(f"Unknown probe constraint {key!r}")
-        if key in ("center_probe", "tv_weight") and value:
-            raise NotImplementedError(f"probe constraint {key}={value!r} is not part of the B200 path")
         self._constraints[key] = value
 
     @property
@@ -289,16 +287,29 @@ class ProbePixelated(OptimizerMixin):
     def reset_iter_constraint_losses(self):
         pass
 
+    @property
+    def has_soft_constraints(self) -> bool:
+        return bool(self._constraints.get("tv_weight", 0))
+
     def apply_soft_constraints(self, probe):
-        return torch.zeros((), device=self._probe.device)
+        """The probe TV soft loss on the hard-constrained probe (probe_models.py:441-450,
+        ptychography.py:134), zero when ``tv_weight`` is 0."""
+        w = float(self._constraints.get("tv_weight", 0) or 0)
+        if not w:
+            return torch.zeros((), device=self._probe.device)
+        return probe_tv_loss(probe, w)
 
     # ------------------------------------------------------------ compute
     @property
     def probe(self) -> torch.Tensor:
-        """Probe modes after the hard constraints (Gram-Schmidt + sort if enabled)."""
+        """Probe modes after the hard constraints in the reference's order (probe_models.py:
+        452-458): Gram-Schmidt + sort if enabled, then the centre-of-mass shift if enabled."""
+        p = self._probe
         if self._constraints.get("orthogonalize_probe", True):
-            return orthogonalize_probes(self._probe)
-        return self._probe
+            p = orthogonalize_probes(p)
+        if self._constraints.get("center_probe", False):
+            p = center_probe(p)
+        return p
 
     def _compute_propagator_arrays(self, sampling, num_slices, slice_thicknesses) -> torch.Tensor:
         """(S-1, H, W) complex64 propagators evaluated like probe_models.py:376-427."""

@@ -185,3 +185,103 @@ def orthogonalize_probes(start_probe: torch.Tensor) -> torch.Tensor:
     intensities = torch.sum(torch.abs(probes).square(), dim=(-2, -1))
     order = torch.argsort(intensities, descending=True)
     return torch.complex(probes.real[order], probes.imag[order])
+
+
+_CENTER_N = (64, 96, 128, 256)
+
+
+class _CenterProbe(torch.autograd.Function):
+    """The centre-of-mass shift on the GPU: ``ptycho_probe_center`` forward (centres of mass,
+    probe FFT, ramp, inverse FFT), ``ptycho_probe_center_vjp`` backward."""
+
+    @staticmethod
+    def forward(ctx, probe):
+        from .. import _lib, ops
+
+        probe = ops.dense(probe.detach())
+        P, n = probe.shape[0], probe.shape[-1]
+        lib = _lib.lib()
+        we = int(lib.ptycho_probe_center_work_elems(P, n))
+        work = torch.empty(we, dtype=torch.complex64, device=probe.device)
+        out = torch.empty_like(probe)
+        _lib.check(lib.ptycho_probe_center(ops._p(probe), ops._p(out), P, n, ops._p(work), we, ops._stream()),
+                   "probe_center")
+        ctx.save_for_backward(probe, work)
+        return out
+
+    @staticmethod
+    def backward(ctx, grad_out):
+        from .. import _lib, ops
+
+        probe, work = ctx.saved_tensors
+        P, n = probe.shape[0], probe.shape[-1]
+        g = ops.dense(grad_out.to(torch.complex64))
+        grad = torch.empty_like(probe)
+        _lib.check(_lib.lib().ptycho_probe_center_vjp(ops._p(probe), ops._p(g), ops._p(grad), P, n, ops._p(work),
+                                                      work.numel(), ops._stream()), "probe_center_vjp")
+        return grad
+
+
+def center_probe(start_probe: torch.Tensor) -> torch.Tensor:
+    """Probe centre-of-mass constraint (probe_models.py:467-482): every mode's |psi|^2 centre
+    of mass on the fftshifted grid, minus n // 2, shifted back to the origin with a Fourier
+    ramp (fourier_shift_expand, ptycho_utils.py:128-139).  Differentiable, through the centre
+    of mass too.  CUDA complex64 stacks run on the probe-centring kernels; host tensors
+    (set-up code) use the same steps as tensor ops."""
+    P, nr, nc = start_probe.shape[-3:]
+    if (start_probe.is_cuda and start_probe.dtype == torch.complex64 and 1 <= P <= 16 and nr == nc
+            and nr in _CENTER_N):
+        return _CenterProbe.apply(start_probe)
+    inten = torch.fft.fftshift(start_probe.abs().square(), dim=(-2, -1))
+    yr = torch.arange(nr, device=inten.device, dtype=inten.dtype)
+    yc = torch.arange(nc, device=inten.device, dtype=inten.dtype)
+    tot = inten.sum(dim=(-2, -1))
+    com = torch.stack([(inten * yr[:, None]).sum(dim=(-2, -1)) / tot - nr // 2,
+                       (inten * yc[None, :]).sum(dim=(-2, -1)) / tot - nc // 2], dim=-1)
+    kr = torch.as_tensor(np.fft.fftfreq(nr).astype(np.float32), device=inten.device)
+    kc = torch.as_tensor(np.fft.fftfreq(nc).astype(np.float32), device=inten.device)
+    shift = -com
+    ramp = (torch.exp(-2j * np.pi * kr[None, :, None] * shift[:, 0, None, None])
+            * torch.exp(-2j * np.pi * kc[None, None, :] * shift[:, 1, None, None])).to(start_probe.dtype)
+    return torch.fft.ifft2(torch.fft.fft2(start_probe) * ramp)
+
+
+class _ProbeTV(torch.autograd.Function):
+    """The probe TV soft loss on the GPU: one ``ptycho_probe_tv`` call computes the loss and
+    its gradient together; backward scales the gradient."""
+
+    @staticmethod
+    def forward(ctx, probe, weight):
+        from .. import _lib, ops
+
+        probe = ops.dense(probe.detach())
+        P, n = probe.shape[0], probe.shape[-1]
+        lib = _lib.lib()
+        nw = int(lib.ptycho_probe_tv_work_elems())
+        work = torch.empty(nw, dtype=torch.float64, device=probe.device)
+        loss = torch.empty((), dtype=torch.float32, device=probe.device)
+        grad = torch.empty_like(probe)
+        _lib.check(lib.ptycho_probe_tv(ops._p(probe), P, n, float(weight), ops._p(loss), ops._p(grad), ops._p(work),
+                                       nw, ops._stream()), "probe_tv")
+        ctx.save_for_backward(grad)
+        return loss
+
+    @staticmethod
+    def backward(ctx, g):
+        (grad,) = ctx.saved_tensors
+        return grad * g.to(grad.real.dtype), None
+
+
+def probe_tv_loss(probe: torch.Tensor, weight: float) -> torch.Tensor:
+    """Probe total-variation soft loss (probe_models.py:460-466): weight x (mean |diff| along
+    the last axis + mean |diff| along the second-last); CUDA complex64 stacks on the TV
+    kernel, host tensors with tensor ops."""
+    if not weight:
+        return torch.zeros((), device=probe.device)
+    P, nr, nc = probe.shape[-3:]
+    if probe.is_cuda and probe.dtype == torch.complex64 and nr == nc and nr >= 2:
+        return _ProbeTV.apply(probe, float(weight))
+    tv = torch.zeros((), device=probe.device)
+    for dim in (-1, -2):
+        tv = tv + torch.mean(torch.abs(torch.diff(probe, dim=dim)))
+    return weight * tv

@@ -787,6 +787,8 @@ class Ptychography:
                     if self.obj_model.has_soft_constraints:
                         loss = loss + self.obj_model.apply_soft_constraints(
                             soft_obj if soft_obj is not None else self.obj_model.obj)
+                    if self.probe_model.has_soft_constraints:
+                        loss = loss + self.probe_model.apply_soft_constraints(probe_o)
                     if descan is not None and self.dset.constraints.get("descan_tv_weight", 0) > 0:
                         loss = loss + self.dset.apply_soft_constraints(descan)
                     if (obj_raw.requires_grad or self.probe_model._probe.requires_grad or pos.requires_grad
@@ -806,6 +808,8 @@ class Ptychography:
                         raise NotImplementedError("learned descan shifts need autograd=True")
                     if self.obj_model._ext_constraints() or self.obj_model.has_soft_constraints:
                         raise NotImplementedError("the optional object constraints need autograd=True")
+                    if self.probe_model.has_soft_constraints or self.probe_model.constraints.get("center_probe"):
+                        raise NotImplementedError("the optional probe constraints need autograd=True")
                     with torch.no_grad():
                         probe_o = self.probe_model.probe.detach().contiguous()
                         obj_c, _ = ops.obj_constrain(self.obj_model._obj.detach().contiguous())
@@ -827,6 +831,7 @@ class Ptychography:
             # the logger receives the consistency loss alone (ptychography.py:284-292)
             consistency_loss = total_loss
             if self.logger is not None and (self.obj_model.has_soft_constraints or
+                                            self.probe_model.has_soft_constraints or
                                             self.dset.constraints.get("descan_tv_weight", 0) > 0):
                 consistency_loss = float((consistency / max(nb, 1)).item())
             ops.check_status(dev)  # out-of-range batch indices / non-finite intensities since the last check

@@ -650,6 +650,107 @@ def objconstraints_cases(seed=91):
               f"total={out['batch_total_loss']:.4g} losses={out['recon_losses']}")
 
 
+def probeconstraints_cases(seed=131):
+    """Optional probe constraints (probe_models.py:430-482): the centre-of-mass shift
+    (``center_probe``) after Gram-Schmidt and the TV soft loss (``tv_weight``), on a raw probe
+    moved off centre.  Each case records the constrained probe, the probe's soft loss, one
+    batch's loss (consistency + soft) and autograd gradients, and 2 Adam iterations."""
+    import torch
+    from quantem.core.datastructures.dataset4dstem import Dataset4dstem
+    from quantem.diffractive_imaging.complex_probe import real_space_probe
+    from quantem.diffractive_imaging.dataset_models import PtychographyDatasetRaster
+    from quantem.diffractive_imaging.detector_models import DetectorPixelated
+    from quantem.diffractive_imaging.object_models import ObjectPixelated
+    from quantem.diffractive_imaging.probe_models import ProbePixelated
+    from quantem.diffractive_imaging.ptychography import Ptychography
+
+    H, S, nscan, step_px, pad, dz, counts, batch, iters = 64, 2, 5, 6, 32, 20.0, 1e5, 10, 2
+    px, energy = 0.2, 300e3
+    rs = 1.0 / (H * px)
+    # (name, probe modes, mode weights, probe constraints, roll of the raw probe in px)
+    cases = [
+        ("centertv", 2, [0.8, 0.2], {"orthogonalize_probe": True, "center_probe": True, "tv_weight": 0.05}, (3, -2)),
+        ("center1", 1, [1.0], {"orthogonalize_probe": False, "center_probe": True, "tv_weight": 0.0}, (-4, 5)),
+        ("tv3", 3, [0.7, 0.2, 0.1], {"orthogonalize_probe": True, "center_probe": False, "tv_weight": 0.1}, (0, 0)),
+    ]
+    for k, (name, P, weights, pcons, roll) in enumerate(cases):
+        rng = np.random.default_rng(seed + k)
+        probe1 = real_space_probe(gpts=(H, H), sampling=(px, px), energy=energy, semiangle_cutoff=20.0,
+                                  aberration_coefs={"C10": -200.0}).numpy().astype(np.complex128)
+        probes = np.stack([probe1 * np.sqrt(w) * np.exp(2j * np.pi * j * np.arange(H)[None, :] / H)
+                           for j, w in enumerate(weights)])
+        obj_hw = int((nscan - 1) * step_px + 2 * pad)
+        obj_hw += (-obj_hw) % 8
+        phase = np.stack([O.gaussian_atom_phase((obj_hw, obj_hw), obj_hw * obj_hw // 400, 1.5, 0.1, rng)
+                          for _ in range(S)])
+        grid = np.stack(np.meshgrid(np.arange(nscan), np.arange(nscan), indexing="ij"), -1).reshape(-1, 2)
+        pos = grid * step_px + pad + rng.uniform(-0.5, 0.5, size=(nscan * nscan, 2))
+        props_true = O.propagators((H, H), (px, px), energy, [dz] * (S - 1))
+        data = simulate_data(np.exp(1j * phase), probes, pos, props_true, counts, rng)
+        d4 = Dataset4dstem.from_array(data.reshape(nscan, nscan, H, H), sampling=(step_px * px, step_px * px, rs, rs),
+                                      units=("A", "A", "A^-1", "A^-1"))
+        pd = PtychographyDatasetRaster.from_dataset4dstem(d4, verbose=0)
+        pd.preprocess(com_fit_function="constant", force_com_rotation=0, force_com_transpose=False,
+                      plot_rotation=False, plot_com=False, probe_energy=energy)
+        obj_model = ObjectPixelated.from_uniform(num_slices=S, slice_thicknesses=dz, obj_type="complex")
+        probe_model = ProbePixelated.from_params(
+            probe_params={"energy": energy, "defocus": 200.0, "semiangle_cutoff": 20.0},
+            num_probes=P, rng=seed + 1, initial_probe_weights=weights)
+        pt = Ptychography.from_models(dset=pd, obj_model=obj_model, probe_model=probe_model,
+                                      detector_model=DetectorPixelated(), device="cpu", verbose=0, rng=seed + 2)
+        pt.preprocess(obj_padding_px=(pad, pad))
+        constraints = {"probe": dict(pcons)}
+        pt.constraints = constraints
+        with torch.no_grad():
+            shp = tuple(obj_model._obj.shape)
+            amp = 1.0 - 0.3 * rng.random(shp)
+            ph = 0.4 * rng.standard_normal(shp)
+            obj_model._obj.data = torch.tensor(amp * np.exp(1j * ph), dtype=torch.complex64)
+            raw = probe_model._probe.detach().numpy()
+            raw = np.roll(raw, roll, axis=(-2, -1)) * np.exp(0.2j * rng.standard_normal(raw.shape))
+            probe_model._probe.data = torch.tensor(raw, dtype=torch.complex64)
+        out = dict(H=H, S=S, P=P, nscan=nscan, step_px=step_px, pad=pad, dz=dz, px=px, energy=energy, batch=batch,
+                   iters=iters, seed=seed + k, counts=counts, weights=np.asarray(weights, dtype=np.float64),
+                   probe_constraints=np.asarray(repr(pcons)), data=data,
+                   targets=_f32(pd.targets.numpy()), mean_intensity=np.float64(pd.mean_diffraction_intensity),
+                   positions=_f32(pd.scan_positions_px.detach().numpy()), obj_shape=np.asarray(pt.obj_shape_full),
+                   obj_padding_px=np.asarray(pt.obj_padding_px), upsample_factor=np.float64(pd.upsample_factor),
+                   probe_init=_c64(probe_model._probe.detach().numpy()), propagators=_c64(pt._propagators.numpy()),
+                   obj_perturbed=obj_model._obj.detach().numpy().copy())
+        probe2 = probe_model.probe
+        out["probe_constrained"] = _c64(probe2.detach().numpy())
+        out["probe_soft_loss"] = np.float64(probe_model.apply_soft_constraints(probe2).item())
+        bi = np.arange(batch)
+        obj_model._obj.grad = None
+        probe_model._probe.grad = None
+        pt.dset._set_targets("l2_amplitude")
+        pt.compute_propagator_arrays()
+        patch_indices, _pos, frac, descan = pt.dset.forward(bi, pt.obj_padding_px)
+        sp = probe_model.forward(frac)
+        op = obj_model.forward(patch_indices)
+        prop, ov = pt.forward_operator(op, sp, descan)
+        inten = pt.detector_model.forward(ov)
+        loss, tg = pt.error_estimate(inten, bi)
+        total = loss + pt._soft_constraints()
+        pt.backward(total, True, op, prop, ov, patch_indices, tg)
+        out.update(batch_indices=bi, batch_loss=np.float64(loss.item()), batch_total_loss=np.float64(total.item()),
+                   batch_intensities=_f32(inten.detach().numpy()), grad_obj=obj_model._obj.grad.numpy().copy(),
+                   grad_probe=_c64(probe_model._probe.grad.numpy()))
+        obj_model._obj.grad = None
+        probe_model._probe.grad = None
+        pt.rng = seed + 3
+        pt.reconstruct(num_iters=iters, batch_size=batch,
+                       optimizer_params={"object": {"type": "adam"}, "probe": {"type": "adam"}},
+                       constraints=constraints, device="cpu")
+        out.update(recon_obj=obj_model._obj.detach().numpy().copy(),
+                   recon_probe=_c64(probe_model._probe.detach().numpy()),
+                   recon_losses=np.asarray(pt._iter_losses, dtype=np.float64), recon_rng_seed=np.int64(seed + 3))
+        path = os.path.join(HERE, f"probecons_{name}64.npz")
+        np.savez_compressed(path, **out)
+        print(f"wrote {path}: soft={out['probe_soft_loss']:.4g} loss={out['batch_loss']:.4g} "
+              f"total={out['batch_total_loss']:.4g} losses={out['recon_losses']}")
+
+
 def whitenoise_case():
     """The reference gradient test's fixture (test_ptychography.py:19-212), restated."""
     import torch
@@ -722,6 +823,9 @@ def main(src):
         return
     if os.environ.get("GOLDEN_ONLY") == "objconstraints":
         objconstraints_cases()
+        return
+    if os.environ.get("GOLDEN_ONLY") == "probeconstraints":
+        probeconstraints_cases()
         return
     run_case("single64", H=64, S=1, P=1, nscan=6, step_px=4, pad=32, dz=20.0, counts=1e5,
              jitter=False, batch=12, iters=3, seed=11)

@@ -127,3 +127,21 @@ def test_reference_api_surface_on_the_host():
     c = pt.clone()
     assert c is not pt and c.obj_model is not pt.obj_model
     assert torch.equal(c.obj_model._obj.detach(), pt.obj_model._obj.detach())
+
+
+@pytest.mark.parametrize("case", ["centertv", "center1", "tv3"])
+def test_probe_constraints_on_the_host_match_reference(case):
+    """The probe's optional constraints on host tensors (set-up code): the centred /
+    orthogonalised probe and its TV loss against the reference's own (fixtures probecons_*64)."""
+    from quantem_b200.diffractive_imaging import ProbePixelated
+    from tests.test_oracle_golden import PROBECONS_CASES
+
+    z = load_golden(f"probecons_{case}64")
+    pm = ProbePixelated.from_params(probe_params={"energy": float(z["energy"]), "defocus": 200.0,
+                                                  "semiangle_cutoff": 20.0}, num_probes=int(z["P"]))
+    pm.constraints = PROBECONS_CASES[case]
+    pm._probe = torch.as_tensor(z["probe_init"])
+    p = pm.probe
+    assert rel(p.numpy(), z["probe_constrained"]) < 2e-5
+    soft = float(pm.apply_soft_constraints(p))
+    assert abs(soft - float(z["probe_soft_loss"])) <= 1e-5 * max(float(z["probe_soft_loss"]), 1e-3)

@@ -244,3 +244,34 @@ def test_oracle_constraint_chain_vjp_matches_fp64_finite_differences(obj_type):
     fd = (ls(y + t * dy) - ls(y - t * dy)) / (2 * t)
     adj = float(np.sum((np.conj(gs) * dy).real))
     assert abs(fd - adj) <= 1e-5 * abs(adj) + 1e-8, (fd, adj)
+
+
+@pytest.mark.parametrize("P", [1, 3])
+def test_oracle_probe_constraints_match_fp64_finite_differences(P):
+    """The probe's centre-of-mass shift (through the centre of mass itself) and its TV soft
+    loss, after Gram-Schmidt, through a random linear functional of the constrained probe:
+    Re<g, d> of the reverse chain against central differences along random directions."""
+    rng = np.random.default_rng(61 + P)
+    n = 32
+    y, x = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    base = np.exp(-(((y - 5.3) % n) ** 2 + ((x - n + 4.1) % n) ** 2) / 30.0)  # off-centre blob
+    probe = np.stack([base * np.exp(1j * 0.3 * k * x) + 0.05 * (rng.standard_normal((n, n))
+                                                                 + 1j * rng.standard_normal((n, n)))
+                      for k in range(P)])
+    w = rng.standard_normal((P, n, n)) + 1j * rng.standard_normal((P, n, n))
+    cons = {"orthogonalize_probe": True, "center_probe": True, "tv_weight": 0.07}
+
+    def loss(p):
+        c, _ = O.constrain_probe(p, cons)
+        tv, _ = O.probe_tv_loss(c, cons["tv_weight"])
+        return float(np.sum((np.conj(w) * c).real)) + tv
+
+    c, cache = O.constrain_probe(probe, cons)
+    _, g_tv = O.probe_tv_loss(c, cons["tv_weight"])
+    g = O.constrain_probe_vjp(cache, w + g_tv)
+    for _ in range(3):
+        d = rng.standard_normal(probe.shape) + 1j * rng.standard_normal(probe.shape)
+        t = 1e-6 * np.abs(probe).max() / np.abs(d).max()
+        fd = (loss(probe + t * d) - loss(probe - t * d)) / (2 * t)
+        an = float(np.sum((np.conj(g) * d).real))
+        assert abs(fd - an) <= 1e-6 * abs(an) + 1e-9

@@ -265,3 +265,42 @@ def test_oracle_object_constraints_match_reference(case):
         obj_constraints=cons, obj_mask=mask, obj_sampling=smp)
     np.testing.assert_allclose(losses, z["recon_losses"], rtol=2e-5)
     assert rel(obj, z["recon_obj"]) < 2e-4
+
+
+PROBECONS_CASES = {
+    "centertv": {"orthogonalize_probe": True, "center_probe": True, "tv_weight": 0.05},
+    "center1": {"orthogonalize_probe": False, "center_probe": True, "tv_weight": 0.0},
+    "tv3": {"orthogonalize_probe": True, "center_probe": False, "tv_weight": 0.1},
+}
+
+
+@pytest.mark.parametrize("case", sorted(PROBECONS_CASES))
+def test_oracle_probe_constraints_match_reference(case):
+    """Optional probe constraints (fixtures probecons_*64, made by the reference): the
+    centre-of-mass shifted / orthogonalised probe, the probe TV loss, one batch's total loss
+    and gradients, and 2 Adam iterations."""
+    cons = PROBECONS_CASES[case]
+    z = load_golden(f"probecons_{case}64")
+    H = int(z["H"])
+    raw_p = z["probe_init"].astype(np.complex128)
+    probe_c, _ = O.constrain_probe(raw_p, cons)
+    assert rel(probe_c, z["probe_constrained"]) < 1e-5
+    soft, _ = O.probe_tv_loss(probe_c, cons["tv_weight"])
+    assert abs(soft - float(z["probe_soft_loss"])) <= 1e-5 * max(abs(float(z["probe_soft_loss"])), 1e-3)
+    raw = z["obj_perturbed"].astype(np.complex128)
+    bi = z["batch_indices"]
+    props = z["propagators"].astype(np.complex128)
+    args = (props, z["targets"].astype(np.float64)[bi], np.ones((H, H)), z["positions"].shape[0],
+            float(z["mean_intensity"]), float(z["upsample_factor"]))
+    loss, g_obj, g_probe, _ = O.full_gradients(raw, raw_p, z["positions"].astype(np.float64)[bi], *args,
+                                               probe_constraints=cons)
+    assert abs(loss - float(z["batch_total_loss"])) / float(z["batch_total_loss"]) < 2e-6
+    assert rel(g_obj, z["grad_obj"]) < 5e-5
+    assert rel(g_probe, z["grad_probe"]) < 5e-5
+    obj, probe, losses = O.reconstruct(
+        raw, raw_p, z["positions"].astype(np.float64), props, z["targets"].astype(np.float64), np.ones((H, H)),
+        float(z["mean_intensity"]), float(z["upsample_factor"]), int(z["iters"]), int(z["batch"]),
+        np.random.default_rng(int(z["recon_rng_seed"])), probe_constraints=cons)
+    np.testing.assert_allclose(losses, z["recon_losses"], rtol=2e-5)
+    assert rel(obj, z["recon_obj"]) < 2e-4
+    assert rel(probe, z["recon_probe"]) < 2e-4
