@@ -632,10 +632,25 @@ def run_c1(args):
         loss = engine.run_iteration(pt, batcher, opts)
     e1.record()
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / iters
+    ms_eager = e0.elapsed_time(e1) / iters
+    eager_loss = float(loss)
+    # the same full-batch iteration captured in a CUDA graph and replayed (the iteration is
+    # launch-bound at this size: 256 positions of 64 x 64 on one slice)
+    git = engine.GraphedIteration(pt).capture(warmup=args.warmup)
+    torch.cuda.synchronize()
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g0.record()
+    for _ in range(iters):
+        gl = git.replay()
+    g1.record()
+    torch.cuda.synchronize()
+    ms = g0.elapsed_time(g1) / iters
     npos = pt.num_gpts
     ours = {"positions_per_s": round(npos / (ms * 1e-3), 1), "ms_per_iteration": round(ms, 4),
-            "final_loss": float(loss)}
+            "final_loss": float(gl), "graphed": True,
+            "eager": {"positions_per_s": round(npos / (ms_eager * 1e-3), 1), "ms_per_iteration": round(ms_eager, 4),
+                      "final_loss": eager_loss}}
+    del git
     ref = {name: reference_torch_gpu_subprocess(0, npos, steps=iters, warmup=args.warmup,
                                                  extra=["--workload", "c1", "--ref-device", name])
            for name in ("gpu", "cpu")}
