@@ -552,19 +552,77 @@ class Ptychography:
         """sum over modes of |orthonormal fft2(exit waves)|^2, corner-centred
         (ptychography_base.py:963-968); exit waves (P, B, n, n) complex64 on the GPU, n one of the
         built window sizes."""
-        ov = ops.dense(overlap_array.detach().to(torch.complex64))
-        n = int(ov.shape[-1])
-        far = ops.fft2(ov.reshape(-1, n, n), scale=1.0 / n).reshape(ov.shape)
-        return far.abs().square().sum(0)
+        return self._ortho_fft2(overlap_array.detach()).abs().square().sum(0)
 
     def estimate_amplitudes(self, overlap_array: torch.Tensor, corner_centered: bool = False) -> torch.Tensor:
         """sqrt of the mode sum of |orthonormal fft2(exit waves) + 1e-9|^2, fftshifted unless
         ``corner_centered`` (ptychography_base.py:949-961)."""
-        ov = ops.dense(overlap_array.detach().to(torch.complex64))
-        n = int(ov.shape[-1])
-        far = ops.fft2(ov.reshape(-1, n, n), scale=1.0 / n).reshape(ov.shape)
+        far = self._ortho_fft2(overlap_array.detach())
         amps = torch.sqrt((far + 1e-9).abs().square().sum(0))
         return amps if corner_centered else torch.fft.fftshift(amps, dim=(-2, -1))
+
+    @property
+    def obj_fov_mask(self) -> np.ndarray:
+        """The probe-overlap FOV mask (1, Ho, Wo) that preprocess builds (ptychography_base.py:
+        346-359); the object model keeps it as (Ho, Wo)."""
+        m = self.obj_model.mask
+        if m is None:
+            raise AttributeError("obj_fov_mask is set by preprocess()")
+        return m.detach().cpu().numpy()[None]
+
+    @obj_fov_mask.setter
+    def obj_fov_mask(self, mask) -> None:
+        m = np.asarray(mask.detach().cpu() if isinstance(mask, torch.Tensor) else mask, dtype=np.float32)
+        if m.ndim == 2:
+            m = m[None]
+        if m.ndim != 3:
+            raise ValueError(f"obj_fov_mask must be 2-D or 3-D, got {m.ndim} dimensions")
+        self.obj_model.mask = m
+
+    def _ortho_fft2(self, x: torch.Tensor, inverse: bool = False) -> torch.Tensor:
+        """Orthonormal (i)fft2 of a (..., n, n) complex stack on the library's FFT kernels."""
+        x = ops.dense(x.to(torch.complex64))
+        n = int(x.shape[-1])
+        return ops.fft2(x.reshape(-1, n, n), inverse=inverse, scale=1.0 / n).reshape(x.shape)
+
+    def overlap_projection(self, obj_patches: torch.Tensor, input_probe: torch.Tensor):
+        """The multislice forward of gathered patches (ptychography_base.py:934-947): the wave
+        entering each slice (S, P, B, n, n) and the exit wave (P, B, n, n), propagating with
+        ifft2(fft2(wave) prop_s) on the library's FFT kernels.  The reconstruction gathers the
+        patches and runs this chain inside the batch kernel; this is the analysis form."""
+        obj_patches = ops.dense(obj_patches.detach().to(torch.complex64))
+        probe = ops.dense(input_probe.detach().to(torch.complex64))
+        n = int(probe.shape[-1])
+        S = int(obj_patches.shape[0])
+        props = self.propagators
+        waves = [probe]
+        overlap = obj_patches[0] * probe
+        for s in range(1, S):
+            f = ops.fft2(ops.dense(overlap).reshape(-1, n, n)).reshape(overlap.shape)
+            wave = ops.fft2(ops.dense(f * props[s - 1].to(f.device)).reshape(-1, n, n), inverse=True,
+                            scale=1.0 / (n * n)).reshape(overlap.shape)
+            waves.append(wave)
+            overlap = obj_patches[s] * wave
+        return torch.stack(waves, dim=0), overlap
+
+    def fourier_projection(self, measured_amplitudes: torch.Tensor, overlap_array: torch.Tensor) -> torch.Tensor:
+        """Exit waves with their far-field amplitude replaced by the measured one (detector
+        layout in, ptychography.py:356-372): one mode keeps the far-field phase; several modes
+        scale every mode by measured / estimated amplitude (0 where the estimate is 0)."""
+        meas = torch.fft.fftshift(measured_amplitudes.to(torch.float32), dim=(-2, -1))
+        far = self._ortho_fft2(overlap_array)
+        if self.num_probes == 1:
+            mod = meas * torch.exp(1j * torch.angle(far))
+        else:
+            est = self.estimate_amplitudes(overlap_array, corner_centered=True)
+            est = torch.where(est == 0, torch.full_like(est, float("inf")), est)
+            mod = (meas / est)[None] * far
+        return self._ortho_fft2(mod, inverse=True)
+
+    def gradient_step(self, amplitudes: torch.Tensor, overlap: torch.Tensor) -> torch.Tensor:
+        """The analytic update direction of the exit waves, fourier_projection - overlap
+        (ptychography.py:350-354); ``reconstruct(autograd=False)`` computes it in-kernel."""
+        return self.fourier_projection(amplitudes, overlap) - overlap.to(torch.complex64)
 
     def error_estimate(self, pred_intensities: torch.Tensor, batch_indices, loss_type="l2_amplitude"):
         """The consistency loss of predicted (detector-layout) intensities against the batch's

@@ -71,3 +71,38 @@ def test_backward_rescales_the_pixelated_object_gradient(cuda_device):
     assert rel(probe.grad.cpu().numpy(), g_probe.cpu().numpy()) < 1e-5
     with pytest.raises(NotImplementedError):
         pt.backward(loss(), autograd=False)
+
+
+@pytest.mark.parametrize("case", ["single64", "mixed64"])
+def test_overlap_projection_and_fourier_projection(cuda_device, case):
+    """overlap_projection on gathered patches against the batch kernel's own waves and exit
+    waves; fourier_projection / gradient_step against a torch FP32 restatement of
+    ptychography.py:350-372, and a zero step where the measured amplitudes are the estimate."""
+    z, pt = _problem(cuda_device, case)
+    batch = np.arange(0, pt.dset.num_gpts, 4)
+    waves, exits = pt.forward_operator(batch_indices=batch)
+    n = int(z["H"])
+    obj_t = pt.obj_model.transmission().detach()
+    pos = pt.dset.scan_positions_px.detach().to(cuda_device)[torch.as_tensor(batch, device=cuda_device)]
+    origin = torch.round(pos).to(torch.int64)
+    fr = torch.as_tensor(np.fft.fftfreq(n, d=1.0 / n).astype(np.int64), device=cuda_device)
+    rows = (origin[:, 0, None] + fr[None]) % obj_t.shape[-2]
+    cols = (origin[:, 1, None] + fr[None]) % obj_t.shape[-1]
+    patches = obj_t[:, rows[:, :, None], cols[:, None, :]]  # (S, B, n, n)
+    got_w, got_e = pt.overlap_projection(patches, waves[0])
+    assert rel(got_w.cpu().numpy(), waves.cpu().numpy()) < 1e-5
+    assert rel(got_e.cpu().numpy(), exits.cpu().numpy()) < 1e-5
+    amps = pt.dset.targets[torch.as_tensor(batch, device=pt.dset.targets.device)].to(cuda_device)
+    proj = pt.fourier_projection(amps, exits)
+    meas = torch.fft.fftshift(amps, dim=(-2, -1))
+    far = torch.fft.fft2(exits, norm="ortho")
+    if exits.shape[0] == 1:
+        ref = torch.fft.ifft2(meas * torch.exp(1j * torch.angle(far)), norm="ortho")
+    else:
+        est = torch.sqrt((far + 1e-9).abs().square().sum(0))
+        est[est == 0] = torch.inf
+        ref = torch.fft.ifft2((meas / est)[None] * far, norm="ortho")
+    assert rel(proj.cpu().numpy(), ref.cpu().numpy()) < 1e-5
+    assert rel(pt.gradient_step(amps, exits).cpu().numpy(), (ref - exits).cpu().numpy()) < 1e-4
+    step = pt.gradient_step(pt.estimate_amplitudes(exits), exits)
+    assert float(step.abs().square().sum().sqrt()) < 1e-4 * float(exits.abs().square().sum().sqrt())

@@ -124,6 +124,10 @@ def test_reference_api_surface_on_the_host():
     assert pt.obj_type == "pure_phase"
     pt.set_obj_type("complex")
     assert pt.schedulers == {}
+    m = pt.obj_fov_mask
+    assert m.shape == (1, *tuple(pt.obj_shape_full[-2:]))
+    pt.obj_fov_mask = 0.5 * m[0]
+    np.testing.assert_array_equal(pt.obj_fov_mask, 0.5 * m)
     c = pt.clone()
     assert c is not pt and c.obj_model is not pt.obj_model
     assert torch.equal(c.obj_model._obj.detach(), pt.obj_model._obj.detach())
