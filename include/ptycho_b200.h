@@ -466,6 +466,14 @@ int ptycho_pattern_shift_ramp(void* spectra, const double* shifts, int npos, int
 int ptycho_pattern_center(const void* shifted, int npos, int n, float scale, float* centered_amplitudes,
                           float* centered_intensities, void* stream);
 
+/* The bilinear form of the same centring (`preprocess(bilinear=True)`, shift_array with
+ * bilinear=True, ptycho_utils.py:273-284): amplitudes (npos, n, n) float32 rolled by
+ * floor(shift) and blended with the next pixel by the fractional parts, periodic, in float64,
+ * then centred amplitudes = fftshift(max(., 0)) and (nullable) their squares; shifts (2, npos)
+ * = (rs, cs) as for ptycho_pattern_shift_ramp, n even.  Outputs must not alias the input. */
+int ptycho_pattern_bilinear(const float* amplitudes, const double* shifts, int npos, int n,
+                            float* centered_amplitudes, float* centered_intensities, void* stream);
+
 /* ---- probe-mode orthogonalisation (ProbePixelated._probe_orthogonalization_constraint,
  * probe_models.py:484-525): modified Gram-Schmidt with the running vector, every mode
  * rescaled to its original norm, modes sorted by descending intensity; one CTA. ---- */

@@ -70,6 +70,7 @@ EXPORTED = (
     "ptycho_pattern_prepare",
     "ptycho_pattern_shift_ramp",
     "ptycho_pattern_center",
+    "ptycho_pattern_bilinear",
     "ptycho_probe_ortho_work_elems",
     "ptycho_probe_orthogonalize",
     "ptycho_probe_orthogonalize_vjp",
@@ -168,6 +169,7 @@ def _declare(lib):
         "ptycho_pattern_prepare": (_int, [_vp, _i64, _vp, _vp, _vp, _vp, _i64, _vp, _vp]),
         "ptycho_pattern_shift_ramp": (_int, [_vp, _vp, _int, _int, _vp]),
         "ptycho_pattern_center": (_int, [_vp, _int, _int, _flt, _vp, _vp, _vp]),
+        "ptycho_pattern_bilinear": (_int, [_vp, _vp, _int, _int, _vp, _vp, _vp]),
         "ptycho_probe_ortho_work_elems": (_i64, [_int, _i64]),
         "ptycho_probe_orthogonalize": (_int, [_vp, _vp, _int, _i64, _vp, _i64, _vp]),
         "ptycho_probe_orthogonalize_vjp": (_int, [_vp, _vp, _vp, _int, _i64, _vp, _i64, _vp]),

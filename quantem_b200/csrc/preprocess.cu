@@ -146,6 +146,37 @@ __global__ void pattern_center_kernel(const float2* __restrict__ sh, int npos, i
   }
 }
 
+// Bilinear centring (ptycho_utils.py:273-284 with dataset_models.py:1427-1435): the
+// amplitude rolled by floor(shift) and blended with its neighbours one pixel further by the
+// fractional parts (periodic), in float64 like the reference's numpy arithmetic, clipped at 0
+// and written fftshifted; shifts (2, npos) = (row, column) shift of every pattern.
+__global__ void pattern_bilinear_kernel(const float* __restrict__ amp, const double* __restrict__ shifts, int npos,
+                                        int n, float* __restrict__ camp, float* __restrict__ cint) {
+  const int64_t nn = (int64_t)n * n;
+  const int64_t total = (int64_t)npos * nn;
+  const int h = n / 2;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t p = i / nn;
+    const int k = (int)(i % nn);
+    const int r = k / n, c = k % n;
+    const double rs = shifts[p], cs = shifts[npos + p];
+    const double rf = floor(rs), cf = floor(cs);
+    const double wr = rs - rf, wc = cs - cf;
+    const int ir = (int)(((int64_t)rf % n + n) % n), ic = (int)(((int64_t)cf % n + n) % n);
+    const int r0 = (r - ir + n) % n, r1 = (r - ir - 1 + 2 * n) % n;
+    const int c0 = (c - ic + n) % n, c1 = (c - ic - 1 + 2 * n) % n;
+    const float* a = amp + p * nn;
+    double v = (double)a[r0 * n + c0] * ((1.0 - wr) * (1.0 - wc));
+    v += (double)a[r1 * n + c0] * (wr * (1.0 - wc));
+    v += (double)a[r0 * n + c1] * ((1.0 - wr) * wc);
+    v += (double)a[r1 * n + c1] * (wr * wc);
+    v = v > 0.0 ? v : 0.0;
+    const int64_t d = p * nn + (int64_t)((r + h) % n) * n + (c + h) % n;
+    camp[d] = (float)v;
+    if (cint) cint[d] = (float)(v * v);
+  }
+}
+
 int blocks_for(int64_t n, int cap = kPartBlocks) {
   int64_t b = (n + kThreads - 1) / kThreads;
   if (b < 1) b = 1;
@@ -192,6 +223,19 @@ int ptycho_pattern_center(const void* shifted, int npos, int n, float scale, flo
                           static_cast<cudaStream_t>(stream)>>>(static_cast<const float2*>(shifted), npos, n, scale,
                                                                centered_amplitudes, centered_intensities);
   return check_launch("pattern_center_kernel");
+}
+
+int ptycho_pattern_bilinear(const float* amplitudes, const double* shifts, int npos, int n,
+                            float* centered_amplitudes, float* centered_intensities, void* stream) {
+  if (!amplitudes || !shifts || !centered_amplitudes || npos < 0 || n < 2 || (n & 1))
+    return fail(PTYCHO_ERR_INVALID, "pattern_bilinear: bad arguments (even n)");
+  if (centered_amplitudes == amplitudes || centered_intensities == amplitudes)
+    return fail(PTYCHO_ERR_INVALID, "pattern_bilinear: outputs must not alias the amplitudes");
+  if (npos == 0) return PTYCHO_OK;
+  pattern_bilinear_kernel<<<blocks_for((int64_t)npos * n * n, 148 * 16), kThreads, 0,
+                            static_cast<cudaStream_t>(stream)>>>(amplitudes, shifts, npos, n, centered_amplitudes,
+                                                                 centered_intensities);
+  return check_launch("pattern_bilinear_kernel");
 }
 
 }  // extern "C"

@@ -69,6 +69,31 @@ def fourier_shift_real(ar: np.ndarray, rshift, cshift) -> np.ndarray:
     return np.real(np.fft.ifft2(np.fft.fft2(ar) * p))
 
 
+def bilinear_shift(ar: np.ndarray, rshift, cshift) -> np.ndarray:
+    """Periodic bilinear shift of real images (ptycho_utils.py:273-284, bilinear=True): each
+    image rolled by floor(shift) and blended with the roll one pixel further by the fractional
+    parts, in float64.  Works on (..., nr, nc) stacks with per-image shifts of shape (...)."""
+    nr, nc = ar.shape[-2:]
+    a = ar.reshape(-1, nr, nc)
+    rs = np.asarray(rshift, dtype=np.float64).reshape(-1)
+    cs = np.asarray(cshift, dtype=np.float64).reshape(-1)
+    rf, cf = np.floor(rs), np.floor(cs)
+    wr, wc = (rs - rf)[:, None, None], (cs - cf)[:, None, None]
+    rf, cf = rf.astype(np.int64), cf.astype(np.int64)
+    b = np.arange(a.shape[0])[:, None, None]
+    r0 = (np.arange(nr)[None] - rf[:, None]) % nr
+    r1 = (np.arange(nr)[None] - rf[:, None] - 1) % nr
+    c0 = (np.arange(nc)[None] - cf[:, None]) % nc
+    c1 = (np.arange(nc)[None] - cf[:, None] - 1) % nc
+
+    def g(ri, ci):
+        return a[b, ri[:, :, None], ci[:, None, :]].astype(np.float64)
+
+    out = g(r0, c0) * ((1 - wr) * (1 - wc)) + g(r1, c0) * (wr * (1 - wc))
+    out = out + g(r0, c1) * ((1 - wr) * wc) + g(r1, c1) * (wr * wc)
+    return out.reshape(ar.shape)
+
+
 class PtychographyDatasetRaster(OptimizerMixin):
     """4D-STEM raster dataset: targets, scan positions and their constraints."""
 
@@ -93,6 +118,8 @@ class PtychographyDatasetRaster(OptimizerMixin):
         self.intensities_4d = np.asarray(dset.array).copy()
         shp = self.intensities_4d.shape
         self._array3d = self.intensities_4d.reshape(shp[0] * shp[1], shp[2], shp[3])
+        self._dset = dset
+        self._diffraction_padding = np.zeros(2, dtype=int)
         self.detector_sampling = np.asarray(dset.sampling[-2:], dtype=float)
         self.detector_units = list(dset.units[-2:])
         self.verbose = verbose
@@ -115,6 +142,87 @@ class PtychographyDatasetRaster(OptimizerMixin):
         self._targets_on_host = False
         self._patch_indices = None
         self._last_patch_positions_px = None
+
+    @classmethod
+    def from_array(cls, array, name=None, origin=None, sampling=None, units=None, signal_units="arb. units",
+                   detector_mask=None, verbose=1, learn_descan=True, learn_scan_positions=True):
+        """A dataset from a 4-D array (dataset_models.py:734-780): a Dataset4dstem with the
+        given metadata, then the raster dataset on it."""
+        d4 = Dataset4dstem.from_array(array, name=name, origin=origin, sampling=sampling, units=units,
+                                      signal_units=signal_units)
+        return cls(d4, detector_mask, verbose, learn_descan, learn_scan_positions, _token=cls._token)
+
+    @property
+    def dset(self) -> Dataset4dstem:
+        """The source 4D-STEM dataset (dataset_models.py:251-259)."""
+        return self._dset
+
+    @property
+    def shape(self) -> np.ndarray:
+        return np.array(self._dset.shape)
+
+    @property
+    def reciprocal_units(self) -> list[str]:
+        return ["A^-1", "A^-1"]
+
+    @property
+    def diffraction_padding(self) -> np.ndarray:
+        return self._diffraction_padding
+
+    @diffraction_padding.setter
+    def diffraction_padding(self, padding):
+        pad = np.asarray(padding, dtype=int)
+        if pad.shape != (2,):
+            raise ValueError(f"diffraction_padding must have shape (2,), got {pad.shape}")
+        self._diffraction_padding = pad
+
+    @property
+    def intensities(self) -> torch.Tensor:
+        """Raw intensities (npos, qx, qy), clipped at 0 (dataset_models.py:313-327)."""
+        return self._intensities
+
+    @intensities.setter
+    def intensities(self, arr):
+        self._intensities = self._checked_patterns(arr, "intensities")
+
+    @property
+    def centered_intensities(self) -> torch.Tensor:
+        """Intensities centred on the detector (npos, qx, qy) (dataset_models.py:295-311)."""
+        return self._centered_intensities
+
+    @centered_intensities.setter
+    def centered_intensities(self, arr):
+        self._centered_intensities = self._checked_patterns(arr, "centered_intensities")
+
+    def _checked_patterns(self, arr, name):
+        t = torch.as_tensor(arr.detach() if isinstance(arr, torch.Tensor) else np.asarray(arr),
+                            dtype=getattr(torch, config.get("dtype_real")))
+        shape = (self.num_gpts, *(int(x) for x in self.roi_shape))
+        if tuple(t.shape) != shape:
+            raise ValueError(f"{name} must have shape {shape}, got {tuple(t.shape)}")
+        return t
+
+    def vprint(self, m, level: int = 1, *args, **kwargs) -> None:
+        """Print when verbose (dataset_models.py:509-512)."""
+        if self.verbose >= level:
+            print(m, *args, **kwargs)
+
+    def patch_indices_need_update(self) -> bool:
+        """Whether the rounded scan positions moved since the patch windows were last set
+        (dataset_models.py:541-548).  The batch kernels form the windows from the positions
+        themselves, so the answer only matters to callers of ``patch_indices``."""
+        if self._last_patch_positions_px is None:
+            return True
+        old = torch.round(self._last_patch_positions_px.to(self.scan_positions_px.device))
+        return not torch.equal(old, torch.round(self.scan_positions_px.detach()))
+
+    def get_descan_tv_loss(self, descan_shifts: torch.Tensor, weight: float = 0.0) -> torch.Tensor:
+        """weight x the mean absolute difference of consecutive descan shifts, averaged over the
+        two axes (dataset_models.py:580-587)."""
+        if weight == 0:
+            return torch.zeros((), dtype=getattr(torch, config.get("dtype_real")), device=descan_shifts.device)
+        return weight * (torch.mean(torch.abs(descan_shifts[:, 0].diff())) +
+                         torch.mean(torch.abs(descan_shifts[:, 1].diff()))) / 2
 
     @classmethod
     def from_dataset4dstem(cls, dset: Dataset4dstem, detector_mask=None, verbose=1, learn_descan=True,
@@ -395,11 +503,13 @@ class PtychographyDatasetRaster(OptimizerMixin):
         otherwise they run vectorised on the host.  Only the small CoM fit and the
         rotation search stay on the host in both cases."""
         if padded_diffraction_intensities_shape is not None:
+            # the reference's own padding step forwards in_place=True to numpy.pad and raises
+            # (dataset_models.py:976-983, core/datastructures/dataset.py:409-418)
             raise NotImplementedError("padded diffraction intensities are not part of the B200 path")
-        if bilinear:
-            raise NotImplementedError("bilinear centring is not part of the B200 path")
+        self._bilinear = bool(bilinear)
         self._preprocessing_params = dict(com_fit_function=com_fit_function, force_com_rotation=force_com_rotation,
-                                          force_com_transpose=force_com_transpose, obj_padding_px=obj_padding_px)
+                                          force_com_transpose=force_com_transpose, bilinear=bool(bilinear),
+                                          obj_padding_px=obj_padding_px)
         if probe_energy is not None:
             self.probe_energy = probe_energy
         dev = torch.device(config.validate_device(device if device is not None else self._device)[0])
@@ -516,7 +626,10 @@ class PtychographyDatasetRaster(OptimizerMixin):
         centered_i = np.empty_like(amp)
         chunk = max(1, 2048 // max(1, nc))
         for r0 in range(0, nr, chunk):
-            sh = fourier_shift_real(amp[r0:r0 + chunk].astype(np.float64), cr[r0:r0 + chunk], cc[r0:r0 + chunk])
+            if getattr(self, "_bilinear", False):
+                sh = bilinear_shift(amp[r0:r0 + chunk], cr[r0:r0 + chunk], cc[r0:r0 + chunk])
+            else:
+                sh = fourier_shift_real(amp[r0:r0 + chunk].astype(np.float64), cr[r0:r0 + chunk], cc[r0:r0 + chunk])
             sh = np.fft.fftshift(np.maximum(sh, 0), axes=(-2, -1))
             centered[r0:r0 + chunk] = sh.astype(dt)
             centered_i[r0:r0 + chunk] = (sh**2).astype(dt)
@@ -560,8 +673,12 @@ class PtychographyDatasetRaster(OptimizerMixin):
                                                   ops._p(amp[c0:c1]), ops._p(ac), ops._p(work), work.numel(),
                                                   ops._p(sums), st), "pattern_prepare")
             total += sums
-            ops.fft2(ac, out=ac)
             sh = shifts[:, c0:c1].contiguous()
+            if getattr(self, "_bilinear", False):
+                _lib.check(lib.ptycho_pattern_bilinear(ops._p(amp[c0:c1]), ops._p(sh), m, n, ops._p(camp[c0:c1]),
+                                                       ops._p(cint[c0:c1]), st), "pattern_bilinear")
+                continue
+            ops.fft2(ac, out=ac)
             _lib.check(lib.ptycho_pattern_shift_ramp(ops._p(ac), ops._p(sh), m, n, st), "pattern_shift_ramp")
             ops.fft2(ac, inverse=True, scale=1.0 / (n * n), out=ac)
             _lib.check(lib.ptycho_pattern_center(ops._p(ac), m, n, 1.0, ops._p(camp[c0:c1]), ops._p(cint[c0:c1]), st),

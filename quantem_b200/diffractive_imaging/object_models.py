@@ -104,6 +104,78 @@ class ObjectPixelated(OptimizerMixin):
         c = self._constraints
         return bool(c.get("tv_weight_z", 0) or c.get("tv_weight_xy", 0) or c.get("surface_zero_weight", 0))
 
+    @property
+    def name(self) -> str:
+        return "ObjPixelized"
+
+    @property
+    def shape_2d(self) -> tuple[int, int]:
+        return tuple(self.shape[1:])
+
+    def apply_hard_constraints(self, obj: torch.Tensor, mask=None) -> torch.Tensor:
+        """The hard constraints of this model (object_models.py:289-339) on any object array of
+        its type (S, Ho, Wo), differentiable, on the constraint kernels; the FOV mask applies
+        only when given, as in the reference."""
+        from .. import ops
+
+        m = None
+        if mask is not None:
+            m = torch.as_tensor(mask.detach() if isinstance(mask, torch.Tensor) else np.asarray(mask),
+                                dtype=torch.float32)
+            m = (m[0] if m.ndim == 3 else m).to(obj.device).contiguous()
+        c = self._constraints
+        if ((c.get("apply_fov_mask") and m is not None) or c.get("gaussian_sigma") is not None
+                or c.get("q_lowpass") or c.get("q_highpass") or (c.get("identical_slices") and obj.shape[0] > 1)
+                or (self.obj_type == "potential" and c.get("fix_potential_baseline"))):
+            return ops.constrained_object_ext(obj, self.obj_type, c, m, self._sampling)
+        if self.obj_type == "complex":
+            return ops.constrained_object(obj)
+        if self.obj_type == "pure_phase":
+            return ops.object_transmission(obj, self.transmission_spec())
+        return torch.clamp(obj, min=0.0) if c.get("positivity", True) else obj
+
+    def get_tv_loss(self, array: torch.Tensor, weights=None) -> torch.Tensor:
+        """TV soft loss (object_models.py:360-411): weights (z, xy) from the constraints by
+        default, a scalar for both, or a pair; the z term is dropped for one slice."""
+        from .. import ops
+
+        if weights is None:
+            w = (self._constraints.get("tv_weight_z", 0), self._constraints.get("tv_weight_xy", 0))
+        elif isinstance(weights, (int, float)):
+            w = (weights, weights)
+        else:
+            if len(weights) != 2:
+                raise ValueError(f"weights must be a tuple of length 2, got {weights}")
+            w = tuple(weights)
+        if not any(w):
+            return torch.zeros((), device=array.device)
+        return ops.soft_constraint_loss(array, self.obj_type, w[0], w[1], 0.0)
+
+    def get_surface_zero_loss(self, array: torch.Tensor, weight: float = 0.0) -> torch.Tensor:
+        """Surface-zero soft loss of the first and last slices (object_models.py:413-435)."""
+        from .. import ops
+
+        if weight == 0:
+            return torch.zeros((), device=array.device)
+        return ops.soft_constraint_loss(array, self.obj_type, 0.0, 0.0, weight)
+
+    def gaussian_blur_2d(self, tensor: torch.Tensor, sigma: float = 1.0) -> torch.Tensor:
+        """Zero-padded separable Gaussian blur along the last two axes of an (S, Ho, Wo) array
+        (object_models.py:437-479), differentiable, on the blur kernel."""
+        from .. import ops
+
+        return ops._BlurFn.apply(tensor, ops.gaussian_taps(sigma, tensor.device))
+
+    def butterworth_constraint(self, tensor: torch.Tensor, sampling) -> torch.Tensor:
+        """The Butterworth low / high-pass filter of the constraints (object_models.py:481-520)
+        on an (S, Ho, Wo) array, differentiable, on the line-DFT kernels."""
+        from .. import ops
+
+        c = self._constraints
+        env = ops.butterworth_env(tensor.shape[-2:], sampling, c.get("q_lowpass"), c.get("q_highpass"),
+                                  c.get("butterworth_order", 4), tensor.device)
+        return ops._ButterworthFn.apply(tensor, env)
+
     def _mask_on_device(self):
         m = self._mask
         if m is None:

@@ -1,8 +1,8 @@
 """Mixed-state pixelated probe model (quantem probe_models.ProbePixelated).
 
 Initial probe synthesis (probe_models.py:722-759 with complex_probe.py:475-507),
-seeded per-mode phase ramps (846-858), mode weights (860-873), Gram-Schmidt
-orthogonalisation on every access (484-525) and the Fresnel propagators
+seeded per-mode phase ramps (846-858), mode weights (860-873), the hard constraints
+(Gram-Schmidt, optional centre of mass; 452-525) on every access and the Fresnel propagators
 (376-427).  The per-position Fourier shift runs inside the fused batch kernel;
 ``forward`` is kept for callers that want explicit shifted probes.
 """
@@ -288,6 +288,35 @@ class ProbePixelated(OptimizerMixin):
         pass
 
     @property
+    def name(self) -> str:
+        return "ProbePixelated"
+
+    @property
+    def shape(self) -> np.ndarray:
+        return np.array((self.num_probes, *(int(x) for x in self._roi_shape)))
+
+    def check_probe_params(self) -> None:
+        """Report missing probe parameters; a missing defocus is taken from -C10
+        (probe_models.py:342-350)."""
+        pp = self._probe_params
+        for k in self.DEFAULT_PROBE_PARAMS:
+            if pp.get(k) is None:
+                c10 = (pp.get("aberration_coefs") or {}).get("C10", 0)
+                if k == "defocus" and c10:
+                    pp[k] = -1 * c10
+                    continue
+                print(f"Missing probe parameter '{k}' in probe_params")
+
+    def apply_hard_constraints(self, probe: torch.Tensor) -> torch.Tensor:
+        """The probe's hard constraints on any (P, n, n) stack (probe_models.py:452-458):
+        Gram-Schmidt + sort, then the centre-of-mass shift, as enabled; differentiable."""
+        if self._constraints.get("orthogonalize_probe", True):
+            probe = orthogonalize_probes(probe)
+        if self._constraints.get("center_probe", False):
+            probe = center_probe(probe)
+        return probe
+
+    @property
     def has_soft_constraints(self) -> bool:
         return bool(self._constraints.get("tv_weight", 0))
 
@@ -304,12 +333,7 @@ class ProbePixelated(OptimizerMixin):
     def probe(self) -> torch.Tensor:
         """Probe modes after the hard constraints in the reference's order (probe_models.py:
         452-458): Gram-Schmidt + sort if enabled, then the centre-of-mass shift if enabled."""
-        p = self._probe
-        if self._constraints.get("orthogonalize_probe", True):
-            p = orthogonalize_probes(p)
-        if self._constraints.get("center_probe", False):
-            p = center_probe(p)
-        return p
+        return self.apply_hard_constraints(self._probe)
 
     def _compute_propagator_arrays(self, sampling, num_slices, slice_thicknesses) -> torch.Tensor:
         """(S-1, H, W) complex64 propagators evaluated like probe_models.py:376-427."""

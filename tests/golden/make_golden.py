@@ -751,6 +751,32 @@ def probeconstraints_cases(seed=131):
               f"total={out['batch_total_loss']:.4g} losses={out['recon_losses']}")
 
 
+def bilinear_case():
+    """preprocess(bilinear=True) (dataset_models.py:946-1025, 1372-1480 with shift_array's
+    bilinear branch, ptycho_utils.py:273-284) on the mixed64 patterns, with a plane CoM fit
+    (a different shift for every pattern): centred targets, mean intensity and the CoM fit."""
+    from quantem.core.datastructures.dataset4dstem import Dataset4dstem
+    from quantem.diffractive_imaging.dataset_models import PtychographyDatasetRaster
+
+    z = np.load(os.path.join(HERE, "mixed64.npz"))
+    H, nscan = int(z["H"]), int(z["nscan"])
+    px, step = float(z["px"]), float(z["step_px"])
+    rs = 1.0 / (H * px)
+    out = dict(H=H, nscan=nscan, px=px, step_px=step, energy=z["energy"], data=z["data"])
+    for fit in ("plane", "constant"):
+        d4 = Dataset4dstem.from_array(z["data"].reshape(nscan, nscan, H, H), sampling=(step * px, step * px, rs, rs),
+                                      units=("A", "A", "A^-1", "A^-1"))
+        pd = PtychographyDatasetRaster.from_dataset4dstem(d4, verbose=0)
+        pd.preprocess(com_fit_function=fit, force_com_rotation=0, force_com_transpose=False, bilinear=True,
+                      plot_rotation=False, plot_com=False, probe_energy=float(z["energy"]))
+        out[f"targets_{fit}"] = _f32(pd.targets.numpy())
+        out[f"mean_intensity_{fit}"] = np.float64(pd.mean_diffraction_intensity)
+        out[f"com_fit_{fit}"] = np.asarray(pd.com_fit, dtype=np.float64)
+    path = os.path.join(HERE, "bilinear64.npz")
+    np.savez_compressed(path, **out)
+    print(f"wrote {path}")
+
+
 def whitenoise_case():
     """The reference gradient test's fixture (test_ptychography.py:19-212), restated."""
     import torch
@@ -823,6 +849,9 @@ def main(src):
         return
     if os.environ.get("GOLDEN_ONLY") == "objconstraints":
         objconstraints_cases()
+        return
+    if os.environ.get("GOLDEN_ONLY") == "bilinear":
+        bilinear_case()
         return
     if os.environ.get("GOLDEN_ONLY") == "probeconstraints":
         probeconstraints_cases()

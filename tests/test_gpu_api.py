@@ -106,3 +106,36 @@ def test_overlap_projection_and_fourier_projection(cuda_device, case):
     assert rel(pt.gradient_step(amps, exits).cpu().numpy(), (ref - exits).cpu().numpy()) < 1e-4
     step = pt.gradient_step(pt.estimate_amplitudes(exits), exits)
     assert float(step.abs().square().sum().sqrt()) < 1e-4 * float(exits.abs().square().sum().sqrt())
+
+
+@pytest.mark.parametrize("case", ["complex", "potential"])
+def test_object_model_helpers_match_the_constraint_path(cuda_device, case):
+    """ObjectPixelated.apply_hard_constraints on an arbitrary array equals the model's own
+    constrained object; the TV / surface / blur / Butterworth helpers equal the oracle."""
+    from oracle import ptycho_oracle as O
+    from tests.test_gpu_objconstraints import _dropin
+    from tests.test_oracle_golden import OBJCONS_CASES
+
+    obj_type, cons = OBJCONS_CASES[case]
+    z = load_golden(f"objcons_{case}64")
+    pt = _dropin(z, cuda_device, obj_type)
+    pt.constraints = {"object": dict(cons)}
+    om = pt.obj_model
+    mask = om.mask
+    got = om.apply_hard_constraints(om._obj, mask)
+    assert torch.equal(got.detach(), om.obj.detach())
+    x = got.detach()
+    xs = x.cpu().numpy().astype(np.complex128 if obj_type != "potential" else np.float64)
+    tv = om.get_tv_loss(x, (0.02, 0.05))
+    tv_o, _ = O.soft_constraint_loss(xs, obj_type, 0.02, 0.05, 0.0)
+    assert abs(tv.item() - tv_o) <= 1e-5 * abs(tv_o)
+    sz = om.get_surface_zero_loss(x, 0.01)
+    sz_o, _ = O.soft_constraint_loss(xs, obj_type, 0.0, 0.0, 0.01)
+    assert abs(sz.item() - sz_o) <= 1e-5 * max(abs(sz_o), 1e-6)
+    bl = om.gaussian_blur_2d(x, 1.3)
+    assert rel(bl.cpu().numpy(), O.blur(xs, O.gaussian_taps(1.3))) < 1e-5
+    om.add_constraint("q_lowpass", 1.4)
+    bw = om.butterworth_constraint(x, om._sampling)
+    env = O.butterworth_env(x.shape[-2:], om._sampling, 1.4, om.constraints.get("q_highpass"),
+                            om.constraints.get("butterworth_order", 4))
+    assert rel(bw.cpu().numpy(), O.butterworth(xs, env)) < 1e-5

@@ -52,3 +52,28 @@ def test_gpu_preprocess_matches_host_path(cuda_device, n):
     assert rel(g.centered_amplitudes.cpu().numpy(), h.centered_amplitudes.numpy()) < 1e-5
     assert rel(g.amplitudes.cpu().numpy(), h.amplitudes.numpy()) < 1e-6
     assert g.com_rotation_rad == h.com_rotation_rad and g.com_transpose == h.com_transpose
+
+
+@pytest.mark.parametrize("fit", ["plane", "constant"])
+def test_gpu_bilinear_centring_matches_reference(cuda_device, fit):
+    """preprocess(bilinear=True) on the GPU (ptycho_pattern_bilinear) against the reference's
+    own centred targets (fixture bilinear64) and the host path."""
+    from quantem_b200.diffractive_imaging import Dataset4dstem, PtychographyDatasetRaster
+
+    z = load_golden("bilinear64")
+    H, nscan = int(z["H"]), int(z["nscan"])
+    px, step = float(z["px"]), float(z["step_px"])
+    rs = 1.0 / (H * px)
+    out = {}
+    for dev in ("gpu", "cpu"):
+        d4 = Dataset4dstem.from_array(z["data"].reshape(nscan, nscan, H, H),
+                                      sampling=(step * px, step * px, rs, rs), units=("A", "A", "A^-1", "A^-1"))
+        pd = PtychographyDatasetRaster.from_dataset4dstem(d4, verbose=0)
+        pd.preprocess(com_fit_function=fit, force_com_rotation=0, force_com_transpose=False, bilinear=True,
+                      plot_rotation=False, plot_com=False, probe_energy=float(z["energy"]), device=dev)
+        out[dev] = pd
+    g = out["gpu"]
+    assert g.targets.is_cuda
+    assert rel(g.targets.cpu().numpy(), z[f"targets_{fit}"]) < 1e-6
+    assert rel(g.targets.cpu().numpy(), out["cpu"].targets.numpy()) < 1e-6
+    assert abs(g.mean_diffraction_intensity - float(z[f"mean_intensity_{fit}"])) <= 1e-6 * g.mean_diffraction_intensity

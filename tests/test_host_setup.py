@@ -149,3 +149,52 @@ def test_probe_constraints_on_the_host_match_reference(case):
     assert rel(p.numpy(), z["probe_constrained"]) < 2e-5
     soft = float(pm.apply_soft_constraints(p))
     assert abs(soft - float(z["probe_soft_loss"])) <= 1e-5 * max(float(z["probe_soft_loss"]), 1e-3)
+
+
+@pytest.mark.parametrize("fit", ["plane", "constant"])
+def test_bilinear_centring_matches_reference(fit):
+    """preprocess(bilinear=True) on the host against the reference's own (fixture
+    bilinear64): the CoM fit, the centred targets and the mean intensity."""
+    from quantem_b200.diffractive_imaging import Dataset4dstem, PtychographyDatasetRaster
+
+    z = load_golden("bilinear64")
+    H, nscan = int(z["H"]), int(z["nscan"])
+    px, step = float(z["px"]), float(z["step_px"])
+    rs = 1.0 / (H * px)
+    d4 = Dataset4dstem.from_array(z["data"].reshape(nscan, nscan, H, H), sampling=(step * px, step * px, rs, rs),
+                                  units=("A", "A", "A^-1", "A^-1"))
+    pd = PtychographyDatasetRaster.from_dataset4dstem(d4, verbose=0)
+    pd.preprocess(com_fit_function=fit, force_com_rotation=0, force_com_transpose=False, bilinear=True,
+                  plot_rotation=False, plot_com=False, probe_energy=float(z["energy"]), device="cpu")
+    np.testing.assert_allclose(pd.com_fit, z[f"com_fit_{fit}"], rtol=0, atol=1e-5)  # float32 CoM sums
+    assert rel(pd.targets.numpy(), z[f"targets_{fit}"]) < 1e-6
+    assert abs(pd.mean_diffraction_intensity - float(z[f"mean_intensity_{fit}"])) <= 1e-6 * pd.mean_diffraction_intensity
+
+
+def test_model_api_members_on_the_host():
+    """Members of the reference's dataset, probe and object models that need no GPU."""
+    from quantem_b200.diffractive_imaging import PtychographyDatasetRaster
+
+    z = load_golden("mixed64")
+    pt = build_from_golden(z)
+    d = pt.dset
+    H, nscan = int(z["H"]), int(z["nscan"])
+    assert tuple(d.shape) == (nscan, nscan, H, H) and tuple(d.dset.shape) == tuple(d.shape)
+    assert d.reciprocal_units == ["A^-1", "A^-1"] and d.diffraction_padding.tolist() == [0, 0]
+    assert tuple(d.intensities.shape) == (nscan * nscan, H, H)
+    assert tuple(d.centered_intensities.shape) == (nscan * nscan, H, H)
+    assert rel(d.centered_intensities.numpy(), d.centered_amplitudes.numpy() ** 2) < 1e-6
+    assert not d.patch_indices_need_update()
+    sh = torch.arange(12, dtype=torch.float32).reshape(6, 2) ** 2
+    ref = 0.3 * (sh[:, 0].diff().abs().mean() + sh[:, 1].diff().abs().mean()) / 2
+    assert torch.allclose(d.get_descan_tv_loss(sh, 0.3), ref)
+    with pytest.raises(ValueError):
+        d.intensities = np.zeros((2, H, H))
+    d2 = PtychographyDatasetRaster.from_array(z["data"].reshape(nscan, nscan, H, H), sampling=(1, 1, 0.1, 0.1),
+                                              units=("A", "A", "A^-1", "A^-1"), verbose=0)
+    assert d2.num_gpts == nscan * nscan and d2.dset.name == "4D-STEM dataset"
+    pm = pt.probe_model
+    assert pm.name == "ProbePixelated" and tuple(pm.shape) == (int(z["P"]), H, H)
+    assert torch.equal(pm.apply_hard_constraints(pm._probe.detach()), pm.probe.detach())
+    om = pt.obj_model
+    assert om.name == "ObjPixelized" and om.shape_2d == tuple(pt.obj_shape_full[-2:])
