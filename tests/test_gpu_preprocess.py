@@ -65,15 +65,15 @@ def test_gpu_bilinear_centring_matches_reference(cuda_device, fit):
     px, step = float(z["px"]), float(z["step_px"])
     rs = 1.0 / (H * px)
     out = {}
-    for dev in ("gpu", "cpu"):
+    for dev in (cuda_device, "cpu"):
         d4 = Dataset4dstem.from_array(z["data"].reshape(nscan, nscan, H, H),
                                       sampling=(step * px, step * px, rs, rs), units=("A", "A", "A^-1", "A^-1"))
         pd = PtychographyDatasetRaster.from_dataset4dstem(d4, verbose=0)
         pd.preprocess(com_fit_function=fit, force_com_rotation=0, force_com_transpose=False, bilinear=True,
                       plot_rotation=False, plot_com=False, probe_energy=float(z["energy"]), device=dev)
-        out[dev] = pd
-    g = out["gpu"]
-    assert g.targets.is_cuda
+        out[str(dev)] = pd
+    g = out[str(cuda_device)]
+    assert g._preprocessed_on == "gpu" and out["cpu"]._preprocessed_on == "host"
     assert rel(g.targets.cpu().numpy(), z[f"targets_{fit}"]) < 1e-6
     assert rel(g.targets.cpu().numpy(), out["cpu"].targets.numpy()) < 1e-6
     assert abs(g.mean_diffraction_intensity - float(z[f"mean_intensity_{fit}"])) <= 1e-6 * g.mean_diffraction_intensity
