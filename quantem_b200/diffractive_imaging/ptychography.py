@@ -4,8 +4,8 @@ Same construction and call sequence as the reference (ptychography.py:36-58,
 ptychography_base.py:135-189, ptychography.py:146-308): ``from_models`` ->
 ``preprocess`` -> ``reconstruct``.  Each batch runs one fused forward + loss +
 adjoint CUDA launch (quantem_b200.ops) followed by the fused optimiser kernels;
-the batch loss stays on the device and every iteration reads the loss back once
-(the reference reads it twice per batch).
+the batch loss stays on the device and is read back once per iteration, or once per
+call when nothing consumes it during the run (the reference reads it twice per batch).
 """
 from __future__ import annotations
 
@@ -83,6 +83,7 @@ class Ptychography:
         self.logger = logger
         self._propagators = torch.tensor([])
         self._prop_factors = None
+        self.loss_readback: Literal["auto", "iteration"] = "auto"
         self.to(self._device)
 
     @classmethod
@@ -803,6 +804,13 @@ class Ptychography:
         stream = HostTargetStream(tg, dev) if tg.device.type != "cuda" and num_iters > 0 else None
         self.last_h2d_bytes_per_iter = stream.bytes_per_copy if stream is not None else 0
         nvtx = torch.cuda.nvtx  # profiler ranges (iteration, batch); no cost without a profiler
+        # when nothing reads the loss during the run (no scheduler, logger, validation split or
+        # snapshots) and ``loss_readback`` is "auto", each iteration's loss stays on the device and
+        # all are read once at the end, with the status word: the host queues iteration after
+        # iteration without waiting.  "iteration" reads every iteration's loss when it ends.
+        defer = (self.loss_readback == "auto" and self.logger is None and not batcher.has_validation
+                 and not self._store_snapshots and not self.schedulers)
+        pending = []
         for a0 in range(num_iters):
             nvtx.range_push(f"reconstruct iteration {self.num_iters}")
             total = torch.zeros((), dtype=torch.float32, device=dev)
@@ -885,6 +893,10 @@ class Ptychography:
                 nvtx.range_pop()
             if stream is not None:
                 stream.release()
+            if defer:
+                pending.append(total / max(nb, 1))
+                nvtx.range_pop()
+                continue
             total_loss = float((total / max(nb, 1)).item())
             # the logger receives the consistency loss alone (ptychography.py:284-292)
             consistency_loss = total_loss
@@ -911,6 +923,11 @@ class Ptychography:
                 self.logger.log_iter(self.obj_model, self.probe_model, self.dset, self.num_iters - 1,
                                      consistency_loss, nb, self._get_current_lrs())
             nvtx.range_pop()
+        if pending:  # one read of every iteration's loss and of the status word
+            losses = torch.stack(pending).cpu().tolist()
+            ops.check_status(dev)
+            for loss in losses:
+                self._record_iter(float(loss))
         return self
 
     def _get_current_lrs(self):

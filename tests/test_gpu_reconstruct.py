@@ -171,3 +171,24 @@ def test_host_resident_targets_match_device_targets(cuda_device):
         runs.append((np.asarray(pt.iter_losses), pt.obj_model._obj.detach().cpu().numpy()))
     np.testing.assert_allclose(runs[1][0], runs[0][0], rtol=1e-6)
     assert rel(runs[1][1], runs[0][1]) < 1e-5
+
+
+def test_deferred_loss_readback_matches_per_iteration_readback(cuda_device):
+    """loss_readback='auto' (every iteration's loss read once at the end of the call, nothing
+    consuming it in between) gives the same losses and parameters as reading each iteration."""
+    z = load_golden("mixed64")
+    out = {}
+    for mode in ("iteration", "auto"):
+        pt = build_from_golden(z, device="gpu")
+        pt.dset.scan_positions_px = torch.as_tensor(z["positions"])
+        pt.obj_model._obj = torch.as_tensor(z["obj_perturbed"]).to(cuda_device).requires_grad_(True)
+        pt.probe_model._probe = torch.as_tensor(z["probe_init"]).to(cuda_device).requires_grad_(True)
+        pt.rng = int(z["recon_rng_seed"])
+        pt.loss_readback = mode
+        pt.reconstruct(num_iters=4, batch_size=int(z["batch"]),
+                       optimizer_params={"object": {"type": "adam"}, "probe": {"type": "adam"}}, device="gpu")
+        out[mode] = pt
+    a, b = out["iteration"], out["auto"]
+    assert len(b.iter_losses) == 4
+    np.testing.assert_allclose(b.iter_losses, a.iter_losses, rtol=1e-6)
+    assert rel(b.obj_model._obj.detach().cpu().numpy(), a.obj_model._obj.detach().cpu().numpy()) < 1e-5
