@@ -1020,26 +1020,32 @@ def fourier_projection_seed(far: np.ndarray, targets: np.ndarray) -> np.ndarray:
     return mod - far
 
 
-def analytic_gradients(obj_raw, probe_raw, positions_px, props, targets, orthogonalize=False):
+def analytic_gradients(obj_raw, probe_raw, positions_px, props, targets, orthogonalize=False, obj_type="complex"):
     """Object and probe update directions of the analytic path, as
     ``Ptychography.backward(autograd=False)`` leaves them in ``.grad``
     (ptychography.py:339-348, object_models.py:686-725, probe_models.py:774-783).
+    ``obj_type``: complex and pure-phase objects take sum_patches(conj(psi) g); a potential
+    takes the real sum_patches(Re(-i conj(o) conj(psi) g)) with o its transmission patches.
     """
-    obj_c = constrain_object(obj_raw)
+    obj_c = constrain_object(obj_raw) if obj_type == "complex" else object_transmission(obj_raw, obj_type)
     probe_o = gram_schmidt(probe_raw)[0] if orthogonalize else probe_raw
     S = obj_c.shape[0]
     P, H, W = probe_o.shape
     st = forward(obj_c, probe_o, positions_px, props)
     grad = ifft2(fourier_projection_seed(st.far, targets), norm="ortho")
-    g_obj = np.zeros(obj_c.shape, dtype=obj_c.dtype)
+    pot = obj_type == "potential"
+    g_obj = np.zeros(obj_c.shape, dtype=obj_c.real.dtype if pot else obj_c.dtype)
     for s in reversed(range(S)):
         psi = st.waves[s]
         norm = 0.0
-        upd = np.zeros(obj_c.shape[1:], dtype=obj_c.dtype)
+        upd = np.zeros(obj_c.shape[1:], dtype=g_obj.dtype)
         for a in range(P):
             inten = scatter_patches((np.abs(psi[a]) ** 2)[None], st.rows, st.cols, (1,) + obj_c.shape[1:])[0]
             norm += inten.max()
-            upd += scatter_patches((np.conj(psi[a]) * grad[a])[None], st.rows, st.cols, (1,) + obj_c.shape[1:])[0]
+            term = np.conj(psi[a]) * grad[a]
+            if pot:
+                term = np.real(-1j * np.conj(st.patches[s]) * term)
+            upd += scatter_patches(term[None], st.rows, st.cols, (1,) + obj_c.shape[1:])[0]
         g_obj[s] = upd / norm
         grad = np.conj(st.patches[s])[None] * grad
         if s > 0:

@@ -867,9 +867,6 @@ class Ptychography:
                     # analytic update directions (ptychography.py:339-348), no autograd graph
                     if type(self.obj_model).__name__ == "ObjectDIP":
                         raise NotImplementedError("the analytic update applies to pixelated objects (autograd=True)")
-                    if self.obj_model.obj_type != "complex":
-                        raise NotImplementedError("the analytic update of this path covers complex objects; "
-                                                  "use autograd=True for pure-phase and potential objects")
                     if self.dset.batch_descan() is not None:
                         raise NotImplementedError("learned descan shifts need autograd=True")
                     if self.obj_model._ext_constraints() or self.obj_model.has_soft_constraints:
@@ -878,10 +875,19 @@ class Ptychography:
                         raise NotImplementedError("the optional probe constraints need autograd=True")
                     with torch.no_grad():
                         probe_o = self.probe_model.probe.detach().contiguous()
-                        obj_c, _ = ops.obj_constrain(self.obj_model._obj.detach().contiguous())
+                        obj_type = self.obj_model.obj_type
+                        if obj_type == "complex":
+                            obj_c, _ = ops.obj_constrain(self.obj_model._obj.detach().contiguous())
+                        else:
+                            obj_c = self.obj_model.transmission().detach().contiguous()
                         loss, g_obj, g_probe = ops.batch_analytic(
                             obj_c, probe_o, prop, pos, idx, tg, mask, self.dset.num_gpts,
                             self.dset.mean_diffraction_intensity, loss_type)
+                        if obj_type == "potential":
+                            # sum_patches Re(-i conj(o) conj(psi) g) (object_models.py:705-709) is
+                            # Im(conj(o) sum_patches conj(psi) g): every patch covering a pixel
+                            # carries that pixel's transmission o
+                            g_obj = (obj_c.conj() * g_obj).imag.contiguous()
                     self.obj_model._obj.grad = g_obj
                     self.probe_model._probe.grad = g_probe
                     closs = loss

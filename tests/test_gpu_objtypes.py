@@ -126,3 +126,51 @@ def test_reconstruct_matches_reference_object_types(cuda_device, case):
     if str(z["obj_type"]) == "potential":
         v = pt.obj  # the constrained potential: real, non-negative
         assert np.isrealobj(v) and v.min() >= 0.0
+
+
+def _dropin_objtype(z, dev):
+    from quantem_b200.diffractive_imaging import (Dataset4dstem, DetectorPixelated, ObjectPixelated,
+                                                  ProbePixelated, Ptychography, PtychographyDatasetRaster)
+
+    H, nscan = int(z["H"]), int(z["nscan"])
+    px, step = float(z["px"]), float(z["step_px"])
+    rs = 1.0 / (H * px)
+    d4 = Dataset4dstem.from_array(z["data"].reshape(nscan, nscan, H, H), sampling=(step * px, step * px, rs, rs),
+                                  units=("A", "A", "A^-1", "A^-1"))
+    pd = PtychographyDatasetRaster.from_dataset4dstem(d4, verbose=0)
+    pd.preprocess(com_fit_function="constant", force_com_rotation=0, force_com_transpose=False,
+                  probe_energy=float(z["energy"]), device="gpu")
+    obj = ObjectPixelated.from_uniform(num_slices=int(z["S"]), slice_thicknesses=float(z["dz"]),
+                                       obj_type=str(z["obj_type"]))
+    probe = ProbePixelated.from_params(probe_params={"energy": float(z["energy"]), "defocus": 200.0,
+                                                     "semiangle_cutoff": 20.0},
+                                       num_probes=int(z["P"]), rng=int(z["seed"]) + 1,
+                                       initial_probe_weights=list(z["weights"]))
+    pt = Ptychography.from_models(dset=pd, obj_model=obj, probe_model=probe, detector_model=DetectorPixelated(),
+                                  device="gpu", verbose=0, rng=int(z["seed"]) + 2)
+    pt.preprocess(obj_padding_px=(int(z["pad"]), int(z["pad"])))
+    pt.dset.scan_positions_px = torch.as_tensor(z["positions"])
+    pt.obj_model._obj = torch.as_tensor(z["obj_perturbed"]).to(dev).requires_grad_(True)
+    pt.probe_model._probe = torch.as_tensor(z["probe_init"]).to(dev).requires_grad_(True)
+    return pt
+
+
+@pytest.mark.parametrize("case", ["purephase64", "potential64"])
+def test_analytic_update_of_object_types_through_reconstruct(cuda_device, case):
+    """reconstruct(autograd=False) with pure-phase and potential objects: one full-batch pass
+    with zero-step SGD leaves the analytic update directions in .grad; they equal the FP64
+    oracle's (pinned to the reference's own analytic gradients of these object types)."""
+    z = load_golden(case)
+    pt = _dropin_objtype(z, cuda_device)
+    obj_type = str(z["obj_type"])
+    pt.reconstruct(num_iters=1, batch_size=pt.dset.num_gpts, autograd=False,
+                   optimizer_params={"object": {"type": "sgd", "lr": 0.0}, "probe": {"type": "sgd", "lr": 0.0}},
+                   constraints={"probe": {"orthogonalize_probe": True}}, device="gpu")
+    raw = z["obj_perturbed"].astype(np.float64 if obj_type == "potential" else np.complex128)
+    g_obj, g_probe, _ = O.analytic_gradients(raw, z["probe_init"].astype(np.complex128),
+                                             z["positions"].astype(np.float64), z["propagators"].astype(np.complex128),
+                                             z["targets"].astype(np.float64), orthogonalize=True, obj_type=obj_type)
+    got = pt.obj_model._obj.grad
+    assert got.dtype == (torch.float32 if obj_type == "potential" else torch.complex64)
+    assert rel(got.cpu().numpy(), g_obj) < 1e-4
+    assert rel(pt.probe_model._probe.grad.cpu().numpy(), g_probe) < 1e-4

@@ -304,3 +304,20 @@ def test_oracle_probe_constraints_match_reference(case):
     np.testing.assert_allclose(losses, z["recon_losses"], rtol=2e-5)
     assert rel(obj, z["recon_obj"]) < 2e-4
     assert rel(probe, z["recon_probe"]) < 2e-4
+
+
+@pytest.mark.parametrize("case,obj_type", [("purephase64", "pure_phase"), ("potential64", "potential")])
+def test_oracle_analytic_update_of_other_object_types_matches_reference(case, obj_type):
+    """The analytic update directions of pure-phase and potential objects (object_models.py:
+    705-712: a potential takes Re(-i conj(o) conj(psi) g)) against the reference's own."""
+    z = load_golden(case)
+    bi = z["batch_indices"]
+    raw = z["obj_perturbed"].astype(np.float64 if obj_type == "potential" else np.complex128)
+    g_obj, g_probe, _ = O.analytic_gradients(raw, z["probe_init"].astype(np.complex128),
+                                             z["positions"].astype(np.float64)[bi],
+                                             z["propagators"].astype(np.complex128),
+                                             z["targets"].astype(np.float64)[bi],
+                                             orthogonalize=bool(z["orthogonalize"]), obj_type=obj_type)
+    assert np.isrealobj(g_obj) == (obj_type == "potential")
+    assert rel(g_obj, z["grad_obj_an"]) < 5e-6
+    assert rel(g_probe, z["grad_probe_an"]) < 5e-6
