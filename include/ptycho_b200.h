@@ -302,6 +302,20 @@ int ptycho_add_scalar(float* x, float v, void* stream);
 int ptycho_sgd_step(float* param, const float* grad, int64_t count, float lr, const float* lr_dev,
                     float weight_decay, void* stream);
 
+/* torch.optim.Adam / AdamW step with amsgrad=True (optimizer_mixin.py:117-123): as
+ * ptycho_adam_step, with max_exp_avg_sq = max(max_exp_avg_sq, exp_avg_sq) in the denominator. */
+int ptycho_adam_amsgrad_step(float* param, const float* grad, float* exp_avg, float* exp_avg_sq,
+                             float* max_exp_avg_sq, int64_t count, float lr, const float* lr_dev, float beta1,
+                             float beta2, float eps, float weight_decay, int decoupled, float bc1, float bc2_sqrt,
+                             void* stream);
+
+/* torch.optim.SGD step with momentum: g = grad + wd * param; buf = g on the first step
+ * (first_step != 0), else momentum * buf + (1 - dampening) * g; param -= lr * (g + momentum *
+ * buf) with nesterov, lr * buf otherwise. */
+int ptycho_sgd_momentum_step(float* param, const float* grad, float* momentum_buffer, int64_t count, float lr,
+                             const float* lr_dev, float weight_decay, float momentum, float dampening, int nesterov,
+                             int first_step, void* stream);
+
 /* Analytic (autograd=False) update, finalisation steps after an analytic adjoint launch
  * (a->analytic = 1; object_models.py:686-725, probe_models.py:774-783):
  *   ptycho_patch_energy_max        out[0] = max over slices and batch positions of sum |o_patch|^2

@@ -71,6 +71,8 @@ EXPORTED = (
     "ptycho_pattern_shift_ramp",
     "ptycho_pattern_center",
     "ptycho_pattern_bilinear",
+    "ptycho_adam_amsgrad_step",
+    "ptycho_sgd_momentum_step",
     "ptycho_probe_ortho_work_elems",
     "ptycho_probe_orthogonalize",
     "ptycho_probe_orthogonalize_vjp",
@@ -170,6 +172,9 @@ def _declare(lib):
         "ptycho_pattern_shift_ramp": (_int, [_vp, _vp, _int, _int, _vp]),
         "ptycho_pattern_center": (_int, [_vp, _int, _int, _flt, _vp, _vp, _vp]),
         "ptycho_pattern_bilinear": (_int, [_vp, _vp, _int, _int, _vp, _vp, _vp]),
+        "ptycho_adam_amsgrad_step": (_int, [_vp, _vp, _vp, _vp, _vp, _i64, _flt, _vp, _flt, _flt, _flt, _flt, _int,
+                                             _flt, _flt, _vp]),
+        "ptycho_sgd_momentum_step": (_int, [_vp, _vp, _vp, _i64, _flt, _vp, _flt, _flt, _flt, _int, _int, _vp]),
         "ptycho_probe_ortho_work_elems": (_i64, [_int, _i64]),
         "ptycho_probe_orthogonalize": (_int, [_vp, _vp, _int, _i64, _vp, _i64, _vp]),
         "ptycho_probe_orthogonalize_vjp": (_int, [_vp, _vp, _vp, _int, _i64, _vp, _i64, _vp]),

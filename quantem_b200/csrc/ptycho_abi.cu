@@ -290,6 +290,50 @@ __global__ void sgd_kernel(float* __restrict__ p, const float* __restrict__ g, i
   }
 }
 
+// torch.optim.Adam with amsgrad=True: the denominator takes the running maximum of the
+// second moment (vmax), otherwise the same step as adam_kernel
+__global__ void adam_amsgrad_kernel(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                                    float* __restrict__ v, float* __restrict__ vmax, int64_t n, float lr,
+                                    const float* lr_dev, float b1, float b2, float eps, float wd, int decoupled,
+                                    float bc1, float bc2_sqrt) {
+  const float lr_ = lr_dev ? *lr_dev : lr;
+  const float step = lr_ / bc1;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    float pi = p[i];
+    float gi = g[i];
+    if (wd != 0.0f) {
+      if (decoupled) pi *= 1.0f - lr_ * wd;
+      else gi = fmaf(wd, pi, gi);
+    }
+    float mi = m[i];
+    mi = mi + (1.0f - b1) * (gi - mi);
+    const float vi = v[i] * b2 + (1.0f - b2) * gi * gi;
+    const float vm = fmaxf(vmax[i], vi);
+    const float denom = sqrtf(vm) / bc2_sqrt + eps;
+    p[i] = pi - step * (mi / denom);
+    m[i] = mi;
+    v[i] = vi;
+    vmax[i] = vm;
+  }
+}
+
+// torch.optim.SGD with momentum (dampening, Nesterov): the first step seeds the buffer with
+// the gradient, later ones take buf = momentum buf + (1 - dampening) g
+__global__ void sgd_momentum_kernel(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ buf,
+                                    int64_t n, float lr, const float* lr_dev, float wd, float momentum,
+                                    float dampening, int nesterov, int first) {
+  const float lr_ = lr_dev ? *lr_dev : lr;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const float pi = p[i];
+    float gi = g[i];
+    if (wd != 0.0f) gi = fmaf(wd, pi, gi);
+    const float b = first ? gi : fmaf(1.0f - dampening, gi, buf[i] * momentum);
+    buf[i] = b;
+    const float d = nesterov ? fmaf(momentum, b, gi) : b;
+    p[i] = pi - lr_ * d;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // analytic update finalisation (object_models.py:686-725, probe_models.py:774-783)
 // ---------------------------------------------------------------------------
@@ -818,6 +862,29 @@ int ptycho_sgd_step(float* param, const float* grad, int64_t count, float lr, co
   sgd_kernel<<<grid_for(count, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(param, grad, count, lr, lr_dev,
                                                                                    weight_decay);
   return check_launch("sgd_kernel");
+}
+
+int ptycho_adam_amsgrad_step(float* param, const float* grad, float* exp_avg, float* exp_avg_sq,
+                             float* max_exp_avg_sq, int64_t count, float lr, const float* lr_dev, float beta1,
+                             float beta2, float eps, float weight_decay, int decoupled, float bc1, float bc2_sqrt,
+                             void* stream) {
+  if (!param || !grad || !exp_avg || !exp_avg_sq || !max_exp_avg_sq || count < 0)
+    return fail(PTYCHO_ERR_INVALID, "adam_amsgrad: bad arguments");
+  if (count == 0) return PTYCHO_OK;
+  adam_amsgrad_kernel<<<grid_for(count, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      param, grad, exp_avg, exp_avg_sq, max_exp_avg_sq, count, lr, lr_dev, beta1, beta2, eps, weight_decay, decoupled,
+      bc1, bc2_sqrt);
+  return check_launch("adam_amsgrad_kernel");
+}
+
+int ptycho_sgd_momentum_step(float* param, const float* grad, float* momentum_buffer, int64_t count, float lr,
+                             const float* lr_dev, float weight_decay, float momentum, float dampening, int nesterov,
+                             int first_step, void* stream) {
+  if (!param || !grad || !momentum_buffer || count < 0) return fail(PTYCHO_ERR_INVALID, "sgd_momentum: bad arguments");
+  if (count == 0) return PTYCHO_OK;
+  sgd_momentum_kernel<<<grid_for(count, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      param, grad, momentum_buffer, count, lr, lr_dev, weight_decay, momentum, dampening, nesterov, first_step);
+  return check_launch("sgd_momentum_kernel");
 }
 
 }  // extern "C"

@@ -23,10 +23,8 @@ class FusedAdam(torch.optim.Optimizer):
 
     def __init__(self, params, lr=1e-3, betas=(0.9, 0.999), eps=1e-8, weight_decay=0.0, decoupled=False,
                  amsgrad=False, **unused):
-        if amsgrad:
-            raise NotImplementedError("amsgrad is not supported by the fused optimiser")
         super().__init__(params, dict(lr=lr, betas=betas, eps=eps, weight_decay=weight_decay,
-                                      decoupled=decoupled))
+                                      decoupled=decoupled, amsgrad=bool(amsgrad)))
 
     @torch.no_grad()
     def step(self, closure=None):
@@ -40,28 +38,42 @@ class FusedAdam(torch.optim.Optimizer):
                     st["step"] = 0
                     st["exp_avg"] = torch.zeros_like(p)
                     st["exp_avg_sq"] = torch.zeros_like(p)
+                    if group.get("amsgrad"):
+                        st["max_exp_avg_sq"] = torch.zeros_like(p)
                 st["step"] += 1
                 ops.adam_step(p.data, p.grad.contiguous(), st["exp_avg"], st["exp_avg_sq"], st["step"],
                               group["lr"], group["betas"], group["eps"], group["weight_decay"],
-                              group["decoupled"])
+                              group["decoupled"], max_exp_avg_sq=st.get("max_exp_avg_sq"))
         return loss
 
 
 class FusedSGD(torch.optim.Optimizer):
-    """torch.optim.SGD without momentum, update in one CUDA kernel per parameter."""
+    """torch.optim.SGD (momentum, dampening, Nesterov, weight decay), the update in one CUDA
+    kernel per parameter."""
 
-    def __init__(self, params, lr=1e-3, weight_decay=0.0, momentum=0.0, **unused):
-        if momentum:
-            raise NotImplementedError("momentum is not supported by the fused optimiser")
-        super().__init__(params, dict(lr=lr, weight_decay=weight_decay))
+    def __init__(self, params, lr=1e-3, weight_decay=0.0, momentum=0.0, dampening=0.0, nesterov=False, **unused):
+        if nesterov and (momentum <= 0 or dampening != 0):
+            raise ValueError("Nesterov momentum requires a momentum and zero dampening")
+        super().__init__(params, dict(lr=lr, weight_decay=weight_decay, momentum=momentum, dampening=dampening,
+                                      nesterov=bool(nesterov)))
 
     @torch.no_grad()
     def step(self, closure=None):
         loss = closure() if closure is not None else None
         for group in self.param_groups:
             for p in group["params"]:
-                if p.grad is not None:
+                if p.grad is None:
+                    continue
+                if not group["momentum"]:
                     ops.sgd_step(p.data, p.grad.contiguous(), group["lr"], group["weight_decay"])
+                    continue
+                st = self.state[p]
+                first = "momentum_buffer" not in st
+                if first:
+                    st["momentum_buffer"] = torch.empty_like(p)
+                ops.sgd_momentum_step(p.data, p.grad.contiguous(), st["momentum_buffer"], first, group["lr"],
+                                      group["momentum"], group["dampening"], group["nesterov"],
+                                      group["weight_decay"])
         return loss
 
 

@@ -976,14 +976,23 @@ def _real_view(t: torch.Tensor) -> torch.Tensor:
 
 
 def adam_step(param, grad, exp_avg, exp_avg_sq, step: int, lr: float, betas=(0.9, 0.999), eps=1e-8,
-              weight_decay=0.0, decoupled=False, lr_tensor=None):
+              weight_decay=0.0, decoupled=False, lr_tensor=None, max_exp_avg_sq=None):
+    """One Adam / AdamW step; with ``max_exp_avg_sq`` the AMSGrad variant."""
     p, g = _real_view(param), _real_view(grad)
     m, v = _real_view(exp_avg), _real_view(exp_avg_sq)
-    for name, t in (("param", p), ("grad", g), ("exp_avg", m), ("exp_avg_sq", v)):
-        _req(t.reshape(-1) if t.is_contiguous() else t, name, torch.float32)
+    vm = None if max_exp_avg_sq is None else _real_view(max_exp_avg_sq)
+    for name, t in (("param", p), ("grad", g), ("exp_avg", m), ("exp_avg_sq", v), ("max_exp_avg_sq", vm)):
+        if t is not None:
+            _req(t.reshape(-1) if t.is_contiguous() else t, name, torch.float32)
     b1, b2 = betas
     bc1 = 1.0 - b1 ** step
     bc2s = (1.0 - b2 ** step) ** 0.5
+    if vm is not None:
+        _lib.check(_lib.lib().ptycho_adam_amsgrad_step(_p(p), _p(g), _p(m), _p(v), _p(vm), p.numel(), float(lr),
+                                                       _p(lr_tensor), float(b1), float(b2), float(eps),
+                                                       float(weight_decay), int(bool(decoupled)), float(bc1),
+                                                       float(bc2s), _stream()), "adam_amsgrad_step")
+        return
     _lib.check(_lib.lib().ptycho_adam_step(_p(p), _p(g), _p(m), _p(v), p.numel(), float(lr), _p(lr_tensor),
                                            float(b1), float(b2), float(eps), float(weight_decay),
                                            int(bool(decoupled)), float(bc1), float(bc2s), _stream()), "adam_step")
@@ -995,3 +1004,15 @@ def sgd_step(param, grad, lr: float, weight_decay=0.0, lr_tensor=None):
     _req(g, "grad", torch.float32)
     _lib.check(_lib.lib().ptycho_sgd_step(_p(p), _p(g), p.numel(), float(lr), _p(lr_tensor),
                                           float(weight_decay), _stream()), "sgd_step")
+
+
+def sgd_momentum_step(param, grad, momentum_buffer, first: bool, lr: float, momentum: float, dampening=0.0,
+                      nesterov=False, weight_decay=0.0, lr_tensor=None):
+    """One torch.optim.SGD step with momentum (the buffer is seeded on the first step)."""
+    p, g, b = _real_view(param), _real_view(grad), _real_view(momentum_buffer)
+    for name, t in (("param", p), ("grad", g), ("momentum_buffer", b)):
+        _req(t, name, torch.float32)
+    _lib.check(_lib.lib().ptycho_sgd_momentum_step(_p(p), _p(g), _p(b), p.numel(), float(lr), _p(lr_tensor),
+                                                   float(weight_decay), float(momentum), float(dampening),
+                                                   int(bool(nesterov)), int(bool(first)), _stream()),
+               "sgd_momentum_step")

@@ -376,3 +376,27 @@ def test_probe_orthogonalization_kernels_match_fp64_oracle(cuda_device, P, n):
     loss = torch.sum(torch.real(torch.conj(torch.tensor(gs, dtype=torch.complex64, device=cuda_device)) * out))
     loss.backward()
     assert rel(pt.grad.cpu().numpy(), g_o) < TOL_G
+
+
+@pytest.mark.parametrize("kind,kw", [
+    ("adam", {"amsgrad": True}), ("adamw", {"amsgrad": True, "weight_decay": 0.05}),
+    ("sgd", {"momentum": 0.9}), ("sgd", {"momentum": 0.8, "dampening": 0.3, "weight_decay": 0.01}),
+    ("sgd", {"momentum": 0.9, "nesterov": True})])
+def test_fused_optimiser_options_match_torch(cuda_device, kind, kw):
+    """AMSGrad and SGD momentum / dampening / Nesterov of the fused optimisers against
+    torch.optim on complex parameters (optimizer_mixin.py:117-123)."""
+    from quantem_b200 import engine
+
+    torch.manual_seed(1)
+    p = torch.randn(3000, dtype=torch.complex64, device=cuda_device).requires_grad_(True)
+    p_ref = p.detach().clone().requires_grad_(True)
+    lr = 5e-3 if kind != "sgd" else 0.05
+    ref_cls = {"adam": torch.optim.Adam, "adamw": torch.optim.AdamW, "sgd": torch.optim.SGD}[kind]
+    opt_ref = ref_cls([p_ref], lr=lr, **kw)
+    opt = engine.make_optimizer([p], {"type": kind, "lr": lr, **kw})
+    for _ in range(5):
+        g = torch.randn_like(p)
+        p.grad, p_ref.grad = g.clone(), g.clone()
+        opt.step()
+        opt_ref.step()
+    assert rel(p.detach().cpu().numpy(), p_ref.detach().cpu().numpy()) < 1e-6
