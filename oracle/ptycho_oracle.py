@@ -1020,15 +1020,20 @@ def fourier_projection_seed(far: np.ndarray, targets: np.ndarray) -> np.ndarray:
     return mod - far
 
 
-def analytic_gradients(obj_raw, probe_raw, positions_px, props, targets, orthogonalize=False, obj_type="complex"):
+def analytic_gradients(obj_raw, probe_raw, positions_px, props, targets, orthogonalize=False, obj_type="complex",
+                       obj_c=None, probe_o=None):
     """Object and probe update directions of the analytic path, as
     ``Ptychography.backward(autograd=False)`` leaves them in ``.grad``
     (ptychography.py:339-348, object_models.py:686-725, probe_models.py:774-783).
     ``obj_type``: complex and pure-phase objects take sum_patches(conj(psi) g); a potential
     takes the real sum_patches(Re(-i conj(o) conj(psi) g)) with o its transmission patches.
+    ``obj_c`` / ``probe_o`` (optional) replace the default hard-constrained transmission and
+    probe, for the optional constraints, which act through the forward model only.
     """
-    obj_c = constrain_object(obj_raw) if obj_type == "complex" else object_transmission(obj_raw, obj_type)
-    probe_o = gram_schmidt(probe_raw)[0] if orthogonalize else probe_raw
+    if obj_c is None:
+        obj_c = constrain_object(obj_raw) if obj_type == "complex" else object_transmission(obj_raw, obj_type)
+    if probe_o is None:
+        probe_o = gram_schmidt(probe_raw)[0] if orthogonalize else probe_raw
     S = obj_c.shape[0]
     P, H, W = probe_o.shape
     st = forward(obj_c, probe_o, positions_px, props)

@@ -869,14 +869,13 @@ class Ptychography:
                         raise NotImplementedError("the analytic update applies to pixelated objects (autograd=True)")
                     if self.dset.batch_descan() is not None:
                         raise NotImplementedError("learned descan shifts need autograd=True")
-                    if self.obj_model._ext_constraints() or self.obj_model.has_soft_constraints:
-                        raise NotImplementedError("the optional object constraints need autograd=True")
-                    if self.probe_model.has_soft_constraints or self.probe_model.constraints.get("center_probe"):
-                        raise NotImplementedError("the optional probe constraints need autograd=True")
+                    # the optional constraints act through the forward model only, as in the
+                    # reference: the update directions are applied to the raw parameters, and
+                    # the soft terms join the loss value but not the directions
                     with torch.no_grad():
                         probe_o = self.probe_model.probe.detach().contiguous()
                         obj_type = self.obj_model.obj_type
-                        if obj_type == "complex":
+                        if obj_type == "complex" and not self.obj_model._ext_constraints():
                             obj_c, _ = ops.obj_constrain(self.obj_model._obj.detach().contiguous())
                         else:
                             obj_c = self.obj_model.transmission().detach().contiguous()
@@ -888,9 +887,13 @@ class Ptychography:
                             # Im(conj(o) sum_patches conj(psi) g): every patch covering a pixel
                             # carries that pixel's transmission o
                             g_obj = (obj_c.conj() * g_obj).imag.contiguous()
+                        closs = loss
+                        if self.obj_model.has_soft_constraints:
+                            loss = loss + self.obj_model.apply_soft_constraints(self.obj_model.obj).detach()
+                        if self.probe_model.has_soft_constraints:
+                            loss = loss + self.probe_model.apply_soft_constraints(probe_o).detach()
                     self.obj_model._obj.grad = g_obj
                     self.probe_model._probe.grad = g_probe
-                    closs = loss
                 for o in opts:
                     o.step()
                 total += loss.detach()

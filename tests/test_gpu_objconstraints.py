@@ -207,3 +207,39 @@ def test_reconstruct_with_object_constraints_like_reference(cuda_device, case):
         obj_mask=z["fov_mask"].astype(np.float64), obj_sampling=tuple(z["obj_sampling"]))
     got = pt.obj_model._obj.detach().cpu().numpy()
     assert rel(got, obj64) < max(3 * rel(z["recon_obj"], obj64), 1e-5)
+
+
+@pytest.mark.parametrize("case", ["complex", "potential"])
+def test_analytic_update_with_optional_constraints(cuda_device, case):
+    """reconstruct(autograd=False) with the optional object constraints and the probe's
+    centre-of-mass shift and TV term: the constraints shape the forward model, the update
+    directions land on the raw parameters (object_models.py:686-725, probe_models.py:774-783),
+    and the soft terms join the loss only.  One full-batch pass with zero-step SGD against the
+    FP64 oracle's analytic directions on the oracle's constrained object and probe."""
+    obj_type, cons = OBJCONS_CASES[case]
+    z = load_golden(f"objcons_{case}64")
+    dev = cuda_device
+    pt = _dropin(z, dev, obj_type)
+    pcons = {"orthogonalize_probe": True, "center_probe": True, "tv_weight": 0.05}
+    pt.reconstruct(num_iters=1, batch_size=pt.dset.num_gpts, autograd=False,
+                   optimizer_params={"object": {"type": "sgd", "lr": 0.0}, "probe": {"type": "sgd", "lr": 0.0}},
+                   constraints={"object": dict(cons), "probe": dict(pcons)}, device="gpu")
+    H = int(z["H"])
+    raw = z["obj_perturbed"].astype(np.complex128 if obj_type != "potential" else np.float64)
+    mask = z["fov_mask"].astype(np.float64)
+    ext = O._ext_args(cons, mask, raw.shape[-2:], tuple(z["obj_sampling"]))
+    obj2 = O.constrain_object_ext(raw, obj_type, **ext)
+    obj_c = np.exp(1j * obj2) if obj_type == "potential" else obj2
+    probe_c, _ = O.constrain_probe(z["probe_init"].astype(np.complex128), pcons)
+    g_obj, g_probe, _ = O.analytic_gradients(raw, None, z["positions"].astype(np.float64),
+                                             z["propagators"].astype(np.complex128), z["targets"].astype(np.float64),
+                                             obj_type=obj_type, obj_c=obj_c, probe_o=probe_c)
+    assert rel(pt.obj_model._obj.grad.cpu().numpy(), g_obj) < 2e-4
+    assert rel(pt.probe_model._probe.grad.cpu().numpy(), g_probe) < 2e-4
+    soft, _ = O.soft_constraint_loss(obj2, obj_type, cons.get("tv_weight_z", 0), cons.get("tv_weight_xy", 0),
+                                     cons.get("surface_zero_weight", 0))
+    tv, _ = O.probe_tv_loss(probe_c, pcons["tv_weight"])
+    st = O.forward(obj_c, probe_c, z["positions"].astype(np.float64), z["propagators"].astype(np.complex128))
+    cl, _ = O.loss_and_seed(st.intensity, z["targets"].astype(np.float64), np.ones((H, H)),
+                            z["positions"].shape[0], float(z["mean_intensity"]))
+    assert abs(pt.iter_losses[0] - (cl + soft + tv)) <= 1e-4 * abs(cl + soft + tv)
