@@ -215,6 +215,13 @@ class CNN2d(torch.nn.Module):
     def eval(self):
         return self.train(False)
 
+    def config(self) -> dict:
+        """Construction arguments (a checkpoint rebuilds the network from them)."""
+        return dict(in_channels=self.in_channels, out_channels=self.out_channels, start_filters=self.start_filters,
+                    num_layers=self.num_layers, num_per_layer=self._num_per_layer,
+                    use_skip_connections=self.use_skip_connections, use_batchnorm=self._use_batchnorm,
+                    final_activation="relu" if self._final_relu else "identity")
+
     def state_dict(self, *args, **kwargs):
         """Parameters and batch-norm buffers under the reference's module names, torch layouts."""
         return self._export(self.flat.data, buffers=True)
@@ -801,6 +808,14 @@ class ComplexCNN2d(torch.nn.Module):
         return torch.complex(y[:, :C], y[:, C:])
 
     __call__ = forward
+
+    def config(self) -> dict:
+        """Construction arguments (a checkpoint rebuilds the network from them)."""
+        r = self.real
+        return dict(in_channels=self.in_channels, out_channels=self.out_channels, start_filters=self.start_filters,
+                    num_layers=self.num_layers, num_per_layer=r._num_per_layer,
+                    use_skip_connections=self.use_skip_connections, use_batchnorm=r._use_batchnorm,
+                    final_activation="relu" if r._final_relu else "identity")
 
     def state_dict(self, *args, **kwargs):
         from .complex_map import real_to_complex_state

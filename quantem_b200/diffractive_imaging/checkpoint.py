@@ -59,16 +59,56 @@ def _restore_opt_state(model, st, num_iter=None):
 def _object_state(obj):
     from .object_models import ObjectDIP
 
+    dip = isinstance(obj, ObjectDIP)
     state = {"class": type(obj).__name__, "obj_type": obj.obj_type, "initialize_mode": obj._initialize_mode,
              "num_slices": obj.num_slices, "slice_thicknesses": obj.slice_thicknesses.tolist(),
              "rng_seed": obj._rng_seed, "constraints": dict(obj.constraints),
-             "obj": _cpu(obj._obj), "initial_obj": _cpu(obj._initial_obj), "sampling": obj._sampling,
-             "mask": _cpu(obj.mask) if isinstance(obj.mask, torch.Tensor) else None}
-    if isinstance(obj, ObjectDIP):
-        raise NotImplementedError("checkpointing a DIP object model is not supported; save the network "
-                                  "weights with torch.save(obj_model.model.state_dict())")
+             "obj": None if dip else _cpu(obj._obj), "initial_obj": None if dip else _cpu(obj._initial_obj),
+             "sampling": obj._sampling, "mask": _cpu(obj.mask) if isinstance(obj.mask, torch.Tensor) else None}
+    if dip:
+        # the network (class, construction arguments, weights and batch-norm statistics), its
+        # input, pre-training target and weights, and the input-noise generator's state
+        m = obj.model
+        state["dip"] = {"model_class": type(m).__name__, "model_config": m.config(),
+                        "model_state": {k: _cpu(v) for k, v in m.state_dict().items()},
+                        "model_input": _cpu(obj._model_input), "pretrain_target": _cpu(obj._pretrain_target),
+                        "pretrained_weights": None if obj._pretrained_weights is None else
+                        {k: _cpu(v) for k, v in obj._pretrained_weights.items()},
+                        "pretrain_losses": list(obj._pretrain_losses), "pretrain_lrs": list(obj._pretrain_lrs),
+                        "input_noise_std": obj._input_noise_std,
+                        "noise_generator": None if obj._gen is None else obj._gen.get_state()}
     state.update(_opt_state(obj))
     return state
+
+
+def _build_dip(os_, device):
+    """The DIP object model of a checkpoint, its network rebuilt on ``device`` (CUDA)."""
+    from ..core import config
+    from ..core.ml.cnn import CNN2d, ComplexCNN2d
+    from .object_models import ObjectDIP
+
+    d = os_["dip"]
+    dev = torch.device(config.validate_device(device if device is not None else "gpu")[0])
+    if dev.type != "cuda":
+        raise ValueError("a DIP object model is restored onto a CUDA device (its network runs there)")
+    mcls = ComplexCNN2d if d["model_class"] == "ComplexCNN2d" else CNN2d
+    model = mcls(**d["model_config"], device=dev)
+    model.load_state_dict({k: v.to(dev) for k, v in d["model_state"].items()})
+    th = os_["slice_thicknesses"]
+    obj = ObjectDIP.from_model(model, d["model_input"].to(dev), num_slices=os_["num_slices"],
+                               slice_thicknesses=np.asarray(th) if th else None,
+                               input_noise_std=d["input_noise_std"], device=dev, obj_type=os_["obj_type"],
+                               rng=os_["rng_seed"])
+    if d["pretrained_weights"] is not None:
+        obj._pretrained_weights = {k: v.to(dev) for k, v in d["pretrained_weights"].items()}
+    if d["pretrain_target"] is not None and d["pretrain_target"].numel():
+        obj.pretrain_target = d["pretrain_target"].to(dev)
+    obj._pretrain_losses = list(d["pretrain_losses"])
+    obj._pretrain_lrs = list(d["pretrain_lrs"])
+    if d["noise_generator"] is not None:
+        obj._gen = torch.Generator(device=dev)
+        obj._gen.set_state(d["noise_generator"])
+    return obj, dev
 
 
 def _probe_state(probe):
@@ -164,11 +204,16 @@ def from_state(cls, state, dset=None, device=None, verbose=None):
     elif not dset.preprocessed:
         dset.preprocess(probe_energy=ds["probe_energy"], plot_rotation=False, plot_com=False,
                         **ds["preprocessing_params"])
-    if os_["class"] != "ObjectPixelated":
+    dip = os_["class"] == "ObjectDIP"
+    if os_["class"] not in ("ObjectPixelated", "ObjectDIP"):
         raise NotImplementedError(f"object model {os_['class']} cannot be restored from a checkpoint")
-    th = os_["slice_thicknesses"]
-    obj = ObjectPixelated(os_["num_slices"], th if th else None, os_["obj_type"], os_["initialize_mode"],
-                          "cpu", os_["rng_seed"], _token=ObjectPixelated._token)
+    build_dev = "cpu"
+    if dip:  # the network lives on its device from the start
+        obj, build_dev = _build_dip(os_, device)
+    else:
+        th = os_["slice_thicknesses"]
+        obj = ObjectPixelated(os_["num_slices"], th if th else None, os_["obj_type"], os_["initialize_mode"],
+                              "cpu", os_["rng_seed"], _token=ObjectPixelated._token)
     probe = ProbePixelated(pr["num_probes"], pr["probe_params"], tuple(pr["probe_tilt"]),
                            bool(pr.get("learn_probe_tilt", False)), pr["roi_shape"],
                            torch.complex64, "cpu", pr["rng_seed"], pr["initial_probe_weights"], None,
@@ -176,14 +221,15 @@ def from_state(cls, state, dset=None, device=None, verbose=None):
     if pr["initial_probe"] is not None:
         probe._initial_probe = pr["initial_probe"].clone()
         probe._from_params = False  # the initial probe is restored as saved, no regeneration
-    pt = cls.from_models(dset, obj, probe, DetectorPixelated(), device="cpu",
+    pt = cls.from_models(dset, obj, probe, DetectorPixelated(), device=build_dev,
                          verbose=ps["verbose"] if verbose is None else verbose)
     probe._from_params = pr["from_params"]
     pt._obj_padding_force_power2_level = ps["power2_level"]
     pt.obj_padding_px = ps["obj_padding_px"]
     # raw parameters and initial values exactly as saved
-    obj._initial_obj = os_["initial_obj"].clone()
-    obj._obj = os_["obj"].clone().requires_grad_(True)
+    if not dip:
+        obj._initial_obj = os_["initial_obj"].clone()
+        obj._obj = os_["obj"].clone().requires_grad_(True)
     obj.constraints = os_["constraints"]
     if os_["mask"] is not None:
         obj.mask = os_["mask"]
@@ -212,7 +258,7 @@ def from_state(cls, state, dset=None, device=None, verbose=None):
     pt._snapshots = list(ps["snapshots"])
     pt._preprocessed = True
     # device first: moving a model re-creates its optimiser, so states are loaded after the move
-    pt.to(device if device is not None else "cpu")
+    pt.to(device if device is not None else build_dev)
     pt.compute_propagator_arrays()
     _restore_opt_state(obj, os_)
     _restore_opt_state(probe, pr)

@@ -58,3 +58,55 @@ def test_resume_equals_uninterrupted(cuda_device, tmp_path, raw):
     np.testing.assert_allclose(losses, losses_a, rtol=1e-6)
     assert rel(obj, obj_a) <= 3 * spread + 1e-6
     assert rel(probe, probe_a) <= 3 * spread + 1e-6
+
+
+@pytest.mark.parametrize("complex_net", [False, True])
+def test_dip_resume_equals_uninterrupted(cuda_device, tmp_path, complex_net):
+    """A DIP reconstruction (real or complex network, input noise on) saved after 2 iterations
+    and resumed equals 4 uninterrupted iterations: network weights, batch-norm statistics,
+    Adam moments and the input-noise generator all come back.  The BF16 GEMMs reduce split-K
+    partials with float atomics, so the bar is the run-to-run spread of uninterrupted runs."""
+    from quantem_b200.core.ml.cnn import CNN2d, ComplexCNN2d
+    from quantem_b200.diffractive_imaging import ObjectDIP, Ptychography
+
+    z = load_golden("mixed64")
+    opt = {"object": {"type": "adam", "lr": 1e-3}, "probe": {"type": "adam"}}
+
+    def fresh():
+        base = _fresh(z)
+        S = base.obj_model.num_slices
+        net = (ComplexCNN2d if complex_net else CNN2d)(S, S, start_filters=8, num_layers=3, device=cuda_device,
+                                                       seed=7)
+        dip = ObjectDIP.from_pixelated(net, base.obj_model, input_noise_std=0.01)
+        pt = Ptychography.from_models(dset=base.dset, obj_model=dip, probe_model=base.probe_model,
+                                      detector_model=base.detector_model, device="gpu", verbose=0,
+                                      rng=int(z["recon_rng_seed"]))
+        pt.preprocess(obj_padding_px=base.obj_padding_px)
+        return pt
+
+    def state(pt):
+        return (pt.obj_model.model.state_dict(), pt.probe_model._probe.detach().cpu().numpy(),
+                np.asarray(pt.iter_losses))
+
+    runs = []
+    for _ in range(2):
+        pt = fresh()
+        pt.reconstruct(num_iters=4, batch_size=9, optimizer_params=opt, device="gpu")
+        runs.append(state(pt))
+    pt = fresh()
+    pt.reconstruct(num_iters=2, batch_size=9, optimizer_params=opt, device="gpu")
+    path = tmp_path / "dip.pt"
+    pt.save(path, save_raw_data=True, verbose=False)
+    q = Ptychography.from_file(path, device="gpu")
+    assert type(q.obj_model).__name__ == "ObjectDIP" and q.num_iters == 2
+    q.reconstruct(num_iters=2, device="gpu")
+    sd, probe, losses = state(q)
+    (sd_a, probe_a, losses_a), (sd_b, probe_b, losses_b) = runs
+    assert losses.shape == (4,)
+    keys = [k for k in sd_a if sd_a[k].is_floating_point() or sd_a[k].is_complex()]
+    w = lambda d: np.concatenate([d[k].detach().cpu().numpy().ravel().view(np.float32) if d[k].is_complex()
+                                  else d[k].detach().cpu().numpy().ravel().astype(np.float32) for k in keys])
+    spread = max(rel(w(sd_b), w(sd_a)), rel(probe_b, probe_a))
+    np.testing.assert_allclose(losses, losses_a, rtol=max(1e-5, 10 * spread))
+    assert rel(w(sd), w(sd_a)) <= 3 * spread + 1e-5
+    assert rel(probe, probe_a) <= 3 * spread + 1e-5
