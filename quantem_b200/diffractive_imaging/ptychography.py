@@ -815,12 +815,16 @@ class Ptychography:
             nvtx.range_push(f"reconstruct iteration {self.num_iters}")
             total = torch.zeros((), dtype=torch.float32, device=dev)
             nb = 0
-            # the batch order goes up before the next targets copy takes the copy engine
+            # the batch order goes up before the next targets copy takes the copy engine: that
+            # copy waits for the order's upload (when the host runs iterations ahead, both would
+            # otherwise become ready together and the order could queue behind the targets)
             batches = device_batches(batcher, dev)
             if stream is not None:
                 tg = stream.acquire()
                 if a0 + 1 < num_iters:
-                    stream.prefetch_next()
+                    uploaded = torch.cuda.Event()
+                    uploaded.record()
+                    stream.prefetch_next(after=uploaded)
             consistency = torch.zeros((), dtype=torch.float32, device=dev)
             for idx in batches:
                 nvtx.range_push("batch")

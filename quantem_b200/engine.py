@@ -230,10 +230,12 @@ class HostTargetStream:
         self.bytes_per_copy = host.numel() * host.element_size()
         self._issue(0)
 
-    def _issue(self, i):
+    def _issue(self, i, after=None):
         with torch.cuda.stream(self.stream):
             if self.free[i] is not None:
                 self.stream.wait_event(self.free[i])
+            if after is not None:
+                self.stream.wait_event(after)
             self.buf[i].copy_(self.host, non_blocking=True)
             self.ready[i].record(self.stream)
 
@@ -242,8 +244,10 @@ class HostTargetStream:
         torch.cuda.current_stream(self.device).wait_event(self.ready[i])
         return self.buf[i]
 
-    def prefetch_next(self):
-        self._issue((self.k + 1) % 2)
+    def prefetch_next(self, after=None):
+        """Start the next copy; with ``after`` (an event) it also waits for that event, so a
+        small copy the current stream issued before it is not queued behind this transfer."""
+        self._issue((self.k + 1) % 2, after)
 
     def release(self):
         i = self.k % 2
