@@ -127,16 +127,64 @@ def maxpool2_bwd(dy, arg, shape):
 
 
 # ----------------------------------------------------------------------------- network
+ACTIVATIONS = {"relu": "relu", "leaky_relu": "leaky_relu", "leakyrelu": "leaky_relu", "lrelu": "leaky_relu",
+               "elu": "elu", "tanh": "tanh", "sigmoid": "sigmoid", "softplus": "softplus",
+               "identity": None, "eye": None, "ident": None}
+
+
+def act_fwd(name, z):
+    """The real activations of activation_functions.py:166-181 (torch defaults: leaky slope
+    0.01, ELU alpha 1, softplus beta 1 with threshold 20)."""
+    if name is None:
+        return z
+    if name == "relu":
+        return np.maximum(z, 0.0)
+    if name == "leaky_relu":
+        return np.where(z > 0, z, 0.01 * z)
+    if name == "elu":
+        return np.where(z > 0, z, np.expm1(np.minimum(z, 0.0)))
+    if name == "tanh":
+        return np.tanh(z)
+    if name == "sigmoid":
+        return 1.0 / (1.0 + np.exp(-z))
+    if name == "softplus":
+        return np.where(z > 20, z, np.log1p(np.exp(np.minimum(z, 20.0))))
+    raise ValueError(name)
+
+
+def act_grad(name, z):
+    """d act / dz at the pre-activation z."""
+    if name is None:
+        return np.ones_like(z)
+    if name == "relu":
+        return (z > 0).astype(z.dtype)
+    if name == "leaky_relu":
+        return np.where(z > 0, 1.0, 0.01)
+    if name == "elu":
+        return np.where(z > 0, 1.0, np.exp(np.minimum(z, 0.0)))
+    if name == "tanh":
+        return 1.0 - np.tanh(z) ** 2
+    if name == "sigmoid":
+        s = 1.0 / (1.0 + np.exp(-z))
+        return s * (1.0 - s)
+    if name == "softplus":
+        return np.where(z > 20, 1.0, 1.0 / (1.0 + np.exp(-np.minimum(z, 20.0))))
+    raise ValueError(name)
+
+
 class CNN2dOracle:
     """CNN2d (cnn.py:17-212) in FP64 from a reference-format state dict."""
 
     def __init__(self, sd: dict, in_channels, out_channels, start_filters, num_layers, num_per_layer,
                  use_skip_connections=True, use_batchnorm=True, final_relu=False, emulate_bf16=False,
-                 momentum=0.1, eps=1e-5):
+                 momentum=0.1, eps=1e-5, activation="relu", final_activation=None):
         self.sd = {k: np.array(v, dtype=np.float64) for k, v in sd.items()}
         self.cin, self.cout, self.sf = in_channels, out_channels, start_filters
         self.L, self.npl = num_layers, num_per_layer
-        self.skip, self.bn, self.final_relu = use_skip_connections, use_batchnorm, final_relu
+        self.skip, self.bn = use_skip_connections, use_batchnorm
+        self.act = ACTIVATIONS[str(activation).lower()]
+        fa = final_activation if final_activation is not None else ("relu" if final_relu else "identity")
+        self.final_act = ACTIVATIONS[str(fa).lower()]
         self.emu = emulate_bf16
         self.momentum, self.eps = momentum, eps
         self.r = bf16 if emulate_bf16 else (lambda a: a)
@@ -151,9 +199,10 @@ class CNN2dOracle:
     def _conv_layer(self, x, prefix, j, training, tape, with_bn=True, relu=True):
         cname, bname = self._conv_names(prefix, j) if with_bn else (f"{prefix}.block.{2 * j}", None)
         z = conv3x3_circ(x, self._w(cname + ".weight"), self.sd[cname + ".bias"])
-        a = np.maximum(z, 0.0) if relu else z
+        act = self.act if relu else None
+        a = act_fwd(act, z)
         if bname is None:
-            tape.append(("conv", prefix, j, x, a, None, relu, with_bn))
+            tape.append(("conv", prefix, j, x, a, None, (act, z), with_bn))
             return a if not with_bn else self.r(a)
         if training:
             y, cache = batchnorm_train(a, self.sd[bname + ".weight"], self.sd[bname + ".bias"], self.eps)
@@ -162,7 +211,7 @@ class CNN2dOracle:
             y = batchnorm_eval(a, self.sd[bname + ".weight"], self.sd[bname + ".bias"],
                                self.sd[bname + ".running_mean"], self.sd[bname + ".running_var"], self.eps)
             cache = None
-        tape.append(("conv", prefix, j, x, a, cache, relu, with_bn))
+        tape.append(("conv", prefix, j, x, a, cache, (act, z), with_bn))
         return self.r(y)
 
     def _update_running(self, bname, a, cache):
@@ -210,8 +259,8 @@ class CNN2dOracle:
                 y = np.concatenate([y, skips[self.L - 1 - u]], axis=1)
             x = self._block(y, f"up_conv_blocks.{u}", training, tape)
         z = conv3x3_circ(x, self._w("final_conv.block.0.weight"), self.sd["final_conv.block.0.bias"])
-        out = np.maximum(z, 0.0) if self.final_relu else z
-        tape.append(("final", x, out))
+        out = act_fwd(self.final_act, z)
+        tape.append(("final", x, z))
         self.tape = tape
         self.training = training
         return out
@@ -224,10 +273,8 @@ class CNN2dOracle:
         """Gradients of sum(out * dout): (dx, {param name: grad}) for the last forward."""
         grads = {}
         tape = list(self.tape)
-        _, xin, out = tape.pop()
-        g = np.asarray(dout, dtype=np.float64)
-        if self.final_relu:
-            g = g * (out > 0)
+        _, xin, zf = tape.pop()
+        g = np.asarray(dout, dtype=np.float64) * act_grad(self.final_act, zf)
         dxf, dw, db = conv3x3_circ_bwd(xin, self._w("final_conv.block.0.weight"), self._dz(g))
         grads["final_conv.block.0.weight"] = dw
         grads["final_conv.block.0.bias"] = g.sum(axis=(0, 2, 3))
@@ -267,14 +314,14 @@ class CNN2dOracle:
 
     def _block_bwd(self, g, prefix, tape, grads, need_dx_first=True):
         for j in range(self.npl - 1, -1, -1):
-            _, pre, jj, x, a, cache, relu, with_bn = tape.pop()
+            _, pre, jj, x, a, cache, (act, z), with_bn = tape.pop()
             assert pre == prefix and jj == j
             cname, bname = self._conv_names(prefix, j)
             if bname is not None:
                 g, dg, dbb = batchnorm_train_bwd(g, self.sd[bname + ".weight"], cache)
                 grads[bname + ".weight"], grads[bname + ".bias"] = dg, dbb
-            if relu:
-                g = g * (a > 0)
+            if act is not None:
+                g = g * act_grad(act, z)
             grads[cname + ".bias"] = g.sum(axis=(0, 2, 3))
             dx, dw, _ = conv3x3_circ_bwd(x, self._w(cname + ".weight"), self._dz(g))
             grads[cname + ".weight"] = dw

@@ -34,14 +34,26 @@ CASES = {
 }
 
 
-def run_case(name, cfg):
+# the other real activations of the reference (activation_functions.py:166-181) on a
+# small U-Net: name: (config as above, hidden activation, final activation)
+ACT_CASES = {
+    "cnn_act_leaky_relu": ((4, 3, 8, 2, 2, True, True, 2, 16, 16), "leaky_relu", "identity"),
+    "cnn_act_elu": ((4, 3, 8, 2, 2, True, True, 2, 16, 16), "elu", "sigmoid"),
+    "cnn_act_tanh": ((4, 2, 8, 1, 2, True, False, 2, 16, 16), "tanh", "tanh"),
+    "cnn_act_sigmoid": ((4, 3, 8, 2, 2, False, True, 2, 16, 16), "sigmoid", "softplus"),
+    "cnn_act_softplus": ((4, 3, 8, 2, 2, True, True, 2, 16, 16), "softplus", "relu"),
+}
+
+
+def run_case(name, cfg, activation="relu", final_activation="identity"):
     import torch
     from quantem.core.ml.cnn import CNN2d
 
     cin, cout, sf, L, npl, skip, bn, B, H, W = cfg
     torch.manual_seed(1234 + len(name))
     net = CNN2d(cin, cout, start_filters=sf, num_layers=L, num_per_layer=npl, use_skip_connections=skip,
-                use_batchnorm=bn, dtype=torch.float32).double()
+                use_batchnorm=bn, dtype=torch.float32, activation=activation,
+                final_activation=final_activation).double()
     net.train()
     g = torch.Generator().manual_seed(99)
     x = torch.randn(B, cin, H, W, generator=g, dtype=torch.float64).requires_grad_(True)
@@ -50,7 +62,8 @@ def run_case(name, cfg):
     y = net(x)
     (y * dy).sum().backward()
     out = {"x": x.detach().numpy(), "dy": dy.numpy(), "y_train": y.detach().numpy(),
-           "dx": x.grad.numpy(), "config": np.array(cfg[:5] + (int(skip), int(bn)), dtype=np.int64)}
+           "dx": x.grad.numpy(), "config": np.array(cfg[:5] + (int(skip), int(bn)), dtype=np.int64),
+           "activation": np.asarray(activation), "final_activation": np.asarray(final_activation)}
     for k, v in sd0.items():
         out["sd/" + k] = v.numpy()
     for k, p in net.named_parameters():  # unused parameters (the upsample bn without batch norm) get zeros
@@ -132,6 +145,10 @@ def main():
         sys.exit(f"usage: python {os.path.relpath(__file__)} <reference source dir (the one holding quantem/)>")
     src = sys.argv[1]
     import_reference(src)
+    if os.environ.get("GOLDEN_ONLY") == "activations":
+        for name, (cfg, act, fin) in ACT_CASES.items():
+            run_case(name, cfg, act, fin)
+        return
     if os.environ.get("GOLDEN_ONLY") != "complex":
         for name, cfg in CASES.items():
             run_case(name, cfg)

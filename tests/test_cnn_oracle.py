@@ -8,6 +8,8 @@ from oracle.cnn_oracle import CNN2dOracle, bf16
 from tests.conftest import load_golden
 
 CASES = ["cnn_unet2", "cnn_unet2_noskip", "cnn_unet1_nobn"]
+# the reference's other real activations (hidden / final), fixtures made with them
+ACT_CASES = ["cnn_act_leaky_relu", "cnn_act_elu", "cnn_act_tanh", "cnn_act_sigmoid", "cnn_act_softplus"]
 
 
 def _rel(a, b):
@@ -17,10 +19,12 @@ def _rel(a, b):
 def oracle_for(z, **kw):
     cfg = [int(c) for c in z["config"]]
     sd = {k[3:]: z[k] for k in z if k.startswith("sd/")}
+    if "activation" in z:
+        kw = dict(activation=str(z["activation"]), final_activation=str(z["final_activation"]), **kw)
     return CNN2dOracle(sd, *cfg[:5], use_skip_connections=bool(cfg[5]), use_batchnorm=bool(cfg[6]), **kw)
 
 
-@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("name", CASES + ACT_CASES)
 def test_cnn_oracle_matches_reference(name):
     z = load_golden(name)
     net = oracle_for(z)
