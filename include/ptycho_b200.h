@@ -373,6 +373,19 @@ int ptycho_forward_loss_noalloc(const ptycho_batch_args* a, float* out_loss, voi
 #define PTYCHO_GEMM_BF16 1   /* store BF16 instead of FP32 */
 #define PTYCHO_GEMM_RELU 2   /* max(x, 0) after the bias */
 #define PTYCHO_GEMM_ATOMIC 4 /* add into FP32 C atomically, C not cleared (splits > 1 without it clears C) */
+/* Activation applied after the bias, in flag bits 8-11: PTYCHO_GEMM_ACT(a) with a one of
+ * PTYCHO_ACT_* (core/ml/activation_functions.py:166-181, torch's default parameters);
+ * PTYCHO_GEMM_RELU is PTYCHO_GEMM_ACT(PTYCHO_ACT_RELU).  Not with atomic / split-K output. */
+#define PTYCHO_GEMM_ACT(a) ((a) << 8)
+enum {
+  PTYCHO_ACT_NONE = 0,
+  PTYCHO_ACT_RELU = 1,
+  PTYCHO_ACT_LEAKY_RELU = 2, /* slope 0.01 */
+  PTYCHO_ACT_ELU = 3,        /* alpha 1 */
+  PTYCHO_ACT_TANH = 4,
+  PTYCHO_ACT_SIGMOID = 5,
+  PTYCHO_ACT_SOFTPLUS = 6    /* beta 1, threshold 20 */
+};
 
 /* C[M][ldc] (op)= A[M][lda] * B[N][ldb]^T (+ bias[N]): BF16 operands, K-major
  * (K contiguous), FP32 accumulation on the tcgen05 tensor cores (TMA-fed
@@ -415,11 +428,12 @@ int ptycho_cnn_bn_forward(const float* x, int ldx, int R, int C, const float* ga
                           float* run_mean, float* run_var, float momentum, float eps, int training, float* mean,
                           float* rstd, double* work, int64_t work_elems, void* out, int ldo, void* stream);
 
-/* Backward of batch norm (gamma != NULL) followed by the ReLU mask of its input x
- * (relu != 0): dz = [x > 0] * dBN(dy).  Writes dgamma / dbeta and dz as FP32
- * and/or BF16 (either may be NULL). */
+/* Backward of batch norm (gamma != NULL) followed by the derivative of the activation that
+ * produced its input x (act = PTYCHO_ACT_*, taken from the activation's output x; 1 = the
+ * ReLU mask [x > 0], 0 = none): dz = act'(x) * dBN(dy).  Writes dgamma / dbeta and dz as
+ * FP32 and/or BF16 (either may be NULL). */
 int ptycho_cnn_bn_backward(const float* dy, int lddy, const float* x, int ldx, int R, int C, const float* gamma,
-                           const float* mean, const float* rstd, int training, int relu, float* dgamma, float* dbeta,
+                           const float* mean, const float* rstd, int training, int act, float* dgamma, float* dbeta,
                            double* work, int64_t work_elems, float* dz32, void* dz16, int ldz, void* stream);
 
 /* out[c] (+)= sum_r a[r][c] (bias gradients), deterministic order. */

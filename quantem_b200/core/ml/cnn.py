@@ -27,6 +27,7 @@ from dataclasses import dataclass
 import torch
 
 from . import kernels as kk
+from .kernels import ACT_IDS
 
 
 def _up8(n: int) -> int:
@@ -39,6 +40,27 @@ class _Seg:
     off: int        # element offset in the flat buffers
     shape: tuple    # shape inside the flat buffer
     numel: int
+
+
+def _activation_name(a) -> str:
+    """Canonical name of an activation given as a string or a torch module (the reference's
+    get_activation_function names, activation_functions.py:150-181)."""
+    if isinstance(a, torch.nn.Module):
+        for cls, name in ((torch.nn.Identity, "identity"), (torch.nn.ReLU, "relu"), (torch.nn.Tanh, "tanh"),
+                          (torch.nn.Sigmoid, "sigmoid")):
+            if type(a) is cls:
+                return name
+        if type(a) is torch.nn.LeakyReLU and a.negative_slope == 0.01:
+            return "leaky_relu"
+        if type(a) is torch.nn.ELU and a.alpha == 1.0:
+            return "elu"
+        if type(a) is torch.nn.Softplus and a.beta == 1.0 and a.threshold == 20.0:
+            return "softplus"
+        raise NotImplementedError(f"activation {a!r} is not one of the B200 kernels' activations")
+    name = str(a).lower()
+    if name not in ACT_IDS:
+        raise NotImplementedError(f"activation {a!r}: the B200 kernels implement {sorted(set(ACT_IDS))}")
+    return {"eye": "identity", "ident": "identity", "leakyrelu": "leaky_relu", "lrelu": "leaky_relu"}.get(name, name)
 
 
 class CNN2d(torch.nn.Module):
@@ -65,11 +87,11 @@ class CNN2d(torch.nn.Module):
             raise NotImplementedError("complex CNN2d is not part of the B200 path (real phase maps only)")
         if dropout:
             raise NotImplementedError("dropout is not implemented on the B200 path")
-        if str(activation).lower() != "relu":
-            raise NotImplementedError(f"activation {activation!r}: the B200 kernels implement relu")
-        fa = "identity" if isinstance(final_activation, torch.nn.Identity) else str(final_activation).lower()
-        if fa not in ("identity", "relu"):
-            raise NotImplementedError(f"final_activation {final_activation!r}: identity or relu")
+        self._act_name = _activation_name(activation)
+        fa = _activation_name(final_activation)
+        self._final_act_name = fa
+        self._act = ACT_IDS[self._act_name]
+        self._final_act = ACT_IDS[fa]
         if self.start_filters % 8:
             raise ValueError("start_filters must be a multiple of 8 (16-byte rows of the BF16 operands)")
         self.use_skip_connections = bool(use_skip_connections)
@@ -220,7 +242,7 @@ class CNN2d(torch.nn.Module):
         return dict(in_channels=self.in_channels, out_channels=self.out_channels, start_filters=self.start_filters,
                     num_layers=self.num_layers, num_per_layer=self._num_per_layer,
                     use_skip_connections=self.use_skip_connections, use_batchnorm=self._use_batchnorm,
-                    final_activation="relu" if self._final_relu else "identity")
+                    activation=self._act_name, final_activation=self._final_act_name)
 
     def state_dict(self, *args, **kwargs):
         """Parameters and batch-norm buffers under the reference's module names, torch layouts."""
@@ -340,8 +362,8 @@ class _Run:
     def empty(self, *shape, dtype=torch.float32):
         return torch.empty(*shape, dtype=dtype, device=self.dev)
 
-    # --- conv3x3 + bias + relu (+ BN) -> bf16 into `out` ------------------------
-    def conv_fwd(self, key, layer, x16, B, H, W, out16, relu=True, final=False):
+    # --- conv3x3 + bias + activation (+ BN) -> bf16 into `out` ------------------
+    def conv_fwd(self, key, layer, x16, B, H, W, out16, act=None, final=False):
         net = self.net
         R = B * H * W
         co = layer["co"]
@@ -349,7 +371,7 @@ class _Run:
         kk.im2col3x3(x16, B, H, W, col)
         w16 = net.view(layer["w"], net.flat16)
         r = self.empty(R, co if not final else co)
-        kk.gemm(col, w16, r, bias=net.view(layer["b"]), relu=relu)
+        kk.gemm(col, w16, r, bias=net.view(layer["b"]), act=net._act if act is None else act)
         del col
         tr = self.net.trace
         if final:
@@ -463,13 +485,13 @@ class _Run:
             out = self.empty(R, up["block"][-1]["co"], dtype=torch.bfloat16)
             y = self.block_fwd(("upc", u), up["block"], src, B, h, w, out)
         fin = net.final
-        r = self.conv_fwd(("final",), fin, y, B, H, W, None, relu=net._final_relu, final=True)
+        r = self.conv_fwd(("final",), fin, y, B, H, W, None, act=net._final_act, final=True)
         out = self.empty(B, net.out_channels, H * W)
         kk.transpose(r.view(B, H * W, net.out_channels), out)
         return out.view(B, net.out_channels, H, W)
 
     # ------------------------------------------------------------------ backward
-    def conv_bwd(self, key, layer, dy, B, H, W, grad, dx_out=None, dx_accumulate=False, relu=True):
+    def conv_bwd(self, key, layer, dy, B, H, W, grad, dx_out=None, dx_accumulate=False, act=None):
         """dy: FP32 gradient w.r.t. the layer output (after BN).  Accumulates the
         weight / bias / BN gradients into `grad` and writes dx (FP32) if asked."""
         net = self.net
@@ -482,12 +504,13 @@ class _Run:
         ldz = _up8(co)
         dz32 = self.empty(R, ldz)[:, :co]
         dz16 = self.empty(R, ldz, dtype=torch.bfloat16)[:, :co]
+        act = net._act if act is None else act
         if layer["bn"] is not None:
             gseg, bseg, _ = layer["bn"]
-            kk.bn_backward(dy, r, net.view(gseg), mean, rstd, self.training, relu, net.view(gseg, grad),
+            kk.bn_backward(dy, r, net.view(gseg), mean, rstd, self.training, act, net.view(gseg, grad),
                            net.view(bseg, grad), self.work, dz32=dz32, dz16=dz16)
         else:
-            kk.bn_backward(dy, r, None, None, None, self.training, relu, None, None, self.work, dz32=dz32, dz16=dz16)
+            kk.bn_backward(dy, r, None, None, None, self.training, act, None, None, self.work, dz32=dz32, dz16=dz16)
         kk.colsum(dz32, net.view(layer["b"], grad), self.work)
         del dz32
         # weight gradient: dW[co][9ci] = dz^T @ col
@@ -530,7 +553,7 @@ class _Run:
         dfin = self.empty(R0, net.out_channels)
         kk.transpose(dout.reshape(B, net.out_channels, H * W), dfin.view(B, H * W, net.out_channels))
         dy = self.empty(R0, net.final["ci_store"])
-        self.conv_bwd(("final",), net.final, dfin, B, H, W, grad, dy, relu=net._final_relu)
+        self.conv_bwd(("final",), net.final, dfin, B, H, W, grad, dy, act=net._final_act)
         dcat = [None] * L
         # decoder, last level first
         for u in range(L - 1, -1, -1):
@@ -696,6 +719,20 @@ class ComplexCNN2d(torch.nn.Module):
 
         if not dtype.is_complex:
             raise ValueError("ComplexCNN2d takes a complex dtype (use CNN2d for real networks)")
+        # Complex_ReLU acts on the real and imaginary parts separately, which the doubled real
+        # network reproduces; modReLU and the phase ReLU couple them and are not built
+        act = str(activation).lower() if not isinstance(activation, torch.nn.Module) else activation
+        if act in ("complexrelu", "complex_relu"):
+            act = "relu"
+        if act != "relu":
+            raise NotImplementedError(f"activation {activation!r}: complex networks take complexrelu")
+        fin = final_activation
+        if isinstance(fin, str) and fin.lower() in ("complexrelu", "complex_relu"):
+            fin = "relu"
+        if _activation_name(fin) not in ("identity", "relu"):
+            raise NotImplementedError(f"final_activation {final_activation!r}: complex networks take identity or "
+                                      "complexrelu")
+        activation, final_activation = act, fin
         self.in_channels = int(in_channels)
         self.out_channels = int(out_channels) if out_channels is not None else int(in_channels)
         self.start_filters = int(start_filters)
@@ -815,7 +852,7 @@ class ComplexCNN2d(torch.nn.Module):
         return dict(in_channels=self.in_channels, out_channels=self.out_channels, start_filters=self.start_filters,
                     num_layers=self.num_layers, num_per_layer=r._num_per_layer,
                     use_skip_connections=self.use_skip_connections, use_batchnorm=r._use_batchnorm,
-                    final_activation="relu" if r._final_relu else "identity")
+                    final_activation=r._final_act_name)
 
     def state_dict(self, *args, **kwargs):
         from .complex_map import real_to_complex_state

@@ -17,6 +17,10 @@ from ... import _lib
 GEMM_BF16 = 1
 GEMM_RELU = 2
 GEMM_ATOMIC = 4
+# activation ids of the GEMM epilogue and the batch-norm backward (core/ml/activation_functions.py:
+# 166-181, torch's default parameters); 0 = identity
+ACT_IDS = {"identity": 0, "eye": 0, "ident": 0, "relu": 1, "leaky_relu": 2, "leakyrelu": 2, "lrelu": 2, "elu": 3,
+           "tanh": 4, "sigmoid": 5, "softplus": 6}
 
 _F32, _BF16 = 0, 1
 
@@ -50,19 +54,20 @@ def _call(name: str, *args):
 
 
 def gemm(A: torch.Tensor, B: torch.Tensor, C: torch.Tensor, bias: torch.Tensor | None = None, relu: bool = False,
-         splits: int = 1, status: torch.Tensor | None = None, accumulate: bool = False) -> torch.Tensor:
-    """C (op)= A @ B.T (+ bias) (ReLU) on the tcgen05 tensor cores.
+         splits: int = 1, status: torch.Tensor | None = None, accumulate: bool = False, act: int = 0) -> torch.Tensor:
+    """C (op)= A @ B.T (+ bias) (activation) on the tcgen05 tensor cores.
 
     A (M, K) and B (N, K) are BF16; C (M, N) is FP32 or BF16.  splits > 1
     splits K over CTAs with FP32 atomics (C is cleared first); accumulate=True
-    adds into FP32 C atomically without clearing it."""
+    adds into FP32 C atomically without clearing it.  ``act`` is an activation id
+    (``ACT_IDS``); ``relu=True`` is act 1."""
     if A.dtype != torch.bfloat16 or B.dtype != torch.bfloat16:
         raise TypeError("gemm operands must be bfloat16")
     M, K = A.shape
     N, K2 = B.shape
     if K2 != K or tuple(C.shape) != (M, N):
         raise ValueError(f"gemm shapes: A {tuple(A.shape)}, B {tuple(B.shape)}, C {tuple(C.shape)}")
-    flags = (GEMM_BF16 if C.dtype == torch.bfloat16 else 0) | (GEMM_RELU if relu else 0) | \
+    flags = (GEMM_BF16 if C.dtype == torch.bfloat16 else 0) | (GEMM_RELU if relu else (int(act) << 8)) | \
         (GEMM_ATOMIC if accumulate else 0)
     _call("ptycho_gemm_bf16", _p(A), _ld(A, "A"), _p(B), _ld(B, "B"), _p(C), _ld(C, "C"), M, N, K, _p(bias), flags,
           int(splits), _p(status), _s())
@@ -116,13 +121,15 @@ def bn_forward(x, gamma, beta, run_mean, run_var, momentum, eps, training, mean,
     return out
 
 
-def bn_backward(dy, x, gamma, mean, rstd, training, relu, dgamma, dbeta, work, dz32=None, dz16=None):
+def bn_backward(dy, x, gamma, mean, rstd, training, act, dgamma, dbeta, work, dz32=None, dz16=None):
+    """Batch-norm backward (gamma given) times the derivative of activation ``act`` (an id of
+    ``ACT_IDS``; True is ReLU) evaluated from its output x."""
     R, C = x.shape
     z = dz32 if dz32 is not None else dz16
     if dz32 is not None and dz16 is not None and dz32.stride(0) != dz16.stride(0):
         raise ValueError("dz32 and dz16 must share a leading dimension")
     _call("ptycho_cnn_bn_backward", _p(dy), _ld(dy, "dy"), _p(x), _ld(x, "x"), R, C, _p(gamma), _p(mean), _p(rstd),
-          int(training), int(relu), _p(dgamma), _p(dbeta), _p(work), work.numel(), _p(dz32), _p(dz16),
+          int(training), int(act), _p(dgamma), _p(dbeta), _p(work), work.numel(), _p(dz32), _p(dz16),
           _ld(z, "dz"), _s())
 
 

@@ -337,13 +337,14 @@ __global__ void bn_apply_kernel(const float* __restrict__ x, int ldx, int R, int
   }
 }
 
-// Batch-norm backward (training statistics) followed by the ReLU mask of its input:
-// dx = [x > 0] * gamma * rstd * (dy - s_dy/R - xhat * s_dyxhat/R); without batch norm
-// (mean null) dx = [x > 0] * dy.  relu = 0 drops the mask.  Writes FP32 and BF16 copies.
+// Batch-norm backward (training statistics) followed by the derivative of the activation
+// that produced its input x: dx = act'(x) * gamma * rstd * (dy - s_dy/R - xhat * s_dyxhat/R);
+// without batch norm (mean null) dx = act'(x) * dy.  act = qb::ACT_* (1 = ReLU: the mask
+// [x > 0]; 0: none).  Writes FP32 and BF16 copies.
 __global__ void bn_relu_backward_kernel(const float* __restrict__ dy, int lddy, const float* __restrict__ x, int ldx,
                                         int R, int C, const float* __restrict__ mean, const float* __restrict__ rstd,
                                         const float* __restrict__ gamma, const float* __restrict__ sdy,
-                                        const float* __restrict__ sdyx, int relu, float* __restrict__ dz32,
+                                        const float* __restrict__ sdyx, int act, float* __restrict__ dz32,
                                         bf16* __restrict__ dz16, int ldz) {
   const int64_t total = (int64_t)R * C;
   const float invR = 1.0f / (float)R;
@@ -356,22 +357,22 @@ __global__ void bn_relu_backward_kernel(const float* __restrict__ dy, int lddy, 
       const float xh = (xv - mean[c]) * rstd[c];
       g = gamma[c] * rstd[c] * (g - sdy[c] * invR - xh * sdyx[c] * invR);
     }
-    if (relu && !(xv > 0.0f)) g = 0.0f;
+    if (act) g *= qb::act_grad_from_output(act, xv);
     if (dz32) dz32[r * ldz + c] = g;
     if (dz16) dz16[r * ldz + c] = __float2bfloat16_rn(g);
   }
 }
 
-// Eval-mode batch-norm backward is a per-channel scale: dx = dy * gamma * rstd (then the mask).
+// Eval-mode batch-norm backward is a per-channel scale: dx = dy * gamma * rstd (then act').
 __global__ void bn_eval_backward_kernel(const float* __restrict__ dy, int lddy, const float* __restrict__ x, int ldx,
                                         int R, int C, const float* __restrict__ rstd, const float* __restrict__ gamma,
-                                        int relu, float* __restrict__ dz32, bf16* __restrict__ dz16, int ldz) {
+                                        int act, float* __restrict__ dz32, bf16* __restrict__ dz16, int ldz) {
   const int64_t total = (int64_t)R * C;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
     const int c = (int)(i % C);
     const int64_t r = i / C;
     float g = dy[r * lddy + c] * gamma[c] * rstd[c];
-    if (relu && !(x[r * ldx + c] > 0.0f)) g = 0.0f;
+    if (act) g *= qb::act_grad_from_output(act, x[r * ldx + c]);
     if (dz32) dz32[r * ldz + c] = g;
     if (dz16) dz16[r * ldz + c] = __float2bfloat16_rn(g);
   }
@@ -515,14 +516,19 @@ int ptycho_gemm_bf16(const void* A, int lda, const void* B, int ldb, void* C, in
     return fail(PTYCHO_ERR_INVALID, "gemm: bad sizes (M=%d N=%d K=%d lda=%d ldb=%d ldc=%d)", M, N, K, lda, ldb, ldc);
   if ((lda & 7) || (ldb & 7) || !al16(A) || !al16(B))
     return fail(PTYCHO_ERR_INVALID, "gemm: A/B must be 16-byte aligned with leading dimensions a multiple of 8");
-  if (flags & ~(EPI_BF16 | EPI_RELU | EPI_ATOMIC)) return fail(PTYCHO_ERR_INVALID, "gemm: unknown flags %d", flags);
+  if (flags & ~(EPI_BF16 | EPI_RELU | EPI_ATOMIC | EPI_ACT_MASK))
+    return fail(PTYCHO_ERR_INVALID, "gemm: unknown flags %d", flags);
+  int act = (flags & EPI_ACT_MASK) >> EPI_ACT_SHIFT;
+  if (act >= qb::ACT_COUNT || ((flags & EPI_RELU) && act && act != qb::ACT_RELU))
+    return fail(PTYCHO_ERR_INVALID, "gemm: bad activation in flags %d", flags);
+  if (flags & EPI_RELU) act = qb::ACT_RELU;
   const int nkb = (K + BK - 1) / BK;
   if (splits < 1) splits = 1;
   if (splits > nkb) splits = nkb;
   const bool accumulate = (flags & EPI_ATOMIC) != 0;  // add into C as it is
   if (splits > 1) flags |= EPI_ATOMIC;
-  if ((flags & EPI_ATOMIC) && (flags & (EPI_BF16 | EPI_RELU)))
-    return fail(PTYCHO_ERR_INVALID, "gemm: split-K / atomic output needs FP32 output without ReLU");
+  if ((flags & EPI_ATOMIC) && ((flags & EPI_BF16) || act))
+    return fail(PTYCHO_ERR_INVALID, "gemm: split-K / atomic output needs FP32 output without an activation");
   if (int rc = encode_fn()) return rc;
   const int kb_per = (nkb + splits - 1) / splits;
   splits = (nkb + kb_per - 1) / kb_per;  // every split gets >= 1 k-block
@@ -535,7 +541,7 @@ int ptycho_gemm_bf16(const void* A, int lda, const void* B, int ldb, void* C, in
     if (cudaMemset2DAsync(C, (size_t)ldc * 4, 0, (size_t)N * 4, (size_t)M, st) != cudaSuccess)
       return check_launch("gemm: clear split-K output");
   }
-  Epilogue epi{C, bias, ldc, flags};
+  Epilogue epi{C, bias, ldc, flags, act};
   switch (BN) {
     case 32: return launch_gemm<32>(ta, tb, M, N, K, splits, kb_per, epi, status, st);
     case 64: return launch_gemm<64>(ta, tb, M, N, K, splits, kb_per, epi, status, st);
@@ -632,9 +638,10 @@ int ptycho_cnn_bn_forward(const float* x, int ldx, int R, int C, const float* ga
 }
 
 int ptycho_cnn_bn_backward(const float* dy, int lddy, const float* x, int ldx, int R, int C, const float* gamma,
-                           const float* mean, const float* rstd, int training, int relu, float* dgamma, float* dbeta,
+                           const float* mean, const float* rstd, int training, int act, float* dgamma, float* dbeta,
                            double* work, int64_t work_elems, float* dz32, void* dz16, int ldz, void* stream) {
-  if (!dy || !x || R < 1 || C < 1 || lddy < C || ldx < C || ldz < C || (!dz32 && !dz16))
+  if (!dy || !x || R < 1 || C < 1 || lddy < C || ldx < C || ldz < C || (!dz32 && !dz16) || act < 0 ||
+      act >= qb::ACT_COUNT)
     return fail(PTYCHO_ERR_INVALID, "bn_backward: bad arguments");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const int g = blocks_for((int64_t)R * C, 256);
@@ -644,14 +651,14 @@ int ptycho_cnn_bn_backward(const float* dy, int lddy, const float* x, int ldx, i
                         nullptr, 0, st))
       return rc;
     if (training)
-      bn_relu_backward_kernel<<<g, 256, 0, st>>>(dy, lddy, x, ldx, R, C, mean, rstd, gamma, dbeta, dgamma, relu, dz32,
+      bn_relu_backward_kernel<<<g, 256, 0, st>>>(dy, lddy, x, ldx, R, C, mean, rstd, gamma, dbeta, dgamma, act, dz32,
                                                  static_cast<bf16*>(dz16), ldz);
     else
-      bn_eval_backward_kernel<<<g, 256, 0, st>>>(dy, lddy, x, ldx, R, C, rstd, gamma, relu, dz32,
+      bn_eval_backward_kernel<<<g, 256, 0, st>>>(dy, lddy, x, ldx, R, C, rstd, gamma, act, dz32,
                                                  static_cast<bf16*>(dz16), ldz);
   } else {
     bn_relu_backward_kernel<<<g, 256, 0, st>>>(dy, lddy, x, ldx, R, C, nullptr, nullptr, nullptr, nullptr, nullptr,
-                                               relu, dz32, static_cast<bf16*>(dz16), ldz);
+                                               act, dz32, static_cast<bf16*>(dz16), ldz);
   }
   return check_launch("bn_backward");
 }

@@ -30,6 +30,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "cnn_act.cuh"
+
 namespace qb {
 namespace gemm {
 
@@ -39,7 +41,8 @@ constexpr int STAGES = 4;
 constexpr int THREADS = 128;
 constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s bound on any single wait
 
-enum : int { EPI_BF16 = 1, EPI_RELU = 2, EPI_ATOMIC = 4 };
+// EPI_RELU is activation 1; bits EPI_ACT_SHIFT.. hold any activation id (qb::ACT_*)
+enum : int { EPI_BF16 = 1, EPI_RELU = 2, EPI_ATOMIC = 4, EPI_ACT_SHIFT = 8, EPI_ACT_MASK = 0xF00 };
 enum : int { GEMM_TIMEOUT = 1 };
 
 struct Epilogue {
@@ -47,6 +50,7 @@ struct Epilogue {
   const float* bias;  // [N] or null
   int ldc;
   int flags;
+  int act;  // qb::ACT_* applied to acc + bias
 };
 
 template <int BN>
@@ -238,7 +242,7 @@ __global__ void __launch_bounds__(THREADS, 1)
 #pragma unroll
       for (int j = 0; j < 16; ++j) {
         if (add_bias && j < ncols) v[j] += epi.bias[col0 + j];
-        if (epi.flags & EPI_RELU) v[j] = fmaxf(v[j], 0.0f);
+        v[j] = act_forward(epi.act, v[j]);
       }
       const size_t off = size_t(row) * epi.ldc + col0;
       if (epi.flags & EPI_ATOMIC) {

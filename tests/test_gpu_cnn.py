@@ -24,7 +24,10 @@ from tests.conftest import load_golden
 
 pytestmark = pytest.mark.gpu
 
-CASES = ["cnn_unet2", "cnn_unet2_noskip", "cnn_unet1_nobn"]
+CASES = ["cnn_unet2", "cnn_unet2_noskip", "cnn_unet1_nobn",
+         # the reference's other real activations (hidden / final): leaky ReLU / identity,
+         # ELU / sigmoid, tanh / tanh, sigmoid / softplus, softplus / ReLU
+         "cnn_act_leaky_relu", "cnn_act_elu", "cnn_act_tanh", "cnn_act_sigmoid", "cnn_act_softplus"]
 
 
 def _rel(a, b):
@@ -41,8 +44,11 @@ def _crel(a, b):
 
 def _cfg(z):
     c = [int(v) for v in z["config"]]
-    return dict(in_channels=c[0], out_channels=c[1], start_filters=c[2], num_layers=c[3], num_per_layer=c[4],
-                use_skip_connections=bool(c[5]), use_batchnorm=bool(c[6]))
+    cfg = dict(in_channels=c[0], out_channels=c[1], start_filters=c[2], num_layers=c[3], num_per_layer=c[4],
+               use_skip_connections=bool(c[5]), use_batchnorm=bool(c[6]))
+    if "activation" in z:
+        cfg.update(activation=str(z["activation"]), final_activation=str(z["final_activation"]))
+    return cfg
 
 
 def _flatgrads(d, keys):
