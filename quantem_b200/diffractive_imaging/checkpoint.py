@@ -93,14 +93,14 @@ def _build_dip(os_, device):
         raise ValueError("a DIP object model is restored onto a CUDA device (its network runs there)")
     mcls = ComplexCNN2d if d["model_class"] == "ComplexCNN2d" else CNN2d
     model = mcls(**d["model_config"], device=dev)
-    model.load_state_dict({k: v.to(dev) for k, v in d["model_state"].items()})
+    model.load_state_dict(d["model_state"])  # host tensors: the networks place them themselves
     th = os_["slice_thicknesses"]
     obj = ObjectDIP.from_model(model, d["model_input"].to(dev), num_slices=os_["num_slices"],
                                slice_thicknesses=np.asarray(th) if th else None,
                                input_noise_std=d["input_noise_std"], device=dev, obj_type=os_["obj_type"],
                                rng=os_["rng_seed"])
     if d["pretrained_weights"] is not None:
-        obj._pretrained_weights = {k: v.to(dev) for k, v in d["pretrained_weights"].items()}
+        obj._pretrained_weights = dict(d["pretrained_weights"])
     if d["pretrain_target"] is not None and d["pretrain_target"].numel():
         obj.pretrain_target = d["pretrain_target"].to(dev)
     obj._pretrain_losses = list(d["pretrain_losses"])
