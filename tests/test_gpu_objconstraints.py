@@ -206,7 +206,10 @@ def test_reconstruct_with_object_constraints_like_reference(cuda_device, case):
         np.random.default_rng(int(z["recon_rng_seed"])), obj_type=obj_type, obj_constraints=cons,
         obj_mask=z["fov_mask"].astype(np.float64), obj_sampling=tuple(z["obj_sampling"]))
     got = pt.obj_model._obj.detach().cpu().numpy()
-    assert rel(got, obj64) < max(3 * rel(z["recon_obj"], obj64), 1e-5)
+    # Adam's first steps are ~lr * sign(g): the run-to-run order of the float atomics flips the
+    # sign of near-zero gradient components (many under the Butterworth filters' flat response),
+    # so the floor is 1e-4 (4e-5 measured on one box, below 1e-5 on others)
+    assert rel(got, obj64) < max(3 * rel(z["recon_obj"], obj64), 1e-4)
 
 
 @pytest.mark.parametrize("case", ["complex", "potential"])
