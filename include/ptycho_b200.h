@@ -436,6 +436,11 @@ int ptycho_cnn_bn_backward(const float* dy, int lddy, const float* x, int ldx, i
                            const float* mean, const float* rstd, int training, int act, float* dgamma, float* dbeta,
                            double* work, int64_t work_elems, float* dz32, void* dz16, int ldz, void* stream);
 
+/* Dropout in place (nn.Dropout, core/ml/blocks.py:134-135): x[r][c] *= keep / (1 - p) with
+ * keep = u >= p for a uniform u drawn from a counter-based hash of (seed, r * C + c); the same
+ * seed regenerates the mask for the backward.  dtype 0 = FP32, 1 = BF16; 0 <= p <= 1. */
+int ptycho_cnn_dropout(void* x, int dtype, int R, int C, int ld, float p, uint64_t seed, void* stream);
+
 /* out[c] (+)= sum_r a[r][c] (bias gradients), deterministic order. */
 int ptycho_cnn_colsum(const float* a, int lda, int R, int C, float* out, int accumulate, double* work,
                       int64_t work_elems, void* stream);

@@ -73,6 +73,7 @@ EXPORTED = (
     "ptycho_pattern_bilinear",
     "ptycho_adam_amsgrad_step",
     "ptycho_sgd_momentum_step",
+    "ptycho_cnn_dropout",
     "ptycho_probe_ortho_work_elems",
     "ptycho_probe_orthogonalize",
     "ptycho_probe_orthogonalize_vjp",
@@ -175,6 +176,7 @@ def _declare(lib):
         "ptycho_adam_amsgrad_step": (_int, [_vp, _vp, _vp, _vp, _vp, _i64, _flt, _vp, _flt, _flt, _flt, _flt, _int,
                                              _flt, _flt, _vp]),
         "ptycho_sgd_momentum_step": (_int, [_vp, _vp, _vp, _i64, _flt, _vp, _flt, _flt, _flt, _int, _int, _vp]),
+        "ptycho_cnn_dropout": (_int, [_vp, _int, _int, _int, _int, _flt, ctypes.c_uint64, _vp]),
         "ptycho_probe_ortho_work_elems": (_i64, [_int, _i64]),
         "ptycho_probe_orthogonalize": (_int, [_vp, _vp, _int, _i64, _vp, _i64, _vp]),
         "ptycho_probe_orthogonalize_vjp": (_int, [_vp, _vp, _vp, _int, _i64, _vp, _i64, _vp]),

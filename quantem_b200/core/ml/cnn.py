@@ -85,8 +85,11 @@ class CNN2d(torch.nn.Module):
                              "channel concatenation.")
         if dtype.is_complex:
             raise NotImplementedError("complex CNN2d is not part of the B200 path (real phase maps only)")
-        if dropout:
-            raise NotImplementedError("dropout is not implemented on the B200 path")
+        if not 0.0 <= float(dropout) <= 1.0:
+            raise ValueError(f"dropout must be in [0, 1], got {dropout}")
+        self.dropout = float(dropout)
+        self._dropout_calls = 0
+        self._dropout_seed = int(seed) if seed is not None else 0
         self._act_name = _activation_name(activation)
         fa = _activation_name(final_activation)
         self._final_act_name = fa
@@ -122,14 +125,16 @@ class CNN2d(torch.nn.Module):
 
         self.convs = {}  # prefix -> dict(ci, co, w, b, bn)
         npl, bn = self._num_per_layer, self._use_batchnorm
-        step = 3 if bn else 2
+        # conv, activation, (batch norm), (dropout) per layer of a Conv2dBlock (blocks.py:117-136)
+        drop = 1 if self.dropout > 0 else 0
+        step = (3 if bn else 2) + drop
 
         def conv_block(prefix, ci, co, layers, with_bn=True):
             out = []
             for j in range(layers):
                 cin = ci if j == 0 else co
                 cin_store = self.cin_pad if (prefix == "down_conv_blocks.0" and j == 0) else cin
-                p = f"{prefix}.block.{step * j if with_bn else 2 * j}"
+                p = f"{prefix}.block.{step * j if with_bn else (2 + drop) * j}"
                 w = add(p + ".weight", (co, 9 * cin_store))
                 b = add(p + ".bias", (co,))
                 layer = dict(ci=cin, ci_store=cin_store, co=co, w=w, b=b, bn=None)
@@ -242,7 +247,7 @@ class CNN2d(torch.nn.Module):
         return dict(in_channels=self.in_channels, out_channels=self.out_channels, start_filters=self.start_filters,
                     num_layers=self.num_layers, num_per_layer=self._num_per_layer,
                     use_skip_connections=self.use_skip_connections, use_batchnorm=self._use_batchnorm,
-                    activation=self._act_name, final_activation=self._final_act_name)
+                    activation=self._act_name, final_activation=self._final_act_name, dropout=self.dropout)
 
     def state_dict(self, *args, **kwargs):
         """Parameters and batch-norm buffers under the reference's module names, torch layouts."""
@@ -374,11 +379,14 @@ class _Run:
         kk.gemm(col, w16, r, bias=net.view(layer["b"]), act=net._act if act is None else act)
         del col
         tr = self.net.trace
+        seed = self._next_dropout_seed()
         if final:
-            self.saved[key] = (x16, r, None, None)
+            # the activation's output r stays for the backward; the dropped copy is the output
+            y = r if seed is None else kk.dropout(r.clone(), net.dropout, seed)
+            self.saved[key] = (x16, r, None, None, seed)
             if tr is not None:
                 tr[("fwd",) + key] = dict(x=x16.clone(), r=r.clone())
-            return r
+            return y
         if layer["bn"] is not None:
             gseg, bseg, pref = layer["bn"]
             mean, rstd = self.empty(co), self.empty(co)
@@ -388,10 +396,20 @@ class _Run:
         else:
             mean = rstd = None
             kk.bn_forward(r, None, None, None, None, 0.0, 0.0, False, None, None, self.work, out16)
-        self.saved[key] = (x16, r, mean, rstd)
+        if seed is not None:
+            kk.dropout(out16, net.dropout, seed)
+        self.saved[key] = (x16, r, mean, rstd, seed)
         if tr is not None:
             tr[("fwd",) + key] = dict(x=x16.clone(), r=r.clone(), y=out16.clone())
         return out16
+
+    def _next_dropout_seed(self):
+        """A fresh mask seed per layer and pass in training mode with dropout, else None."""
+        net = self.net
+        if not (self.training and net.dropout > 0):
+            return None
+        net._dropout_calls += 1
+        return (net._dropout_seed * 0x9E3779B1 + net._dropout_calls) & 0xFFFFFFFFFFFF
 
     def block_fwd(self, prefix, layers, x16, B, H, W, out16_last):
         y = x16
@@ -495,7 +513,9 @@ class _Run:
         """dy: FP32 gradient w.r.t. the layer output (after BN).  Accumulates the
         weight / bias / BN gradients into `grad` and writes dx (FP32) if asked."""
         net = self.net
-        x16, r, mean, rstd = self.saved.pop(key)
+        x16, r, mean, rstd, seed = self.saved.pop(key)
+        if seed is not None:  # the forward's dropout mask on the incoming gradient
+            dy = kk.dropout(dy.contiguous().clone(), net.dropout, seed)
         tr = net.trace
         if tr is not None:
             tr[("bwd",) + key] = dict(dy=dy.clone())
@@ -719,6 +739,8 @@ class ComplexCNN2d(torch.nn.Module):
 
         if not dtype.is_complex:
             raise ValueError("ComplexCNN2d takes a complex dtype (use CNN2d for real networks)")
+        if dropout:  # nn.Dropout drops a complex element whole; the doubled real network would not
+            raise NotImplementedError("dropout in complex networks is not part of the B200 path")
         # Complex_ReLU acts on the real and imaginary parts separately, which the doubled real
         # network reproduces; modReLU and the phase ReLU couple them and are not built
         act = str(activation).lower() if not isinstance(activation, torch.nn.Module) else activation

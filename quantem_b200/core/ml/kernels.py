@@ -133,6 +133,14 @@ def bn_backward(dy, x, gamma, mean, rstd, training, act, dgamma, dbeta, work, dz
           _ld(z, "dz"), _s())
 
 
+def dropout(x: torch.Tensor, p: float, seed: int) -> torch.Tensor:
+    """x (R, C) FP32 or BF16, in place: keep / (1 - p) with the mask of ``seed``."""
+    R, C = x.shape
+    _call("ptycho_cnn_dropout", _p(x), _dt(x), R, C, _ld(x, "x"), ctypes.c_float(p),
+          ctypes.c_uint64(int(seed) & 0xFFFFFFFFFFFFFFFF), _s())
+    return x
+
+
 def colsum(a: torch.Tensor, out: torch.Tensor, work: torch.Tensor, accumulate: bool = False):
     R, C = a.shape
     _call("ptycho_cnn_colsum", _p(a), _ld(a, "a"), R, C, _p(out), int(accumulate), _p(work), work.numel(), _s())

@@ -504,6 +504,34 @@ int colsum(int mode, const float* a, int lda, const float* b, int ldb, const flo
 
 }  // namespace
 
+// Dropout (nn.Dropout, blocks.py:134-135): x *= keep / (1 - p) with keep = u >= p, u a
+// uniform draw per element from a counter-based hash of (seed, row * C + column) -- the
+// SplitMix64 finaliser (Steele, Lea and Flood, 2014) -- so the backward regenerates the
+// forward's mask from the same seed instead of storing it.
+__device__ __forceinline__ float dropout_uniform(uint64_t seed, uint64_t i) {
+  uint64_t z = seed + (i + 1) * 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z ^= z >> 31;
+  return (float)(z >> 40) * (1.0f / 16777216.0f);  // 24 random bits in [0, 1)
+}
+
+template <typename T>
+__global__ void dropout_kernel(T* __restrict__ x, int R, int C, int ld, float p, float scale, uint64_t seed) {
+  const int64_t total = (int64_t)R * C;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = i / C;
+    const int c = (int)(i % C);
+    const bool keep = dropout_uniform(seed, (uint64_t)i) >= p;
+    T* e = x + r * ld + c;
+    if constexpr (sizeof(T) == 4) {
+      *e = keep ? *e * scale : 0.0f;
+    } else {
+      *e = keep ? __float2bfloat16_rn(__bfloat162float(*e) * scale) : __float2bfloat16_rn(0.0f);
+    }
+  }
+}
+
 // ===========================================================================
 // C ABI
 // ===========================================================================
@@ -716,6 +744,19 @@ int ptycho_cnn_bin_features(const float* patterns, int npos, int n, int bin, int
   bin_features_kernel<<<blocks_for(total, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
       patterns, npos, n, bin, amplitudes, norm, mean, scale, static_cast<bf16*>(out), ldo);
   return check_launch("bin_features_kernel");
+}
+
+int ptycho_cnn_dropout(void* x, int dtype, int R, int C, int ld, float p, uint64_t seed, void* stream) {
+  if (!x || R < 1 || C < 1 || ld < C || !(p >= 0.0f && p <= 1.0f) || (dtype != 0 && dtype != 1))
+    return fail(PTYCHO_ERR_INVALID, "dropout: bad arguments");
+  const float scale = p < 1.0f ? 1.0f / (1.0f - p) : 0.0f;  // p = 1 drops everything
+  const int g = blocks_for((int64_t)R * C, 256);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (dtype == 0)
+    dropout_kernel<float><<<g, 256, 0, st>>>(static_cast<float*>(x), R, C, ld, p, scale, seed);
+  else
+    dropout_kernel<bf16><<<g, 256, 0, st>>>(static_cast<bf16*>(x), R, C, ld, p, scale, seed);
+  return check_launch("dropout_kernel");
 }
 
 }  // extern "C"

@@ -306,3 +306,46 @@ def test_complex_cnn_matches_reference(cuda_device):
     assert _crel(y, z["y_train"]) < bar(_crel(yo, z["y_train"]))
     assert _crel(dx, z["dx"]) < bar(_crel(dxo, z["dx"]))
     assert _crel(flat(g), gref) < bar(_crel(flat(gco), gref))
+
+
+def test_cnn_dropout(cuda_device):
+    """CNN2d(dropout=p) (nn.Dropout after each conv layer's activation / batch norm,
+    blocks.py:134-135): the reference's state-dict layout (conv, activation, batch norm,
+    dropout), eval mode equal to the same weights without dropout, about a fraction p of the
+    outputs zeroed in training mode with fresh masks each pass, and the backward applying the
+    forward's mask (final-layer bias gradient = sum of dy * keep / (1 - p))."""
+    from quantem_b200.core.ml.cnn import CNN2d
+
+    p = 0.3
+    net = CNN2d(4, 3, start_filters=8, num_layers=2, dropout=p, device=cuda_device, seed=1)
+    keys = set(net.state_dict())
+    for k in ("down_conv_blocks.0.block.0.weight", "down_conv_blocks.0.block.2.weight",
+              "down_conv_blocks.0.block.4.weight", "down_conv_blocks.0.block.6.weight", "final_conv.block.0.weight"):
+        assert k in keys, k
+    ref = CNN2d(4, 3, start_filters=8, num_layers=2, device=cuda_device, seed=1)
+
+    def rename(k):
+        parts = k.split(".")
+        if "block" in parts and not k.startswith("final_conv"):
+            i = parts.index("block") + 1
+            j, pos = divmod(int(parts[i]), 4)
+            parts[i] = str(3 * j + pos)
+        return ".".join(parts)
+
+    ref.load_state_dict({rename(k): v for k, v in net.state_dict().items()})
+    x = torch.randn(2, 4, 16, 16, device=cuda_device)
+    net.eval()
+    ref.eval()
+    with torch.no_grad():
+        assert torch.equal(net(x), ref(x))
+    net.train()
+    y = net(x)
+    y2 = net(x)
+    frac = float((y == 0).float().mean())
+    assert abs(frac - p) < 0.05
+    assert not torch.equal(y, y2)
+    dy = torch.randn_like(y2)
+    (y2 * dy).sum().backward()
+    g = net.named_gradients()["final_conv.block.0.bias"]
+    want = (dy * (y2 != 0).float() / (1 - p)).sum(dim=(0, 2, 3))
+    assert torch.allclose(g, want, rtol=1e-4, atol=1e-5)
