@@ -130,7 +130,9 @@ template <int E, int T>
 __device__ __forceinline__ void store_pairs(float2* dst, int tid, const float2 (&x)[E]) {
   float4* d = reinterpret_cast<float4*>(dst) + tid;
 #pragma unroll
-  for (int e = 0; e < E; e += 2) d[(e >> 1) * T] = make_float4(x[e].x, x[e].y, x[e + 1].x, x[e + 1].y);
+  for (int e = 0; e < E; e += 2)
+    asm volatile("st.global.L1::no_allocate.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(d + (e >> 1) * T),
+                 "f"(x[e].x), "f"(x[e].y), "f"(x[e + 1].x), "f"(x[e + 1].y) : "memory");
 }
 template <int E, int T>
 __device__ __forceinline__ void load_pairs(const float2* src, int tid, float2 (&x)[E]) {
