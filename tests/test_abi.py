@@ -125,3 +125,38 @@ def test_lazy_conjugate_views_are_rejected_or_resolved():
         ops._req(z.conj(), "x", torch.complex64)
     d = ops.dense(z.conj())
     assert not d.is_conj() and torch.equal(d, torch.tensor([1 - 2j, 3 + 1j], dtype=torch.complex64))
+
+
+def test_new_entry_points_validate_arguments_without_gpu():
+    """Probe constraints, bilinear centring, AMSGrad / momentum steps, dropout and the GEMM
+    activation flags: bad arguments are rejected before any CUDA call."""
+    from quantem_b200 import _lib
+
+    lib = _lib.lib()
+    d = ctypes.c_void_p(256)  # never dereferenced: every call below fails validation
+    assert lib.ptycho_probe_center_work_elems(2, 64) == 2 * 2 * 64 * 64 + 6 * 16
+    assert lib.ptycho_probe_center(d, d, 17, 64, ctypes.c_void_p(512), 10 ** 9, None) == 1   # P <= 16
+    assert lib.ptycho_probe_center(d, d, 2, 100, ctypes.c_void_p(512), 10 ** 9, None) == 2   # n not built
+    assert lib.ptycho_probe_center(d, d, 2, 64, ctypes.c_void_p(512), 10, None) == 1         # work too small
+    assert lib.ptycho_probe_center(d, d, 2, 64, ctypes.c_void_p(512), 10 ** 9, None) == 1    # out aliases probe
+    assert lib.ptycho_probe_center_vjp(d, ctypes.c_void_p(512), d, 2, 64, ctypes.c_void_p(768), 10 ** 9,
+                                       None) == 1                                             # grad aliases probe
+    nw = lib.ptycho_probe_tv_work_elems()
+    assert lib.ptycho_probe_tv(d, 2, 64, ctypes.c_float(0.1), ctypes.c_void_p(512), None, ctypes.c_void_p(768),
+                               nw - 1, None) == 1                                             # work too small
+    assert lib.ptycho_probe_tv(d, 2, 64, ctypes.c_float(0.1), ctypes.c_void_p(512), d, ctypes.c_void_p(768), nw,
+                               None) == 1                                                     # grad aliases probe
+    assert lib.ptycho_pattern_bilinear(d, ctypes.c_void_p(512), 4, 63, ctypes.c_void_p(768), None, None) == 1  # odd n
+    assert lib.ptycho_pattern_bilinear(d, ctypes.c_void_p(512), 4, 64, d, None, None) == 1   # output aliases input
+    assert lib.ptycho_adam_amsgrad_step(d, d, d, d, None, 10, ctypes.c_float(1e-3), None, ctypes.c_float(0.9),
+                                        ctypes.c_float(0.999), ctypes.c_float(1e-8), ctypes.c_float(0), 0,
+                                        ctypes.c_float(0.1), ctypes.c_float(0.1), None) == 1  # no max buffer
+    assert lib.ptycho_sgd_momentum_step(d, d, None, 10, ctypes.c_float(0.1), None, ctypes.c_float(0),
+                                        ctypes.c_float(0.9), ctypes.c_float(0), 0, 1, None) == 1  # no buffer
+    assert lib.ptycho_cnn_dropout(d, 0, 4, 4, 4, ctypes.c_float(1.5), ctypes.c_uint64(1), None) == 1  # p > 1
+    assert lib.ptycho_cnn_dropout(d, 2, 4, 4, 4, ctypes.c_float(0.5), ctypes.c_uint64(1), None) == 1  # dtype
+    flags = 1 | (9 << 8)  # BF16 output with an activation id that does not exist
+    assert lib.ptycho_gemm_bf16(d, 64, d, 64, d, 64, 128, 64, 64, None, flags, 1, None, None) == 1
+    assert "activation" in _lib.last_error()
+    assert lib.ptycho_gemm_bf16(d, 64, d, 64, d, 64, 128, 64, 64, None, 4 | (4 << 8), 1, None, None) == 1
+    assert "atomic" in _lib.last_error()
