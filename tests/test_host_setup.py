@@ -198,3 +198,28 @@ def test_model_api_members_on_the_host():
     assert torch.equal(pm.apply_hard_constraints(pm._probe.detach()), pm.probe.detach())
     om = pt.obj_model
     assert om.name == "ObjPixelized" and om.shape_2d == tuple(pt.obj_shape_full[-2:])
+
+
+def test_host_probe_constraint_gradients_match_oracle():
+    """The host (set-up) forms of the probe's centre-of-mass shift and TV loss: torch autograd
+    through them against the FP64 oracle's reverse chain."""
+    from oracle import ptycho_oracle as O
+    from quantem_b200.diffractive_imaging.ptycho_utils import center_probe, probe_tv_loss
+
+    rng = np.random.default_rng(12)
+    n = 32
+    y, x = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    p = np.stack([np.exp(-(((y - 4.2) % n) ** 2 + ((x - n + 6.1) % n) ** 2) / 25.0) * np.exp(0.3j * k * x)
+                  for k in range(2)]) + 0.02 * rng.standard_normal((2, n, n))
+    g = rng.standard_normal((2, n, n)) + 1j * rng.standard_normal((2, n, n))
+    t = torch.as_tensor(p, dtype=torch.complex128).requires_grad_(True)
+    out = center_probe(t)
+    ref, cache = O.center_probe(p)
+    # the host form forms -2 pi i k in complex64 first, as the reference's ramp does; the oracle
+    # keeps it in float64
+    assert rel(out.detach().numpy(), ref) < 1e-6
+    (out.conj() * torch.as_tensor(g)).real.sum().backward()
+    assert rel(t.grad.numpy(), O.center_probe_vjp(cache, g)) < 1e-6
+    t.grad = None
+    probe_tv_loss(t, 0.2).backward()
+    assert rel(t.grad.numpy(), O.probe_tv_loss(p, 0.2)[1]) < 1e-12
