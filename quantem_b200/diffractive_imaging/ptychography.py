@@ -14,6 +14,7 @@ from typing import Literal
 import numpy as np
 import scipy.ndimage as ndi
 import torch
+from tqdm.auto import tqdm
 
 from ..core import config
 from .. import ops
@@ -804,14 +805,16 @@ class Ptychography:
         stream = HostTargetStream(tg, dev) if tg.device.type != "cuda" and num_iters > 0 else None
         self.last_h2d_bytes_per_iter = stream.bytes_per_copy if stream is not None else 0
         nvtx = torch.cuda.nvtx  # profiler ranges (iteration, batch); no cost without a profiler
-        # when nothing reads the loss during the run (no scheduler, logger, validation split or
-        # snapshots) and ``loss_readback`` is "auto", each iteration's loss stays on the device and
-        # all are read once at the end, with the status word: the host queues iteration after
-        # iteration without waiting.  "iteration" reads every iteration's loss when it ends.
+        # when nothing reads the loss during the run (no scheduler, logger, validation split,
+        # snapshots or progress bar) and ``loss_readback`` is "auto", each iteration's loss stays
+        # on the device and all are read once at the end, with the status word: the host queues
+        # iteration after iteration without waiting.  "iteration" reads each when it ends.
         defer = (self.loss_readback == "auto" and self.logger is None and not batcher.has_validation
-                 and not self._store_snapshots and not self.schedulers)
+                 and not self._store_snapshots and not self.schedulers and not self.verbose)
         pending = []
-        for a0 in range(num_iters):
+        # progress bar with the loss when verbose (ptychography.py:206-300), on stderr
+        pbar = tqdm(range(num_iters), disable=not self.verbose)
+        for a0 in pbar:
             nvtx.range_push(f"reconstruct iteration {self.num_iters}")
             total = torch.zeros((), dtype=torch.float32, device=dev)
             nb = 0
@@ -935,6 +938,9 @@ class Ptychography:
             if self.logger is not None:
                 self.logger.log_iter(self.obj_model, self.probe_model, self.dset, self.num_iters - 1,
                                      consistency_loss, nb, self._get_current_lrs())
+            if self.verbose:
+                text = f"Iter {a0 + 1}/{num_iters}, Loss: {total_loss:.3e}"
+                pbar.set_description(text if val_loss is None else f"{text}, Val: {val_loss:.3e}")
             nvtx.range_pop()
         if pending:  # one read of every iteration's loss and of the status word
             losses = torch.stack(pending).cpu().tolist()
