@@ -160,3 +160,6 @@ def test_new_entry_points_validate_arguments_without_gpu():
     assert "activation" in _lib.last_error()
     assert lib.ptycho_gemm_bf16(d, 64, d, 64, d, 64, 128, 64, 64, None, 4 | (4 << 8), 1, None, None) == 1
     assert "atomic" in _lib.last_error()
+    for act in (-1, 7):  # activation ids of the batch-norm backward: 0 .. 6
+        assert lib.ptycho_cnn_bn_backward(d, 8, d, 8, 16, 8, None, None, None, 1, act, None, None, None, 0, d, None, 8,
+                                          None) == 1
